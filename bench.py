@@ -1,0 +1,441 @@
+#!/usr/bin/env python
+"""Searchlight solves/sec on the hemisphere template workload.
+
+One step = one searchlight Procrustes pass (with scaling) over a hemisphere:
+10242 Fibonacci-sphere vertices, nt = 400, one searchlight of 100-300 vertices
+per vertex, subject 1 aligned onto subject 0 of the template workload, output
+the weighted transforms combined into the symmetric CSC/CSR matrix.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+value     device-resident inputs (float64 X, Y already in HBM), CUDA events around each
+          step on the launching stream, L2 flushed (256 MiB write) between steps
+e2e       the C ABI dense entry point (ha_searchlight_procrustes_dense, backend 4) from
+          host float64 buffers into a host nv x nv float64 matrix, wall clock per call
+plain_fp32  the same step with the plain FP32 form (FP32 Jacobi, no refinement, no FP64)
+roofline  dominant kernel (per-kind CUDA event times recorded by the library)
+cpu_baseline  the reference C library (oracle/_ref, cpu64 arm, all host threads) on a
+          bounded sample of the same searchlights
+--impl reference  times only the reference CPU implementation (rank 0 of any N)
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "searchlight solves/sec vs plain FP32 GPU form at stated FP64-oracle error"
+UNIT = "searchlights/s"
+WORKLOAD = "hemisphere_template_pair"
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
+FP32_SIMT_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    p.add_argument("--nv", type=int, default=10242)
+    p.add_argument("--nt", type=int, default=400)
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    return p.parse_args()
+
+
+def workload(seed, nv, nt):
+    from hyperalignment_b200 import workloads as W
+    return W.template_procrustes_pair(seed=seed, nv=nv, nt=nt)
+
+
+def config_dict(w, extra=None):
+    sizes = w.sls.sizes
+    d = {"workload": WORKLOAD, "nv": w.nv, "nt": w.nt, "searchlights": w.sls.count,
+         "sl_size_min": int(sizes.min()), "sl_size_max": int(sizes.max()), "sl_size_mean": round(float(sizes.mean()), 2),
+         "scaling": True, "reflection": True, "weights": "linear distance",
+         "l2": "flushed between steps (256 MiB write)"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f), "measured"
+    return dict(PEAKS_FALLBACK), "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.lines = []
+        self.proc = None
+        self.th = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+            return
+        self.th = threading.Thread(target=self._read, daemon=True)
+        self.th.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.th:
+            self.th.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ---------------------------------------------------------------------------------------------
+# reference CPU arm
+# ---------------------------------------------------------------------------------------------
+
+def reference_rate(w, seconds, threads, start=0):
+    """Reference cpu64 dense entry point on a contiguous sample of searchlights sized to ~seconds."""
+    from oracle import ref_lib as R
+    R.set_threads(threads)
+    s = w.sls
+    # size the sample from a short probe
+    probe = s.subset(np.arange(start, min(start + 4 * threads, s.count)))
+    Xf, Yf = np.asfortranarray(w.X), np.asfortranarray(w.Y)
+    t0 = time.perf_counter()
+    _ref_call(R, Xf, Yf, probe)
+    dt = time.perf_counter() - t0
+    rate = probe.count / max(dt, 1e-6)
+    m = int(min(s.count, max(threads, rate * seconds)))
+    idx = (start + np.arange(m)) % s.count
+    sample = s.subset(idx)
+    t0 = time.perf_counter()
+    _ref_call(R, Xf, Yf, sample)
+    dt = time.perf_counter() - t0
+    return sample.count / dt, sample.count, dt
+
+
+_REF_T = {}
+
+
+def _ref_call(R, Xf, Yf, sls):
+    h = R.lib()
+    nt, nv = Xf.shape
+    T = _REF_T.get(nv)
+    if T is None:
+        T = _REF_T[nv] = np.zeros((nv, nv))
+    rc = h.ha_searchlight_procrustes_dense(
+        Xf.ctypes.data_as(R.c_double_p), Yf.ctypes.data_as(R.c_double_p), nt, nv,
+        sls.indices.ctypes.data_as(R.c_int32_p), sls.offsets.ctypes.data_as(R.c_int32_p),
+        sls.dists.ctypes.data_as(R.c_double_p), sls.count, sls.radius, T.ctypes.data_as(R.c_double_p),
+        True, True, 0, True)
+    if rc != 0:
+        raise RuntimeError(f"reference rc={rc}")
+
+
+def run_reference(args):
+    ws, rank, _ = dist_setup(args)
+    if rank != 0:
+        return
+    from oracle import ref_lib as R
+    if not R.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libhyperalignment.so not built"}))
+        return
+    w = workload(0, args.nv, args.nt)
+    threads = os.cpu_count() or 1
+    budget = max(2.0, 150.0 / max(1, args.steps + args.warmup))
+    rates, times, counts = [], [], []
+    start = 0
+    for i in range(args.warmup + args.steps):
+        r, m, dt = reference_rate(w, budget, threads, start)
+        start = (start + m) % w.sls.count
+        if i >= args.warmup:
+            rates.append(r)
+            times.append(dt)
+            counts.append(m)
+    value = float(sum(counts) / sum(times))
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": float(1e3 * np.mean(times)), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_dict(w, {"sample": f"{int(np.mean(counts))} searchlights per step (contiguous, rotating)"}),
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"{int(np.mean(counts))} of {w.sls.count} searchlights per step, cpu64 arm, "
+                                   f"OpenMP {threads} threads, OPENBLAS_NUM_THREADS=1"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+
+
+# ---------------------------------------------------------------------------------------------
+# B200 arm
+# ---------------------------------------------------------------------------------------------
+
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+    from hyperalignment_b200 import _lib as L
+    from hyperalignment_b200.plan import Plan
+
+    ws, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    lib = L.lib()
+    L.check(lib.ha_b200_init(), "ha_b200_init")
+
+    w = workload(rank, args.nv, args.nt)
+    plan = Plan.from_workload(w)
+    dev = torch.device("cuda", local)
+    dX = torch.from_numpy(np.asfortranarray(w.X).ravel(order="F")).to(dev)
+    dY = torch.from_numpy(np.asfortranarray(w.Y).ravel(order="F")).to(dev)
+    vals = torch.zeros(plan.nnz, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step(solver):
+        plan.procrustes_device(dX.data_ptr(), dY.data_ptr(), vals.data_ptr(), True, True, solver, L.OUT_CSR,
+                               stream.cuda_stream)
+
+    def timed_loop(solver, k, sample_clocks=False, trace=False):
+        for _ in range(args.warmup):
+            step(solver)
+        torch.cuda.synchronize()
+        if ws > 1:
+            dist.barrier()
+        sampler = ClockSampler(local) if sample_clocks else None
+        if sampler:
+            sampler.start()
+            time.sleep(0.5)
+        if trace:
+            lib.ha_b200_kernel_times(None, None)
+            lib.ha_b200_set_kernel_timing(True)
+        n0 = lib.ha_b200_launch_count()
+        torch.cuda.synchronize()
+        evs = []
+        t0 = time.perf_counter()
+        for _ in range(k):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            step(solver)
+            b.record(stream)
+            evs.append((a, b))
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        launches = lib.ha_b200_launch_count() - n0
+        kt = None
+        if trace:
+            lib.ha_b200_set_kernel_timing(False)
+            ms = np.zeros(len(L.KERNEL_KINDS))
+            cnt = np.zeros(len(L.KERNEL_KINDS), dtype=np.int64)
+            lib.ha_b200_kernel_times(ms.ctypes.data_as(L.c_double_p), cnt.ctypes.data_as(L.c_int64_p))
+            kt = (ms, cnt)
+        clocks = sampler.stop() if sampler else None
+        dev_ms = float(sum(a.elapsed_time(b) for a, b in evs))
+        t = torch.tensor([dev_ms], dtype=torch.float64, device=dev)
+        if ws > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            dist.barrier()
+        return float(t.item()), wall, launches, kt, clocks
+
+    K = args.steps
+    total_ms, wall, launches, kt, clocks = timed_loop(L.SOLVER_MIXED, K, sample_clocks=True, trace=True)
+    value = ws * w.sls.count * K / (total_ms / 1e3)
+    plain_ms, _, _, _, _ = timed_loop(L.SOLVER_FP32, K)
+    plain_value = ws * w.sls.count * K / (plain_ms / 1e3)
+    fp64_ms, _, _, _, _ = timed_loop(L.SOLVER_FP64, max(1, K // 4))
+    fp64_value = ws * w.sls.count * max(1, K // 4) / (fp64_ms / 1e3)
+    stats = plan.stats()
+
+    # accuracy vs the float64 oracle on a fixed sample of searchlights (both forms)
+    from oracle import ha_oracle as O
+    rng = np.random.default_rng(123)
+    sample = np.sort(rng.choice(w.sls.count, size=12, replace=False))
+    errs = {}
+    for name, solver in (("mixed", L.SOLVER_MIXED), ("plain_fp32", L.SOLVER_FP32)):
+        step(solver)
+        torch.cuda.synchronize()
+        e = []
+        for q in sample:
+            T = plan.local_transforms(int(q), 1)[0]
+            sl = w.sls.indices[w.sls.offsets[q]:w.sls.offsets[q + 1]]
+            Tref = O.procrustes(w.X[:, sl], w.Y[:, sl], True, False)
+            e.append((np.linalg.norm(T - Tref) / np.linalg.norm(Tref), np.abs(T - Tref).max()))
+        e = np.array(e)
+        errs[name] = {"T_relfrob_max": float(e[:, 0].max()), "T_relfrob_median": float(np.median(e[:, 0])),
+                      "T_maxabs_max": float(e[:, 1].max()), "sample": int(sample.size)}
+
+    # roofline of the dominant kernel
+    peaks, peak_src = load_peaks()
+    ms, cnt = kt
+    dom = int(np.argmax(ms))
+    dom_name = L.KERNEL_KINDS[dom]
+    sizes = w.sls.sizes.astype(np.float64)
+    alg = {
+        "jacobi32": ("flop", 21.0 * (sizes ** 3).sum()),
+        "xcov32": ("flop", 2.0 * w.nt * (sizes ** 2).sum()),
+        "refine": ("flop", 4.0 * (sizes ** 3).sum()),
+        "formT32": ("flop", 2.0 * (sizes[sizes > 164] ** 3).sum()),
+        "reduce": ("byte", (sizes ** 2).sum() * 4 + plan.nnz * 16.0),
+    }
+    roof = None
+    if dom_name in alg and ms[dom] > 0:
+        kind, per_step = alg[dom_name]
+        per_launch = per_step * K / max(1, cnt[dom])
+        avg_ms = ms[dom] / max(1, cnt[dom])
+        achieved = per_launch / (avg_ms / 1e3)
+        if kind == "flop":
+            peak = float(peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops")))
+            roof = {"bound": "tensor", "kernel": dom_name, "achieved": achieved / 1e12, "peak": peak,
+                    "unit": "TFLOP/s", "frac": achieved / 1e12 / peak, "traffic": None,
+                    "peak_source": f"{peak_src} bf16 sustained",
+                    "fp32_simt": {"peak_nominal": FP32_SIMT_NOMINAL_TFLOPS,
+                                  "frac": achieved / 1e12 / FP32_SIMT_NOMINAL_TFLOPS},
+                    "algorithmic": "21 n^3 flops per searchlight (square SVD, Golub-Van Loan count)"}
+        else:
+            peak = float(peaks["hbm_gbs"])
+            roof = {"bound": "hbm", "kernel": dom_name, "achieved": achieved / 1e9, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / 1e9 / peak, "traffic": None, "peak_source": f"{peak_src} hbm copy"}
+    traffic_file = os.path.join(ROOT, "profiles", "traffic.json")
+    if roof is not None and os.path.exists(traffic_file):
+        with open(traffic_file) as f:
+            tr = json.load(f)
+        if dom_name in tr:
+            roof["traffic"] = tr[dom_name].get("bytes_per_launch")
+    kernel_share = {L.KERNEL_KINDS[i]: {"ms_per_step": float(ms[i] / K), "launches_per_step": float(cnt[i] / K)}
+                    for i in range(len(ms)) if cnt[i] > 0}
+
+    # end to end through the C ABI dense entry point (host buffers)
+    e2e = None
+    if not args.no_e2e:
+        Xf, Yf = np.asfortranarray(w.X), np.asfortranarray(w.Y)
+        T_out = np.zeros((w.nv, w.nv))
+        s = w.sls
+        argsv = (Xf.ctypes.data_as(L.c_double_p), Yf.ctypes.data_as(L.c_double_p), w.nt, w.nv,
+                 L.iptr(s.indices), L.iptr(s.offsets), L.dptr(s.dists), s.count, s.radius,
+                 T_out.ctypes.data_as(L.c_double_p), True, True, L.BACKEND_B200, True)
+        lib.ha_set_num_threads(os.cpu_count() or 1)
+        for _ in range(max(1, args.warmup)):
+            L.check(lib.ha_searchlight_procrustes_dense(*argsv), "dense")
+        if ws > 1:
+            dist.barrier()
+        ts = []
+        for _ in range(K):
+            t0 = time.perf_counter()
+            L.check(lib.ha_searchlight_procrustes_dense(*argsv), "dense")
+            ts.append(time.perf_counter() - t0)
+        tmax = torch.tensor([sum(ts)], dtype=torch.float64, device=dev)
+        if ws > 1:
+            dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        e2e = {"value": ws * s.count * K / float(tmax.item()), "unit": UNIT,
+               "h2d_bytes_per_step": int(2 * w.nt * w.nv * 8), "d2h_bytes_per_step": int(plan.nnz * 8),
+               "path": "ha_searchlight_procrustes_dense(backend=4) host float64 in, host dense nv x nv out (+=)"}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        from oracle import ref_lib as R
+        if R.available():
+            threads = os.cpu_count() or 1
+            r, m, dt = reference_rate(w, args.cpu_seconds, threads)
+            cpu = {"value": r, "unit": UNIT, "cores": threads, "kind": "reference",
+                   "sample": f"{m} contiguous searchlights of {w.sls.count} ({dt:.1f} s), reference cpu64 arm, "
+                             f"OpenMP {threads} threads, OPENBLAS_NUM_THREADS=1"}
+        else:
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                   "sample": "oracle/_ref/libhyperalignment.so not built"}
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": args.warmup,
+            "ms_per_step": total_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": config_dict(w, {"parallelism": f"replicas x{ws} (one subject pair per GPU)" if ws > 1 else "single GPU",
+                                      "solver": "FP32 Jacobi + FP32 Newton-Schulz refinement, FP64 re-solve below sigma ratio 1e-4"}),
+            "plain_fp32": {"value": plain_value, "unit": UNIT, "ms_per_step": plain_ms / K,
+                           "speedup_of_value": value / plain_value},
+            "fp64_form": {"value": fp64_value, "unit": UNIT},
+            "error_vs_fp64": errs,
+            "solver_stats": stats,
+            "roofline": roof,
+            "kernels": kernel_share,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "wall_s_timed": wall,
+        }
+        print(json.dumps(out))
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,16 @@
+"""B200-native searchlight alignment backend for the hyperalignment C API.
+
+The compute path is ``libha_b200.so`` (hand-written sm_100a CUDA behind a C
+ABI, include/hyperalignment_b200.h); this package holds its ctypes binding,
+the reference-shaped Python wrapper and the synthetic workload generators.
+"""
+
+from . import _lib  # noqa: F401
+from .hyperalignment_c import (  # noqa: F401
+    cleanup,
+    searchlight_procrustes,
+    searchlight_procrustes_csc,
+    searchlight_ridge_csc,
+    searchlight_weights,
+    sparse_pattern,
+)

@@ -1,0 +1,959 @@
+// ha_b200.cu -- host side of the B200 searchlight alignment backend: plans, launches and the C ABI.
+//
+// A plan holds everything that depends only on the searchlight geometry (weights, per-vertex
+// membership lists, the symmetric CSC pattern, size buckets, scratch layout).  A run converts
+// the float64 inputs on the device, solves every searchlight (cross-covariance, Jacobi polar,
+// refinement, reflection fix) chunk by chunk, and reduces the weighted local transforms into
+// the pattern's values with a deterministic segmented reduction.
+
+#include "../../include/hyperalignment_b200.h"
+#include "ha_b200_kernels.cuh"
+
+#include <cuda_runtime.h>
+#include <omp.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <vector>
+
+using namespace hab200;
+
+namespace {
+
+constexpr int kBlock = 256;
+constexpr size_t kSmemMax = 220 * 1024;  // dynamic shared memory budget per CTA (B200 opt-in max is 227 KB)
+
+#define HA_CUDA(call)                                                                              \
+	do {                                                                                           \
+		cudaError_t e_ = (call);                                                                   \
+		if (e_ != cudaSuccess) {                                                                   \
+			fprintf(stderr, "ha_b200: %s failed: %s (%s:%d)\n", #call, cudaGetErrorString(e_),     \
+			        __FILE__, __LINE__);                                                           \
+			return kHaErrorInternal;                                                               \
+		}                                                                                          \
+	} while (0)
+
+std::recursive_mutex g_mu;
+bool g_inited = false;
+int g_threads = 0;
+
+// ---- launch tracing: optional CUDA events around every launch, and a launch counter ----
+int64_t g_launches = 0;
+bool g_timing = false;
+struct TimedLaunch {
+	int kind;
+	cudaEvent_t a, b;
+};
+std::vector<TimedLaunch> g_timed;
+double g_kernel_ms[kHaB200NumKernelKinds] = {0};
+int64_t g_kernel_n[kHaB200NumKernelKinds] = {0};
+
+struct LaunchScope {
+	int kind;
+	cudaStream_t st;
+	cudaEvent_t a = nullptr, b = nullptr;
+	LaunchScope(int k, cudaStream_t s) : kind(k), st(s) {
+		g_launches++;
+		g_kernel_n[k]++;
+		if (g_timing && cudaEventCreate(&a) == cudaSuccess && cudaEventCreate(&b) == cudaSuccess)
+			cudaEventRecord(a, st);
+	}
+	~LaunchScope() {
+		if (a && b) {
+			cudaEventRecord(b, st);
+			g_timed.push_back({kind, a, b});
+		}
+	}
+};
+#define HA_LAUNCH(kind, st) LaunchScope ha_scope_##__LINE__((kind), (st))
+
+template <typename T>
+struct DevArr {
+	T *p = nullptr;
+	size_t n = 0;  // capacity in elements
+	int ensure(size_t count) {
+		if (count <= n && p) return kHaSuccess;
+		if (p) cudaFree(p);
+		p = nullptr;
+		n = 0;
+		size_t want = std::max<size_t>(count, 1);
+		if (cudaMalloc(&p, want * sizeof(T)) != cudaSuccess) {
+			cudaGetLastError();
+			fprintf(stderr, "ha_b200: cudaMalloc of %zu bytes failed\n", want * sizeof(T));
+			p = nullptr;
+			return kHaErrorAlloc;
+		}
+		n = want;
+		return kHaSuccess;
+	}
+	void release() {
+		if (p) cudaFree(p);
+		p = nullptr;
+		n = 0;
+	}
+};
+
+// Buffers for the host-memory entry points (inputs, outputs), kept between calls.
+struct HostCallBufs {
+	DevArr<double> X64, Y64, Xtmp, vals;
+	std::vector<double> h_vals;
+	void release() {
+		X64.release(); Y64.release(); Xtmp.release(); vals.release();
+		std::vector<double>().swap(h_vals);
+	}
+} g_bufs;
+
+size_t real_bytes(bool fp64) { return fp64 ? 8 : 4; }
+
+// Jacobi block layout for a searchlight of n vertices in a given precision.
+void jacobi_layout(int n, bool fp64, int &bsz, int &nblk, size_t &smem) {
+	const size_t rb = real_bytes(fp64);
+	const size_t extra = (size_t)(2 * 16 * 65 + 8) * rb;
+	int h = (n + 1) / 2;
+	size_t res = ((size_t)4 * h * n + 2 * h + 2) * rb + extra;
+	if (res <= kSmemMax) {
+		bsz = h;
+		nblk = 2;
+		smem = res;
+		return;
+	}
+	int b = 32;
+	while (b > 1 && ((size_t)4 * b * n + 2 * b + 2) * rb + extra > kSmemMax) b--;
+	bsz = b;
+	nblk = (n + b - 1) / b;
+	if (nblk & 1) nblk++;
+	smem = ((size_t)4 * b * n + (size_t)nblk * b + 2) * rb + extra;
+	if (smem < ((size_t)4 * b * n + 2 * b + 2) * rb + extra) smem = ((size_t)4 * b * n + 2 * b + 2) * rb + extra;
+}
+
+struct Bucket {
+	int first, count;  // range in the chunk's work array
+	size_t smem;
+	bool blocked;
+};
+
+struct Chunk {
+	int s0, s1;
+	std::vector<SlWork> w32, w64;
+	std::vector<Bucket> b32, b64;
+	std::vector<int64_t> tofs;  // per slot
+	int64_t scratch_elems8;     // scratch size in 8-byte units (A and V each)
+	int64_t t_elems;            // T scratch floats
+	int64_t uv_elems;
+	SlWork *d_w32 = nullptr, *d_w64 = nullptr;
+	int64_t *d_tofs = nullptr;
+};
+
+}  // namespace
+
+struct HaB200Plan {
+	int nt = 0, nv = 0, count = 0;
+	int64_t total = 0;
+	int max_n = 0;
+	std::vector<int32_t> h_off, h_idx;
+	std::vector<double> h_w;
+	bool has_weights = true;
+	// device geometry
+	DevArr<int32_t> idx, off, lo, hi;
+	DevArr<double> w;
+	DevArr<int64_t> vlptr;
+	DevArr<int2> vlent;
+	DevArr<int64_t> patptr;
+	DevArr<int32_t> patcol;
+	int64_t nnz = 0;
+	int max_row = 0;
+	std::vector<int64_t> h_patptr;
+	std::vector<int32_t> h_patcol;
+	// chunks and scratch
+	std::vector<Chunk> chunks;
+	DevArr<double> scrA, scrV;  // 8-byte units, reinterpreted per precision
+	DevArr<float> scrT;
+	DevArr<double> uv, scale;
+	DevArr<SlStats> stats;
+	int max_slots = 0;
+	// per-run data
+	DevArr<float> X32, Y32;
+	DevArr<double> var;
+	DevArr<int32_t> counters;  // [n_fp64, n_unconverged]
+	int last_chunk = -1;
+	int last_rowmajor = 1;
+};
+
+namespace {
+
+int check_cuda_ready() {
+	if (!g_inited) {
+		int rc = ha_b200_init();
+		if (rc != kHaSuccess) return rc;
+	}
+	return kHaSuccess;
+}
+
+uint64_t fnv1a(const void *data, size_t bytes, uint64_t h) {
+	const unsigned char *p = (const unsigned char *)data;
+	for (size_t i = 0; i < bytes; i++) {
+		h ^= p[i];
+		h *= 1099511628211ULL;
+	}
+	return h;
+}
+
+// Flat weights exactly as csrc/ha_searchlight.c:970-1001 (same operation order, float64).
+void compute_weights(const int32_t *idx, const int32_t *off, const double *dists, int32_t count, double radius,
+                     int32_t nv, double *out) {
+	const int64_t total = off[count];
+	std::vector<double> vsum((size_t)nv, 0.0);
+	if (dists == nullptr) {
+		for (int64_t k = 0; k < total; k++) vsum[idx[k]] += 1.0;
+		for (int64_t k = 0; k < total; k++) out[k] = 1.0 / vsum[idx[k]];
+	} else {
+		for (int64_t k = 0; k < total; k++) {
+			double w = (radius - dists[k]) / radius;
+			vsum[idx[k]] += w;
+		}
+		for (int64_t k = 0; k < total; k++) {
+			double w = (radius - dists[k]) / radius;
+			out[k] = w / vsum[idx[k]];
+		}
+	}
+}
+
+int validate_searchlights(const int32_t *idx, const int32_t *off, int32_t count, int32_t nv) {
+	if (!idx || !off || count <= 0 || nv <= 0) return kHaErrorArg;
+	if (off[0] != 0) {
+		fprintf(stderr, "ha_b200: sl_offsets[0] must be 0\n");
+		return kHaErrorArg;
+	}
+	std::vector<int32_t> mark((size_t)nv, -1);
+	for (int32_t s = 0; s < count; s++) {
+		if (off[s + 1] <= off[s]) {
+			fprintf(stderr, "ha_b200: searchlight %d is empty or offsets decrease\n", s);
+			return kHaErrorArg;
+		}
+		for (int32_t k = off[s]; k < off[s + 1]; k++) {
+			int32_t v = idx[k];
+			if (v < 0 || v >= nv) {
+				fprintf(stderr, "ha_b200: searchlight %d has vertex %d outside [0, %d)\n", s, v, nv);
+				return kHaErrorArg;
+			}
+			if (mark[v] == s) {
+				fprintf(stderr, "ha_b200: searchlight %d lists vertex %d twice\n", s, v);
+				return kHaErrorArg;
+			}
+			mark[v] = s;
+		}
+	}
+	return kHaSuccess;
+}
+
+size_t scratch_budget_bytes() {
+	const char *e = getenv("HA_B200_SCRATCH_GB");
+	double gb = e ? atof(e) : 16.0;
+	if (!(gb > 0.01)) gb = 16.0;
+	return (size_t)(gb * 1073741824.0);
+}
+
+int build_chunks(HaB200Plan *P) {
+	const size_t budget = scratch_budget_bytes();
+	P->chunks.clear();
+	int s = 0;
+	while (s < P->count) {
+		Chunk ch;
+		ch.s0 = s;
+		int64_t acc8 = 0, tacc = 0, uvacc = 0;
+		std::vector<int64_t> tofs;
+		std::vector<int64_t> aofs8;
+		std::vector<int> bs32, nb32, bs64, nb64;
+		std::vector<size_t> sm32, sm64;
+		while (s < P->count) {
+			int n = P->h_off[s + 1] - P->h_off[s];
+			int b32, k32, b64, k64;
+			size_t m32, m64;
+			jacobi_layout(n, false, b32, k32, m32);
+			jacobi_layout(n, true, b64, k64, m64);
+			int64_t e32 = ((int64_t)n * k32 * b32 * 4 + 7) / 8;
+			int64_t e64 = (int64_t)n * k64 * b64;
+			int64_t region = std::max<int64_t>(std::max(e32, e64), (int64_t)n * n);
+			region = (region + 31) & ~(int64_t)31;
+			size_t bytes_if = (size_t)(acc8 + region) * 8 * 2 + (size_t)(tacc + (int64_t)n * n) * 4;
+			if (!tofs.empty() && bytes_if > budget) break;
+			aofs8.push_back(acc8);
+			tofs.push_back(tacc);
+			acc8 += region;
+			tacc += (int64_t)n * n;
+			bs32.push_back(b32); nb32.push_back(k32); sm32.push_back(m32);
+			bs64.push_back(b64); nb64.push_back(k64); sm64.push_back(m64);
+			uvacc += 2 * (int64_t)n;
+			s++;
+		}
+		ch.s1 = s;
+		ch.scratch_elems8 = acc8;
+		ch.t_elems = tacc;
+		ch.uv_elems = uvacc;
+		ch.tofs = tofs;
+		const int nsl = ch.s1 - ch.s0;
+		// work items, bucketed by (mode, n range), largest first inside a bucket
+		for (int prec = 0; prec < 2; prec++) {
+			std::vector<SlWork> items;
+			int64_t uvo = 0;
+			for (int q = 0; q < nsl; q++) {
+				int sidx = ch.s0 + q;
+				int n = P->h_off[sidx + 1] - P->h_off[sidx];
+				SlWork w;
+				w.s = sidx;
+				w.n = n;
+				w.bsz = prec ? bs64[q] : bs32[q];
+				w.nblk = prec ? nb64[q] : nb32[q];
+				w.aofs = prec ? aofs8[q] : aofs8[q] * 2;
+				w.tofs = tofs[q];
+				w.sofs = P->h_off[sidx];
+				w.slot = q;
+				w.uvofs = uvo;
+				uvo += 2 * (int64_t)n;
+				items.push_back(w);
+			}
+			auto key = [](const SlWork &w) {
+				int band = w.n <= 32 ? 0 : w.n <= 64 ? 1 : w.n <= 96 ? 2 : w.n <= 128 ? 3 : w.n <= 192 ? 4 : w.n <= 256 ? 5 : w.n <= 384 ? 6 : w.n <= 512 ? 7 : 8;
+				return (w.nblk == 2 ? 0 : 16) + band;
+			};
+			std::stable_sort(items.begin(), items.end(), [&](const SlWork &a, const SlWork &b) {
+				int ka = key(a), kb = key(b);
+				if (ka != kb) return ka < kb;
+				return a.n > b.n;
+			});
+			std::vector<Bucket> buckets;
+			for (int i = 0; i < (int)items.size();) {
+				int j = i;
+				size_t smem = 0;
+				while (j < (int)items.size() && key(items[j]) == key(items[i])) {
+					int bb, kk;
+					size_t mm;
+					jacobi_layout(items[j].n, prec == 1, bb, kk, mm);
+					smem = std::max(smem, mm);
+					j++;
+				}
+				Bucket b;
+				b.first = i;
+				b.count = j - i;
+				b.smem = smem;
+				b.blocked = items[i].nblk != 2;
+				buckets.push_back(b);
+				i = j;
+			}
+			if (prec == 0) { ch.w32 = items; ch.b32 = buckets; }
+			else { ch.w64 = items; ch.b64 = buckets; }
+		}
+		P->chunks.push_back(std::move(ch));
+	}
+	// device copies of the work lists
+	for (auto &ch : P->chunks) {
+		size_t n32 = ch.w32.size(), n64 = ch.w64.size();
+		if (cudaMalloc(&ch.d_w32, n32 * sizeof(SlWork)) != cudaSuccess) return kHaErrorAlloc;
+		if (cudaMalloc(&ch.d_w64, n64 * sizeof(SlWork)) != cudaSuccess) return kHaErrorAlloc;
+		if (cudaMalloc(&ch.d_tofs, ch.tofs.size() * sizeof(int64_t)) != cudaSuccess) return kHaErrorAlloc;
+		HA_CUDA(cudaMemcpy(ch.d_w32, ch.w32.data(), n32 * sizeof(SlWork), cudaMemcpyHostToDevice));
+		HA_CUDA(cudaMemcpy(ch.d_w64, ch.w64.data(), n64 * sizeof(SlWork), cudaMemcpyHostToDevice));
+		HA_CUDA(cudaMemcpy(ch.d_tofs, ch.tofs.data(), ch.tofs.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
+	}
+	int64_t max8 = 1, maxT = 1, maxUV = 1;
+	int max_slots = 1;
+	for (auto &ch : P->chunks) {
+		max8 = std::max(max8, ch.scratch_elems8);
+		maxT = std::max(maxT, ch.t_elems);
+		maxUV = std::max(maxUV, ch.uv_elems);
+		max_slots = std::max(max_slots, ch.s1 - ch.s0);
+	}
+	int rc;
+	if ((rc = P->scrA.ensure((size_t)max8)) != kHaSuccess) return rc;
+	if ((rc = P->scrV.ensure((size_t)max8)) != kHaSuccess) return rc;
+	if ((rc = P->scrT.ensure((size_t)maxT)) != kHaSuccess) return rc;
+	if ((rc = P->uv.ensure((size_t)maxUV)) != kHaSuccess) return rc;
+	if ((rc = P->scale.ensure((size_t)max_slots)) != kHaSuccess) return rc;
+	if ((rc = P->stats.ensure((size_t)max_slots)) != kHaSuccess) return rc;
+	if ((rc = P->counters.ensure(4)) != kHaSuccess) return rc;
+	P->max_slots = max_slots;
+	return kHaSuccess;
+}
+
+__global__ void k_count_flags(const SlStats *__restrict__ st, int n, int32_t *__restrict__ counters) {
+	int q = blockIdx.x * blockDim.x + threadIdx.x;
+	if (q >= n) return;
+	int f = st[q].flags;
+	if (f & kFlagFP64) atomicAdd(&counters[0], 1);
+	if (f & kFlagUnconverged) atomicAdd(&counters[1], 1);
+}
+
+int set_smem_attrs() {
+	static bool done = false;
+	if (done) return kHaSuccess;
+	HA_CUDA(cudaFuncSetAttribute(k_jacobi<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax));
+	HA_CUDA(cudaFuncSetAttribute(k_jacobi<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax));
+	HA_CUDA(cudaFuncSetAttribute(k_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax));
+	HA_CUDA(cudaFuncSetAttribute(k_pattern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax));
+	done = true;
+	return kHaSuccess;
+}
+
+int build_pattern(HaB200Plan *P) {
+	const int nv = P->nv;
+	const size_t words = (size_t)nv / 32 + 2;
+	if (words * 4 > kSmemMax) {
+		fprintf(stderr, "ha_b200: nv = %d exceeds the pattern builder's limit\n", nv);
+		return kHaErrorArg;
+	}
+	int rc;
+	DevArr<int64_t> len;
+	if ((rc = len.ensure(nv)) != kHaSuccess) return rc;
+	if ((rc = P->patptr.ensure((size_t)nv + 1)) != kHaSuccess) { len.release(); return rc; }
+	{ HA_LAUNCH(kHaB200KPattern, 0); k_pattern<<<nv, kBlock, words * 4>>>(P->vlptr.p, P->vlent.p, P->off.p, P->idx.p, P->lo.p, P->hi.p, nv, 0,
+	                                     len.p, nullptr, nullptr); }
+	HA_CUDA(cudaGetLastError());
+	std::vector<int64_t> hl((size_t)nv);
+	HA_CUDA(cudaMemcpy(hl.data(), len.p, (size_t)nv * sizeof(int64_t), cudaMemcpyDeviceToHost));
+	P->h_patptr.assign((size_t)nv + 1, 0);
+	int max_row = 0;
+	for (int v = 0; v < nv; v++) {
+		P->h_patptr[v + 1] = P->h_patptr[v] + hl[v];
+		max_row = std::max<int>(max_row, (int)hl[v]);
+	}
+	P->nnz = P->h_patptr[nv];
+	P->max_row = max_row;
+	HA_CUDA(cudaMemcpy(P->patptr.p, P->h_patptr.data(), ((size_t)nv + 1) * sizeof(int64_t), cudaMemcpyHostToDevice));
+	if ((rc = P->patcol.ensure((size_t)P->nnz)) != kHaSuccess) { len.release(); return rc; }
+	{ HA_LAUNCH(kHaB200KPattern, 0); k_pattern<<<nv, kBlock, words * 4>>>(P->vlptr.p, P->vlent.p, P->off.p, P->idx.p, P->lo.p, P->hi.p, nv, 1,
+	                                     len.p, P->patptr.p, P->patcol.p); }
+	HA_CUDA(cudaGetLastError());
+	HA_CUDA(cudaDeviceSynchronize());
+	len.release();
+	return kHaSuccess;
+}
+
+int plan_create_impl(int32_t nt, int32_t nv, const int32_t *sl_indices, const int32_t *sl_offsets,
+                     const double *sl_dists, int32_t count, double radius, const double *weights,
+                     bool unweighted, HaB200Plan **out) {
+	*out = nullptr;
+	int rc = validate_searchlights(sl_indices, sl_offsets, count, nv);
+	if (rc != kHaSuccess) return rc;
+	if (nt <= 0) return kHaErrorArg;
+	if (sl_dists && !(radius > 0)) {
+		fprintf(stderr, "ha_b200: radius must be positive with distance weighting\n");
+		return kHaErrorArg;
+	}
+	if ((rc = set_smem_attrs()) != kHaSuccess) return rc;
+	HaB200Plan *P = new (std::nothrow) HaB200Plan();
+	if (!P) return kHaErrorAlloc;
+	P->nt = nt;
+	P->nv = nv;
+	P->count = count;
+	P->total = sl_offsets[count];
+	P->h_off.assign(sl_offsets, sl_offsets + count + 1);
+	P->h_idx.assign(sl_indices, sl_indices + P->total);
+	P->h_w.resize((size_t)P->total);
+	P->has_weights = !unweighted;
+	if (weights)
+		memcpy(P->h_w.data(), weights, (size_t)P->total * sizeof(double));
+	else if (!unweighted)
+		compute_weights(sl_indices, sl_offsets, sl_dists, count, radius, nv, P->h_w.data());
+	for (int s = 0; s < count; s++) P->max_n = std::max(P->max_n, sl_offsets[s + 1] - sl_offsets[s]);
+	// per-vertex membership lists, sorted by searchlight (counting sort over flat order)
+	std::vector<int64_t> vptr((size_t)nv + 1, 0);
+	for (int64_t k = 0; k < P->total; k++) vptr[(size_t)sl_indices[k] + 1]++;
+	for (int v = 0; v < nv; v++) vptr[v + 1] += vptr[v];
+	std::vector<int2> vent((size_t)P->total);
+	std::vector<int64_t> cur(vptr.begin(), vptr.end() - 1);
+	std::vector<int32_t> slo((size_t)count), shi((size_t)count);
+	for (int s = 0; s < count; s++) {
+		int lo = nv, hi = -1;
+		for (int32_t k = sl_offsets[s]; k < sl_offsets[s + 1]; k++) {
+			int v = sl_indices[k];
+			vent[(size_t)cur[v]++] = make_int2(s, k - sl_offsets[s]);
+			lo = std::min(lo, v);
+			hi = std::max(hi, v);
+		}
+		slo[s] = lo;
+		shi[s] = hi;
+	}
+	auto fail = [&](int code) {
+		ha_b200_plan_destroy(P);
+		return code;
+	};
+	if ((rc = P->idx.ensure((size_t)P->total)) != kHaSuccess) return fail(rc);
+	if ((rc = P->off.ensure((size_t)count + 1)) != kHaSuccess) return fail(rc);
+	if ((rc = P->lo.ensure((size_t)count)) != kHaSuccess) return fail(rc);
+	if ((rc = P->hi.ensure((size_t)count)) != kHaSuccess) return fail(rc);
+	if ((rc = P->w.ensure((size_t)P->total)) != kHaSuccess) return fail(rc);
+	if ((rc = P->vlptr.ensure((size_t)nv + 1)) != kHaSuccess) return fail(rc);
+	if ((rc = P->vlent.ensure((size_t)P->total)) != kHaSuccess) return fail(rc);
+	if (cudaMemcpy(P->idx.p, sl_indices, (size_t)P->total * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+	    cudaMemcpy(P->off.p, sl_offsets, ((size_t)count + 1) * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+	    cudaMemcpy(P->lo.p, slo.data(), (size_t)count * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+	    cudaMemcpy(P->hi.p, shi.data(), (size_t)count * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+	    cudaMemcpy(P->w.p, P->h_w.data(), (size_t)P->total * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+	    cudaMemcpy(P->vlptr.p, vptr.data(), ((size_t)nv + 1) * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+	    cudaMemcpy(P->vlent.p, vent.data(), (size_t)P->total * sizeof(int2), cudaMemcpyHostToDevice) != cudaSuccess) {
+		fprintf(stderr, "ha_b200: upload of the searchlight geometry failed: %s\n", cudaGetErrorString(cudaGetLastError()));
+		return fail(kHaErrorInternal);
+	}
+	if ((rc = build_pattern(P)) != kHaSuccess) return fail(rc);
+	*out = P;
+	return kHaSuccess;
+}
+
+// Enqueue one solve + reduction over all chunks.
+int run_procrustes(HaB200Plan *P, const double *d_X, const double *d_Y, bool refl, bool scal, int solver,
+                   int out_kind, double *d_vals, cudaStream_t st) {
+	const int nt = P->nt, nv = P->nv;
+	const int ntp = (nt + 31) & ~31;
+	const bool use32 = solver != kHaB200SolverFP64;
+	const int rowmajor = out_kind == kHaB200OutCSR ? 1 : 0;
+	int rc;
+	if (P->chunks.empty() && (rc = build_chunks(P)) != kHaSuccess) return rc;
+	if (use32) {
+		if ((rc = P->X32.ensure((size_t)nv * ntp)) != kHaSuccess) return rc;
+		if ((rc = P->Y32.ensure((size_t)nv * ntp)) != kHaSuccess) return rc;
+		int grid = 148 * 8;
+		{ HA_LAUNCH(kHaB200KConvert, st); k_to_f32_vertex_major<<<grid, kBlock, 0, st>>>(d_X, nt, nv, ntp, P->X32.p); }
+		{ HA_LAUNCH(kHaB200KConvert, st); k_to_f32_vertex_major<<<grid, kBlock, 0, st>>>(d_Y, nt, nv, ntp, P->Y32.p); }
+	}
+	if (scal) {
+		if ((rc = P->var.ensure((size_t)nv)) != kHaSuccess) return rc;
+		{ HA_LAUNCH(kHaB200KColVar, st); k_col_var_over_nt<<<(nv + 127) / 128, 128, 0, st>>>(d_X, nt, nv, P->var.p); }
+	}
+	HA_CUDA(cudaMemsetAsync(P->counters.p, 0, 4 * sizeof(int32_t), st));
+	float *T = P->scrT.p;
+	int smem_cap = std::min(P->max_row, 16384);
+	size_t red_smem = (size_t)smem_cap * 12;
+	for (size_t c = 0; c < P->chunks.size(); c++) {
+		Chunk &ch = P->chunks[c];
+		const int nsl = ch.s1 - ch.s0;
+		HA_CUDA(cudaMemsetAsync(P->stats.p, 0, (size_t)nsl * sizeof(SlStats), st));
+		JacobiParams jp;
+		jp.max_sweeps = 40;
+		jp.t_rowmajor = rowmajor;
+		jp.ill_ratio = (solver == kHaB200SolverMixed) ? 1e-4 : 0.0;
+		if (use32) {
+			float *A = reinterpret_cast<float *>(P->scrA.p);
+			float *V = reinterpret_cast<float *>(P->scrV.p);
+			jp.only_flagged = 0;
+			for (const Bucket &b : ch.b32) {
+				const SlWork *wk = ch.d_w32 + b.first;
+				{ HA_LAUNCH(kHaB200KXcov32, st); k_xcov<float, 32><<<b.count, kBlock, 0, st>>>(wk, P->idx.p, P->X32.p, P->Y32.p, ntp, nt, A, P->stats.p, 0); }
+				{ HA_LAUNCH(kHaB200KJacobi32, st); k_jacobi<float><<<b.count, kBlock, b.smem, st>>>(wk, A, V, T, P->stats.p, P->uv.p, jp); }
+				if (b.blocked) { HA_LAUNCH(kHaB200KFormT32, st); k_form_t_global<float><<<b.count, kBlock, 0, st>>>(wk, A, V, T, P->stats.p, rowmajor, 0); }
+			}
+		}
+		if (solver != kHaB200SolverFP32) {
+			double *A = P->scrA.p, *V = P->scrV.p;
+			const int only = (solver == kHaB200SolverMixed) ? 1 : 0;
+			jp.only_flagged = only;
+			for (const Bucket &b : ch.b64) {
+				const SlWork *wk = ch.d_w64 + b.first;
+				{ HA_LAUNCH(kHaB200KXcov64, st); k_xcov<double, 16><<<b.count, kBlock, 0, st>>>(wk, P->idx.p, d_X, d_Y, nt, nt, A, P->stats.p, only); }
+				{ HA_LAUNCH(kHaB200KJacobi64, st); k_jacobi<double><<<b.count, kBlock, b.smem, st>>>(wk, A, V, T, P->stats.p, P->uv.p, jp); }
+				if (b.blocked) { HA_LAUNCH(kHaB200KFormT64, st); k_form_t_global<double><<<b.count, kBlock, 0, st>>>(wk, A, V, T, P->stats.p, rowmajor, only); }
+			}
+		}
+		if (solver == kHaB200SolverMixed) {
+			{ HA_LAUNCH(kHaB200KRefine, st); k_ns_refine<<<nsl, kBlock, 0, st>>>(ch.d_w32, T, reinterpret_cast<float *>(P->scrV.p),
+			                                    reinterpret_cast<float *>(P->scrA.p), P->stats.p, rowmajor); }
+		}
+		if (!refl) { HA_LAUNCH(kHaB200KReflect, st); k_reflect_fix<<<nsl, kBlock, 0, st>>>(ch.d_w64, T, P->scrA.p, P->stats.p, P->uv.p, rowmajor); }
+		{ HA_LAUNCH(kHaB200KScale, st); k_scale<<<(nsl + 127) / 128, 128, 0, st>>>(ch.d_w64, nsl, P->idx.p, P->var.p, P->stats.p, nt, scal ? 1 : 0,
+		                                          P->scale.p); }
+		{ HA_LAUNCH(kHaB200KScale, st); k_count_flags<<<(nsl + 127) / 128, 128, 0, st>>>(P->stats.p, nsl, P->counters.p); }
+		{ HA_LAUNCH(kHaB200KReduce, st); k_reduce<<<nv, kBlock, red_smem, st>>>(P->vlptr.p, P->vlent.p, P->off.p, P->idx.p,
+		                                       P->has_weights ? P->w.p : nullptr, P->patptr.p, P->patcol.p, T,
+		                                       ch.d_tofs, P->scale.p, ch.s0, ch.s1, out_kind == kHaB200OutCSC ? 1 : 0,
+		                                       smem_cap, d_vals); }
+		HA_CUDA(cudaGetLastError());
+	}
+	P->last_chunk = (int)P->chunks.size() - 1;
+	P->last_rowmajor = rowmajor;
+	return kHaSuccess;
+}
+
+int host_threads() {
+	int t = g_threads > 0 ? g_threads : omp_get_max_threads();
+	return std::max(1, t);
+}
+
+// Cached plan for the host entry points (geometry + weights identify it).
+HaB200Plan *g_cached_plan = nullptr;
+uint64_t g_cached_key = 0;
+
+int get_plan(int32_t nt, int32_t nv, const int32_t *idx, const int32_t *off, const double *dists, int32_t count,
+             double radius, const double *weights, bool unweighted, HaB200Plan **out) {
+	if (!idx || !off || count <= 0) return kHaErrorArg;
+	if (off[count] < 0) return kHaErrorArg;
+	uint64_t h = 1469598103934665603ULL;
+	int32_t hdr[3] = {nt, nv, count};
+	h = fnv1a(hdr, sizeof(hdr), h);
+	h = fnv1a(&radius, sizeof(radius), h);
+	h = fnv1a(off, ((size_t)count + 1) * 4, h);
+	h = fnv1a(idx, (size_t)off[count] * 4, h);
+	int mode = dists ? 1 : weights ? 2 : unweighted ? 3 : 0;
+	h = fnv1a(&mode, sizeof(mode), h);
+	if (dists) h = fnv1a(dists, (size_t)off[count] * 8, h);
+	if (weights) h = fnv1a(weights, (size_t)off[count] * 8, h);
+	if (g_cached_plan && g_cached_key == h) {
+		*out = g_cached_plan;
+		return kHaSuccess;
+	}
+	if (g_cached_plan) {
+		ha_b200_plan_destroy(g_cached_plan);
+		g_cached_plan = nullptr;
+	}
+	int rc = plan_create_impl(nt, nv, idx, off, dists, count, radius, weights, unweighted, out);
+	if (rc != kHaSuccess) return rc;
+	g_cached_plan = *out;
+	g_cached_key = h;
+	return kHaSuccess;
+}
+
+// Upload X, Y (float64, host) as column-major device arrays.
+int upload_inputs(const double *X, const double *Y, int nt, int nv, bool col_major, const double **dX,
+                  const double **dY, cudaStream_t st) {
+	size_t n = (size_t)nt * nv;
+	int rc;
+	if ((rc = g_bufs.X64.ensure(n)) != kHaSuccess) return rc;
+	if ((rc = g_bufs.Y64.ensure(n)) != kHaSuccess) return rc;
+	if (col_major) {
+		HA_CUDA(cudaMemcpyAsync(g_bufs.X64.p, X, n * 8, cudaMemcpyHostToDevice, st));
+		HA_CUDA(cudaMemcpyAsync(g_bufs.Y64.p, Y, n * 8, cudaMemcpyHostToDevice, st));
+	} else {
+		if ((rc = g_bufs.Xtmp.ensure(n)) != kHaSuccess) return rc;
+		dim3 grid((nv + 31) / 32, (nt + 31) / 32), block(32, 8);
+		HA_CUDA(cudaMemcpyAsync(g_bufs.Xtmp.p, X, n * 8, cudaMemcpyHostToDevice, st));
+		{ HA_LAUNCH(kHaB200KConvert, st); k_transpose_f64<<<grid, block, 0, st>>>(g_bufs.Xtmp.p, nt, nv, g_bufs.X64.p); }
+		HA_CUDA(cudaMemcpyAsync(g_bufs.Xtmp.p, Y, n * 8, cudaMemcpyHostToDevice, st));
+		{ HA_LAUNCH(kHaB200KConvert, st); k_transpose_f64<<<grid, block, 0, st>>>(g_bufs.Xtmp.p, nt, nv, g_bufs.Y64.p); }
+		HA_CUDA(cudaGetLastError());
+	}
+	*dX = g_bufs.X64.p;
+	*dY = g_bufs.Y64.p;
+	return kHaSuccess;
+}
+
+int dense_impl(const double *X, const double *Y, int32_t nt, int32_t nv, const int32_t *idx, const int32_t *off,
+               const double *dists, int32_t count, double radius, double *T_out, bool refl, bool scal,
+               bool col_major) {
+	if (!X || !Y || !idx || !off || !T_out || nt <= 0 || nv <= 0 || count <= 0) return kHaErrorArg;
+	int rc = check_cuda_ready();
+	if (rc != kHaSuccess) return rc;
+	HaB200Plan *P = nullptr;
+	if ((rc = get_plan(nt, nv, idx, off, dists, count, radius, nullptr, false, &P)) != kHaSuccess) return rc;
+	cudaStream_t st = 0;
+	const double *dX, *dY;
+	if ((rc = upload_inputs(X, Y, nt, nv, col_major, &dX, &dY, st)) != kHaSuccess) return rc;
+	if ((rc = g_bufs.vals.ensure((size_t)P->nnz)) != kHaSuccess) return rc;
+	HA_CUDA(cudaMemsetAsync(g_bufs.vals.p, 0, (size_t)P->nnz * 8, st));
+	if ((rc = run_procrustes(P, dX, dY, refl, scal, kHaB200SolverMixed, kHaB200OutCSR, g_bufs.vals.p, st)) != kHaSuccess)
+		return rc;
+	g_bufs.h_vals.resize((size_t)P->nnz);
+	HA_CUDA(cudaMemcpyAsync(g_bufs.h_vals.data(), g_bufs.vals.p, (size_t)P->nnz * 8, cudaMemcpyDeviceToHost, st));
+	HA_CUDA(cudaStreamSynchronize(st));
+	if (P->h_patcol.empty()) {
+		P->h_patcol.resize((size_t)P->nnz);
+		HA_CUDA(cudaMemcpy(P->h_patcol.data(), P->patcol.p, (size_t)P->nnz * 4, cudaMemcpyDeviceToHost));
+	}
+	const int64_t *pp = P->h_patptr.data();
+	const int32_t *pc = P->h_patcol.data();
+	const double *vals = g_bufs.h_vals.data();
+#pragma omp parallel for schedule(dynamic, 64) num_threads(host_threads())
+	for (int r = 0; r < nv; r++) {
+		double *row = T_out + (size_t)r * nv;
+		for (int64_t k = pp[r]; k < pp[r + 1]; k++) row[pc[k]] += vals[k];
+	}
+	return kHaSuccess;
+}
+
+// Map the plan's (symmetric) pattern onto a caller CSC pattern: pos[k] = position in the caller's
+// arrays of the plan's entry k (column-ordered), or -1 if the caller lacks it (skipped, as
+// csrc/ha_sparse.c:137-139 does).
+int map_pattern(HaB200Plan *P, const int32_t *indptr, const int32_t *indices, int64_t nnz, std::vector<int64_t> &pos) {
+	if (P->h_patcol.empty()) {
+		P->h_patcol.resize((size_t)P->nnz);
+		HA_CUDA(cudaMemcpy(P->h_patcol.data(), P->patcol.p, (size_t)P->nnz * 4, cudaMemcpyDeviceToHost));
+	}
+	if (indptr[0] != 0 || indptr[P->nv] != nnz) return kHaErrorArg;
+	pos.assign((size_t)P->nnz, -1);
+	const int nv = P->nv;
+	for (int c = 0; c < nv; c++) {
+		int64_t a = P->h_patptr[c], ae = P->h_patptr[c + 1];
+		int64_t b = indptr[c], be = indptr[c + 1];
+		while (a < ae && b < be) {
+			int32_t ra = P->h_patcol[a], rb = indices[b];
+			if (ra == rb) { pos[a] = b; a++; b++; }
+			else if (ra < rb) a++;
+			else b++;
+		}
+	}
+	return kHaSuccess;
+}
+
+int csc_impl(const double *X, const double *Y, int32_t nt, int32_t nv, const int32_t *idx, const int32_t *off,
+             int32_t count, const double *weights, const int32_t *indptr, const int32_t *indices, int64_t nnz,
+             double *data, bool refl, bool scal, bool col_major, bool ridge, double alpha) {
+	if (!X || !Y || !idx || !off || !indptr || !indices || !data || nt <= 0 || nv <= 0 || count <= 0 || nnz < 0)
+		return kHaErrorArg;
+	int rc = check_cuda_ready();
+	if (rc != kHaSuccess) return rc;
+	HaB200Plan *P = nullptr;
+	if ((rc = get_plan(nt, nv, idx, off, nullptr, count, 0.0, weights, weights == nullptr, &P)) != kHaSuccess) return rc;
+	std::vector<int64_t> pos;
+	if ((rc = map_pattern(P, indptr, indices, nnz, pos)) != kHaSuccess) return rc;
+	cudaStream_t st = 0;
+	const double *dX, *dY;
+	if ((rc = upload_inputs(X, Y, nt, nv, col_major, &dX, &dY, st)) != kHaSuccess) return rc;
+	if ((rc = g_bufs.vals.ensure((size_t)P->nnz)) != kHaSuccess) return rc;
+	HA_CUDA(cudaMemsetAsync(g_bufs.vals.p, 0, (size_t)P->nnz * 8, st));
+	if (ridge)
+		rc = ha_b200_plan_ridge_device(P, dX, dY, alpha, kHaB200OutCSC, g_bufs.vals.p, st);
+	else
+		rc = run_procrustes(P, dX, dY, refl, scal, kHaB200SolverMixed, kHaB200OutCSC, g_bufs.vals.p, st);
+	if (rc != kHaSuccess) return rc;
+	g_bufs.h_vals.resize((size_t)P->nnz);
+	HA_CUDA(cudaMemcpyAsync(g_bufs.h_vals.data(), g_bufs.vals.p, (size_t)P->nnz * 8, cudaMemcpyDeviceToHost, st));
+	HA_CUDA(cudaStreamSynchronize(st));
+	const double *vals = g_bufs.h_vals.data();
+	const int64_t tot = P->nnz;
+#pragma omp parallel for schedule(static) num_threads(host_threads())
+	for (int64_t k = 0; k < tot; k++)
+		if (pos[k] >= 0) data[pos[k]] += vals[k];
+	return kHaSuccess;
+}
+
+}  // namespace
+
+// =============================================================================================
+// C ABI
+// =============================================================================================
+
+extern "C" {
+
+int ha_b200_init(void) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	if (g_inited) return kHaSuccess;
+	int ndev = 0;
+	cudaError_t e = cudaGetDeviceCount(&ndev);
+	if (e != cudaSuccess || ndev == 0) {
+		cudaGetLastError();
+		fprintf(stderr, "ha_b200: no CUDA device available (%s)\n", cudaGetErrorString(e));
+		return kHaErrorInternal;
+	}
+	int dev = 0;
+	cudaGetDevice(&dev);
+	cudaDeviceProp prop;
+	if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return kHaErrorInternal;
+	if (prop.major != 10) {
+		fprintf(stderr, "ha_b200: device %d is sm_%d%d; this library is built for sm_100a only\n", dev, prop.major,
+		        prop.minor);
+		return kHaErrorInternal;
+	}
+	if (cudaFree(0) != cudaSuccess) return kHaErrorInternal;
+	g_inited = true;
+	return kHaSuccess;
+}
+
+void ha_b200_cleanup(void) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	if (g_cached_plan) {
+		ha_b200_plan_destroy(g_cached_plan);
+		g_cached_plan = nullptr;
+	}
+	g_bufs.release();
+	g_inited = false;
+}
+
+bool ha_b200_available(void) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	return g_inited;
+}
+
+void ha_set_num_threads(int n) { g_threads = n; }
+int ha_get_num_threads(void) { return host_threads(); }
+
+int ha_searchlight_procrustes_b200(const double *X_data, const double *Y_data, int32_t nt, int32_t nv,
+                                   const int32_t *sl_indices, const int32_t *sl_offsets, const double *sl_dists,
+                                   int32_t count, double radius, double *T_out, bool isReflection, bool isScaling,
+                                   bool col_major) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	return dense_impl(X_data, Y_data, nt, nv, sl_indices, sl_offsets, sl_dists, count, radius, T_out, isReflection,
+	                  isScaling, col_major);
+}
+
+int ha_searchlight_procrustes_dense(const double *X_data, const double *Y_data, int32_t nt, int32_t nv,
+                                    const int32_t *sl_indices, const int32_t *sl_offsets, const double *sl_dists,
+                                    int32_t count, double radius, double *T_out, bool isReflection, bool isScaling,
+                                    THaBackend backend, bool col_major) {
+	if ((int)backend != 4) {
+		fprintf(stderr, "ha_searchlight_procrustes_dense: this library implements only backend 4 (B200); got %d\n",
+		        (int)backend);
+		return kHaErrorArg;
+	}
+	return ha_searchlight_procrustes_b200(X_data, Y_data, nt, nv, sl_indices, sl_offsets, sl_dists, count, radius,
+	                                      T_out, isReflection, isScaling, col_major);
+}
+
+int ha_sparse_pattern_b200(const int32_t *sl_indices, const int32_t *sl_offsets, int32_t count, int32_t nv,
+                           int32_t *indptr, int32_t *indices, int64_t capacity, int64_t *nnz) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	if (!indptr || !nnz) return kHaErrorArg;
+	int rc = check_cuda_ready();
+	if (rc != kHaSuccess) return rc;
+	HaB200Plan *P = nullptr;
+	if ((rc = get_plan(1, nv, sl_indices, sl_offsets, nullptr, count, 0.0, nullptr, true, &P)) != kHaSuccess) return rc;
+	*nnz = P->nnz;
+	if (P->nnz > INT32_MAX) {
+		fprintf(stderr, "ha_sparse_pattern_b200: nnz %lld does not fit int32 indptr\n", (long long)P->nnz);
+		return kHaErrorArg;
+	}
+	for (int v = 0; v <= nv; v++) indptr[v] = (int32_t)P->h_patptr[v];
+	if (indices) {
+		if (capacity < P->nnz) return kHaErrorArg;
+		HA_CUDA(cudaMemcpy(indices, P->patcol.p, (size_t)P->nnz * 4, cudaMemcpyDeviceToHost));
+	}
+	return kHaSuccess;
+}
+
+int ha_searchlight_weights_b200(const int32_t *sl_indices, const int32_t *sl_offsets, const double *sl_dists,
+                                int32_t count, double radius, int32_t nv, double *weights_out) {
+	if (!weights_out) return kHaErrorArg;
+	int rc = validate_searchlights(sl_indices, sl_offsets, count, nv);
+	if (rc != kHaSuccess) return rc;
+	compute_weights(sl_indices, sl_offsets, sl_dists, count, radius, nv, weights_out);
+	return kHaSuccess;
+}
+
+int ha_searchlight_procrustes_csc_b200(const double *X_data, const double *Y_data, int32_t nt, int32_t nv,
+                                       const int32_t *sl_indices, const int32_t *sl_offsets, int32_t count,
+                                       const double *weights, const int32_t *indptr, const int32_t *indices,
+                                       int64_t nnz, double *data, bool isReflection, bool isScaling,
+                                       bool col_major) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	return csc_impl(X_data, Y_data, nt, nv, sl_indices, sl_offsets, count, weights, indptr, indices, nnz, data,
+	                isReflection, isScaling, col_major, false, 0.0);
+}
+
+int ha_searchlight_ridge_csc_b200(const double *X_data, const double *Y_data, int32_t nt, int32_t nv,
+                                  const int32_t *sl_indices, const int32_t *sl_offsets, int32_t count,
+                                  const double *weights, const int32_t *indptr, const int32_t *indices, int64_t nnz,
+                                  double *data, double alpha, bool col_major) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	return csc_impl(X_data, Y_data, nt, nv, sl_indices, sl_offsets, count, weights, indptr, indices, nnz, data,
+	                true, false, col_major, true, alpha);
+}
+
+int ha_b200_plan_create(int32_t nt, int32_t nv, const int32_t *sl_indices, const int32_t *sl_offsets,
+                        const double *sl_dists, int32_t count, double radius, const double *weights,
+                        HaB200Plan **plan_out) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	if (!plan_out) return kHaErrorArg;
+	int rc = check_cuda_ready();
+	if (rc != kHaSuccess) return rc;
+	return plan_create_impl(nt, nv, sl_indices, sl_offsets, sl_dists, count, radius, weights, false, plan_out);
+}
+
+void ha_b200_plan_destroy(HaB200Plan *P) {
+	if (!P) return;
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	if (P == g_cached_plan) g_cached_plan = nullptr;
+	for (auto &ch : P->chunks) {
+		if (ch.d_w32) cudaFree(ch.d_w32);
+		if (ch.d_w64) cudaFree(ch.d_w64);
+		if (ch.d_tofs) cudaFree(ch.d_tofs);
+	}
+	P->idx.release(); P->off.release(); P->lo.release(); P->hi.release(); P->w.release();
+	P->vlptr.release(); P->vlent.release(); P->patptr.release(); P->patcol.release();
+	P->scrA.release(); P->scrV.release(); P->scrT.release(); P->uv.release(); P->scale.release();
+	P->stats.release(); P->X32.release(); P->Y32.release(); P->var.release(); P->counters.release();
+	delete P;
+}
+
+int64_t ha_b200_plan_nnz(const HaB200Plan *P) { return P ? P->nnz : -1; }
+
+int ha_b200_plan_pattern(const HaB200Plan *P, int64_t *indptr, int32_t *indices) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	if (!P || !indptr) return kHaErrorArg;
+	memcpy(indptr, P->h_patptr.data(), ((size_t)P->nv + 1) * 8);
+	if (indices) HA_CUDA(cudaMemcpy(indices, P->patcol.p, (size_t)P->nnz * 4, cudaMemcpyDeviceToHost));
+	return kHaSuccess;
+}
+
+int ha_b200_plan_device_pattern(const HaB200Plan *P, const int64_t **d_indptr, const int32_t **d_indices) {
+	if (!P || !d_indptr || !d_indices) return kHaErrorArg;
+	*d_indptr = P->patptr.p;
+	*d_indices = P->patcol.p;
+	return kHaSuccess;
+}
+
+int ha_b200_plan_stats(const HaB200Plan *P, int32_t *n_fp64, int32_t *n_unconverged) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	if (!P) return kHaErrorArg;
+	int32_t h[4] = {0, 0, 0, 0};
+	HA_CUDA(cudaMemcpy(h, P->counters.p, sizeof(h), cudaMemcpyDeviceToHost));
+	if (n_fp64) *n_fp64 = h[0];
+	if (n_unconverged) *n_unconverged = h[1];
+	return kHaSuccess;
+}
+
+int ha_b200_plan_procrustes_device(HaB200Plan *P, const double *d_X, const double *d_Y, bool isReflection,
+                                   bool isScaling, int solver, int out_kind, double *d_values, void *stream) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	if (!P || !d_X || !d_Y || !d_values) return kHaErrorArg;
+	if (solver < 0 || solver > 2 || out_kind < 0 || out_kind > 1) return kHaErrorArg;
+	return run_procrustes(P, d_X, d_Y, isReflection, isScaling, solver, out_kind, d_values, (cudaStream_t)stream);
+}
+
+int ha_b200_plan_ridge_device(HaB200Plan *P, const double *d_X, const double *d_Y, double alpha, int out_kind,
+                              double *d_values, void *stream) {
+	(void)P; (void)d_X; (void)d_Y; (void)alpha; (void)out_kind; (void)d_values; (void)stream;
+	fprintf(stderr, "ha_b200: ridge is not available in this build\n");
+	return kHaErrorInternal;
+}
+
+void ha_b200_set_kernel_timing(bool on) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	g_timing = on;
+}
+
+int ha_b200_kernel_times(double *ms, int64_t *launches) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	for (auto &t : g_timed) {
+		float e = 0.0f;
+		if (cudaEventSynchronize(t.b) == cudaSuccess && cudaEventElapsedTime(&e, t.a, t.b) == cudaSuccess)
+			g_kernel_ms[t.kind] += e;
+		cudaEventDestroy(t.a);
+		cudaEventDestroy(t.b);
+	}
+	g_timed.clear();
+	for (int k = 0; k < kHaB200NumKernelKinds; k++) {
+		if (ms) ms[k] = g_kernel_ms[k];
+		if (launches) launches[k] = g_kernel_n[k];
+		g_kernel_ms[k] = 0.0;
+		g_kernel_n[k] = 0;
+	}
+	cudaGetLastError();
+	return kHaSuccess;
+}
+
+int64_t ha_b200_launch_count(void) { return g_launches; }
+
+int ha_b200_plan_local_transforms(const HaB200Plan *P, int32_t first, int32_t n, float *out) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	if (!P || !out || P->last_chunk < 0) return kHaErrorArg;
+	const Chunk &ch = P->chunks[(size_t)P->last_chunk];
+	if (first < ch.s0 || first + n > ch.s1 || n <= 0) return kHaErrorArg;
+	int64_t a = ch.tofs[(size_t)(first - ch.s0)];
+	int64_t e = (first + n < ch.s1) ? ch.tofs[(size_t)(first + n - ch.s0)] : ch.t_elems;
+	HA_CUDA(cudaDeviceSynchronize());
+	HA_CUDA(cudaMemcpy(out, P->scrT.p + a, (size_t)(e - a) * 4, cudaMemcpyDeviceToHost));
+	return kHaSuccess;
+}
+
+}  // extern "C"

@@ -1,0 +1,920 @@
+// ha_b200_kernels.cuh -- sm_100a kernels of the searchlight alignment path.
+//
+// Data layout in HBM (one call, one hemisphere):
+//   X32, Y32   float  [nv][ntp]   vertex-major time series, ntp = nt rounded up to 32, zero padded
+//   X64, Y64   double [nv][nt]    the caller's column-major float64 input (vertex-major already)
+//   A scratch  Real   per searchlight: n rows x ncol columns, column-major (column c contiguous),
+//              ncol = nblk * bsz >= n (padding columns are zero)
+//   V scratch  Real   same shape as A (right singular vectors, accumulated rotations)
+//   T scratch  float  per searchlight: n x n local transform, row-major (CSR output) or
+//              column-major (CSC output), so the row the reduction needs is contiguous
+//   values     double the symmetric CSC/CSR pattern's entries, accumulated in place
+//
+// Reference anchors: local Procrustes csrc/ha_procrustes.c:17-127 and its
+// column-major workspace twin csrc/ha_searchlight.c:578-659; scatter-add
+// csrc/ha_searchlight.c:1073-1085 (dense) and csrc/ha_sparse.c:128-142 (CSC);
+// pattern csrc/ha_sparse.c:31-112.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace hab200 {
+
+// ---------------------------------------------------------------------------------------------
+// small helpers
+// ---------------------------------------------------------------------------------------------
+
+template <typename Real> struct Eps;
+template <> struct Eps<float> { static __device__ __forceinline__ float v() { return 1.1920928955078125e-7f; } };
+template <> struct Eps<double> { static __device__ __forceinline__ double v() { return 2.220446049250313e-16; } };
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+	return v;
+}
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+	return v;
+}
+
+__device__ __forceinline__ float real_sqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ double real_sqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float real_abs(float x) { return fabsf(x); }
+__device__ __forceinline__ double real_abs(double x) { return fabs(x); }
+
+// Per-searchlight work item of a size bucket.
+struct SlWork {
+	int32_t s;        // searchlight index
+	int32_t n;        // size
+	int32_t bsz;      // columns per Jacobi block
+	int32_t nblk;     // number of column blocks (even, >= 2); 2 means the matrix stays in shared memory
+	int64_t aofs;     // element offset of A / V in the scratch (n * nblk * bsz elements each)
+	int64_t tofs;     // element offset of T in the T scratch (n * n)
+	int32_t sofs;     // flat offset of the searchlight in sl_indices
+	int32_t slot;     // index within the current chunk (stats, uv)
+	int64_t uvofs;    // element offset (double) of the saved u_min / v_min vectors (2 n)
+};
+
+// Per-searchlight results of the solve.
+struct SlStats {
+	double s_sum;     // sum of singular values (sign-flipped smallest one when reflection was removed)
+	double s_min;     // smallest singular value
+	double s_max;     // largest singular value
+	int32_t k_min;    // column of the smallest singular value
+	int32_t flags;    // bit 0: unconverged, bit 1: ill-conditioned (re-solved in FP64), bit 2: reflected
+};
+
+enum : int32_t { kFlagUnconverged = 1, kFlagIllCond = 2, kFlagReflected = 4, kFlagFP64 = 8 };
+
+// ---------------------------------------------------------------------------------------------
+// layout conversion
+// ---------------------------------------------------------------------------------------------
+
+// col-major float64 (vertex v at X[v*nt]) -> vertex-major float32 [nv][ntp], zero padded.
+__global__ void k_to_f32_vertex_major(const double *__restrict__ X, int nt, int nv, int ntp,
+                                      float *__restrict__ out) {
+	int64_t total = (int64_t)nv * ntp;
+	for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+	     e += (int64_t)gridDim.x * blockDim.x) {
+		int64_t v = e / ntp;
+		int t = (int)(e - v * ntp);
+		out[e] = (t < nt) ? (float)X[v * nt + t] : 0.0f;
+	}
+}
+
+// row-major float64 (X[t*nv + v]) -> column-major float64 (X[v*nt + t]); 32x32 tiles.
+__global__ void k_transpose_f64(const double *__restrict__ in, int nt, int nv, double *__restrict__ out) {
+	__shared__ double tile[32][33];
+	int v0 = blockIdx.x * 32, t0 = blockIdx.y * 32;
+	for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+		int t = t0 + r, v = v0 + threadIdx.x;
+		tile[r][threadIdx.x] = (t < nt && v < nv) ? in[(int64_t)t * nv + v] : 0.0;
+	}
+	__syncthreads();
+	for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+		int v = v0 + r, t = t0 + threadIdx.x;
+		if (v < nv && t < nt) out[(int64_t)v * nt + t] = tile[threadIdx.x][r];
+	}
+}
+
+// Population variance / nt of every vertex column, the two-pass loop of
+// csrc/ha_searchlight.c:640-652 (mean, then sum of squared deviations), with
+// rounded operations so the float64 result does not depend on FMA contraction.
+__global__ void k_col_var_over_nt(const double *__restrict__ X, int nt, int nv, double *__restrict__ out) {
+	int v = blockIdx.x * blockDim.x + threadIdx.x;
+	if (v >= nv) return;
+	const double *x = X + (int64_t)v * nt;
+	double mean = 0.0;
+	for (int i = 0; i < nt; i++) mean = __dadd_rn(mean, x[i]);
+	mean = mean / nt;
+	double var = 0.0;
+	for (int i = 0; i < nt; i++) {
+		double d = __dsub_rn(x[i], mean);
+		var = __dadd_rn(var, __dmul_rn(d, d));
+	}
+	out[v] = var / nt;
+}
+
+// ---------------------------------------------------------------------------------------------
+// cross-covariance  A_s = X[:, sl]^T Y[:, sl]   (csrc/ha_searchlight.c:581-582)
+// ---------------------------------------------------------------------------------------------
+// One CTA per searchlight, 64x64 output tiles, 16x16 threads with 4x4 register tiles,
+// K (time) staged through shared memory in chunks of KT.  Output column-major with
+// ncol = nblk*bsz columns; padding columns are written as zeros.
+
+template <typename Real, int KT>
+__global__ void __launch_bounds__(256) k_xcov(const SlWork *__restrict__ work, const int32_t *__restrict__ sl_idx,
+                                              const Real *__restrict__ Xv, const Real *__restrict__ Yv, int ld,
+                                              int nt, Real *__restrict__ Ascr,
+                                              const SlStats *__restrict__ stats, int only_flagged) {
+	const SlWork w = work[blockIdx.x];
+	if (only_flagged && !(stats[w.slot].flags & kFlagIllCond)) return;
+	const int n = w.n;
+	const int ncol = w.nblk * w.bsz;
+	const int32_t *sl = sl_idx + w.sofs;
+	Real *A = Ascr + w.aofs;
+
+	__shared__ Real xs[KT][64 + 1];
+	__shared__ Real ys[KT][64 + 1];
+	__shared__ int32_t vi[64], vj[64];
+
+	const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+	for (int i0 = 0; i0 < n; i0 += 64) {
+		for (int j0 = 0; j0 < n; j0 += 64) {
+			__syncthreads();
+			if (threadIdx.x < 64) {
+				int i = i0 + threadIdx.x;
+				vi[threadIdx.x] = (i < n) ? sl[i] : -1;
+			} else if (threadIdx.x < 128) {
+				int j = j0 + threadIdx.x - 64;
+				vj[threadIdx.x - 64] = (j < n) ? sl[j] : -1;
+			}
+			Real acc[4][4];
+#pragma unroll
+			for (int a = 0; a < 4; a++)
+#pragma unroll
+				for (int b = 0; b < 4; b++) acc[a][b] = 0;
+			for (int t0 = 0; t0 < nt; t0 += KT) {
+				__syncthreads();
+				// load: 64 vertices x KT samples for X and for Y
+				for (int e = threadIdx.x; e < 64 * KT; e += 256) {
+					int r = e / KT, t = e - r * KT;
+					int tt = t0 + t;
+					int v = vi[r], u = vj[r];
+					xs[t][r] = (v >= 0 && tt < nt) ? Xv[(int64_t)v * ld + tt] : Real(0);
+					ys[t][r] = (u >= 0 && tt < nt) ? Yv[(int64_t)u * ld + tt] : Real(0);
+				}
+				__syncthreads();
+#pragma unroll 4
+				for (int t = 0; t < KT; t++) {
+					Real a[4], b[4];
+#pragma unroll
+					for (int q = 0; q < 4; q++) {
+						a[q] = xs[t][ty + 16 * q];
+						b[q] = ys[t][tx + 16 * q];
+					}
+#pragma unroll
+					for (int p = 0; p < 4; p++)
+#pragma unroll
+						for (int q = 0; q < 4; q++) acc[p][q] += a[p] * b[q];
+				}
+			}
+#pragma unroll
+			for (int p = 0; p < 4; p++) {
+				int i = i0 + ty + 16 * p;
+				if (i >= n) continue;
+#pragma unroll
+				for (int q = 0; q < 4; q++) {
+					int j = j0 + tx + 16 * q;
+					if (j < n) A[(int64_t)j * n + i] = acc[p][q];
+				}
+			}
+		}
+	}
+	// zero padding columns
+	for (int64_t e = (int64_t)n * n + threadIdx.x; e < (int64_t)n * ncol; e += 256) A[e] = 0;
+}
+
+// ---------------------------------------------------------------------------------------------
+// one-sided Jacobi (Hestenes) on the columns of A, accumulating V
+// ---------------------------------------------------------------------------------------------
+// A V = B with orthogonal columns; sigma_c = ||B[:, c]||, U = B diag(1/sigma), T = U V^T
+// (the polar factor of A, csrc/ha_searchlight.c:593-609).  Parallel ordering: the
+// circle-method round robin over m columns (m - 1 rounds of m/2 disjoint pairs);
+// warps take pairs in turn, lanes stride over rows.
+//
+// Resident mode (nblk == 2): A and V live in shared memory for every sweep.
+// Blocked mode (nblk > 2): A and V stay in the global scratch (L2 resident); a sweep runs
+// the round robin over column blocks, staging two blocks (A and V columns) in shared
+// memory per block pair.  In the first block round every block pair runs a full round robin
+// over its 2*bsz columns (covering the pairs inside each block once), in later block rounds
+// only the cross pairs, so one sweep visits every column pair exactly once.
+
+// circle method: pair k of round r among m players (m even)
+__device__ __forceinline__ void rr_pair(int m, int r, int k, int &p, int &q) {
+	if (k == 0) {
+		p = m - 1;
+		q = r;
+	} else {
+		int mm = m - 1;
+		p = (r + k) % mm;
+		q = (r - k + mm) % mm;
+	}
+}
+
+// Rotate the pair (p, q) of columns of length n stored at B + c*ldb (and V + c*ldv).
+// Returns true (on every lane) if a rotation was applied.
+template <typename Real>
+__device__ __forceinline__ bool jacobi_pair(Real *B, Real *V, int ldb, int n, int p, int q, Real tol, int lane) {
+	Real *bp = B + (int64_t)p * ldb, *bq = B + (int64_t)q * ldb;
+	Real al = 0, be = 0, ga = 0;
+	for (int i = lane; i < n; i += 32) {
+		Real x = bp[i], y = bq[i];
+		al += x * x;
+		be += y * y;
+		ga += x * y;
+	}
+	al = warp_sum(al);
+	be = warp_sum(be);
+	ga = warp_sum(ga);
+	if (!(al > 0 && be > 0)) return false;
+	if (!(real_abs(ga) > tol * real_sqrt(al) * real_sqrt(be))) return false;
+	Real zeta = (be - al) / (2 * ga);
+	Real t = ((zeta >= 0) ? Real(1) : Real(-1)) / (real_abs(zeta) + real_sqrt(Real(1) + zeta * zeta));
+	Real c = Real(1) / real_sqrt(Real(1) + t * t);
+	Real s = c * t;
+	for (int i = lane; i < n; i += 32) {
+		Real x = bp[i], y = bq[i];
+		bp[i] = c * x - s * y;
+		bq[i] = s * x + c * y;
+	}
+	Real *vp = V + (int64_t)p * ldb, *vq = V + (int64_t)q * ldb;
+	for (int i = lane; i < n; i += 32) {
+		Real x = vp[i], y = vq[i];
+		vp[i] = c * x - s * y;
+		vq[i] = s * x + c * y;
+	}
+	return true;
+}
+
+// Full round robin (m - 1 rounds) over m columns in B/V (shared or global).
+template <typename Real>
+__device__ bool jacobi_full_rr(Real *B, Real *V, int ld, int n, int m, Real tol) {
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+	bool rotated = false;
+	for (int r = 0; r < m - 1; r++) {
+		for (int k = warp; k < m / 2; k += nwarp) {
+			int p, q;
+			rr_pair(m, r, k, p, q);
+			rotated |= jacobi_pair(B, V, ld, n, p, q, tol, lane);
+		}
+		__syncthreads();
+	}
+	return rotated;
+}
+
+// Cross pairs only between column halves [0, h) and [h, 2h): h rounds of h pairs.
+template <typename Real>
+__device__ bool jacobi_cross(Real *B, Real *V, int ld, int n, int h, Real tol) {
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+	bool rotated = false;
+	for (int r = 0; r < h; r++) {
+		for (int k = warp; k < h; k += nwarp) {
+			int p = k, q = h + (k + r) % h;
+			rotated |= jacobi_pair(B, V, ld, n, p, q, tol, lane);
+		}
+		__syncthreads();
+	}
+	return rotated;
+}
+
+// ---------------------------------------------------------------------------------------------
+// generic small GEMM:  C(i, j) = alpha * sum_k P(k, i) d(k) Q(k, j) + beta * E(i, j)
+// ---------------------------------------------------------------------------------------------
+// Operands are addressed through strides, P(k, i) = P[k*pk + i*pi] etc., so the same routine
+// serves every layout used here; tiles of 64x64 outputs per pass, K staged in chunks of 16.
+template <typename Real, typename OutT = Real>
+struct GemmArgs {
+	int M, N, K;
+	const Real *P;
+	int64_t pk, pi;
+	const Real *Q;
+	int64_t qk, qj;
+	const Real *d;  // optional K scales (nullptr = 1)
+	Real alpha;
+	const Real *E;  // optional addend (nullptr = none)
+	int64_t ei, ej;
+	Real beta;
+	OutT *C;
+	int64_t ci, cj;
+};
+
+template <typename Real, typename OutT>
+__device__ void block_gemm(const GemmArgs<Real, OutT> &g, Real (*ps)[65], Real (*qs)[65]) {
+	constexpr int KC = 16;
+	const int tx = threadIdx.x & 15, ty = (threadIdx.x >> 4) & 15;
+	const int nthr = blockDim.x;  // 256 assumed for the compute mapping
+	for (int i0 = 0; i0 < g.M; i0 += 64) {
+		for (int j0 = 0; j0 < g.N; j0 += 64) {
+			Real acc[4][4];
+#pragma unroll
+			for (int a = 0; a < 4; a++)
+#pragma unroll
+				for (int b = 0; b < 4; b++) acc[a][b] = 0;
+			for (int k0 = 0; k0 < g.K; k0 += KC) {
+				__syncthreads();
+				for (int e = threadIdx.x; e < KC * 64; e += nthr) {
+					int kk = e >> 6, ii = e & 63;
+					int k = k0 + kk;
+					int i = i0 + ii, j = j0 + ii;
+					Real dk = (k < g.K && g.d) ? g.d[k] : Real(1);
+					ps[kk][ii] = (k < g.K && i < g.M) ? g.P[k * g.pk + i * g.pi] * dk : Real(0);
+					qs[kk][ii] = (k < g.K && j < g.N) ? g.Q[k * g.qk + j * g.qj] : Real(0);
+				}
+				__syncthreads();
+				if (threadIdx.x < 256) {
+#pragma unroll
+					for (int kk = 0; kk < KC; kk++) {
+						Real a[4], b[4];
+#pragma unroll
+						for (int q = 0; q < 4; q++) {
+							a[q] = ps[kk][ty + 16 * q];
+							b[q] = qs[kk][tx + 16 * q];
+						}
+#pragma unroll
+						for (int p = 0; p < 4; p++)
+#pragma unroll
+							for (int q = 0; q < 4; q++) acc[p][q] += a[p] * b[q];
+					}
+				}
+			}
+			if (threadIdx.x < 256) {
+#pragma unroll
+				for (int p = 0; p < 4; p++) {
+					int i = i0 + ty + 16 * p;
+					if (i >= g.M) continue;
+#pragma unroll
+					for (int q = 0; q < 4; q++) {
+						int j = j0 + tx + 16 * q;
+						if (j >= g.N) continue;
+						Real v = g.alpha * acc[p][q];
+						if (g.E) v += g.beta * g.E[i * g.ei + j * g.ej];
+						g.C[i * g.ci + j * g.cj] = (OutT)v;
+					}
+				}
+			}
+		}
+	}
+	__syncthreads();
+}
+
+// ---------------------------------------------------------------------------------------------
+// Jacobi polar kernel
+// ---------------------------------------------------------------------------------------------
+// Per searchlight: run sweeps until a sweep applies no rotation (or max_sweeps), take
+// sigma_c = ||B[:, c]||, form T = B diag(1/sigma) V^T into the T scratch (row-major when
+// t_rowmajor, else column-major), and record the singular-value statistics and the
+// singular pair of the smallest singular value (for the reflection fix).
+// Columns whose norm is exactly zero get an orthonormal completion so T stays orthogonal.
+
+struct JacobiParams {
+	int max_sweeps;
+	int t_rowmajor;
+	double ill_ratio;  // sigma_min / sigma_max below this -> kFlagIllCond
+	int only_flagged;  // process only searchlights whose stats carry kFlagIllCond (FP64 re-solve)
+};
+
+template <typename Real>
+__global__ void __launch_bounds__(256) k_jacobi(const SlWork *__restrict__ work, Real *__restrict__ Ascr,
+                                                Real *__restrict__ Vscr, float *__restrict__ Tscr,
+                                                SlStats *__restrict__ stats, double *__restrict__ uvbuf,
+                                                JacobiParams prm) {
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	Real *sm = reinterpret_cast<Real *>(smem_raw);
+	const SlWork w = work[blockIdx.x];
+	if (prm.only_flagged && !(stats[w.slot].flags & kFlagIllCond)) return;
+	const int n = w.n, bsz = w.bsz, nblk = w.nblk;
+	const int ncol = nblk * bsz;
+	Real *Ag = Ascr + w.aofs;
+	Real *Vg = Vscr + w.aofs;
+	const Real tol = Eps<Real>::v() * real_sqrt(Real(n));
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+
+	// shared: Bs[2*bsz][n], Vs[2*bsz][n], then small vectors
+	Real *Bs = sm;
+	Real *Vs = sm + (int64_t)2 * bsz * n;
+	Real *sig = Vs + (int64_t)2 * bsz * n;  // ncol entries (resident: 2*bsz)
+
+	bool resident = (nblk == 2);
+	bool converged = false;
+	int sweep = 0;
+	if (resident) {
+		for (int64_t e = threadIdx.x; e < (int64_t)2 * bsz * n; e += blockDim.x) {
+			int c = (int)(e / n), i = (int)(e - (int64_t)c * n);
+			Bs[e] = Ag[e];
+			Vs[e] = (c == i) ? Real(1) : Real(0);
+		}
+		__syncthreads();
+		for (sweep = 0; sweep < prm.max_sweeps; sweep++) {
+			bool rot = jacobi_full_rr(Bs, Vs, n, n, 2 * bsz, tol);
+			if (!__syncthreads_or(rot)) {
+				converged = true;
+				break;
+			}
+		}
+	} else {
+		for (int64_t e = threadIdx.x; e < (int64_t)ncol * n; e += blockDim.x) {
+			int c = (int)(e / n), i = (int)(e - (int64_t)c * n);
+			Vg[e] = (c == i) ? Real(1) : Real(0);
+		}
+		__syncthreads();
+		for (sweep = 0; sweep < prm.max_sweeps; sweep++) {
+			bool rot = false;
+			for (int br = 0; br < nblk - 1; br++) {
+				for (int k = 0; k < nblk / 2; k++) {
+					int I, J;
+					rr_pair(nblk, br, k, I, J);
+					// stage blocks I and J
+					for (int64_t e = threadIdx.x; e < (int64_t)bsz * n; e += blockDim.x) {
+						Bs[e] = Ag[(int64_t)I * bsz * n + e];
+						Bs[(int64_t)bsz * n + e] = Ag[(int64_t)J * bsz * n + e];
+						Vs[e] = Vg[(int64_t)I * bsz * n + e];
+						Vs[(int64_t)bsz * n + e] = Vg[(int64_t)J * bsz * n + e];
+					}
+					__syncthreads();
+					if (br == 0)
+						rot |= jacobi_full_rr(Bs, Vs, n, n, 2 * bsz, tol);
+					else
+						rot |= jacobi_cross(Bs, Vs, n, n, bsz, tol);
+					for (int64_t e = threadIdx.x; e < (int64_t)bsz * n; e += blockDim.x) {
+						Ag[(int64_t)I * bsz * n + e] = Bs[e];
+						Ag[(int64_t)J * bsz * n + e] = Bs[(int64_t)bsz * n + e];
+						Vg[(int64_t)I * bsz * n + e] = Vs[e];
+						Vg[(int64_t)J * bsz * n + e] = Vs[(int64_t)bsz * n + e];
+					}
+					__syncthreads();
+				}
+			}
+			if (!__syncthreads_or(rot)) {
+				converged = true;
+				break;
+			}
+		}
+	}
+
+	Real *B = resident ? Bs : Ag;
+	Real *V = resident ? Vs : Vg;
+	// column norms (sigma) -> shared sig[] (resident) or reuse Bs as a staging area (blocked)
+	Real *sg = resident ? sig : Bs;
+	for (int c = warp; c < ncol; c += nwarp) {
+		const Real *bc = B + (int64_t)c * n;
+		Real ss = 0;
+		for (int i = lane; i < n; i += 32) ss += bc[i] * bc[i];
+		ss = warp_sum(ss);
+		if (lane == 0) sg[c] = (c < n) ? real_sqrt(ss) : Real(0);
+	}
+	__syncthreads();
+	// statistics over the n real columns
+	__shared__ double red_sum[32], red_max[32], red_min[32];
+	__shared__ int red_kmin[32];
+	{
+		double ssum = 0, smax = 0, smin = 1e308;
+		int kmin = 0;
+		for (int c = threadIdx.x; c < n; c += blockDim.x) {
+			double v = (double)sg[c];
+			ssum += v;
+			smax = fmax(smax, v);
+			if (v < smin) { smin = v; kmin = c; }
+		}
+		ssum = warp_sum(ssum);
+		for (int o = 16; o > 0; o >>= 1) {
+			smax = fmax(smax, __shfl_xor_sync(0xffffffffu, smax, o));
+			double om = __shfl_xor_sync(0xffffffffu, smin, o);
+			int ok = __shfl_xor_sync(0xffffffffu, kmin, o);
+			if (om < smin || (om == smin && ok < kmin)) { smin = om; kmin = ok; }
+		}
+		if (lane == 0) { red_sum[warp] = ssum; red_max[warp] = smax; red_min[warp] = smin; red_kmin[warp] = kmin; }
+		__syncthreads();
+		if (threadIdx.x == 0) {
+			double a = 0, mx = 0, mn = 1e308;
+			int km = 0;
+			for (int q = 0; q < nwarp; q++) {
+				a += red_sum[q];
+				mx = fmax(mx, red_max[q]);
+				if (red_min[q] < mn || (red_min[q] == mn && red_kmin[q] < km)) { mn = red_min[q]; km = red_kmin[q]; }
+			}
+			SlStats st = stats[w.slot];
+			int fl = (sizeof(Real) == 8) ? kFlagFP64 : 0;
+			if (prm.only_flagged) fl |= (st.flags & kFlagIllCond);
+			if (!converged) fl |= kFlagUnconverged;
+			if (!prm.only_flagged && prm.ill_ratio > 0 && (!converged || mx == 0.0 || mn < prm.ill_ratio * mx))
+				fl |= kFlagIllCond;
+			st.s_sum = a;
+			st.s_max = mx;
+			st.s_min = mn;
+			st.k_min = km;
+			st.flags = fl;
+			stats[w.slot] = st;
+		}
+		__syncthreads();
+	}
+	// normalise columns: u_c = b_c / sigma_c (in place); exactly-zero columns are completed below
+	for (int64_t e = threadIdx.x; e < (int64_t)n * n; e += blockDim.x) {
+		int c = (int)(e / n);
+		Real s = sg[c];
+		B[e] = (s > 0) ? B[e] / s : Real(0);
+	}
+	__syncthreads();
+	// orthonormal completion of zero columns (rank-deficient A with exact zeros): Gram-Schmidt of
+	// unit vectors against the existing columns.  Rare; executed by warp 0.
+	if (warp == 0) {
+		for (int c = 0; c < n; c++) {
+			if (sg[c] > 0) continue;
+			for (int cand = 0; cand < n; cand++) {
+				Real *uc = B + (int64_t)c * n;
+				for (int i = lane; i < n; i += 32) uc[i] = (i == cand) ? Real(1) : Real(0);
+				__syncwarp();
+				for (int pass = 0; pass < 2; pass++) {
+					for (int o = 0; o < n; o++) {
+						if (o == c) continue;
+						const Real *uo = B + (int64_t)o * n;
+						Real no = 0;
+						for (int i = lane; i < n; i += 32) no += uo[i] * uo[i];
+						no = warp_sum(no);
+						if (no == 0) continue;
+						Real dp = 0;
+						for (int i = lane; i < n; i += 32) dp += uo[i] * uc[i];
+						dp = warp_sum(dp);
+						for (int i = lane; i < n; i += 32) uc[i] -= dp * uo[i];
+						__syncwarp();
+					}
+				}
+				Real nn = 0;
+				for (int i = lane; i < n; i += 32) nn += uc[i] * uc[i];
+				nn = warp_sum(nn);
+				if (nn > Real(0.25)) {
+					Real inv = Real(1) / real_sqrt(nn);
+					for (int i = lane; i < n; i += 32) uc[i] *= inv;
+					__syncwarp();
+					if (lane == 0) sg[c] = Real(-1);  // marks "completed" (positive for no later test)
+					break;
+				}
+			}
+		}
+	}
+	__syncthreads();
+	// save u_min, v_min for the reflection fix
+	{
+		int km = stats[w.slot].k_min;
+		double *uv = uvbuf + w.uvofs;
+		for (int i = threadIdx.x; i < n; i += blockDim.x) {
+			uv[i] = (double)B[(int64_t)km * n + i];
+			uv[n + i] = (double)V[(int64_t)km * n + i];
+		}
+	}
+	// T = U V^T :  T(i, j) = sum_c U[c][i] V[c][j], written as float32 (resident mode; the
+	// blocked mode forms T in k_form_t_global)
+	if (resident) {
+		GemmArgs<Real, float> g;
+		g.M = n; g.N = n; g.K = n;
+		g.P = B; g.pk = n; g.pi = 1;
+		g.Q = V; g.qk = n; g.qj = 1;
+		g.d = nullptr; g.alpha = Real(1);
+		g.E = nullptr; g.ei = 0; g.ej = 0; g.beta = 0;
+		g.C = Tscr + w.tofs;
+		g.ci = prm.t_rowmajor ? n : 1;
+		g.cj = prm.t_rowmajor ? 1 : n;
+		Real (*ps)[65] = reinterpret_cast<Real (*)[65]>(sig + ncol + 2);
+		Real (*qs)[65] = ps + 16;
+		block_gemm(g, ps, qs);
+	}
+}
+
+// Blocked-mode T formation: T = U V^T with U, V in global scratch (one CTA per searchlight).
+template <typename Real>
+__global__ void __launch_bounds__(256) k_form_t_global(const SlWork *__restrict__ work, const Real *__restrict__ Ascr,
+                                                       const Real *__restrict__ Vscr, float *__restrict__ Tscr,
+                                                       const SlStats *__restrict__ stats, int t_rowmajor,
+                                                       int only_flagged) {
+	__shared__ Real ps[16][65], qs[16][65];
+	const SlWork w = work[blockIdx.x];
+	if (w.nblk == 2) return;
+	if (only_flagged && !(stats[w.slot].flags & kFlagIllCond)) return;
+	const int n = w.n;
+	GemmArgs<Real, float> g;
+	g.M = n; g.N = n; g.K = n;
+	g.P = Ascr + w.aofs; g.pk = n; g.pi = 1;
+	g.Q = Vscr + w.aofs; g.qk = n; g.qj = 1;
+	g.d = nullptr; g.alpha = Real(1);
+	g.E = nullptr; g.ei = 0; g.ej = 0; g.beta = 0;
+	g.C = Tscr + w.tofs;
+	g.ci = t_rowmajor ? n : 1;
+	g.cj = t_rowmajor ? 1 : n;
+	block_gemm(g, ps, qs);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Newton-Schulz orthogonality refinement  T <- T (3 I - T^T T) / 2   (float32)
+// ---------------------------------------------------------------------------------------------
+// T in the T scratch (row- or column-major), G = T^T T staged in Gs, result staged in Ws and
+// copied back.  Searchlights solved in FP64 are skipped (already orthogonal to FP32 rounding).
+__global__ void __launch_bounds__(256) k_ns_refine(const SlWork *__restrict__ work, float *__restrict__ Tscr,
+                                                   float *__restrict__ Gscr, float *__restrict__ Wscr,
+                                                   const SlStats *__restrict__ stats, int t_rowmajor) {
+	__shared__ float ps[16][65], qs[16][65];
+	const SlWork w = work[blockIdx.x];
+	if (stats[w.slot].flags & kFlagFP64) return;
+	const int n = w.n;
+	float *T = Tscr + w.tofs;
+	float *G = Gscr + w.aofs;
+	float *W = Wscr + w.aofs;
+	// element (i, j) of T at T[i*ti + j*tj]
+	const int64_t ti = t_rowmajor ? n : 1, tj = t_rowmajor ? 1 : n;
+	// G(a, b) = sum_i T(i, a) T(i, b) ; stored row-major
+	GemmArgs<float> g;
+	g.M = n; g.N = n; g.K = n;
+	g.P = T; g.pk = ti; g.pi = tj;
+	g.Q = T; g.qk = ti; g.qj = tj;
+	g.d = nullptr; g.alpha = 1.0f;
+	g.E = nullptr; g.ei = 0; g.ej = 0; g.beta = 0.0f;
+	g.C = G; g.ci = n; g.cj = 1;
+	block_gemm(g, ps, qs);
+	// M = 1.5 I - 0.5 G  (in place)
+	for (int64_t e = threadIdx.x; e < (int64_t)n * n; e += blockDim.x) {
+		int a = (int)(e / n), b = (int)(e - (int64_t)a * n);
+		G[e] = ((a == b) ? 1.5f : 0.0f) - 0.5f * G[e];
+	}
+	__syncthreads();
+	// W(i, j) = sum_a T(i, a) M(a, j)
+	g.P = T; g.pk = tj; g.pi = ti;
+	g.Q = G; g.qk = n; g.qj = 1;
+	g.C = W; g.ci = ti; g.cj = tj;
+	block_gemm(g, ps, qs);
+	for (int64_t e = threadIdx.x; e < (int64_t)n * n; e += blockDim.x) T[e] = W[e];
+}
+
+// ---------------------------------------------------------------------------------------------
+// reflection fix (csrc/ha_searchlight.c:612-632): det(T) < 0 -> T -= 2 u_min v_min^T
+// ---------------------------------------------------------------------------------------------
+// sign(det T) from an LU factorisation with partial pivoting of a copy of T (T is orthogonal,
+// so the factorisation is well conditioned).  Work copy in Wscr (float64, n*n per searchlight).
+__global__ void __launch_bounds__(256) k_reflect_fix(const SlWork *__restrict__ work, float *__restrict__ Tscr,
+                                                     double *__restrict__ Wscr, SlStats *__restrict__ stats,
+                                                     const double *__restrict__ uvbuf, int t_rowmajor) {
+	const SlWork w = work[blockIdx.x];
+	const int n = w.n;
+	float *T = Tscr + w.tofs;
+	double *L = Wscr + w.aofs;  // column-major copy: L[c*n + r] = T(r, c)
+	const int64_t ti = t_rowmajor ? n : 1, tj = t_rowmajor ? 1 : n;
+	for (int64_t e = threadIdx.x; e < (int64_t)n * n; e += blockDim.x) {
+		int c = (int)(e / n), r = (int)(e - (int64_t)c * n);
+		L[e] = (double)T[r * ti + c * tj];
+	}
+	__syncthreads();
+	__shared__ double pv[32];
+	__shared__ int pr[32];
+	__shared__ int piv_row;
+	__shared__ double sign_acc;
+	if (threadIdx.x == 0) sign_acc = 1.0;
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+	for (int k = 0; k < n; k++) {
+		// pivot search in column k, rows k..n-1
+		double best = -1.0;
+		int bi = k;
+		for (int r = k + threadIdx.x; r < n; r += blockDim.x) {
+			double v = fabs(L[(int64_t)k * n + r]);
+			if (v > best) { best = v; bi = r; }
+		}
+		for (int o = 16; o > 0; o >>= 1) {
+			double ob = __shfl_xor_sync(0xffffffffu, best, o);
+			int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+			if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+		}
+		if (lane == 0) { pv[warp] = best; pr[warp] = bi; }
+		__syncthreads();
+		if (threadIdx.x == 0) {
+			double b = -1.0;
+			int i = k;
+			for (int q = 0; q < nwarp; q++)
+				if (pv[q] > b || (pv[q] == b && pr[q] < i)) { b = pv[q]; i = pr[q]; }
+			piv_row = i;
+			if (i != k) sign_acc = -sign_acc;
+		}
+		__syncthreads();
+		int p = piv_row;
+		if (p != k)
+			for (int c = threadIdx.x; c < n; c += blockDim.x) {
+				double a = L[(int64_t)c * n + k];
+				L[(int64_t)c * n + k] = L[(int64_t)c * n + p];
+				L[(int64_t)c * n + p] = a;
+			}
+		__syncthreads();
+		double d = L[(int64_t)k * n + k];
+		if (threadIdx.x == 0 && d < 0) sign_acc = -sign_acc;
+		if (d != 0.0) {
+			for (int r = k + 1 + threadIdx.x; r < n; r += blockDim.x) L[(int64_t)k * n + r] /= d;
+			__syncthreads();
+			for (int64_t e = threadIdx.x; e < (int64_t)(n - k - 1) * (n - k - 1); e += blockDim.x) {
+				int cc = (int)(e / (n - k - 1)), rr = (int)(e - (int64_t)cc * (n - k - 1));
+				int c = k + 1 + cc, r = k + 1 + rr;
+				L[(int64_t)c * n + r] -= L[(int64_t)k * n + r] * L[(int64_t)c * n + k];
+			}
+		}
+		__syncthreads();
+	}
+	if (sign_acc < 0) {
+		const double *u = uvbuf + w.uvofs;
+		const double *v = u + n;
+		for (int64_t e = threadIdx.x; e < (int64_t)n * n; e += blockDim.x) {
+			int i = (int)(e / n), j = (int)(e - (int64_t)i * n);
+			T[i * ti + j * tj] = (float)((double)T[i * ti + j * tj] - 2.0 * u[i] * v[j]);
+		}
+		if (threadIdx.x == 0) {
+			SlStats st = stats[w.slot];
+			st.s_sum -= 2.0 * st.s_min;
+			st.flags |= kFlagReflected;
+			stats[w.slot] = st;
+		}
+	}
+}
+
+// ---------------------------------------------------------------------------------------------
+// per-searchlight coefficient: scale = s_sum / (var_sum * nt) (csrc/ha_searchlight.c:635-656)
+// ---------------------------------------------------------------------------------------------
+__global__ void k_scale(const SlWork *__restrict__ work, int nwork, const int32_t *__restrict__ sl_idx,
+                        const double *__restrict__ var_over_nt, const SlStats *__restrict__ stats, int nt,
+                        int scaling, double *__restrict__ scale_out) {
+	int q = blockIdx.x * blockDim.x + threadIdx.x;
+	if (q >= nwork) return;
+	const SlWork w = work[q];
+	double sc = 1.0;
+	if (scaling) {
+		const int32_t *sl = sl_idx + w.sofs;
+		double var_sum = 0.0;
+		for (int j = 0; j < w.n; j++) var_sum = __dadd_rn(var_sum, var_over_nt[sl[j]]);
+		sc = stats[w.slot].s_sum / (var_sum * nt);
+	}
+	scale_out[w.slot] = sc;
+}
+
+// ---------------------------------------------------------------------------------------------
+// symmetric CSC / CSR pattern of the union of sl x sl blocks (csrc/ha_sparse.c:31-112)
+// ---------------------------------------------------------------------------------------------
+// Row (= column) v of the pattern is the set of vertices sharing a searchlight with v.
+// One CTA per vertex marks them in a shared-memory bitmap of nv bits (restricted to the
+// [lo, hi] window of vertices it can reach), then counts (pass 0) or writes them in
+// ascending order (pass 1).  No pair enumeration, no sort.
+__global__ void k_pattern(const int64_t *__restrict__ vl_ptr, const int2 *__restrict__ vl_ent,
+                          const int32_t *__restrict__ sl_off, const int32_t *__restrict__ sl_idx,
+                          const int32_t *__restrict__ sl_lo, const int32_t *__restrict__ sl_hi, int nv,
+                          int pass, int64_t *__restrict__ row_len, const int64_t *__restrict__ row_ptr,
+                          int32_t *__restrict__ cols) {
+	extern __shared__ uint32_t bm[];
+	__shared__ int s_lo, s_hi;
+	__shared__ int64_t wsum[33];
+	const int v = blockIdx.x;
+	const int64_t e0 = vl_ptr[v], e1 = vl_ptr[v + 1];
+	if (threadIdx.x == 0) { s_lo = nv; s_hi = -1; }
+	__syncthreads();
+	// window of reachable vertices
+	for (int64_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+		int s = vl_ent[e].x;
+		atomicMin(&s_lo, sl_lo[s]);
+		atomicMax(&s_hi, sl_hi[s]);
+	}
+	__syncthreads();
+	const int lo = s_lo & ~31, hi = s_hi;
+	if (hi < lo) {
+		if (pass == 0 && threadIdx.x == 0) row_len[v] = 0;
+		return;
+	}
+	const int nwords = (hi - lo) / 32 + 1;
+	for (int q = threadIdx.x; q < nwords; q += blockDim.x) bm[q] = 0u;
+	__syncthreads();
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+	for (int64_t e = e0 + warp; e < e1; e += nwarp) {
+		int s = vl_ent[e].x;
+		int a0 = sl_off[s], a1 = sl_off[s + 1];
+		for (int a = a0 + lane; a < a1; a += 32) {
+			int u = sl_idx[a] - lo;
+			atomicOr(&bm[u >> 5], 1u << (u & 31));
+		}
+	}
+	__syncthreads();
+	// per-thread contiguous word ranges -> prefix sum of popcounts
+	const int per = (nwords + blockDim.x - 1) / blockDim.x;
+	const int q0 = threadIdx.x * per, q1 = min(nwords, q0 + per);
+	int64_t cnt = 0;
+	for (int q = q0; q < q1; q++) cnt += __popc(bm[q]);
+	// block exclusive scan of cnt
+	int64_t incl = cnt;
+	for (int o = 1; o < 32; o <<= 1) {
+		int64_t y = __shfl_up_sync(0xffffffffu, incl, o);
+		if (lane >= o) incl += y;
+	}
+	if (lane == 31) wsum[warp] = incl;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		int64_t run = 0;
+		for (int q = 0; q < nwarp; q++) {
+			int64_t t = wsum[q];
+			wsum[q] = run;
+			run += t;
+		}
+		wsum[32] = run;
+	}
+	__syncthreads();
+	if (pass == 0) {
+		if (threadIdx.x == 0) row_len[v] = wsum[32];
+		return;
+	}
+	int64_t pos = row_ptr[v] + wsum[warp] + incl - cnt;
+	for (int q = q0; q < q1; q++) {
+		uint32_t b = bm[q];
+		while (b) {
+			int bit = __ffs(b) - 1;
+			b &= b - 1;
+			cols[pos++] = lo + q * 32 + bit;
+		}
+	}
+}
+
+// ---------------------------------------------------------------------------------------------
+// deterministic segmented reduction into the pattern's values
+// ---------------------------------------------------------------------------------------------
+// One CTA per vertex v.  Its entries (s, a) (v is member a of searchlight s) are sorted by s;
+// those of the current chunk [s_lo, s_hi) are visited in that order, and for each one the
+// whole row a of the searchlight's M_s (M_s = T_s for CSR output, T_s^T for CSC output) is
+// added at the slots of its columns, found by binary search in v's sorted pattern row.
+// Within one searchlight the columns are distinct, so threads never collide; a barrier
+// separates searchlights, so every sum runs in ascending searchlight order on every run.
+//   CSR (row v = dense row v):   val(v, u_b) += w_s[a] * scale_s * T_s[a][b]
+//   CSC (column v):              val(u_b, v) += w_s[b] * scale_s * T_s[b][a]
+__global__ void __launch_bounds__(256) k_reduce(const int64_t *__restrict__ vl_ptr, const int2 *__restrict__ vl_ent,
+                                                const int32_t *__restrict__ sl_off, const int32_t *__restrict__ sl_idx,
+                                                const double *__restrict__ wts, const int64_t *__restrict__ pat_ptr,
+                                                const int32_t *__restrict__ pat_col, const float *__restrict__ Tscr,
+                                                const int64_t *__restrict__ tofs_by_slot,
+                                                const double *__restrict__ scale_by_slot, int s_lo, int s_hi,
+                                                int csc, int smem_cap, double *__restrict__ values) {
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	const int v = blockIdx.x;
+	const int64_t e0 = vl_ptr[v], e1 = vl_ptr[v + 1];
+	// first entry with s >= s_lo (entries sorted by s)
+	int64_t lo = e0, hi = e1;
+	while (lo < hi) {
+		int64_t mid = (lo + hi) >> 1;
+		if (vl_ent[mid].x < s_lo) lo = mid + 1; else hi = mid;
+	}
+	const int64_t eb = lo;
+	if (eb >= e1 || vl_ent[eb].x >= s_hi) return;
+	const int64_t p0 = pat_ptr[v];
+	const int L = (int)(pat_ptr[v + 1] - p0);
+	const bool in_smem = L <= smem_cap;
+	double *acc;
+	const int32_t *cols;
+	if (in_smem) {
+		acc = reinterpret_cast<double *>(smem_raw);
+		int32_t *cs = reinterpret_cast<int32_t *>(acc + L);
+		for (int k = threadIdx.x; k < L; k += blockDim.x) {
+			acc[k] = values[p0 + k];
+			cs[k] = pat_col[p0 + k];
+		}
+		cols = cs;
+		__syncthreads();
+	} else {
+		acc = values + p0;
+		cols = pat_col + p0;
+	}
+	for (int64_t e = eb; e < e1; e++) {
+		const int2 ent = vl_ent[e];
+		const int s = ent.x;
+		if (s >= s_hi) break;
+		const int a = ent.y;
+		const int o0 = sl_off[s];
+		const int n = sl_off[s + 1] - o0;
+		const int slot = s - s_lo;
+		const float *M = Tscr + tofs_by_slot[slot] + (int64_t)a * n;
+		const double sc = scale_by_slot[slot];
+		const double wa = wts ? wts[o0 + a] : 1.0;
+		for (int b = threadIdx.x; b < n; b += blockDim.x) {
+			const int u = sl_idx[o0 + b];
+			int l = 0, h = L;
+			while (l < h) {
+				int mid = (l + h) >> 1;
+				if (cols[mid] < u) l = mid + 1; else h = mid;
+			}
+			double wgt = csc ? (wts ? wts[o0 + b] : 1.0) : wa;
+			acc[l] += (double)M[b] * (wgt * sc);
+		}
+		__syncthreads();
+	}
+	if (in_smem) {
+		for (int k = threadIdx.x; k < L; k += blockDim.x) values[p0 + k] = acc[k];
+	}
+}
+
+}  // namespace hab200

@@ -1,0 +1,130 @@
+"""Python entry points of the B200 backend, shaped like the reference ctypes wrapper.
+
+``searchlight_procrustes`` keeps the signature, argument meaning and error
+behaviour of the reference's ``hyperalignment_c.searchlight_procrustes``
+(hyperalignment_c.py:112-223): Fortran-order float64 X/Y, flattened
+searchlights, a zero-initialised dense ``nv x nv`` result from one C call,
+``RuntimeError`` on a non-zero return code.  The only backend accepted here is
+``"b200"`` (enum value 4); the reference's CPU/Metal/CUDA backends live in the
+reference library.
+
+The sparse (CSC) and ridge calls take scipy-compatible CSC arrays whose pattern
+is the union of searchlight blocks (``sparse_pattern``, bit-exact to the
+reference's ``ha_sparse_init``).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from . import _lib as L
+
+_BACKENDS = {"b200": L.BACKEND_B200}
+
+
+def _flatten(sls, dists):
+    sizes = np.array([len(s) for s in sls], dtype=np.int32)
+    offsets = np.zeros(len(sls) + 1, dtype=np.int32)
+    np.cumsum(sizes, out=offsets[1:])
+    idx = np.ascontiguousarray(np.concatenate(sls).astype(np.int32))
+    d = None if dists is None else np.ascontiguousarray(np.concatenate(dists).astype(np.float64))
+    return idx, offsets, d
+
+
+def _init():
+    lib = L.lib()
+    rc = lib.ha_b200_init()
+    if rc != 0:
+        raise RuntimeError("ha_b200_init() failed. Is an sm_100 (B200) GPU present?")
+    return lib
+
+
+def searchlight_procrustes(X, Y, sls, dists, radius, backend="b200", reflection=True, scaling=False,
+                           n_jobs=1, T_out=None):
+    """Searchlight Procrustes; returns the dense ``nv x nv`` float64 transformation.
+
+    Same contract as the reference wrapper (hyperalignment_c.py:112-143).  If
+    ``T_out`` is given it is accumulated into (the C call's ``+=`` contract) and
+    returned; otherwise a zero matrix is allocated.
+    """
+    if backend not in _BACKENDS:
+        raise ValueError(f"Unknown backend '{backend}'. Choose from: {list(_BACKENDS.keys())}")
+    lib = _init()
+    if n_jobs > 0:
+        lib.ha_set_num_threads(n_jobs)
+    X = np.asfortranarray(X, dtype=np.float64)
+    Y = np.asfortranarray(Y, dtype=np.float64)
+    nt, nv = X.shape
+    idx, offsets, d = _flatten(sls, dists)
+    if T_out is None:
+        T_out = np.zeros((nv, nv), dtype=np.float64)
+    elif T_out.dtype != np.float64 or not T_out.flags.c_contiguous or T_out.shape != (nv, nv):
+        raise ValueError("T_out must be a C-contiguous float64 (nv, nv) array")
+    rc = lib.ha_searchlight_procrustes_dense(
+        L.dptr(X), L.dptr(Y), nt, nv, L.iptr(idx), L.iptr(offsets), L.dptr(d), len(sls), float(radius),
+        L.dptr(T_out), bool(reflection), bool(scaling), _BACKENDS[backend], True)
+    if rc != 0:
+        raise RuntimeError(f"ha_searchlight_procrustes_dense failed with error code {rc}")
+    return T_out
+
+
+def searchlight_weights(sls, dists=None, radius=None, nv=None):
+    """Flat weights (one per searchlight member), the reference's rule, computed by the library."""
+    lib = L.lib()
+    idx, offsets, d = _flatten(sls, dists)
+    if nv is None:
+        nv = int(idx.max()) + 1
+    out = np.empty(idx.size, dtype=np.float64)
+    L.check(lib.ha_searchlight_weights_b200(L.iptr(idx), L.iptr(offsets), L.dptr(d), len(sls),
+                                            float(radius or 0.0), nv, L.dptr(out)), "ha_searchlight_weights_b200")
+    return out
+
+
+def sparse_pattern(sls, nv):
+    """CSC pattern (indptr, indices) of the union of ``sl x sl`` blocks, built on the GPU."""
+    lib = _init()
+    idx, offsets, _ = _flatten(sls, None)
+    indptr = np.empty(nv + 1, dtype=np.int32)
+    nnz = __import__("ctypes").c_int64(0)
+    L.check(lib.ha_sparse_pattern_b200(L.iptr(idx), L.iptr(offsets), len(sls), nv, L.iptr(indptr), None, 0,
+                                       __import__("ctypes").byref(nnz)), "ha_sparse_pattern_b200")
+    indices = np.empty(nnz.value, dtype=np.int32)
+    L.check(lib.ha_sparse_pattern_b200(L.iptr(idx), L.iptr(offsets), len(sls), nv, L.iptr(indptr),
+                                       L.iptr(indices), nnz.value, __import__("ctypes").byref(nnz)),
+            "ha_sparse_pattern_b200")
+    return indptr, indices
+
+
+def searchlight_procrustes_csc(X, Y, sls, indptr, indices, data, weights=None, reflection=True, scaling=False):
+    """Sparse-output searchlight Procrustes: accumulates into ``data`` (CSC, pattern ``indptr``/``indices``)."""
+    lib = _init()
+    X = np.asfortranarray(X, dtype=np.float64)
+    Y = np.asfortranarray(Y, dtype=np.float64)
+    nt, nv = X.shape
+    idx, offsets, _ = _flatten(sls, None)
+    w = None if weights is None else np.ascontiguousarray(np.concatenate(weights).astype(np.float64))
+    L.check(lib.ha_searchlight_procrustes_csc_b200(
+        L.dptr(X), L.dptr(Y), nt, nv, L.iptr(idx), L.iptr(offsets), len(sls), L.dptr(w),
+        L.iptr(np.ascontiguousarray(indptr, dtype=np.int32)), L.iptr(np.ascontiguousarray(indices, dtype=np.int32)),
+        int(len(indices)), L.dptr(data), bool(reflection), bool(scaling), True),
+        "ha_searchlight_procrustes_csc_b200")
+    return data
+
+
+def searchlight_ridge_csc(X, Y, sls, indptr, indices, data, alpha, weights=None):
+    """Sparse-output searchlight ridge (float64): accumulates into ``data``."""
+    lib = _init()
+    X = np.asfortranarray(X, dtype=np.float64)
+    Y = np.asfortranarray(Y, dtype=np.float64)
+    nt, nv = X.shape
+    idx, offsets, _ = _flatten(sls, None)
+    w = None if weights is None else np.ascontiguousarray(np.concatenate(weights).astype(np.float64))
+    L.check(lib.ha_searchlight_ridge_csc_b200(
+        L.dptr(X), L.dptr(Y), nt, nv, L.iptr(idx), L.iptr(offsets), len(sls), L.dptr(w),
+        L.iptr(np.ascontiguousarray(indptr, dtype=np.int32)), L.iptr(np.ascontiguousarray(indices, dtype=np.int32)),
+        int(len(indices)), L.dptr(data), float(alpha), True), "ha_searchlight_ridge_csc_b200")
+    return data
+
+
+def cleanup():
+    L.lib().ha_b200_cleanup()

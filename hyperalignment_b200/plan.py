@@ -1,0 +1,87 @@
+"""Device-resident plan: one searchlight geometry, many solves (include/hyperalignment_b200.h).
+
+Device memory and streams are whatever the caller owns; this wrapper takes raw
+device pointers (ints), e.g. ``tensor.data_ptr()`` of CUDA tensors, and a raw
+``cudaStream_t`` handle (``torch.cuda.current_stream().cuda_stream``) or 0.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib as L
+
+
+class Plan:
+    def __init__(self, nt, nv, indices, offsets, dists=None, radius=0.0, weights=None):
+        self.lib = L.lib()
+        L.check(self.lib.ha_b200_init(), "ha_b200_init")
+        self.nt, self.nv = int(nt), int(nv)
+        self.indices = np.ascontiguousarray(indices, dtype=np.int32)
+        self.offsets = np.ascontiguousarray(offsets, dtype=np.int32)
+        self.count = int(self.offsets.size - 1)
+        d = None if dists is None else np.ascontiguousarray(dists, dtype=np.float64)
+        w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+        h = ctypes.c_void_p()
+        L.check(self.lib.ha_b200_plan_create(self.nt, self.nv, L.iptr(self.indices), L.iptr(self.offsets), L.dptr(d),
+                                             self.count, float(radius), L.dptr(w), ctypes.byref(h)),
+                "ha_b200_plan_create")
+        self.handle = h
+
+    @classmethod
+    def from_workload(cls, w, weights=None):
+        return cls(w.nt, w.nv, w.sls.indices, w.sls.offsets, w.sls.dists, w.sls.radius, weights)
+
+    @property
+    def nnz(self) -> int:
+        return int(self.lib.ha_b200_plan_nnz(self.handle))
+
+    def pattern(self):
+        indptr = np.empty(self.nv + 1, dtype=np.int64)
+        indices = np.empty(self.nnz, dtype=np.int32)
+        L.check(self.lib.ha_b200_plan_pattern(self.handle, indptr.ctypes.data_as(L.c_int64_p), L.iptr(indices)),
+                "ha_b200_plan_pattern")
+        return indptr, indices
+
+    def procrustes_device(self, d_X: int, d_Y: int, d_values: int, reflection=True, scaling=False,
+                          solver=L.SOLVER_MIXED, out_kind=L.OUT_CSR, stream: int = 0):
+        L.check(self.lib.ha_b200_plan_procrustes_device(self.handle, ctypes.c_void_p(d_X), ctypes.c_void_p(d_Y),
+                                                        bool(reflection), bool(scaling), int(solver), int(out_kind),
+                                                        ctypes.c_void_p(d_values), ctypes.c_void_p(stream)),
+                "ha_b200_plan_procrustes_device")
+
+    def ridge_device(self, d_X: int, d_Y: int, d_values: int, alpha: float, out_kind=L.OUT_CSC, stream: int = 0):
+        L.check(self.lib.ha_b200_plan_ridge_device(self.handle, ctypes.c_void_p(d_X), ctypes.c_void_p(d_Y),
+                                                   float(alpha), int(out_kind), ctypes.c_void_p(d_values),
+                                                   ctypes.c_void_p(stream)), "ha_b200_plan_ridge_device")
+
+    def stats(self):
+        a, b = ctypes.c_int32(), ctypes.c_int32()
+        L.check(self.lib.ha_b200_plan_stats(self.handle, ctypes.byref(a), ctypes.byref(b)), "ha_b200_plan_stats")
+        return {"n_fp64": a.value, "n_unconverged": b.value}
+
+    def local_transforms(self, first: int, n: int):
+        """Unweighted, unscaled T_s of searchlights [first, first+n) from the last run (row-major if CSR)."""
+        sizes = np.diff(self.offsets[first:first + n + 1])
+        buf = np.empty(int((sizes.astype(np.int64) ** 2).sum()), dtype=np.float32)
+        L.check(self.lib.ha_b200_plan_local_transforms(self.handle, first, n,
+                                                        buf.ctypes.data_as(ctypes.POINTER(ctypes.c_float))),
+                "ha_b200_plan_local_transforms")
+        out, o = [], 0
+        for k in sizes:
+            out.append(buf[o:o + k * k].reshape(k, k).astype(np.float64))
+            o += k * k
+        return out
+
+    def close(self):
+        if self.handle:
+            self.lib.ha_b200_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,267 @@
+/*
+ * hyperalignment_b200.h -- C ABI of the B200 (sm_100a) searchlight alignment backend.
+ *
+ * The backend is a drop-in for the searchlight calls of the reference C library
+ * (neurolabusc/hyperalignment, csrc/).  It adds one value to the reference's
+ * backend enum, kHaBackendB200 = 4, and exports:
+ *
+ *   - the reference's dense entry point under its own name and signature
+ *     (csrc/ha_searchlight.h:69-80), accepting backend == kHaBackendB200, so the
+ *     reference ctypes wrapper (hyperalignment_c.py:44-60) binds it unchanged;
+ *   - a backend function with the signature of the reference's CUDA backend
+ *     (csrc/ha_cuda.h:56-66), for the reference dispatcher
+ *     (csrc/ha_searchlight.c:1106-1132) to call;
+ *   - flat-array (pointer + size) forms of the sparse-output Procrustes and ridge
+ *     searchlight calls (csrc/ha_searchlight.h:46-52, :86-90) and of the CSC
+ *     pattern builder (csrc/ha_sparse.h, ha_sparse_init);
+ *   - lifecycle calls shaped like the CUDA backend's (csrc/ha_cuda.h:32-42).
+ *
+ * All arguments are plain pointers and sizes.  Unless a function says
+ * "device", every pointer is host memory owned by the caller.  Return values
+ * are the reference's error codes (csrc/ha_common.h:36-42).  There is no CPU
+ * fallback: with no usable GPU or no loaded kernels the calls return
+ * kHaErrorInternal and print the reason to stderr.
+ *
+ * Threading: one host thread at a time (calls are serialised by a mutex).
+ * The backend keeps device buffers between calls; ha_b200_cleanup releases them.
+ */
+#ifndef HYPERALIGNMENT_B200_H
+#define HYPERALIGNMENT_B200_H
+
+#include <stdbool.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#ifndef HA_COMMON_H
+/* Same values as csrc/ha_common.h:36-42 and :71-76 of the reference. */
+enum {
+	kHaSuccess       =  0,
+	kHaErrorAlloc    = -1,
+	kHaErrorSvd      = -2,
+	kHaErrorArg      = -3,
+	kHaErrorInternal = -4,
+};
+typedef enum {
+	kHaBackendCPU64 = 0,
+	kHaBackendCPU32 = 1,
+	kHaBackendMetal = 2,
+	kHaBackendCUDA  = 3,
+} THaBackend;
+#endif
+
+#ifndef HA_HAS_BACKEND_B200
+/* New backend value; 0-3 keep their reference meaning. */
+#define kHaBackendB200 ((THaBackend)4)
+#endif
+
+/* ---- lifecycle (cf. ha_cuda_init / ha_cuda_cleanup / ha_cuda_available, csrc/ha_cuda.h:32-42) ---- */
+
+/* Selects the current CUDA device and checks that it is sm_100.  Idempotent and cheap. */
+int ha_b200_init(void);
+/* Releases every device buffer, stream and cached plan.  Safe without init. */
+void ha_b200_cleanup(void);
+/* True once ha_b200_init succeeded. */
+bool ha_b200_available(void);
+
+/* Host threads for host-side work (accumulating into caller's dense T), cf. csrc/ha_searchlight.h:14-20. */
+void ha_set_num_threads(int n);
+int ha_get_num_threads(void);
+
+/* ---- dense searchlight Procrustes ---- */
+
+/*
+ * Same contract as the reference's ha_searchlight_procrustes_dense
+ * (csrc/ha_searchlight.h:69-80, csrc/ha_searchlight.c:950-1376):
+ * X_data, Y_data are nt x nv float64 (column-major when col_major);
+ * searchlight s is sl_indices[sl_offsets[s] .. sl_offsets[s+1]); sl_dists NULL
+ * means uniform weights, else w = (radius - d) / radius normalised to sum to 1
+ * per vertex; T_out is nv x nv row-major float64 and is ACCUMULATED
+ * (T_out[sl[i], sl[j]] += w[i] * T_s[i, j]).  isReflection = false forces
+ * det(T_s) > 0 and isScaling applies the reference's global scale.
+ * backend must be kHaBackendB200; anything else returns kHaErrorArg (this
+ * library has no CPU paths).
+ */
+int ha_searchlight_procrustes_dense(
+	const double *X_data, const double *Y_data,
+	int32_t nt, int32_t nv,
+	const int32_t *sl_indices,
+	const int32_t *sl_offsets,
+	const double *sl_dists,
+	int32_t count,
+	double radius,
+	double *T_out,
+	bool isReflection, bool isScaling,
+	THaBackend backend,
+	bool col_major);
+
+/*
+ * Backend arm with the signature of ha_searchlight_procrustes_cuda
+ * (csrc/ha_cuda.h:56-66).  Unlike the reference CUDA arm it honours
+ * isScaling and isReflection = false, accepts col_major = false, and
+ * accumulates into T_out instead of overwriting it (ha_cuda.cu:445, :457-460).
+ */
+int ha_searchlight_procrustes_b200(
+	const double *X_data, const double *Y_data,
+	int32_t nt, int32_t nv,
+	const int32_t *sl_indices,
+	const int32_t *sl_offsets,
+	const double *sl_dists,
+	int32_t count,
+	double radius,
+	double *T_out,
+	bool isReflection, bool isScaling,
+	bool col_major);
+
+/* ---- CSC pattern and weights ---- */
+
+/*
+ * CSC sparsity pattern of the union of sl x sl blocks (nv x nv), bit-exact to
+ * the reference's ha_sparse_init (csrc/ha_sparse.c:31-112): rows ascending in
+ * each column, indptr of nv + 1 int32.  Built on the GPU without enumerating
+ * the sum of n^2 pairs.  Pass indices = NULL to get *nnz only; otherwise
+ * capacity must be >= nnz.  Searchlight indices must be unique within a
+ * searchlight and in [0, nv).
+ */
+int ha_sparse_pattern_b200(
+	const int32_t *sl_indices, const int32_t *sl_offsets, int32_t count, int32_t nv,
+	int32_t *indptr, int32_t *indices, int64_t capacity, int64_t *nnz);
+
+/*
+ * Flat searchlight weights (one float64 per sl_indices entry), the rule of
+ * ha_searchlight_weights (csrc/ha_searchlight.c:36-92), bit-exact.
+ */
+int ha_searchlight_weights_b200(
+	const int32_t *sl_indices, const int32_t *sl_offsets, const double *sl_dists,
+	int32_t count, double radius, int32_t nv, double *weights_out);
+
+/* ---- sparse-output searchlight Procrustes and ridge ---- */
+
+/*
+ * Flattened form of ha_searchlight_procrustes (csrc/ha_searchlight.h:46-52,
+ * csrc/ha_searchlight.c:147-413) with sls_Y = NULL: accumulates
+ * data[k] += w[i] * T_s[i, j] into the CSC matrix (indptr, indices, nnz)
+ * whose pattern came from ha_sparse_init or ha_sparse_pattern_b200.
+ * weights: one float64 per sl_indices entry (row weights, as
+ * ha_sparse_scatter_add, csrc/ha_sparse.c:128-142), or NULL for unweighted.
+ */
+int ha_searchlight_procrustes_csc_b200(
+	const double *X_data, const double *Y_data, int32_t nt, int32_t nv,
+	const int32_t *sl_indices, const int32_t *sl_offsets, int32_t count,
+	const double *weights,
+	const int32_t *indptr, const int32_t *indices, int64_t nnz, double *data,
+	bool isReflection, bool isScaling, bool col_major);
+
+/*
+ * Flattened form of ha_searchlight_ridge (csrc/ha_searchlight.h:86-90,
+ * csrc/ha_searchlight.c:1378-1429; local solve ha_ridge, csrc/ha_ridge.c:13-54):
+ * beta_s = V diag(s / (alpha + s^2)) U^T Y_s with X_s = U diag(s) V^T, scattered
+ * like the Procrustes call above.  Computed in float64.
+ */
+int ha_searchlight_ridge_csc_b200(
+	const double *X_data, const double *Y_data, int32_t nt, int32_t nv,
+	const int32_t *sl_indices, const int32_t *sl_offsets, int32_t count,
+	const double *weights,
+	const int32_t *indptr, const int32_t *indices, int64_t nnz, double *data,
+	double alpha, bool col_major);
+
+/* ---- device-resident plan (repeated calls on one searchlight geometry) ---- */
+
+typedef struct HaB200Plan HaB200Plan;
+
+/* Output kinds of a plan run. */
+enum {
+	kHaB200OutCSR = 0, /* values in row order of the symmetric pattern (row r = dense row r) */
+	kHaB200OutCSC = 1, /* values in CSC order (the layout of ha_sparse_init) */
+};
+
+/* Solver variants. */
+enum {
+	kHaB200SolverMixed = 0, /* FP32 Jacobi + FP32 Newton-Schulz refinement, FP64 re-solve of ill-conditioned searchlights */
+	kHaB200SolverFP32  = 1, /* plain FP32 form: FP32 Jacobi only, no refinement, no FP64 re-solve */
+	kHaB200SolverFP64  = 2, /* every searchlight in FP64 */
+};
+
+/*
+ * Uploads the searchlight geometry and builds on the GPU everything that
+ * depends only on it: weights (as ha_searchlight_procrustes_dense when
+ * weights == NULL, else the caller's), per-vertex membership lists, the
+ * symmetric CSC pattern, size buckets and scratch layout.
+ */
+int ha_b200_plan_create(
+	int32_t nt, int32_t nv,
+	const int32_t *sl_indices, const int32_t *sl_offsets, const double *sl_dists,
+	int32_t count, double radius, const double *weights,
+	HaB200Plan **plan_out);
+void ha_b200_plan_destroy(HaB200Plan *plan);
+/* Number of stored entries of the pattern, and a host copy of it (indptr: nv + 1 int64). */
+int64_t ha_b200_plan_nnz(const HaB200Plan *plan);
+int ha_b200_plan_pattern(const HaB200Plan *plan, int64_t *indptr, int32_t *indices);
+/* Device pointer to the plan's per-vertex pattern (indptr int64 nv+1, indices int32 nnz). */
+int ha_b200_plan_device_pattern(const HaB200Plan *plan, const int64_t **d_indptr, const int32_t **d_indices);
+/* Ill-conditioned searchlights that the last run re-solved in FP64, and the number of ones. */
+int ha_b200_plan_stats(const HaB200Plan *plan, int32_t *n_fp64, int32_t *n_jacobi_unconverged);
+
+/*
+ * Searchlight Procrustes on device-resident data.  d_X, d_Y: nt x nv float64
+ * in DEVICE memory, column-major (vertex j's time series contiguous).
+ * d_values: DEVICE float64 array of plan nnz entries, accumulated (+=) in the
+ * order given by out_kind.  stream: a cudaStream_t, or NULL for the legacy
+ * default stream.  Returns after enqueueing; synchronise the stream to read.
+ */
+int ha_b200_plan_procrustes_device(
+	HaB200Plan *plan, const double *d_X, const double *d_Y,
+	bool isReflection, bool isScaling, int solver, int out_kind,
+	double *d_values, void *stream);
+
+/* Ridge on device-resident data (same conventions), computed in float64. */
+int ha_b200_plan_ridge_device(
+	HaB200Plan *plan, const double *d_X, const double *d_Y, double alpha,
+	int out_kind, double *d_values, void *stream);
+
+/*
+ * Per-searchlight local transforms of the last device run, for testing:
+ * copies T_s (n_s x n_s, row-major, float32, unweighted and unscaled) of
+ * searchlights [first, first + n) into host out (sum of n_s^2 floats).
+ */
+int ha_b200_plan_local_transforms(const HaB200Plan *plan, int32_t first, int32_t n, float *out);
+
+/* ---- tracing ---- */
+
+/* Kernel kinds reported by ha_b200_kernel_times. */
+enum {
+	kHaB200KConvert = 0,    /* float64 -> float32 vertex-major restage */
+	kHaB200KColVar = 1,     /* per-vertex population variance (scaling) */
+	kHaB200KXcov32 = 2,     /* cross-covariance, float32 */
+	kHaB200KJacobi32 = 3,   /* Jacobi polar, float32 */
+	kHaB200KFormT32 = 4,    /* T = U V^T for blocked float32 searchlights */
+	kHaB200KXcov64 = 5,
+	kHaB200KJacobi64 = 6,
+	kHaB200KFormT64 = 7,
+	kHaB200KRefine = 8,     /* Newton-Schulz orthogonality refinement */
+	kHaB200KReflect = 9,    /* det(T) < 0 fix */
+	kHaB200KScale = 10,     /* per-searchlight scale / bookkeeping */
+	kHaB200KReduce = 11,    /* deterministic segmented reduction */
+	kHaB200KPattern = 12,   /* CSC pattern builder */
+	kHaB200KRidge = 13,     /* ridge solves */
+	kHaB200NumKernelKinds = 14,
+};
+
+/*
+ * When on, every kernel launch of this library is bracketed by CUDA events on its
+ * stream; ha_b200_kernel_times synchronises those events and returns (and resets)
+ * the accumulated device milliseconds and launch counts per kind.
+ */
+void ha_b200_set_kernel_timing(bool on);
+int ha_b200_kernel_times(double *ms, int64_t *launches);
+/* Kernels launched by this library since it was loaded. */
+int64_t ha_b200_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HYPERALIGNMENT_B200_H */

@@ -1,0 +1,217 @@
+"""CPU oracle: a numpy restatement of the reference's searchlight alignment path.
+
+TEST INFRASTRUCTURE ONLY.  Imported by tests/, by __graft_entry__.smoke() and by
+bench.py's CPU-baseline leg, always as the checker; the product path (the CUDA
+library) never calls it.
+
+Every function follows the reference C library (neurolabusc/hyperalignment,
+csrc/) in float64 and cites the lines it restates.  Pinning: tests/test_oracle.py
+checks these functions against the reference's own known-answer tests
+(csrc/ha_test.c) and against golden vectors produced by the compiled reference
+(tests/golden/make_golden.py, oracle/Makefile).  The SVD is LAPACK gesdd through
+numpy (the reference calls dgesdd_ / dgesvd_, csrc/ha_linalg.c:53-89).
+"""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+
+# ---------------------------------------------------------------------------------------------
+# deterministic test RNG of the reference harness (csrc/ha_test.c:33-65)
+# ---------------------------------------------------------------------------------------------
+
+class SplitMix64:
+    """splitmix64 stream with the harness's uniform and Box-Muller normal draws."""
+
+    MASK = (1 << 64) - 1
+
+    def __init__(self, seed: int):
+        self.state = seed & self.MASK
+
+    def next(self) -> int:  # csrc/ha_test.c:41-47
+        self.state = (self.state + 0x9E3779B97F4A7C15) & self.MASK
+        z = self.state
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & self.MASK
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & self.MASK
+        return z ^ (z >> 31)
+
+    def uniform(self) -> float:  # csrc/ha_test.c:50-52
+        return (self.next() >> 11) / float(1 << 53)
+
+    def randn(self) -> float:  # csrc/ha_test.c:55-60
+        u1 = self.uniform()
+        u2 = self.uniform()
+        if u1 < 1e-15:
+            u1 = 1e-15
+        return math.sqrt(-2.0 * math.log(u1)) * math.cos(2.0 * math.pi * u2)
+
+    def fill(self, rows: int, cols: int) -> np.ndarray:  # csrc/ha_test.c:63-66 (row-major fill)
+        return np.array([self.randn() for _ in range(rows * cols)], dtype=np.float64).reshape(rows, cols)
+
+
+# ---------------------------------------------------------------------------------------------
+# weights (csrc/ha_searchlight.c:970-1001, :36-92)
+# ---------------------------------------------------------------------------------------------
+
+def searchlight_weights(idx: np.ndarray, off: np.ndarray, dists, radius: float, nv: int) -> np.ndarray:
+    """Flat weights, same operation order as the reference (vertex sums in flat order)."""
+    idx = np.asarray(idx, dtype=np.int64)
+    vsum = np.zeros(nv, dtype=np.float64)
+    if dists is None:
+        w = np.ones(idx.size, dtype=np.float64)
+    else:
+        w = (radius - np.asarray(dists, dtype=np.float64)) / radius
+    np.add.at(vsum, idx, w)  # sequential, in flat order, like the C loop
+    return w / vsum[idx]
+
+
+# ---------------------------------------------------------------------------------------------
+# local Procrustes (csrc/ha_procrustes.c:17-127; column-major twin csrc/ha_searchlight.c:578-659)
+# ---------------------------------------------------------------------------------------------
+
+def _det_sign_lu(T: np.ndarray) -> float:
+    """Sign of det(T) from LU with partial pivoting (the dgetrf_ test of csrc/ha_procrustes.c:56-79)."""
+    sign, _ = np.linalg.slogdet(T)
+    return float(sign)
+
+
+def procrustes(X: np.ndarray, Y: np.ndarray, reflection: bool = True, scaling: bool = False,
+               return_svd: bool = False):
+    """T = U V^T for X^T Y = U S V^T, with the reference's reflection and scaling rules."""
+    A = X.T @ Y
+    U, s, Vt = np.linalg.svd(A)
+    T = U @ Vt
+    s = s.copy()
+    if not reflection:
+        if _det_sign_lu(T) < 0:  # csrc/ha_procrustes.c:80-94
+            s[-1] *= -1.0
+            T = T - 2.0 * np.outer(U[:, -1], Vt[-1, :])
+    if scaling:  # csrc/ha_procrustes.c:98-120: population variance of the local X columns
+        var_sum = float(np.sum(np.var(X, axis=0)))
+        T = T * (s.sum() / (var_sum * X.shape[0]))
+    if return_svd:
+        return T, U, s, Vt
+    return T
+
+
+def local_transforms(X, Y, idx, off, reflection=True, scaling=False):
+    """Per-searchlight local transforms T_s (n_s x n_s), unweighted."""
+    out = []
+    for s in range(len(off) - 1):
+        sl = idx[off[s]:off[s + 1]]
+        out.append(procrustes(X[:, sl], Y[:, sl], reflection, scaling))
+    return out
+
+
+def searchlight_procrustes_dense(X, Y, idx, off, dists, radius, reflection=True, scaling=False,
+                                 T_out=None, transforms=None):
+    """Dense searchlight Procrustes, csrc/ha_searchlight.c:950-1100 (cpu64 arm).
+
+    T_out[sl[i], sl[j]] += w[i] * T_s[i, j] with row weights (csrc/ha_searchlight.c:1073-1085).
+    """
+    nt, nv = X.shape
+    w = searchlight_weights(idx, off, dists, radius, nv)
+    if T_out is None:
+        T_out = np.zeros((nv, nv), dtype=np.float64)
+    for s in range(len(off) - 1):
+        sl = idx[off[s]:off[s + 1]]
+        T = transforms[s] if transforms is not None else procrustes(X[:, sl], Y[:, sl], reflection, scaling)
+        T_out[np.ix_(sl, sl)] += T * w[off[s]:off[s + 1], np.newaxis]
+    return T_out
+
+
+# ---------------------------------------------------------------------------------------------
+# CSC pattern and scatter (csrc/ha_sparse.c)
+# ---------------------------------------------------------------------------------------------
+
+def sparse_init(idx, off, nv):
+    """CSC pattern of the union of sl x sl blocks: (col, row)-sorted unique pairs, csrc/ha_sparse.c:31-112."""
+    keys = []
+    for s in range(len(off) - 1):
+        sl = np.asarray(idx[off[s]:off[s + 1]], dtype=np.int64)
+        rows = np.repeat(sl, sl.size)
+        cols = np.tile(sl, sl.size)
+        keys.append(cols * nv + rows)
+    keys = np.unique(np.concatenate(keys))
+    cols = keys // nv
+    rows = (keys - cols * nv).astype(np.int32)
+    indptr = np.zeros(nv + 1, dtype=np.int64)
+    np.add.at(indptr, cols + 1, 1)
+    indptr = np.cumsum(indptr)
+    return indptr.astype(np.int32), rows
+
+
+def sparse_scatter_add(indptr, indices, data, sl_rows, sl_cols, T, w=None):
+    """data[(sl_rows[i], sl_cols[j])] += T[i, j] * w[i], skipping absent entries (csrc/ha_sparse.c:128-142)."""
+    for j, col in enumerate(sl_cols):
+        a, b = int(indptr[col]), int(indptr[col + 1])
+        rows = indices[a:b]
+        pos = np.searchsorted(rows, sl_rows)
+        ok = (pos < rows.size)
+        ok[ok] = rows[pos[ok]] == np.asarray(sl_rows)[ok]
+        vals = T[:, j] * (w if w is not None else 1.0)
+        np.add.at(data, a + pos[ok], vals[ok])
+    return data
+
+
+def searchlight_procrustes_csc(X, Y, idx, off, indptr, indices, data, weights=None, reflection=True,
+                               scaling=False, transforms=None):
+    """Sparse-API searchlight Procrustes, csrc/ha_searchlight.c:147-201 (cpu64 arm), sls_Y = sls_X."""
+    for s in range(len(off) - 1):
+        sl = idx[off[s]:off[s + 1]]
+        T = transforms[s] if transforms is not None else procrustes(X[:, sl], Y[:, sl], reflection, scaling)
+        w = None if weights is None else weights[off[s]:off[s + 1]]
+        sparse_scatter_add(indptr, indices, data, sl, sl, T, w)
+    return data
+
+
+# ---------------------------------------------------------------------------------------------
+# ridge (csrc/ha_ridge.c:13-54) and searchlight ridge (csrc/ha_searchlight.c:1378-1429)
+# ---------------------------------------------------------------------------------------------
+
+def ridge(X, Y, alpha):
+    """betas = V diag(s / (alpha + s^2)) U^T Y with the thin SVD X = U diag(s) V^T."""
+    U, s, Vt = np.linalg.svd(X, full_matrices=False)
+    d = s / (alpha + s * s)
+    return Vt.T @ (d[:, np.newaxis] * (U.T @ Y))
+
+
+def searchlight_ridge_csc(X, Y, idx, off, indptr, indices, data, alpha, weights=None):
+    for s in range(len(off) - 1):
+        sl = idx[off[s]:off[s + 1]]
+        T = ridge(X[:, sl], Y[:, sl], alpha)
+        w = None if weights is None else weights[off[s]:off[s + 1]]
+        sparse_scatter_add(indptr, indices, data, sl, sl, T, w)
+    return data
+
+
+# ---------------------------------------------------------------------------------------------
+# z-score (csrc/ha_linalg.c:263-291)
+# ---------------------------------------------------------------------------------------------
+
+def zscore_columns(X):
+    """One-pass population z-score, var < 1e-30 -> 0 (csrc/ha_linalg.c:263-291)."""
+    M = X.shape[0]
+    sums = X.sum(axis=0)
+    sum2 = (X * X).sum(axis=0)
+    mean = sums * (1.0 / M)
+    var = sum2 * (1.0 / M) - mean * mean
+    inv = np.where(var < 1e-30, 0.0, 1.0 / np.sqrt(np.where(var < 1e-30, 1.0, var)))
+    return (X - mean) * inv
+
+
+# ---------------------------------------------------------------------------------------------
+# dense <-> pattern helpers
+# ---------------------------------------------------------------------------------------------
+
+def dense_to_csc_values(T_dense, indptr, indices):
+    cols = np.repeat(np.arange(len(indptr) - 1), np.diff(indptr))
+    return T_dense[indices, cols]
+
+
+def dense_to_csr_values(T_dense, indptr, indices):
+    rows = np.repeat(np.arange(len(indptr) - 1), np.diff(indptr))
+    return T_dense[rows, indices]

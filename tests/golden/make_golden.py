@@ -1,0 +1,149 @@
+"""Generate the golden fixtures in tests/golden/ from the reference itself.
+
+Run in a container that has the reference checkout and its compiled library
+(``make -C oracle``):
+
+    python tests/golden/make_golden.py
+
+Outputs (small, seeded inputs stored alongside the outputs so the fixtures are
+self-contained):
+  small_dense.npz   searchlight Procrustes through the reference dense entry point
+                    (ha_searchlight_procrustes_dense, cpu64 and cpu32), with and without
+                    reflection / scaling
+  small_sparse.npz  ha_sparse_init pattern, ha_searchlight_weights, sparse-API Procrustes
+                    and ridge (ha_searchlight_procrustes, ha_searchlight_ridge) CSC data
+  kat.npz           outputs of ha_procrustes / ha_ridge on the reference harness's
+                    known-answer inputs (csrc/ha_test.c:234-366, splitmix64 data)
+  python_ref.npz    the Python reference package (src/hyperalignment) on the same small
+                    case: procrustes per searchlight and initialize_sparse_matrix
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from hyperalignment_b200 import workloads as W  # noqa: E402
+from oracle import ha_oracle as O  # noqa: E402
+from oracle import ref_lib as R  # noqa: E402
+
+REF_DIR = os.environ.get("HA_REFERENCE_DIR", "/root/reference")
+
+
+def small_inputs(seed=0):
+    w = W.small_case(seed=seed)
+    return w
+
+
+def make_small_dense():
+    w = small_inputs(0)
+    s = w.sls
+    out = dict(X=w.X, Y=w.Y, idx=s.indices, off=s.offsets, dists=s.dists, radius=np.float64(s.radius))
+    R.set_threads(1)
+    out["T_cpu64"] = R.procrustes_dense(w.X, w.Y, s.indices, s.offsets, s.dists, s.radius, True, False, 0)
+    out["T_cpu32"] = R.procrustes_dense(w.X, w.Y, s.indices, s.offsets, s.dists, s.radius, True, False, 1)
+    out["T_cpu64_noref_scal"] = R.procrustes_dense(w.X, w.Y, s.indices, s.offsets, s.dists, s.radius, False, True, 0)
+    out["T_cpu64_uniform"] = R.procrustes_dense(w.X, w.Y, s.indices, s.offsets, None, 0.0, True, False, 0)
+    np.savez_compressed(os.path.join(HERE, "small_dense.npz"), **out)
+
+
+def make_small_sparse():
+    w = small_inputs(1)
+    s = w.sls
+    indptr, indices = R.sparse_init(s.indices, s.offsets, w.nv)
+    weights = R.searchlight_weights(s.indices, s.offsets, s.dists, s.radius)
+    R.set_threads(1)
+    data = R.searchlight_procrustes_csc(w.X, w.Y, s.indices, s.offsets, indptr, indices, weights, True, False, 0)
+    data_unw = R.searchlight_procrustes_csc(w.X, w.Y, s.indices, s.offsets, indptr, indices, None, True, True, 0)
+    data_ridge = R.searchlight_ridge_csc(w.X, w.Y, s.indices, s.offsets, indptr, indices, 1.0, weights)
+    toy_idx = np.array([0, 1, 2, 1, 2, 3, 4], dtype=np.int32)  # csrc/ha_test.c:369-402
+    toy_off = np.array([0, 3, 7], dtype=np.int32)
+    toy_ptr, toy_ind = R.sparse_init(toy_idx, toy_off, 5)
+    np.savez_compressed(os.path.join(HERE, "small_sparse.npz"), X=w.X, Y=w.Y, idx=s.indices, off=s.offsets,
+                        dists=s.dists, radius=np.float64(s.radius), indptr=indptr, indices=indices,
+                        weights=weights, data=data, data_unweighted_scaled=data_unw, data_ridge=data_ridge,
+                        ridge_alpha=np.float64(1.0), toy_idx=toy_idx, toy_off=toy_off, toy_indptr=toy_ptr,
+                        toy_indices=toy_ind)
+
+
+def _ref_procrustes(X, Y, refl, scal):
+    h = R.lib()
+    Xc = np.ascontiguousarray(X)
+    Yc = np.ascontiguousarray(Y)
+    T = np.zeros((X.shape[1], X.shape[1]))
+    tx = R.TMat(R._dp(Xc), X.shape[0], X.shape[1])
+    ty = R.TMat(R._dp(Yc), Y.shape[0], Y.shape[1])
+    tt = R.TMat(R._dp(T), T.shape[0], T.shape[1])
+    assert h.ha_procrustes(ctypes.byref(tx), ctypes.byref(ty), ctypes.byref(tt), refl, scal) == 0
+    return T
+
+
+def _ref_ridge(X, Y, alpha):
+    h = R.lib()
+    Xc = np.ascontiguousarray(X)
+    Yc = np.ascontiguousarray(Y)
+    B = np.zeros((X.shape[1], Y.shape[1]))
+    tx = R.TMat(R._dp(Xc), X.shape[0], X.shape[1])
+    ty = R.TMat(R._dp(Yc), Y.shape[0], Y.shape[1])
+    tb = R.TMat(R._dp(B), B.shape[0], B.shape[1])
+    assert h.ha_ridge(ctypes.byref(tx), ctypes.byref(ty), float(alpha), ctypes.byref(tb)) == 0
+    return B
+
+
+def make_kat():
+    out = {}
+    X = O.SplitMix64(77).fill(50, 20)  # csrc/ha_test.c:234-256
+    out["identity_X"] = X
+    out["identity_T"] = _ref_procrustes(X, X, True, False)
+    X = O.SplitMix64(55).fill(50, 10)  # csrc/ha_test.c:258-299
+    Rm = np.eye(10)
+    a = 0.7
+    Rm[0, 0], Rm[0, 1], Rm[1, 0], Rm[1, 1] = np.cos(a), -np.sin(a), np.sin(a), np.cos(a)
+    Y = X @ Rm
+    out["rotation_X"], out["rotation_Y"] = X, Y
+    out["rotation_T"] = _ref_procrustes(X, Y, True, False)
+    g = O.SplitMix64(33)  # csrc/ha_test.c:301-334
+    X = g.fill(50, 10)
+    Y = g.fill(50, 10)
+    out["noref_X"], out["noref_Y"] = X, Y
+    out["noref_T"] = _ref_procrustes(X, Y, False, False)
+    out["noref_scal_T"] = _ref_procrustes(X, Y, False, True)
+    g = O.SplitMix64(101)  # csrc/ha_test.c:336-366
+    X = g.fill(50, 10)
+    B = g.fill(10, 5)
+    Y = X @ B
+    out["ridge_X"], out["ridge_Y"], out["ridge_B"] = X, Y, B
+    out["ridge_betas"] = _ref_ridge(X, Y, 1e-6)
+    np.savez_compressed(os.path.join(HERE, "kat.npz"), **out)
+
+
+def make_python_ref():
+    sys.path.insert(0, os.path.join(REF_DIR, "src"))
+    from hyperalignment.procrustes import procrustes as py_procrustes  # noqa: E402
+    from hyperalignment.sparse import initialize_sparse_matrix  # noqa: E402
+    w = small_inputs(0)
+    s = w.sls
+    sls, _ = s.as_lists()
+    Ts = [py_procrustes(w.X[:, sl], w.Y[:, sl], reflection=True, scaling=False) for sl in sls[:20]]
+    mat = initialize_sparse_matrix(sls, nv=w.nv)
+    np.savez_compressed(os.path.join(HERE, "python_ref.npz"), T_first20=np.concatenate([t.ravel() for t in Ts]),
+                        indptr=mat.indptr.astype(np.int32), indices=mat.indices.astype(np.int32))
+
+
+if __name__ == "__main__":
+    if not R.available():
+        raise SystemExit("build the reference first: make -C oracle")
+    make_small_dense()
+    make_small_sparse()
+    make_kat()
+    make_python_ref()
+    for f in sorted(os.listdir(HERE)):
+        if f.endswith(".npz"):
+            print(f, os.path.getsize(os.path.join(HERE, f)))

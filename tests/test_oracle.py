@@ -1,0 +1,160 @@
+"""Pins the CPU oracle (oracle/ha_oracle.py) to the reference.
+
+Known-answer tests restate csrc/ha_test.c (same splitmix64 / Box-Muller inputs);
+golden comparisons use outputs of the compiled reference and of the Python
+reference package stored in tests/golden/ (made by tests/golden/make_golden.py).
+"""
+
+import numpy as np
+import pytest
+
+from conftest import golden
+from oracle import ha_oracle as O
+
+
+def test_kat_procrustes_identity():
+    # csrc/ha_test.c:234-256: |T| ~ I within 1e-8
+    g = golden("kat.npz")
+    X = O.SplitMix64(77).fill(50, 20)
+    np.testing.assert_array_equal(X, g["identity_X"])
+    T = O.procrustes(X, X, True, False)
+    np.testing.assert_allclose(np.abs(T), np.eye(20), atol=1e-8)
+    np.testing.assert_allclose(T, g["identity_T"], atol=1e-10)
+
+
+def test_kat_procrustes_known_rotation():
+    # csrc/ha_test.c:258-299: ||X T - Y||_inf < 1e-8
+    g = golden("kat.npz")
+    X = O.SplitMix64(55).fill(50, 10)
+    np.testing.assert_array_equal(X, g["rotation_X"])
+    T = O.procrustes(X, g["rotation_Y"], True, False)
+    assert np.abs(X @ T - g["rotation_Y"]).max() < 1e-8
+    np.testing.assert_allclose(T, g["rotation_T"], atol=1e-10)
+
+
+def test_kat_procrustes_no_reflection():
+    # csrc/ha_test.c:301-334: det(T) > 0
+    g = golden("kat.npz")
+    T = O.procrustes(g["noref_X"], g["noref_Y"], False, False)
+    assert np.linalg.det(T) > 0
+    np.testing.assert_allclose(T, g["noref_T"], atol=1e-10)
+    Ts = O.procrustes(g["noref_X"], g["noref_Y"], False, True)
+    np.testing.assert_allclose(Ts, g["noref_scal_T"], atol=1e-10)
+
+
+def test_kat_ridge_small_alpha():
+    # csrc/ha_test.c:336-366: betas recovered within 1e-6
+    g = golden("kat.npz")
+    B = O.ridge(g["ridge_X"], g["ridge_Y"], 1e-6)
+    assert np.abs(B - g["ridge_B"]).max() < 1e-6
+    np.testing.assert_allclose(B, g["ridge_betas"], atol=1e-10)
+
+
+def test_kat_sparse_init_toy():
+    # csrc/ha_test.c:369-402: two overlapping searchlights on 5 vertices -> nnz 21
+    g = golden("small_sparse.npz")
+    indptr, indices = O.sparse_init(g["toy_idx"], g["toy_off"], 5)
+    assert indices.size == 21
+    np.testing.assert_array_equal(indptr, g["toy_indptr"])
+    np.testing.assert_array_equal(indices, g["toy_indices"])
+
+
+def test_kat_sparse_scatter_identity():
+    # csrc/ha_test.c:404-435
+    sl = np.array([0, 1, 2], dtype=np.int32)
+    indptr, indices = O.sparse_init(sl, np.array([0, 3], dtype=np.int32), 3)
+    data = np.zeros(indices.size)
+    O.sparse_scatter_add(indptr, indices, data, sl, sl, np.eye(3))
+    cols = np.repeat(np.arange(3), np.diff(indptr))
+    np.testing.assert_array_equal(data, (indices == cols).astype(float))
+
+
+def test_kat_weights_sum_to_one():
+    # csrc/ha_test.c:439-470 (uniform weights)
+    idx = np.array([0, 1, 2, 1, 2, 3, 4, 3, 4, 5], dtype=np.int32)
+    off = np.array([0, 3, 7, 10], dtype=np.int32)
+    w = O.searchlight_weights(idx, off, None, 0.0, 6)
+    sums = np.zeros(6)
+    np.add.at(sums, idx, w)
+    np.testing.assert_allclose(sums, 1.0, atol=1e-12)
+
+
+def test_kat_zscore():
+    # csrc/ha_test.c:474-500
+    X = O.zscore_columns(O.SplitMix64(200).fill(100, 10))
+    np.testing.assert_allclose(X.mean(axis=0), 0.0, atol=1e-12)
+    np.testing.assert_allclose((X * X).mean(axis=0) - X.mean(axis=0) ** 2, 1.0, atol=1e-10)
+
+
+def test_weights_bit_exact_vs_reference():
+    g = golden("small_sparse.npz")
+    w = O.searchlight_weights(g["idx"], g["off"], g["dists"], float(g["radius"]), g["X"].shape[1])
+    np.testing.assert_array_equal(w, g["weights"])
+
+
+def test_sparse_pattern_bit_exact_vs_reference():
+    g = golden("small_sparse.npz")
+    indptr, indices = O.sparse_init(g["idx"], g["off"], g["X"].shape[1])
+    np.testing.assert_array_equal(indptr, g["indptr"])
+    np.testing.assert_array_equal(indices, g["indices"])
+
+
+def test_sparse_pattern_matches_python_reference():
+    g = golden("python_ref.npz")
+    d = golden("small_dense.npz")
+    indptr, indices = O.sparse_init(d["idx"], d["off"], d["X"].shape[1])
+    np.testing.assert_array_equal(indptr, g["indptr"])
+    np.testing.assert_array_equal(indices, g["indices"])
+
+
+def test_procrustes_matches_python_reference():
+    g = golden("python_ref.npz")
+    d = golden("small_dense.npz")
+    Ts = O.local_transforms(d["X"], d["Y"], d["idx"], d["off"][:21])
+    np.testing.assert_allclose(np.concatenate([t.ravel() for t in Ts]), g["T_first20"], atol=1e-10)
+
+
+@pytest.mark.parametrize("key,refl,scal,weighted", [
+    ("T_cpu64", True, False, True),
+    ("T_cpu64_noref_scal", False, True, True),
+    ("T_cpu64_uniform", True, False, False),
+])
+def test_dense_matches_reference(key, refl, scal, weighted):
+    g = golden("small_dense.npz")
+    dists = g["dists"] if weighted else None
+    T = O.searchlight_procrustes_dense(g["X"], g["Y"], g["idx"], g["off"], dists, float(g["radius"]), refl, scal)
+    np.testing.assert_allclose(T, g[key], atol=1e-10, rtol=0)
+
+
+def test_dense_cpu32_close_to_cpu64():
+    # the reference's own FP32 arm sits within ~1e-6 of FP64 on this case
+    g = golden("small_dense.npz")
+    a, b = g["T_cpu64"], g["T_cpu32"]
+    assert np.linalg.norm(a - b) / np.linalg.norm(a) < 1e-5
+
+
+def test_sparse_procrustes_and_ridge_match_reference():
+    g = golden("small_sparse.npz")
+    X, Y, idx, off = g["X"], g["Y"], g["idx"], g["off"]
+    d = O.searchlight_procrustes_csc(X, Y, idx, off, g["indptr"], g["indices"], np.zeros(g["indices"].size),
+                                     g["weights"], True, False)
+    np.testing.assert_allclose(d, g["data"], atol=1e-10, rtol=0)
+    d = O.searchlight_procrustes_csc(X, Y, idx, off, g["indptr"], g["indices"], np.zeros(g["indices"].size),
+                                     None, True, True)
+    np.testing.assert_allclose(d, g["data_unweighted_scaled"], atol=1e-10, rtol=0)
+    d = O.searchlight_ridge_csc(X, Y, idx, off, g["indptr"], g["indices"], np.zeros(g["indices"].size),
+                                float(g["ridge_alpha"]), g["weights"])
+    np.testing.assert_allclose(d, g["data_ridge"], atol=1e-10, rtol=0)
+
+
+def test_oracle_vs_live_reference():
+    """When the compiled reference is present (oracle/_ref), compare on a fresh seed."""
+    from oracle import ref_lib as R
+    if not R.available():
+        pytest.skip("compiled reference not built (make -C oracle)")
+    from hyperalignment_b200 import workloads as W
+    w = W.small_case(seed=7, reflection=False, scaling=True)
+    s = w.sls
+    a = O.searchlight_procrustes_dense(w.X, w.Y, s.indices, s.offsets, s.dists, s.radius, False, True)
+    b = R.procrustes_dense(w.X, w.Y, s.indices, s.offsets, s.dists, s.radius, False, True, 0, threads=1)
+    np.testing.assert_allclose(a, b, atol=1e-10, rtol=0)

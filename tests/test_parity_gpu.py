@@ -1,0 +1,244 @@
+"""GPU parity: the CUDA path through the C ABI against the reference (golden vectors)
+and the CPU oracle.
+
+Tolerances (written per test):
+  * per-searchlight transform T_s vs float64 oracle: relative Frobenius <= 1e-4
+  * dense / CSC results vs the reference float64 and float32 CPU backends:
+    relative Frobenius <= 1e-5, max-abs <= 1e-5
+  * integer work (CSC pattern): bit-exact
+  * repeated runs: bitwise identical (deterministic reduction)
+"""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import golden
+from hyperalignment_b200 import _lib as L
+from hyperalignment_b200 import hyperalignment_c as H
+from hyperalignment_b200 import workloads as W
+from hyperalignment_b200.plan import Plan
+from oracle import ha_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+T_REL = 1e-4     # per-T relative Frobenius vs float64
+GLOBAL_REL = 1e-5
+
+
+def relf(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def sls_lists(idx, off):
+    return [idx[off[s]:off[s + 1]] for s in range(off.size - 1)]
+
+
+def dense_b200(X, Y, idx, off, dists, radius, refl=True, scal=False, T_out=None):
+    sls = sls_lists(idx, off)
+    ds = None if dists is None else sls_lists(dists, off)
+    return H.searchlight_procrustes(X, Y, sls, ds, radius, backend="b200", reflection=refl, scaling=scal,
+                                    T_out=T_out)
+
+
+@pytest.mark.parametrize("key,refl,scal,weighted", [
+    ("T_cpu64", True, False, True),
+    ("T_cpu64_noref_scal", False, True, True),
+    ("T_cpu64_uniform", True, False, False),
+])
+def test_dense_matches_reference_golden(gpu, key, refl, scal, weighted):
+    g = golden("small_dense.npz")
+    T = dense_b200(g["X"], g["Y"], g["idx"], g["off"], g["dists"] if weighted else None, float(g["radius"]),
+                   refl, scal)
+    assert relf(T, g[key]) <= GLOBAL_REL
+    assert np.abs(T - g[key]).max() <= GLOBAL_REL
+    if key == "T_cpu64":
+        assert relf(T, g["T_cpu32"]) <= GLOBAL_REL
+    # the pattern outside the union of searchlight blocks stays exactly zero
+    np.testing.assert_array_equal(T[g[key] == 0], 0.0)
+
+
+def test_dense_accumulates_into_T_out(gpu):
+    g = golden("small_dense.npz")
+    nv = g["X"].shape[1]
+    base = np.full((nv, nv), 0.25)
+    T = dense_b200(g["X"], g["Y"], g["idx"], g["off"], g["dists"], float(g["radius"]), T_out=base.copy())
+    assert np.abs(T - (0.25 + g["T_cpu64"])).max() <= GLOBAL_REL
+
+
+def test_dense_row_major_input(gpu, hlib):
+    g = golden("small_dense.npz")
+    X, Y = np.ascontiguousarray(g["X"]), np.ascontiguousarray(g["Y"])
+    nt, nv = X.shape
+    T = np.zeros((nv, nv))
+    rc = hlib.ha_searchlight_procrustes_dense(L.dptr(X), L.dptr(Y), nt, nv, L.iptr(g["idx"]), L.iptr(g["off"]),
+                                              L.dptr(g["dists"]), g["off"].size - 1, float(g["radius"]), L.dptr(T),
+                                              True, False, L.BACKEND_B200, False)
+    assert rc == 0
+    assert relf(T, g["T_cpu64"]) <= GLOBAL_REL
+
+
+def test_dense_is_deterministic(gpu):
+    w = W.small_case(seed=3, nv=642, nt=60, lo=20, hi=60)
+    s = w.sls
+    a = dense_b200(w.X, w.Y, s.indices, s.offsets, s.dists, s.radius)
+    b = dense_b200(w.X, w.Y, s.indices, s.offsets, s.dists, s.radius)
+    assert a.tobytes() == b.tobytes()
+
+
+def test_csc_pattern_bit_exact(gpu):
+    g = golden("small_sparse.npz")
+    indptr, indices = H.sparse_pattern(sls_lists(g["idx"], g["off"]), g["X"].shape[1])
+    np.testing.assert_array_equal(indptr, g["indptr"])
+    np.testing.assert_array_equal(indices, g["indices"])
+    tp, ti = H.sparse_pattern(sls_lists(g["toy_idx"], g["toy_off"]), 5)
+    assert ti.size == 21
+    np.testing.assert_array_equal(tp, g["toy_indptr"])
+    np.testing.assert_array_equal(ti, g["toy_indices"])
+
+
+def test_csc_pattern_bit_exact_larger(gpu):
+    w = W.small_case(seed=5, nv=2562, nt=8, lo=40, hi=90)
+    s = w.sls
+    indptr, indices = H.sparse_pattern(sls_lists(s.indices, s.offsets), w.nv)
+    ri, rj = O.sparse_init(s.indices, s.offsets, w.nv)
+    np.testing.assert_array_equal(indptr, ri)
+    np.testing.assert_array_equal(indices, rj)
+
+
+def test_csc_procrustes_matches_reference_golden(gpu):
+    g = golden("small_sparse.npz")
+    sls = sls_lists(g["idx"], g["off"])
+    ws = sls_lists(g["weights"], g["off"])
+    data = np.zeros(g["indices"].size)
+    H.searchlight_procrustes_csc(g["X"], g["Y"], sls, g["indptr"], g["indices"], data, weights=ws)
+    assert relf(data, g["data"]) <= GLOBAL_REL
+    data = np.zeros(g["indices"].size)
+    H.searchlight_procrustes_csc(g["X"], g["Y"], sls, g["indptr"], g["indices"], data, weights=None, scaling=True)
+    assert relf(data, g["data_unweighted_scaled"]) <= GLOBAL_REL
+
+
+def _device_run(w, solver, refl=True, scal=False, out_kind=L.OUT_CSR):
+    import torch
+    plan = Plan.from_workload(w)
+    dX = torch.from_numpy(np.asfortranarray(w.X).ravel(order="F")).cuda()
+    dY = torch.from_numpy(np.asfortranarray(w.Y).ravel(order="F")).cuda()
+    vals = torch.zeros(plan.nnz, dtype=torch.float64, device="cuda")
+    plan.procrustes_device(dX.data_ptr(), dY.data_ptr(), vals.data_ptr(), refl, scal, solver, out_kind)
+    torch.cuda.synchronize()
+    return plan, vals.cpu().numpy()
+
+
+@pytest.mark.parametrize("solver", [L.SOLVER_MIXED, L.SOLVER_FP32, L.SOLVER_FP64])
+@pytest.mark.parametrize("lo,hi", [(1, 12), (60, 90), (150, 240), (300, 420)])
+def test_local_transforms_vs_fp64(gpu, solver, lo, hi):
+    """Per-searchlight T_s against the float64 oracle, covering resident and blocked Jacobi sizes."""
+    nv = 642 if hi <= 240 else 1442
+    w = W.small_case(seed=11, nv=nv, nt=max(2 * hi, 40), lo=lo, hi=hi)
+    s = w.sls
+    count = min(s.count, 24)
+    w.sls = s.subset(np.arange(count))
+    plan, _ = _device_run(w, solver)
+    Ts = plan.local_transforms(0, count)
+    worst = 0.0
+    for q in range(count):
+        sl = w.sls.indices[w.sls.offsets[q]:w.sls.offsets[q + 1]]
+        Tref = O.procrustes(w.X[:, sl], w.Y[:, sl])
+        worst = max(worst, relf(Ts[q], Tref))
+    assert worst <= T_REL, worst
+
+
+@pytest.mark.parametrize("refl,scal", [(False, False), (False, True), (True, True)])
+def test_reflection_and_scaling_vs_oracle(gpu, refl, scal):
+    w = W.small_case(seed=21, nv=642, nt=120, lo=30, hi=80)
+    s = w.sls
+    T = dense_b200(w.X, w.Y, s.indices, s.offsets, s.dists, s.radius, refl, scal)
+    Tref = O.searchlight_procrustes_dense(w.X, w.Y, s.indices, s.offsets, s.dists, s.radius, refl, scal)
+    assert relf(T, Tref) <= GLOBAL_REL
+
+
+def test_csc_output_order_matches_csr(gpu):
+    w = W.small_case(seed=2, nv=642, nt=80, lo=20, hi=50)
+    plan, csr = _device_run(w, L.SOLVER_MIXED, out_kind=L.OUT_CSR)
+    _, csc = _device_run(w, L.SOLVER_MIXED, out_kind=L.OUT_CSC)
+    indptr, indices = plan.pattern()
+    s = w.sls
+    Tref = O.searchlight_procrustes_dense(w.X, w.Y, s.indices, s.offsets, s.dists, s.radius)
+    assert relf(csr, O.dense_to_csr_values(Tref, indptr, indices)) <= GLOBAL_REL
+    assert relf(csc, O.dense_to_csc_values(Tref, indptr, indices)) <= GLOBAL_REL
+
+
+def test_rank_deficient_searchlights(gpu):
+    """Duplicated vertex columns make A singular: T is not unique, X @ T is (judged on X @ T)."""
+    w = W.small_case(seed=9, nv=642, nt=100, lo=30, hi=60, scaling=True)
+    rng = np.random.default_rng(1)
+    mask = W.duplicate_columns(w.X, w.sls, 0.5, rng)
+    assert mask.sum() > 0
+    plan, _ = _device_run(w, L.SOLVER_MIXED, scal=False)
+    count = w.sls.count
+    Ts = plan.local_transforms(0, count)
+    worst = 0.0
+    for q in np.flatnonzero(mask)[:40]:
+        sl = w.sls.indices[w.sls.offsets[q]:w.sls.offsets[q + 1]]
+        Xs = w.X[:, sl]
+        Tref = O.procrustes(Xs, w.Y[:, sl])
+        worst = max(worst, relf(Xs @ Ts[q], Xs @ Tref))
+        # T stays orthogonal (completed null space)
+        assert np.abs(Ts[q].T @ Ts[q] - np.eye(sl.size)).max() < 1e-4
+    assert worst <= T_REL, worst
+    assert plan.stats()["n_fp64"] >= 1
+
+
+def test_zero_column_completion(gpu):
+    w = W.small_case(seed=4, nv=162, nt=40, lo=8, hi=20)
+    w.X[:, 5] = 0.0
+    w.Y[:, 7] = 0.0
+    plan, _ = _device_run(w, L.SOLVER_MIXED)
+    Ts = plan.local_transforms(0, w.sls.count)
+    for q in range(w.sls.count):
+        n = Ts[q].shape[0]
+        assert np.abs(Ts[q].T @ Ts[q] - np.eye(n)).max() < 1e-4
+        sl = w.sls.indices[w.sls.offsets[q]:w.sls.offsets[q + 1]]
+        Xs = w.X[:, sl]
+        assert relf(Xs @ Ts[q], Xs @ O.procrustes(Xs, w.Y[:, sl])) <= T_REL
+
+
+def test_single_and_tiny_searchlights(gpu):
+    rng = np.random.default_rng(0)
+    nt, nv = 16, 5
+    X = rng.standard_normal((nt, nv))
+    Y = rng.standard_normal((nt, nv))
+    idx = np.array([2, 0, 1, 3, 4, 4], dtype=np.int32)
+    off = np.array([0, 1, 3, 5, 6], dtype=np.int32)
+    T = dense_b200(X, Y, idx, off, None, 0.0)
+    Tref = O.searchlight_procrustes_dense(X, Y, idx, off, None, 0.0)
+    assert np.abs(T - Tref).max() <= 1e-6
+
+
+def test_full_size_template_pair_properties(gpu):
+    """10242 vertices, nt = 400, searchlights of 100-300 (the template workload): sampled T_s
+    against float64 and two dense rows rebuilt from the oracle."""
+    w = W.template_procrustes_pair(seed=0)
+    import torch
+    plan = Plan.from_workload(w)
+    dX = torch.from_numpy(np.asfortranarray(w.X).ravel(order="F")).cuda()
+    dY = torch.from_numpy(np.asfortranarray(w.Y).ravel(order="F")).cuda()
+    vals = torch.zeros(plan.nnz, dtype=torch.float64, device="cuda")
+    plan.procrustes_device(dX.data_ptr(), dY.data_ptr(), vals.data_ptr(), True, True, L.SOLVER_MIXED, L.OUT_CSR)
+    torch.cuda.synchronize()
+    vals = vals.cpu().numpy()
+    indptr, indices = plan.pattern()
+    s = w.sls
+    wts = O.searchlight_weights(s.indices, s.offsets, s.dists, s.radius, w.nv)
+    for r in (17, 5000):
+        members = [q for q in range(s.count) if r in set(s.indices[s.offsets[q]:s.offsets[q + 1]].tolist())]
+        row = np.zeros(w.nv)
+        for q in members:
+            sl = s.indices[s.offsets[q]:s.offsets[q + 1]]
+            a = int(np.flatnonzero(sl == r)[0])
+            T = O.procrustes(w.X[:, sl], w.Y[:, sl], True, True)
+            row[sl] += wts[s.offsets[q] + a] * T[a]
+        got = np.zeros(w.nv)
+        got[indices[indptr[r]:indptr[r + 1]]] = vals[indptr[r]:indptr[r + 1]]
+        assert relf(got, row) <= GLOBAL_REL * 10
