@@ -52,6 +52,9 @@ SIGNATURES = {
     "ha_b200_plan_device_pattern": (ctypes.c_int, [
         ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p)]),
     "ha_b200_plan_stats": (ctypes.c_int, [ctypes.c_void_p, c_int32_p, c_int32_p]),
+    "ha_b200_plan_sweep_stats": (ctypes.c_int, [ctypes.c_void_p, c_int64_p, c_int32_p]),
+    "ha_b200_plan_searchlight_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, c_double_p,
+                                                      c_double_p, c_int32_p, c_int32_p]),
     "ha_b200_plan_procrustes_device": (ctypes.c_int, [
         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_bool, ctypes.c_bool, ctypes.c_int,
         ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]),

@@ -110,12 +110,28 @@ struct HostCallBufs {
 
 size_t real_bytes(bool fp64) { return fp64 ? 8 : 4; }
 
-// Jacobi block layout for a searchlight of n vertices in a given precision.
+// Jacobi kernel instances: rows per lane (column length <= 32 * rpl)
+const int kRplSet[] = {1, 2, 3, 4, 5, 6, 8, 10, 12, 16};
+int rpl_for(int n) {
+	for (int r : kRplSet)
+		if (n <= 32 * r) return r;
+	return -1;
+}
+
+// Shared memory of k_jacobi for 2*b staged columns (plus the zero pair) of LD rows.
+size_t jacobi_smem(int b, int ld, size_t rb) {
+	const size_t mst = (size_t)2 * b + 2;
+	return (2 * mst * ld + mst + 2 + 2 * 16 * 65 + 8) * rb;
+}
+
+// Jacobi block layout for a searchlight of n vertices in a given precision: resident (two
+// blocks covering all columns stay in shared memory) when it fits, else blocked with the
+// widest block that fits.
 void jacobi_layout(int n, bool fp64, int &bsz, int &nblk, size_t &smem) {
 	const size_t rb = real_bytes(fp64);
-	const size_t extra = (size_t)(2 * 16 * 65 + 8) * rb;
+	const int ld = 32 * std::max(1, rpl_for(n));
 	int h = (n + 1) / 2;
-	size_t res = ((size_t)4 * h * n + 2 * h + 2) * rb + extra;
+	size_t res = jacobi_smem(h, ld, rb);
 	if (res <= kSmemMax) {
 		bsz = h;
 		nblk = 2;
@@ -123,19 +139,55 @@ void jacobi_layout(int n, bool fp64, int &bsz, int &nblk, size_t &smem) {
 		return;
 	}
 	int b = 32;
-	while (b > 1 && ((size_t)4 * b * n + 2 * b + 2) * rb + extra > kSmemMax) b--;
+	while (b > 1 && jacobi_smem(b, ld, rb) > kSmemMax) b--;
 	bsz = b;
 	nblk = (n + b - 1) / b;
 	if (nblk & 1) nblk++;
-	smem = ((size_t)4 * b * n + (size_t)nblk * b + 2) * rb + extra;
-	if (smem < ((size_t)4 * b * n + 2 * b + 2) * rb + extra) smem = ((size_t)4 * b * n + 2 * b + 2) * rb + extra;
+	smem = jacobi_smem(b, ld, rb);
 }
 
 struct Bucket {
 	int first, count;  // range in the chunk's work array
 	size_t smem;
 	bool blocked;
+	int threads;       // Jacobi block size: about two column pairs per warp per round
+	int rpl;           // rows per lane of the Jacobi kernel instance (n <= 32 * rpl)
 };
+
+template <typename Real>
+int launch_jacobi(int rpl, int grid, int threads, size_t smem, cudaStream_t st, const SlWork *wk, Real *A, Real *V,
+                  float *T, SlStats *stats, double *uv, JacobiParams jp) {
+	switch (rpl) {
+#define HA_RPL_CASE(R) \
+	case R: k_jacobi<Real, R><<<grid, threads, smem, st>>>(wk, A, V, T, stats, uv, jp); break;
+		HA_RPL_CASE(1) HA_RPL_CASE(2) HA_RPL_CASE(3) HA_RPL_CASE(4) HA_RPL_CASE(5)
+		HA_RPL_CASE(6) HA_RPL_CASE(8) HA_RPL_CASE(10) HA_RPL_CASE(12) HA_RPL_CASE(16)
+#undef HA_RPL_CASE
+	default:
+		fprintf(stderr, "ha_b200: no Jacobi kernel for %d rows per lane\n", rpl);
+		return kHaErrorArg;
+	}
+	return kHaSuccess;
+}
+
+template <typename Real>
+int set_jacobi_attrs() {
+	const int m = (int)kSmemMax;
+#define HA_RPL_ATTR(R) \
+	if (cudaFuncSetAttribute(k_jacobi<Real, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, m) != cudaSuccess) \
+		return kHaErrorInternal;
+	HA_RPL_ATTR(1) HA_RPL_ATTR(2) HA_RPL_ATTR(3) HA_RPL_ATTR(4) HA_RPL_ATTR(5)
+	HA_RPL_ATTR(6) HA_RPL_ATTR(8) HA_RPL_ATTR(10) HA_RPL_ATTR(12) HA_RPL_ATTR(16)
+#undef HA_RPL_ATTR
+	return kHaSuccess;
+}
+
+int jacobi_threads(int bsz, bool fp64) {
+	int warps = (bsz + 1) / 2;
+	(void)fp64;
+	warps = std::max(8, std::min(16, warps));
+	return warps * 32;
+}
 
 struct Chunk {
 	int s0, s1;
@@ -317,10 +369,7 @@ int build_chunks(HaB200Plan *P) {
 				uvo += 2 * (int64_t)n;
 				items.push_back(w);
 			}
-			auto key = [](const SlWork &w) {
-				int band = w.n <= 32 ? 0 : w.n <= 64 ? 1 : w.n <= 96 ? 2 : w.n <= 128 ? 3 : w.n <= 192 ? 4 : w.n <= 256 ? 5 : w.n <= 384 ? 6 : w.n <= 512 ? 7 : 8;
-				return (w.nblk == 2 ? 0 : 16) + band;
-			};
+			auto key = [](const SlWork &w) { return (w.nblk == 2 ? 0 : 32) + rpl_for(w.n); };
 			std::stable_sort(items.begin(), items.end(), [&](const SlWork &a, const SlWork &b) {
 				int ka = key(a), kb = key(b);
 				if (ka != kb) return ka < kb;
@@ -342,6 +391,8 @@ int build_chunks(HaB200Plan *P) {
 				b.count = j - i;
 				b.smem = smem;
 				b.blocked = items[i].nblk != 2;
+				b.threads = jacobi_threads(items[i].bsz, prec == 1);
+				b.rpl = rpl_for(items[i].n);
 				buckets.push_back(b);
 				i = j;
 			}
@@ -386,13 +437,17 @@ __global__ void k_count_flags(const SlStats *__restrict__ st, int n, int32_t *__
 	int f = st[q].flags;
 	if (f & kFlagFP64) atomicAdd(&counters[0], 1);
 	if (f & kFlagUnconverged) atomicAdd(&counters[1], 1);
+	atomicAdd(&counters[2], st[q].sweeps);
+	atomicMax(&counters[3], st[q].sweeps);
 }
 
 int set_smem_attrs() {
 	static bool done = false;
 	if (done) return kHaSuccess;
-	HA_CUDA(cudaFuncSetAttribute(k_jacobi<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax));
-	HA_CUDA(cudaFuncSetAttribute(k_jacobi<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax));
+	if (set_jacobi_attrs<float>() != kHaSuccess || set_jacobi_attrs<double>() != kHaSuccess) {
+		fprintf(stderr, "ha_b200: cudaFuncSetAttribute on the Jacobi kernels failed\n");
+		return kHaErrorInternal;
+	}
 	HA_CUDA(cudaFuncSetAttribute(k_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax));
 	HA_CUDA(cudaFuncSetAttribute(k_pattern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax));
 	done = true;
@@ -460,6 +515,12 @@ int plan_create_impl(int32_t nt, int32_t nv, const int32_t *sl_indices, const in
 	else if (!unweighted)
 		compute_weights(sl_indices, sl_offsets, sl_dists, count, radius, nv, P->h_w.data());
 	for (int s = 0; s < count; s++) P->max_n = std::max(P->max_n, sl_offsets[s + 1] - sl_offsets[s]);
+	if (rpl_for(P->max_n) < 0) {
+		fprintf(stderr, "ha_b200: searchlight of %d vertices exceeds the supported maximum of %d\n", P->max_n,
+		        32 * kRplSet[sizeof(kRplSet) / sizeof(kRplSet[0]) - 1]);
+		delete P;
+		return kHaErrorArg;
+	}
 	// per-vertex membership lists, sorted by searchlight (counting sort over flat order)
 	std::vector<int64_t> vptr((size_t)nv + 1, 0);
 	for (int64_t k = 0; k < P->total; k++) vptr[(size_t)sl_indices[k] + 1]++;
@@ -543,7 +604,11 @@ int run_procrustes(HaB200Plan *P, const double *d_X, const double *d_Y, bool ref
 			for (const Bucket &b : ch.b32) {
 				const SlWork *wk = ch.d_w32 + b.first;
 				{ HA_LAUNCH(kHaB200KXcov32, st); k_xcov<float, 32><<<b.count, kBlock, 0, st>>>(wk, P->idx.p, P->X32.p, P->Y32.p, ntp, nt, A, P->stats.p, 0); }
-				{ HA_LAUNCH(kHaB200KJacobi32, st); k_jacobi<float><<<b.count, kBlock, b.smem, st>>>(wk, A, V, T, P->stats.p, P->uv.p, jp); }
+				{
+					HA_LAUNCH(kHaB200KJacobi32, st);
+					if ((rc = launch_jacobi<float>(b.rpl, b.count, b.threads, b.smem, st, wk, A, V, T, P->stats.p, P->uv.p, jp)) != kHaSuccess)
+						return rc;
+				}
 				if (b.blocked) { HA_LAUNCH(kHaB200KFormT32, st); k_form_t_global<float><<<b.count, kBlock, 0, st>>>(wk, A, V, T, P->stats.p, rowmajor, 0); }
 			}
 		}
@@ -554,7 +619,11 @@ int run_procrustes(HaB200Plan *P, const double *d_X, const double *d_Y, bool ref
 			for (const Bucket &b : ch.b64) {
 				const SlWork *wk = ch.d_w64 + b.first;
 				{ HA_LAUNCH(kHaB200KXcov64, st); k_xcov<double, 16><<<b.count, kBlock, 0, st>>>(wk, P->idx.p, d_X, d_Y, nt, nt, A, P->stats.p, only); }
-				{ HA_LAUNCH(kHaB200KJacobi64, st); k_jacobi<double><<<b.count, kBlock, b.smem, st>>>(wk, A, V, T, P->stats.p, P->uv.p, jp); }
+				{
+					HA_LAUNCH(kHaB200KJacobi64, st);
+					if ((rc = launch_jacobi<double>(b.rpl, b.count, b.threads, b.smem, st, wk, A, V, T, P->stats.p, P->uv.p, jp)) != kHaSuccess)
+						return rc;
+				}
 				if (b.blocked) { HA_LAUNCH(kHaB200KFormT64, st); k_form_t_global<double><<<b.count, kBlock, 0, st>>>(wk, A, V, T, P->stats.p, rowmajor, only); }
 			}
 		}
@@ -899,6 +968,34 @@ int ha_b200_plan_stats(const HaB200Plan *P, int32_t *n_fp64, int32_t *n_unconver
 	HA_CUDA(cudaMemcpy(h, P->counters.p, sizeof(h), cudaMemcpyDeviceToHost));
 	if (n_fp64) *n_fp64 = h[0];
 	if (n_unconverged) *n_unconverged = h[1];
+	return kHaSuccess;
+}
+
+int ha_b200_plan_sweep_stats(const HaB200Plan *P, int64_t *sweeps_sum, int32_t *sweeps_max) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	if (!P) return kHaErrorArg;
+	int32_t h[4] = {0, 0, 0, 0};
+	HA_CUDA(cudaMemcpy(h, P->counters.p, sizeof(h), cudaMemcpyDeviceToHost));
+	if (sweeps_sum) *sweeps_sum = h[2];
+	if (sweeps_max) *sweeps_max = h[3];
+	return kHaSuccess;
+}
+
+int ha_b200_plan_searchlight_stats(const HaB200Plan *P, int32_t first, int32_t n, double *s_min, double *s_max,
+                                   int32_t *flags, int32_t *sweeps) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	if (!P || P->last_chunk < 0 || n <= 0) return kHaErrorArg;
+	const Chunk &ch = P->chunks[(size_t)P->last_chunk];
+	if (first < ch.s0 || first + n > ch.s1) return kHaErrorArg;
+	std::vector<SlStats> st((size_t)n);
+	HA_CUDA(cudaDeviceSynchronize());
+	HA_CUDA(cudaMemcpy(st.data(), P->stats.p + (first - ch.s0), (size_t)n * sizeof(SlStats), cudaMemcpyDeviceToHost));
+	for (int q = 0; q < n; q++) {
+		if (s_min) s_min[q] = st[q].s_min;
+		if (s_max) s_max[q] = st[q].s_max;
+		if (flags) flags[q] = st[q].flags;
+		if (sweeps) sweeps[q] = st[q].sweeps;
+	}
 	return kHaSuccess;
 }
 

@@ -65,6 +65,8 @@ struct SlStats {
 	double s_max;     // largest singular value
 	int32_t k_min;    // column of the smallest singular value
 	int32_t flags;    // bit 0: unconverged, bit 1: ill-conditioned (re-solved in FP64), bit 2: reflected
+	int32_t sweeps;   // Jacobi sweeps of the last solve
+	int32_t pad;
 };
 
 enum : int32_t { kFlagUnconverged = 1, kFlagIllCond = 2, kFlagReflected = 4, kFlagFP64 = 8 };
@@ -203,8 +205,14 @@ __global__ void __launch_bounds__(256) k_xcov(const SlWork *__restrict__ work, c
 // ---------------------------------------------------------------------------------------------
 // A V = B with orthogonal columns; sigma_c = ||B[:, c]||, U = B diag(1/sigma), T = U V^T
 // (the polar factor of A, csrc/ha_searchlight.c:593-609).  Parallel ordering: the
-// circle-method round robin over m columns (m - 1 rounds of m/2 disjoint pairs);
-// warps take pairs in turn, lanes stride over rows.
+// circle-method round robin over m columns (m - 1 rounds of m/2 disjoint pairs).
+// Squared column norms are cached in shared memory (recomputed exactly at the start of
+// every sweep or staging, updated by alpha' = alpha - t gamma, beta' = beta + t gamma after a
+// rotation), so a pair needs one dot product; each warp takes up to JP pairs of a round at
+// once so their reductions overlap.  A pair is rotated when |cos| > tol_rot; a sweep whose
+// largest |cos| is <= tol_conv ends the iteration.  Columns whose norm is below zero_thr
+// (numerically zero, e.g. rank-deficient A) are not rotated; they are completed to an
+// orthonormal basis at the end.
 //
 // Resident mode (nblk == 2): A and V live in shared memory for every sweep.
 // Blocked mode (nblk > 2): A and V stay in the global scratch (L2 resident); a sweep runs
@@ -213,82 +221,196 @@ __global__ void __launch_bounds__(256) k_xcov(const SlWork *__restrict__ work, c
 // over its 2*bsz columns (covering the pairs inside each block once), in later block rounds
 // only the cross pairs, so one sweep visits every column pair exactly once.
 
-// circle method: pair k of round r among m players (m even)
+// Pairs processed together by one warp (their reductions overlap), by rows per lane.
+template <int RPL>
+struct PairsPerWarp {
+	static constexpr int value = RPL <= 2 ? 4 : (RPL <= 5 ? 2 : 1);
+};
+
+// circle method: pair k of round r among m players (m even); no integer division
 __device__ __forceinline__ void rr_pair(int m, int r, int k, int &p, int &q) {
 	if (k == 0) {
 		p = m - 1;
 		q = r;
 	} else {
-		int mm = m - 1;
-		p = (r + k) % mm;
-		q = (r - k + mm) % mm;
+		const int mm = m - 1;
+		p = r + k;
+		if (p >= mm) p -= mm;
+		q = r - k;
+		if (q < 0) q += mm;
 	}
 }
 
-// Rotate the pair (p, q) of columns of length n stored at B + c*ldb (and V + c*ldv).
-// Returns true (on every lane) if a rotation was applied.
 template <typename Real>
-__device__ __forceinline__ bool jacobi_pair(Real *B, Real *V, int ldb, int n, int p, int q, Real tol, int lane) {
-	Real *bp = B + (int64_t)p * ldb, *bq = B + (int64_t)q * ldb;
-	Real al = 0, be = 0, ga = 0;
-	for (int i = lane; i < n; i += 32) {
-		Real x = bp[i], y = bq[i];
-		al += x * x;
-		be += y * y;
-		ga += x * y;
+struct JacobiTol {
+	Real rot;    // rotate when |cos| > rot
+	Real zero2;  // squared norm at or below which a column counts as zero
+};
+
+// Rotate JPW pairs (p[k], q[k]) of columns stored at B + c*LD (and V + c*LD) in shared memory,
+// LD = 32*RPL rows with rows >= n zero, so every lane handles exactly RPL rows and no row test
+// is needed.  Unused pair slots point at two zero columns and are skipped like any zero column.
+// nrm[] holds the cached squared norms.  The columns of B stay in registers between the dot
+// products and the rotation; lane k computes the rotation of pair k and broadcasts it.
+// Returns the largest |cos| seen.
+template <typename Real, int RPL>
+__device__ __forceinline__ Real jacobi_pairs(Real *B, Real *V, Real *nrm, const int *p, const int *q,
+                                             const JacobiTol<Real> &tol, int lane, bool &rotated) {
+	constexpr int JPW = PairsPerWarp<RPL>::value;
+	constexpr int LD = 32 * RPL;
+	Real x[JPW][RPL], y[JPW][RPL], g[JPW];
+#pragma unroll
+	for (int k = 0; k < JPW; k++) {
+		g[k] = 0;
+		const Real *bp = B + p[k] * LD + lane;
+		const Real *bq = B + q[k] * LD + lane;
+#pragma unroll
+		for (int r = 0; r < RPL; r++) {
+			x[k][r] = bp[32 * r];
+			y[k][r] = bq[32 * r];
+			g[k] += x[k][r] * y[k][r];
+		}
 	}
-	al = warp_sum(al);
-	be = warp_sum(be);
-	ga = warp_sum(ga);
-	if (!(al > 0 && be > 0)) return false;
-	if (!(real_abs(ga) > tol * real_sqrt(al) * real_sqrt(be))) return false;
-	Real zeta = (be - al) / (2 * ga);
-	Real t = ((zeta >= 0) ? Real(1) : Real(-1)) / (real_abs(zeta) + real_sqrt(Real(1) + zeta * zeta));
-	Real c = Real(1) / real_sqrt(Real(1) + t * t);
-	Real s = c * t;
-	for (int i = lane; i < n; i += 32) {
-		Real x = bp[i], y = bq[i];
-		bp[i] = c * x - s * y;
-		bq[i] = s * x + c * y;
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+		for (int k = 0; k < JPW; k++) g[k] += __shfl_xor_sync(0xffffffffu, g[k], o);
+	// lane k (< JPW) evaluates pair k
+	Real mycos = 0, myc = 1, mys = 0;
+	int mydo = 0;
+	if (lane < JPW) {
+		int pk = p[0], qk = q[0];
+		Real gk = g[0];
+#pragma unroll
+		for (int k = 1; k < JPW; k++)
+			if (lane == k) { pk = p[k]; qk = q[k]; gk = g[k]; }
+		const Real al = nrm[pk], be = nrm[qk];
+		if (al > tol.zero2 && be > tol.zero2) {
+			mycos = real_abs(gk) / (real_sqrt(al) * real_sqrt(be));
+			if (mycos > tol.rot) {
+				const Real zeta = (be - al) / (2 * gk);
+				const Real t = ((zeta >= 0) ? Real(1) : Real(-1)) / (real_abs(zeta) + real_sqrt(Real(1) + zeta * zeta));
+				myc = Real(1) / real_sqrt(Real(1) + t * t);
+				mys = myc * t;
+				mydo = 1;
+				nrm[pk] = al - t * gk;
+				nrm[qk] = be + t * gk;
+			}
+		}
 	}
-	Real *vp = V + (int64_t)p * ldb, *vq = V + (int64_t)q * ldb;
-	for (int i = lane; i < n; i += 32) {
-		Real x = vp[i], y = vq[i];
-		vp[i] = c * x - s * y;
-		vq[i] = s * x + c * y;
+#pragma unroll
+	for (int k = 0; k < JPW; k++) {
+		if (!__shfl_sync(0xffffffffu, mydo, k)) continue;
+		const Real c = __shfl_sync(0xffffffffu, myc, k);
+		const Real s = __shfl_sync(0xffffffffu, mys, k);
+		Real *bp = B + p[k] * LD + lane, *bq = B + q[k] * LD + lane;
+		Real *vp = V + p[k] * LD + lane, *vq = V + q[k] * LD + lane;
+#pragma unroll
+		for (int r = 0; r < RPL; r++) {
+			bp[32 * r] = c * x[k][r] - s * y[k][r];
+			bq[32 * r] = s * x[k][r] + c * y[k][r];
+			const Real u = vp[32 * r], w = vq[32 * r];
+			vp[32 * r] = c * u - s * w;
+			vq[32 * r] = s * u + c * w;
+		}
+		rotated = true;
 	}
-	return true;
+	__syncwarp();
+	return mycos;
 }
 
-// Full round robin (m - 1 rounds) over m columns in B/V (shared or global).
-template <typename Real>
-__device__ bool jacobi_full_rr(Real *B, Real *V, int ld, int n, int m, Real tol) {
+// exact squared norms of columns [0, m) (stride LD) into nrm[]
+template <typename Real, int RPL>
+__device__ __forceinline__ void column_norms(const Real *B, Real *nrm, int m) {
+	constexpr int LD = 32 * RPL;
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-	bool rotated = false;
+	for (int c = warp; c < m; c += nwarp) {
+		const Real *bc = B + c * LD + lane;
+		Real ss = 0;
+#pragma unroll
+		for (int r = 0; r < RPL; r++) ss += bc[32 * r] * bc[32 * r];
+		ss = warp_sum(ss);
+		if (lane == 0) nrm[c] = ss;
+	}
+	__syncthreads();
+}
+
+// Full round robin (m - 1 rounds) over m columns; columns m and m+1 are the zero pair used to
+// pad a warp's last group.  Returns this thread's max |cos|.
+template <typename Real, int RPL>
+__device__ __forceinline__ Real jacobi_full_rr(Real *B, Real *V, Real *nrm, int m, const JacobiTol<Real> &tol,
+                                               bool &rotated) {
+	constexpr int JPW = PairsPerWarp<RPL>::value;
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+	Real mc = 0;
+	const int npairs = m / 2;
 	for (int r = 0; r < m - 1; r++) {
-		for (int k = warp; k < m / 2; k += nwarp) {
-			int p, q;
-			rr_pair(m, r, k, p, q);
-			rotated |= jacobi_pair(B, V, ld, n, p, q, tol, lane);
+		for (int k0 = warp * JPW; k0 < npairs; k0 += nwarp * JPW) {
+			int p[JPW], q[JPW];
+#pragma unroll
+			for (int k = 0; k < JPW; k++) {
+				if (k0 + k < npairs) {
+					rr_pair(m, r, k0 + k, p[k], q[k]);
+				} else {
+					p[k] = m;
+					q[k] = m + 1;
+				}
+			}
+			Real c = jacobi_pairs<Real, RPL>(B, V, nrm, p, q, tol, lane, rotated);
+			mc = c > mc ? c : mc;
 		}
 		__syncthreads();
 	}
-	return rotated;
+	return mc;
 }
 
-// Cross pairs only between column halves [0, h) and [h, 2h): h rounds of h pairs.
-template <typename Real>
-__device__ bool jacobi_cross(Real *B, Real *V, int ld, int n, int h, Real tol) {
+// Cross pairs only between column halves [0, h) and [h, 2h): h rounds of h pairs; columns 2h and
+// 2h+1 are the zero padding pair.
+template <typename Real, int RPL>
+__device__ __forceinline__ Real jacobi_cross(Real *B, Real *V, Real *nrm, int h, const JacobiTol<Real> &tol,
+                                             bool &rotated) {
+	constexpr int JPW = PairsPerWarp<RPL>::value;
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-	bool rotated = false;
+	Real mc = 0;
 	for (int r = 0; r < h; r++) {
-		for (int k = warp; k < h; k += nwarp) {
-			int p = k, q = h + (k + r) % h;
-			rotated |= jacobi_pair(B, V, ld, n, p, q, tol, lane);
+		for (int k0 = warp * JPW; k0 < h; k0 += nwarp * JPW) {
+			int p[JPW], q[JPW];
+#pragma unroll
+			for (int k = 0; k < JPW; k++) {
+				if (k0 + k < h) {
+					p[k] = k0 + k;
+					int qq = k0 + k + r;
+					if (qq >= h) qq -= h;
+					q[k] = h + qq;
+				} else {
+					p[k] = 2 * h;
+					q[k] = 2 * h + 1;
+				}
+			}
+			Real c = jacobi_pairs<Real, RPL>(B, V, nrm, p, q, tol, lane, rotated);
+			mc = c > mc ? c : mc;
 		}
 		__syncthreads();
 	}
-	return rotated;
+	return mc;
+}
+
+// block-wide maximum of a non-negative value (all threads get the result)
+template <typename Real>
+__device__ Real block_max_nonneg(Real v, Real *scratch32) {
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) {
+		Real w = __shfl_xor_sync(0xffffffffu, v, o);
+		v = w > v ? w : v;
+	}
+	__syncthreads();
+	if (lane == 0) scratch32[warp] = v;
+	__syncthreads();
+	Real m = 0;
+	for (int q = 0; q < nwarp; q++) m = scratch32[q] > m ? scratch32[q] : m;
+	__syncthreads();
+	return m;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -374,11 +496,11 @@ __device__ void block_gemm(const GemmArgs<Real, OutT> &g, Real (*ps)[65], Real (
 // ---------------------------------------------------------------------------------------------
 // Jacobi polar kernel
 // ---------------------------------------------------------------------------------------------
-// Per searchlight: run sweeps until a sweep applies no rotation (or max_sweeps), take
-// sigma_c = ||B[:, c]||, form T = B diag(1/sigma) V^T into the T scratch (row-major when
-// t_rowmajor, else column-major), and record the singular-value statistics and the
-// singular pair of the smallest singular value (for the reflection fix).
-// Columns whose norm is exactly zero get an orthonormal completion so T stays orthogonal.
+// Per searchlight: run sweeps until converged (or max_sweeps), take sigma_c = ||B[:, c]||,
+// form T = B diag(1/sigma) V^T into the T scratch (row-major when t_rowmajor, else
+// column-major), and record the singular-value statistics and the singular pair of the
+// smallest singular value (for the reflection fix).  Numerically zero columns get an
+// orthonormal completion so T stays orthogonal.
 
 struct JacobiParams {
 	int max_sweeps;
@@ -387,90 +509,125 @@ struct JacobiParams {
 	int only_flagged;  // process only searchlights whose stats carry kFlagIllCond (FP64 re-solve)
 };
 
-template <typename Real>
-__global__ void __launch_bounds__(256) k_jacobi(const SlWork *__restrict__ work, Real *__restrict__ Ascr,
-                                                Real *__restrict__ Vscr, float *__restrict__ Tscr,
-                                                SlStats *__restrict__ stats, double *__restrict__ uvbuf,
-                                                JacobiParams prm) {
+template <typename Real, int RPL>
+__global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) k_jacobi(const SlWork *__restrict__ work, Real *__restrict__ Ascr,
+                                                   Real *__restrict__ Vscr, float *__restrict__ Tscr,
+                                                   SlStats *__restrict__ stats, double *__restrict__ uvbuf,
+                                                   JacobiParams prm) {
+	constexpr int LD = 32 * RPL;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	Real *sm = reinterpret_cast<Real *>(smem_raw);
 	const SlWork w = work[blockIdx.x];
 	if (prm.only_flagged && !(stats[w.slot].flags & kFlagIllCond)) return;
 	const int n = w.n, bsz = w.bsz, nblk = w.nblk;
 	const int ncol = nblk * bsz;
+	const int mst = 2 * bsz + 2;  // staged columns: two blocks plus the zero padding pair
 	Real *Ag = Ascr + w.aofs;
 	Real *Vg = Vscr + w.aofs;
-	const Real tol = Eps<Real>::v() * real_sqrt(Real(n));
+	const Real eps = Eps<Real>::v();
+	const Real sqn = real_sqrt(Real(n));
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
 
-	// shared: Bs[2*bsz][n], Vs[2*bsz][n], then small vectors
+	// shared: Bs[mst][LD], Vs[mst][LD], nrm[mst], then GEMM tiles (resident mode)
 	Real *Bs = sm;
-	Real *Vs = sm + (int64_t)2 * bsz * n;
-	Real *sig = Vs + (int64_t)2 * bsz * n;  // ncol entries (resident: 2*bsz)
+	Real *Vs = sm + mst * LD;
+	Real *nrm = Vs + mst * LD;
+	__shared__ Real red[32];
+	__shared__ double frob2;
 
-	bool resident = (nblk == 2);
+	const bool resident = (nblk == 2);
+	// ||A||_F^2 (invariant under the rotations) sets the zero threshold
+	{
+		Real ss = 0;
+		for (int e = threadIdx.x; e < n * n; e += blockDim.x) ss += Ag[e] * Ag[e];
+		ss = warp_sum(ss);
+		if (threadIdx.x == 0) frob2 = 0;
+		__syncthreads();
+		if (lane == 0) atomicAdd(&frob2, (double)ss);
+		__syncthreads();
+	}
+	JacobiTol<Real> tol;
+	tol.rot = eps * sqn;
+	tol.zero2 = (Real)(frob2 * (double)(eps * sqn) * (double)(eps * sqn));
+	const Real tol_conv = Real(4) * eps * sqn;
+
 	bool converged = false;
 	int sweep = 0;
 	if (resident) {
-		for (int64_t e = threadIdx.x; e < (int64_t)2 * bsz * n; e += blockDim.x) {
-			int c = (int)(e / n), i = (int)(e - (int64_t)c * n);
-			Bs[e] = Ag[e];
-			Vs[e] = (c == i) ? Real(1) : Real(0);
+		for (int e = threadIdx.x; e < mst * LD; e += blockDim.x) {
+			const int c = e / LD, i = e - c * LD;
+			Bs[e] = (c < ncol && i < n) ? Ag[c * n + i] : Real(0);
+			Vs[e] = (c == i && c < n) ? Real(1) : Real(0);
 		}
 		__syncthreads();
 		for (sweep = 0; sweep < prm.max_sweeps; sweep++) {
-			bool rot = jacobi_full_rr(Bs, Vs, n, n, 2 * bsz, tol);
-			if (!__syncthreads_or(rot)) {
+			column_norms<Real, RPL>(Bs, nrm, mst);
+			bool rot = false;
+			Real mc = jacobi_full_rr<Real, RPL>(Bs, Vs, nrm, 2 * bsz, tol, rot);
+			mc = block_max_nonneg(mc, red);
+			if (mc <= tol_conv) {
 				converged = true;
+				sweep++;
 				break;
 			}
 		}
 	} else {
-		for (int64_t e = threadIdx.x; e < (int64_t)ncol * n; e += blockDim.x) {
-			int c = (int)(e / n), i = (int)(e - (int64_t)c * n);
+		for (int e = threadIdx.x; e < ncol * n; e += blockDim.x) {
+			const int c = e / n, i = e - c * n;
 			Vg[e] = (c == i) ? Real(1) : Real(0);
+		}
+		for (int e = threadIdx.x; e < mst * LD; e += blockDim.x) {
+			Bs[e] = Real(0);
+			Vs[e] = Real(0);
 		}
 		__syncthreads();
 		for (sweep = 0; sweep < prm.max_sweeps; sweep++) {
+			Real mc = 0;
 			bool rot = false;
 			for (int br = 0; br < nblk - 1; br++) {
 				for (int k = 0; k < nblk / 2; k++) {
 					int I, J;
 					rr_pair(nblk, br, k, I, J);
-					// stage blocks I and J
-					for (int64_t e = threadIdx.x; e < (int64_t)bsz * n; e += blockDim.x) {
-						Bs[e] = Ag[(int64_t)I * bsz * n + e];
-						Bs[(int64_t)bsz * n + e] = Ag[(int64_t)J * bsz * n + e];
-						Vs[e] = Vg[(int64_t)I * bsz * n + e];
-						Vs[(int64_t)bsz * n + e] = Vg[(int64_t)J * bsz * n + e];
+					for (int e = threadIdx.x; e < 2 * bsz * n; e += blockDim.x) {
+						const int c = e / n, i = e - c * n;
+						const int gc = (c < bsz) ? I * bsz + c : J * bsz + (c - bsz);
+						Bs[c * LD + i] = Ag[gc * n + i];
+						Vs[c * LD + i] = Vg[gc * n + i];
 					}
 					__syncthreads();
+					column_norms<Real, RPL>(Bs, nrm, mst);
+					Real c;
 					if (br == 0)
-						rot |= jacobi_full_rr(Bs, Vs, n, n, 2 * bsz, tol);
+						c = jacobi_full_rr<Real, RPL>(Bs, Vs, nrm, 2 * bsz, tol, rot);
 					else
-						rot |= jacobi_cross(Bs, Vs, n, n, bsz, tol);
-					for (int64_t e = threadIdx.x; e < (int64_t)bsz * n; e += blockDim.x) {
-						Ag[(int64_t)I * bsz * n + e] = Bs[e];
-						Ag[(int64_t)J * bsz * n + e] = Bs[(int64_t)bsz * n + e];
-						Vg[(int64_t)I * bsz * n + e] = Vs[e];
-						Vg[(int64_t)J * bsz * n + e] = Vs[(int64_t)bsz * n + e];
+						c = jacobi_cross<Real, RPL>(Bs, Vs, nrm, bsz, tol, rot);
+					mc = c > mc ? c : mc;
+					for (int e = threadIdx.x; e < 2 * bsz * n; e += blockDim.x) {
+						const int cc = e / n, i = e - cc * n;
+						const int gc = (cc < bsz) ? I * bsz + cc : J * bsz + (cc - bsz);
+						Ag[gc * n + i] = Bs[cc * LD + i];
+						Vg[gc * n + i] = Vs[cc * LD + i];
 					}
 					__syncthreads();
 				}
 			}
-			if (!__syncthreads_or(rot)) {
+			mc = block_max_nonneg(mc, red);
+			if (mc <= tol_conv) {
 				converged = true;
+				sweep++;
 				break;
 			}
 		}
 	}
 
+	// from here on: B, V with column stride ldb (shared, LD, or global, n)
 	Real *B = resident ? Bs : Ag;
 	Real *V = resident ? Vs : Vg;
-	// column norms (sigma) -> shared sig[] (resident) or reuse Bs as a staging area (blocked)
-	Real *sg = resident ? sig : Bs;
+	const int ldb = resident ? LD : n;
+	// column norms (sigma) -> sg[] (resident: the nrm area; blocked: the staging area)
+	Real *sg = resident ? nrm : Bs;
 	for (int c = warp; c < ncol; c += nwarp) {
-		const Real *bc = B + (int64_t)c * n;
+		const Real *bc = B + c * ldb;
 		Real ss = 0;
 		for (int i = lane; i < n; i += 32) ss += bc[i] * bc[i];
 		ss = warp_sum(ss);
@@ -517,50 +674,64 @@ __global__ void __launch_bounds__(256) k_jacobi(const SlWork *__restrict__ work,
 			st.s_min = mn;
 			st.k_min = km;
 			st.flags = fl;
+			st.sweeps = sweep;
 			stats[w.slot] = st;
 		}
 		__syncthreads();
 	}
-	// normalise columns: u_c = b_c / sigma_c (in place); exactly-zero columns are completed below
-	for (int64_t e = threadIdx.x; e < (int64_t)n * n; e += blockDim.x) {
-		int c = (int)(e / n);
-		Real s = sg[c];
-		B[e] = (s > 0) ? B[e] / s : Real(0);
+	// normalise columns: u_c = b_c / sigma_c (in place)
+	for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+		const int c = e / n, i = e - c * n;
+		const Real s = sg[c];
+		B[c * ldb + i] = (s > 0) ? B[c * ldb + i] / s : Real(0);
 	}
 	__syncthreads();
-	// orthonormal completion of zero columns (rank-deficient A with exact zeros): Gram-Schmidt of
-	// unit vectors against the existing columns.  Rare; executed by warp 0.
-	if (warp == 0) {
-		for (int c = 0; c < n; c++) {
-			if (sg[c] > 0) continue;
-			for (int cand = 0; cand < n; cand++) {
-				Real *uc = B + (int64_t)c * n;
-				for (int i = lane; i < n; i += 32) uc[i] = (i == cand) ? Real(1) : Real(0);
-				__syncwarp();
-				for (int pass = 0; pass < 2; pass++) {
-					for (int o = 0; o < n; o++) {
-						if (o == c) continue;
-						const Real *uo = B + (int64_t)o * n;
-						Real no = 0;
-						for (int i = lane; i < n; i += 32) no += uo[i] * uo[i];
-						no = warp_sum(no);
-						if (no == 0) continue;
-						Real dp = 0;
-						for (int i = lane; i < n; i += 32) dp += uo[i] * uc[i];
-						dp = warp_sum(dp);
-						for (int i = lane; i < n; i += 32) uc[i] -= dp * uo[i];
-						__syncwarp();
-					}
-				}
-				Real nn = 0;
-				for (int i = lane; i < n; i += 32) nn += uc[i] * uc[i];
-				nn = warp_sum(nn);
-				if (nn > Real(0.25)) {
-					Real inv = Real(1) / real_sqrt(nn);
-					for (int i = lane; i < n; i += 32) uc[i] *= inv;
+	// Weak columns (sigma <= 1e3 eps sigma_max) carry directions that the rotations cannot make
+	// orthogonal to working precision, and exactly null ones carry none.  Each is re-orthogonalised
+	// (two Gram-Schmidt passes) against the strong columns and the weak ones before it; if little
+	// of it is left it is replaced by an orthonormal completion: the unit vector e_i with the
+	// largest remainder after the same projection.  The complement of the other columns has at
+	// least one dimension, so some e_i keeps a squared remainder >= 1/n; any remainder above
+	// 1/(2n) is accepted, else the best one.  Executed by warp 0.
+	{
+		const Real smax = (Real)stats[w.slot].s_max;
+		const Real weak = smax * Real(1000) * eps;
+		if (warp == 0) {
+			for (int c = 0; c < n; c++) {
+				if (sg[c] > weak) continue;
+				Real *uc = B + c * ldb;
+				Real best = -1;
+				int best_cand = 0;
+				for (int cand = -1; cand <= n; cand++) {
+					const int use = (cand == n) ? best_cand : cand;  // final pass: rebuild the best
+					if (cand >= 0)
+						for (int i = lane; i < n; i += 32) uc[i] = (i == use) ? Real(1) : Real(0);
 					__syncwarp();
-					if (lane == 0) sg[c] = Real(-1);  // marks "completed" (positive for no later test)
-					break;
+					for (int pass = 0; pass < 2; pass++) {
+						for (int o = 0; o < n; o++) {
+							if (o == c || (o > c && sg[o] <= weak)) continue;
+							const Real *uo = B + o * ldb;
+							Real dp = 0;
+							for (int i = lane; i < n; i += 32) dp += uo[i] * uc[i];
+							dp = warp_sum(dp);
+							for (int i = lane; i < n; i += 32) uc[i] -= dp * uo[i];
+							__syncwarp();
+						}
+					}
+					Real nn = 0;
+					for (int i = lane; i < n; i += 32) nn += uc[i] * uc[i];
+					nn = warp_sum(nn);
+					const Real accept = (cand < 0) ? Real(0.25) : Real(0.5) / Real(n);
+					if (nn > accept || (cand == n && nn > 0)) {
+						Real inv = Real(1) / real_sqrt(nn);
+						for (int i = lane; i < n; i += 32) uc[i] *= inv;
+						__syncwarp();
+						break;
+					}
+					if (cand >= 0 && cand < n && nn > best) {
+						best = nn;
+						best_cand = cand;
+					}
 				}
 			}
 		}
@@ -568,11 +739,11 @@ __global__ void __launch_bounds__(256) k_jacobi(const SlWork *__restrict__ work,
 	__syncthreads();
 	// save u_min, v_min for the reflection fix
 	{
-		int km = stats[w.slot].k_min;
+		const int km = stats[w.slot].k_min;
 		double *uv = uvbuf + w.uvofs;
 		for (int i = threadIdx.x; i < n; i += blockDim.x) {
-			uv[i] = (double)B[(int64_t)km * n + i];
-			uv[n + i] = (double)V[(int64_t)km * n + i];
+			uv[i] = (double)B[km * ldb + i];
+			uv[n + i] = (double)V[km * ldb + i];
 		}
 	}
 	// T = U V^T :  T(i, j) = sum_c U[c][i] V[c][j], written as float32 (resident mode; the
@@ -580,14 +751,14 @@ __global__ void __launch_bounds__(256) k_jacobi(const SlWork *__restrict__ work,
 	if (resident) {
 		GemmArgs<Real, float> g;
 		g.M = n; g.N = n; g.K = n;
-		g.P = B; g.pk = n; g.pi = 1;
-		g.Q = V; g.qk = n; g.qj = 1;
+		g.P = B; g.pk = LD; g.pi = 1;
+		g.Q = V; g.qk = LD; g.qj = 1;
 		g.d = nullptr; g.alpha = Real(1);
 		g.E = nullptr; g.ei = 0; g.ej = 0; g.beta = 0;
 		g.C = Tscr + w.tofs;
 		g.ci = prm.t_rowmajor ? n : 1;
 		g.cj = prm.t_rowmajor ? 1 : n;
-		Real (*ps)[65] = reinterpret_cast<Real (*)[65]>(sig + ncol + 2);
+		Real (*ps)[65] = reinterpret_cast<Real (*)[65]>(nrm + mst + 2);
 		Real (*qs)[65] = ps + 16;
 		block_gemm(g, ps, qs);
 	}

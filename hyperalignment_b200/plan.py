@@ -60,7 +60,20 @@ class Plan:
     def stats(self):
         a, b = ctypes.c_int32(), ctypes.c_int32()
         L.check(self.lib.ha_b200_plan_stats(self.handle, ctypes.byref(a), ctypes.byref(b)), "ha_b200_plan_stats")
-        return {"n_fp64": a.value, "n_unconverged": b.value}
+        ssum, smax = ctypes.c_int64(), ctypes.c_int32()
+        L.check(self.lib.ha_b200_plan_sweep_stats(self.handle, ctypes.byref(ssum), ctypes.byref(smax)),
+                "ha_b200_plan_sweep_stats")
+        return {"n_fp64": a.value, "n_unconverged": b.value, "sweeps_mean": ssum.value / max(1, self.count),
+                "sweeps_max": smax.value}
+
+    def searchlight_stats(self, first: int, n: int):
+        """Per-searchlight sigma_min, sigma_max, flags and sweeps of the last run (last chunk)."""
+        smin, smax = np.empty(n), np.empty(n)
+        flags, sweeps = np.empty(n, dtype=np.int32), np.empty(n, dtype=np.int32)
+        L.check(self.lib.ha_b200_plan_searchlight_stats(self.handle, first, n, L.dptr(smin), L.dptr(smax),
+                                                         L.iptr(flags), L.iptr(sweeps)),
+                "ha_b200_plan_searchlight_stats")
+        return {"s_min": smin, "s_max": smax, "flags": flags, "sweeps": sweeps}
 
     def local_transforms(self, first: int, n: int):
         """Unweighted, unscaled T_s of searchlights [first, first+n) from the last run (row-major if CSR)."""

@@ -202,8 +202,17 @@ int64_t ha_b200_plan_nnz(const HaB200Plan *plan);
 int ha_b200_plan_pattern(const HaB200Plan *plan, int64_t *indptr, int32_t *indices);
 /* Device pointer to the plan's per-vertex pattern (indptr int64 nv+1, indices int32 nnz). */
 int ha_b200_plan_device_pattern(const HaB200Plan *plan, const int64_t **d_indptr, const int32_t **d_indices);
-/* Ill-conditioned searchlights that the last run re-solved in FP64, and the number of ones. */
+/* Searchlights of the last run that were solved in FP64, and that hit the sweep limit. */
 int ha_b200_plan_stats(const HaB200Plan *plan, int32_t *n_fp64, int32_t *n_jacobi_unconverged);
+/* Jacobi sweeps of the last run: sum over searchlights (final solve of each) and maximum. */
+int ha_b200_plan_sweep_stats(const HaB200Plan *plan, int64_t *sweeps_sum, int32_t *sweeps_max);
+/*
+ * Per-searchlight solve record of the last run, searchlights [first, first + n) of its last
+ * chunk: smallest and largest singular value, flags (1 unconverged, 2 ill-conditioned,
+ * 4 reflection removed, 8 solved in FP64) and Jacobi sweeps.  Any output may be NULL.
+ */
+int ha_b200_plan_searchlight_stats(const HaB200Plan *plan, int32_t first, int32_t n, double *s_min,
+                                   double *s_max, int32_t *flags, int32_t *sweeps);
 
 /*
  * Searchlight Procrustes on device-resident data.  d_X, d_Y: nt x nv float64

@@ -74,14 +74,16 @@ def lib():
         h.ha_ridge.restype = ctypes.c_int
         h.ha_ridge.argtypes = [ctypes.POINTER(TMat), ctypes.POINTER(TMat), ctypes.c_double, ctypes.POINTER(TMat)]
         _lib = h
-        try:
-            ob = ctypes.CDLL(None)
+        # one BLAS thread per OpenMP thread (the reference parallelises over searchlights)
+        import glob
+        import scipy
+        libs = os.path.join(os.path.dirname(scipy.__file__), "..", "scipy.libs")
+        for path in glob.glob(os.path.join(libs, "libscipy_openblas*.so")):
+            ob = ctypes.CDLL(path)
             fn = getattr(ob, "scipy_openblas_set_num_threads", None)
             if fn is not None:
                 fn.argtypes = [ctypes.c_int]
                 fn(1)
-        except OSError:
-            pass
     return _lib
 
 
