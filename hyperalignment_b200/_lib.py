@@ -62,6 +62,9 @@ SIGNATURES = {
         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_void_p,
         ctypes.c_void_p]),
     "ha_b200_plan_local_transforms": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, c_float_p]),
+    "ha_b200_local_procrustes_noalloc": (ctypes.c_int, [
+        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, c_int32_p, ctypes.c_int32,
+        ctypes.c_void_p, ctypes.c_void_p]),
     "ha_b200_set_kernel_timing": (None, [ctypes.c_bool]),
     "ha_b200_kernel_times": (ctypes.c_int, [c_double_p, c_int64_p]),
     "ha_b200_launch_count": (ctypes.c_int64, []),

@@ -1054,3 +1054,247 @@ int ha_b200_plan_local_transforms(const HaB200Plan *P, int32_t first, int32_t n,
 }
 
 }  // extern "C"
+
+// =============================================================================================
+// Local Procrustes without allocation
+// =============================================================================================
+//
+// Some callers cannot call cudaMalloc: applications whose own pool allocator has already
+// reserved the GPU's memory and hands out nothing else, plugins whose host program forbids
+// them to create device allocations, and loops where the device-wide synchronisation of
+// cudaMalloc/cudaFree is not acceptable.  For them this entry point computes the local
+// transforms of searchlights of up to kNoAllocMaxN vertices from buffers the caller already
+// owns, using as scratch only the file-scope device array below.  That array is part of the
+// library image: every GPU that loads the library holds it until the process exits.
+
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = (size_t)64 << 20;  // 64 MiB
+constexpr int kNoAllocMaxN = 160;                          // largest searchlight (resident FP32 Jacobi)
+constexpr int kNoAllocMaxBatch = 2048;                     // searchlights per launch
+constexpr int kNoAllocMaxDevices = 64;
+
+// Scratch of every call: [status word | work items | solve records | u/v pairs | A matrices].
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr size_t kNaStatusOfs = 0;
+constexpr size_t kNaWorkOfs = 256;
+constexpr size_t kNaStatsOfs = kNaWorkOfs + (((size_t)kNoAllocMaxBatch * sizeof(SlWork) + 255) & ~(size_t)255);
+constexpr size_t kNaUvOfs = kNaStatsOfs + (((size_t)kNoAllocMaxBatch * sizeof(SlStats) + 255) & ~(size_t)255);
+constexpr size_t kNaAOfs = kNaUvOfs + (((size_t)kNoAllocMaxBatch * 2 * kNoAllocMaxN * sizeof(double) + 255) & ~(size_t)255);
+constexpr size_t kNaAFloats = (kNoAllocScratchBytes - kNaAOfs) / sizeof(float);
+static_assert(kNaAOfs < kNoAllocScratchBytes, "no-alloc scratch layout");
+
+// Device address of g_noalloc_scratch per device (host code may not use the symbol itself).
+unsigned char *g_noalloc_ptr[kNoAllocMaxDevices] = {nullptr};
+SlWork g_noalloc_items[kNoAllocMaxBatch];  // host staging of one batch's work items
+int32_t g_noalloc_status_host = 0;
+
+// Cross-covariance from float64 vertex-major inputs, rounded to float32 on load (the same
+// tiling and summation order as k_xcov<float>).  Indices outside [0, nv) are read as zero
+// columns and reported through *status.
+template <int KT>
+__global__ void __launch_bounds__(256) k_xcov_f64in(const SlWork *__restrict__ work, const int32_t *__restrict__ sl_idx,
+                                                    const double *__restrict__ X, const double *__restrict__ Y, int nt,
+                                                    int nv, float *__restrict__ Ascr, int32_t *__restrict__ status) {
+	const SlWork w = work[blockIdx.x];
+	const int n = w.n;
+	const int ncol = w.nblk * w.bsz;
+	const int32_t *sl = sl_idx + w.sofs;
+	float *A = Ascr + w.aofs;
+	__shared__ float xs[KT][64 + 1];
+	__shared__ float ys[KT][64 + 1];
+	__shared__ int32_t vi[64], vj[64];
+	const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+	for (int i0 = 0; i0 < n; i0 += 64) {
+		for (int j0 = 0; j0 < n; j0 += 64) {
+			__syncthreads();
+			if (threadIdx.x < 128) {
+				const int r = threadIdx.x & 63;
+				const int idx = (threadIdx.x < 64 ? i0 : j0) + r;
+				int v = -1;
+				if (idx < n) {
+					v = sl[idx];
+					if (v < 0 || v >= nv) {
+						atomicOr(status, 1);
+						v = -1;
+					}
+				}
+				if (threadIdx.x < 64) vi[r] = v; else vj[r] = v;
+			}
+			float acc[4][4];
+#pragma unroll
+			for (int a = 0; a < 4; a++)
+#pragma unroll
+				for (int b = 0; b < 4; b++) acc[a][b] = 0.0f;
+			for (int t0 = 0; t0 < nt; t0 += KT) {
+				__syncthreads();
+				for (int e = threadIdx.x; e < 64 * KT; e += 256) {
+					const int r = e / KT, t = e - r * KT;
+					const int tt = t0 + t;
+					const int v = vi[r], u = vj[r];
+					xs[t][r] = (v >= 0 && tt < nt) ? (float)X[(int64_t)v * nt + tt] : 0.0f;
+					ys[t][r] = (u >= 0 && tt < nt) ? (float)Y[(int64_t)u * nt + tt] : 0.0f;
+				}
+				__syncthreads();
+#pragma unroll 4
+				for (int t = 0; t < KT; t++) {
+					float a[4], b[4];
+#pragma unroll
+					for (int q = 0; q < 4; q++) {
+						a[q] = xs[t][ty + 16 * q];
+						b[q] = ys[t][tx + 16 * q];
+					}
+#pragma unroll
+					for (int p = 0; p < 4; p++)
+#pragma unroll
+						for (int q = 0; q < 4; q++) acc[p][q] += a[p] * b[q];
+				}
+			}
+#pragma unroll
+			for (int p = 0; p < 4; p++) {
+				const int i = i0 + ty + 16 * p;
+				if (i >= n) continue;
+#pragma unroll
+				for (int q = 0; q < 4; q++) {
+					const int j = j0 + tx + 16 * q;
+					if (j < n) A[(int64_t)j * n + i] = acc[p][q];
+				}
+			}
+		}
+	}
+	for (int64_t e = (int64_t)n * n + threadIdx.x; e < (int64_t)n * ncol; e += 256) A[e] = 0.0f;
+}
+
+// Once per device, with that device current: find the scratch array's device address and
+// raise the shared-memory limit of the kernels used below.
+int noalloc_setup(int dev, unsigned char **out) {
+	if (dev < 0 || dev >= kNoAllocMaxDevices) {
+		fprintf(stderr, "ha_b200_local_procrustes_noalloc: device %d out of range\n", dev);
+		return kHaErrorInternal;
+	}
+	if (!g_noalloc_ptr[dev]) {
+		void *p = nullptr;
+		cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+		if (e != cudaSuccess || !p) {
+			fprintf(stderr, "ha_b200_local_procrustes_noalloc: cudaGetSymbolAddress failed: %s\n",
+			        cudaGetErrorString(e));
+			cudaGetLastError();
+			return kHaErrorInternal;
+		}
+		if (set_jacobi_attrs<float>() != kHaSuccess) {
+			fprintf(stderr, "ha_b200_local_procrustes_noalloc: cudaFuncSetAttribute failed\n");
+			return kHaErrorInternal;
+		}
+		g_noalloc_ptr[dev] = (unsigned char *)p;
+	}
+	*out = g_noalloc_ptr[dev];
+	return kHaSuccess;
+}
+
+}  // namespace
+
+extern "C" int ha_b200_local_procrustes_noalloc(const double *d_X, const double *d_Y, int32_t nt, int32_t nv,
+                                                const int32_t *d_sl_indices, const int32_t *sl_offsets,
+                                                int32_t count, float *d_T_out, void *stream) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	if (!d_X || !d_Y || !d_sl_indices || !sl_offsets || !d_T_out || nt <= 0 || nv <= 0 || count <= 0)
+		return kHaErrorArg;
+	if (sl_offsets[0] != 0) {
+		fprintf(stderr, "ha_b200_local_procrustes_noalloc: sl_offsets[0] must be 0\n");
+		return kHaErrorArg;
+	}
+	for (int32_t s = 0; s < count; s++) {
+		const int32_t n = sl_offsets[s + 1] - sl_offsets[s];
+		if (n < 1 || n > kNoAllocMaxN) {
+			fprintf(stderr,
+			        "ha_b200_local_procrustes_noalloc: searchlight %d has %d vertices; this entry point "
+			        "supports 1 to %d (use ha_b200_plan_procrustes_device for larger ones)\n",
+			        s, n, kNoAllocMaxN);
+			return kHaErrorArg;
+		}
+	}
+	int rc = check_cuda_ready();
+	if (rc != kHaSuccess) return rc;
+	int dev = 0;
+	if (cudaGetDevice(&dev) != cudaSuccess) return kHaErrorInternal;
+	unsigned char *base = nullptr;
+	if ((rc = noalloc_setup(dev, &base)) != kHaSuccess) return rc;
+	cudaStream_t st = (cudaStream_t)stream;
+	int32_t *d_status = reinterpret_cast<int32_t *>(base + kNaStatusOfs);
+	SlWork *d_work = reinterpret_cast<SlWork *>(base + kNaWorkOfs);
+	SlStats *d_stats = reinterpret_cast<SlStats *>(base + kNaStatsOfs);
+	double *d_uv = reinterpret_cast<double *>(base + kNaUvOfs);
+	float *d_A = reinterpret_cast<float *>(base + kNaAOfs);
+	// the array keeps the previous call's contents: clear the status word and the solve records
+	HA_CUDA(cudaMemsetAsync(d_status, 0, sizeof(int32_t), st));
+
+	JacobiParams jp;
+	jp.max_sweeps = 40;
+	jp.t_rowmajor = 1;
+	jp.ill_ratio = 0.0;
+	jp.only_flagged = 0;
+	int64_t tofs = 0;  // packed output offset of the current searchlight
+	int32_t s = 0;
+	while (s < count) {
+		// one batch: as many searchlights as fit the work-item and A areas
+		int nb = 0;
+		int64_t a_used = 0, uv_used = 0;
+		while (s + nb < count && nb < kNoAllocMaxBatch) {
+			const int32_t n = sl_offsets[s + nb + 1] - sl_offsets[s + nb];
+			int bsz, nblk;
+			size_t smem;
+			jacobi_layout(n, false, bsz, nblk, smem);
+			const int64_t need = ((int64_t)n * nblk * bsz + 63) & ~(int64_t)63;
+			if (a_used + need > (int64_t)kNaAFloats) break;
+			SlWork &w = g_noalloc_items[nb];
+			w.s = s + nb;
+			w.n = n;
+			w.bsz = bsz;
+			w.nblk = nblk;
+			w.aofs = a_used;
+			w.tofs = tofs;
+			w.sofs = sl_offsets[s + nb];
+			w.slot = nb;
+			w.uvofs = uv_used;
+			a_used += need;
+			uv_used += 2 * (int64_t)n;
+			tofs += (int64_t)n * n;
+			nb++;
+		}
+		HA_CUDA(cudaMemcpyAsync(d_work, g_noalloc_items, (size_t)nb * sizeof(SlWork), cudaMemcpyHostToDevice, st));
+		HA_CUDA(cudaMemsetAsync(d_stats, 0, (size_t)nb * sizeof(SlStats), st));
+		// one launch per rows-per-lane group (items of a batch are in searchlight order)
+		k_xcov_f64in<32><<<nb, kBlock, 0, st>>>(d_work, d_sl_indices, d_X, d_Y, nt, nv, d_A, d_status);
+		HA_CUDA(cudaGetLastError());
+		int q = 0;
+		while (q < nb) {
+			const int rpl = rpl_for(g_noalloc_items[q].n);
+			int e = q, maxb = 0;
+			size_t smem = 0;
+			while (e < nb && rpl_for(g_noalloc_items[e].n) == rpl) {
+				int bsz, nblk;
+				size_t sm;
+				jacobi_layout(g_noalloc_items[e].n, false, bsz, nblk, sm);
+				smem = std::max(smem, sm);
+				maxb = std::max(maxb, bsz);
+				e++;
+			}
+			if ((rc = launch_jacobi<float>(rpl, e - q, jacobi_threads(maxb, false), smem, st, d_work + q, d_A, d_A,
+			                               d_T_out, d_stats, d_uv, jp)) != kHaSuccess)
+				return rc;
+			HA_CUDA(cudaGetLastError());
+			q = e;
+		}
+		// the next batch reuses the scratch: finish this one before its items are overwritten
+		HA_CUDA(cudaStreamSynchronize(st));
+		s += nb;
+	}
+	HA_CUDA(cudaMemcpyAsync(&g_noalloc_status_host, d_status, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+	HA_CUDA(cudaStreamSynchronize(st));
+	if (g_noalloc_status_host != 0) {
+		fprintf(stderr, "ha_b200_local_procrustes_noalloc: a searchlight index is outside [0, %d)\n", nv);
+		return kHaErrorArg;
+	}
+	return kHaSuccess;
+}

@@ -238,6 +238,33 @@ int ha_b200_plan_ridge_device(
  */
 int ha_b200_plan_local_transforms(const HaB200Plan *plan, int32_t first, int32_t n, float *out);
 
+/* ---- local Procrustes without allocation ---- */
+
+/*
+ * No counterpart in the reference.  For callers that cannot allocate device memory (their own
+ * pool allocator owns the GPU, or their host program forbids new allocations, or the
+ * device-wide synchronisation of cudaMalloc/cudaFree is not acceptable in their loop): computes
+ * the local transforms T_s (the unscaled, unweighted polar factors of X[:, sl]^T Y[:, sl],
+ * reflection allowed, plain FP32 Jacobi) of searchlights of at most kHaB200NoAllocMaxSize vertices
+ * and writes them packed, row-major, searchlight after searchlight, to d_T_out (float32, sum of
+ * n_s^2 entries).  d_X, d_Y (nt x nv float64, column-major), d_sl_indices and d_T_out are DEVICE
+ * memory owned by the caller; sl_offsets (count + 1 entries) is host memory.
+ *
+ * The only scratch is a static 64 MiB device array inside this library, held by every GPU that
+ * loads it until the process exits; the call allocates nothing.  The first call on a device
+ * looks up that array's address and raises kernel shared-memory limits; make it before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU (from other host
+ * threads or other streams) race.  Returns after the work on `stream` is finished;
+ * kHaErrorArg for a searchlight size outside 1..kHaB200NoAllocMaxSize (checked before any work)
+ * or a vertex index outside [0, nv) (checked on the device).
+ */
+#define kHaB200NoAllocMaxSize 160
+#define kHaB200NoAllocScratchBytes (64u << 20)
+int ha_b200_local_procrustes_noalloc(
+	const double *d_X, const double *d_Y, int32_t nt, int32_t nv,
+	const int32_t *d_sl_indices, const int32_t *sl_offsets, int32_t count,
+	float *d_T_out, void *stream);
+
 /* ---- tracing ---- */
 
 /* Kernel kinds reported by ha_b200_kernel_times. */
