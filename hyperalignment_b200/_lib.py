@@ -43,6 +43,9 @@ SIGNATURES = {
     "ha_searchlight_ridge_csc_b200": (ctypes.c_int, [
         c_double_p, c_double_p, ctypes.c_int32, ctypes.c_int32, c_int32_p, c_int32_p, ctypes.c_int32,
         c_double_p, c_int32_p, c_int32_p, ctypes.c_int64, c_double_p, ctypes.c_double, ctypes.c_bool]),
+    "ha_searchlight_template_b200": (ctypes.c_int, [
+        c_double_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, c_int32_p, c_int32_p, c_double_p, ctypes.c_int32,
+        ctypes.c_double, ctypes.c_bool, ctypes.c_bool, ctypes.c_bool, ctypes.c_int32, c_double_p]),
     "ha_b200_plan_create": (ctypes.c_int, [
         ctypes.c_int32, ctypes.c_int32, c_int32_p, c_int32_p, c_double_p, ctypes.c_int32, ctypes.c_double,
         c_double_p, ctypes.POINTER(ctypes.c_void_p)]),

@@ -225,6 +225,7 @@ struct HaB200Plan {
 	std::vector<Chunk> chunks;
 	DevArr<double> scrA, scrV;  // 8-byte units, reinterpreted per precision
 	DevArr<float> scrT;
+	DevArr<double> scrT64;  // float64 local results (ridge), allocated on first use
 	DevArr<double> uv, scale;
 	DevArr<SlStats> stats;
 	int max_slots = 0;
@@ -448,7 +449,8 @@ int set_smem_attrs() {
 		fprintf(stderr, "ha_b200: cudaFuncSetAttribute on the Jacobi kernels failed\n");
 		return kHaErrorInternal;
 	}
-	HA_CUDA(cudaFuncSetAttribute(k_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax));
+	HA_CUDA(cudaFuncSetAttribute(k_reduce<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax));
+	HA_CUDA(cudaFuncSetAttribute(k_reduce<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax));
 	HA_CUDA(cudaFuncSetAttribute(k_pattern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax));
 	done = true;
 	return kHaSuccess;
@@ -635,8 +637,45 @@ int run_procrustes(HaB200Plan *P, const double *d_X, const double *d_Y, bool ref
 		{ HA_LAUNCH(kHaB200KScale, st); k_scale<<<(nsl + 127) / 128, 128, 0, st>>>(ch.d_w64, nsl, P->idx.p, P->var.p, P->stats.p, nt, scal ? 1 : 0,
 		                                          P->scale.p); }
 		{ HA_LAUNCH(kHaB200KScale, st); k_count_flags<<<(nsl + 127) / 128, 128, 0, st>>>(P->stats.p, nsl, P->counters.p); }
-		{ HA_LAUNCH(kHaB200KReduce, st); k_reduce<<<nv, kBlock, red_smem, st>>>(P->vlptr.p, P->vlent.p, P->off.p, P->idx.p,
+		{ HA_LAUNCH(kHaB200KReduce, st); k_reduce<float><<<nv, kBlock, red_smem, st>>>(P->vlptr.p, P->vlent.p, P->off.p, P->idx.p,
 		                                       P->has_weights ? P->w.p : nullptr, P->patptr.p, P->patcol.p, T,
+		                                       ch.d_tofs, P->scale.p, ch.s0, ch.s1, out_kind == kHaB200OutCSC ? 1 : 0,
+		                                       smem_cap, d_vals); }
+		HA_CUDA(cudaGetLastError());
+	}
+	P->last_chunk = (int)P->chunks.size() - 1;
+	P->last_rowmajor = rowmajor;
+	return kHaSuccess;
+}
+
+// Enqueue the searchlight ridge solve + reduction over all chunks (float64 throughout).
+int run_ridge(HaB200Plan *P, const double *d_X, const double *d_Y, double alpha, int out_kind, double *d_vals,
+              cudaStream_t st) {
+	const int nt = P->nt, nv = P->nv;
+	const int rowmajor = out_kind == kHaB200OutCSR ? 1 : 0;
+	int rc;
+	if (P->chunks.empty() && (rc = build_chunks(P)) != kHaSuccess) return rc;
+	int64_t maxT = 1;
+	for (auto &ch : P->chunks) maxT = std::max(maxT, ch.t_elems);
+	if ((rc = P->scrT64.ensure((size_t)maxT)) != kHaSuccess) return rc;
+	HA_CUDA(cudaMemsetAsync(P->counters.p, 0, 4 * sizeof(int32_t), st));
+	const int smem_cap = std::min(P->max_row, 16384);
+	const size_t red_smem = (size_t)smem_cap * 12;
+	for (size_t c = 0; c < P->chunks.size(); c++) {
+		Chunk &ch = P->chunks[c];
+		const int nsl = ch.s1 - ch.s0;
+		HA_CUDA(cudaMemsetAsync(P->stats.p, 0, (size_t)nsl * sizeof(SlStats), st));
+		double *G = P->scrA.p, *R = P->scrV.p;
+		for (const Bucket &b : ch.b64) {
+			const SlWork *wk = ch.d_w64 + b.first;
+			{ HA_LAUNCH(kHaB200KXcov64, st); k_xcov<double, 16><<<b.count, kBlock, 0, st>>>(wk, P->idx.p, d_X, d_X, nt, nt, G, P->stats.p, 0); }
+			{ HA_LAUNCH(kHaB200KXcov64, st); k_xcov<double, 16><<<b.count, kBlock, 0, st>>>(wk, P->idx.p, d_X, d_Y, nt, nt, R, P->stats.p, 0); }
+			{ HA_LAUNCH(kHaB200KRidge, st); k_ridge_chol<<<b.count, kBlock, 0, st>>>(wk, G, R, P->scrT64.p, alpha, rowmajor, P->stats.p); }
+		}
+		{ HA_LAUNCH(kHaB200KScale, st); k_scale<<<(nsl + 127) / 128, 128, 0, st>>>(ch.d_w64, nsl, P->idx.p, nullptr, P->stats.p, nt, 0, P->scale.p); }
+		{ HA_LAUNCH(kHaB200KScale, st); k_count_flags<<<(nsl + 127) / 128, 128, 0, st>>>(P->stats.p, nsl, P->counters.p); }
+		{ HA_LAUNCH(kHaB200KReduce, st); k_reduce<double><<<nv, kBlock, red_smem, st>>>(P->vlptr.p, P->vlent.p, P->off.p, P->idx.p,
+		                                       P->has_weights ? P->w.p : nullptr, P->patptr.p, P->patcol.p, P->scrT64.p,
 		                                       ch.d_tofs, P->scale.p, ch.s0, ch.s1, out_kind == kHaB200OutCSC ? 1 : 0,
 		                                       smem_cap, d_vals); }
 		HA_CUDA(cudaGetLastError());
@@ -799,6 +838,72 @@ int csc_impl(const double *X, const double *Y, int32_t nt, int32_t nv, const int
 
 }  // namespace
 
+// Searchlight template loop on the device (csrc/ha_template.c:14-114 with searchlight solves).
+int template_impl(const double *dms, int ns, int nt, int nv, const int32_t *idx, const int32_t *off,
+                  const double *dists, int count, double radius, bool refl, bool scal, bool zs, int level2,
+                  double *tpl_out) {
+	if (!dms || !tpl_out || ns < 2 || nt <= 0 || nv <= 0 || count <= 0 || level2 < 0) return kHaErrorArg;
+	int rc = check_cuda_ready();
+	if (rc != kHaSuccess) return rc;
+	HaB200Plan *P = nullptr;
+	if ((rc = get_plan(nt, nv, idx, off, dists, count, radius, nullptr, false, &P)) != kHaSuccess) return rc;
+	const size_t m = (size_t)nt * nv;
+	DevArr<double> D, A, common, ref, vals;
+	auto done = [&](int code) {
+		D.release(); A.release(); common.release(); ref.release(); vals.release();
+		return code;
+	};
+	if ((rc = D.ensure(m * ns)) != kHaSuccess) return done(rc);
+	if ((rc = A.ensure(m * ns)) != kHaSuccess) return done(rc);
+	if ((rc = common.ensure(m)) != kHaSuccess) return done(rc);
+	if ((rc = ref.ensure(m)) != kHaSuccess) return done(rc);
+	if ((rc = vals.ensure((size_t)P->nnz)) != kHaSuccess) return done(rc);
+	cudaStream_t st = 0;
+	if (cudaMemcpyAsync(D.p, dms, m * ns * 8, cudaMemcpyHostToDevice, st) != cudaSuccess) return done(kHaErrorInternal);
+	const int eg = 148 * 8;
+	const int zg = (nv + 127) / 128;
+	// aligned_s = X_s @ SL(X_s -> target)
+	auto align = [&](int s, const double *target) -> int {
+		if (cudaMemsetAsync(vals.p, 0, (size_t)P->nnz * 8, st) != cudaSuccess) return kHaErrorInternal;
+		int r = run_procrustes(P, D.p + m * s, target, refl, scal, kHaB200SolverMixed, kHaB200OutCSC, vals.p, st);
+		if (r != kHaSuccess) return r;
+		k_spmm_csc<<<nv, 128, 0, st>>>(D.p + m * s, nt, nv, P->patptr.p, P->patcol.p, vals.p, A.p + m * s);
+		return cudaGetLastError() == cudaSuccess ? kHaSuccess : kHaErrorInternal;
+	};
+	if (cudaMemcpyAsync(common.p, D.p, m * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+	    cudaMemcpyAsync(A.p, D.p, m * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+		return done(kHaErrorInternal);
+	for (int s = 1; s < ns; s++) {
+		if ((rc = align(s, common.p)) != kHaSuccess) return done(rc);
+		if (zs) k_zscore_cols<<<zg, 128, 0, st>>>(A.p + m * s, nt, nv);
+		k_axpbz<<<eg, 256, 0, st>>>(common.p, common.p, A.p + m * s, 0.5, 1.0, (int64_t)m);
+		if (zs) k_zscore_cols<<<zg, 128, 0, st>>>(common.p, nt, nv);
+	}
+	for (int it = 0; it < level2; it++) {
+		// common = sum over subjects (in subject order)
+		k_axpbz<<<eg, 256, 0, st>>>(common.p, A.p, nullptr, 1.0, 0.0, (int64_t)m);
+		for (int s = 1; s < ns; s++) k_axpbz<<<eg, 256, 0, st>>>(common.p, common.p, A.p + m * s, 1.0, 1.0, (int64_t)m);
+		for (int s = 0; s < ns; s++) {
+			k_axpbz<<<eg, 256, 0, st>>>(ref.p, common.p, A.p + m * s, 1.0 / (ns - 1), -1.0, (int64_t)m);
+			if (zs) k_zscore_cols<<<zg, 128, 0, st>>>(ref.p, nt, nv);
+			if ((rc = align(s, ref.p)) != kHaSuccess) return done(rc);
+		}
+	}
+	k_axpbz<<<eg, 256, 0, st>>>(common.p, A.p, nullptr, 1.0, 0.0, (int64_t)m);
+	for (int s = 1; s < ns; s++) k_axpbz<<<eg, 256, 0, st>>>(common.p, common.p, A.p + m * s, 1.0, 1.0, (int64_t)m);
+	if (zs)
+		k_zscore_cols<<<zg, 128, 0, st>>>(common.p, nt, nv);
+	else
+		k_axpbz<<<eg, 256, 0, st>>>(common.p, common.p, nullptr, 1.0 / ns, 0.0, (int64_t)m);
+	if (cudaGetLastError() != cudaSuccess ||
+	    cudaMemcpyAsync(tpl_out, common.p, m * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+	    cudaStreamSynchronize(st) != cudaSuccess) {
+		fprintf(stderr, "ha_searchlight_template_b200: CUDA failure: %s\n", cudaGetErrorString(cudaGetLastError()));
+		return done(kHaErrorInternal);
+	}
+	return done(kHaSuccess);
+}
+
 // =============================================================================================
 // C ABI
 // =============================================================================================
@@ -867,6 +972,15 @@ int ha_searchlight_procrustes_dense(const double *X_data, const double *Y_data, 
 	}
 	return ha_searchlight_procrustes_b200(X_data, Y_data, nt, nv, sl_indices, sl_offsets, sl_dists, count, radius,
 	                                      T_out, isReflection, isScaling, col_major);
+}
+
+int ha_searchlight_template_b200(const double *dms, int32_t n_subj, int32_t nt, int32_t nv,
+                                 const int32_t *sl_indices, const int32_t *sl_offsets, const double *sl_dists,
+                                 int32_t count, double radius, bool isReflection, bool isScaling,
+                                 bool isZscoreCommon, int32_t level2_iter, double *tpl_out) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	return template_impl(dms, n_subj, nt, nv, sl_indices, sl_offsets, sl_dists, count, radius, isReflection,
+	                     isScaling, isZscoreCommon, level2_iter, tpl_out);
 }
 
 int ha_sparse_pattern_b200(const int32_t *sl_indices, const int32_t *sl_offsets, int32_t count, int32_t nv,
@@ -939,7 +1053,7 @@ void ha_b200_plan_destroy(HaB200Plan *P) {
 	}
 	P->idx.release(); P->off.release(); P->lo.release(); P->hi.release(); P->w.release();
 	P->vlptr.release(); P->vlent.release(); P->patptr.release(); P->patcol.release();
-	P->scrA.release(); P->scrV.release(); P->scrT.release(); P->uv.release(); P->scale.release();
+	P->scrA.release(); P->scrV.release(); P->scrT.release(); P->scrT64.release(); P->uv.release(); P->scale.release();
 	P->stats.release(); P->X32.release(); P->Y32.release(); P->var.release(); P->counters.release();
 	delete P;
 }
@@ -1009,9 +1123,13 @@ int ha_b200_plan_procrustes_device(HaB200Plan *P, const double *d_X, const doubl
 
 int ha_b200_plan_ridge_device(HaB200Plan *P, const double *d_X, const double *d_Y, double alpha, int out_kind,
                               double *d_values, void *stream) {
-	(void)P; (void)d_X; (void)d_Y; (void)alpha; (void)out_kind; (void)d_values; (void)stream;
-	fprintf(stderr, "ha_b200: ridge is not available in this build\n");
-	return kHaErrorInternal;
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	if (!P || !d_X || !d_Y || !d_values || out_kind < 0 || out_kind > 1) return kHaErrorArg;
+	if (!(alpha >= 0.0)) {
+		fprintf(stderr, "ha_b200: ridge alpha must be >= 0\n");
+		return kHaErrorArg;
+	}
+	return run_ridge(P, d_X, d_Y, alpha, out_kind, d_values, (cudaStream_t)stream);
 }
 
 void ha_b200_set_kernel_timing(bool on) {

@@ -1024,10 +1024,11 @@ __global__ void k_pattern(const int64_t *__restrict__ vl_ptr, const int2 *__rest
 // separates searchlights, so every sum runs in ascending searchlight order on every run.
 //   CSR (row v = dense row v):   val(v, u_b) += w_s[a] * scale_s * T_s[a][b]
 //   CSC (column v):              val(u_b, v) += w_s[b] * scale_s * T_s[b][a]
+template <typename TT>
 __global__ void __launch_bounds__(256) k_reduce(const int64_t *__restrict__ vl_ptr, const int2 *__restrict__ vl_ent,
                                                 const int32_t *__restrict__ sl_off, const int32_t *__restrict__ sl_idx,
                                                 const double *__restrict__ wts, const int64_t *__restrict__ pat_ptr,
-                                                const int32_t *__restrict__ pat_col, const float *__restrict__ Tscr,
+                                                const int32_t *__restrict__ pat_col, const TT *__restrict__ Tscr,
                                                 const int64_t *__restrict__ tofs_by_slot,
                                                 const double *__restrict__ scale_by_slot, int s_lo, int s_hi,
                                                 int csc, int smem_cap, double *__restrict__ values) {
@@ -1068,7 +1069,7 @@ __global__ void __launch_bounds__(256) k_reduce(const int64_t *__restrict__ vl_p
 		const int o0 = sl_off[s];
 		const int n = sl_off[s + 1] - o0;
 		const int slot = s - s_lo;
-		const float *M = Tscr + tofs_by_slot[slot] + (int64_t)a * n;
+		const TT *M = Tscr + tofs_by_slot[slot] + (int64_t)a * n;
 		const double sc = scale_by_slot[slot];
 		const double wa = wts ? wts[o0 + a] : 1.0;
 		for (int b = threadIdx.x; b < n; b += blockDim.x) {
@@ -1085,6 +1086,133 @@ __global__ void __launch_bounds__(256) k_reduce(const int64_t *__restrict__ vl_p
 	}
 	if (in_smem) {
 		for (int k = threadIdx.x; k < L; k += blockDim.x) values[p0 + k] = acc[k];
+	}
+}
+
+// ---------------------------------------------------------------------------------------------
+// ridge  beta_s = (X_s^T X_s + alpha I)^-1 X_s^T Y_s   (csrc/ha_ridge.c:13-54, float64)
+// ---------------------------------------------------------------------------------------------
+// The reference computes V diag(s / (alpha + s^2)) U^T Y from the thin SVD X_s = U diag(s) V^T;
+// for alpha > 0 that is exactly the solution of the regularised normal equations, solved here
+// by a Cholesky factorisation of G + alpha I (G = X_s^T X_s in the A scratch, column-major) and
+// two triangular solves with the n right-hand sides X_s^T Y_s (in the V scratch, column-major:
+// column j holds right-hand side j).  One CTA per searchlight, float64 throughout, the factor
+// overwriting G in place.  beta is written (float64) in the T layout: row-major for CSR output
+// (row i = source vertex i), column-major for CSC output.  A non-positive pivot (alpha = 0 with a
+// rank-deficient X_s) marks the searchlight kFlagUnconverged and writes zeros.
+__global__ void __launch_bounds__(256) k_ridge_chol(const SlWork *__restrict__ work, double *__restrict__ Gscr,
+                                                    double *__restrict__ Rscr, double *__restrict__ Bout, double alpha,
+                                                    int t_rowmajor, SlStats *__restrict__ stats) {
+	const SlWork w = work[blockIdx.x];
+	const int n = w.n;
+	double *G = Gscr + w.aofs;  // G[c * n + r] = G(r, c); lower triangle used
+	double *R = Rscr + w.aofs;  // R[j * n + i] = rhs(i, j)
+	__shared__ int bad;
+	__shared__ double piv;
+	if (threadIdx.x == 0) bad = 0;
+	for (int k = threadIdx.x; k < n; k += blockDim.x) G[(int64_t)k * n + k] += alpha;
+	__syncthreads();
+	// right-looking Cholesky, column k at a time
+	for (int k = 0; k < n; k++) {
+		if (threadIdx.x == 0) {
+			double d = G[(int64_t)k * n + k];
+			if (!(d > 0.0)) {
+				bad = 1;
+				d = 1.0;
+			}
+			piv = sqrt(d);
+			G[(int64_t)k * n + k] = piv;
+		}
+		__syncthreads();
+		const double p = piv;
+		for (int r = k + 1 + threadIdx.x; r < n; r += blockDim.x) G[(int64_t)k * n + r] /= p;
+		__syncthreads();
+		const int m = n - k - 1;
+		for (int64_t e = threadIdx.x; e < (int64_t)m * m; e += blockDim.x) {
+			const int c = k + 1 + (int)(e / m), r = k + 1 + (int)(e % m);
+			if (r >= c) G[(int64_t)c * n + r] -= G[(int64_t)k * n + r] * G[(int64_t)k * n + c];
+		}
+		__syncthreads();
+	}
+	// forward solve L Z = rhs (all n right-hand sides), Z over R
+	for (int k = 0; k < n; k++) {
+		const double lkk = G[(int64_t)k * n + k];
+		for (int j = threadIdx.x; j < n; j += blockDim.x) R[(int64_t)j * n + k] /= lkk;
+		__syncthreads();
+		const int m = n - k - 1;
+		for (int64_t e = threadIdx.x; e < (int64_t)m * n; e += blockDim.x) {
+			const int j = (int)(e / m), r = k + 1 + (int)(e % m);
+			R[(int64_t)j * n + r] -= G[(int64_t)k * n + r] * R[(int64_t)j * n + k];
+		}
+		__syncthreads();
+	}
+	// backward solve L^T beta = Z
+	for (int k = n - 1; k >= 0; k--) {
+		const double lkk = G[(int64_t)k * n + k];
+		for (int j = threadIdx.x; j < n; j += blockDim.x) R[(int64_t)j * n + k] /= lkk;
+		__syncthreads();
+		for (int64_t e = threadIdx.x; e < (int64_t)k * n; e += blockDim.x) {
+			const int j = (int)(e / k), r = (int)(e % k);
+			R[(int64_t)j * n + r] -= G[(int64_t)r * n + k] * R[(int64_t)j * n + k];
+		}
+		__syncthreads();
+	}
+	double *Bo = Bout + w.tofs;
+	const int64_t ti = t_rowmajor ? n : 1, tj = t_rowmajor ? 1 : n;
+	for (int64_t e = threadIdx.x; e < (int64_t)n * n; e += blockDim.x) {
+		const int j = (int)(e / n), i = (int)(e % n);
+		Bo[i * ti + j * tj] = bad ? 0.0 : R[e];
+	}
+	if (threadIdx.x == 0) {
+		SlStats st = stats[w.slot];
+		st.s_sum = 0.0;
+		st.flags = bad ? (kFlagUnconverged | kFlagFP64) : kFlagFP64;
+		stats[w.slot] = st;
+	}
+}
+
+// ---------------------------------------------------------------------------------------------
+// template loop helpers (csrc/ha_template.c:14-114 with searchlight solves)
+// ---------------------------------------------------------------------------------------------
+
+// out[:, c] = sum_k vals[ptr[c] + k] * X[:, col[ptr[c] + k]]  for every column c, i.e. X @ T with T
+// given in CSC order over the symmetric pattern.  X, out: float64 vertex-major [nv][nt].  One
+// CTA per output column, threads over time samples; the sum runs in pattern order.
+__global__ void k_spmm_csc(const double *__restrict__ X, int nt, int nv, const int64_t *__restrict__ ptr,
+                           const int32_t *__restrict__ col, const double *__restrict__ vals, double *__restrict__ out) {
+	const int c = blockIdx.x;
+	const int64_t k0 = ptr[c], k1 = ptr[c + 1];
+	for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+		double acc = 0.0;
+		for (int64_t k = k0; k < k1; k++) acc += vals[k] * X[(int64_t)col[k] * nt + t];
+		out[(int64_t)c * nt + t] = acc;
+	}
+}
+
+// One-pass column z-score of csrc/ha_linalg.c:263-291 (population variance from E[x^2] - m^2,
+// var < 1e-30 -> the column becomes 0), float64, one thread per column summing in time order.
+__global__ void k_zscore_cols(double *__restrict__ X, int nt, int nv) {
+	const int v = blockIdx.x * blockDim.x + threadIdx.x;
+	if (v >= nv) return;
+	double *x = X + (int64_t)v * nt;
+	double s = 0.0, s2 = 0.0;
+	for (int i = 0; i < nt; i++) {
+		s = __dadd_rn(s, x[i]);
+		s2 = __dadd_rn(s2, __dmul_rn(x[i], x[i]));
+	}
+	const double inv_m = 1.0 / nt;
+	const double mean = __dmul_rn(s, inv_m);
+	const double var = __dsub_rn(__dmul_rn(s2, inv_m), __dmul_rn(mean, mean));
+	const double is = (var < 1e-30) ? 0.0 : 1.0 / sqrt(var);
+	for (int i = 0; i < nt; i++) x[i] = __dmul_rn(__dsub_rn(x[i], mean), is);
+}
+
+// y = a * (x + b * z) elementwise over n entries (z may be null: y = a * x)
+__global__ void k_axpbz(double *__restrict__ y, const double *__restrict__ x, const double *__restrict__ z, double a,
+                        double b, int64_t n) {
+	for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+		const double v = z ? __dadd_rn(x[e], __dmul_rn(b, z[e])) : x[e];
+		y[e] = __dmul_rn(a, v);
 	}
 }
 

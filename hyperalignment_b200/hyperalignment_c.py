@@ -128,3 +128,25 @@ def searchlight_ridge_csc(X, Y, sls, indptr, indices, data, alpha, weights=None)
 
 def cleanup():
     L.lib().ha_b200_cleanup()
+
+
+def searchlight_template(dms, sls, dists, radius, reflection=True, scaling=False, zscore_common=True,
+                         level2_iter=1):
+    """Searchlight Procrustes template of subjects ``dms`` (list of nt x nv arrays), on the GPU.
+
+    The loop of the reference's ``ha_template_procrustes`` (csrc/ha_template.c:14-114) with each
+    whole-matrix Procrustes replaced by a searchlight solve; returns the nt x nv template.
+    """
+    lib = _init()
+    ns = len(dms)
+    nt, nv = dms[0].shape
+    stack = np.empty((ns, nv, nt), dtype=np.float64)  # each subject column-major
+    for s, D in enumerate(dms):
+        stack[s] = np.asarray(D, dtype=np.float64).T
+    idx, offsets, d = _flatten(sls, dists)
+    out = np.empty((nv, nt), dtype=np.float64)
+    L.check(lib.ha_searchlight_template_b200(
+        L.dptr(stack), ns, nt, nv, L.iptr(idx), L.iptr(offsets), L.dptr(d), len(sls), float(radius),
+        bool(reflection), bool(scaling), bool(zscore_common), int(level2_iter), L.dptr(out)),
+        "ha_searchlight_template_b200")
+    return np.ascontiguousarray(out.T)

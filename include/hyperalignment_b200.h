@@ -168,6 +168,27 @@ int ha_searchlight_ridge_csc_b200(
 	const int32_t *indptr, const int32_t *indices, int64_t nnz, double *data,
 	double alpha, bool col_major);
 
+/*
+ * Searchlight Procrustes template (the loop of ha_template_procrustes, csrc/ha_template.c:14-114,
+ * with every whole-matrix Procrustes replaced by a searchlight solve and aligned = X @ T taken
+ * as a sparse product over the searchlight pattern):
+ *   common = X_0; for s = 1..n_subj-1: T = SL(X_s -> common), A_s = X_s @ T, [zscore A_s],
+ *   common = (common + A_s) / 2, [zscore common];
+ *   level2_iter times: sum = sum_s A_s; for s: ref = (sum - A_s) / (n_subj - 1), [zscore ref],
+ *   A_s = X_s @ SL(X_s -> ref);
+ *   tpl = sum_s A_s, then zscore (isZscoreCommon) or / n_subj.
+ * dms: n_subj consecutive nt x nv float64 column-major matrices (host); tpl_out: nt x nv
+ * float64 column-major (host, overwritten).  Searchlights, weights and flags as in
+ * ha_searchlight_procrustes_dense; z-scores use the one-pass rule of ha_zscore_columns
+ * (csrc/ha_linalg.c:263-291).
+ */
+int ha_searchlight_template_b200(
+	const double *dms, int32_t n_subj, int32_t nt, int32_t nv,
+	const int32_t *sl_indices, const int32_t *sl_offsets, const double *sl_dists,
+	int32_t count, double radius,
+	bool isReflection, bool isScaling, bool isZscoreCommon, int32_t level2_iter,
+	double *tpl_out);
+
 /* ---- device-resident plan (repeated calls on one searchlight geometry) ---- */
 
 typedef struct HaB200Plan HaB200Plan;

@@ -215,3 +215,39 @@ def dense_to_csc_values(T_dense, indptr, indices):
 def dense_to_csr_values(T_dense, indptr, indices):
     rows = np.repeat(np.arange(len(indptr) - 1), np.diff(indptr))
     return T_dense[rows, indices]
+
+
+# ---------------------------------------------------------------------------------------------
+# searchlight template loop (csrc/ha_template.c:14-114, each ha_procrustes -> searchlight solve)
+# ---------------------------------------------------------------------------------------------
+
+def searchlight_template(dms, idx, off, dists, radius, reflection=True, scaling=False, zscore_common=True,
+                         level2_iter=1):
+    """Sequential running-average template plus leave-one-out passes; aligned = X @ T_searchlight."""
+    ns = len(dms)
+
+    def solve(X, Y):
+        return searchlight_procrustes_dense(X, Y, idx, off, dists, radius, reflection, scaling)
+
+    common = dms[0].copy()
+    aligned = [dms[0].copy()] + [None] * (ns - 1)
+    for s in range(1, ns):  # csrc/ha_template.c:39-59
+        aligned[s] = dms[s] @ solve(dms[s], common)
+        if zscore_common:
+            aligned[s] = zscore_columns(aligned[s])
+        common = (common + aligned[s]) * 0.5
+        if zscore_common:
+            common = zscore_columns(common)
+    for _ in range(level2_iter):  # csrc/ha_template.c:62-89
+        total = aligned[0].copy()
+        for s in range(1, ns):
+            total = total + aligned[s]
+        for s in range(ns):
+            ref = (total - aligned[s]) * (1.0 / (ns - 1))
+            if zscore_common:
+                ref = zscore_columns(ref)
+            aligned[s] = dms[s] @ solve(dms[s], ref)
+    tpl = aligned[0].copy()  # csrc/ha_template.c:92-103
+    for s in range(1, ns):
+        tpl = tpl + aligned[s]
+    return zscore_columns(tpl) if zscore_common else tpl * (1.0 / ns)

@@ -158,3 +158,13 @@ def test_oracle_vs_live_reference():
     a = O.searchlight_procrustes_dense(w.X, w.Y, s.indices, s.offsets, s.dists, s.radius, False, True)
     b = R.procrustes_dense(w.X, w.Y, s.indices, s.offsets, s.dists, s.radius, False, True, 0, threads=1)
     np.testing.assert_allclose(a, b, atol=1e-10, rtol=0)
+
+
+def test_template_identical_subjects_oracle():
+    """Searchlight form of csrc/ha_test.c:503-537: identical subjects give the input back."""
+    from hyperalignment_b200 import workloads as W
+    _, sls, subj = W.hemisphere_subjects(seed=4, nv=162, nt=60, n_subj=3, size_lo=8, size_hi=20)
+    base = subj[0]
+    tpl = O.searchlight_template([base, base.copy(), base.copy()], sls.indices, sls.offsets, sls.dists, sls.radius,
+                                 True, False, False, 1)
+    assert np.abs(tpl - base).max() < 1e-8

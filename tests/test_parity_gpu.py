@@ -254,3 +254,60 @@ def test_full_size_template_pair_properties(gpu):
         got = np.zeros(w.nv)
         got[indices[indptr[r]:indptr[r + 1]]] = vals[indptr[r]:indptr[r + 1]]
         assert relf(got, row) <= GLOBAL_REL * 10
+
+
+# ---------------------------------------------------------------------------------------------
+# ridge (csrc/ha_searchlight.c:1378-1429, csrc/ha_ridge.c:13-54), float64
+# ---------------------------------------------------------------------------------------------
+
+RIDGE_REL = 1e-9  # float64 Cholesky vs the reference's SVD formula
+
+
+def test_ridge_csc_matches_reference_golden(gpu):
+    g = golden("small_sparse.npz")
+    sls = sls_lists(g["idx"], g["off"])
+    ws = sls_lists(g["weights"], g["off"])
+    data = np.zeros(g["indices"].size)
+    H.searchlight_ridge_csc(g["X"], g["Y"], sls, g["indptr"], g["indices"], data, float(g["ridge_alpha"]), weights=ws)
+    assert relf(data, g["data_ridge"]) <= RIDGE_REL
+
+
+@pytest.mark.parametrize("alpha", [1e-3, 1.0, 1e3])
+@pytest.mark.parametrize("lo,hi", [(5, 30), (100, 260)])
+def test_ridge_csc_vs_oracle(gpu, alpha, lo, hi):
+    w = W.small_case(seed=13, nv=642, nt=300, lo=lo, hi=hi)
+    s = w.sls
+    indptr, indices = H.sparse_pattern(sls_lists(s.indices, s.offsets), w.nv)
+    wts = O.searchlight_weights(s.indices, s.offsets, s.dists, s.radius, w.nv)
+    data = np.zeros(indices.size)
+    H.searchlight_ridge_csc(w.X, w.Y, sls_lists(s.indices, s.offsets), indptr, indices, data, alpha,
+                            weights=sls_lists(wts, s.offsets))
+    ref = O.searchlight_ridge_csc(w.X, w.Y, s.indices, s.offsets, indptr, indices, np.zeros(indices.size), alpha, wts)
+    assert relf(data, ref) <= RIDGE_REL
+
+
+# ---------------------------------------------------------------------------------------------
+# template loop (csrc/ha_template.c:14-114 with searchlight solves)
+# ---------------------------------------------------------------------------------------------
+
+TEMPLATE_REL = 1e-4  # several chained solves, each within 1e-5 of float64
+
+
+@pytest.mark.parametrize("zscore,level2,scal", [(True, 1, True), (False, 0, False), (True, 2, False)])
+def test_template_vs_oracle(gpu, zscore, level2, scal):
+    _, sls, subj = W.hemisphere_subjects(seed=3, nv=162, nt=40, n_subj=4, size_lo=8, size_hi=24)
+    s = sls
+    tpl = H.searchlight_template(subj, sls_lists(s.indices, s.offsets), sls_lists(s.dists, s.offsets), s.radius,
+                                 True, scal, zscore, level2)
+    ref = O.searchlight_template(subj, s.indices, s.offsets, s.dists, s.radius, True, scal, zscore, level2)
+    assert relf(tpl, ref) <= TEMPLATE_REL
+
+
+def test_template_identical_subjects(gpu):
+    # searchlight form of csrc/ha_test.c:503-537: identical subjects, no z-scoring -> the input back
+    _, sls, subj = W.hemisphere_subjects(seed=4, nv=162, nt=60, n_subj=3, size_lo=8, size_hi=20)
+    base = subj[0]
+    s = sls
+    tpl = H.searchlight_template([base, base.copy(), base.copy()], sls_lists(s.indices, s.offsets),
+                                 sls_lists(s.dists, s.offsets), s.radius, True, False, False, 1)
+    assert np.abs(tpl - base).max() < 1e-4
