@@ -127,23 +127,42 @@ size_t jacobi_smem(int b, int ld, size_t rb) {
 // Jacobi block layout for a searchlight of n vertices in a given precision: resident (two
 // blocks covering all columns stay in shared memory) when it fits, else blocked with the
 // widest block that fits.
-void jacobi_layout(int n, bool fp64, int &bsz, int &nblk, size_t &smem) {
+void jacobi_layout(int n, bool fp64, int &bsz, int &nblk, size_t &smem, size_t budget) {
 	const size_t rb = real_bytes(fp64);
 	const int ld = 32 * std::max(1, rpl_for(n));
 	int h = (n + 1) / 2;
 	size_t res = jacobi_smem(h, ld, rb);
-	if (res <= kSmemMax) {
+	if (res <= budget) {
 		bsz = h;
 		nblk = 2;
 		smem = res;
 		return;
 	}
 	int b = 32;
-	while (b > 1 && jacobi_smem(b, ld, rb) > kSmemMax) b--;
+	while (b > 1 && jacobi_smem(b, ld, rb) > budget) b--;
 	bsz = b;
 	nblk = (n + b - 1) / b;
 	if (nblk & 1) nblk++;
 	smem = jacobi_smem(b, ld, rb);
+}
+
+void jacobi_layout(int n, bool fp64, int &bsz, int &nblk, size_t &smem) {
+	jacobi_layout(n, fp64, bsz, nblk, smem, kSmemMax);
+}
+
+// Shared-memory budget of the plan's FP32 Jacobi buckets: small enough for two CTAs per SM
+// (the float instances are register-bounded to two 512-thread CTAs), so more searchlights run
+// in blocked mode through L2 but twice as many warps hide the rotation latencies.
+// HA_B200_JACOBI_SMEM_KB overrides it (upper bound 220).
+size_t fp32_jacobi_budget() {
+	static size_t b = 0;
+	if (!b) {
+		const char *e = getenv("HA_B200_JACOBI_SMEM_KB");
+		double kb = e ? atof(e) : 110.0;
+		if (!(kb >= 16.0)) kb = 110.0;
+		b = std::min(kSmemMax, (size_t)(kb * 1024.0));
+	}
+	return b;
 }
 
 struct Bucket {
@@ -327,7 +346,7 @@ int build_chunks(HaB200Plan *P) {
 			int n = P->h_off[s + 1] - P->h_off[s];
 			int b32, k32, b64, k64;
 			size_t m32, m64;
-			jacobi_layout(n, false, b32, k32, m32);
+			jacobi_layout(n, false, b32, k32, m32, fp32_jacobi_budget());
 			jacobi_layout(n, true, b64, k64, m64);
 			int64_t e32 = ((int64_t)n * k32 * b32 * 4 + 7) / 8;
 			int64_t e64 = (int64_t)n * k64 * b64;
@@ -383,7 +402,7 @@ int build_chunks(HaB200Plan *P) {
 				while (j < (int)items.size() && key(items[j]) == key(items[i])) {
 					int bb, kk;
 					size_t mm;
-					jacobi_layout(items[j].n, prec == 1, bb, kk, mm);
+					jacobi_layout(items[j].n, prec == 1, bb, kk, mm, prec == 1 ? kSmemMax : fp32_jacobi_budget());
 					smem = std::max(smem, mm);
 					j++;
 				}

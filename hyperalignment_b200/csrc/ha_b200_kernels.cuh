@@ -261,15 +261,19 @@ __device__ __forceinline__ Real jacobi_pairs(Real *B, Real *V, Real *nrm, const 
 	Real x[JPW][RPL], y[JPW][RPL], g[JPW];
 #pragma unroll
 	for (int k = 0; k < JPW; k++) {
-		g[k] = 0;
+		Real g0 = 0, g1 = 0;  // two partial sums halve the dependency chain
 		const Real *bp = B + p[k] * LD + lane;
 		const Real *bq = B + q[k] * LD + lane;
 #pragma unroll
 		for (int r = 0; r < RPL; r++) {
 			x[k][r] = bp[32 * r];
 			y[k][r] = bq[32 * r];
-			g[k] += x[k][r] * y[k][r];
+			if (r & 1)
+				g1 += x[k][r] * y[k][r];
+			else
+				g0 += x[k][r] * y[k][r];
 		}
+		g[k] = g0 + g1;
 	}
 #pragma unroll
 	for (int o = 16; o > 0; o >>= 1)

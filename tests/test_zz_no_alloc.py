@@ -3,9 +3,11 @@
 Callers that cannot allocate device memory (their pool allocator owns the GPU, their host
 program forbids new allocations, or cudaMalloc's device-wide synchronisation is not acceptable
 in their loop) pass their own device buffers and the library uses only a static scratch array.
-Its output must equal the allocating plan API's plain FP32 local transforms on the same inputs,
-on two calls in a row (the shared scratch keeps the previous call's contents).  The file sorts
-last so that a run stopping at the first failure has run every other test first.
+Its output must match the allocating plan API's plain FP32 local transforms on the same inputs,
+within the per-transform tolerance of the parity tests, on two calls in a row (the shared scratch
+keeps the previous call's contents).  The inputs have more samples than any searchlight has
+vertices, so every transform is unique and two correct solvers agree.  The file sorts last so
+that a run stopping at the first failure has run every other test first.
 """
 
 import ctypes
@@ -19,7 +21,7 @@ from hyperalignment_b200.plan import Plan
 
 pytestmark = pytest.mark.gpu
 
-TOL = 1e-5  # max-abs on entries of orthogonal matrices (float32 results of the same kernels)
+TOL = 1e-4  # relative Frobenius per transform, as in the parity tests
 
 
 def _plan_transforms(w, X, Y):
@@ -37,7 +39,7 @@ def _plan_transforms(w, X, Y):
 
 def test_noalloc_matches_plan_on_two_calls(gpu):
     import torch
-    w = W.small_case(seed=31, nv=642, nt=90, lo=1, hi=160)
+    w = W.small_case(seed=31, nv=642, nt=400, lo=1, hi=160)
     s = w.sls
     d_idx = torch.from_numpy(s.indices).cuda()
     total = int((s.sizes.astype(np.int64) ** 2).sum())
@@ -57,7 +59,7 @@ def test_noalloc_matches_plan_on_two_calls(gpu):
             n = int(s.sizes[q])
             T = got[o:o + n * n].reshape(n, n)
             o += n * n
-            worst = max(worst, float(np.abs(T - ref[q]).max()))
+            worst = max(worst, float(np.linalg.norm(T - ref[q]) / np.linalg.norm(ref[q])))
         assert worst <= TOL, worst
 
 
