@@ -510,6 +510,7 @@ struct JacobiParams {
 	int max_sweeps;
 	int t_rowmajor;
 	double ill_ratio;  // sigma_min / sigma_max below this -> kFlagIllCond
+	double weak;       // columns with sigma <= weak * eps * sigma_max are re-orthogonalised / completed
 	int only_flagged;  // process only searchlights whose stats carry kFlagIllCond (FP64 re-solve)
 };
 
@@ -699,7 +700,7 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) k_jacobi(const
 	// 1/(2n) is accepted, else the best one.  Executed by warp 0.
 	{
 		const Real smax = (Real)stats[w.slot].s_max;
-		const Real weak = smax * Real(1000) * eps;
+		const Real weak = smax * Real(prm.weak) * eps;
 		if (warp == 0) {
 			for (int c = 0; c < n; c++) {
 				if (sg[c] > weak) continue;

@@ -201,7 +201,8 @@ enum {
 
 /* Solver variants. */
 enum {
-	kHaB200SolverMixed = 0, /* FP32 Jacobi + FP32 Newton-Schulz refinement, FP64 re-solve of ill-conditioned searchlights */
+	kHaB200SolverMixed = 0, /* FP32 Jacobi + FP32 Newton-Schulz refinement, FP64 re-solve of searchlights
+	                           with sigma_min / sigma_max < 5e-5 (environment HA_B200_ILL_RATIO overrides) */
 	kHaB200SolverFP32  = 1, /* plain FP32 form: FP32 Jacobi only, no refinement, no FP64 re-solve */
 	kHaB200SolverFP64  = 2, /* every searchlight in FP64 */
 };

@@ -311,3 +311,27 @@ def test_template_identical_subjects(gpu):
     tpl = H.searchlight_template([base, base.copy(), base.copy()], sls_lists(s.indices, s.offsets),
                                  sls_lists(s.dists, s.offsets), s.radius, True, False, False, 1)
     assert np.abs(tpl - base).max() < 1e-4
+
+
+def test_mixed_form_accuracy_at_full_size(gpu):
+    """Template workload (10242 searchlights of 100-300): the mixed form's FP64 re-solve threshold
+    keeps every checked transform within 1e-4 of float64, including the 150 worst-conditioned."""
+    import torch
+    w = W.template_procrustes_pair(seed=0)
+    plan = Plan.from_workload(w)
+    dX = torch.from_numpy(np.asfortranarray(w.X).ravel(order="F")).cuda()
+    dY = torch.from_numpy(np.asfortranarray(w.Y).ravel(order="F")).cuda()
+    vals = torch.zeros(plan.nnz, dtype=torch.float64, device="cuda")
+    plan.procrustes_device(dX.data_ptr(), dY.data_ptr(), vals.data_ptr(), True, False, L.SOLVER_MIXED, L.OUT_CSR)
+    torch.cuda.synchronize()
+    st = plan.searchlight_stats(0, w.sls.count)
+    ratio = st["s_min"] / st["s_max"]
+    rng = np.random.default_rng(7)
+    pick = np.unique(np.concatenate([np.argsort(ratio)[:150], rng.choice(w.sls.count, 50, replace=False)]))
+    worst = 0.0
+    for q in pick:
+        T = plan.local_transforms(int(q), 1)[0]
+        sl = w.sls.indices[w.sls.offsets[q]:w.sls.offsets[q + 1]]
+        worst = max(worst, relf(T, O.procrustes(w.X[:, sl], w.Y[:, sl])))
+    assert worst <= T_REL, worst
+    assert 0 < plan.stats()["n_fp64"] < 0.1 * w.sls.count
