@@ -224,7 +224,7 @@ __global__ void __launch_bounds__(256) k_xcov(const SlWork *__restrict__ work, c
 // Pairs processed together by one warp (their reductions overlap), by rows per lane.
 template <int RPL>
 struct PairsPerWarp {
-	static constexpr int value = RPL <= 2 ? 4 : (RPL <= 5 ? 2 : 1);
+	static constexpr int value = RPL <= 4 ? 4 : (RPL <= 8 ? 2 : 1);
 };
 
 // circle method: pair k of round r among m players (m even); no integer division
@@ -240,6 +240,21 @@ __device__ __forceinline__ void rr_pair(int m, int r, int k, int &p, int &q) {
 		if (q < 0) q += mm;
 	}
 }
+
+// Rotation parameters: the hardware reciprocal square root and fast division in float32 (a
+// rotation only needs c^2 + s^2 = 1 to working precision, which c = rsqrt(1 + t^2), s = c t
+// keeps); IEEE operations in float64.
+__device__ __forceinline__ float rot_rsqrt(float x) { return rsqrtf(x); }
+__device__ __forceinline__ double rot_rsqrt(double x) { return 1.0 / sqrt(x); }
+__device__ __forceinline__ float rot_div(float a, float b) { return __fdividef(a, b); }
+// c = 1 / sqrt(x) to full float32 precision (hardware estimate + one Newton step), so that
+// c^2 + s^2 = 1 holds to rounding and V stays orthogonal over thousands of rotations
+__device__ __forceinline__ float rot_cos(float x) {
+	const float y = rsqrtf(x);
+	return y * fmaf(-0.5f * x * y, y, 1.5f);
+}
+__device__ __forceinline__ double rot_cos(double x) { return 1.0 / sqrt(x); }
+__device__ __forceinline__ double rot_div(double a, double b) { return a / b; }
 
 template <typename Real>
 struct JacobiTol {
@@ -290,11 +305,11 @@ __device__ __forceinline__ Real jacobi_pairs(Real *B, Real *V, Real *nrm, const 
 			if (lane == k) { pk = p[k]; qk = q[k]; gk = g[k]; }
 		const Real al = nrm[pk], be = nrm[qk];
 		if (al > tol.zero2 && be > tol.zero2) {
-			mycos = real_abs(gk) / (real_sqrt(al) * real_sqrt(be));
+			mycos = real_abs(gk) * rot_rsqrt(al) * rot_rsqrt(be);
 			if (mycos > tol.rot) {
-				const Real zeta = (be - al) / (2 * gk);
-				const Real t = ((zeta >= 0) ? Real(1) : Real(-1)) / (real_abs(zeta) + real_sqrt(Real(1) + zeta * zeta));
-				myc = Real(1) / real_sqrt(Real(1) + t * t);
+				const Real zeta = rot_div(be - al, 2 * gk);
+				const Real t = rot_div((zeta >= 0) ? Real(1) : Real(-1), real_abs(zeta) + real_sqrt(Real(1) + zeta * zeta));
+				myc = rot_cos(Real(1) + t * t);
 				mys = myc * t;
 				mydo = 1;
 				nrm[pk] = al - t * gk;
