@@ -375,7 +375,11 @@ def run_b200(args):
         with open(traffic_file) as f:
             tr = json.load(f)
         if dom_name in tr:
-            roof["traffic"] = tr[dom_name].get("bytes_per_launch")
+            per_sl = tr[dom_name].get("bytes_per_searchlight")
+            if per_sl:
+                # ncu capture of a smaller case scaled to a full launch by the searchlights it solves
+                roof["traffic"] = per_sl * w.sls.count * K / max(1, cnt[dom])
+                roof["traffic_source"] = tr[dom_name].get("source")
     kernel_share = {L.KERNEL_KINDS[i]: {"ms_per_step": float(ms[i] / K), "launches_per_step": float(cnt[i] / K)}
                     for i in range(len(ms)) if cnt[i] > 0}
 
