@@ -43,6 +43,14 @@ SIGNATURES = {
     "ha_searchlight_ridge_csc_b200": (ctypes.c_int, [
         c_double_p, c_double_p, ctypes.c_int32, ctypes.c_int32, c_int32_p, c_int32_p, ctypes.c_int32,
         c_double_p, c_int32_p, c_int32_p, ctypes.c_int64, c_double_p, ctypes.c_double, ctypes.c_bool]),
+    "ha_searchlight_ridge_grid_b200": (ctypes.c_int, [
+        c_double_p, c_double_p, ctypes.c_int32, ctypes.c_int32, c_int32_p, c_int32_p, ctypes.c_int32,
+        c_double_p, c_int32_p, c_int32_p, ctypes.c_int64, c_double_p, c_double_p, ctypes.c_int32, c_int32_p,
+        ctypes.c_int32, ctypes.POINTER(c_int32_p), ctypes.POINTER(c_int32_p), c_int32_p, c_int32_p, ctypes.c_int32,
+        c_int32_p, c_double_p, ctypes.c_bool]),
+    "ha_ensemble_indices_b200": (ctypes.c_int, [
+        ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_uint64,
+        ctypes.POINTER(ctypes.c_bool), c_int32_p, c_int32_p, c_int32_p]),
     "ha_searchlight_template_b200": (ctypes.c_int, [
         c_double_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, c_int32_p, c_int32_p, c_double_p, ctypes.c_int32,
         ctypes.c_double, ctypes.c_bool, ctypes.c_bool, ctypes.c_bool, ctypes.c_int32, c_double_p]),
@@ -64,6 +72,10 @@ SIGNATURES = {
     "ha_b200_plan_ridge_device": (ctypes.c_int, [
         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_void_p,
         ctypes.c_void_p]),
+    "ha_b200_plan_ridge_grid_device": (ctypes.c_int, [
+        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, c_double_p, ctypes.c_int32, c_int32_p, ctypes.c_int32,
+        ctypes.POINTER(c_int32_p), ctypes.POINTER(c_int32_p), c_int32_p, c_int32_p, ctypes.c_int32, ctypes.c_int,
+        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "ha_b200_plan_local_transforms": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, c_float_p]),
     "ha_b200_local_procrustes_noalloc": (ctypes.c_int, [
         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, c_int32_p, ctypes.c_int32,
@@ -74,7 +86,7 @@ SIGNATURES = {
 }
 
 KERNEL_KINDS = ["convert", "colvar", "xcov32", "jacobi32", "formT32", "xcov64", "jacobi64", "formT64", "refine",
-                "reflect", "scale", "reduce", "pattern", "ridge"]
+                "reflect", "scale", "reduce", "pattern", "ridge", "grid"]
 
 # Error codes and enum values (include/hyperalignment_b200.h, same as the reference's ha_common.h).
 SUCCESS, ERROR_ALLOC, ERROR_SVD, ERROR_ARG, ERROR_INTERNAL = 0, -1, -2, -3, -4
@@ -112,3 +124,17 @@ def dptr(a):
 
 def iptr(a):
     return None if a is None else a.ctypes.data_as(c_int32_p)
+
+
+class IndexLists:
+    """Lists of int32 row arrays as the C ``const int32_t *const *`` + sizes pair (kept alive here)."""
+
+    def __init__(self, lists):
+        import numpy as np
+        self.arrays = [np.ascontiguousarray(a, dtype=np.int32) for a in lists]
+        self.keep = [a if a.size else np.zeros(1, dtype=np.int32) for a in self.arrays]
+        self.ptrs = (c_int32_p * len(self.keep))(*[iptr(a) for a in self.keep])
+        self.sizes = np.array([a.size for a in self.arrays], dtype=np.int32)
+
+    def __len__(self):
+        return len(self.arrays)

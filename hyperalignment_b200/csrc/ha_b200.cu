@@ -8,6 +8,7 @@
 
 #include "../../include/hyperalignment_b200.h"
 #include "ha_b200_kernels.cuh"
+#include "ha_b200_grid.cuh"
 
 #include <cuda_runtime.h>
 #include <omp.h>
@@ -252,6 +253,11 @@ struct HaB200Plan {
 	DevArr<float> X32, Y32;
 	DevArr<double> var;
 	DevArr<int32_t> counters;  // [n_fp64, n_unconverged]
+	// ridge grid search: scratch and the uploaded grid / CV description, allocated on first use
+	DevArr<double> gridscr, galpha, gwinv;
+	DevArr<int64_t> gbase;
+	DevArr<int32_t> gnpcs, grows, gtpos, gurows, guntested;
+	DevArr<GridModel> gmdl;
 	int last_chunk = -1;
 	int last_rowmajor = 1;
 };
@@ -645,6 +651,7 @@ int run_procrustes(HaB200Plan *P, const double *d_X, const double *d_Y, bool ref
 		jp.t_rowmajor = rowmajor;
 		jp.ill_ratio = (solver == kHaB200SolverMixed) ? ill_ratio() : 0.0;
 		jp.weak = weak_factor();
+		jp.eig = 0;
 		if (use32) {
 			float *A = reinterpret_cast<float *>(P->scrA.p);
 			float *V = reinterpret_cast<float *>(P->scrV.p);
@@ -728,6 +735,325 @@ int run_ridge(HaB200Plan *P, const double *d_X, const double *d_Y, double alpha,
 	}
 	P->last_chunk = (int)P->chunks.size() - 1;
 	P->last_rowmajor = rowmajor;
+	return kHaSuccess;
+}
+
+// ---- ridge grid search with cross-validated ensembles ----
+
+// Host description of the grid and the CV models (validated), in the layout the grid kernels use.
+struct GridSpec {
+	std::vector<double> alphas;
+	std::vector<int32_t> npcs;
+	std::vector<GridModel> mdl;
+	std::vector<int32_t> rows, tpos, urows, untested;
+	std::vector<double> winv;
+	int mte = 1, ntu = 0;
+};
+
+int grid_spec(int nt, const double *alphas, int n_alphas, const int32_t *npcs, int n_npcs,
+              const int32_t *const *train_li, const int32_t *const *test_li, const int32_t *train_sizes,
+              const int32_t *test_sizes, int n_models, GridSpec &gs) {
+	if (!alphas || !npcs || !train_li || !test_li || !train_sizes || !test_sizes || n_alphas < 1 || n_npcs < 1 ||
+	    n_models < 1)
+		return kHaErrorArg;
+	for (int a = 0; a < n_alphas; a++)
+		if (!std::isfinite(alphas[a])) return kHaErrorArg;
+	for (int p = 0; p < n_npcs; p++)
+		if (npcs[p] < 0) {
+			fprintf(stderr, "ha_b200 ridge grid: negative PC count %d\n", npcs[p]);
+			return kHaErrorArg;
+		}
+	gs.alphas.assign(alphas, alphas + n_alphas);
+	gs.npcs.assign(npcs, npcs + n_npcs);
+	std::vector<int32_t> count((size_t)nt, 0);
+	for (int m = 0; m < n_models; m++) {
+		const int tr = train_sizes[m], te = test_sizes[m];
+		if (tr < 1 || te < 0 || !train_li[m] || (te > 0 && !test_li[m])) return kHaErrorArg;
+		for (int i = 0; i < tr; i++)
+			if (train_li[m][i] < 0 || train_li[m][i] >= nt) return kHaErrorArg;
+		for (int i = 0; i < te; i++) {
+			const int t = test_li[m] ? test_li[m][i] : -1;
+			if (t < 0 || t >= nt) return kHaErrorArg;
+		}
+	}
+	std::vector<int32_t> seen((size_t)nt, -1);
+	for (int m = 0; m < n_models; m++) {
+		for (int i = 0; i < test_sizes[m]; i++) {
+			const int t = test_li[m][i];
+			if (seen[t] == m) {
+				fprintf(stderr, "ha_b200 ridge grid: row %d repeats in the test list of model %d\n", t, m);
+				return kHaErrorArg;
+			}
+			seen[t] = m;
+			count[t]++;
+		}
+	}
+	std::vector<int32_t> upos((size_t)nt, -1);
+	gs.urows.clear();
+	gs.untested.clear();
+	gs.winv.clear();
+	for (int t = 0; t < nt; t++) {
+		if (count[t] > 0) {
+			upos[t] = (int32_t)gs.urows.size();
+			gs.urows.push_back(t);
+			gs.winv.push_back(1.0 / count[t]);
+		} else {
+			gs.untested.push_back(t);
+		}
+	}
+	gs.ntu = (int)gs.urows.size();
+	gs.mdl.resize(n_models);
+	gs.rows.clear();
+	gs.tpos.clear();
+	gs.mte = 1;
+	for (int m = 0; m < n_models; m++) {
+		GridModel md;
+		md.tr_ofs = (int32_t)gs.rows.size();
+		md.tr_n = train_sizes[m];
+		gs.rows.insert(gs.rows.end(), train_li[m], train_li[m] + train_sizes[m]);
+		gs.tpos.resize(gs.rows.size(), -1);
+		md.te_ofs = (int32_t)gs.rows.size();
+		md.te_n = test_sizes[m];
+		for (int i = 0; i < test_sizes[m]; i++) {
+			gs.rows.push_back(test_li[m][i]);
+			gs.tpos.push_back(upos[test_li[m][i]]);
+		}
+		gs.mte = std::max(gs.mte, md.te_n);
+		gs.mdl[m] = md;
+	}
+	return kHaSuccess;
+}
+
+template <typename T>
+int upload_vec(DevArr<T> &d, const std::vector<T> &h, cudaStream_t st) {
+	int rc = d.ensure(std::max<size_t>(h.size(), 1));
+	if (rc != kHaSuccess) return rc;
+	if (!h.empty()) HA_CUDA(cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+	return kHaSuccess;
+}
+
+// Grid scratch budget per sub-batch of searchlights (HA_B200_GRID_GB overrides the default).
+size_t grid_budget_bytes() {
+	const char *e = getenv("HA_B200_GRID_GB");
+	double gb = e ? atof(e) : 8.0;
+	if (!(gb > 0.001)) gb = 8.0;
+	return (size_t)(gb * 1073741824.0);
+}
+
+// Enqueue the searchlight ridge grid search + reduction of the winners' betas over all chunks.
+// Per sub-batch of searchlights (bounded by the grid scratch budget) and CV model: the Gram and
+// cross-covariance over the model's training rows, the float64 Jacobi eigen decomposition of the
+// Gram, and the per-model products; then the grid evaluation and the winner's beta.
+int run_ridge_grid(HaB200Plan *P, const double *d_X, const double *d_Y, const GridSpec &gs, int out_kind,
+                   double *d_vals, int32_t *d_best, double *d_cost, cudaStream_t st) {
+	const int nt = P->nt, nv = P->nv;
+	const int rowmajor = out_kind == kHaB200OutCSR ? 1 : 0;
+	if (P->max_n > kGridMaxN) {
+		fprintf(stderr, "ha_b200 ridge grid: searchlight of %d vertices exceeds the grid limit of %d\n", P->max_n,
+		        kGridMaxN);
+		return kHaErrorArg;
+	}
+	int rc;
+	if (P->chunks.empty() && (rc = build_chunks(P)) != kHaSuccess) return rc;
+	int64_t maxT = 1;
+	for (auto &ch : P->chunks) maxT = std::max(maxT, ch.t_elems);
+	if ((rc = P->scrT64.ensure((size_t)maxT)) != kHaSuccess) return rc;
+	if ((rc = upload_vec(P->galpha, gs.alphas, st)) != kHaSuccess) return rc;
+	if ((rc = upload_vec(P->gnpcs, gs.npcs, st)) != kHaSuccess) return rc;
+	if ((rc = upload_vec(P->gmdl, gs.mdl, st)) != kHaSuccess) return rc;
+	if ((rc = upload_vec(P->grows, gs.rows, st)) != kHaSuccess) return rc;
+	if ((rc = upload_vec(P->gtpos, gs.tpos, st)) != kHaSuccess) return rc;
+	if ((rc = upload_vec(P->gwinv, gs.winv, st)) != kHaSuccess) return rc;
+	if ((rc = upload_vec(P->gurows, gs.urows, st)) != kHaSuccess) return rc;
+	if ((rc = upload_vec(P->guntested, gs.untested, st)) != kHaSuccess) return rc;
+	if ((rc = P->gbase.ensure((size_t)P->max_slots)) != kHaSuccess) return rc;
+	GridParams gp;
+	gp.models = (int)gs.mdl.size();
+	gp.mte = gs.mte;
+	gp.ntu = gs.ntu;
+	gp.n_alphas = (int)gs.alphas.size();
+	gp.n_npcs = (int)gs.npcs.size();
+	gp.nt = nt;
+	gp.n_untested = (int)gs.untested.size();
+	gp.alphas = P->galpha.p;
+	gp.npcs = P->gnpcs.p;
+	gp.mdl = P->gmdl.p;
+	gp.rows = P->grows.p;
+	gp.tpos = P->gtpos.p;
+	gp.winv = P->gwinv.p;
+	gp.urows = P->gurows.p;
+	gp.untested = P->guntested.p;
+	gp.gbase = P->gbase.p;
+	const int grid = gp.n_alphas * gp.n_npcs;
+	const size_t budget = grid_budget_bytes();
+	HA_CUDA(cudaMemsetAsync(P->counters.p, 0, 4 * sizeof(int32_t), st));
+	const int smem_cap = std::min(P->max_row, 16384);
+	const size_t red_smem = (size_t)smem_cap * 12;
+	JacobiParams jp;
+	jp.max_sweeps = 40;
+	jp.t_rowmajor = 0;
+	jp.ill_ratio = 0.0;
+	jp.weak = weak_factor();
+	jp.eig = 1;
+	jp.only_flagged = 0;
+	std::vector<int64_t> gbase;
+	for (size_t c = 0; c < P->chunks.size(); c++) {
+		Chunk &ch = P->chunks[c];
+		const int nsl = ch.s1 - ch.s0;
+		HA_CUDA(cudaMemsetAsync(P->stats.p, 0, (size_t)nsl * sizeof(SlStats), st));
+		const int nitems = (int)ch.w64.size();
+		int i0 = 0;
+		while (i0 < nitems) {
+			gbase.assign((size_t)nsl, 0);
+			int64_t total = 0;
+			int i1 = i0;
+			while (i1 < nitems) {
+				const GridLayout L = GridLayout::make(ch.w64[i1].n, gp.models, gp.mte, gp.ntu, grid);
+				if (i1 > i0 && (size_t)(total + L.total) * 8 > budget) break;
+				gbase[ch.w64[i1].slot] = total;
+				total += L.total;
+				i1++;
+			}
+			if ((rc = P->gridscr.ensure((size_t)total)) != kHaSuccess) return rc;
+			HA_CUDA(cudaMemcpyAsync(P->gbase.p, gbase.data(), (size_t)nsl * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+			double *A = P->scrA.p, *V = P->scrV.p;
+			for (int mo = 0; mo < gp.models; mo++) {
+				const GridModel &md = gs.mdl[mo];
+				const int32_t *tr = P->grows.p + md.tr_ofs;
+				for (const Bucket &b : ch.b64) {
+					const int x0 = std::max(i0, b.first), x1 = std::min(i1, b.first + b.count);
+					if (x1 <= x0) continue;
+					const SlWork *wk = ch.d_w64 + x0;
+					{ HA_LAUNCH(kHaB200KXcov64, st); k_xcov_rows<16><<<x1 - x0, kBlock, 0, st>>>(wk, P->idx.p, d_X, d_X, nt, tr, md.tr_n, A, P->gridscr.p, gp, 0); }
+					{ HA_LAUNCH(kHaB200KXcov64, st); k_xcov_rows<16><<<x1 - x0, kBlock, 0, st>>>(wk, P->idx.p, d_X, d_Y, nt, tr, md.tr_n, A, P->gridscr.p, gp, 1); }
+					{
+						HA_LAUNCH(kHaB200KJacobi64, st);
+						if ((rc = launch_jacobi<double>(b.rpl, x1 - x0, b.threads, b.smem, st, wk, A, V, P->scrT.p, P->stats.p, P->uv.p, jp)) != kHaSuccess)
+							return rc;
+					}
+				}
+				{ HA_LAUNCH(kHaB200KGrid, st); k_grid_model<<<i1 - i0, kBlock, 0, st>>>(ch.d_w64 + i0, P->idx.p, d_X, V, P->uv.p, mo, P->gridscr.p, gp); }
+			}
+			{ HA_LAUNCH(kHaB200KGrid, st); k_grid_eval<<<i1 - i0, kBlock, 0, st>>>(ch.d_w64 + i0, P->idx.p, d_Y, P->gridscr.p, gp, P->scrT64.p, rowmajor, d_best, d_cost); }
+			HA_CUDA(cudaGetLastError());
+			i0 = i1;
+		}
+		{ HA_LAUNCH(kHaB200KScale, st); k_scale<<<(nsl + 127) / 128, 128, 0, st>>>(ch.d_w64, nsl, P->idx.p, nullptr, P->stats.p, nt, 0, P->scale.p); }
+		{ HA_LAUNCH(kHaB200KScale, st); k_count_flags<<<(nsl + 127) / 128, 128, 0, st>>>(P->stats.p, nsl, P->counters.p); }
+		{ HA_LAUNCH(kHaB200KReduce, st); k_reduce<double><<<nv, kBlock, red_smem, st>>>(P->vlptr.p, P->vlent.p, P->off.p, P->idx.p,
+		                                       P->has_weights ? P->w.p : nullptr, P->patptr.p, P->patcol.p, P->scrT64.p,
+		                                       ch.d_tofs, P->scale.p, ch.s0, ch.s1, out_kind == kHaB200OutCSC ? 1 : 0,
+		                                       smem_cap, d_vals); }
+		HA_CUDA(cudaGetLastError());
+	}
+	P->last_chunk = (int)P->chunks.size() - 1;
+	P->last_rowmajor = rowmajor;
+	return kHaSuccess;
+}
+
+// ---- CV split indices (csrc/ha_ensemble.c:12-249) ----
+
+// xoshiro256** seeded through splitmix64, with modulo range reduction (csrc/ha_ensemble.c:12-46).
+struct CvRng {
+	uint64_t s[4];
+	static uint64_t rotl(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
+	explicit CvRng(uint64_t seed) {
+		for (int i = 0; i < 4; i++) {
+			seed += 0x9e3779b97f4a7c15ULL;
+			uint64_t z = seed;
+			z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+			z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+			s[i] = z ^ (z >> 31);
+		}
+	}
+	uint64_t next() {
+		const uint64_t out = rotl(s[1] * 5, 7) * 9;
+		const uint64_t t = s[1] << 17;
+		s[2] ^= s[0];
+		s[3] ^= s[1];
+		s[1] ^= s[2];
+		s[0] ^= s[3];
+		s[2] ^= t;
+		s[3] = rotl(s[3], 45);
+		return out;
+	}
+	int32_t below(int32_t n) { return (int32_t)(next() % (uint64_t)n); }
+};
+
+// Temporally blocked CV splits with buffer zones: the blocks are shuffled and dealt to folds;
+// training rows are a bootstrap of nt draws from the rows outside the test blocks' buffers;
+// test rows are the rows outside the buffers of the drawn training rows.  The draws follow
+// csrc/ha_ensemble.c:58-249 one for one, so the same seed gives the same splits.
+int ensemble_indices(int32_t nt, int32_t n_perms, int32_t n_folds, int32_t blocksize, int32_t buffersize,
+                     uint64_t seed, const bool *mask, int32_t *train_out, int32_t *test_out, int32_t *test_sizes) {
+	if (nt < 1 || n_perms < 1 || n_folds < 1 || blocksize < 1 || buffersize < 0 || !train_out || !test_out ||
+	    !test_sizes)
+		return kHaErrorArg;
+	CvRng rng(seed);
+	const int32_t n_blocks = nt / blocksize, remainder = nt % blocksize;
+	const int32_t padded = nt + 2 * buffersize;
+	std::vector<int32_t> mapping, order((size_t)n_blocks), test_raw, valid;
+	if (mask) {
+		mapping.assign((size_t)nt, -1);
+		int32_t cum = 0;
+		for (int32_t i = 0; i < nt; i++)
+			if (mask[i]) mapping[i] = cum++;
+	}
+	std::vector<char> trm((size_t)padded), tem((size_t)padded), used((size_t)nt);
+	auto block_out = [&](std::vector<char> &mk, int32_t centre) {
+		for (int32_t b = -buffersize; b <= buffersize; b++) {
+			const int32_t pos = centre + buffersize + b;
+			if (pos >= 0 && pos < padded) mk[pos] = 0;
+		}
+	};
+	int split = 0;
+	for (int32_t perm = 0; perm < n_perms; perm++) {
+		const int32_t shift = rng.below(remainder + 1);
+		for (int32_t i = 0; i < n_blocks; i++) order[i] = i;
+		for (int32_t i = n_blocks - 1; i > 0; i--) std::swap(order[i], order[rng.below(i + 1)]);
+		int32_t f0 = 0;
+		for (int32_t fold = 0; fold < n_folds; fold++, split++) {
+			const int32_t f1 = (int32_t)((int64_t)(fold + 1) * n_blocks / n_folds);
+			test_raw.clear();
+			for (int32_t b = f0; b < f1; b++)
+				for (int32_t k = 0; k < blocksize; k++) {
+					const int32_t t = order[b] * blocksize + k + shift;
+					if (t < nt) test_raw.push_back(t);
+				}
+			std::fill(trm.begin(), trm.end(), 1);
+			for (int32_t t : test_raw) block_out(trm, t);
+			if (mask)
+				for (int32_t i = 0; i < nt; i++)
+					if (!mask[i]) trm[i + buffersize] = 0;
+			valid.clear();
+			for (int32_t i = 0; i < nt; i++)
+				if (trm[i + buffersize]) valid.push_back(i);
+			if (valid.empty()) {
+				fprintf(stderr, "ha_ensemble_indices_b200: fold %d leaves no training rows\n", fold);
+				return kHaErrorArg;
+			}
+			int32_t *train = train_out + (size_t)split * nt;
+			for (int32_t i = 0; i < nt; i++) train[i] = valid[rng.below((int32_t)valid.size())];
+			std::fill(tem.begin(), tem.end(), 1);
+			std::fill(used.begin(), used.end(), 0);
+			for (int32_t i = 0; i < nt; i++) used[train[i]] = 1;
+			for (int32_t i = 0; i < nt; i++)
+				if (used[i]) block_out(tem, i);
+			if (mask)
+				for (int32_t i = 0; i < nt; i++)
+					if (!mask[i]) tem[i + buffersize] = 0;
+			int32_t *test = test_out + (size_t)split * nt;
+			int32_t nte = 0;
+			for (int32_t i = 0; i < nt; i++)
+				if (tem[i + buffersize]) test[nte++] = i;
+			if (mask) {
+				for (int32_t i = 0; i < nt; i++) train[i] = mapping[train[i]];
+				for (int32_t i = 0; i < nte; i++) test[i] = mapping[test[i]];
+			}
+			test_sizes[split] = nte;
+			f0 = f1;
+		}
+	}
 	return kHaSuccess;
 }
 
@@ -880,6 +1206,52 @@ int csc_impl(const double *X, const double *Y, int32_t nt, int32_t nv, const int
 	for (int64_t k = 0; k < tot; k++)
 		if (pos[k] >= 0) data[pos[k]] += vals[k];
 	return kHaSuccess;
+}
+
+int grid_csc_impl(const double *X, const double *Y, int32_t nt, int32_t nv, const int32_t *idx, const int32_t *off,
+                  int32_t count, const double *weights, const int32_t *indptr, const int32_t *indices, int64_t nnz,
+                  double *data, const GridSpec &gs, int32_t *best_out, double *cost_out, bool col_major) {
+	if (!X || !Y || !idx || !off || !indptr || !indices || !data || !best_out || nt <= 0 || nv <= 0 || count <= 0 ||
+	    nnz < 0)
+		return kHaErrorArg;
+	int rc = check_cuda_ready();
+	if (rc != kHaSuccess) return rc;
+	HaB200Plan *P = nullptr;
+	if ((rc = get_plan(nt, nv, idx, off, nullptr, count, 0.0, weights, weights == nullptr, &P)) != kHaSuccess) return rc;
+	std::vector<int64_t> pos;
+	if ((rc = map_pattern(P, indptr, indices, nnz, pos)) != kHaSuccess) return rc;
+	cudaStream_t st = 0;
+	const double *dX, *dY;
+	if ((rc = upload_inputs(X, Y, nt, nv, col_major, &dX, &dY, st)) != kHaSuccess) return rc;
+	const int grid = (int)(gs.alphas.size() * gs.npcs.size());
+	DevArr<int32_t> dbest;
+	DevArr<double> dcost;
+	auto done = [&](int code) {
+		dbest.release();
+		dcost.release();
+		return code;
+	};
+	if ((rc = g_bufs.vals.ensure((size_t)P->nnz)) != kHaSuccess) return done(rc);
+	if ((rc = dbest.ensure((size_t)count)) != kHaSuccess) return done(rc);
+	if (cost_out && (rc = dcost.ensure((size_t)count * grid)) != kHaSuccess) return done(rc);
+	if (cudaMemsetAsync(g_bufs.vals.p, 0, (size_t)P->nnz * 8, st) != cudaSuccess) return done(kHaErrorInternal);
+	if ((rc = run_ridge_grid(P, dX, dY, gs, kHaB200OutCSC, g_bufs.vals.p, dbest.p, cost_out ? dcost.p : nullptr, st)) !=
+	    kHaSuccess)
+		return done(rc);
+	g_bufs.h_vals.resize((size_t)P->nnz);
+	if (cudaMemcpyAsync(g_bufs.h_vals.data(), g_bufs.vals.p, (size_t)P->nnz * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+	    cudaMemcpyAsync(best_out, dbest.p, (size_t)count * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+	    (cost_out && cudaMemcpyAsync(cost_out, dcost.p, (size_t)count * grid * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess) ||
+	    cudaStreamSynchronize(st) != cudaSuccess) {
+		fprintf(stderr, "ha_searchlight_ridge_grid_b200: CUDA failure: %s\n", cudaGetErrorString(cudaGetLastError()));
+		return done(kHaErrorInternal);
+	}
+	const double *vals = g_bufs.h_vals.data();
+	const int64_t tot = P->nnz;
+#pragma omp parallel for schedule(static) num_threads(host_threads())
+	for (int64_t k = 0; k < tot; k++)
+		if (pos[k] >= 0) data[pos[k]] += vals[k];
+	return done(kHaSuccess);
 }
 
 }  // namespace
@@ -1069,6 +1441,30 @@ int ha_searchlight_procrustes_csc_b200(const double *X_data, const double *Y_dat
 	                isReflection, isScaling, col_major, false, 0.0);
 }
 
+int ha_searchlight_ridge_grid_b200(const double *X_data, const double *Y_data, int32_t nt, int32_t nv,
+                                   const int32_t *sl_indices, const int32_t *sl_offsets, int32_t count,
+                                   const double *weights, const int32_t *indptr, const int32_t *indices, int64_t nnz,
+                                   double *data, const double *alphas, int32_t n_alphas, const int32_t *npcs,
+                                   int32_t n_npcs, const int32_t *const *train_idx_li,
+                                   const int32_t *const *test_idx_li, const int32_t *train_sizes,
+                                   const int32_t *test_sizes, int32_t n_models, int32_t *best_out, double *cost_out,
+                                   bool col_major) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	if (nt <= 0) return kHaErrorArg;
+	GridSpec gs;
+	int rc = grid_spec(nt, alphas, n_alphas, npcs, n_npcs, train_idx_li, test_idx_li, train_sizes, test_sizes,
+	                   n_models, gs);
+	if (rc != kHaSuccess) return rc;
+	return grid_csc_impl(X_data, Y_data, nt, nv, sl_indices, sl_offsets, count, weights, indptr, indices, nnz, data,
+	                     gs, best_out, cost_out, col_major);
+}
+
+int ha_ensemble_indices_b200(int32_t nt, int32_t n_perms, int32_t n_folds, int32_t blocksize, int32_t buffersize,
+                             uint64_t seed, const bool *mask, int32_t *train_out, int32_t *test_out,
+                             int32_t *test_sizes) {
+	return ensemble_indices(nt, n_perms, n_folds, blocksize, buffersize, seed, mask, train_out, test_out, test_sizes);
+}
+
 int ha_searchlight_ridge_csc_b200(const double *X_data, const double *Y_data, int32_t nt, int32_t nv,
                                   const int32_t *sl_indices, const int32_t *sl_offsets, int32_t count,
                                   const double *weights, const int32_t *indptr, const int32_t *indices, int64_t nnz,
@@ -1101,6 +1497,8 @@ void ha_b200_plan_destroy(HaB200Plan *P) {
 	P->vlptr.release(); P->vlent.release(); P->patptr.release(); P->patcol.release();
 	P->scrA.release(); P->scrV.release(); P->scrT.release(); P->scrT64.release(); P->uv.release(); P->scale.release();
 	P->stats.release(); P->X32.release(); P->Y32.release(); P->var.release(); P->counters.release();
+	P->gridscr.release(); P->galpha.release(); P->gwinv.release(); P->gbase.release(); P->gnpcs.release();
+	P->grows.release(); P->gtpos.release(); P->gurows.release(); P->guntested.release(); P->gmdl.release();
 	delete P;
 }
 
@@ -1181,6 +1579,21 @@ int ha_b200_plan_ridge_device(HaB200Plan *P, const double *d_X, const double *d_
 void ha_b200_set_kernel_timing(bool on) {
 	std::lock_guard<std::recursive_mutex> lk(g_mu);
 	g_timing = on;
+}
+
+int ha_b200_plan_ridge_grid_device(HaB200Plan *P, const double *d_X, const double *d_Y, const double *alphas,
+                                   int32_t n_alphas, const int32_t *npcs, int32_t n_npcs,
+                                   const int32_t *const *train_idx_li, const int32_t *const *test_idx_li,
+                                   const int32_t *train_sizes, const int32_t *test_sizes, int32_t n_models,
+                                   int out_kind, double *d_values, int32_t *d_best, double *d_cost, void *stream) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	if (!P || !d_X || !d_Y || !d_values || !d_best) return kHaErrorArg;
+	if (out_kind != kHaB200OutCSR && out_kind != kHaB200OutCSC) return kHaErrorArg;
+	GridSpec gs;
+	int rc = grid_spec(P->nt, alphas, n_alphas, npcs, n_npcs, train_idx_li, test_idx_li, train_sizes, test_sizes,
+	                   n_models, gs);
+	if (rc != kHaSuccess) return rc;
+	return run_ridge_grid(P, d_X, d_Y, gs, out_kind, d_values, d_best, d_cost, (cudaStream_t)stream);
 }
 
 int ha_b200_kernel_times(double *ms, int64_t *launches) {
@@ -1398,6 +1811,7 @@ extern "C" int ha_b200_local_procrustes_noalloc(const double *d_X, const double 
 	jp.t_rowmajor = 1;
 	jp.ill_ratio = 0.0;
 	jp.weak = 1000.0;
+	jp.eig = 0;
 	jp.only_flagged = 0;
 	int64_t tofs = 0;  // packed output offset of the current searchlight
 	int32_t s = 0;

@@ -1,0 +1,376 @@
+// ha_b200_grid.cuh -- per-searchlight ridge grid search with cross-validated ensembles (float64).
+//
+// Composition of the reference's ha_ridge_grid (csrc/ha_ridge.c:97-227) and ha_ensemble_ridge
+// (csrc/ha_ridge.c:229-345) applied to every searchlight: X = X[:, sl] and the searchlight's n
+// target columns Y[:, sl], with the prediction cost summed over the targets (one winner per
+// searchlight).  For CV model m with training rows tr_m (bootstrap, duplicates kept) and test
+// rows te_m:
+//   G = X_tr^T X_tr = V diag(lambda) V^T   (X_tr = U diag(s) V^T, lambda = s^2),
+//   Q = V^T X_tr^T Y_tr,  component k contributes v_k q_k^T / (alpha + lambda_k)
+// which is the reference's V diag(s / (alpha + s^2)) U^T Y per component.  Components are taken
+// in decreasing lambda (the SVD's order), the PC chunks [npcs[p-1], npcs[p]) are clipped at
+// K = min(rows, n) and summed cumulatively over p (csrc/ha_ridge.c:185-220, also for non-monotone
+// npcs).  Test predictions of model m are X_te V diag(c) Q; every tested time point averages the
+// predictions of the models that test it (csrc/ha_ridge.c:262-303), and the cost of a grid point
+// is the squared error over all time points and targets (csrc/ha_ridge.c:305-319; untested time
+// points predict zero).  The winner is the first grid point with the smallest cost (g = a * n_npcs
+// + p, csrc/ha_ridge.c:322-327); its model-averaged beta is written like the ridge solve's.
+#pragma once
+
+#include "ha_b200_kernels.cuh"
+
+namespace hab200 {
+
+constexpr int kGridMaxN = 512;  // searchlight size limit of the grid kernels (shared rank arrays)
+
+struct GridModel {
+	int32_t tr_ofs, tr_n;  // training rows: rows[tr_ofs .. tr_ofs + tr_n)
+	int32_t te_ofs, te_n;  // test rows: rows[te_ofs .. te_ofs + te_n); union positions tpos[te_ofs ..]
+};
+
+struct GridParams {
+	int models, mte, ntu, n_alphas, n_npcs, nt, n_untested;
+	const double *alphas;      // n_alphas
+	const int32_t *npcs;       // n_npcs
+	const GridModel *mdl;      // models
+	const int32_t *rows;       // concatenated training and test row lists
+	const int32_t *tpos;       // per test-list entry: position in the union of tested rows
+	const double *winv;        // per union position: 1 / (number of models that test it)
+	const int32_t *urows;      // union of tested rows, ntu
+	const int32_t *untested;   // rows no model tests, n_untested
+	const int64_t *gbase;      // per work slot: base offset of the searchlight's grid scratch
+};
+
+// Per-searchlight layout of the grid scratch (float64 elements from the searchlight's base).
+// Per model: V and Q with components in decreasing-lambda order (V column r = r-th component,
+// Q row r), lambda in that order, E = X_te V (mte x n, column-major, ld mte) and the cumulative
+// test predictions Pm (mte x n).  P and Yu are the averaged predictions and the targets on the
+// union of tested rows (ntu x n, column-major), C the cross-covariance of the current model.
+struct GridLayout {
+	int64_t C, Vst, Qst, Lst, Est, Pm, P, Yu, Xte, cost, total;
+	__host__ __device__ static GridLayout make(int n, int models, int mte, int ntu, int grid) {
+		GridLayout L;
+		const int64_t n2 = (int64_t)n * n, mn = (int64_t)mte * n;
+		int64_t o = 0;
+		L.C = o; o += n2;
+		L.Vst = o; o += (int64_t)models * n2;
+		L.Qst = o; o += (int64_t)models * n2;
+		L.Lst = o; o += (int64_t)models * n;
+		L.Est = o; o += (int64_t)models * mn;
+		L.Pm = o; o += (int64_t)models * mn;
+		L.P = o; o += (int64_t)max(ntu, n) * n;  // also the n x n beta accumulator at the end
+		L.Yu = o; o += (int64_t)ntu * n;
+		L.Xte = o; o += mn;
+		L.cost = o; o += grid;
+		L.total = (o + 31) & ~(int64_t)31;
+		return L;
+	}
+};
+
+__device__ __forceinline__ GridLayout grid_layout(const GridParams &gp, int n) {
+	return GridLayout::make(n, gp.models, gp.mte, gp.ntu, gp.n_alphas * gp.n_npcs);
+}
+
+// A_s = X[rows, sl]^T Z[rows, sl] (Z = X for the Gram, Y for the cross-covariance) over one row
+// list with duplicates, float64, the k_xcov tiling with gathered rows.  Output column-major with
+// ncol columns (padding columns zero) at Ascr + w.aofs, or (to_grid) into the searchlight's C.
+template <int KT>
+__global__ void __launch_bounds__(256) k_xcov_rows(const SlWork *__restrict__ work, const int32_t *__restrict__ sl_idx,
+                                                   const double *__restrict__ X, const double *__restrict__ Z, int nt,
+                                                   const int32_t *__restrict__ rows, int nrows, double *__restrict__ Ascr,
+                                                   double *__restrict__ Gscr, GridParams gp, int to_grid) {
+	const SlWork w = work[blockIdx.x];
+	const int n = w.n;
+	const int ncol = w.nblk * w.bsz;
+	const int32_t *sl = sl_idx + w.sofs;
+	double *A = to_grid ? Gscr + gp.gbase[w.slot] + grid_layout(gp, n).C : Ascr + w.aofs;
+	__shared__ double xs[KT][64 + 1];
+	__shared__ double zs[KT][64 + 1];
+	__shared__ int32_t vi[64], vj[64];
+	__shared__ int32_t rt[KT];
+	const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+	for (int i0 = 0; i0 < n; i0 += 64) {
+		for (int j0 = 0; j0 < n; j0 += 64) {
+			__syncthreads();
+			if (threadIdx.x < 64) {
+				const int i = i0 + threadIdx.x;
+				vi[threadIdx.x] = (i < n) ? sl[i] : -1;
+			} else if (threadIdx.x < 128) {
+				const int j = j0 + threadIdx.x - 64;
+				vj[threadIdx.x - 64] = (j < n) ? sl[j] : -1;
+			}
+			double acc[4][4];
+#pragma unroll
+			for (int a = 0; a < 4; a++)
+#pragma unroll
+				for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
+			for (int t0 = 0; t0 < nrows; t0 += KT) {
+				__syncthreads();
+				if (threadIdx.x < KT) rt[threadIdx.x] = (t0 + threadIdx.x < nrows) ? rows[t0 + threadIdx.x] : -1;
+				__syncthreads();
+				for (int e = threadIdx.x; e < 64 * KT; e += 256) {
+					const int r = e / KT, t = e - r * KT;
+					const int tt = rt[t];
+					const int v = vi[r], u = vj[r];
+					xs[t][r] = (v >= 0 && tt >= 0) ? X[(int64_t)v * nt + tt] : 0.0;
+					zs[t][r] = (u >= 0 && tt >= 0) ? Z[(int64_t)u * nt + tt] : 0.0;
+				}
+				__syncthreads();
+#pragma unroll 4
+				for (int t = 0; t < KT; t++) {
+					double a[4], b[4];
+#pragma unroll
+					for (int q = 0; q < 4; q++) {
+						a[q] = xs[t][ty + 16 * q];
+						b[q] = zs[t][tx + 16 * q];
+					}
+#pragma unroll
+					for (int p = 0; p < 4; p++)
+#pragma unroll
+						for (int q = 0; q < 4; q++) acc[p][q] += a[p] * b[q];
+				}
+			}
+#pragma unroll
+			for (int p = 0; p < 4; p++) {
+				const int i = i0 + ty + 16 * p;
+				if (i >= n) continue;
+#pragma unroll
+				for (int q = 0; q < 4; q++) {
+					const int j = j0 + tx + 16 * q;
+					if (j < n) A[(int64_t)j * n + i] = acc[p][q];
+				}
+			}
+		}
+	}
+	if (!to_grid)
+		for (int64_t e = (int64_t)n * n + threadIdx.x; e < (int64_t)n * ncol; e += 256) A[e] = 0.0;
+}
+
+// Rank of every component by decreasing lambda (ties by index): order[r] = k.
+__device__ __forceinline__ void rank_desc(const double *lam, int n, int *order) {
+	for (int k = threadIdx.x; k < n; k += blockDim.x) {
+		const double lk = lam[k];
+		int r = 0;
+		for (int l = 0; l < n; l++) {
+			const double ll = lam[l];
+			r += (ll > lk) || (ll == lk && l < k);
+		}
+		order[r] = k;
+	}
+}
+
+// One CV model of every searchlight: V (column-major, ld n) in the V scratch and lambda in the
+// u/v buffer come from the float64 Jacobi kernel in eigenvector mode; C is in the grid scratch.
+// Stores V, lambda in decreasing-lambda order, Q = V^T C and E = X_te V for the model.
+__global__ void __launch_bounds__(256) k_grid_model(const SlWork *__restrict__ work, const int32_t *__restrict__ sl_idx,
+                                                    const double *__restrict__ X, const double *__restrict__ Vscr,
+                                                    const double *__restrict__ uvbuf, int model,
+                                                    double *__restrict__ Gscr, GridParams gp) {
+	__shared__ double ps[16][65], qs[16][65];
+	__shared__ int order[kGridMaxN];
+	const SlWork w = work[blockIdx.x];
+	const int n = w.n;
+	const GridLayout L = grid_layout(gp, n);
+	double *base = Gscr + gp.gbase[w.slot];
+	const double *V = Vscr + w.aofs;
+	const double *lam = uvbuf + w.uvofs;
+	const int32_t *sl = sl_idx + w.sofs;
+	const GridModel md = gp.mdl[model];
+	const int m = md.te_n;
+	const int64_t n2 = (int64_t)n * n, mn = (int64_t)gp.mte * n;
+	double *Vst = base + L.Vst + model * n2;
+	double *Qst = base + L.Qst + model * n2;
+	double *Lst = base + L.Lst + (int64_t)model * n;
+	double *Est = base + L.Est + model * mn;
+	double *Xte = base + L.Xte;
+	const double *C = base + L.C;
+	const int32_t *te = gp.rows + md.te_ofs;
+	rank_desc(lam, n, order);
+	__syncthreads();
+	for (int64_t e = threadIdx.x; e < n2; e += blockDim.x) {
+		const int r = (int)(e / n), i = (int)(e - (int64_t)r * n);
+		Vst[e] = V[(int64_t)order[r] * n + i];
+	}
+	for (int r = threadIdx.x; r < n; r += blockDim.x) Lst[r] = lam[order[r]];
+	// test rows of X, column-major by vertex: Xte[v * m + t]
+	for (int64_t e = threadIdx.x; e < (int64_t)m * n; e += blockDim.x) {
+		const int v = (int)(e / m), t = (int)(e - (int64_t)v * m);
+		Xte[e] = X[(int64_t)sl[v] * gp.nt + te[t]];
+	}
+	__syncthreads();
+	GemmArgs<double, double> g;
+	g.d = nullptr; g.alpha = 1.0; g.E = nullptr; g.ei = 0; g.ej = 0; g.beta = 0.0;
+	// Q(r, j) = sum_k Vst(k, r) C(k, j), column-major ld n
+	g.M = n; g.N = n; g.K = n;
+	g.P = Vst; g.pk = 1; g.pi = n;
+	g.Q = C; g.qk = 1; g.qj = n;
+	g.C = Qst; g.ci = 1; g.cj = n;
+	block_gemm(g, ps, qs);
+	if (m > 0) {
+		// E(t, r) = sum_v Xte(t, v) Vst(v, r), column-major ld m
+		g.M = m; g.N = n; g.K = n;
+		g.P = Xte; g.pk = m; g.pi = 1;
+		g.Q = Vst; g.qk = 1; g.qj = n;
+		g.C = Est; g.ci = 1; g.cj = m;
+		block_gemm(g, ps, qs);
+	}
+}
+
+// First and one-past-last component of PC chunk p of a model with K usable components, or an
+// empty range (csrc/ha_ridge.c:187-210).
+__device__ __forceinline__ void pc_chunk(const int32_t *npcs, int p, int K, int &r0, int &r1) {
+	const int lo = p ? npcs[p - 1] : 0;
+	const int hi = npcs[p];
+	r0 = lo;
+	r1 = lo;
+	if (hi - lo > 0 && lo < K) r1 = min(hi, K);
+}
+
+// Block-wide sum of one value per thread (256 threads), result in every thread.
+__device__ __forceinline__ double block_sum256(double v, double *red) {
+	v = warp_sum(v);
+	__syncthreads();
+	if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+	__syncthreads();
+	double tot = 0.0;
+	for (int q = 0; q < (int)(blockDim.x >> 5); q++) tot += red[q];
+	return tot;
+}
+
+// The grid evaluation of every searchlight after all models: cost of every (alpha, PC count),
+// the winner, and the winner's model-averaged beta, written float64 in the T layout (row-major for
+// CSR output, column-major for CSC).  cost_out (may be null) gets the grid's costs per
+// searchlight, best_out the winning grid index.
+__global__ void __launch_bounds__(256) k_grid_eval(const SlWork *__restrict__ work, const int32_t *__restrict__ sl_idx,
+                                                   const double *__restrict__ Y, double *__restrict__ Gscr, GridParams gp,
+                                                   double *__restrict__ Bout, int t_rowmajor,
+                                                   int32_t *__restrict__ best_out, double *__restrict__ cost_out) {
+	__shared__ double ps[16][65], qs[16][65];
+	__shared__ double cval[kGridMaxN];
+	__shared__ double red[32];
+	__shared__ int best;
+	const SlWork w = work[blockIdx.x];
+	const int n = w.n;
+	const int grid = gp.n_alphas * gp.n_npcs;
+	const GridLayout L = grid_layout(gp, n);
+	double *base = Gscr + gp.gbase[w.slot];
+	const int32_t *sl = sl_idx + w.sofs;
+	const int64_t n2 = (int64_t)n * n, mn = (int64_t)gp.mte * n;
+	const int ntu = gp.ntu;
+	double *P = base + L.P, *Yu = base + L.Yu, *cost = base + L.cost;
+	// targets on the tested rows, and the squared targets of the untested rows (zero prediction)
+	for (int64_t e = threadIdx.x; e < (int64_t)ntu * n; e += blockDim.x) {
+		const int j = (int)(e / ntu), u = (int)(e - (int64_t)j * ntu);
+		Yu[e] = Y[(int64_t)sl[j] * gp.nt + gp.urows[u]];
+	}
+	double yc = 0.0;
+	for (int64_t e = threadIdx.x; e < (int64_t)gp.n_untested * n; e += blockDim.x) {
+		const int j = (int)(e / gp.n_untested), t = (int)(e - (int64_t)j * gp.n_untested);
+		const double y = Y[(int64_t)sl[j] * gp.nt + gp.untested[t]];
+		yc += y * y;
+	}
+	const double yconst = block_sum256(yc, red);
+	GemmArgs<double, double> g;
+	g.alpha = 1.0;
+	g.beta = 1.0;
+	for (int a = 0; a < gp.n_alphas; a++) {
+		const double al = gp.alphas[a];
+		for (int64_t e = threadIdx.x; e < gp.models * mn; e += blockDim.x) base[L.Pm + e] = 0.0;
+		__syncthreads();
+		for (int p = 0; p < gp.n_npcs; p++) {
+			// Pm += E[:, r0:r1] diag(1 / (alpha + lambda)) Q[r0:r1, :] for every model
+			for (int mo = 0; mo < gp.models; mo++) {
+				const GridModel md = gp.mdl[mo];
+				const int m = md.te_n;
+				int r0, r1;
+				pc_chunk(gp.npcs, p, min(md.tr_n, n), r0, r1);
+				if (r1 <= r0 || m == 0) continue;
+				const double *lam = base + L.Lst + (int64_t)mo * n;
+				__syncthreads();
+				for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x) cval[r] = 1.0 / (al + lam[r]);
+				__syncthreads();
+				const double *E = base + L.Est + mo * mn;
+				const double *Q = base + L.Qst + mo * n2;
+				double *Pm = base + L.Pm + mo * mn;
+				g.M = m; g.N = n; g.K = r1 - r0;
+				g.P = E + (int64_t)r0 * m; g.pk = m; g.pi = 1;
+				g.Q = Q + r0; g.qk = 1; g.qj = n;
+				g.d = cval + r0;
+				g.E = Pm; g.ei = 1; g.ej = m;
+				g.C = Pm; g.ci = 1; g.cj = m;
+				block_gemm(g, ps, qs);
+			}
+			// average over the models that test each row, then the squared error
+			__syncthreads();
+			for (int64_t e = threadIdx.x; e < (int64_t)ntu * n; e += blockDim.x) P[e] = 0.0;
+			for (int mo = 0; mo < gp.models; mo++) {
+				const GridModel md = gp.mdl[mo];
+				const int m = md.te_n;
+				const double *Pm = base + L.Pm + mo * mn;
+				const int32_t *tp = gp.tpos + md.te_ofs;
+				__syncthreads();
+				for (int64_t e = threadIdx.x; e < (int64_t)m * n; e += blockDim.x) {
+					const int j = (int)(e / m), i = (int)(e - (int64_t)j * m);
+					const int u = tp[i];
+					P[(int64_t)j * ntu + u] += gp.winv[u] * Pm[e];
+				}
+			}
+			__syncthreads();
+			double s = 0.0;
+			for (int64_t e = threadIdx.x; e < (int64_t)ntu * n; e += blockDim.x) {
+				const double d = Yu[e] - P[e];
+				s += d * d;
+			}
+			s = block_sum256(s, red);
+			if (threadIdx.x == 0) cost[a * gp.n_npcs + p] = s + yconst;
+		}
+	}
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		int b = 0;
+		for (int gi = 1; gi < grid; gi++)
+			if (cost[gi] < cost[b]) b = gi;
+		best = b;
+		best_out[w.s] = b;
+	}
+	__syncthreads();
+	if (cost_out)
+		for (int gi = threadIdx.x; gi < grid; gi += blockDim.x) cost_out[(int64_t)w.s * grid + gi] = cost[gi];
+	// beta of the winner: the cumulative PC chunks up to p of every model, averaged
+	const int ba = best / gp.n_npcs, bp = best % gp.n_npcs;
+	const double al = gp.alphas[ba];
+	double *acc = P;  // n x n accumulator (column-major); the prediction scratch is free now
+	__syncthreads();
+	for (int64_t e = threadIdx.x; e < n2; e += blockDim.x) acc[e] = 0.0;
+	for (int mo = 0; mo < gp.models; mo++) {
+		const GridModel md = gp.mdl[mo];
+		const double *V = base + L.Vst + mo * n2;
+		const double *Q = base + L.Qst + mo * n2;
+		const double *lam = base + L.Lst + (int64_t)mo * n;
+		for (int p = 0; p <= bp; p++) {
+			int r0, r1;
+			pc_chunk(gp.npcs, p, min(md.tr_n, n), r0, r1);
+			if (r1 <= r0) continue;
+			__syncthreads();
+			for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x) cval[r] = 1.0 / (al + lam[r]);
+			__syncthreads();
+			// acc(i, j) += sum_r V(i, r) c_r Q(r, j)
+			g.M = n; g.N = n; g.K = r1 - r0;
+			g.P = V + (int64_t)r0 * n; g.pk = n; g.pi = 1;
+			g.Q = Q + r0; g.qk = 1; g.qj = n;
+			g.d = cval + r0;
+			g.E = acc; g.ei = 1; g.ej = n;
+			g.C = acc; g.ci = 1; g.cj = n;
+			block_gemm(g, ps, qs);
+		}
+	}
+	__syncthreads();
+	double *Bo = Bout + w.tofs;
+	const int64_t ti = t_rowmajor ? n : 1, tj = t_rowmajor ? 1 : n;
+	for (int64_t e = threadIdx.x; e < n2; e += blockDim.x) {
+		const int j = (int)(e / n), i = (int)(e - (int64_t)j * n);
+		Bo[i * ti + j * tj] = acc[e] / gp.models;
+	}
+}
+
+}  // namespace hab200

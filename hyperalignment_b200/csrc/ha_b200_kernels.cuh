@@ -526,6 +526,7 @@ struct JacobiParams {
 	int t_rowmajor;
 	double ill_ratio;  // sigma_min / sigma_max below this -> kFlagIllCond
 	double weak;       // columns with sigma <= weak * eps * sigma_max are re-orthogonalised / completed
+	int eig;           // eigenvector mode: write V (column-major, ld n) to the V scratch and sigma to uvbuf
 	int only_flagged;  // process only searchlights whose stats carry kFlagIllCond (FP64 re-solve)
 };
 
@@ -698,6 +699,17 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) k_jacobi(const
 			stats[w.slot] = st;
 		}
 		__syncthreads();
+	}
+	// eigenvector mode (symmetric positive semi-definite A): B = A V = V diag(lambda), so the column
+	// norms are the eigenvalues and V holds the eigenvectors
+	if (prm.eig) {
+		if (resident)
+			for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+				const int c = e / n, i = e - c * n;
+				Vg[e] = Vs[c * LD + i];
+			}
+		for (int k = threadIdx.x; k < n; k += blockDim.x) uvbuf[w.uvofs + k] = (double)sg[k];
+		return;
 	}
 	// normalise columns: u_c = b_c / sigma_c (in place)
 	for (int e = threadIdx.x; e < n * n; e += blockDim.x) {

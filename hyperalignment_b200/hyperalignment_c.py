@@ -15,6 +15,8 @@ reference's ``ha_sparse_init``).
 
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 
 from . import _lib as L
@@ -124,6 +126,48 @@ def searchlight_ridge_csc(X, Y, sls, indptr, indices, data, alpha, weights=None)
         L.iptr(np.ascontiguousarray(indptr, dtype=np.int32)), L.iptr(np.ascontiguousarray(indices, dtype=np.int32)),
         int(len(indices)), L.dptr(data), float(alpha), True), "ha_searchlight_ridge_csc_b200")
     return data
+
+
+def searchlight_ridge_grid(X, Y, sls, indptr, indices, data, alphas, npcs, train_li, test_li, weights=None,
+                           return_costs=False):
+    """Searchlight ridge grid search with CV ensembles (float64): the winner's model-averaged
+    betas of every searchlight accumulate into ``data`` (CSC); returns the winning grid index per
+    searchlight (g = alpha index * len(npcs) + PC index), and the cost grid when asked."""
+    lib = _init()
+    X = np.asfortranarray(X, dtype=np.float64)
+    Y = np.asfortranarray(Y, dtype=np.float64)
+    nt, nv = X.shape
+    idx, offsets, _ = _flatten(sls, None)
+    w = None if weights is None else np.ascontiguousarray(np.concatenate(weights).astype(np.float64))
+    al = np.ascontiguousarray(alphas, dtype=np.float64)
+    pc = np.ascontiguousarray(npcs, dtype=np.int32)
+    tr, te = L.IndexLists(train_li), L.IndexLists(test_li)
+    if len(tr) != len(te):
+        raise ValueError("train and test lists differ in length")
+    best = np.zeros(len(sls), dtype=np.int32)
+    costs = np.zeros((len(sls), al.size, pc.size)) if return_costs else None
+    L.check(lib.ha_searchlight_ridge_grid_b200(
+        L.dptr(X), L.dptr(Y), nt, nv, L.iptr(idx), L.iptr(offsets), len(sls), L.dptr(w),
+        L.iptr(np.ascontiguousarray(indptr, dtype=np.int32)), L.iptr(np.ascontiguousarray(indices, dtype=np.int32)),
+        int(len(indices)), L.dptr(data), L.dptr(al), al.size, L.iptr(pc), pc.size, tr.ptrs, te.ptrs,
+        L.iptr(tr.sizes), L.iptr(te.sizes), len(tr), L.iptr(best), L.dptr(costs), True),
+        "ha_searchlight_ridge_grid_b200")
+    return (best, costs) if return_costs else best
+
+
+def ensemble_indices(nt, n_perms, n_folds, blocksize, buffersize, seed, mask=None):
+    """CV split indices with the reference's draws: (train_li, test_li), lists of int32 arrays."""
+    lib = L.lib()
+    ns = n_perms * n_folds
+    train = np.zeros((ns, nt), dtype=np.int32)
+    test = np.zeros((ns, nt), dtype=np.int32)
+    sizes = np.zeros(ns, dtype=np.int32)
+    mk = None
+    if mask is not None:
+        mk = (ctypes.c_bool * nt)(*[bool(m) for m in mask])
+    L.check(lib.ha_ensemble_indices_b200(nt, n_perms, n_folds, blocksize, buffersize, ctypes.c_uint64(seed), mk,
+                                         L.iptr(train), L.iptr(test), L.iptr(sizes)), "ha_ensemble_indices_b200")
+    return [train[k].copy() for k in range(ns)], [test[k, :sizes[k]].copy() for k in range(ns)]
 
 
 def cleanup():

@@ -57,6 +57,17 @@ class Plan:
                                                    float(alpha), int(out_kind), ctypes.c_void_p(d_values),
                                                    ctypes.c_void_p(stream)), "ha_b200_plan_ridge_device")
 
+    def ridge_grid_device(self, d_X: int, d_Y: int, d_values: int, d_best: int, alphas, npcs, train_li, test_li,
+                          d_cost: int = 0, out_kind=L.OUT_CSC, stream: int = 0):
+        al = np.ascontiguousarray(alphas, dtype=np.float64)
+        pc = np.ascontiguousarray(npcs, dtype=np.int32)
+        tr, te = L.IndexLists(train_li), L.IndexLists(test_li)
+        L.check(self.lib.ha_b200_plan_ridge_grid_device(
+            self.handle, ctypes.c_void_p(d_X), ctypes.c_void_p(d_Y), L.dptr(al), al.size, L.iptr(pc), pc.size,
+            tr.ptrs, te.ptrs, L.iptr(tr.sizes), L.iptr(te.sizes), len(tr), out_kind, ctypes.c_void_p(d_values),
+            ctypes.c_void_p(d_best), ctypes.c_void_p(d_cost or None), ctypes.c_void_p(stream)),
+            "ha_b200_plan_ridge_grid_device")
+
     def stats(self):
         a, b = ctypes.c_int32(), ctypes.c_int32()
         L.check(self.lib.ha_b200_plan_stats(self.handle, ctypes.byref(a), ctypes.byref(b)), "ha_b200_plan_stats")

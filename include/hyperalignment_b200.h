@@ -169,6 +169,46 @@ int ha_searchlight_ridge_csc_b200(
 	double alpha, bool col_major);
 
 /*
+ * Searchlight ridge grid search with cross-validated ensembles: the reference's ha_ridge_grid
+ * (csrc/ha_ridge.c:97-227) inside ha_ensemble_ridge (csrc/ha_ridge.c:229-345), applied to every
+ * searchlight with X_s = X[:, sl] and the n_s targets Y[:, sl].  For every CV model m the grid of
+ * betas over alphas x PC counts is fitted on the training rows train_idx_li[m] (train_sizes[m]
+ * rows, duplicates kept); every tested row averages the predictions of the models that test it,
+ * and the cost of a grid point is the squared prediction error over all rows, SUMMED OVER THE
+ * TARGETS of the searchlight, so each searchlight gets one winner: the first grid index
+ * g = a * n_npcs + p with the smallest cost (best_out[s], int32 per searchlight).  The winner's
+ * model-averaged beta (n_s x n_s) is scattered like ha_searchlight_ridge_csc_b200.  PC chunks
+ * follow the reference: [npcs[p-1], npcs[p]) clipped at min(train rows, n_s), summed over p.
+ * cost_out (count x n_alphas x n_npcs float64, may be NULL) receives every grid cost.
+ * Computed in float64 (eigen decomposition of X_tr^T X_tr by Jacobi rotations).  kHaErrorArg for
+ * negative PC counts, non-finite alphas, empty training lists, rows outside [0, nt), a row
+ * repeated within one test list, or a searchlight of more than 512 vertices.
+ */
+int ha_searchlight_ridge_grid_b200(
+	const double *X_data, const double *Y_data, int32_t nt, int32_t nv,
+	const int32_t *sl_indices, const int32_t *sl_offsets, int32_t count,
+	const double *weights,
+	const int32_t *indptr, const int32_t *indices, int64_t nnz, double *data,
+	const double *alphas, int32_t n_alphas, const int32_t *npcs, int32_t n_npcs,
+	const int32_t *const *train_idx_li, const int32_t *const *test_idx_li,
+	const int32_t *train_sizes, const int32_t *test_sizes, int32_t n_models,
+	int32_t *best_out, double *cost_out, bool col_major);
+
+/*
+ * CV split indices, the same draws as ha_ensemble_indices (csrc/ha_ensemble.h,
+ * csrc/ha_ensemble.c:58-249: xoshiro256** seeded by splitmix64, shuffled blocks dealt to folds,
+ * bootstrap training rows outside the test blocks' buffers, test rows outside the training rows'
+ * buffers, optional mask with index remapping), into caller buffers: split k = perm * n_folds +
+ * fold has nt training rows at train_out[k * nt] and test_sizes[k] test rows at test_out[k * nt]
+ * (both buffers n_perms * n_folds * nt int32).  kHaErrorArg where the reference would read
+ * uninitialised memory (a fold without training rows) or divide by zero (blocksize < 1).
+ */
+int ha_ensemble_indices_b200(
+	int32_t nt, int32_t n_perms, int32_t n_folds, int32_t blocksize, int32_t buffersize,
+	uint64_t seed, const bool *mask,
+	int32_t *train_out, int32_t *test_out, int32_t *test_sizes);
+
+/*
  * Searchlight Procrustes template (the loop of ha_template_procrustes, csrc/ha_template.c:14-114,
  * with every whole-matrix Procrustes replaced by a searchlight solve and aligned = X @ T taken
  * as a sparse product over the searchlight pattern):
@@ -254,6 +294,18 @@ int ha_b200_plan_ridge_device(
 	int out_kind, double *d_values, void *stream);
 
 /*
+ * Ridge grid search on device-resident data (conventions of ha_b200_plan_ridge_device; grid and
+ * CV lists in host memory as ha_searchlight_ridge_grid_b200).  d_best (count int32) and d_cost
+ * (count x n_alphas x n_npcs float64, may be NULL) are DEVICE memory, overwritten.
+ */
+int ha_b200_plan_ridge_grid_device(
+	HaB200Plan *plan, const double *d_X, const double *d_Y,
+	const double *alphas, int32_t n_alphas, const int32_t *npcs, int32_t n_npcs,
+	const int32_t *const *train_idx_li, const int32_t *const *test_idx_li,
+	const int32_t *train_sizes, const int32_t *test_sizes, int32_t n_models,
+	int out_kind, double *d_values, int32_t *d_best, double *d_cost, void *stream);
+
+/*
  * Per-searchlight local transforms of the last device run, for testing:
  * copies T_s (n_s x n_s, row-major, float32, unweighted and unscaled) of
  * searchlights [first, first + n) into host out (sum of n_s^2 floats).
@@ -305,7 +357,8 @@ enum {
 	kHaB200KReduce = 11,    /* deterministic segmented reduction */
 	kHaB200KPattern = 12,   /* CSC pattern builder */
 	kHaB200KRidge = 13,     /* ridge solves */
-	kHaB200NumKernelKinds = 14,
+	kHaB200KGrid = 14,      /* ridge grid: per-model products and grid evaluation */
+	kHaB200NumKernelKinds = 15,
 };
 
 /*

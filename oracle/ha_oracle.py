@@ -189,6 +189,173 @@ def searchlight_ridge_csc(X, Y, idx, off, indptr, indices, data, alpha, weights=
 
 
 # ---------------------------------------------------------------------------------------------
+# ridge grid (csrc/ha_ridge.c:97-227), ensemble ridge (csrc/ha_ridge.c:229-345), CV split indices
+# (csrc/ha_ensemble.c:12-249), and their composition over searchlights
+# ---------------------------------------------------------------------------------------------
+
+def ridge_grid(X, y, alphas, npcs, train_idx=None):
+    """betas[v, a, p] (a trailing target axis when y is 2-D), csrc/ha_ridge.c:97-227.
+
+    Thin SVD of the training rows; d[k, a] = s_k / (alpha_a + s_k^2) times U^T y; the PC chunk
+    [npcs[p-1], npcs[p]) clipped at K = min(rows, cols) is summed into slot p (empty chunks leave
+    it zero), then the slots are summed cumulatively over p.
+    """
+    alphas = np.asarray(alphas, dtype=np.float64)
+    Xt = X if train_idx is None else X[np.asarray(train_idx)]
+    yt = y if train_idx is None else y[np.asarray(train_idx)]
+    U, s, Vt = np.linalg.svd(Xt, full_matrices=False)
+    K = s.size
+    d = s[:, None] / (alphas[None, :] + (s * s)[:, None])  # K x A
+    uty = U.T @ yt                                           # K (x T)
+    dut = d * uty[:, None] if uty.ndim == 1 else d[:, :, None] * uty[:, None, :]
+    N = X.shape[1]
+    betas = np.zeros((N, alphas.size, len(npcs)) + uty.shape[1:])
+    prev = 0
+    for p, cur in enumerate(npcs):
+        cur = int(cur)
+        if cur - prev > 0 and prev < K:
+            end = min(cur, K)
+            betas[:, :, p] = np.tensordot(Vt[prev:end].T, dut[prev:end], axes=(1, 0))
+        prev = cur
+    return np.cumsum(betas, axis=2)
+
+
+def ensemble_ridge(X, y, alphas, npcs, train_li, test_li):
+    """csrc/ha_ridge.c:229-345 with y of one target (1-D) or several (2-D, cost summed over them).
+
+    Returns (weights, pred, r2, alpha, npc, best, cost): the model-averaged betas of the winner,
+    its averaged test predictions, 1 - cost / sum(y^2), and the full cost grid (A x P).
+    """
+    alphas = np.asarray(alphas, dtype=np.float64)
+    nt = X.shape[0]
+    A, P = alphas.size, len(npcs)
+    tshape = y.shape[1:]
+    wsum = None
+    psum = np.zeros((nt, A, P) + tshape)
+    count = np.zeros(nt, dtype=np.int64)
+    for tr, te in zip(train_li, test_li):
+        b = ridge_grid(X, y, alphas, npcs, tr)
+        wsum = b.copy() if wsum is None else wsum + b
+        te = np.asarray(te, dtype=np.int64)
+        if te.size:
+            psum[te] += np.einsum("tv,va...->ta...", X[te], b)
+            count[te] += 1
+    weights_avg = wsum / len(train_li)
+    pred = np.zeros_like(psum)
+    hit = count > 0
+    pred[hit] = psum[hit] / count[hit].reshape((-1,) + (1,) * (psum.ndim - 1))
+    diff = y.reshape((nt, 1, 1) + tshape) - pred
+    cost = (diff * diff).reshape(nt, A, P, -1).sum(axis=(0, 3))
+    best = int(np.argmin(cost.ravel()))  # first minimum, csrc/ha_ridge.c:322-327
+    ba, bp = divmod(best, P)
+    r2 = 1.0 - cost.ravel()[best] / float((y * y).sum())
+    return weights_avg[:, ba, bp], pred[:, ba, bp], r2, float(alphas[ba]), int(npcs[bp]), best, cost
+
+
+def searchlight_ridge_grid_csc(X, Y, idx, off, indptr, indices, data, alphas, npcs, train_li, test_li,
+                               weights=None):
+    """Per searchlight: ensemble_ridge of X[:, sl] on the n targets Y[:, sl] (one winner per
+    searchlight, cost summed over the targets), the winner's betas scattered like the ridge solve
+    (csrc/ha_searchlight.c:1378-1429).  Returns (data, best[count], cost[count, A, P])."""
+    count = len(off) - 1
+    best = np.zeros(count, dtype=np.int32)
+    costs = np.zeros((count, len(alphas), len(npcs)))
+    for s in range(count):
+        sl = idx[off[s]:off[s + 1]]
+        B, _, _, _, _, b, c = ensemble_ridge(X[:, sl], Y[:, sl], alphas, npcs, train_li, test_li)
+        best[s] = b
+        costs[s] = c
+        w = None if weights is None else weights[off[s]:off[s + 1]]
+        sparse_scatter_add(indptr, indices, data, sl, sl, B, w)
+    return data, best, costs
+
+
+class Xoshiro256:
+    """xoshiro256** seeded by splitmix64, modulo range reduction (csrc/ha_ensemble.c:12-46)."""
+    M = (1 << 64) - 1
+
+    def __init__(self, seed: int):
+        self.s = []
+        seed &= self.M
+        for _ in range(4):
+            seed = (seed + 0x9E3779B97F4A7C15) & self.M
+            z = seed
+            z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & self.M
+            z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & self.M
+            self.s.append(z ^ (z >> 31))
+
+    @staticmethod
+    def _rotl(x, k):
+        return ((x << k) | (x >> (64 - k))) & Xoshiro256.M
+
+    def next(self) -> int:
+        s = self.s
+        out = (self._rotl((s[1] * 5) & self.M, 7) * 9) & self.M
+        t = (s[1] << 17) & self.M
+        s[2] ^= s[0]
+        s[3] ^= s[1]
+        s[1] ^= s[2]
+        s[0] ^= s[3]
+        s[2] ^= t
+        s[3] = self._rotl(s[3], 45)
+        return out
+
+    def below(self, n: int) -> int:
+        return self.next() % n
+
+
+def ensemble_indices(nt, n_perms, n_folds, blocksize, buffersize, seed, mask=None):
+    """CV splits of csrc/ha_ensemble.c:58-249, draw for draw.  Returns (train_li, test_li)."""
+    rng = Xoshiro256(seed)
+    n_blocks, remainder = nt // blocksize, nt % blocksize
+    padded = nt + 2 * buffersize
+    mapping = None
+    if mask is not None:
+        mask = np.asarray(mask, dtype=bool)
+        mapping = np.full(nt, -1, dtype=np.int64)
+        mapping[mask] = np.arange(int(mask.sum()))
+    train_li, test_li = [], []
+
+    def block_out(mk, centre):
+        lo = max(centre, 0)
+        hi = min(centre + 2 * buffersize, padded - 1)
+        mk[lo:hi + 1] = False
+
+    for _ in range(n_perms):
+        shift = rng.below(remainder + 1)
+        order = list(range(n_blocks))
+        for i in range(n_blocks - 1, 0, -1):
+            j = rng.below(i + 1)
+            order[i], order[j] = order[j], order[i]
+        f0 = 0
+        for fold in range(n_folds):
+            f1 = (fold + 1) * n_blocks // n_folds
+            test_raw = [order[b] * blocksize + k + shift for b in range(f0, f1) for k in range(blocksize)]
+            test_raw = [t for t in test_raw if t < nt]
+            trm = np.ones(padded, dtype=bool)
+            for t in test_raw:
+                block_out(trm, t)
+            if mask is not None:
+                trm[buffersize:buffersize + nt][~mask] = False
+            valid = np.flatnonzero(trm[buffersize:buffersize + nt])
+            if valid.size == 0:
+                raise ValueError("fold without training rows")
+            train = np.array([valid[rng.below(valid.size)] for _ in range(nt)], dtype=np.int64)
+            tem = np.ones(padded, dtype=bool)
+            for i in np.flatnonzero(np.bincount(train, minlength=nt)):
+                block_out(tem, int(i))
+            if mask is not None:
+                tem[buffersize:buffersize + nt][~mask] = False
+            test = np.flatnonzero(tem[buffersize:buffersize + nt])
+            if mapping is not None:
+                train, test = mapping[train], mapping[test]
+            train_li.append(train.astype(np.int32))
+            test_li.append(test.astype(np.int32))
+            f0 = f1
+    return train_li, test_li
+
+
+# ---------------------------------------------------------------------------------------------
 # z-score (csrc/ha_linalg.c:263-291)
 # ---------------------------------------------------------------------------------------------
 

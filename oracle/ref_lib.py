@@ -73,6 +73,23 @@ def lib():
                                     ctypes.c_bool]
         h.ha_ridge.restype = ctypes.c_int
         h.ha_ridge.argtypes = [ctypes.POINTER(TMat), ctypes.POINTER(TMat), ctypes.c_double, ctypes.POINTER(TMat)]
+        h.ha_ridge_grid.restype = ctypes.c_int  # csrc/ha_ridge.h
+        h.ha_ridge_grid.argtypes = [ctypes.POINTER(TMat), c_double_p, c_double_p, ctypes.c_int32, c_int32_p,
+                                    ctypes.c_int32, c_int32_p, ctypes.c_int32, c_double_p]
+        h.ha_ensemble_ridge.restype = ctypes.c_int
+        h.ha_ensemble_ridge.argtypes = [ctypes.POINTER(TMat), c_double_p, c_double_p, ctypes.c_int32, c_int32_p,
+                                        ctypes.c_int32, ctypes.POINTER(c_int32_p), ctypes.POINTER(c_int32_p),
+                                        c_int32_p, c_int32_p, ctypes.c_int32, c_double_p, c_double_p, c_double_p,
+                                        c_double_p, c_int32_p]
+        h.ha_ensemble_indices.restype = ctypes.c_int  # csrc/ha_ensemble.h
+        h.ha_ensemble_indices.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                          ctypes.c_int32, ctypes.c_uint64, ctypes.POINTER(ctypes.c_bool),
+                                          ctypes.POINTER(ctypes.POINTER(c_int32_p)),
+                                          ctypes.POINTER(ctypes.POINTER(c_int32_p)),
+                                          ctypes.POINTER(c_int32_p), ctypes.POINTER(c_int32_p), c_int32_p]
+        h.ha_ensemble_indices_free.restype = None
+        h.ha_ensemble_indices_free.argtypes = [ctypes.POINTER(c_int32_p), ctypes.POINTER(c_int32_p), c_int32_p,
+                                               c_int32_p, ctypes.c_int32]
         _lib = h
         # one BLAS thread per OpenMP thread (the reference parallelises over searchlights)
         import glob
@@ -214,3 +231,73 @@ def searchlight_ridge_csc(X, Y, idx, off, indptr, indices, alpha, weights=None, 
     if rc != 0:
         raise RuntimeError(f"reference ha_searchlight_ridge rc={rc}")
     return data
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def ridge_grid(X, y, alphas, npcs, train_idx=None):
+    """ha_ridge_grid (csrc/ha_ridge.c:97-227): betas[v, a, p] for one target vector y."""
+    h = lib()
+    Xc = np.ascontiguousarray(X, dtype=np.float64)
+    yc = np.ascontiguousarray(y, dtype=np.float64)
+    al = np.ascontiguousarray(alphas, dtype=np.float64)
+    npc = _i32(npcs)
+    out = np.zeros((Xc.shape[1], al.size, npc.size))
+    tx = TMat(_dp(Xc), Xc.shape[0], Xc.shape[1])
+    tr = None if train_idx is None else _i32(train_idx)
+    rc = h.ha_ridge_grid(ctypes.byref(tx), _dp(yc), _dp(al), al.size, _ip(npc), npc.size,
+                         None if tr is None else _ip(tr), 0 if tr is None else tr.size, _dp(out))
+    if rc != 0:
+        raise RuntimeError(f"reference ha_ridge_grid rc={rc}")
+    return out
+
+
+def ensemble_ridge(X, y, alphas, npcs, train_li, test_li):
+    """ha_ensemble_ridge (csrc/ha_ridge.c:229-345) for one target: (weights, pred, r2, alpha, npc)."""
+    h = lib()
+    Xc = np.ascontiguousarray(X, dtype=np.float64)
+    yc = np.ascontiguousarray(y, dtype=np.float64)
+    al = np.ascontiguousarray(alphas, dtype=np.float64)
+    npc = _i32(npcs)
+    trs = [_i32(t) for t in train_li]
+    tes = [_i32(t) if len(t) else np.zeros(1, dtype=np.int32) for t in test_li]
+    trp = (c_int32_p * len(trs))(*[_ip(t) for t in trs])
+    tep = (c_int32_p * len(tes))(*[_ip(t) for t in tes])
+    trn = _i32([t.size for t in trs])
+    ten = _i32([len(t) for t in test_li])
+    nt, nv = Xc.shape
+    w = np.zeros(nv)
+    pred = np.zeros(nt)
+    r2, alpha = ctypes.c_double(), ctypes.c_double()
+    npc_out = ctypes.c_int32()
+    tx = TMat(_dp(Xc), nt, nv)
+    rc = h.ha_ensemble_ridge(ctypes.byref(tx), _dp(yc), _dp(al), al.size, _ip(npc), npc.size, trp, tep, _ip(trn),
+                             _ip(ten), len(trs), _dp(w), _dp(pred), ctypes.byref(r2), ctypes.byref(alpha),
+                             ctypes.byref(npc_out))
+    if rc != 0:
+        raise RuntimeError(f"reference ha_ensemble_ridge rc={rc}")
+    return w, pred, r2.value, alpha.value, npc_out.value
+
+
+def ensemble_indices(nt, n_perms, n_folds, blocksize, buffersize, seed, mask=None):
+    """ha_ensemble_indices (csrc/ha_ensemble.c:58-249): (train_li, test_li) as numpy arrays."""
+    h = lib()
+    tr = ctypes.POINTER(c_int32_p)()
+    te = ctypes.POINTER(c_int32_p)()
+    trn, ten = c_int32_p(), c_int32_p()
+    ns = ctypes.c_int32()
+    mk = None
+    if mask is not None:
+        mk = (ctypes.c_bool * nt)(*[bool(m) for m in mask])
+    rc = h.ha_ensemble_indices(nt, n_perms, n_folds, blocksize, buffersize, ctypes.c_uint64(seed), mk,
+                               ctypes.byref(tr), ctypes.byref(te), ctypes.byref(trn), ctypes.byref(ten),
+                               ctypes.byref(ns))
+    if rc != 0:
+        raise RuntimeError(f"reference ha_ensemble_indices rc={rc}")
+    train_li = [np.ctypeslib.as_array(tr[k], shape=(trn[k],)).copy() for k in range(ns.value)]
+    test_li = [np.ctypeslib.as_array(te[k], shape=(ten[k],)).copy() if ten[k] else np.zeros(0, dtype=np.int32)
+               for k in range(ns.value)]
+    h.ha_ensemble_indices_free(tr, te, trn, ten, ns.value)
+    return train_li, test_li

@@ -14,6 +14,9 @@ self-contained):
                     and ridge (ha_searchlight_procrustes, ha_searchlight_ridge) CSC data
   kat.npz           outputs of ha_procrustes / ha_ridge on the reference harness's
                     known-answer inputs (csrc/ha_test.c:234-366, splitmix64 data)
+  grid.npz          ha_ensemble_indices splits (with and without a mask), ha_ridge_grid betas
+                    (monotone and non-monotone PC counts, bootstrap rows) and ha_ensemble_ridge
+                    outputs on seeded inputs
   python_ref.npz    the Python reference package (src/hyperalignment) on the same small
                     case: procrustes per searchlight and initialize_sparse_matrix
 """
@@ -124,6 +127,41 @@ def make_kat():
     np.savez_compressed(os.path.join(HERE, "kat.npz"), **out)
 
 
+def make_grid():
+    """CV splits (ha_ensemble_indices), ridge grid (ha_ridge_grid) and ensemble ridge
+    (ha_ensemble_ridge) of the compiled reference on small seeded inputs."""
+    out = {}
+    tr, te = R.ensemble_indices(500, 1, 5, 10, 10, 5)
+    out["cv_train"] = np.stack(tr)
+    out["cv_test"] = np.concatenate(te)
+    out["cv_test_sizes"] = np.array([t.size for t in te], dtype=np.int32)
+    rng = np.random.default_rng(12)
+    mask = rng.random(150) > 0.2
+    tr, te = R.ensemble_indices(150, 2, 3, 7, 4, 9, mask)
+    out["cvm_mask"] = mask
+    out["cvm_train"] = np.stack(tr)
+    out["cvm_test"] = np.concatenate(te)
+    out["cvm_test_sizes"] = np.array([t.size for t in te], dtype=np.int32)
+    X = rng.standard_normal((60, 10))
+    y = X @ rng.standard_normal(10) + 0.5 * rng.standard_normal(60)
+    alphas = np.logspace(-3, 3, 7)
+    out["grid_X"], out["grid_y"], out["grid_alphas"] = X, y, alphas
+    out["grid_npcs"] = np.array([2, 4, 20], dtype=np.int32)
+    out["grid_npcs_odd"] = np.array([5, 3, 7, 0, 20], dtype=np.int32)
+    boot = rng.integers(0, 60, 60).astype(np.int32)
+    out["grid_boot"] = boot
+    out["grid_betas"] = R.ridge_grid(X, y, alphas, out["grid_npcs"], boot)
+    out["grid_betas_odd"] = R.ridge_grid(X, y, alphas, out["grid_npcs_odd"])
+    tr, te = R.ensemble_indices(60, 1, 4, 5, 2, 3)
+    out["ens_train"] = np.stack(tr)
+    out["ens_test"] = np.concatenate(te)
+    out["ens_test_sizes"] = np.array([t.size for t in te], dtype=np.int32)
+    w, pred, r2, alpha, npc = R.ensemble_ridge(X, y, alphas, out["grid_npcs"], tr, te)
+    out["ens_w"], out["ens_pred"] = w, pred
+    out["ens_r2"], out["ens_alpha"], out["ens_npc"] = np.float64(r2), np.float64(alpha), np.int32(npc)
+    np.savez_compressed(os.path.join(HERE, "grid.npz"), **out)
+
+
 def make_python_ref():
     sys.path.insert(0, os.path.join(REF_DIR, "src"))
     from hyperalignment.procrustes import procrustes as py_procrustes  # noqa: E402
@@ -143,6 +181,7 @@ if __name__ == "__main__":
     make_small_dense()
     make_small_sparse()
     make_kat()
+    make_grid()
     make_python_ref()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):

@@ -91,3 +91,55 @@ def test_init_reports_missing_gpu(hlib):
         pass
     assert hlib.ha_b200_init() == L.ERROR_INTERNAL
     assert not hlib.ha_b200_available()
+
+
+@pytest.mark.parametrize("pre,args,mask", [("cv", (500, 1, 5, 10, 10, 5), False), ("cvm", (150, 2, 3, 7, 4, 9), True)])
+def test_ensemble_indices_c_abi_bit_exact(hlib, pre, args, mask):
+    # host-only entry: the same draws as the reference's ha_ensemble_indices
+    from hyperalignment_b200 import hyperalignment_c as H
+    g = golden("grid.npz")
+    tr, te = H.ensemble_indices(*args, mask=g["cvm_mask"] if mask else None)
+    sizes = g[pre + "_test_sizes"]
+    rte = np.split(g[pre + "_test"], np.cumsum(sizes)[:-1])
+    for a, b in zip(tr, g[pre + "_train"]):
+        np.testing.assert_array_equal(a, b)
+    for a, b in zip(te, rte):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_ensemble_indices_argument_errors(hlib):
+    buf = np.zeros(100, dtype=np.int32)
+    sz = np.zeros(4, dtype=np.int32)
+    # blocksize 0 (the reference divides by it), and a single fold that leaves no training rows
+    assert hlib.ha_ensemble_indices_b200(20, 1, 2, 0, 1, 1, None, L.iptr(buf), L.iptr(buf), L.iptr(sz)) == L.ERROR_ARG
+    assert hlib.ha_ensemble_indices_b200(20, 1, 1, 5, 2, 1, None, L.iptr(buf), L.iptr(buf), L.iptr(sz)) == L.ERROR_ARG
+
+
+def test_ridge_grid_argument_errors(hlib):
+    # checked on the host before any device work: negative PC counts, a repeated test row,
+    # a training row outside [0, nt), an empty training list
+    X = np.zeros((10, 4))
+    sls = [np.array([0, 1], dtype=np.int32), np.array([2, 3], dtype=np.int32)]
+    indptr = np.array([0, 2, 4, 6, 8], dtype=np.int32)
+    indices = np.array([0, 1, 0, 1, 2, 3, 2, 3], dtype=np.int32)
+    data = np.zeros(8)
+    ok_tr, ok_te = [np.arange(10)], [np.arange(3)]
+    bad = [
+        ([1.0], [-1], ok_tr, ok_te),
+        ([1.0], [2], ok_tr, [np.array([1, 1])]),
+        ([1.0], [2], [np.array([0, 10])], ok_te),
+        ([1.0], [2], [np.zeros(0)], ok_te),
+        ([float("nan")], [2], ok_tr, ok_te),
+    ]
+    idx = np.concatenate(sls)
+    off = np.array([0, 2, 4], dtype=np.int32)
+    best = np.zeros(2, dtype=np.int32)
+    for alphas, npcs, tr, te in bad:
+        al = np.asarray(alphas, dtype=np.float64)
+        pc = np.asarray(npcs, dtype=np.int32)
+        trl, tel = L.IndexLists(tr), L.IndexLists(te)
+        rc = hlib.ha_searchlight_ridge_grid_b200(
+            L.dptr(X), L.dptr(X), 10, 4, L.iptr(idx), L.iptr(off), 2, None, L.iptr(indptr), L.iptr(indices), 8,
+            L.dptr(data), L.dptr(al), al.size, L.iptr(pc), pc.size, trl.ptrs, tel.ptrs, L.iptr(trl.sizes),
+            L.iptr(tel.sizes), 1, L.iptr(best), None, True)
+        assert rc == L.ERROR_ARG

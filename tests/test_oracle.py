@@ -168,3 +168,82 @@ def test_template_identical_subjects_oracle():
     tpl = O.searchlight_template([base, base.copy(), base.copy()], sls.indices, sls.offsets, sls.dists, sls.radius,
                                  True, False, False, 1)
     assert np.abs(tpl - base).max() < 1e-8
+
+
+def _split(g, pre):
+    sizes = g[pre + "_test_sizes"]
+    test = np.split(g[pre + "_test"], np.cumsum(sizes)[:-1])
+    return list(g[pre + "_train"]), test
+
+
+@pytest.mark.parametrize("pre,args,mask", [
+    ("cv", (500, 1, 5, 10, 10, 5), False),   # the temporally blocked 5-fold layout of the grid search
+    ("cvm", (150, 2, 3, 7, 4, 9), True),     # two permutations, masked time points, remapped indices
+])
+def test_ensemble_indices_bit_exact(pre, args, mask):
+    # csrc/ha_ensemble.c:58-249 draw for draw (xoshiro256** / splitmix64, modulo sampling)
+    g = golden("grid.npz")
+    tr, te = O.ensemble_indices(*args, mask=g["cvm_mask"] if mask else None)
+    rtr, rte = _split(g, pre)
+    assert len(tr) == len(rtr)
+    for a, b in zip(tr + te, rtr + rte):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_ensemble_test_sets_overlap():
+    # buffer rows next to a test block can be tested by two folds: the ensemble averages them
+    g = golden("grid.npz")
+    _, te = _split(g, "cv")
+    count = np.zeros(500, dtype=int)
+    for t in te:
+        count[t] += 1
+    assert count.max() >= 2
+
+
+def test_ridge_grid_matches_reference():
+    # csrc/ha_ridge.c:97-227: PC chunks clipped at K, cumulative over p; bootstrap training rows
+    g = golden("grid.npz")
+    B = O.ridge_grid(g["grid_X"], g["grid_y"], g["grid_alphas"], g["grid_npcs"], g["grid_boot"])
+    np.testing.assert_allclose(B, g["grid_betas"], atol=1e-12, rtol=0)
+    # non-monotone PC counts: empty chunks and double-counted components as the reference sums them
+    B = O.ridge_grid(g["grid_X"], g["grid_y"], g["grid_alphas"], g["grid_npcs_odd"])
+    np.testing.assert_allclose(B, g["grid_betas_odd"], atol=1e-12, rtol=0)
+
+
+def test_ensemble_ridge_matches_reference():
+    # csrc/ha_ridge.c:229-345: averaged test predictions, first argmin, r2
+    g = golden("grid.npz")
+    tr, te = _split(g, "ens")
+    w, pred, r2, alpha, npc, best, cost = O.ensemble_ridge(g["grid_X"], g["grid_y"], g["grid_alphas"],
+                                                           g["grid_npcs"], tr, te)
+    np.testing.assert_allclose(w, g["ens_w"], atol=1e-12, rtol=0)
+    np.testing.assert_allclose(pred, g["ens_pred"], atol=1e-12, rtol=0)
+    assert abs(r2 - float(g["ens_r2"])) < 1e-12
+    assert alpha == float(g["ens_alpha"]) and npc == int(g["ens_npc"])
+    assert cost.shape == (g["grid_alphas"].size, g["grid_npcs"].size)
+
+
+def test_ensemble_ridge_multi_target_sums_costs():
+    # the searchlight composition: one winner per searchlight, cost summed over its targets
+    g = golden("grid.npz")
+    tr, te = _split(g, "ens")
+    X = g["grid_X"]
+    Y = np.stack([g["grid_y"], X[:, 0] - X[:, 3], X[:, 5]], axis=1)
+    *_, cost = O.ensemble_ridge(X, Y, g["grid_alphas"], g["grid_npcs"], tr, te)
+    per = sum(O.ensemble_ridge(X, Y[:, k], g["grid_alphas"], g["grid_npcs"], tr, te)[6] for k in range(3))
+    np.testing.assert_allclose(cost, per, rtol=1e-12)
+
+
+def test_grid_oracle_vs_live_reference():
+    from oracle import ref_lib as R
+    if not R.available():
+        pytest.skip("compiled reference not built (make -C oracle)")
+    rng = np.random.default_rng(3)
+    X = rng.standard_normal((90, 14))
+    y = X @ rng.standard_normal(14) + rng.standard_normal(90)
+    al, npcs = np.logspace(-2, 2, 4), [3, 8, 100]
+    tr, te = R.ensemble_indices(90, 1, 3, 6, 3, 21)
+    a = O.ensemble_ridge(X, y, al, npcs, tr, te)
+    b = R.ensemble_ridge(X, y, al, npcs, tr, te)
+    np.testing.assert_allclose(a[0], b[0], atol=1e-12, rtol=0)
+    assert (a[3], a[4]) == (b[3], b[4])

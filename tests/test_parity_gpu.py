@@ -335,3 +335,87 @@ def test_mixed_form_accuracy_at_full_size(gpu):
         worst = max(worst, relf(T, O.procrustes(w.X[:, sl], w.Y[:, sl])))
     assert worst <= T_REL, worst
     assert 0 < plan.stats()["n_fp64"] < 0.1 * w.sls.count
+
+
+# ---------------------------------------------------------------------------------------------
+# ridge grid search with CV ensembles (csrc/ha_ridge.c:97-345, splits csrc/ha_ensemble.c:58-249)
+# composed per searchlight: one winner per searchlight, cost summed over its targets
+# ---------------------------------------------------------------------------------------------
+
+GRID_REL = 1e-8   # float64 Jacobi eigen route vs the reference's SVD formula (costs, betas)
+
+
+def _grid_case(seed, nv, nt, lo, hi, noise=1.0):
+    w = W.small_case(seed=seed, nv=nv, nt=nt, lo=lo, hi=hi)
+    rng = np.random.default_rng(seed + 100)
+    Y = 0.5 * w.Y + noise * rng.standard_normal(w.Y.shape)  # noisy targets: the winners spread over the grid
+    return w, Y
+
+
+def _check_grid(w, Y, alphas, npcs, tr, te):
+    s = w.sls
+    sls = sls_lists(s.indices, s.offsets)
+    indptr, indices = H.sparse_pattern(sls, w.nv)
+    wts = O.searchlight_weights(s.indices, s.offsets, s.dists, s.radius, w.nv)
+    data = np.zeros(indices.size)
+    best, costs = H.searchlight_ridge_grid(w.X, Y, sls, indptr, indices, data, alphas, npcs, tr, te,
+                                           weights=sls_lists(wts, s.offsets), return_costs=True)
+    ref, rbest, rcosts = O.searchlight_ridge_grid_csc(w.X, Y, s.indices, s.offsets, indptr, indices,
+                                                      np.zeros(indices.size), alphas, npcs, tr, te, wts)
+    np.testing.assert_allclose(costs, rcosts, rtol=GRID_REL, atol=0)
+    # the winner is optimal to the cost tolerance; it is the oracle's winner unless two different
+    # grid points tie within that tolerance (grid points that coincide, such as PC counts past the
+    # searchlight size, tie exactly and both take the first)
+    flat = rcosts.reshape(rcosts.shape[0], -1)
+    gflat = costs.reshape(costs.shape[0], -1)
+    rows = np.arange(flat.shape[0])
+    assert np.all(flat[rows, best] <= flat.min(axis=1) * (1 + 1e-9))
+    near = flat <= flat.min(axis=1, keepdims=True) * (1 + 1e-7)
+    clear = np.array([np.ptp(gflat[q][near[q]]) == 0.0 for q in rows])
+    assert clear.mean() > 0.9
+    np.testing.assert_array_equal(best[clear], rbest[clear])
+    if clear.all():
+        assert relf(data, ref) <= GRID_REL
+    return best
+
+
+@pytest.mark.parametrize("lo,hi,alphas,distinct", [
+    (5, 30, np.logspace(-3, 3, 5), 3),    # resident Jacobi eigen solves; winners spread over the grid
+    (60, 140, np.logspace(-1, 5, 5), 1),  # blocked eigen solves (n up to 140 > 120 rows: K clipping)
+])
+def test_ridge_grid_vs_oracle(gpu, lo, hi, alphas, distinct):
+    # reference CV splits (overlapping test sets)
+    w, Y = _grid_case(21, 642, 120, lo, hi)
+    tr, te = H.ensemble_indices(120, 1, 4, 6, 3, 17)
+    best = _check_grid(w, Y, alphas, [5, 20, 10000], tr, te)
+    assert np.unique(best).size >= distinct  # the grid search is doing real selection
+
+
+def test_ridge_grid_few_rows_odd_pcs_untested_rows(gpu):
+    # fewer training rows than vertices (K = rows clips the PC chunks), non-monotone PC counts,
+    # hand-made folds with rows no model tests and rows two models test
+    w, Y = _grid_case(5, 162, 36, 20, 48)
+    rng = np.random.default_rng(9)
+    tr = [rng.integers(0, 36, 36).astype(np.int32) for _ in range(3)]
+    te = [np.arange(0, 10, dtype=np.int32), np.arange(8, 20, dtype=np.int32), np.arange(24, 30, dtype=np.int32)]
+    _check_grid(w, Y, np.array([1e-2, 1.0, 30.0]), [8, 4, 12, 0, 100], tr, te)
+
+
+def test_ridge_grid_device_deterministic(gpu):
+    import torch
+    w, Y = _grid_case(8, 642, 120, 10, 40)
+    tr, te = H.ensemble_indices(120, 1, 5, 6, 3, 4)
+    plan = Plan(w.nt, w.nv, w.sls.indices, w.sls.offsets, w.sls.dists, w.sls.radius)
+    dX = torch.from_numpy(np.asfortranarray(w.X).ravel(order="F")).cuda()
+    dY = torch.from_numpy(np.asfortranarray(Y).ravel(order="F")).cuda()
+    outs = []
+    for _ in range(2):
+        vals = torch.zeros(plan.nnz, dtype=torch.float64, device="cuda")
+        best = torch.full((w.sls.count,), -1, dtype=torch.int32, device="cuda")
+        plan.ridge_grid_device(dX.data_ptr(), dY.data_ptr(), vals.data_ptr(), best.data_ptr(),
+                               np.logspace(-3, 3, 4), [5, 10, 40], tr, te)
+        torch.cuda.synchronize()
+        outs.append((vals.cpu().numpy(), best.cpu().numpy()))
+    plan.close()
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+    assert outs[0][1].min() >= 0
