@@ -51,6 +51,7 @@ struct TimedLaunch {
 	cudaEvent_t a, b;
 };
 std::vector<TimedLaunch> g_timed;
+cudaEvent_t g_time_base = nullptr;  // recorded when timing starts and after every read-out
 double g_kernel_ms[kHaB200NumKernelKinds] = {0};
 int64_t g_kernel_n[kHaB200NumKernelKinds] = {0};
 
@@ -165,6 +166,50 @@ size_t fp32_jacobi_budget() {
 	}
 	return b;
 }
+
+// Side streams for the size buckets of a chunk.  Buckets own disjoint scratch regions, so their
+// kernels may overlap and fill the SMs that one bucket's last wave leaves idle; begin() makes
+// every side stream wait for the caller's stream, end() makes the caller's stream wait for all.
+struct StreamFan {
+	static constexpr int kN = 6;
+	cudaStream_t s[kN] = {};
+	cudaEvent_t fork = nullptr, join[kN] = {};
+	bool ready = false;
+	int init() {
+		if (ready) return kHaSuccess;
+		for (int i = 0; i < kN; i++) {
+			HA_CUDA(cudaStreamCreateWithFlags(&s[i], cudaStreamNonBlocking));
+			HA_CUDA(cudaEventCreateWithFlags(&join[i], cudaEventDisableTiming));
+		}
+		HA_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+		ready = true;
+		return kHaSuccess;
+	}
+	int begin(cudaStream_t main) {
+		int rc = init();
+		if (rc != kHaSuccess) return rc;
+		HA_CUDA(cudaEventRecord(fork, main));
+		for (int i = 0; i < kN; i++) HA_CUDA(cudaStreamWaitEvent(s[i], fork, 0));
+		return kHaSuccess;
+	}
+	cudaStream_t at(int i) const { return s[i % kN]; }
+	int end(cudaStream_t main) {
+		for (int i = 0; i < kN; i++) {
+			HA_CUDA(cudaEventRecord(join[i], s[i]));
+			HA_CUDA(cudaStreamWaitEvent(main, join[i], 0));
+		}
+		return kHaSuccess;
+	}
+	void release() {
+		if (!ready) return;
+		for (int i = 0; i < kN; i++) {
+			cudaStreamDestroy(s[i]);
+			cudaEventDestroy(join[i]);
+		}
+		cudaEventDestroy(fork);
+		ready = false;
+	}
+} g_fan;
 
 struct Bucket {
 	int first, count;  // range in the chunk's work array
@@ -656,31 +701,39 @@ int run_procrustes(HaB200Plan *P, const double *d_X, const double *d_Y, bool ref
 			float *A = reinterpret_cast<float *>(P->scrA.p);
 			float *V = reinterpret_cast<float *>(P->scrV.p);
 			jp.only_flagged = 0;
-			for (const Bucket &b : ch.b32) {
+			if ((rc = g_fan.begin(st)) != kHaSuccess) return rc;
+			for (size_t bi = 0; bi < ch.b32.size(); bi++) {
+				const Bucket &b = ch.b32[bi];
+				const cudaStream_t bs = g_fan.at((int)bi);
 				const SlWork *wk = ch.d_w32 + b.first;
-				{ HA_LAUNCH(kHaB200KXcov32, st); k_xcov<float, 32><<<b.count, kBlock, 0, st>>>(wk, P->idx.p, P->X32.p, P->Y32.p, ntp, nt, A, P->stats.p, 0); }
+				{ HA_LAUNCH(kHaB200KXcov32, bs); k_xcov<float, 32><<<b.count, kBlock, 0, bs>>>(wk, P->idx.p, P->X32.p, P->Y32.p, ntp, nt, A, P->stats.p, 0); }
 				{
-					HA_LAUNCH(kHaB200KJacobi32, st);
-					if ((rc = launch_jacobi<float>(b.rpl, b.count, b.threads, b.smem, st, wk, A, V, T, P->stats.p, P->uv.p, jp)) != kHaSuccess)
+					HA_LAUNCH(kHaB200KJacobi32, bs);
+					if ((rc = launch_jacobi<float>(b.rpl, b.count, b.threads, b.smem, bs, wk, A, V, T, P->stats.p, P->uv.p, jp)) != kHaSuccess)
 						return rc;
 				}
-				if (b.blocked) { HA_LAUNCH(kHaB200KFormT32, st); k_form_t_global<float><<<b.count, kBlock, 0, st>>>(wk, A, V, T, P->stats.p, rowmajor, 0); }
+				if (b.blocked) { HA_LAUNCH(kHaB200KFormT32, bs); k_form_t_global<float><<<b.count, kBlock, 0, bs>>>(wk, A, V, T, P->stats.p, rowmajor, 0); }
 			}
+			if ((rc = g_fan.end(st)) != kHaSuccess) return rc;
 		}
 		if (solver != kHaB200SolverFP32) {
 			double *A = P->scrA.p, *V = P->scrV.p;
 			const int only = (solver == kHaB200SolverMixed) ? 1 : 0;
 			jp.only_flagged = only;
-			for (const Bucket &b : ch.b64) {
+			if ((rc = g_fan.begin(st)) != kHaSuccess) return rc;
+			for (size_t bi = 0; bi < ch.b64.size(); bi++) {
+				const Bucket &b = ch.b64[bi];
+				const cudaStream_t bs = g_fan.at((int)bi);
 				const SlWork *wk = ch.d_w64 + b.first;
-				{ HA_LAUNCH(kHaB200KXcov64, st); k_xcov<double, 16><<<b.count, kBlock, 0, st>>>(wk, P->idx.p, d_X, d_Y, nt, nt, A, P->stats.p, only); }
+				{ HA_LAUNCH(kHaB200KXcov64, bs); k_xcov<double, 16><<<b.count, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_Y, nt, nt, A, P->stats.p, only); }
 				{
-					HA_LAUNCH(kHaB200KJacobi64, st);
-					if ((rc = launch_jacobi<double>(b.rpl, b.count, b.threads, b.smem, st, wk, A, V, T, P->stats.p, P->uv.p, jp)) != kHaSuccess)
+					HA_LAUNCH(kHaB200KJacobi64, bs);
+					if ((rc = launch_jacobi<double>(b.rpl, b.count, b.threads, b.smem, bs, wk, A, V, T, P->stats.p, P->uv.p, jp)) != kHaSuccess)
 						return rc;
 				}
-				if (b.blocked) { HA_LAUNCH(kHaB200KFormT64, st); k_form_t_global<double><<<b.count, kBlock, 0, st>>>(wk, A, V, T, P->stats.p, rowmajor, only); }
+				if (b.blocked) { HA_LAUNCH(kHaB200KFormT64, bs); k_form_t_global<double><<<b.count, kBlock, 0, bs>>>(wk, A, V, T, P->stats.p, rowmajor, only); }
 			}
+			if ((rc = g_fan.end(st)) != kHaSuccess) return rc;
 		}
 		if (solver == kHaB200SolverMixed) {
 			{ HA_LAUNCH(kHaB200KRefine, st); k_ns_refine<<<nsl, kBlock, 0, st>>>(ch.d_w32, T, reinterpret_cast<float *>(P->scrV.p),
@@ -719,12 +772,16 @@ int run_ridge(HaB200Plan *P, const double *d_X, const double *d_Y, double alpha,
 		const int nsl = ch.s1 - ch.s0;
 		HA_CUDA(cudaMemsetAsync(P->stats.p, 0, (size_t)nsl * sizeof(SlStats), st));
 		double *G = P->scrA.p, *R = P->scrV.p;
-		for (const Bucket &b : ch.b64) {
+		if ((rc = g_fan.begin(st)) != kHaSuccess) return rc;
+		for (size_t bi = 0; bi < ch.b64.size(); bi++) {
+			const Bucket &b = ch.b64[bi];
+			const cudaStream_t bs = g_fan.at((int)bi);
 			const SlWork *wk = ch.d_w64 + b.first;
-			{ HA_LAUNCH(kHaB200KXcov64, st); k_xcov<double, 16><<<b.count, kBlock, 0, st>>>(wk, P->idx.p, d_X, d_X, nt, nt, G, P->stats.p, 0); }
-			{ HA_LAUNCH(kHaB200KXcov64, st); k_xcov<double, 16><<<b.count, kBlock, 0, st>>>(wk, P->idx.p, d_X, d_Y, nt, nt, R, P->stats.p, 0); }
-			{ HA_LAUNCH(kHaB200KRidge, st); k_ridge_chol<<<b.count, kBlock, 0, st>>>(wk, G, R, P->scrT64.p, alpha, rowmajor, P->stats.p); }
+			{ HA_LAUNCH(kHaB200KXcov64, bs); k_xcov<double, 16><<<b.count, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_X, nt, nt, G, P->stats.p, 0); }
+			{ HA_LAUNCH(kHaB200KXcov64, bs); k_xcov<double, 16><<<b.count, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_Y, nt, nt, R, P->stats.p, 0); }
+			{ HA_LAUNCH(kHaB200KRidge, bs); k_ridge_chol<<<b.count, kBlock, 0, bs>>>(wk, G, R, P->scrT64.p, alpha, rowmajor, P->stats.p); }
 		}
+		if ((rc = g_fan.end(st)) != kHaSuccess) return rc;
 		{ HA_LAUNCH(kHaB200KScale, st); k_scale<<<(nsl + 127) / 128, 128, 0, st>>>(ch.d_w64, nsl, P->idx.p, nullptr, P->stats.p, nt, 0, P->scale.p); }
 		{ HA_LAUNCH(kHaB200KScale, st); k_count_flags<<<(nsl + 127) / 128, 128, 0, st>>>(P->stats.p, nsl, P->counters.p); }
 		{ HA_LAUNCH(kHaB200KReduce, st); k_reduce<double><<<nv, kBlock, red_smem, st>>>(P->vlptr.p, P->vlent.p, P->off.p, P->idx.p,
@@ -920,18 +977,24 @@ int run_ridge_grid(HaB200Plan *P, const double *d_X, const double *d_Y, const Gr
 			for (int mo = 0; mo < gp.models; mo++) {
 				const GridModel &md = gs.mdl[mo];
 				const int32_t *tr = P->grows.p + md.tr_ofs;
-				for (const Bucket &b : ch.b64) {
+				if ((rc = g_fan.begin(st)) != kHaSuccess) return rc;
+				for (size_t bi = 0; bi < ch.b64.size(); bi++) {
+					const Bucket &b = ch.b64[bi];
 					const int x0 = std::max(i0, b.first), x1 = std::min(i1, b.first + b.count);
 					if (x1 <= x0) continue;
+					const cudaStream_t bs = g_fan.at((int)bi);
 					const SlWork *wk = ch.d_w64 + x0;
-					{ HA_LAUNCH(kHaB200KXcov64, st); k_xcov_rows<16><<<x1 - x0, kBlock, 0, st>>>(wk, P->idx.p, d_X, d_X, nt, tr, md.tr_n, A, P->gridscr.p, gp, 0); }
-					{ HA_LAUNCH(kHaB200KXcov64, st); k_xcov_rows<16><<<x1 - x0, kBlock, 0, st>>>(wk, P->idx.p, d_X, d_Y, nt, tr, md.tr_n, A, P->gridscr.p, gp, 1); }
+					// Gram into the V scratch, its pivoted Cholesky factor into the A scratch
+					{ HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16><<<x1 - x0, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_X, nt, tr, md.tr_n, V, P->gridscr.p, gp, 0); }
+					{ HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16><<<x1 - x0, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_Y, nt, tr, md.tr_n, A, P->gridscr.p, gp, 1); }
+					{ HA_LAUNCH(kHaB200KGrid, bs); k_pchol<<<x1 - x0, kBlock, 0, bs>>>(wk, V, A, P->stats.p); }
 					{
-						HA_LAUNCH(kHaB200KJacobi64, st);
-						if ((rc = launch_jacobi<double>(b.rpl, x1 - x0, b.threads, b.smem, st, wk, A, V, P->scrT.p, P->stats.p, P->uv.p, jp)) != kHaSuccess)
+						HA_LAUNCH(kHaB200KJacobi64, bs);
+						if ((rc = launch_jacobi<double>(b.rpl, x1 - x0, b.threads, b.smem, bs, wk, A, V, P->scrT.p, P->stats.p, P->uv.p, jp)) != kHaSuccess)
 							return rc;
 					}
 				}
+				if ((rc = g_fan.end(st)) != kHaSuccess) return rc;
 				{ HA_LAUNCH(kHaB200KGrid, st); k_grid_model<<<i1 - i0, kBlock, 0, st>>>(ch.d_w64 + i0, P->idx.p, d_X, V, P->uv.p, mo, P->gridscr.p, gp); }
 			}
 			{ HA_LAUNCH(kHaB200KGrid, st); k_grid_eval<<<i1 - i0, kBlock, 0, st>>>(ch.d_w64 + i0, P->idx.p, d_Y, P->gridscr.p, gp, P->scrT64.p, rowmajor, d_best, d_cost); }
@@ -1359,6 +1422,7 @@ void ha_b200_cleanup(void) {
 		g_cached_plan = nullptr;
 	}
 	g_bufs.release();
+	g_fan.release();
 	g_inited = false;
 }
 
@@ -1579,6 +1643,7 @@ int ha_b200_plan_ridge_device(HaB200Plan *P, const double *d_X, const double *d_
 void ha_b200_set_kernel_timing(bool on) {
 	std::lock_guard<std::recursive_mutex> lk(g_mu);
 	g_timing = on;
+	if (on && (g_time_base || cudaEventCreate(&g_time_base) == cudaSuccess)) cudaEventRecord(g_time_base, 0);
 }
 
 int ha_b200_plan_ridge_grid_device(HaB200Plan *P, const double *d_X, const double *d_Y, const double *alphas,
@@ -1598,14 +1663,38 @@ int ha_b200_plan_ridge_grid_device(HaB200Plan *P, const double *d_X, const doubl
 
 int ha_b200_kernel_times(double *ms, int64_t *launches) {
 	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	// per kind: the union of the launch intervals (launches of one kind on different side streams
+	// overlap; for serial launches the union is the sum of the durations)
+	std::vector<std::vector<std::pair<float, float>>> iv(kHaB200NumKernelKinds);
 	for (auto &t : g_timed) {
-		float e = 0.0f;
-		if (cudaEventSynchronize(t.b) == cudaSuccess && cudaEventElapsedTime(&e, t.a, t.b) == cudaSuccess)
-			g_kernel_ms[t.kind] += e;
+		float a = 0.0f, b = 0.0f;
+		if (cudaEventSynchronize(t.b) == cudaSuccess) {
+			if (g_time_base && cudaEventElapsedTime(&a, g_time_base, t.a) == cudaSuccess &&
+			    cudaEventElapsedTime(&b, g_time_base, t.b) == cudaSuccess)
+				iv[t.kind].push_back({a, b});
+			else if (cudaEventElapsedTime(&b, t.a, t.b) == cudaSuccess)
+				g_kernel_ms[t.kind] += b;
+		}
 		cudaEventDestroy(t.a);
 		cudaEventDestroy(t.b);
 	}
 	g_timed.clear();
+	for (int k = 0; k < kHaB200NumKernelKinds; k++) {
+		auto &v = iv[k];
+		std::sort(v.begin(), v.end());
+		double lo = 0.0, hi = -1.0;
+		for (auto &x : v) {
+			if (x.first > hi) {
+				if (hi > lo) g_kernel_ms[k] += hi - lo;
+				lo = x.first;
+				hi = x.second;
+			} else if (x.second > hi) {
+				hi = x.second;
+			}
+		}
+		if (hi > lo) g_kernel_ms[k] += hi - lo;
+	}
+	if (g_time_base) cudaEventRecord(g_time_base, 0);
 	for (int k = 0; k < kHaB200NumKernelKinds; k++) {
 		if (ms) ms[k] = g_kernel_ms[k];
 		if (launches) launches[k] = g_kernel_n[k];

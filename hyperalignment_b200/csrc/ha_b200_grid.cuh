@@ -146,6 +146,93 @@ __global__ void __launch_bounds__(256) k_xcov_rows(const SlWork *__restrict__ wo
 		for (int64_t e = (int64_t)n * n + threadIdx.x; e < (int64_t)n * ncol; e += 256) A[e] = 0.0;
 }
 
+// Pivoted Cholesky G = sum_k r_k r_k^T (right-looking; pivot = largest remaining diagonal, ties to
+// the smaller vertex index), stopped when the largest remaining diagonal is at most
+// n * eps * max(diag G).  The Schur complements overwrite G (column-major, ld n, at Gscr + w.aofs);
+// r_k (original vertex order, zero at earlier pivots) becomes column k of Rt (ld n, ncol columns,
+// the rest zero), so G = Rt Rt^T; the number of columns (the numerical rank) goes to the stats.  The one-sided Jacobi rotations then run on Rt: its columns
+// come in decreasing, graded norms and only rank(G) of them are nonzero, which takes fewer sweeps
+// than rotating G itself and needs no accumulated rotations.
+__global__ void __launch_bounds__(256) k_pchol(const SlWork *__restrict__ work, double *__restrict__ Gscr,
+                                               double *__restrict__ Rscr, SlStats *__restrict__ stats) {
+	__shared__ int rem[kGridMaxN];      // vertices not yet pivoted (positions 0 .. m-1)
+	__shared__ double rk[kGridMaxN];    // the current r_k at those positions
+	__shared__ double rv[32];
+	__shared__ int ri[32], rpos[32];
+	__shared__ double s_tol, s_piv;
+	__shared__ int s_pos;
+	const SlWork w = work[blockIdx.x];
+	const int n = w.n, ncol = w.nblk * w.bsz;
+	double *S = Gscr + w.aofs;
+	double *Rt = Rscr + w.aofs;
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+	for (int i = threadIdx.x; i < n; i += blockDim.x) rem[i] = i;
+	for (int64_t e = threadIdx.x; e < (int64_t)n * ncol; e += blockDim.x) Rt[e] = 0.0;
+	{
+		double mx = 0.0;
+		for (int i = threadIdx.x; i < n; i += blockDim.x) mx = fmax(mx, S[(int64_t)i * n + i]);
+		for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+		if (lane == 0) rv[warp] = mx;
+		__syncthreads();
+		if (threadIdx.x == 0) {
+			double t = 0.0;
+			for (int q = 0; q < nwarp; q++) t = fmax(t, rv[q]);
+			s_tol = (double)n * 2.220446049250313e-16 * t;
+		}
+		__syncthreads();
+	}
+	int m = n, k = 0;
+	for (; k < n; k++) {
+		// pivot: largest remaining diagonal (ties: smaller vertex index)
+		double bv = -1.0;
+		int bi = 0x7fffffff, bpos = 0;
+		for (int a = threadIdx.x; a < m; a += blockDim.x) {
+			const int v = rem[a];
+			const double d = S[(int64_t)v * n + v];
+			if (d > bv || (d == bv && v < bi)) { bv = d; bi = v; bpos = a; }
+		}
+		for (int o = 16; o > 0; o >>= 1) {
+			const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+			const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+			const int op = __shfl_xor_sync(0xffffffffu, bpos, o);
+			if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; bpos = op; }
+		}
+		if (lane == 0) { rv[warp] = bv; ri[warp] = bi; rpos[warp] = bpos; }
+		__syncthreads();
+		if (threadIdx.x == 0) {
+			double v = rv[0];
+			int vi = ri[0], pos = rpos[0];
+			for (int q = 1; q < nwarp; q++)
+				if (rv[q] > v || (rv[q] == v && ri[q] < vi)) { v = rv[q]; vi = ri[q]; pos = rpos[q]; }
+			s_piv = v;
+			s_pos = pos;
+		}
+		__syncthreads();
+		if (!(s_piv > s_tol)) break;
+		const int a = s_pos, p = rem[a];
+		const double rp = sqrt(s_piv);
+		for (int b = threadIdx.x; b < m; b += blockDim.x) {
+			const double r = (b == a) ? rp : S[(int64_t)p * n + rem[b]] / rp;
+			rk[b] = r;
+			Rt[(int64_t)k * n + rem[b]] = r;
+		}
+		__syncthreads();
+		// Schur complement on the remaining vertices other than the pivot
+		for (int c = warp; c < m; c += nwarp) {
+			if (c == a) continue;
+			const double rc = rk[c];
+			double *Sc = S + (int64_t)rem[c] * n;
+			for (int b = lane; b < m; b += 32)
+				if (b != a) Sc[rem[b]] -= rk[b] * rc;
+		}
+		__syncthreads();
+		if (threadIdx.x == 0) rem[a] = rem[m - 1];
+		m--;
+		__syncthreads();
+	}
+	if (threadIdx.x == 0) stats[w.slot].ncols = max(k, 1);
+}
+
 // Rank of every component by decreasing lambda (ties by index): order[r] = k.
 __device__ __forceinline__ void rank_desc(const double *lam, int n, int *order) {
 	for (int k = threadIdx.x; k < n; k += blockDim.x) {
@@ -159,8 +246,9 @@ __device__ __forceinline__ void rank_desc(const double *lam, int n, int *order) 
 	}
 }
 
-// One CV model of every searchlight: V (column-major, ld n) in the V scratch and lambda in the
-// u/v buffer come from the float64 Jacobi kernel in eigenvector mode; C is in the grid scratch.
+// One CV model of every searchlight: the eigenvectors (column-major, ld n) in the V scratch and
+// lambda in the u/v buffer come from the float64 Jacobi kernel in eigenvector mode run on the
+// pivoted Cholesky factor of the Gram; C is in the grid scratch.
 // Stores V, lambda in decreasing-lambda order, Q = V^T C and E = X_te V for the model.
 __global__ void __launch_bounds__(256) k_grid_model(const SlWork *__restrict__ work, const int32_t *__restrict__ sl_idx,
                                                     const double *__restrict__ X, const double *__restrict__ Vscr,

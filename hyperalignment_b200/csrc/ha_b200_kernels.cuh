@@ -66,7 +66,7 @@ struct SlStats {
 	int32_t k_min;    // column of the smallest singular value
 	int32_t flags;    // bit 0: unconverged, bit 1: ill-conditioned (re-solved in FP64), bit 2: reflected
 	int32_t sweeps;   // Jacobi sweeps of the last solve
-	int32_t pad;
+	int32_t ncols;    // eigenvector mode: the nonzero columns of A lead and number ncols (0: all)
 };
 
 enum : int32_t { kFlagUnconverged = 1, kFlagIllCond = 2, kFlagReflected = 4, kFlagFP64 = 8 };
@@ -323,14 +323,19 @@ __device__ __forceinline__ Real jacobi_pairs(Real *B, Real *V, Real *nrm, const 
 		const Real c = __shfl_sync(0xffffffffu, myc, k);
 		const Real s = __shfl_sync(0xffffffffu, mys, k);
 		Real *bp = B + p[k] * LD + lane, *bq = B + q[k] * LD + lane;
-		Real *vp = V + p[k] * LD + lane, *vq = V + q[k] * LD + lane;
 #pragma unroll
 		for (int r = 0; r < RPL; r++) {
 			bp[32 * r] = c * x[k][r] - s * y[k][r];
 			bq[32 * r] = s * x[k][r] + c * y[k][r];
-			const Real u = vp[32 * r], w = vq[32 * r];
-			vp[32 * r] = c * u - s * w;
-			vq[32 * r] = s * u + c * w;
+		}
+		if (V) {  // null when the rotations are not accumulated (eigenvector mode)
+			Real *vp = V + p[k] * LD + lane, *vq = V + q[k] * LD + lane;
+#pragma unroll
+			for (int r = 0; r < RPL; r++) {
+				const Real u = vp[32 * r], w = vq[32 * r];
+				vp[32 * r] = c * u - s * w;
+				vq[32 * r] = s * u + c * w;
+			}
 		}
 		rotated = true;
 	}
@@ -526,7 +531,8 @@ struct JacobiParams {
 	int t_rowmajor;
 	double ill_ratio;  // sigma_min / sigma_max below this -> kFlagIllCond
 	double weak;       // columns with sigma <= weak * eps * sigma_max are re-orthogonalised / completed
-	int eig;           // eigenvector mode: write V (column-major, ld n) to the V scratch and sigma to uvbuf
+	int eig;           // eigenvector mode (A A^T = G): no V; write u_c = b_c / sigma_c (column-major, ld n,
+	                   // zero for numerically zero columns) to the V scratch and sigma_c^2 to uvbuf
 	int only_flagged;  // process only searchlights whose stats carry kFlagIllCond (FP64 re-solve)
 };
 
@@ -584,7 +590,7 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) k_jacobi(const
 		for (sweep = 0; sweep < prm.max_sweeps; sweep++) {
 			column_norms<Real, RPL>(Bs, nrm, mst);
 			bool rot = false;
-			Real mc = jacobi_full_rr<Real, RPL>(Bs, Vs, nrm, 2 * bsz, tol, rot);
+			Real mc = jacobi_full_rr<Real, RPL>(Bs, prm.eig ? nullptr : Vs, nrm, 2 * bsz, tol, rot);
 			mc = block_max_nonneg(mc, red);
 			if (mc <= tol_conv) {
 				converged = true;
@@ -593,41 +599,50 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) k_jacobi(const
 			}
 		}
 	} else {
-		for (int e = threadIdx.x; e < ncol * n; e += blockDim.x) {
-			const int c = e / n, i = e - c * n;
-			Vg[e] = (c == i) ? Real(1) : Real(0);
-		}
+		if (!prm.eig)
+			for (int e = threadIdx.x; e < ncol * n; e += blockDim.x) {
+				const int c = e / n, i = e - c * n;
+				Vg[e] = (c == i) ? Real(1) : Real(0);
+			}
+		Real *Vst = prm.eig ? nullptr : Vs;
 		for (int e = threadIdx.x; e < mst * LD; e += blockDim.x) {
 			Bs[e] = Real(0);
 			Vs[e] = Real(0);
 		}
 		__syncthreads();
+		// only the blocks holding the leading nonzero columns take part (eigenvector mode)
+		int nb = nblk;
+		if (prm.eig && stats[w.slot].ncols > 0) {
+			nb = max(2, (stats[w.slot].ncols + bsz - 1) / bsz);
+			nb += nb & 1;
+			nb = min(nb, nblk);
+		}
 		for (sweep = 0; sweep < prm.max_sweeps; sweep++) {
 			Real mc = 0;
 			bool rot = false;
-			for (int br = 0; br < nblk - 1; br++) {
-				for (int k = 0; k < nblk / 2; k++) {
+			for (int br = 0; br < nb - 1; br++) {
+				for (int k = 0; k < nb / 2; k++) {
 					int I, J;
-					rr_pair(nblk, br, k, I, J);
+					rr_pair(nb, br, k, I, J);
 					for (int e = threadIdx.x; e < 2 * bsz * n; e += blockDim.x) {
 						const int c = e / n, i = e - c * n;
 						const int gc = (c < bsz) ? I * bsz + c : J * bsz + (c - bsz);
 						Bs[c * LD + i] = Ag[gc * n + i];
-						Vs[c * LD + i] = Vg[gc * n + i];
+						if (Vst) Vs[c * LD + i] = Vg[gc * n + i];
 					}
 					__syncthreads();
 					column_norms<Real, RPL>(Bs, nrm, mst);
 					Real c;
 					if (br == 0)
-						c = jacobi_full_rr<Real, RPL>(Bs, Vs, nrm, 2 * bsz, tol, rot);
+						c = jacobi_full_rr<Real, RPL>(Bs, Vst, nrm, 2 * bsz, tol, rot);
 					else
-						c = jacobi_cross<Real, RPL>(Bs, Vs, nrm, bsz, tol, rot);
+						c = jacobi_cross<Real, RPL>(Bs, Vst, nrm, bsz, tol, rot);
 					mc = c > mc ? c : mc;
 					for (int e = threadIdx.x; e < 2 * bsz * n; e += blockDim.x) {
 						const int cc = e / n, i = e - cc * n;
 						const int gc = (cc < bsz) ? I * bsz + cc : J * bsz + (cc - bsz);
 						Ag[gc * n + i] = Bs[cc * LD + i];
-						Vg[gc * n + i] = Vs[cc * LD + i];
+						if (Vst) Vg[gc * n + i] = Vs[cc * LD + i];
 					}
 					__syncthreads();
 				}
@@ -700,15 +715,18 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) k_jacobi(const
 		}
 		__syncthreads();
 	}
-	// eigenvector mode (symmetric positive semi-definite A): B = A V = V diag(lambda), so the column
-	// norms are the eigenvalues and V holds the eigenvectors
+	// eigenvector mode: A W = B with orthogonal columns, so G = A A^T = B B^T has the eigenvectors
+	// b_c / sigma_c and the eigenvalues sigma_c^2
 	if (prm.eig) {
-		if (resident)
-			for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
-				const int c = e / n, i = e - c * n;
-				Vg[e] = Vs[c * LD + i];
-			}
-		for (int k = threadIdx.x; k < n; k += blockDim.x) uvbuf[w.uvofs + k] = (double)sg[k];
+		for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+			const int c = e / n, i = e - c * n;
+			const Real sc = sg[c];
+			Vg[e] = (sc * sc > tol.zero2) ? B[c * ldb + i] / sc : Real(0);
+		}
+		for (int k = threadIdx.x; k < n; k += blockDim.x) {
+			const double sk = (double)sg[k];
+			uvbuf[w.uvofs + k] = (sg[k] * sg[k] > tol.zero2) ? sk * sk : 0.0;
+		}
 		return;
 	}
 	// normalise columns: u_c = b_c / sigma_c (in place)

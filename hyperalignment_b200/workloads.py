@@ -221,6 +221,20 @@ def template_procrustes_pair(seed: int = 0, nv: int = 10242, nt: int = 400) -> W
     return Workload("template_procrustes", subj[1], subj[0], sls, True, True)
 
 
+GRID_ALPHAS = np.logspace(-3.0, 3.0, 10)   # 10 log-spaced ridge penalties in [1e-3, 1e3]
+GRID_NPCS = np.array([10, 20, 50, 1 << 30], dtype=np.int32)  # PC counts; the last is "all" (clipped at K)
+
+
+def ridge_grid_pair(seed: int = 0, nv: int = 40962, nt: int = 500, size_lo: int = 50, size_hi: int = 500,
+                    n_subj: int = 2, pair=(0, 1)) -> Workload:
+    """Searchlight ridge grid search inputs: subjects of the hemisphere generator with AR(1)
+    noise (rho 0.5), searchlight sizes uniform in [size_lo, size_hi]; X = subject pair[0],
+    Y = subject pair[1] (the ridge predicts Y's searchlight columns from X's)."""
+    _, sls, subj = hemisphere_subjects(seed, nv=nv, nt=nt, n_subj=n_subj, size_lo=size_lo, size_hi=size_hi,
+                                       ar_rho=0.5)
+    return Workload("ridge_grid", subj[pair[0]], subj[pair[1]], sls, True, False)
+
+
 def duplicate_columns(X: np.ndarray, sls: Searchlights, frac: float, rng) -> np.ndarray:
     """Copy a neighbour's column into a searchlight member for about ``frac`` of searchlights.
 

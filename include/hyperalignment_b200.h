@@ -363,8 +363,10 @@ enum {
 
 /*
  * When on, every kernel launch of this library is bracketed by CUDA events on its
- * stream; ha_b200_kernel_times synchronises those events and returns (and resets)
- * the accumulated device milliseconds and launch counts per kind.
+ * stream; ha_b200_kernel_times synchronises those events and returns (and resets), per
+ * kind, the device milliseconds during which at least one launch of that kind ran (the
+ * union of the launch intervals: launches of independent size buckets run on side streams
+ * and overlap) and the launch counts.
  */
 void ha_b200_set_kernel_timing(bool on);
 int ha_b200_kernel_times(double *ms, int64_t *launches);
