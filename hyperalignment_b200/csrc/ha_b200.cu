@@ -9,6 +9,7 @@
 #include "../../include/hyperalignment_b200.h"
 #include "ha_b200_kernels.cuh"
 #include "ha_b200_grid.cuh"
+#include "ha_b200_mlp.cuh"
 
 #include <cuda_runtime.h>
 #include <omp.h>
@@ -1014,6 +1015,58 @@ int run_ridge_grid(HaB200Plan *P, const double *d_X, const double *d_Y, const Gr
 	return kHaSuccess;
 }
 
+// ---- learned (alpha, PC count) proposal: perceptron training and inference ----
+
+size_t mlp_smem(int C) {
+	return ((size_t)kMlpSamples * kMlpIn + 4 * (size_t)kMlpSamples * kMlpHidden + (size_t)kMlpSamples * C) * 4;
+}
+
+int mlp_check(int C) {
+	if (C < 1 || C > kMlpMaxClasses) {
+		fprintf(stderr, "ha_b200 mlp: %d classes outside 1..%d\n", C, kMlpMaxClasses);
+		return kHaErrorArg;
+	}
+	static bool attr = false;
+	if (!attr) {
+		const int m = (int)mlp_smem(kMlpMaxClasses);
+		HA_CUDA(cudaFuncSetAttribute(k_mlp_fwdbwd, cudaFuncAttributeMaxDynamicSharedMemorySize, m));
+		HA_CUDA(cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, m));
+		attr = true;
+	}
+	return kHaSuccess;
+}
+
+int mlp_labels_ok(const int32_t *d_y, int n, int C) {
+	std::vector<int32_t> h((size_t)n);
+	HA_CUDA(cudaMemcpy(h.data(), d_y, (size_t)n * 4, cudaMemcpyDeviceToHost));
+	for (int i = 0; i < n; i++)
+		if (h[i] < 0 || h[i] >= C) {
+			fprintf(stderr, "ha_b200 mlp: label %d of sample %d outside 0..%d\n", h[i], i, C - 1);
+			return kHaErrorArg;
+		}
+	return kHaSuccess;
+}
+
+// SplitMix64 stream for the host-side initialisation and shuffles.
+struct HostRng {
+	uint64_t x;
+	explicit HostRng(uint64_t s) : x(s) {}
+	uint64_t next() {
+		uint64_t z = (x += 0x9e3779b97f4a7c15ULL);
+		z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+		z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+		return z ^ (z >> 31);
+	}
+	double uniform() { return (double)(next() >> 11) * (1.0 / 9007199254740992.0); }
+};
+
+struct MlpBufs {
+	DevArr<float> part, loss, m, v;
+	DevArr<int32_t> idx;
+	DevArr<__nv_bfloat16> pbf;
+	void release() { part.release(); loss.release(); m.release(); v.release(); idx.release(); pbf.release(); }
+} g_mlp;
+
 // ---- CV split indices (csrc/ha_ensemble.c:12-249) ----
 
 // xoshiro256** seeded through splitmix64, with modulo range reduction (csrc/ha_ensemble.c:12-46).
@@ -1423,6 +1476,7 @@ void ha_b200_cleanup(void) {
 	}
 	g_bufs.release();
 	g_fan.release();
+	g_mlp.release();
 	g_inited = false;
 }
 
@@ -1659,6 +1713,126 @@ int ha_b200_plan_ridge_grid_device(HaB200Plan *P, const double *d_X, const doubl
 	                   n_models, gs);
 	if (rc != kHaSuccess) return rc;
 	return run_ridge_grid(P, d_X, d_Y, gs, out_kind, d_values, d_best, d_cost, (cudaStream_t)stream);
+}
+
+int64_t ha_b200_mlp_param_count(int32_t n_classes) {
+	if (n_classes < 1 || n_classes > kMlpMaxClasses) return -1;
+	return MlpLayout::make(n_classes).total;
+}
+
+int ha_b200_mlp_init(float *d_params, int32_t n_classes, uint64_t seed) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	if (!d_params) return kHaErrorArg;
+	int rc = check_cuda_ready();
+	if (rc != kHaSuccess) return rc;
+	if ((rc = mlp_check(n_classes)) != kHaSuccess) return rc;
+	const MlpLayout L = MlpLayout::make(n_classes);
+	std::vector<float> h((size_t)L.total, 0.0f);
+	HostRng g(seed);
+	auto fill = [&](int64_t ofs, int fan_in, int64_t count) {
+		const double a = 1.0 / std::sqrt((double)fan_in);
+		for (int64_t k = 0; k < count; k++) h[(size_t)(ofs + k)] = (float)((2.0 * g.uniform() - 1.0) * a);
+	};
+	fill(L.W1, kMlpIn, (int64_t)kMlpIn * kMlpHidden);
+	fill(L.b1, kMlpIn, kMlpHidden);
+	fill(L.W2, kMlpHidden, (int64_t)kMlpHidden * kMlpHidden);
+	fill(L.b2, kMlpHidden, kMlpHidden);
+	fill(L.W3, kMlpHidden, (int64_t)kMlpHidden * n_classes);
+	fill(L.b3, kMlpHidden, n_classes);
+	HA_CUDA(cudaMemcpy(d_params, h.data(), (size_t)L.total * 4, cudaMemcpyHostToDevice));
+	return kHaSuccess;
+}
+
+int ha_b200_mlp_grad(const float *d_params, int32_t n_classes, const float *d_x, const int32_t *d_y, int32_t n,
+                     float *d_grad, float *loss_out) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	if (!d_params || !d_x || !d_y || !d_grad || n < 1) return kHaErrorArg;
+	int rc = check_cuda_ready();
+	if (rc != kHaSuccess) return rc;
+	if ((rc = mlp_check(n_classes)) != kHaSuccess) return rc;
+	if ((rc = mlp_labels_ok(d_y, n, n_classes)) != kHaSuccess) return rc;
+	const MlpLayout L = MlpLayout::make(n_classes);
+	const int nb = (n + kMlpSamples - 1) / kMlpSamples;
+	if ((rc = g_mlp.part.ensure((size_t)nb * L.total)) != kHaSuccess) return rc;
+	if ((rc = g_mlp.loss.ensure((size_t)nb)) != kHaSuccess) return rc;
+	{ HA_LAUNCH(kHaB200KMlp, 0); k_mlp_fwdbwd<<<nb, kBlock, mlp_smem(n_classes)>>>(d_params, n_classes, d_x, d_y, nullptr, n, 1.0f / n, g_mlp.part.p, g_mlp.loss.p); }
+	{ HA_LAUNCH(kHaB200KMlp, 0); k_mlp_adam<<<(unsigned)((L.total + 255) / 256), 256>>>(nullptr, g_mlp.part.p, nb, L.total, nullptr, nullptr, 0.f, 0.f, 0.f, 0.f, 1.f, 1.f, d_grad); }
+	HA_CUDA(cudaGetLastError());
+	if (loss_out) {
+		std::vector<float> lp((size_t)nb);
+		HA_CUDA(cudaMemcpy(lp.data(), g_mlp.loss.p, (size_t)nb * 4, cudaMemcpyDeviceToHost));
+		double a = 0.0;
+		for (float x : lp) a += x;
+		*loss_out = (float)(a / n);
+	}
+	HA_CUDA(cudaDeviceSynchronize());
+	return kHaSuccess;
+}
+
+int ha_b200_mlp_train(float *d_params, int32_t n_classes, const float *d_x, const int32_t *d_y, int32_t n,
+                      int32_t epochs, int32_t batch, float lr, uint64_t seed, float *final_loss) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	if (!d_params || !d_x || !d_y || n < 1 || epochs < 0 || batch < 1 || !(lr > 0.0f)) return kHaErrorArg;
+	int rc = check_cuda_ready();
+	if (rc != kHaSuccess) return rc;
+	if ((rc = mlp_check(n_classes)) != kHaSuccess) return rc;
+	if ((rc = mlp_labels_ok(d_y, n, n_classes)) != kHaSuccess) return rc;
+	const MlpLayout L = MlpLayout::make(n_classes);
+	batch = std::min(batch, n);
+	const int nbmax = (batch + kMlpSamples - 1) / kMlpSamples;
+	if ((rc = g_mlp.part.ensure((size_t)nbmax * L.total)) != kHaSuccess) return rc;
+	if ((rc = g_mlp.loss.ensure((size_t)nbmax)) != kHaSuccess) return rc;
+	if ((rc = g_mlp.m.ensure((size_t)L.total)) != kHaSuccess) return rc;
+	if ((rc = g_mlp.v.ensure((size_t)L.total)) != kHaSuccess) return rc;
+	if ((rc = g_mlp.idx.ensure((size_t)n)) != kHaSuccess) return rc;
+	HA_CUDA(cudaMemset(g_mlp.m.p, 0, (size_t)L.total * 4));
+	HA_CUDA(cudaMemset(g_mlp.v.p, 0, (size_t)L.total * 4));
+	const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+	HostRng g(seed);
+	std::vector<int32_t> perm((size_t)n);
+	int64_t step = 0;
+	const unsigned pg = (unsigned)((L.total + 255) / 256);
+	for (int ep = 0; ep < epochs; ep++) {
+		for (int i = 0; i < n; i++) perm[i] = i;
+		for (int i = n - 1; i > 0; i--) std::swap(perm[i], perm[(int)(g.next() % (uint64_t)(i + 1))]);
+		HA_CUDA(cudaMemcpy(g_mlp.idx.p, perm.data(), (size_t)n * 4, cudaMemcpyHostToDevice));
+		for (int b0 = 0; b0 < n; b0 += batch) {
+			const int nbt = std::min(batch, n - b0);
+			const int nb = (nbt + kMlpSamples - 1) / kMlpSamples;
+			step++;
+			const float bc1 = 1.0f - (float)std::pow((double)b1, (double)step);
+			const float bc2 = 1.0f - (float)std::pow((double)b2, (double)step);
+			{ HA_LAUNCH(kHaB200KMlp, 0); k_mlp_fwdbwd<<<nb, kBlock, mlp_smem(n_classes)>>>(d_params, n_classes, d_x, d_y, g_mlp.idx.p + b0, nbt, 1.0f / nbt, g_mlp.part.p, g_mlp.loss.p); }
+			{ HA_LAUNCH(kHaB200KMlp, 0); k_mlp_adam<<<pg, 256>>>(d_params, g_mlp.part.p, nb, L.total, g_mlp.m.p, g_mlp.v.p, lr, b1, b2, eps, bc1, bc2, nullptr); }
+		}
+		HA_CUDA(cudaGetLastError());
+	}
+	HA_CUDA(cudaDeviceSynchronize());
+	if (final_loss) {
+		DevArr<float> gr;
+		if ((rc = gr.ensure((size_t)L.total)) != kHaSuccess) return rc;
+		rc = ha_b200_mlp_grad(d_params, n_classes, d_x, d_y, n, gr.p, final_loss);
+		gr.release();
+		return rc;
+	}
+	return kHaSuccess;
+}
+
+int ha_b200_mlp_infer(const float *d_params, int32_t n_classes, const float *d_x, int32_t n, int32_t *d_class,
+                      float *d_prob, void *stream) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	if (!d_params || !d_x || !d_class || !d_prob || n < 0) return kHaErrorArg;
+	if (n == 0) return kHaSuccess;
+	int rc = check_cuda_ready();
+	if (rc != kHaSuccess) return rc;
+	if ((rc = mlp_check(n_classes)) != kHaSuccess) return rc;
+	const cudaStream_t st = (cudaStream_t)stream;
+	const MlpLayout L = MlpLayout::make(n_classes);
+	if ((rc = g_mlp.pbf.ensure((size_t)L.total)) != kHaSuccess) return rc;
+	{ HA_LAUNCH(kHaB200KMlp, st); k_f32_to_bf16<<<(unsigned)((L.total + 255) / 256), 256, 0, st>>>(d_params, g_mlp.pbf.p, L.total); }
+	{ HA_LAUNCH(kHaB200KMlp, st); k_mlp_infer<<<(n + kMlpSamples - 1) / kMlpSamples, kBlock, mlp_smem(n_classes), st>>>(g_mlp.pbf.p, n_classes, d_x, n, d_class, d_prob); }
+	HA_CUDA(cudaGetLastError());
+	return kHaSuccess;
 }
 
 int ha_b200_kernel_times(double *ms, int64_t *launches) {

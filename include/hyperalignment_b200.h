@@ -339,6 +339,29 @@ int ha_b200_local_procrustes_noalloc(
 	const int32_t *d_sl_indices, const int32_t *sl_offsets, int32_t count,
 	float *d_T_out, void *stream);
 
+/* ---- learned (alpha, PC count) proposal ---- */
+
+/*
+ * No reference counterpart.  A perceptron 65 -> 128 GELU -> 128 GELU -> n_classes (softmax) that
+ * proposes the grid point (g = a * n_npcs + p) of a searchlight from its features (the 64 largest
+ * singular values of the searchlight's training block divided by the largest, zero-padded, and
+ * log n; ha_b200_plan_ridge_features_device).  Parameters: float32, packed W1[65][128], b1[128],
+ * W2[128][128], b2[128], W3[128][C], b3[C], in DEVICE memory.  Features: DEVICE float32 [n][65];
+ * labels DEVICE int32 [n] in 0..C-1.  C at most 64.
+ */
+int64_t ha_b200_mlp_param_count(int32_t n_classes);
+/* Uniform(+-1/sqrt(fan_in)) initialisation from a SplitMix64 stream (seed). */
+int ha_b200_mlp_init(float *d_params, int32_t n_classes, uint64_t seed);
+/* Gradient (d_grad, DEVICE) and value (loss_out, host) of the mean cross-entropy over n samples. */
+int ha_b200_mlp_grad(const float *d_params, int32_t n_classes, const float *d_x, const int32_t *d_y, int32_t n,
+                     float *d_grad, float *loss_out);
+/* Adam (0.9, 0.999, 1e-8) over shuffled mini-batches for epochs passes; final mean loss if asked. */
+int ha_b200_mlp_train(float *d_params, int32_t n_classes, const float *d_x, const int32_t *d_y, int32_t n,
+                      int32_t epochs, int32_t batch, float lr, uint64_t seed, float *final_loss);
+/* bfloat16 inference: most probable class (ties to the lower index) and its probability (DEVICE). */
+int ha_b200_mlp_infer(const float *d_params, int32_t n_classes, const float *d_x, int32_t n, int32_t *d_class,
+                      float *d_prob, void *stream);
+
 /* ---- tracing ---- */
 
 /* Kernel kinds reported by ha_b200_kernel_times. */
@@ -358,7 +381,8 @@ enum {
 	kHaB200KPattern = 12,   /* CSC pattern builder */
 	kHaB200KRidge = 13,     /* ridge solves */
 	kHaB200KGrid = 14,      /* ridge grid: per-model products and grid evaluation */
-	kHaB200NumKernelKinds = 15,
+	kHaB200KMlp = 15,       /* learned proposal: training and inference */
+	kHaB200NumKernelKinds = 16,
 };
 
 /*

@@ -356,6 +356,81 @@ def ensemble_indices(nt, n_perms, n_folds, blocksize, buffersize, seed, mask=Non
 
 
 # ---------------------------------------------------------------------------------------------
+# learned (alpha, PC count) proposal: the perceptron in float64 (no reference counterpart; the
+# checker for the GPU forward / backward / inference kernels)
+# ---------------------------------------------------------------------------------------------
+
+MLP_IN, MLP_HIDDEN = 65, 128
+
+
+def mlp_layout(C):
+    """Offsets of W1[65][128], b1, W2[128][128], b2, W3[128][C], b3 in the packed parameters."""
+    sizes = [("W1", MLP_IN * MLP_HIDDEN), ("b1", MLP_HIDDEN), ("W2", MLP_HIDDEN * MLP_HIDDEN), ("b2", MLP_HIDDEN),
+             ("W3", MLP_HIDDEN * C), ("b3", C)]
+    out, o = {}, 0
+    for k, n in sizes:
+        out[k] = (o, n)
+        o += n
+    out["total"] = o
+    return out
+
+
+def _unpack(params, C):
+    L = mlp_layout(C)
+    g = {k: np.asarray(params[L[k][0]:L[k][0] + L[k][1]], dtype=np.float64) for k in L if k != "total"}
+    g["W1"] = g["W1"].reshape(MLP_IN, MLP_HIDDEN)
+    g["W2"] = g["W2"].reshape(MLP_HIDDEN, MLP_HIDDEN)
+    g["W3"] = g["W3"].reshape(MLP_HIDDEN, C)
+    return g
+
+
+def _gelu(z):
+    from scipy.special import erf
+    return 0.5 * z * (1.0 + erf(z / math.sqrt(2.0)))
+
+
+def _gelu_grad(z):
+    from scipy.special import erf
+    return 0.5 * (1.0 + erf(z / math.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / math.sqrt(2.0 * math.pi)
+
+
+def mlp_forward(params, C, X):
+    """Logits of x -> 128 GELU -> 128 GELU -> C for the rows of X (n x 65)."""
+    g = _unpack(params, C)
+    z1 = X @ g["W1"] + g["b1"]
+    h1 = _gelu(z1)
+    z2 = h1 @ g["W2"] + g["b2"]
+    h2 = _gelu(z2)
+    return h2 @ g["W3"] + g["b3"]
+
+
+def mlp_loss_grad(params, C, X, y):
+    """Mean softmax cross-entropy over the rows of X with labels y, and its gradient (packed)."""
+    g = _unpack(params, C)
+    n = X.shape[0]
+    z1 = X @ g["W1"] + g["b1"]
+    h1 = _gelu(z1)
+    z2 = h1 @ g["W2"] + g["b2"]
+    h2 = _gelu(z2)
+    z3 = h2 @ g["W3"] + g["b3"]
+    m = z3.max(axis=1, keepdims=True)
+    lse = m[:, 0] + np.log(np.exp(z3 - m).sum(axis=1))
+    loss = float(np.mean(lse - z3[np.arange(n), y]))
+    d3 = np.exp(z3 - lse[:, None])
+    d3[np.arange(n), y] -= 1.0
+    d3 /= n
+    dz2 = (d3 @ g["W3"].T) * _gelu_grad(z2)
+    dz1 = (dz2 @ g["W2"].T) * _gelu_grad(z1)
+    grads = {"W1": X.T @ dz1, "b1": dz1.sum(0), "W2": h1.T @ dz2, "b2": dz2.sum(0), "W3": h2.T @ d3, "b3": d3.sum(0)}
+    L = mlp_layout(C)
+    out = np.zeros(L["total"])
+    for k in grads:
+        o, cnt = L[k]
+        out[o:o + cnt] = grads[k].ravel()
+    return loss, out
+
+
+# ---------------------------------------------------------------------------------------------
 # z-score (csrc/ha_linalg.c:263-291)
 # ---------------------------------------------------------------------------------------------
 

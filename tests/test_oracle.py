@@ -247,3 +247,22 @@ def test_grid_oracle_vs_live_reference():
     b = R.ensemble_ridge(X, y, al, npcs, tr, te)
     np.testing.assert_allclose(a[0], b[0], atol=1e-12, rtol=0)
     assert (a[3], a[4]) == (b[3], b[4])
+
+
+def test_mlp_oracle_gradient_vs_finite_differences():
+    # the perceptron of the learned proposal has no reference counterpart: its float64 restatement
+    # is checked against central differences before it checks the GPU kernels
+    rng = np.random.default_rng(0)
+    C = 7
+    P = O.mlp_layout(C)["total"]
+    params = rng.uniform(-0.3, 0.3, P)
+    X = rng.standard_normal((9, O.MLP_IN))
+    y = rng.integers(0, C, 9)
+    loss, g = O.mlp_loss_grad(params, C, X, y)
+    for k in rng.choice(P, 40, replace=False):
+        e = np.zeros(P)
+        e[k] = 1e-6
+        fd = (O.mlp_loss_grad(params + e, C, X, y)[0] - O.mlp_loss_grad(params - e, C, X, y)[0]) / 2e-6
+        assert abs(fd - g[k]) <= 1e-7 + 1e-5 * abs(g[k]), (k, fd, g[k])
+    assert np.isclose(loss, np.mean(np.log(np.exp(O.mlp_forward(params, C, X)).sum(1))
+                                    - O.mlp_forward(params, C, X)[np.arange(9), y]))
