@@ -80,6 +80,13 @@ SIGNATURES = {
     "ha_b200_local_procrustes_noalloc": (ctypes.c_int, [
         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, c_int32_p, ctypes.c_int32,
         ctypes.c_void_p, ctypes.c_void_p]),
+    "ha_b200_plan_ridge_features_device": (ctypes.c_int, [
+        ctypes.c_void_p, ctypes.c_void_p, c_int32_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]),
+    "ha_b200_plan_ridge_learned_device": (ctypes.c_int, [
+        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, c_int32_p, ctypes.c_int32, c_double_p, ctypes.c_int32,
+        c_int32_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_float, ctypes.POINTER(c_int32_p),
+        ctypes.POINTER(c_int32_p), c_int32_p, c_int32_p, ctypes.c_int32, ctypes.c_int, ctypes.c_void_p,
+        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "ha_b200_mlp_param_count": (ctypes.c_int64, [ctypes.c_int32]),
     "ha_b200_mlp_init": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_uint64]),
     "ha_b200_mlp_grad": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,

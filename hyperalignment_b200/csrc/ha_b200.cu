@@ -304,6 +304,9 @@ struct HaB200Plan {
 	DevArr<int64_t> gbase;
 	DevArr<int32_t> gnpcs, grows, gtpos, gurows, guntested;
 	DevArr<GridModel> gmdl;
+	DevArr<int32_t> gfit;      // fit rows of the learned form / the features
+	DevArr<float> gfeat;       // features of the learned form
+	DevArr<SlWork> gwork;      // fallback work list of the learned form
 	int last_chunk = -1;
 	int last_rowmajor = 1;
 };
@@ -898,123 +901,6 @@ size_t grid_budget_bytes() {
 	return (size_t)(gb * 1073741824.0);
 }
 
-// Enqueue the searchlight ridge grid search + reduction of the winners' betas over all chunks.
-// Per sub-batch of searchlights (bounded by the grid scratch budget) and CV model: the Gram and
-// cross-covariance over the model's training rows, the float64 Jacobi eigen decomposition of the
-// Gram, and the per-model products; then the grid evaluation and the winner's beta.
-int run_ridge_grid(HaB200Plan *P, const double *d_X, const double *d_Y, const GridSpec &gs, int out_kind,
-                   double *d_vals, int32_t *d_best, double *d_cost, cudaStream_t st) {
-	const int nt = P->nt, nv = P->nv;
-	const int rowmajor = out_kind == kHaB200OutCSR ? 1 : 0;
-	if (P->max_n > kGridMaxN) {
-		fprintf(stderr, "ha_b200 ridge grid: searchlight of %d vertices exceeds the grid limit of %d\n", P->max_n,
-		        kGridMaxN);
-		return kHaErrorArg;
-	}
-	int rc;
-	if (P->chunks.empty() && (rc = build_chunks(P)) != kHaSuccess) return rc;
-	int64_t maxT = 1;
-	for (auto &ch : P->chunks) maxT = std::max(maxT, ch.t_elems);
-	if ((rc = P->scrT64.ensure((size_t)maxT)) != kHaSuccess) return rc;
-	if ((rc = upload_vec(P->galpha, gs.alphas, st)) != kHaSuccess) return rc;
-	if ((rc = upload_vec(P->gnpcs, gs.npcs, st)) != kHaSuccess) return rc;
-	if ((rc = upload_vec(P->gmdl, gs.mdl, st)) != kHaSuccess) return rc;
-	if ((rc = upload_vec(P->grows, gs.rows, st)) != kHaSuccess) return rc;
-	if ((rc = upload_vec(P->gtpos, gs.tpos, st)) != kHaSuccess) return rc;
-	if ((rc = upload_vec(P->gwinv, gs.winv, st)) != kHaSuccess) return rc;
-	if ((rc = upload_vec(P->gurows, gs.urows, st)) != kHaSuccess) return rc;
-	if ((rc = upload_vec(P->guntested, gs.untested, st)) != kHaSuccess) return rc;
-	if ((rc = P->gbase.ensure((size_t)P->max_slots)) != kHaSuccess) return rc;
-	GridParams gp;
-	gp.models = (int)gs.mdl.size();
-	gp.mte = gs.mte;
-	gp.ntu = gs.ntu;
-	gp.n_alphas = (int)gs.alphas.size();
-	gp.n_npcs = (int)gs.npcs.size();
-	gp.nt = nt;
-	gp.n_untested = (int)gs.untested.size();
-	gp.alphas = P->galpha.p;
-	gp.npcs = P->gnpcs.p;
-	gp.mdl = P->gmdl.p;
-	gp.rows = P->grows.p;
-	gp.tpos = P->gtpos.p;
-	gp.winv = P->gwinv.p;
-	gp.urows = P->gurows.p;
-	gp.untested = P->guntested.p;
-	gp.gbase = P->gbase.p;
-	const int grid = gp.n_alphas * gp.n_npcs;
-	const size_t budget = grid_budget_bytes();
-	HA_CUDA(cudaMemsetAsync(P->counters.p, 0, 4 * sizeof(int32_t), st));
-	const int smem_cap = std::min(P->max_row, 16384);
-	const size_t red_smem = (size_t)smem_cap * 12;
-	JacobiParams jp;
-	jp.max_sweeps = 40;
-	jp.t_rowmajor = 0;
-	jp.ill_ratio = 0.0;
-	jp.weak = weak_factor();
-	jp.eig = 1;
-	jp.only_flagged = 0;
-	std::vector<int64_t> gbase;
-	for (size_t c = 0; c < P->chunks.size(); c++) {
-		Chunk &ch = P->chunks[c];
-		const int nsl = ch.s1 - ch.s0;
-		HA_CUDA(cudaMemsetAsync(P->stats.p, 0, (size_t)nsl * sizeof(SlStats), st));
-		const int nitems = (int)ch.w64.size();
-		int i0 = 0;
-		while (i0 < nitems) {
-			gbase.assign((size_t)nsl, 0);
-			int64_t total = 0;
-			int i1 = i0;
-			while (i1 < nitems) {
-				const GridLayout L = GridLayout::make(ch.w64[i1].n, gp.models, gp.mte, gp.ntu, grid);
-				if (i1 > i0 && (size_t)(total + L.total) * 8 > budget) break;
-				gbase[ch.w64[i1].slot] = total;
-				total += L.total;
-				i1++;
-			}
-			if ((rc = P->gridscr.ensure((size_t)total)) != kHaSuccess) return rc;
-			HA_CUDA(cudaMemcpyAsync(P->gbase.p, gbase.data(), (size_t)nsl * sizeof(int64_t), cudaMemcpyHostToDevice, st));
-			double *A = P->scrA.p, *V = P->scrV.p;
-			for (int mo = 0; mo < gp.models; mo++) {
-				const GridModel &md = gs.mdl[mo];
-				const int32_t *tr = P->grows.p + md.tr_ofs;
-				if ((rc = g_fan.begin(st)) != kHaSuccess) return rc;
-				for (size_t bi = 0; bi < ch.b64.size(); bi++) {
-					const Bucket &b = ch.b64[bi];
-					const int x0 = std::max(i0, b.first), x1 = std::min(i1, b.first + b.count);
-					if (x1 <= x0) continue;
-					const cudaStream_t bs = g_fan.at((int)bi);
-					const SlWork *wk = ch.d_w64 + x0;
-					// Gram into the V scratch, its pivoted Cholesky factor into the A scratch
-					{ HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16><<<x1 - x0, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_X, nt, tr, md.tr_n, V, P->gridscr.p, gp, 0); }
-					{ HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16><<<x1 - x0, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_Y, nt, tr, md.tr_n, A, P->gridscr.p, gp, 1); }
-					{ HA_LAUNCH(kHaB200KGrid, bs); k_pchol<<<x1 - x0, kBlock, 0, bs>>>(wk, V, A, P->stats.p); }
-					{
-						HA_LAUNCH(kHaB200KJacobi64, bs);
-						if ((rc = launch_jacobi<double>(b.rpl, x1 - x0, b.threads, b.smem, bs, wk, A, V, P->scrT.p, P->stats.p, P->uv.p, jp)) != kHaSuccess)
-							return rc;
-					}
-				}
-				if ((rc = g_fan.end(st)) != kHaSuccess) return rc;
-				{ HA_LAUNCH(kHaB200KGrid, st); k_grid_model<<<i1 - i0, kBlock, 0, st>>>(ch.d_w64 + i0, P->idx.p, d_X, V, P->uv.p, mo, P->gridscr.p, gp); }
-			}
-			{ HA_LAUNCH(kHaB200KGrid, st); k_grid_eval<<<i1 - i0, kBlock, 0, st>>>(ch.d_w64 + i0, P->idx.p, d_Y, P->gridscr.p, gp, P->scrT64.p, rowmajor, d_best, d_cost); }
-			HA_CUDA(cudaGetLastError());
-			i0 = i1;
-		}
-		{ HA_LAUNCH(kHaB200KScale, st); k_scale<<<(nsl + 127) / 128, 128, 0, st>>>(ch.d_w64, nsl, P->idx.p, nullptr, P->stats.p, nt, 0, P->scale.p); }
-		{ HA_LAUNCH(kHaB200KScale, st); k_count_flags<<<(nsl + 127) / 128, 128, 0, st>>>(P->stats.p, nsl, P->counters.p); }
-		{ HA_LAUNCH(kHaB200KReduce, st); k_reduce<double><<<nv, kBlock, red_smem, st>>>(P->vlptr.p, P->vlent.p, P->off.p, P->idx.p,
-		                                       P->has_weights ? P->w.p : nullptr, P->patptr.p, P->patcol.p, P->scrT64.p,
-		                                       ch.d_tofs, P->scale.p, ch.s0, ch.s1, out_kind == kHaB200OutCSC ? 1 : 0,
-		                                       smem_cap, d_vals); }
-		HA_CUDA(cudaGetLastError());
-	}
-	P->last_chunk = (int)P->chunks.size() - 1;
-	P->last_rowmajor = rowmajor;
-	return kHaSuccess;
-}
-
 // ---- learned (alpha, PC count) proposal: perceptron training and inference ----
 
 size_t mlp_smem(int C) {
@@ -1066,6 +952,268 @@ struct MlpBufs {
 	DevArr<__nv_bfloat16> pbf;
 	void release() { part.release(); loss.release(); m.release(); v.release(); idx.release(); pbf.release(); }
 } g_mlp;
+
+// Upload the grid / CV description and fill the kernel parameters (active: none).
+int grid_upload(HaB200Plan *P, const GridSpec &gs, cudaStream_t st, GridParams &gp) {
+	int rc;
+	if ((rc = upload_vec(P->galpha, gs.alphas, st)) != kHaSuccess) return rc;
+	if ((rc = upload_vec(P->gnpcs, gs.npcs, st)) != kHaSuccess) return rc;
+	if ((rc = upload_vec(P->gmdl, gs.mdl, st)) != kHaSuccess) return rc;
+	if ((rc = upload_vec(P->grows, gs.rows, st)) != kHaSuccess) return rc;
+	if ((rc = upload_vec(P->gtpos, gs.tpos, st)) != kHaSuccess) return rc;
+	if ((rc = upload_vec(P->gwinv, gs.winv, st)) != kHaSuccess) return rc;
+	if ((rc = upload_vec(P->gurows, gs.urows, st)) != kHaSuccess) return rc;
+	if ((rc = upload_vec(P->guntested, gs.untested, st)) != kHaSuccess) return rc;
+	if ((rc = P->gbase.ensure((size_t)P->max_slots)) != kHaSuccess) return rc;
+	gp.models = (int)gs.mdl.size();
+	gp.mte = gs.mte;
+	gp.ntu = gs.ntu;
+	gp.n_alphas = (int)gs.alphas.size();
+	gp.n_npcs = (int)gs.npcs.size();
+	gp.nt = P->nt;
+	gp.n_untested = (int)gs.untested.size();
+	gp.alphas = P->galpha.p;
+	gp.npcs = P->gnpcs.p;
+	gp.mdl = P->gmdl.p;
+	gp.rows = P->grows.p;
+	gp.tpos = P->gtpos.p;
+	gp.winv = P->gwinv.p;
+	gp.urows = P->gurows.p;
+	gp.untested = P->guntested.p;
+	gp.gbase = P->gbase.p;
+	return kHaSuccess;
+}
+
+int grid_prepare(HaB200Plan *P) {
+	if (P->max_n > kGridMaxN) {
+		fprintf(stderr, "ha_b200 ridge grid: searchlight of %d vertices exceeds the grid limit of %d\n", P->max_n,
+		        kGridMaxN);
+		return kHaErrorArg;
+	}
+	int rc;
+	if (P->chunks.empty() && (rc = build_chunks(P)) != kHaSuccess) return rc;
+	int64_t maxT = 1;
+	for (auto &ch : P->chunks) maxT = std::max(maxT, ch.t_elems);
+	return P->scrT64.ensure((size_t)maxT);
+}
+
+JacobiParams eig_params(bool only_flagged) {
+	JacobiParams jp;
+	jp.max_sweeps = 40;
+	jp.t_rowmajor = 0;
+	jp.ill_ratio = 0.0;
+	jp.weak = weak_factor();
+	jp.eig = 1;
+	jp.only_flagged = only_flagged ? 1 : 0;
+	return jp;
+}
+
+// Scale (1), flag counts and the deterministic reduction of one chunk's float64 betas.
+int reduce_chunk64(HaB200Plan *P, Chunk &ch, int out_kind, double *d_vals, cudaStream_t st) {
+	const int nsl = ch.s1 - ch.s0;
+	const int smem_cap = std::min(P->max_row, 16384);
+	const size_t red_smem = (size_t)smem_cap * 12;
+	{ HA_LAUNCH(kHaB200KScale, st); k_scale<<<(nsl + 127) / 128, 128, 0, st>>>(ch.d_w64, nsl, P->idx.p, nullptr, P->stats.p, P->nt, 0, P->scale.p); }
+	{ HA_LAUNCH(kHaB200KScale, st); k_count_flags<<<(nsl + 127) / 128, 128, 0, st>>>(P->stats.p, nsl, P->counters.p); }
+	{ HA_LAUNCH(kHaB200KReduce, st); k_reduce<double><<<P->nv, kBlock, red_smem, st>>>(P->vlptr.p, P->vlent.p, P->off.p, P->idx.p,
+	                                       P->has_weights ? P->w.p : nullptr, P->patptr.p, P->patcol.p, P->scrT64.p,
+	                                       ch.d_tofs, P->scale.p, ch.s0, ch.s1, out_kind == kHaB200OutCSC ? 1 : 0,
+	                                       smem_cap, d_vals); }
+	HA_CUDA(cudaGetLastError());
+	return kHaSuccess;
+}
+
+// The grid search of one chunk: per sub-batch of searchlights (bounded by the grid scratch budget)
+// and CV model, the Gram and cross-covariance over the model's training rows, the pivoted Cholesky
+// factor and its float64 Jacobi eigen decomposition, and the per-model products; then the grid
+// evaluation, the winners (d_best) and their betas in the float64 T scratch.  The chunk's work list
+// may be a subset of the plan chunk's (the learned form's fallback searchlights).
+int grid_chunk(HaB200Plan *P, Chunk &ch, const double *d_X, const double *d_Y, const GridSpec &gs,
+               const GridParams &gp, int rowmajor, int32_t *d_best, double *d_cost, cudaStream_t st) {
+	const int nt = P->nt;
+	const int nsl = ch.s1 - ch.s0;
+	const int grid = gp.n_alphas * gp.n_npcs;
+	const size_t budget = grid_budget_bytes();
+	const JacobiParams jp = eig_params(false);
+	std::vector<int64_t> gbase;
+	int rc;
+	const int nitems = (int)ch.w64.size();
+	int i0 = 0;
+	while (i0 < nitems) {
+		gbase.assign((size_t)nsl, 0);
+		int64_t total = 0;
+		int i1 = i0;
+		while (i1 < nitems) {
+			const SlWork &wi = ch.w64[i1];
+			const GridLayout L = GridLayout::make(wi.n, gp.models, gp.mte, gp.ntu, grid);
+			if (i1 > i0 && (size_t)(total + L.total) * 8 > budget) break;
+			gbase[wi.slot] = total;
+			total += L.total;
+			i1++;
+		}
+		if ((rc = P->gridscr.ensure((size_t)total)) != kHaSuccess) return rc;
+		HA_CUDA(cudaMemcpyAsync(P->gbase.p, gbase.data(), (size_t)nsl * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+		double *A = P->scrA.p, *V = P->scrV.p;
+		for (int mo = 0; mo < gp.models; mo++) {
+			const GridModel &md = gs.mdl[mo];
+			const int32_t *tr = P->grows.p + md.tr_ofs;
+			if ((rc = g_fan.begin(st)) != kHaSuccess) return rc;
+			for (size_t bi = 0; bi < ch.b64.size(); bi++) {
+				const Bucket &b = ch.b64[bi];
+				const int x0 = std::max(i0, b.first), x1 = std::min(i1, b.first + b.count);
+				if (x1 <= x0) continue;
+				const cudaStream_t bs = g_fan.at((int)bi);
+				const SlWork *wk = ch.d_w64 + x0;
+				// Gram into the V scratch, its pivoted Cholesky factor into the A scratch
+				{ HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16><<<x1 - x0, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_X, nt, tr, md.tr_n, V, P->gridscr.p, gp, 0); }
+				{ HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16><<<x1 - x0, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_Y, nt, tr, md.tr_n, A, P->gridscr.p, gp, 1); }
+				{ HA_LAUNCH(kHaB200KGrid, bs); k_pchol<<<x1 - x0, kBlock, 0, bs>>>(wk, V, A, P->stats.p); }
+				{
+					HA_LAUNCH(kHaB200KJacobi64, bs);
+					if ((rc = launch_jacobi<double>(b.rpl, x1 - x0, b.threads, b.smem, bs, wk, A, V, P->scrT.p, P->stats.p, P->uv.p, jp)) != kHaSuccess)
+						return rc;
+				}
+			}
+			if ((rc = g_fan.end(st)) != kHaSuccess) return rc;
+			{ HA_LAUNCH(kHaB200KGrid, st); k_grid_model<<<i1 - i0, kBlock, 0, st>>>(ch.d_w64 + i0, P->idx.p, d_X, V, P->uv.p, mo, P->gridscr.p, gp); }
+		}
+		{ HA_LAUNCH(kHaB200KGrid, st); k_grid_eval<<<i1 - i0, kBlock, 0, st>>>(ch.d_w64 + i0, P->idx.p, d_Y, P->gridscr.p, gp, P->scrT64.p, rowmajor, d_best, d_cost); }
+		HA_CUDA(cudaGetLastError());
+		i0 = i1;
+	}
+	return kHaSuccess;
+}
+
+// Enqueue the searchlight ridge grid search + reduction of the winners' betas over all chunks.
+int run_ridge_grid(HaB200Plan *P, const double *d_X, const double *d_Y, const GridSpec &gs, int out_kind,
+                   double *d_vals, int32_t *d_best, double *d_cost, cudaStream_t st) {
+	const int rowmajor = out_kind == kHaB200OutCSR ? 1 : 0;
+	int rc;
+	if ((rc = grid_prepare(P)) != kHaSuccess) return rc;
+	GridParams gp;
+	if ((rc = grid_upload(P, gs, st, gp)) != kHaSuccess) return rc;
+	HA_CUDA(cudaMemsetAsync(P->counters.p, 0, 4 * sizeof(int32_t), st));
+	for (size_t c = 0; c < P->chunks.size(); c++) {
+		Chunk &ch = P->chunks[c];
+		HA_CUDA(cudaMemsetAsync(P->stats.p, 0, (size_t)(ch.s1 - ch.s0) * sizeof(SlStats), st));
+		if ((rc = grid_chunk(P, ch, d_X, d_Y, gs, gp, rowmajor, d_best, d_cost, st)) != kHaSuccess) return rc;
+		if ((rc = reduce_chunk64(P, ch, out_kind, d_vals, st)) != kHaSuccess) return rc;
+	}
+	P->last_chunk = (int)P->chunks.size() - 1;
+	P->last_rowmajor = rowmajor;
+	return kHaSuccess;
+}
+
+// Eigen decomposition of every searchlight's Gram over the given rows (device list, n_rows
+// entries): the pivoted Cholesky factor and the eigenvector-mode Jacobi leave the eigenvectors in
+// the V scratch and the eigenvalues in the u/v buffer; with d_C, C = X^T Y over the same rows goes
+// to the float64 T scratch.  Then the features of the chunk's searchlights.
+int eigen_chunk(HaB200Plan *P, Chunk &ch, const double *d_X, const double *d_Y, const int32_t *d_rows, int n_rows,
+                float *d_feat, cudaStream_t st) {
+	GridParams gp = {};
+	const JacobiParams jp = eig_params(false);
+	double *A = P->scrA.p, *V = P->scrV.p;
+	int rc;
+	if ((rc = g_fan.begin(st)) != kHaSuccess) return rc;
+	for (size_t bi = 0; bi < ch.b64.size(); bi++) {
+		const Bucket &b = ch.b64[bi];
+		const cudaStream_t bs = g_fan.at((int)bi);
+		const SlWork *wk = ch.d_w64 + b.first;
+		{ HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16><<<b.count, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_X, P->nt, d_rows, n_rows, V, nullptr, gp, 0); }
+		if (d_Y) { HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16><<<b.count, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_Y, P->nt, d_rows, n_rows, P->scrT64.p, nullptr, gp, 2); }
+		{ HA_LAUNCH(kHaB200KGrid, bs); k_pchol<<<b.count, kBlock, 0, bs>>>(wk, V, A, P->stats.p); }
+		{
+			HA_LAUNCH(kHaB200KJacobi64, bs);
+			if ((rc = launch_jacobi<double>(b.rpl, b.count, b.threads, b.smem, bs, wk, A, V, P->scrT.p, P->stats.p, P->uv.p, jp)) != kHaSuccess)
+				return rc;
+		}
+	}
+	if ((rc = g_fan.end(st)) != kHaSuccess) return rc;
+	{ HA_LAUNCH(kHaB200KGrid, st); k_features<<<(int)ch.w64.size(), kBlock, 0, st>>>(ch.d_w64, P->uv.p, d_feat); }
+	HA_CUDA(cudaGetLastError());
+	return kHaSuccess;
+}
+
+int upload_rows(HaB200Plan *P, const int32_t *rows, int n_rows, cudaStream_t st) {
+	if (!rows || n_rows < 1) return kHaErrorArg;
+	for (int i = 0; i < n_rows; i++)
+		if (rows[i] < 0 || rows[i] >= P->nt) return kHaErrorArg;
+	int rc;
+	if ((rc = P->gfit.ensure((size_t)n_rows)) != kHaSuccess) return rc;
+	HA_CUDA(cudaMemcpyAsync(P->gfit.p, rows, (size_t)n_rows * 4, cudaMemcpyHostToDevice, st));
+	HA_CUDA(cudaStreamSynchronize(st));
+	return kHaSuccess;
+}
+
+// Features of every searchlight over the given rows (no fit).
+int run_ridge_features(HaB200Plan *P, const double *d_X, const int32_t *rows, int n_rows, float *d_feat,
+                       cudaStream_t st) {
+	int rc;
+	if ((rc = grid_prepare(P)) != kHaSuccess) return rc;
+	if ((rc = upload_rows(P, rows, n_rows, st)) != kHaSuccess) return rc;
+	for (size_t c = 0; c < P->chunks.size(); c++) {
+		Chunk &ch = P->chunks[c];
+		HA_CUDA(cudaMemsetAsync(P->stats.p, 0, (size_t)(ch.s1 - ch.s0) * sizeof(SlStats), st));
+		if ((rc = eigen_chunk(P, ch, d_X, nullptr, P->gfit.p, n_rows, d_feat, st)) != kHaSuccess) return rc;
+	}
+	return kHaSuccess;
+}
+
+// The learned form: per chunk the eigen decomposition over the fit rows, the features, the
+// perceptron's proposal, the single fit at the proposed grid point for searchlights whose proposal
+// probability is at least min_prob, the full CV grid search for the others, and the reduction.
+int run_ridge_learned(HaB200Plan *P, const double *d_X, const double *d_Y, const int32_t *rows, int n_rows,
+                      const GridSpec &gs, const float *d_params, float min_prob, int out_kind, double *d_vals,
+                      int32_t *d_choice, float *d_prob, cudaStream_t st) {
+	const int rowmajor = out_kind == kHaB200OutCSR ? 1 : 0;
+	const int C = (int)(gs.alphas.size() * gs.npcs.size());
+	int rc;
+	if ((rc = mlp_check(C)) != kHaSuccess) return rc;
+	if ((rc = grid_prepare(P)) != kHaSuccess) return rc;
+	if ((rc = upload_rows(P, rows, n_rows, st)) != kHaSuccess) return rc;
+	GridParams gp;
+	if ((rc = grid_upload(P, gs, st, gp)) != kHaSuccess) return rc;
+	if ((rc = P->gfeat.ensure((size_t)P->count * (kFeatSv + 1))) != kHaSuccess) return rc;
+	HA_CUDA(cudaMemsetAsync(P->counters.p, 0, 4 * sizeof(int32_t), st));
+	std::vector<float> hprob;
+	for (size_t c = 0; c < P->chunks.size(); c++) {
+		Chunk &ch = P->chunks[c];
+		const int nsl = ch.s1 - ch.s0;
+		HA_CUDA(cudaMemsetAsync(P->stats.p, 0, (size_t)nsl * sizeof(SlStats), st));
+		if ((rc = eigen_chunk(P, ch, d_X, d_Y, P->gfit.p, n_rows, P->gfeat.p, st)) != kHaSuccess) return rc;
+		if ((rc = ha_b200_mlp_infer(d_params, C, P->gfeat.p + (size_t)ch.s0 * (kFeatSv + 1), nsl, d_choice + ch.s0,
+		                            d_prob + ch.s0, st)) != kHaSuccess)
+			return rc;
+		{ HA_LAUNCH(kHaB200KGrid, st); k_proposed_fit<<<(int)ch.w64.size(), kBlock, 0, st>>>(ch.d_w64, P->scrV.p, P->uv.p, P->scrA.p, P->scrT64.p, d_choice, d_prob, min_prob, gp.alphas, gp.npcs, gp.n_npcs, n_rows, rowmajor); }
+		HA_CUDA(cudaGetLastError());
+		// searchlights below the threshold: the full grid search
+		hprob.resize((size_t)nsl);
+		HA_CUDA(cudaMemcpyAsync(hprob.data(), d_prob + ch.s0, (size_t)nsl * 4, cudaMemcpyDeviceToHost, st));
+		HA_CUDA(cudaStreamSynchronize(st));
+		// the fallback searchlights as a work list of their own (same buckets, same scratch slots)
+		Chunk fb;
+		fb.s0 = ch.s0;
+		fb.s1 = ch.s1;
+		for (const Bucket &b : ch.b64) {
+			Bucket nb = b;
+			nb.first = (int)fb.w64.size();
+			for (int i = b.first; i < b.first + b.count; i++)
+				if (hprob[(size_t)(ch.w64[i].s - ch.s0)] < min_prob) fb.w64.push_back(ch.w64[i]);
+			nb.count = (int)fb.w64.size() - nb.first;
+			if (nb.count > 0) fb.b64.push_back(nb);
+		}
+		if (!fb.w64.empty()) {
+			if ((rc = P->gwork.ensure(fb.w64.size())) != kHaSuccess) return rc;
+			HA_CUDA(cudaMemcpyAsync(P->gwork.p, fb.w64.data(), fb.w64.size() * sizeof(SlWork), cudaMemcpyHostToDevice, st));
+			fb.d_w64 = P->gwork.p;
+			if ((rc = grid_chunk(P, fb, d_X, d_Y, gs, gp, rowmajor, d_choice, nullptr, st)) != kHaSuccess) return rc;
+		}
+		if ((rc = reduce_chunk64(P, ch, out_kind, d_vals, st)) != kHaSuccess) return rc;
+	}
+	P->last_chunk = (int)P->chunks.size() - 1;
+	P->last_rowmajor = rowmajor;
+	return kHaSuccess;
+}
 
 // ---- CV split indices (csrc/ha_ensemble.c:12-249) ----
 
@@ -1617,6 +1765,7 @@ void ha_b200_plan_destroy(HaB200Plan *P) {
 	P->stats.release(); P->X32.release(); P->Y32.release(); P->var.release(); P->counters.release();
 	P->gridscr.release(); P->galpha.release(); P->gwinv.release(); P->gbase.release(); P->gnpcs.release();
 	P->grows.release(); P->gtpos.release(); P->gurows.release(); P->guntested.release(); P->gmdl.release();
+	P->gfit.release(); P->gfeat.release(); P->gwork.release();
 	delete P;
 }
 
@@ -1713,6 +1862,30 @@ int ha_b200_plan_ridge_grid_device(HaB200Plan *P, const double *d_X, const doubl
 	                   n_models, gs);
 	if (rc != kHaSuccess) return rc;
 	return run_ridge_grid(P, d_X, d_Y, gs, out_kind, d_values, d_best, d_cost, (cudaStream_t)stream);
+}
+
+int ha_b200_plan_ridge_features_device(HaB200Plan *P, const double *d_X, const int32_t *rows, int32_t n_rows,
+                                       float *d_features, void *stream) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	if (!P || !d_X || !d_features) return kHaErrorArg;
+	return run_ridge_features(P, d_X, rows, n_rows, d_features, (cudaStream_t)stream);
+}
+
+int ha_b200_plan_ridge_learned_device(HaB200Plan *P, const double *d_X, const double *d_Y, const int32_t *rows,
+                                      int32_t n_rows, const double *alphas, int32_t n_alphas, const int32_t *npcs,
+                                      int32_t n_npcs, const float *d_params, float min_prob,
+                                      const int32_t *const *train_idx_li, const int32_t *const *test_idx_li,
+                                      const int32_t *train_sizes, const int32_t *test_sizes, int32_t n_models,
+                                      int out_kind, double *d_values, int32_t *d_choice, float *d_prob, void *stream) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	if (!P || !d_X || !d_Y || !d_params || !d_values || !d_choice || !d_prob) return kHaErrorArg;
+	if (out_kind != kHaB200OutCSR && out_kind != kHaB200OutCSC) return kHaErrorArg;
+	GridSpec gs;
+	int rc = grid_spec(P->nt, alphas, n_alphas, npcs, n_npcs, train_idx_li, test_idx_li, train_sizes, test_sizes,
+	                   n_models, gs);
+	if (rc != kHaSuccess) return rc;
+	return run_ridge_learned(P, d_X, d_Y, rows, n_rows, gs, d_params, min_prob, out_kind, d_values, d_choice, d_prob,
+	                         (cudaStream_t)stream);
 }
 
 int64_t ha_b200_mlp_param_count(int32_t n_classes) {

@@ -72,18 +72,19 @@ __device__ __forceinline__ GridLayout grid_layout(const GridParams &gp, int n) {
 }
 
 // A_s = X[rows, sl]^T Z[rows, sl] (Z = X for the Gram, Y for the cross-covariance) over one row
-// list with duplicates, float64, the k_xcov tiling with gathered rows.  Output column-major with
-// ncol columns (padding columns zero) at Ascr + w.aofs, or (to_grid) into the searchlight's C.
+// list with duplicates, float64, the k_xcov tiling with gathered rows.  Output column-major:
+// mode 0 at Ascr + w.aofs with ncol columns (padding columns zero), mode 1 into the searchlight's
+// grid C block, mode 2 at Ascr + w.tofs (n x n).
 template <int KT>
 __global__ void __launch_bounds__(256) k_xcov_rows(const SlWork *__restrict__ work, const int32_t *__restrict__ sl_idx,
                                                    const double *__restrict__ X, const double *__restrict__ Z, int nt,
                                                    const int32_t *__restrict__ rows, int nrows, double *__restrict__ Ascr,
-                                                   double *__restrict__ Gscr, GridParams gp, int to_grid) {
+                                                   double *__restrict__ Gscr, GridParams gp, int mode) {
 	const SlWork w = work[blockIdx.x];
 	const int n = w.n;
 	const int ncol = w.nblk * w.bsz;
 	const int32_t *sl = sl_idx + w.sofs;
-	double *A = to_grid ? Gscr + gp.gbase[w.slot] + grid_layout(gp, n).C : Ascr + w.aofs;
+	double *A = mode == 1 ? Gscr + gp.gbase[w.slot] + grid_layout(gp, n).C : Ascr + (mode == 2 ? w.tofs : w.aofs);
 	__shared__ double xs[KT][64 + 1];
 	__shared__ double zs[KT][64 + 1];
 	__shared__ int32_t vi[64], vj[64];
@@ -142,7 +143,7 @@ __global__ void __launch_bounds__(256) k_xcov_rows(const SlWork *__restrict__ wo
 			}
 		}
 	}
-	if (!to_grid)
+	if (mode == 0)
 		for (int64_t e = (int64_t)n * n + threadIdx.x; e < (int64_t)n * ncol; e += 256) A[e] = 0.0;
 }
 
@@ -459,6 +460,83 @@ __global__ void __launch_bounds__(256) k_grid_eval(const SlWork *__restrict__ wo
 		const int j = (int)(e / n), i = (int)(e - (int64_t)j * n);
 		Bo[i * ti + j * tj] = acc[e] / gp.models;
 	}
+}
+
+// ---------------------------------------------------------------------------------------------
+// learned proposal: features and the single fit at the proposed grid point
+// ---------------------------------------------------------------------------------------------
+
+constexpr int kFeatSv = 64;  // singular values per feature vector (then log n)
+
+// Features of every searchlight from its eigen decomposition (lambda in the u/v buffer): the 64
+// largest singular values sqrt(lambda) divided by the largest (zero-padded), then log n.
+__global__ void __launch_bounds__(256) k_features(const SlWork *__restrict__ work, const double *__restrict__ uvbuf,
+                                                  float *__restrict__ feat) {
+	__shared__ int order[kGridMaxN];
+	const SlWork w = work[blockIdx.x];
+	const int n = w.n;
+	const double *lam = uvbuf + w.uvofs;
+	rank_desc(lam, n, order);
+	__syncthreads();
+	const double s1 = sqrt(fmax(lam[order[0]], 0.0));
+	float *f = feat + (int64_t)w.s * (kFeatSv + 1);
+	for (int k = threadIdx.x; k < kFeatSv; k += blockDim.x)
+		f[k] = (k < n && s1 > 0.0) ? (float)(sqrt(fmax(lam[order[k]], 0.0)) / s1) : 0.0f;
+	if (threadIdx.x == 0) f[kFeatSv] = logf((float)n);
+}
+
+// beta = sum_k v_k q_k^T mult_k / (alpha + lambda_k) at grid point g = cls[w.s] for the
+// searchlights whose proposal probability is at least min_prob: the reference's ha_ridge_grid
+// (csrc/ha_ridge.c:97-227) restricted to one (alpha, PC count), with mult_k the number of PC
+// chunks up to p that contain component k's rank (clipped at K = min(rows, n)).  V (eigenvectors,
+// column-major ld n) and lambda come from the eigenvector-mode Jacobi, C = X_fit^T Y_fit is at
+// Bout + w.tofs and is replaced by beta (T layout); Q = V^T C goes to the A scratch.
+__global__ void __launch_bounds__(256) k_proposed_fit(const SlWork *__restrict__ work, const double *__restrict__ Vscr,
+                                                      const double *__restrict__ uvbuf, double *__restrict__ Ascr,
+                                                      double *__restrict__ Bout, const int32_t *__restrict__ cls,
+                                                      const float *__restrict__ prob, float min_prob,
+                                                      const double *__restrict__ alphas, const int32_t *__restrict__ npcs,
+                                                      int n_npcs, int rows, int t_rowmajor) {
+	__shared__ double ps[16][65], qs[16][65];
+	__shared__ int order[kGridMaxN];
+	__shared__ double cval[kGridMaxN];
+	const SlWork w = work[blockIdx.x];
+	if (prob[w.s] < min_prob) return;
+	const int n = w.n;
+	const double *V = Vscr + w.aofs;
+	const double *lam = uvbuf + w.uvofs;
+	double *Q = Ascr + w.aofs;
+	double *B = Bout + w.tofs;
+	const int g = cls[w.s];
+	const int a = g / n_npcs, p = g - a * n_npcs;
+	const double al = alphas[a];
+	const int K = min(rows, n);
+	rank_desc(lam, n, order);
+	__syncthreads();
+	for (int r = threadIdx.x; r < n; r += blockDim.x) {
+		int mult = 0;
+		for (int pp = 0; pp <= p; pp++) {
+			int r0, r1;
+			pc_chunk(npcs, pp, K, r0, r1);
+			mult += (r >= r0 && r < r1);
+		}
+		const int k = order[r];
+		cval[k] = mult ? mult / (al + lam[k]) : 0.0;
+	}
+	GemmArgs<double, double> gm;
+	gm.d = nullptr; gm.alpha = 1.0; gm.E = nullptr; gm.ei = 0; gm.ej = 0; gm.beta = 0.0;
+	// Q(k, j) = sum_i V(i, k) C(i, j)
+	gm.M = n; gm.N = n; gm.K = n;
+	gm.P = V; gm.pk = 1; gm.pi = n;
+	gm.Q = B; gm.qk = 1; gm.qj = n;
+	gm.C = Q; gm.ci = 1; gm.cj = n;
+	block_gemm(gm, ps, qs);
+	// beta(i, j) = sum_k V(i, k) c_k Q(k, j), in the T layout
+	gm.P = V; gm.pk = n; gm.pi = 1;
+	gm.Q = Q; gm.qk = 1; gm.qj = n;
+	gm.d = cval;
+	gm.C = B; gm.ci = t_rowmajor ? n : 1; gm.cj = t_rowmajor ? 1 : n;
+	block_gemm(gm, ps, qs);
 }
 
 }  // namespace hab200

@@ -68,6 +68,25 @@ class Plan:
             ctypes.c_void_p(d_best), ctypes.c_void_p(d_cost or None), ctypes.c_void_p(stream)),
             "ha_b200_plan_ridge_grid_device")
 
+    def ridge_features_device(self, d_X: int, rows, d_features: int, stream: int = 0):
+        r = np.ascontiguousarray(rows, dtype=np.int32)
+        L.check(self.lib.ha_b200_plan_ridge_features_device(self.handle, ctypes.c_void_p(d_X), L.iptr(r), r.size,
+                                                            ctypes.c_void_p(d_features), ctypes.c_void_p(stream)),
+                "ha_b200_plan_ridge_features_device")
+
+    def ridge_learned_device(self, d_X: int, d_Y: int, rows, alphas, npcs, d_params: int, min_prob: float,
+                             train_li, test_li, d_values: int, d_choice: int, d_prob: int, out_kind=L.OUT_CSC,
+                             stream: int = 0):
+        r = np.ascontiguousarray(rows, dtype=np.int32)
+        al = np.ascontiguousarray(alphas, dtype=np.float64)
+        pc = np.ascontiguousarray(npcs, dtype=np.int32)
+        tr, te = L.IndexLists(train_li), L.IndexLists(test_li)
+        L.check(self.lib.ha_b200_plan_ridge_learned_device(
+            self.handle, ctypes.c_void_p(d_X), ctypes.c_void_p(d_Y), L.iptr(r), r.size, L.dptr(al), al.size,
+            L.iptr(pc), pc.size, ctypes.c_void_p(d_params), float(min_prob), tr.ptrs, te.ptrs, L.iptr(tr.sizes),
+            L.iptr(te.sizes), len(tr), out_kind, ctypes.c_void_p(d_values), ctypes.c_void_p(d_choice),
+            ctypes.c_void_p(d_prob), ctypes.c_void_p(stream)), "ha_b200_plan_ridge_learned_device")
+
     def stats(self):
         a, b = ctypes.c_int32(), ctypes.c_int32()
         L.check(self.lib.ha_b200_plan_stats(self.handle, ctypes.byref(a), ctypes.byref(b)), "ha_b200_plan_stats")

@@ -190,11 +190,13 @@ def _uniform_sizes(rng, nv, lo, hi):
 
 def hemisphere_subjects(seed: int = 0, nv: int = 10242, nt: int = 400, n_subj: int = 10,
                         size_lo: int = 100, size_hi: int = 300, noise: float = 0.2,
-                        ar_rho: float = 0.0):
+                        ar_rho: float = 0.0, noise_span: float = 1.0):
     """Shared N(0,1) latent time series times per-subject block-local rotations plus noise.
 
     Returns (points, searchlights, list of subject matrices nt x nv).  With
-    ``ar_rho`` > 0 the noise is AR(1): e_t = rho e_{t-1} + sqrt(1 - rho^2) eps_t.
+    ``ar_rho`` > 0 the noise is AR(1): e_t = rho e_{t-1} + sqrt(1 - rho^2) eps_t.  With
+    ``noise_span`` > 1 the noise amplitude varies smoothly over the sphere, from ``noise`` at
+    the south pole to ``noise * noise_span`` at the north pole (log-linear in z).
     """
     rng = np.random.default_rng(seed)
     pts = fibonacci_sphere(nv)
@@ -211,7 +213,8 @@ def hemisphere_subjects(seed: int = 0, nv: int = 10242, nt: int = 400, n_subj: i
             for t in range(1, nt):
                 e[t] = ar_rho * e[t - 1] + c * eps[t]
             eps = e
-        subjects.append(np.ascontiguousarray(R.apply(L) + noise * eps))
+        amp = noise * noise_span ** ((pts[:, 2] + 1.0) / 2.0) if noise_span != 1.0 else noise
+        subjects.append(np.ascontiguousarray(R.apply(L) + amp * eps))
     return pts, sls, subjects
 
 
@@ -226,12 +229,12 @@ GRID_NPCS = np.array([10, 20, 50, 1 << 30], dtype=np.int32)  # PC counts; the la
 
 
 def ridge_grid_pair(seed: int = 0, nv: int = 40962, nt: int = 500, size_lo: int = 50, size_hi: int = 500,
-                    n_subj: int = 2, pair=(0, 1)) -> Workload:
+                    n_subj: int = 2, pair=(0, 1), noise: float = 0.2, noise_span: float = 1.0) -> Workload:
     """Searchlight ridge grid search inputs: subjects of the hemisphere generator with AR(1)
     noise (rho 0.5), searchlight sizes uniform in [size_lo, size_hi]; X = subject pair[0],
     Y = subject pair[1] (the ridge predicts Y's searchlight columns from X's)."""
     _, sls, subj = hemisphere_subjects(seed, nv=nv, nt=nt, n_subj=n_subj, size_lo=size_lo, size_hi=size_hi,
-                                       ar_rho=0.5)
+                                       ar_rho=0.5, noise=noise, noise_span=noise_span)
     return Workload("ridge_grid", subj[pair[0]], subj[pair[1]], sls, True, False)
 
 

@@ -362,6 +362,29 @@ int ha_b200_mlp_train(float *d_params, int32_t n_classes, const float *d_x, cons
 int ha_b200_mlp_infer(const float *d_params, int32_t n_classes, const float *d_x, int32_t n, int32_t *d_class,
                       float *d_prob, void *stream);
 
+/*
+ * Features of every searchlight of the plan for the perceptron: the 64 largest singular values of
+ * X[rows, sl] divided by the largest (zero-padded) and log n, d_features DEVICE float32
+ * [count][65].  rows: host int32 list (duplicates allowed) of time points in [0, nt).
+ */
+int ha_b200_plan_ridge_features_device(HaB200Plan *plan, const double *d_X, const int32_t *rows, int32_t n_rows,
+                                       float *d_features, void *stream);
+/*
+ * The learned form of the ridge grid search.  Per searchlight: the features over the fit rows, the
+ * perceptron's proposed grid point g and its probability (d_choice, d_prob: DEVICE, count
+ * entries); where the probability is at least min_prob, ha_ridge_grid's beta at g fitted on the
+ * rows (csrc/ha_ridge.c:97-227 restricted to one grid point, all targets of the searchlight);
+ * below it, the full CV grid search of ha_searchlight_ridge_grid_b200 (its winner replaces
+ * d_choice).  Betas are scattered into d_values like the other plan runs.
+ */
+int ha_b200_plan_ridge_learned_device(
+	HaB200Plan *plan, const double *d_X, const double *d_Y, const int32_t *rows, int32_t n_rows,
+	const double *alphas, int32_t n_alphas, const int32_t *npcs, int32_t n_npcs,
+	const float *d_params, float min_prob,
+	const int32_t *const *train_idx_li, const int32_t *const *test_idx_li,
+	const int32_t *train_sizes, const int32_t *test_sizes, int32_t n_models,
+	int out_kind, double *d_values, int32_t *d_choice, float *d_prob, void *stream);
+
 /* ---- tracing ---- */
 
 /* Kernel kinds reported by ha_b200_kernel_times. */

@@ -270,6 +270,34 @@ def searchlight_ridge_grid_csc(X, Y, idx, off, indptr, indices, data, alphas, np
     return data, best, costs
 
 
+def ridge_features(X, idx, off, rows, n_sv=64):
+    """Perceptron features per searchlight: the n_sv largest singular values of X[rows, sl]
+    divided by the largest (zero-padded), then log n."""
+    out = np.zeros((len(off) - 1, n_sv + 1))
+    Xr = X[np.asarray(rows)]
+    for s in range(len(off) - 1):
+        sl = idx[off[s]:off[s + 1]]
+        sv = np.linalg.svd(Xr[:, sl], compute_uv=False)
+        k = min(n_sv, sv.size)
+        if sv[0] > 0:
+            out[s, :k] = sv[:k] / sv[0]
+        out[s, n_sv] = math.log(sl.size)
+    return out
+
+
+def searchlight_ridge_at(X, Y, idx, off, indptr, indices, data, alphas, npcs, rows, choice, weights=None):
+    """ha_ridge_grid's beta at grid point choice[s] (g = a * len(npcs) + p), fitted on the rows,
+    of every searchlight's targets, scattered like the ridge solve."""
+    P = len(npcs)
+    for s in range(len(off) - 1):
+        sl = idx[off[s]:off[s + 1]]
+        a, p = divmod(int(choice[s]), P)
+        B = ridge_grid(X[:, sl], Y[:, sl], alphas, npcs, rows)[:, a, p, :]
+        w = None if weights is None else weights[off[s]:off[s + 1]]
+        sparse_scatter_add(indptr, indices, data, sl, sl, B, w)
+    return data
+
+
 class Xoshiro256:
     """xoshiro256** seeded by splitmix64, modulo range reduction (csrc/ha_ensemble.c:12-46)."""
     M = (1 << 64) - 1
