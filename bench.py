@@ -58,6 +58,10 @@ def parse_args():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--workload", choices=["template", "grid", "learned"], default="template",
+                   help="template: the headline Procrustes step; grid: the searchlight ridge grid search "
+                        "(40962 vertices, every --grid-step-th searchlight); learned: the learned proposal")
+    p.add_argument("--grid-step", type=int, default=16)
     return p.parse_args()
 
 
@@ -448,10 +452,197 @@ def run_b200(args):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------------------------
+# ridge grid search (40962 vertices, sizes 50-500, nt 500, 10 alphas x 4 PC counts, 5 CV folds)
+# and the learned proposal on top of it
+# ---------------------------------------------------------------------------------------------
+
+FP64_NOMINAL_TFLOPS = 37.0  # B200 float64 (context only; the kernels run on the FP64 SIMT pipe)
+
+
+def _oracle_grid_worker(args):
+    import os as _os
+    _os.environ["OPENBLAS_NUM_THREADS"] = "1"
+    X, Y, sl, alphas, npcs, tr, te = args
+    from oracle import ha_oracle as O
+    O.ensemble_ridge(X[:, sl], Y[:, sl], alphas, npcs, tr, te)
+    return sl.size
+
+
+def grid_cpu_rate(w, sls, tr, te, seconds):
+    """The oracle's composition (numpy, one BLAS thread per process, all host cores) on the first
+    searchlights of the subset, sized to about ``seconds``."""
+    import multiprocessing as mp
+    from hyperalignment_b200 import workloads as W
+    cores = os.cpu_count() or 1
+    m = max(cores, int(seconds * cores / 1.3))
+    m = min(m, sls.count)
+    jobs = []
+    for q in range(m):
+        sl = sls.indices[sls.offsets[q]:sls.offsets[q + 1]]
+        jobs.append((np.ascontiguousarray(w.X[:, sl]), np.ascontiguousarray(w.Y[:, sl]), np.arange(sl.size),
+                     W.GRID_ALPHAS, W.GRID_NPCS, tr, te))
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        t0 = time.perf_counter()
+        pool.map(_oracle_grid_worker, jobs, chunksize=1)
+        dt = time.perf_counter() - t0
+    return m / dt, m, dt, cores
+
+
+def run_grid(args):
+    import torch
+    from hyperalignment_b200 import _lib as L
+    from hyperalignment_b200 import hyperalignment_c as H
+    from hyperalignment_b200 import workloads as W
+    from hyperalignment_b200.plan import Plan
+
+    ws, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    lib = L.lib()
+    L.check(lib.ha_b200_init(), "ha_b200_init")
+    nv = 40962 if args.nv == 10242 else args.nv
+    w = W.ridge_grid_pair(rank, nv=nv, nt=500)
+    sls = w.sls.subset(np.arange(0, w.sls.count, args.grid_step))
+    tr, te = H.ensemble_indices(w.nt, 1, 5, 10, 10, rank)
+    plan = Plan(w.nt, w.nv, sls.indices, sls.offsets, sls.dists, sls.radius)
+    dev = torch.device("cuda", local)
+    dX = torch.from_numpy(np.asfortranarray(w.X).ravel(order="F")).to(dev)
+    dY = torch.from_numpy(np.asfortranarray(w.Y).ravel(order="F")).to(dev)
+    vals = torch.zeros(plan.nnz, dtype=torch.float64, device=dev)
+    best = torch.zeros(sls.count, dtype=torch.int32, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        plan.ridge_grid_device(dX.data_ptr(), dY.data_ptr(), vals.data_ptr(), best.data_ptr(), W.GRID_ALPHAS,
+                               W.GRID_NPCS, tr, te, stream=stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    K = args.steps
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.5)
+    lib.ha_b200_kernel_times(None, None)
+    lib.ha_b200_set_kernel_timing(True)
+    n0 = lib.ha_b200_launch_count()
+    evs = []
+    t0 = time.perf_counter()
+    for _ in range(K):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        step()
+        b.record(stream)
+        evs.append((a, b))
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    launches = lib.ha_b200_launch_count() - n0
+    lib.ha_b200_set_kernel_timing(False)
+    ms = np.zeros(len(L.KERNEL_KINDS))
+    cnt = np.zeros(len(L.KERNEL_KINDS), dtype=np.int64)
+    lib.ha_b200_kernel_times(ms.ctypes.data_as(L.c_double_p), cnt.ctypes.data_as(L.c_int64_p))
+    clocks = sampler.stop()
+    total_ms = float(sum(a.elapsed_time(b) for a, b in evs))
+    value = sls.count * K / (total_ms / 1e3)
+    st = plan.stats()
+
+    # roofline of the dominant kernel: the float64 Jacobi eigen solves (9 n^3 flops per
+    # symmetric eigendecomposition with vectors, Golub-Van Loan count; 5 CV models per searchlight)
+    peaks, peak_src = load_peaks()
+    dom = int(np.argmax(ms))
+    n3 = float((sls.sizes.astype(np.float64) ** 3).sum())
+    roof = None
+    if L.KERNEL_KINDS[dom] == "jacobi64" and ms[dom] > 0:
+        achieved = 9.0 * n3 * len(tr) * K / (ms[dom] / 1e3) / 1e12
+        peak = float(peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops")))
+        roof = {"bound": "tensor", "kernel": "jacobi64 (eigenvector mode)", "achieved": achieved, "peak": peak,
+                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                "peak_source": f"{peak_src} bf16 sustained",
+                "fp64_simt": {"peak_nominal": FP64_NOMINAL_TFLOPS, "frac": achieved / FP64_NOMINAL_TFLOPS},
+                "algorithmic": "9 n^3 flops per symmetric eigendecomposition, 5 per searchlight"}
+
+    # end to end through the host C ABI entry (host float64 in, host CSC values out)
+    e2e = None
+    if not args.no_e2e:
+        indptr, indices = plan.pattern()
+        ip32, ind32 = indptr.astype(np.int32), indices.astype(np.int32)
+        sl_lists = [sls.indices[sls.offsets[q]:sls.offsets[q + 1]] for q in range(sls.count)]
+        wts = H.searchlight_weights(sl_lists, [sls.dists[sls.offsets[q]:sls.offsets[q + 1]] for q in range(sls.count)],
+                                    sls.radius, w.nv)
+        data = np.zeros(indices.size)
+        H.searchlight_ridge_grid(w.X, w.Y, sl_lists, ip32, ind32, data, W.GRID_ALPHAS, W.GRID_NPCS, tr, te,
+                                 weights=[wts])
+        ts = []
+        for _ in range(K):
+            data[:] = 0.0
+            t1 = time.perf_counter()
+            H.searchlight_ridge_grid(w.X, w.Y, sl_lists, ip32, ind32, data, W.GRID_ALPHAS, W.GRID_NPCS, tr, te,
+                                     weights=[wts])
+            ts.append(time.perf_counter() - t1)
+        e2e = {"value": sls.count * K / sum(ts), "unit": UNIT, "h2d_bytes_per_step": int(2 * w.nt * w.nv * 8),
+               "d2h_bytes_per_step": int(plan.nnz * 8 + sls.count * 4),
+               "path": "ha_searchlight_ridge_grid_b200 host float64 in, host CSC values out (+=)"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        r, m, dt, cores = grid_cpu_rate(w, sls, tr, te, args.cpu_seconds)
+        cpu = {"value": r, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"{m} searchlights of the subset ({dt:.1f} s), oracle composition of ha_ensemble_ridge "
+                         f"(numpy, one BLAS thread per process, {cores} processes)"}
+    if rank == 0:
+        sizes = sls.sizes
+        out = {"metric": "searchlight ridge grid searches/sec", "value": value, "unit": UNIT, "n_gpus": 1,
+               "steps": K, "warmup": args.warmup, "ms_per_step": total_ms / K, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+               "config": {"workload": "ridge_grid", "nv": w.nv, "nt": w.nt, "searchlights": sls.count,
+                          "searchlight_subset": f"every {args.grid_step}th of {w.sls.count}",
+                          "sl_size_min": int(sizes.min()), "sl_size_max": int(sizes.max()),
+                          "sl_size_mean": round(float(sizes.mean()), 2), "alphas": "10 log-spaced in [1e-3, 1e3]",
+                          "npcs": [10, 20, 50, "all"], "cv": "ha_ensemble_indices(500, 1, 5, 10, 10, seed)",
+                          "noise": "AR(1) rho 0.5", "l2": "flushed between steps (256 MiB write)"},
+               "solver_stats": st, "winners_distinct": int(np.unique(best.cpu().numpy()).size),
+               "roofline": roof,
+               "kernels": {L.KERNEL_KINDS[i]: {"ms_per_step": float(ms[i] / K), "launches_per_step": float(cnt[i] / K)}
+                           for i in range(len(ms)) if cnt[i] > 0},
+               "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
+               "wall_s_timed": wall}
+        print(json.dumps(out))
+
+
+def run_learned(args):
+    import torch
+    from hyperalignment_b200 import _lib as L
+    from hyperalignment_b200 import learned as LR
+
+    ws, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    L.check(L.lib().ha_b200_init(), "ha_b200_init")
+    nv = args.nv
+    res = LR.study(nv=nv, step=4, size_lo=50, size_hi=500, epochs=60, log=lambda *a: None)
+    if rank == 0:
+        out = {"metric": "searchlight ridge grid searches/sec, learned proposal with grid fallback",
+               "value": res["learned"]["searchlights_per_s"], "unit": UNIT, "n_gpus": 1, "steps": 1, "warmup": 1,
+               "ms_per_step": res["learned"]["ms"], "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f64 (proposal bf16)", "data": "synthetic",
+               "config": {"workload": "ridge_grid_learned", "nv": nv, "nt": 500, "fit_rows": 400, "eval_rows": 100,
+                          "searchlight_subset": "every 4th", "sizes": "50-500",
+                          "noise": "AR(1) rho 0.5, amplitude 0.2 to 6 over the sphere",
+                          "train_seeds": [1, 2, 3, 4], "heldout_seed": 5, "min_prob": 0.6},
+               "study": res}
+        print(json.dumps(out))
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "grid":
+        run_grid(args)
+    elif args.workload == "learned":
+        run_learned(args)
     else:
         run_b200(args)
 

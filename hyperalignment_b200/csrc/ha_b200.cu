@@ -1067,7 +1067,7 @@ int grid_chunk(HaB200Plan *P, Chunk &ch, const double *d_X, const double *d_Y, c
 				// Gram into the V scratch, its pivoted Cholesky factor into the A scratch
 				{ HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16><<<x1 - x0, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_X, nt, tr, md.tr_n, V, P->gridscr.p, gp, 0); }
 				{ HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16><<<x1 - x0, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_Y, nt, tr, md.tr_n, A, P->gridscr.p, gp, 1); }
-				{ HA_LAUNCH(kHaB200KGrid, bs); k_pchol<<<x1 - x0, kBlock, 0, bs>>>(wk, V, A, P->stats.p); }
+				{ HA_LAUNCH(kHaB200KRidge, bs); k_pchol<<<x1 - x0, kBlock, 0, bs>>>(wk, V, A, P->stats.p); }
 				{
 					HA_LAUNCH(kHaB200KJacobi64, bs);
 					if ((rc = launch_jacobi<double>(b.rpl, x1 - x0, b.threads, b.smem, bs, wk, A, V, P->scrT.p, P->stats.p, P->uv.p, jp)) != kHaSuccess)
@@ -1121,7 +1121,7 @@ int eigen_chunk(HaB200Plan *P, Chunk &ch, const double *d_X, const double *d_Y, 
 		const SlWork *wk = ch.d_w64 + b.first;
 		{ HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16><<<b.count, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_X, P->nt, d_rows, n_rows, V, nullptr, gp, 0); }
 		if (d_Y) { HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16><<<b.count, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_Y, P->nt, d_rows, n_rows, P->scrT64.p, nullptr, gp, 2); }
-		{ HA_LAUNCH(kHaB200KGrid, bs); k_pchol<<<b.count, kBlock, 0, bs>>>(wk, V, A, P->stats.p); }
+		{ HA_LAUNCH(kHaB200KRidge, bs); k_pchol<<<b.count, kBlock, 0, bs>>>(wk, V, A, P->stats.p); }
 		{
 			HA_LAUNCH(kHaB200KJacobi64, bs);
 			if ((rc = launch_jacobi<double>(b.rpl, b.count, b.threads, b.smem, bs, wk, A, V, P->scrT.p, P->stats.p, P->uv.p, jp)) != kHaSuccess)

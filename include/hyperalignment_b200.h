@@ -402,7 +402,7 @@ enum {
 	kHaB200KScale = 10,     /* per-searchlight scale / bookkeeping */
 	kHaB200KReduce = 11,    /* deterministic segmented reduction */
 	kHaB200KPattern = 12,   /* CSC pattern builder */
-	kHaB200KRidge = 13,     /* ridge solves */
+	kHaB200KRidge = 13,     /* ridge solves, pivoted Cholesky factors of the grid */
 	kHaB200KGrid = 14,      /* ridge grid: per-model products and grid evaluation */
 	kHaB200KMlp = 15,       /* learned proposal: training and inference */
 	kHaB200NumKernelKinds = 16,

@@ -238,7 +238,8 @@ def ensemble_ridge(X, y, alphas, npcs, train_li, test_li):
         wsum = b.copy() if wsum is None else wsum + b
         te = np.asarray(te, dtype=np.int64)
         if te.size:
-            psum[te] += np.einsum("tv,va...->ta...", X[te], b)
+            # pred[t, a, p(, target)] = sum_v X[t, v] b[v, a, p(, target)]  (csrc/ha_ridge.c:297-303)
+            psum[te] += (X[te] @ b.reshape(b.shape[0], -1)).reshape((te.size,) + b.shape[1:])
             count[te] += 1
     weights_avg = wsum / len(train_li)
     pred = np.zeros_like(psum)
