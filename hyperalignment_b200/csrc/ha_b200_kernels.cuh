@@ -262,27 +262,94 @@ struct JacobiTol {
 	Real zero2;  // squared norm at or below which a column counts as zero
 };
 
+// Rows a lane owns in a column of LD = 32*RPL rows: chunks of VW consecutive rows, chunk c of lane l
+// at row c*32*VW + l*VW, with VW as many rows as 16 bytes hold when RPL allows.  Every row has one
+// owner and the rows keep their natural order in shared memory, so a lane moves its chunk with one
+// 16-byte load or store and consecutive lanes touch consecutive 16-byte words (no bank conflicts).
+template <typename Real, int VW> struct VecOf { using T = Real; };
+template <> struct VecOf<float, 4> { using T = float4; };
+template <> struct VecOf<float, 2> { using T = float2; };
+template <> struct VecOf<double, 2> { using T = double2; };
+
+template <typename Real, int RPL>
+struct LaneRows {
+	static constexpr int W16 = 16 / (int)sizeof(Real);
+	static constexpr int VW = (RPL % W16 == 0) ? W16 : ((RPL % 2 == 0) ? 2 : 1);
+	static constexpr int NC = RPL / VW;
+	using V = typename VecOf<Real, VW>::T;
+	static __device__ __forceinline__ int ofs(int lane, int c) { return c * 32 * VW + lane * VW; }
+	static __device__ __forceinline__ void load(const Real *col, int lane, Real (&x)[RPL]) {
+#pragma unroll
+		for (int c = 0; c < NC; c++) {
+			const V v = *reinterpret_cast<const V *>(col + ofs(lane, c));
+			const Real *e = reinterpret_cast<const Real *>(&v);
+#pragma unroll
+			for (int q = 0; q < VW; q++) x[c * VW + q] = e[q];
+		}
+	}
+	static __device__ __forceinline__ void store(Real *col, int lane, const Real (&x)[RPL]) {
+#pragma unroll
+		for (int c = 0; c < NC; c++) {
+			V v;
+			Real *e = reinterpret_cast<Real *>(&v);
+#pragma unroll
+			for (int q = 0; q < VW; q++) e[q] = x[c * VW + q];
+			*reinterpret_cast<V *>(col + ofs(lane, c)) = v;
+		}
+	}
+};
+
+// sqrt(x) for x >= 1 in the rotation tangent: hardware reciprocal square root in float32 (the
+// tangent only steers the rotation; c and s = c t stay orthogonal through rot_cos), IEEE in float64.
+__device__ __forceinline__ float rot_sqrt(float x) { return x * rsqrtf(x); }
+__device__ __forceinline__ double rot_sqrt(double x) { return sqrt(x); }
+
+// Sum of each of the JPW per-lane partial dot products over the warp, reduce-scatter style: pair k's
+// total ends up in the lanes of group k (32 / JPW consecutive lanes), with log2(JPW) fewer shuffles
+// per pair than one butterfly per pair.
+template <typename Real, int JPW>
+__device__ __forceinline__ Real pair_sums(const Real (&g)[JPW], int lane) {
+	if constexpr (JPW == 4) {
+		const bool hi = lane & 16, h8 = lane & 8;
+		const Real r0 = __shfl_xor_sync(0xffffffffu, hi ? g[0] : g[2], 16);
+		const Real r1 = __shfl_xor_sync(0xffffffffu, hi ? g[1] : g[3], 16);
+		const Real a0 = (hi ? g[2] : g[0]) + r0, a1 = (hi ? g[3] : g[1]) + r1;
+		Real v = (h8 ? a1 : a0) + __shfl_xor_sync(0xffffffffu, h8 ? a0 : a1, 8);
+#pragma unroll
+		for (int o = 4; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+		return v;
+	} else if constexpr (JPW == 2) {
+		const bool hi = lane & 16;
+		Real v = (hi ? g[1] : g[0]) + __shfl_xor_sync(0xffffffffu, hi ? g[0] : g[1], 16);
+#pragma unroll
+		for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+		return v;
+	} else {
+		return warp_sum(g[0]);
+	}
+}
+
 // Rotate JPW pairs (p[k], q[k]) of columns stored at B + c*LD (and V + c*LD) in shared memory,
 // LD = 32*RPL rows with rows >= n zero, so every lane handles exactly RPL rows and no row test
 // is needed.  Unused pair slots point at two zero columns and are skipped like any zero column.
 // nrm[] holds the cached squared norms.  The columns of B stay in registers between the dot
-// products and the rotation; lane k computes the rotation of pair k and broadcasts it.
-// Returns the largest |cos| seen.
+// products and the rotation; the first lane of group k computes pair k's rotation and
+// broadcasts it.  Returns the largest |cos| seen.
 template <typename Real, int RPL>
 __device__ __forceinline__ Real jacobi_pairs(Real *B, Real *V, Real *nrm, const int *p, const int *q,
                                              const JacobiTol<Real> &tol, int lane, bool &rotated) {
 	constexpr int JPW = PairsPerWarp<RPL>::value;
 	constexpr int LD = 32 * RPL;
+	constexpr int GRP = 32 / JPW;  // lanes per pair group
+	using LR = LaneRows<Real, RPL>;
 	Real x[JPW][RPL], y[JPW][RPL], g[JPW];
 #pragma unroll
 	for (int k = 0; k < JPW; k++) {
+		LR::load(B + p[k] * LD, lane, x[k]);
+		LR::load(B + q[k] * LD, lane, y[k]);
 		Real g0 = 0, g1 = 0;  // two partial sums halve the dependency chain
-		const Real *bp = B + p[k] * LD + lane;
-		const Real *bq = B + q[k] * LD + lane;
 #pragma unroll
 		for (int r = 0; r < RPL; r++) {
-			x[k][r] = bp[32 * r];
-			y[k][r] = bq[32 * r];
 			if (r & 1)
 				g1 += x[k][r] * y[k][r];
 			else
@@ -290,25 +357,21 @@ __device__ __forceinline__ Real jacobi_pairs(Real *B, Real *V, Real *nrm, const 
 		}
 		g[k] = g0 + g1;
 	}
-#pragma unroll
-	for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-		for (int k = 0; k < JPW; k++) g[k] += __shfl_xor_sync(0xffffffffu, g[k], o);
-	// lane k (< JPW) evaluates pair k
+	const Real gk = pair_sums<Real, JPW>(g, lane);
+	const int kk = lane / GRP;
 	Real mycos = 0, myc = 1, mys = 0;
 	int mydo = 0;
-	if (lane < JPW) {
+	if ((lane & (GRP - 1)) == 0) {
 		int pk = p[0], qk = q[0];
-		Real gk = g[0];
 #pragma unroll
 		for (int k = 1; k < JPW; k++)
-			if (lane == k) { pk = p[k]; qk = q[k]; gk = g[k]; }
+			if (kk == k) { pk = p[k]; qk = q[k]; }
 		const Real al = nrm[pk], be = nrm[qk];
 		if (al > tol.zero2 && be > tol.zero2) {
 			mycos = real_abs(gk) * rot_rsqrt(al) * rot_rsqrt(be);
 			if (mycos > tol.rot) {
 				const Real zeta = rot_div(be - al, 2 * gk);
-				const Real t = rot_div((zeta >= 0) ? Real(1) : Real(-1), real_abs(zeta) + real_sqrt(Real(1) + zeta * zeta));
+				const Real t = rot_div((zeta >= 0) ? Real(1) : Real(-1), real_abs(zeta) + rot_sqrt(Real(1) + zeta * zeta));
 				myc = rot_cos(Real(1) + t * t);
 				mys = myc * t;
 				mydo = 1;
@@ -319,23 +382,28 @@ __device__ __forceinline__ Real jacobi_pairs(Real *B, Real *V, Real *nrm, const 
 	}
 #pragma unroll
 	for (int k = 0; k < JPW; k++) {
-		if (!__shfl_sync(0xffffffffu, mydo, k)) continue;
-		const Real c = __shfl_sync(0xffffffffu, myc, k);
-		const Real s = __shfl_sync(0xffffffffu, mys, k);
-		Real *bp = B + p[k] * LD + lane, *bq = B + q[k] * LD + lane;
+		if (!__shfl_sync(0xffffffffu, mydo, k * GRP)) continue;
+		const Real c = __shfl_sync(0xffffffffu, myc, k * GRP);
+		const Real s = __shfl_sync(0xffffffffu, mys, k * GRP);
 #pragma unroll
 		for (int r = 0; r < RPL; r++) {
-			bp[32 * r] = c * x[k][r] - s * y[k][r];
-			bq[32 * r] = s * x[k][r] + c * y[k][r];
+			const Real a = x[k][r], b2 = y[k][r];
+			x[k][r] = c * a - s * b2;
+			y[k][r] = s * a + c * b2;
 		}
-		if (V) {  // null when the rotations are not accumulated (eigenvector mode)
-			Real *vp = V + p[k] * LD + lane, *vq = V + q[k] * LD + lane;
+		LR::store(B + p[k] * LD, lane, x[k]);
+		LR::store(B + q[k] * LD, lane, y[k]);
+		if (V) {  // null when the rotations are not accumulated (eigenvector mode); x, y reused
+			LR::load(V + p[k] * LD, lane, x[k]);
+			LR::load(V + q[k] * LD, lane, y[k]);
 #pragma unroll
 			for (int r = 0; r < RPL; r++) {
-				const Real u = vp[32 * r], w = vq[32 * r];
-				vp[32 * r] = c * u - s * w;
-				vq[32 * r] = s * u + c * w;
+				const Real a = x[k][r], b2 = y[k][r];
+				x[k][r] = c * a - s * b2;
+				y[k][r] = s * a + c * b2;
 			}
+			LR::store(V + p[k] * LD, lane, x[k]);
+			LR::store(V + q[k] * LD, lane, y[k]);
 		}
 		rotated = true;
 	}
@@ -349,10 +417,11 @@ __device__ __forceinline__ void column_norms(const Real *B, Real *nrm, int m) {
 	constexpr int LD = 32 * RPL;
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
 	for (int c = warp; c < m; c += nwarp) {
-		const Real *bc = B + c * LD + lane;
+		Real x[RPL];
+		LaneRows<Real, RPL>::load(B + c * LD, lane, x);
 		Real ss = 0;
 #pragma unroll
-		for (int r = 0; r < RPL; r++) ss += bc[32 * r] * bc[32 * r];
+		for (int r = 0; r < RPL; r++) ss += x[r] * x[r];
 		ss = warp_sum(ss);
 		if (lane == 0) nrm[c] = ss;
 	}
