@@ -121,32 +121,35 @@ int rpl_for(int n) {
 	return -1;
 }
 
-// Shared memory of k_jacobi for 2*b staged columns (plus the zero pair) of LD rows.
-size_t jacobi_smem(int b, int ld, size_t rb) {
+// Shared memory of k_jacobi for 2*b staged columns (plus the zero pair) of LD rows: A and V
+// columns, norms and the GEMM tiles of the polar factor; in eigenvector mode (no V) A and norms.
+size_t jacobi_smem(int b, int ld, size_t rb, bool with_v = true) {
 	const size_t mst = (size_t)2 * b + 2;
+	if (!with_v) return (mst * ld + mst + 2 + 8) * rb;
 	return (2 * mst * ld + mst + 2 + 2 * 16 * 65 + 8) * rb;
 }
 
 // Jacobi block layout for a searchlight of n vertices in a given precision: resident (two
 // blocks covering all columns stay in shared memory) when it fits, else blocked with the
 // widest block that fits.
-void jacobi_layout(int n, bool fp64, int &bsz, int &nblk, size_t &smem, size_t budget) {
+// Eigenvector mode (no V) stages twice the columns in the same memory, so its blocks may be wider.
+void jacobi_layout(int n, bool fp64, int &bsz, int &nblk, size_t &smem, size_t budget, bool with_v = true) {
 	const size_t rb = real_bytes(fp64);
 	const int ld = 32 * std::max(1, rpl_for(n));
 	int h = (n + 1) / 2;
-	size_t res = jacobi_smem(h, ld, rb);
+	size_t res = jacobi_smem(h, ld, rb, with_v);
 	if (res <= budget) {
 		bsz = h;
 		nblk = 2;
 		smem = res;
 		return;
 	}
-	int b = 32;
-	while (b > 1 && jacobi_smem(b, ld, rb) > budget) b--;
+	int b = with_v ? 32 : 64;
+	while (b > 1 && jacobi_smem(b, ld, rb, with_v) > budget) b--;
 	bsz = b;
 	nblk = (n + b - 1) / b;
 	if (nblk & 1) nblk++;
-	smem = jacobi_smem(b, ld, rb);
+	smem = jacobi_smem(b, ld, rb, with_v);
 }
 
 void jacobi_layout(int n, bool fp64, int &bsz, int &nblk, size_t &smem) {
@@ -257,13 +260,13 @@ int jacobi_threads(int bsz, bool fp64) {
 
 struct Chunk {
 	int s0, s1;
-	std::vector<SlWork> w32, w64;
-	std::vector<Bucket> b32, b64;
+	std::vector<SlWork> w32, w64, weig;  // float32 polar, float64 polar, float64 eigenvector mode
+	std::vector<Bucket> b32, b64, beig;
 	std::vector<int64_t> tofs;  // per slot
 	int64_t scratch_elems8;     // scratch size in 8-byte units (A and V each)
 	int64_t t_elems;            // T scratch floats
 	int64_t uv_elems;
-	SlWork *d_w32 = nullptr, *d_w64 = nullptr;
+	SlWork *d_w32 = nullptr, *d_w64 = nullptr, *d_weig = nullptr;
 	int64_t *d_tofs = nullptr;
 };
 
@@ -395,7 +398,7 @@ int build_chunks(HaB200Plan *P) {
 		int64_t acc8 = 0, tacc = 0, uvacc = 0;
 		std::vector<int64_t> tofs;
 		std::vector<int64_t> aofs8;
-		std::vector<int> bs32, nb32, bs64, nb64;
+		std::vector<int> bs32, nb32, bs64, nb64, bse, nbe;
 		std::vector<size_t> sm32, sm64;
 		while (s < P->count) {
 			int n = P->h_off[s + 1] - P->h_off[s];
@@ -403,9 +406,13 @@ int build_chunks(HaB200Plan *P) {
 			size_t m32, m64;
 			jacobi_layout(n, false, b32, k32, m32, fp32_jacobi_budget());
 			jacobi_layout(n, true, b64, k64, m64);
+			int be, ke;
+			size_t me;
+			jacobi_layout(n, true, be, ke, me, kSmemMax, false);
 			int64_t e32 = ((int64_t)n * k32 * b32 * 4 + 7) / 8;
 			int64_t e64 = (int64_t)n * k64 * b64;
-			int64_t region = std::max<int64_t>(std::max(e32, e64), (int64_t)n * n);
+			int64_t eeig = (int64_t)n * ke * be;
+			int64_t region = std::max<int64_t>(std::max(std::max(e32, e64), eeig), (int64_t)n * n);
 			region = (region + 31) & ~(int64_t)31;
 			size_t bytes_if = (size_t)(acc8 + region) * 8 * 2 + (size_t)(tacc + (int64_t)n * n) * 4;
 			if (!tofs.empty() && bytes_if > budget) break;
@@ -415,6 +422,7 @@ int build_chunks(HaB200Plan *P) {
 			tacc += (int64_t)n * n;
 			bs32.push_back(b32); nb32.push_back(k32); sm32.push_back(m32);
 			bs64.push_back(b64); nb64.push_back(k64); sm64.push_back(m64);
+			bse.push_back(be); nbe.push_back(ke);
 			uvacc += 2 * (int64_t)n;
 			s++;
 		}
@@ -425,7 +433,7 @@ int build_chunks(HaB200Plan *P) {
 		ch.tofs = tofs;
 		const int nsl = ch.s1 - ch.s0;
 		// work items, bucketed by (mode, n range), largest first inside a bucket
-		for (int prec = 0; prec < 2; prec++) {
+		for (int prec = 0; prec < 3; prec++) {  // float32, float64, float64 eigenvector mode
 			std::vector<SlWork> items;
 			int64_t uvo = 0;
 			for (int q = 0; q < nsl; q++) {
@@ -434,8 +442,8 @@ int build_chunks(HaB200Plan *P) {
 				SlWork w;
 				w.s = sidx;
 				w.n = n;
-				w.bsz = prec ? bs64[q] : bs32[q];
-				w.nblk = prec ? nb64[q] : nb32[q];
+				w.bsz = prec == 2 ? bse[q] : (prec ? bs64[q] : bs32[q]);
+				w.nblk = prec == 2 ? nbe[q] : (prec ? nb64[q] : nb32[q]);
 				w.aofs = prec ? aofs8[q] : aofs8[q] * 2;
 				w.tofs = tofs[q];
 				w.sofs = P->h_off[sidx];
@@ -457,7 +465,7 @@ int build_chunks(HaB200Plan *P) {
 				while (j < (int)items.size() && key(items[j]) == key(items[i])) {
 					int bb, kk;
 					size_t mm;
-					jacobi_layout(items[j].n, prec == 1, bb, kk, mm, prec == 1 ? kSmemMax : fp32_jacobi_budget());
+					jacobi_layout(items[j].n, prec >= 1, bb, kk, mm, prec >= 1 ? kSmemMax : fp32_jacobi_budget(), prec != 2);
 					smem = std::max(smem, mm);
 					j++;
 				}
@@ -466,21 +474,24 @@ int build_chunks(HaB200Plan *P) {
 				b.count = j - i;
 				b.smem = smem;
 				b.blocked = items[i].nblk != 2;
-				b.threads = jacobi_threads(items[i].bsz, prec == 1);
+				b.threads = jacobi_threads(items[i].bsz, prec >= 1);
 				b.rpl = rpl_for(items[i].n);
 				buckets.push_back(b);
 				i = j;
 			}
 			if (prec == 0) { ch.w32 = items; ch.b32 = buckets; }
-			else { ch.w64 = items; ch.b64 = buckets; }
+			else if (prec == 1) { ch.w64 = items; ch.b64 = buckets; }
+			else { ch.weig = items; ch.beig = buckets; }
 		}
 		P->chunks.push_back(std::move(ch));
 	}
 	// device copies of the work lists
 	for (auto &ch : P->chunks) {
-		size_t n32 = ch.w32.size(), n64 = ch.w64.size();
+		size_t n32 = ch.w32.size(), n64 = ch.w64.size(), ne = ch.weig.size();
 		if (cudaMalloc(&ch.d_w32, n32 * sizeof(SlWork)) != cudaSuccess) return kHaErrorAlloc;
 		if (cudaMalloc(&ch.d_w64, n64 * sizeof(SlWork)) != cudaSuccess) return kHaErrorAlloc;
+		if (cudaMalloc(&ch.d_weig, ne * sizeof(SlWork)) != cudaSuccess) return kHaErrorAlloc;
+		HA_CUDA(cudaMemcpy(ch.d_weig, ch.weig.data(), ne * sizeof(SlWork), cudaMemcpyHostToDevice));
 		if (cudaMalloc(&ch.d_tofs, ch.tofs.size() * sizeof(int64_t)) != cudaSuccess) return kHaErrorAlloc;
 		HA_CUDA(cudaMemcpy(ch.d_w32, ch.w32.data(), n32 * sizeof(SlWork), cudaMemcpyHostToDevice));
 		HA_CUDA(cudaMemcpy(ch.d_w64, ch.w64.data(), n64 * sizeof(SlWork), cudaMemcpyHostToDevice));
@@ -1037,14 +1048,14 @@ int grid_chunk(HaB200Plan *P, Chunk &ch, const double *d_X, const double *d_Y, c
 	const JacobiParams jp = eig_params(false);
 	std::vector<int64_t> gbase;
 	int rc;
-	const int nitems = (int)ch.w64.size();
+	const int nitems = (int)ch.weig.size();
 	int i0 = 0;
 	while (i0 < nitems) {
 		gbase.assign((size_t)nsl, 0);
 		int64_t total = 0;
 		int i1 = i0;
 		while (i1 < nitems) {
-			const SlWork &wi = ch.w64[i1];
+			const SlWork &wi = ch.weig[i1];
 			const GridLayout L = GridLayout::make(wi.n, gp.models, gp.mte, gp.ntu, grid);
 			if (i1 > i0 && (size_t)(total + L.total) * 8 > budget) break;
 			gbase[wi.slot] = total;
@@ -1058,12 +1069,12 @@ int grid_chunk(HaB200Plan *P, Chunk &ch, const double *d_X, const double *d_Y, c
 			const GridModel &md = gs.mdl[mo];
 			const int32_t *tr = P->grows.p + md.tr_ofs;
 			if ((rc = g_fan.begin(st)) != kHaSuccess) return rc;
-			for (size_t bi = 0; bi < ch.b64.size(); bi++) {
-				const Bucket &b = ch.b64[bi];
+			for (size_t bi = 0; bi < ch.beig.size(); bi++) {
+				const Bucket &b = ch.beig[bi];
 				const int x0 = std::max(i0, b.first), x1 = std::min(i1, b.first + b.count);
 				if (x1 <= x0) continue;
 				const cudaStream_t bs = g_fan.at((int)bi);
-				const SlWork *wk = ch.d_w64 + x0;
+				const SlWork *wk = ch.d_weig + x0;
 				// Gram into the V scratch, its pivoted Cholesky factor into the A scratch
 				{ HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16><<<x1 - x0, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_X, nt, tr, md.tr_n, V, P->gridscr.p, gp, 0); }
 				{ HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16><<<x1 - x0, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_Y, nt, tr, md.tr_n, A, P->gridscr.p, gp, 1); }
@@ -1075,9 +1086,9 @@ int grid_chunk(HaB200Plan *P, Chunk &ch, const double *d_X, const double *d_Y, c
 				}
 			}
 			if ((rc = g_fan.end(st)) != kHaSuccess) return rc;
-			{ HA_LAUNCH(kHaB200KGrid, st); k_grid_model<<<i1 - i0, kBlock, 0, st>>>(ch.d_w64 + i0, P->idx.p, d_X, V, P->uv.p, mo, P->gridscr.p, gp); }
+			{ HA_LAUNCH(kHaB200KGrid, st); k_grid_model<<<i1 - i0, kBlock, 0, st>>>(ch.d_weig + i0, P->idx.p, d_X, V, P->uv.p, mo, P->gridscr.p, gp); }
 		}
-		{ HA_LAUNCH(kHaB200KGrid, st); k_grid_eval<<<i1 - i0, kBlock, 0, st>>>(ch.d_w64 + i0, P->idx.p, d_Y, P->gridscr.p, gp, P->scrT64.p, rowmajor, d_best, d_cost); }
+		{ HA_LAUNCH(kHaB200KGrid, st); k_grid_eval<<<i1 - i0, kBlock, 0, st>>>(ch.d_weig + i0, P->idx.p, d_Y, P->gridscr.p, gp, P->scrT64.p, rowmajor, d_best, d_cost); }
 		HA_CUDA(cudaGetLastError());
 		i0 = i1;
 	}
@@ -1115,10 +1126,10 @@ int eigen_chunk(HaB200Plan *P, Chunk &ch, const double *d_X, const double *d_Y, 
 	double *A = P->scrA.p, *V = P->scrV.p;
 	int rc;
 	if ((rc = g_fan.begin(st)) != kHaSuccess) return rc;
-	for (size_t bi = 0; bi < ch.b64.size(); bi++) {
-		const Bucket &b = ch.b64[bi];
+	for (size_t bi = 0; bi < ch.beig.size(); bi++) {
+		const Bucket &b = ch.beig[bi];
 		const cudaStream_t bs = g_fan.at((int)bi);
-		const SlWork *wk = ch.d_w64 + b.first;
+		const SlWork *wk = ch.d_weig + b.first;
 		{ HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16><<<b.count, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_X, P->nt, d_rows, n_rows, V, nullptr, gp, 0); }
 		if (d_Y) { HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16><<<b.count, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_Y, P->nt, d_rows, n_rows, P->scrT64.p, nullptr, gp, 2); }
 		{ HA_LAUNCH(kHaB200KRidge, bs); k_pchol<<<b.count, kBlock, 0, bs>>>(wk, V, A, P->stats.p); }
@@ -1129,7 +1140,7 @@ int eigen_chunk(HaB200Plan *P, Chunk &ch, const double *d_X, const double *d_Y, 
 		}
 	}
 	if ((rc = g_fan.end(st)) != kHaSuccess) return rc;
-	{ HA_LAUNCH(kHaB200KGrid, st); k_features<<<(int)ch.w64.size(), kBlock, 0, st>>>(ch.d_w64, P->uv.p, d_feat); }
+	{ HA_LAUNCH(kHaB200KGrid, st); k_features<<<(int)ch.weig.size(), kBlock, 0, st>>>(ch.d_weig, P->uv.p, d_feat); }
 	HA_CUDA(cudaGetLastError());
 	return kHaSuccess;
 }
@@ -1184,7 +1195,7 @@ int run_ridge_learned(HaB200Plan *P, const double *d_X, const double *d_Y, const
 		if ((rc = ha_b200_mlp_infer(d_params, C, P->gfeat.p + (size_t)ch.s0 * (kFeatSv + 1), nsl, d_choice + ch.s0,
 		                            d_prob + ch.s0, st)) != kHaSuccess)
 			return rc;
-		{ HA_LAUNCH(kHaB200KGrid, st); k_proposed_fit<<<(int)ch.w64.size(), kBlock, 0, st>>>(ch.d_w64, P->scrV.p, P->uv.p, P->scrA.p, P->scrT64.p, d_choice, d_prob, min_prob, gp.alphas, gp.npcs, gp.n_npcs, n_rows, rowmajor); }
+		{ HA_LAUNCH(kHaB200KGrid, st); k_proposed_fit<<<(int)ch.weig.size(), kBlock, 0, st>>>(ch.d_weig, P->scrV.p, P->uv.p, P->scrA.p, P->scrT64.p, d_choice, d_prob, min_prob, gp.alphas, gp.npcs, gp.n_npcs, n_rows, rowmajor); }
 		HA_CUDA(cudaGetLastError());
 		// searchlights below the threshold: the full grid search
 		hprob.resize((size_t)nsl);
@@ -1194,18 +1205,18 @@ int run_ridge_learned(HaB200Plan *P, const double *d_X, const double *d_Y, const
 		Chunk fb;
 		fb.s0 = ch.s0;
 		fb.s1 = ch.s1;
-		for (const Bucket &b : ch.b64) {
+		for (const Bucket &b : ch.beig) {
 			Bucket nb = b;
-			nb.first = (int)fb.w64.size();
+			nb.first = (int)fb.weig.size();
 			for (int i = b.first; i < b.first + b.count; i++)
-				if (hprob[(size_t)(ch.w64[i].s - ch.s0)] < min_prob) fb.w64.push_back(ch.w64[i]);
-			nb.count = (int)fb.w64.size() - nb.first;
-			if (nb.count > 0) fb.b64.push_back(nb);
+				if (hprob[(size_t)(ch.weig[i].s - ch.s0)] < min_prob) fb.weig.push_back(ch.weig[i]);
+			nb.count = (int)fb.weig.size() - nb.first;
+			if (nb.count > 0) fb.beig.push_back(nb);
 		}
-		if (!fb.w64.empty()) {
-			if ((rc = P->gwork.ensure(fb.w64.size())) != kHaSuccess) return rc;
-			HA_CUDA(cudaMemcpyAsync(P->gwork.p, fb.w64.data(), fb.w64.size() * sizeof(SlWork), cudaMemcpyHostToDevice, st));
-			fb.d_w64 = P->gwork.p;
+		if (!fb.weig.empty()) {
+			if ((rc = P->gwork.ensure(fb.weig.size())) != kHaSuccess) return rc;
+			HA_CUDA(cudaMemcpyAsync(P->gwork.p, fb.weig.data(), fb.weig.size() * sizeof(SlWork), cudaMemcpyHostToDevice, st));
+			fb.d_weig = P->gwork.p;
 			if ((rc = grid_chunk(P, fb, d_X, d_Y, gs, gp, rowmajor, d_choice, nullptr, st)) != kHaSuccess) return rc;
 		}
 		if ((rc = reduce_chunk64(P, ch, out_kind, d_vals, st)) != kHaSuccess) return rc;
@@ -1757,6 +1768,7 @@ void ha_b200_plan_destroy(HaB200Plan *P) {
 	for (auto &ch : P->chunks) {
 		if (ch.d_w32) cudaFree(ch.d_w32);
 		if (ch.d_w64) cudaFree(ch.d_w64);
+		if (ch.d_weig) cudaFree(ch.d_weig);
 		if (ch.d_tofs) cudaFree(ch.d_tofs);
 	}
 	P->idx.release(); P->off.release(); P->lo.release(); P->hi.release(); P->w.release();

@@ -624,10 +624,11 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) k_jacobi(const
 	const Real sqn = real_sqrt(Real(n));
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
 
-	// shared: Bs[mst][LD], Vs[mst][LD], nrm[mst], then GEMM tiles (resident mode)
+	// shared: Bs[mst][LD], Vs[mst][LD], nrm[mst], then GEMM tiles (resident mode); eigenvector
+	// mode has no Vs (nrm follows Bs)
 	Real *Bs = sm;
 	Real *Vs = sm + mst * LD;
-	Real *nrm = Vs + mst * LD;
+	Real *nrm = prm.eig ? Vs : Vs + mst * LD;
 	__shared__ Real red[32];
 	__shared__ double frob2;
 
@@ -653,7 +654,7 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) k_jacobi(const
 		for (int e = threadIdx.x; e < mst * LD; e += blockDim.x) {
 			const int c = e / LD, i = e - c * LD;
 			Bs[e] = (c < ncol && i < n) ? Ag[c * n + i] : Real(0);
-			Vs[e] = (c == i && c < n) ? Real(1) : Real(0);
+			if (!prm.eig) Vs[e] = (c == i && c < n) ? Real(1) : Real(0);
 		}
 		__syncthreads();
 		for (sweep = 0; sweep < prm.max_sweeps; sweep++) {
@@ -676,7 +677,7 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) k_jacobi(const
 		Real *Vst = prm.eig ? nullptr : Vs;
 		for (int e = threadIdx.x; e < mst * LD; e += blockDim.x) {
 			Bs[e] = Real(0);
-			Vs[e] = Real(0);
+			if (Vst) Vs[e] = Real(0);
 		}
 		__syncthreads();
 		// only the blocks holding the leading nonzero columns take part (eigenvector mode)
