@@ -537,6 +537,7 @@ int set_smem_attrs() {
 	HA_CUDA(cudaFuncSetAttribute(k_reduce<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax));
 	HA_CUDA(cudaFuncSetAttribute(k_reduce<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax));
 	HA_CUDA(cudaFuncSetAttribute(k_pattern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax));
+	HA_CUDA(cudaFuncSetAttribute(k_pchol, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(kPcholNb * kGridMaxN * 8)));
 	done = true;
 	return kHaSuccess;
 }
@@ -904,11 +905,11 @@ int upload_vec(DevArr<T> &d, const std::vector<T> &h, cudaStream_t st) {
 	return kHaSuccess;
 }
 
-// Grid scratch budget per sub-batch of searchlights (HA_B200_GRID_GB overrides the default).
+// Grid scratch budget per sub-batch of searchlights (HA_B200_GRID_GB overrides the default 24 GB).
 size_t grid_budget_bytes() {
 	const char *e = getenv("HA_B200_GRID_GB");
-	double gb = e ? atof(e) : 8.0;
-	if (!(gb > 0.001)) gb = 8.0;
+	double gb = e ? atof(e) : 24.0;
+	if (!(gb > 0.001)) gb = 24.0;
 	return (size_t)(gb * 1073741824.0);
 }
 
@@ -1008,6 +1009,8 @@ int grid_prepare(HaB200Plan *P) {
 	return P->scrT64.ensure((size_t)maxT);
 }
 
+size_t pchol_smem(int rpl) { return (size_t)kPcholNb * 32 * rpl * sizeof(double); }
+
 JacobiParams eig_params(bool only_flagged) {
 	JacobiParams jp;
 	jp.max_sweeps = 40;
@@ -1056,7 +1059,7 @@ int grid_chunk(HaB200Plan *P, Chunk &ch, const double *d_X, const double *d_Y, c
 		int i1 = i0;
 		while (i1 < nitems) {
 			const SlWork &wi = ch.weig[i1];
-			const GridLayout L = GridLayout::make(wi.n, gp.models, gp.mte, gp.ntu, grid);
+			const GridLayout L = GridLayout::make(wi.n, gp.models, gp.mte, gp.ntu, gp.n_alphas, grid);
 			if (i1 > i0 && (size_t)(total + L.total) * 8 > budget) break;
 			gbase[wi.slot] = total;
 			total += L.total;
@@ -1078,7 +1081,7 @@ int grid_chunk(HaB200Plan *P, Chunk &ch, const double *d_X, const double *d_Y, c
 				// Gram into the V scratch, its pivoted Cholesky factor into the A scratch
 				{ HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16><<<x1 - x0, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_X, nt, tr, md.tr_n, V, P->gridscr.p, gp, 0); }
 				{ HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16><<<x1 - x0, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_Y, nt, tr, md.tr_n, A, P->gridscr.p, gp, 1); }
-				{ HA_LAUNCH(kHaB200KRidge, bs); k_pchol<<<x1 - x0, kBlock, 0, bs>>>(wk, V, A, P->stats.p); }
+				{ HA_LAUNCH(kHaB200KRidge, bs); k_pchol<<<x1 - x0, kBlock, pchol_smem(b.rpl), bs>>>(wk, V, A, P->stats.p); }
 				{
 					HA_LAUNCH(kHaB200KJacobi64, bs);
 					if ((rc = launch_jacobi<double>(b.rpl, x1 - x0, b.threads, b.smem, bs, wk, A, V, P->scrT.p, P->stats.p, P->uv.p, jp)) != kHaSuccess)
@@ -1086,9 +1089,10 @@ int grid_chunk(HaB200Plan *P, Chunk &ch, const double *d_X, const double *d_Y, c
 				}
 			}
 			if ((rc = g_fan.end(st)) != kHaSuccess) return rc;
-			{ HA_LAUNCH(kHaB200KGrid, st); k_grid_model<<<i1 - i0, kBlock, 0, st>>>(ch.d_weig + i0, P->idx.p, d_X, V, P->uv.p, mo, P->gridscr.p, gp); }
+			{ HA_LAUNCH(kHaB200KGrid, st); k_grid_model<<<i1 - i0, kBlock, 0, st>>>(ch.d_weig + i0, P->idx.p, d_X, d_Y, V, P->uv.p, mo, P->gridscr.p, gp); }
 		}
-		{ HA_LAUNCH(kHaB200KGrid, st); k_grid_eval<<<i1 - i0, kBlock, 0, st>>>(ch.d_weig + i0, P->idx.p, d_Y, P->gridscr.p, gp, P->scrT64.p, rowmajor, d_best, d_cost); }
+		{ HA_LAUNCH(kHaB200KGrid, st); k_grid_eval<<<dim3(i1 - i0, gp.n_alphas), kBlock, 0, st>>>(ch.d_weig + i0, P->gridscr.p, gp); }
+		{ HA_LAUNCH(kHaB200KGrid, st); k_grid_final<<<i1 - i0, kBlock, 0, st>>>(ch.d_weig + i0, P->idx.p, d_Y, P->gridscr.p, gp, P->scrT64.p, rowmajor, d_best, d_cost); }
 		HA_CUDA(cudaGetLastError());
 		i0 = i1;
 	}
@@ -1132,7 +1136,7 @@ int eigen_chunk(HaB200Plan *P, Chunk &ch, const double *d_X, const double *d_Y, 
 		const SlWork *wk = ch.d_weig + b.first;
 		{ HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16><<<b.count, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_X, P->nt, d_rows, n_rows, V, nullptr, gp, 0); }
 		if (d_Y) { HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16><<<b.count, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_Y, P->nt, d_rows, n_rows, P->scrT64.p, nullptr, gp, 2); }
-		{ HA_LAUNCH(kHaB200KRidge, bs); k_pchol<<<b.count, kBlock, 0, bs>>>(wk, V, A, P->stats.p); }
+		{ HA_LAUNCH(kHaB200KRidge, bs); k_pchol<<<b.count, kBlock, pchol_smem(b.rpl), bs>>>(wk, V, A, P->stats.p); }
 		{
 			HA_LAUNCH(kHaB200KJacobi64, bs);
 			if ((rc = launch_jacobi<double>(b.rpl, b.count, b.threads, b.smem, bs, wk, A, V, P->scrT.p, P->stats.p, P->uv.p, jp)) != kHaSuccess)

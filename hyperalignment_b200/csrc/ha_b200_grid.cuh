@@ -43,12 +43,14 @@ struct GridParams {
 
 // Per-searchlight layout of the grid scratch (float64 elements from the searchlight's base).
 // Per model: V and Q with components in decreasing-lambda order (V column r = r-th component,
-// Q row r), lambda in that order, E = X_te V (mte x n, column-major, ld mte) and the cumulative
-// test predictions Pm (mte x n).  P and Yu are the averaged predictions and the targets on the
-// union of tested rows (ntu x n, column-major), C the cross-covariance of the current model.
+// Q row r), lambda in that order and E = X_te V (mte x n, column-major, ld mte).  Per alpha (the
+// grid evaluation runs one CTA per searchlight and alpha): the models' cumulative test predictions
+// Pm (models x mte x n) and the averaged predictions P on the union of tested rows (ntu x n,
+// column-major; alpha 0's block is also the n x n beta accumulator of the winner).  Yu holds the
+// targets on the tested rows, C the cross-covariance of the current model.
 struct GridLayout {
-	int64_t C, Vst, Qst, Lst, Est, Pm, P, Yu, Xte, cost, total;
-	__host__ __device__ static GridLayout make(int n, int models, int mte, int ntu, int grid) {
+	int64_t C, Vst, Qst, Lst, Est, Yu, Xte, cost, PA, pa_stride, total;
+	__host__ __device__ static GridLayout make(int n, int models, int mte, int ntu, int n_alphas, int grid) {
 		GridLayout L;
 		const int64_t n2 = (int64_t)n * n, mn = (int64_t)mte * n;
 		int64_t o = 0;
@@ -57,18 +59,24 @@ struct GridLayout {
 		L.Qst = o; o += (int64_t)models * n2;
 		L.Lst = o; o += (int64_t)models * n;
 		L.Est = o; o += (int64_t)models * mn;
-		L.Pm = o; o += (int64_t)models * mn;
-		L.P = o; o += (int64_t)max(ntu, n) * n;  // also the n x n beta accumulator at the end
 		L.Yu = o; o += (int64_t)ntu * n;
 		L.Xte = o; o += mn;
 		L.cost = o; o += grid;
+		L.pa_stride = (((int64_t)models * mn + (int64_t)(ntu > n ? ntu : n) * n) + 31) & ~(int64_t)31;
+		L.PA = (o + 31) & ~(int64_t)31;
+		o = L.PA + (int64_t)n_alphas * L.pa_stride;
 		L.total = (o + 31) & ~(int64_t)31;
 		return L;
+	}
+	// per-alpha blocks: Pm at PA + a * pa_stride, P right after it
+	__host__ __device__ int64_t Pm(int a) const { return PA + (int64_t)a * pa_stride; }
+	__host__ __device__ int64_t P(int a, int models, int mte, int n) const {
+		return Pm(a) + (int64_t)models * mte * n;
 	}
 };
 
 __device__ __forceinline__ GridLayout grid_layout(const GridParams &gp, int n) {
-	return GridLayout::make(n, gp.models, gp.mte, gp.ntu, gp.n_alphas * gp.n_npcs);
+	return GridLayout::make(n, gp.models, gp.mte, gp.ntu, gp.n_alphas, gp.n_alphas * gp.n_npcs);
 }
 
 // A_s = X[rows, sl]^T Z[rows, sl] (Z = X for the Gram, Y for the cross-covariance) over one row
@@ -147,17 +155,23 @@ __global__ void __launch_bounds__(256) k_xcov_rows(const SlWork *__restrict__ wo
 		for (int64_t e = (int64_t)n * n + threadIdx.x; e < (int64_t)n * ncol; e += 256) A[e] = 0.0;
 }
 
-// Pivoted Cholesky G = sum_k r_k r_k^T (right-looking; pivot = largest remaining diagonal, ties to
-// the smaller vertex index), stopped when the largest remaining diagonal is at most
-// n * eps * max(diag G).  The Schur complements overwrite G (column-major, ld n, at Gscr + w.aofs);
+// Pivoted Cholesky G = sum_k r_k r_k^T (pivot = largest remaining diagonal, ties to the smaller
+// vertex index), stopped when the largest remaining diagonal is at most n * eps * max(diag G).
+// Panels of kPcholNb columns: inside a panel each new column is corrected by the panel's earlier
+// columns (kept in shared memory, indexed by vertex) and the diagonal is updated per column; the
+// trailing Schur complement in G (column-major, ld n, at Gscr + w.aofs) is updated once per panel.
 // r_k (original vertex order, zero at earlier pivots) becomes column k of Rt (ld n, ncol columns,
-// the rest zero), so G = Rt Rt^T; the number of columns (the numerical rank) goes to the stats.  The one-sided Jacobi rotations then run on Rt: its columns
-// come in decreasing, graded norms and only rank(G) of them are nonzero, which takes fewer sweeps
-// than rotating G itself and needs no accumulated rotations.
+// the rest zero), so G = Rt Rt^T; the number of columns (the numerical rank) goes to the stats.
+// The one-sided Jacobi rotations then run on Rt: its columns come in decreasing, graded norms and
+// only rank(G) of them are nonzero, which takes fewer sweeps than rotating G itself and needs no
+// accumulated rotations.  Dynamic shared memory: kPcholNb * 32 * RPL doubles (>= kPcholNb * n).
+constexpr int kPcholNb = 16;
+
 __global__ void __launch_bounds__(256) k_pchol(const SlWork *__restrict__ work, double *__restrict__ Gscr,
                                                double *__restrict__ Rscr, SlStats *__restrict__ stats) {
-	__shared__ int rem[kGridMaxN];      // vertices not yet pivoted (positions 0 .. m-1)
-	__shared__ double rk[kGridMaxN];    // the current r_k at those positions
+	extern __shared__ __align__(16) double pan[];  // [kPcholNb][n], indexed by vertex
+	__shared__ int rem[kGridMaxN];                  // vertices not yet pivoted (positions 0 .. m-1)
+	__shared__ double dg[kGridMaxN];                // current Schur diagonal, by vertex
 	__shared__ double rv[32];
 	__shared__ int ri[32], rpos[32];
 	__shared__ double s_tol, s_piv;
@@ -167,11 +181,15 @@ __global__ void __launch_bounds__(256) k_pchol(const SlWork *__restrict__ work, 
 	double *S = Gscr + w.aofs;
 	double *Rt = Rscr + w.aofs;
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-	for (int i = threadIdx.x; i < n; i += blockDim.x) rem[i] = i;
+	for (int i = threadIdx.x; i < n; i += blockDim.x) {
+		rem[i] = i;
+		dg[i] = S[(int64_t)i * n + i];
+	}
 	for (int64_t e = threadIdx.x; e < (int64_t)n * ncol; e += blockDim.x) Rt[e] = 0.0;
+	__syncthreads();
 	{
 		double mx = 0.0;
-		for (int i = threadIdx.x; i < n; i += blockDim.x) mx = fmax(mx, S[(int64_t)i * n + i]);
+		for (int i = threadIdx.x; i < n; i += blockDim.x) mx = fmax(mx, dg[i]);
 		for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
 		if (lane == 0) rv[warp] = mx;
 		__syncthreads();
@@ -183,52 +201,71 @@ __global__ void __launch_bounds__(256) k_pchol(const SlWork *__restrict__ work, 
 		__syncthreads();
 	}
 	int m = n, k = 0;
-	for (; k < n; k++) {
-		// pivot: largest remaining diagonal (ties: smaller vertex index)
-		double bv = -1.0;
-		int bi = 0x7fffffff, bpos = 0;
-		for (int a = threadIdx.x; a < m; a += blockDim.x) {
-			const int v = rem[a];
-			const double d = S[(int64_t)v * n + v];
-			if (d > bv || (d == bv && v < bi)) { bv = d; bi = v; bpos = a; }
+	bool stop = false;
+	while (k < n && !stop) {
+		int nbk = 0;  // columns of the current panel
+		for (; nbk < kPcholNb && k < n; nbk++, k++) {
+			// pivot: largest remaining diagonal (ties: smaller vertex index)
+			double bv = -1.0;
+			int bi = 0x7fffffff, bpos = 0;
+			for (int a = threadIdx.x; a < m; a += blockDim.x) {
+				const int v = rem[a];
+				const double d = dg[v];
+				if (d > bv || (d == bv && v < bi)) { bv = d; bi = v; bpos = a; }
+			}
+			for (int o = 16; o > 0; o >>= 1) {
+				const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+				const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+				const int op = __shfl_xor_sync(0xffffffffu, bpos, o);
+				if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; bpos = op; }
+			}
+			if (lane == 0) { rv[warp] = bv; ri[warp] = bi; rpos[warp] = bpos; }
+			__syncthreads();
+			if (threadIdx.x == 0) {
+				double v = rv[0];
+				int vi = ri[0], pos = rpos[0];
+				for (int q = 1; q < nwarp; q++)
+					if (rv[q] > v || (rv[q] == v && ri[q] < vi)) { v = rv[q]; vi = ri[q]; pos = rpos[q]; }
+				s_piv = v;
+				s_pos = pos;
+			}
+			__syncthreads();
+			if (!(s_piv > s_tol)) {
+				stop = true;
+				break;
+			}
+			const int a = s_pos, p = rem[a];
+			const double rp = sqrt(s_piv);
+			double *rk = pan + (int64_t)nbk * n;
+			for (int b = threadIdx.x; b < m; b += blockDim.x) {
+				const int v = rem[b];
+				double r = rp;
+				if (b != a) {
+					double x = S[(int64_t)p * n + v];
+					for (int j = 0; j < nbk; j++) x -= pan[(int64_t)j * n + p] * pan[(int64_t)j * n + v];
+					r = x / rp;
+					dg[v] -= r * r;
+				}
+				rk[v] = r;
+				Rt[(int64_t)k * n + v] = r;
+			}
+			__syncthreads();
+			if (threadIdx.x == 0) rem[a] = rem[m - 1];
+			m--;
+			__syncthreads();
 		}
-		for (int o = 16; o > 0; o >>= 1) {
-			const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
-			const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-			const int op = __shfl_xor_sync(0xffffffffu, bpos, o);
-			if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; bpos = op; }
-		}
-		if (lane == 0) { rv[warp] = bv; ri[warp] = bi; rpos[warp] = bpos; }
-		__syncthreads();
-		if (threadIdx.x == 0) {
-			double v = rv[0];
-			int vi = ri[0], pos = rpos[0];
-			for (int q = 1; q < nwarp; q++)
-				if (rv[q] > v || (rv[q] == v && ri[q] < vi)) { v = rv[q]; vi = ri[q]; pos = rpos[q]; }
-			s_piv = v;
-			s_pos = pos;
-		}
-		__syncthreads();
-		if (!(s_piv > s_tol)) break;
-		const int a = s_pos, p = rem[a];
-		const double rp = sqrt(s_piv);
-		for (int b = threadIdx.x; b < m; b += blockDim.x) {
-			const double r = (b == a) ? rp : S[(int64_t)p * n + rem[b]] / rp;
-			rk[b] = r;
-			Rt[(int64_t)k * n + rem[b]] = r;
-		}
-		__syncthreads();
-		// Schur complement on the remaining vertices other than the pivot
+		if (stop || m == 0) break;
+		// Schur complement on the remaining vertices with the panel's nbk columns
 		for (int c = warp; c < m; c += nwarp) {
-			if (c == a) continue;
-			const double rc = rk[c];
-			double *Sc = S + (int64_t)rem[c] * n;
-			for (int b = lane; b < m; b += 32)
-				if (b != a) Sc[rem[b]] -= rk[b] * rc;
+			const int u = rem[c];
+			double *Su = S + (int64_t)u * n;
+			for (int b = lane; b < m; b += 32) {
+				const int v = rem[b];
+				double acc = 0.0;
+				for (int j = 0; j < nbk; j++) acc += pan[(int64_t)j * n + v] * pan[(int64_t)j * n + u];
+				Su[v] -= acc;
+			}
 		}
-		__syncthreads();
-		if (threadIdx.x == 0) rem[a] = rem[m - 1];
-		m--;
 		__syncthreads();
 	}
 	if (threadIdx.x == 0) stats[w.slot].ncols = max(k, 1);
@@ -252,9 +289,9 @@ __device__ __forceinline__ void rank_desc(const double *lam, int n, int *order) 
 // pivoted Cholesky factor of the Gram; C is in the grid scratch.
 // Stores V, lambda in decreasing-lambda order, Q = V^T C and E = X_te V for the model.
 __global__ void __launch_bounds__(256) k_grid_model(const SlWork *__restrict__ work, const int32_t *__restrict__ sl_idx,
-                                                    const double *__restrict__ X, const double *__restrict__ Vscr,
-                                                    const double *__restrict__ uvbuf, int model,
-                                                    double *__restrict__ Gscr, GridParams gp) {
+                                                    const double *__restrict__ X, const double *__restrict__ Y,
+                                                    const double *__restrict__ Vscr, const double *__restrict__ uvbuf,
+                                                    int model, double *__restrict__ Gscr, GridParams gp) {
 	__shared__ double ps[16][65], qs[16][65];
 	__shared__ int order[kGridMaxN];
 	const SlWork w = work[blockIdx.x];
@@ -274,6 +311,11 @@ __global__ void __launch_bounds__(256) k_grid_model(const SlWork *__restrict__ w
 	double *Xte = base + L.Xte;
 	const double *C = base + L.C;
 	const int32_t *te = gp.rows + md.te_ofs;
+	if (model == 0)  // the targets on the tested rows, for the grid evaluation
+		for (int64_t e = threadIdx.x; e < (int64_t)gp.ntu * n; e += blockDim.x) {
+			const int j = (int)(e / gp.ntu), u = (int)(e - (int64_t)j * gp.ntu);
+			base[L.Yu + e] = Y[(int64_t)sl[j] * gp.nt + gp.urows[u]];
+		}
 	rank_desc(lam, n, order);
 	__syncthreads();
 	for (int64_t e = threadIdx.x; e < n2; e += blockDim.x) {
@@ -326,14 +368,89 @@ __device__ __forceinline__ double block_sum256(double v, double *red) {
 	return tot;
 }
 
-// The grid evaluation of every searchlight after all models: cost of every (alpha, PC count),
-// the winner, and the winner's model-averaged beta, written float64 in the T layout (row-major for
-// CSR output, column-major for CSC).  cost_out (may be null) gets the grid's costs per
-// searchlight, best_out the winning grid index.
-__global__ void __launch_bounds__(256) k_grid_eval(const SlWork *__restrict__ work, const int32_t *__restrict__ sl_idx,
-                                                   const double *__restrict__ Y, double *__restrict__ Gscr, GridParams gp,
-                                                   double *__restrict__ Bout, int t_rowmajor,
-                                                   int32_t *__restrict__ best_out, double *__restrict__ cost_out) {
+// The grid evaluation after all models, one CTA per (searchlight, alpha = blockIdx.y): the models'
+// cumulative test predictions over the PC chunks, their average per tested row and the squared
+// error over the tested rows and the targets, cost[alpha * n_npcs + p] (without the untested
+// rows, which k_grid_final adds).
+__global__ void __launch_bounds__(256) k_grid_eval(const SlWork *__restrict__ work, double *__restrict__ Gscr,
+                                                   GridParams gp) {
+	__shared__ double ps[16][65], qs[16][65];
+	__shared__ double cval[kGridMaxN];
+	__shared__ double red[32];
+	const SlWork w = work[blockIdx.x];
+	const int a = blockIdx.y;
+	const int n = w.n;
+	const GridLayout L = grid_layout(gp, n);
+	double *base = Gscr + gp.gbase[w.slot];
+	const int64_t n2 = (int64_t)n * n, mn = (int64_t)gp.mte * n;
+	const int ntu = gp.ntu;
+	double *Pma = base + L.Pm(a);
+	double *P = base + L.P(a, gp.models, gp.mte, n);
+	const double *Yu = base + L.Yu;
+	double *cost = base + L.cost;
+	const double al = gp.alphas[a];
+	GemmArgs<double, double> g;
+	g.alpha = 1.0;
+	g.beta = 1.0;
+	for (int64_t e = threadIdx.x; e < gp.models * mn; e += blockDim.x) Pma[e] = 0.0;
+	__syncthreads();
+	for (int p = 0; p < gp.n_npcs; p++) {
+		// Pm += E[:, r0:r1] diag(1 / (alpha + lambda)) Q[r0:r1, :] for every model
+		for (int mo = 0; mo < gp.models; mo++) {
+			const GridModel md = gp.mdl[mo];
+			const int m = md.te_n;
+			int r0, r1;
+			pc_chunk(gp.npcs, p, min(md.tr_n, n), r0, r1);
+			if (r1 <= r0 || m == 0) continue;
+			const double *lam = base + L.Lst + (int64_t)mo * n;
+			__syncthreads();
+			for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x) cval[r] = 1.0 / (al + lam[r]);
+			__syncthreads();
+			const double *E = base + L.Est + mo * mn;
+			const double *Q = base + L.Qst + mo * n2;
+			double *Pm = Pma + mo * mn;
+			g.M = m; g.N = n; g.K = r1 - r0;
+			g.P = E + (int64_t)r0 * m; g.pk = m; g.pi = 1;
+			g.Q = Q + r0; g.qk = 1; g.qj = n;
+			g.d = cval + r0;
+			g.E = Pm; g.ei = 1; g.ej = m;
+			g.C = Pm; g.ci = 1; g.cj = m;
+			block_gemm(g, ps, qs);
+		}
+		// average over the models that test each row, then the squared error
+		__syncthreads();
+		for (int64_t e = threadIdx.x; e < (int64_t)ntu * n; e += blockDim.x) P[e] = 0.0;
+		for (int mo = 0; mo < gp.models; mo++) {
+			const GridModel md = gp.mdl[mo];
+			const int m = md.te_n;
+			const double *Pm = Pma + mo * mn;
+			const int32_t *tp = gp.tpos + md.te_ofs;
+			__syncthreads();
+			for (int64_t e = threadIdx.x; e < (int64_t)m * n; e += blockDim.x) {
+				const int j = (int)(e / m), i = (int)(e - (int64_t)j * m);
+				const int u = tp[i];
+				P[(int64_t)j * ntu + u] += gp.winv[u] * Pm[e];
+			}
+		}
+		__syncthreads();
+		double s = 0.0;
+		for (int64_t e = threadIdx.x; e < (int64_t)ntu * n; e += blockDim.x) {
+			const double d = Yu[e] - P[e];
+			s += d * d;
+		}
+		s = block_sum256(s, red);
+		if (threadIdx.x == 0) cost[a * gp.n_npcs + p] = s;
+	}
+}
+
+// Winner per searchlight (first minimum of the summed cost, csrc/ha_ridge.c:322-327) and its
+// model-averaged beta, written float64 in the T layout (row-major for CSR output, column-major for
+// CSC), plus the cost row (cost_out may be null) with the untested rows' squared targets added
+// (their prediction is zero, csrc/ha_ridge.c:297-319).
+__global__ void __launch_bounds__(256) k_grid_final(const SlWork *__restrict__ work, const int32_t *__restrict__ sl_idx,
+                                                    const double *__restrict__ Y, double *__restrict__ Gscr,
+                                                    GridParams gp, double *__restrict__ Bout, int t_rowmajor,
+                                                    int32_t *__restrict__ best_out, double *__restrict__ cost_out) {
 	__shared__ double ps[16][65], qs[16][65];
 	__shared__ double cval[kGridMaxN];
 	__shared__ double red[32];
@@ -344,14 +461,8 @@ __global__ void __launch_bounds__(256) k_grid_eval(const SlWork *__restrict__ wo
 	const GridLayout L = grid_layout(gp, n);
 	double *base = Gscr + gp.gbase[w.slot];
 	const int32_t *sl = sl_idx + w.sofs;
-	const int64_t n2 = (int64_t)n * n, mn = (int64_t)gp.mte * n;
-	const int ntu = gp.ntu;
-	double *P = base + L.P, *Yu = base + L.Yu, *cost = base + L.cost;
-	// targets on the tested rows, and the squared targets of the untested rows (zero prediction)
-	for (int64_t e = threadIdx.x; e < (int64_t)ntu * n; e += blockDim.x) {
-		const int j = (int)(e / ntu), u = (int)(e - (int64_t)j * ntu);
-		Yu[e] = Y[(int64_t)sl[j] * gp.nt + gp.urows[u]];
-	}
+	const int64_t n2 = (int64_t)n * n;
+	const double *cost = base + L.cost;
 	double yc = 0.0;
 	for (int64_t e = threadIdx.x; e < (int64_t)gp.n_untested * n; e += blockDim.x) {
 		const int j = (int)(e / gp.n_untested), t = (int)(e - (int64_t)j * gp.n_untested);
@@ -359,62 +470,6 @@ __global__ void __launch_bounds__(256) k_grid_eval(const SlWork *__restrict__ wo
 		yc += y * y;
 	}
 	const double yconst = block_sum256(yc, red);
-	GemmArgs<double, double> g;
-	g.alpha = 1.0;
-	g.beta = 1.0;
-	for (int a = 0; a < gp.n_alphas; a++) {
-		const double al = gp.alphas[a];
-		for (int64_t e = threadIdx.x; e < gp.models * mn; e += blockDim.x) base[L.Pm + e] = 0.0;
-		__syncthreads();
-		for (int p = 0; p < gp.n_npcs; p++) {
-			// Pm += E[:, r0:r1] diag(1 / (alpha + lambda)) Q[r0:r1, :] for every model
-			for (int mo = 0; mo < gp.models; mo++) {
-				const GridModel md = gp.mdl[mo];
-				const int m = md.te_n;
-				int r0, r1;
-				pc_chunk(gp.npcs, p, min(md.tr_n, n), r0, r1);
-				if (r1 <= r0 || m == 0) continue;
-				const double *lam = base + L.Lst + (int64_t)mo * n;
-				__syncthreads();
-				for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x) cval[r] = 1.0 / (al + lam[r]);
-				__syncthreads();
-				const double *E = base + L.Est + mo * mn;
-				const double *Q = base + L.Qst + mo * n2;
-				double *Pm = base + L.Pm + mo * mn;
-				g.M = m; g.N = n; g.K = r1 - r0;
-				g.P = E + (int64_t)r0 * m; g.pk = m; g.pi = 1;
-				g.Q = Q + r0; g.qk = 1; g.qj = n;
-				g.d = cval + r0;
-				g.E = Pm; g.ei = 1; g.ej = m;
-				g.C = Pm; g.ci = 1; g.cj = m;
-				block_gemm(g, ps, qs);
-			}
-			// average over the models that test each row, then the squared error
-			__syncthreads();
-			for (int64_t e = threadIdx.x; e < (int64_t)ntu * n; e += blockDim.x) P[e] = 0.0;
-			for (int mo = 0; mo < gp.models; mo++) {
-				const GridModel md = gp.mdl[mo];
-				const int m = md.te_n;
-				const double *Pm = base + L.Pm + mo * mn;
-				const int32_t *tp = gp.tpos + md.te_ofs;
-				__syncthreads();
-				for (int64_t e = threadIdx.x; e < (int64_t)m * n; e += blockDim.x) {
-					const int j = (int)(e / m), i = (int)(e - (int64_t)j * m);
-					const int u = tp[i];
-					P[(int64_t)j * ntu + u] += gp.winv[u] * Pm[e];
-				}
-			}
-			__syncthreads();
-			double s = 0.0;
-			for (int64_t e = threadIdx.x; e < (int64_t)ntu * n; e += blockDim.x) {
-				const double d = Yu[e] - P[e];
-				s += d * d;
-			}
-			s = block_sum256(s, red);
-			if (threadIdx.x == 0) cost[a * gp.n_npcs + p] = s + yconst;
-		}
-	}
-	__syncthreads();
 	if (threadIdx.x == 0) {
 		int b = 0;
 		for (int gi = 1; gi < grid; gi++)
@@ -424,13 +479,15 @@ __global__ void __launch_bounds__(256) k_grid_eval(const SlWork *__restrict__ wo
 	}
 	__syncthreads();
 	if (cost_out)
-		for (int gi = threadIdx.x; gi < grid; gi += blockDim.x) cost_out[(int64_t)w.s * grid + gi] = cost[gi];
+		for (int gi = threadIdx.x; gi < grid; gi += blockDim.x) cost_out[(int64_t)w.s * grid + gi] = cost[gi] + yconst;
 	// beta of the winner: the cumulative PC chunks up to p of every model, averaged
 	const int ba = best / gp.n_npcs, bp = best % gp.n_npcs;
 	const double al = gp.alphas[ba];
-	double *acc = P;  // n x n accumulator (column-major); the prediction scratch is free now
-	__syncthreads();
+	double *acc = base + L.P(0, gp.models, gp.mte, n);  // n x n accumulator (column-major)
 	for (int64_t e = threadIdx.x; e < n2; e += blockDim.x) acc[e] = 0.0;
+	GemmArgs<double, double> g;
+	g.alpha = 1.0;
+	g.beta = 1.0;
 	for (int mo = 0; mo < gp.models; mo++) {
 		const GridModel md = gp.mdl[mo];
 		const double *V = base + L.Vst + mo * n2;
