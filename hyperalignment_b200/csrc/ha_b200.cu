@@ -145,7 +145,8 @@ void jacobi_layout(int n, bool fp64, int &bsz, int &nblk, size_t &smem, size_t b
 		return;
 	}
 	int b = with_v ? 32 : 64;
-	while (b > 1 && jacobi_smem(b, ld, rb, with_v) > budget) b--;
+	while (b > 2 && jacobi_smem(b, ld, rb, with_v) > budget) b--;
+	b -= b & 1;  // even blocks: the round robin inside one block needs an even column count
 	bsz = b;
 	nblk = (n + b - 1) / b;
 	if (nblk & 1) nblk++;

@@ -215,11 +215,12 @@ __global__ void __launch_bounds__(256) k_xcov(const SlWork *__restrict__ work, c
 // orthonormal basis at the end.
 //
 // Resident mode (nblk == 2): A and V live in shared memory for every sweep.
-// Blocked mode (nblk > 2): A and V stay in the global scratch (L2 resident); a sweep runs
-// the round robin over column blocks, staging two blocks (A and V columns) in shared
-// memory per block pair.  In the first block round every block pair runs a full round robin
-// over its 2*bsz columns (covering the pairs inside each block once), in later block rounds
-// only the cross pairs, so one sweep visits every column pair exactly once.
+// Blocked mode (nblk > 2): A and V stay in the global scratch (L2 resident); a sweep visits
+// the block pairs in row-cyclic order with two staging slots in shared memory (A and V columns),
+// block I in slot 0 for its whole row and block J in slot 1.  Block 0 meets every block first:
+// (0, 1) runs the full round robin over both blocks, (0, J) the round robin inside block J and
+// then the cross pairs, later pairs only the cross pairs, so one sweep visits every column pair
+// exactly once.  Blocks have an even width.
 
 // Pairs processed together by one warp (their reductions overlap), by rows per lane.
 template <int RPL>
@@ -687,36 +688,61 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) k_jacobi(const
 			nb += nb & 1;
 			nb = min(nb, nblk);
 		}
+		// block b of the scratch <-> staging slot (columns slot*bsz ..): each element is moved by the
+		// same thread in both directions, so a slot can be written back and refilled without a barrier
+		auto unstage = [&](int blk, int slot) {
+			for (int e = threadIdx.x; e < bsz * n; e += blockDim.x) {
+				const int c = e / n, i = e - c * n;
+				const int gc = blk * bsz + c, sc = slot * bsz + c;
+				Ag[gc * n + i] = Bs[sc * LD + i];
+				if (Vst) Vg[gc * n + i] = Vs[sc * LD + i];
+			}
+		};
+		auto stage = [&](int blk, int slot) {
+			for (int e = threadIdx.x; e < bsz * n; e += blockDim.x) {
+				const int c = e / n, i = e - c * n;
+				const int gc = blk * bsz + c, sc = slot * bsz + c;
+				Bs[sc * LD + i] = Ag[gc * n + i];
+				if (Vst) Vs[sc * LD + i] = Vg[gc * n + i];
+			}
+		};
+		// Block pairs in row-cyclic order (0,1), (0,2), .., (0,nb-1), (1,2), ..: block I stays staged
+		// while J streams past, so each pair stages one block.  Each block's internal pairs run when
+		// it first meets block 0 (block 0's own with block 1), so a sweep visits every pair once.
 		for (sweep = 0; sweep < prm.max_sweeps; sweep++) {
 			Real mc = 0;
 			bool rot = false;
-			for (int br = 0; br < nb - 1; br++) {
-				for (int k = 0; k < nb / 2; k++) {
-					int I, J;
-					rr_pair(nb, br, k, I, J);
-					for (int e = threadIdx.x; e < 2 * bsz * n; e += blockDim.x) {
-						const int c = e / n, i = e - c * n;
-						const int gc = (c < bsz) ? I * bsz + c : J * bsz + (c - bsz);
-						Bs[c * LD + i] = Ag[gc * n + i];
-						if (Vst) Vs[c * LD + i] = Vg[gc * n + i];
+			for (int I = 0; I < nb - 1; I++) {
+				for (int J = I + 1; J < nb; J++) {
+					if (J == I + 1) {
+						if (I > 0) {
+							unstage(I - 1, 0);
+							unstage(nb - 1, 1);
+						}
+						stage(I, 0);
+					} else {
+						unstage(J - 1, 1);
 					}
+					stage(J, 1);
 					__syncthreads();
 					column_norms<Real, RPL>(Bs, nrm, mst);
 					Real c;
-					if (br == 0)
+					if (I == 0 && J == 1) {
 						c = jacobi_full_rr<Real, RPL>(Bs, Vst, nrm, 2 * bsz, tol, rot);
-					else
-						c = jacobi_cross<Real, RPL>(Bs, Vst, nrm, bsz, tol, rot);
-					mc = c > mc ? c : mc;
-					for (int e = threadIdx.x; e < 2 * bsz * n; e += blockDim.x) {
-						const int cc = e / n, i = e - cc * n;
-						const int gc = (cc < bsz) ? I * bsz + cc : J * bsz + (cc - bsz);
-						Ag[gc * n + i] = Bs[cc * LD + i];
-						if (Vst) Vg[gc * n + i] = Vs[cc * LD + i];
+					} else {
+						c = 0;
+						if (I == 0)
+							c = jacobi_full_rr<Real, RPL>(Bs + bsz * LD, Vst ? Vs + bsz * LD : nullptr, nrm + bsz, bsz,
+							                             tol, rot);
+						const Real c2 = jacobi_cross<Real, RPL>(Bs, Vst, nrm, bsz, tol, rot);
+						c = c2 > c ? c2 : c;
 					}
-					__syncthreads();
+					mc = c > mc ? c : mc;
 				}
 			}
+			unstage(nb - 2, 0);
+			unstage(nb - 1, 1);
+			__syncthreads();
 			mc = block_max_nonneg(mc, red);
 			if (mc <= tol_conv) {
 				converged = true;
