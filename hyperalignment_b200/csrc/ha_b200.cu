@@ -689,6 +689,11 @@ int run_procrustes(HaB200Plan *P, const double *d_X, const double *d_Y, bool ref
 	const int rowmajor = out_kind == kHaB200OutCSR ? 1 : 0;
 	int rc;
 	if (P->chunks.empty() && (rc = build_chunks(P)) != kHaSuccess) return rc;
+	if (solver == kHaB200SolverMixed) {  // float64 temporaries of the re-solve's warm start
+		int64_t maxT = 1;
+		for (auto &ch : P->chunks) maxT = std::max(maxT, ch.t_elems);
+		if ((rc = P->scrT64.ensure((size_t)maxT)) != kHaSuccess) return rc;
+	}
 	if (use32) {
 		if ((rc = P->X32.ensure((size_t)nv * ntp)) != kHaSuccess) return rc;
 		if ((rc = P->Y32.ensure((size_t)nv * ntp)) != kHaSuccess) return rc;
@@ -714,6 +719,8 @@ int run_procrustes(HaB200Plan *P, const double *d_X, const double *d_Y, bool ref
 		jp.ill_ratio = (solver == kHaB200SolverMixed) ? ill_ratio() : 0.0;
 		jp.weak = weak_factor();
 		jp.eig = 0;
+		jp.keep_v = (solver == kHaB200SolverMixed) ? 1 : 0;
+		jp.warm = 0;
 		if (use32) {
 			float *A = reinterpret_cast<float *>(P->scrA.p);
 			float *V = reinterpret_cast<float *>(P->scrV.p);
@@ -737,12 +744,16 @@ int run_procrustes(HaB200Plan *P, const double *d_X, const double *d_Y, bool ref
 			double *A = P->scrA.p, *V = P->scrV.p;
 			const int only = (solver == kHaB200SolverMixed) ? 1 : 0;
 			jp.only_flagged = only;
+			jp.keep_v = 0;
+			jp.warm = only;  // the mixed solver's re-solve starts from the float32 rotations
 			if ((rc = g_fan.begin(st)) != kHaSuccess) return rc;
 			for (size_t bi = 0; bi < ch.b64.size(); bi++) {
 				const Bucket &b = ch.b64[bi];
 				const cudaStream_t bs = g_fan.at((int)bi);
 				const SlWork *wk = ch.d_w64 + b.first;
+				if (only) { HA_LAUNCH(kHaB200KRefine, bs); k_warm_v<<<b.count, kBlock, 0, bs>>>(wk, A, V, P->scrT64.p, P->stats.p); }
 				{ HA_LAUNCH(kHaB200KXcov64, bs); k_xcov<double, 16><<<b.count, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_Y, nt, nt, A, P->stats.p, only); }
+				if (only) { HA_LAUNCH(kHaB200KRefine, bs); k_warm_av<<<b.count, kBlock, 0, bs>>>(wk, A, V, P->scrT64.p, P->stats.p); }
 				{
 					HA_LAUNCH(kHaB200KJacobi64, bs);
 					if ((rc = launch_jacobi<double>(b.rpl, b.count, b.threads, b.smem, bs, wk, A, V, T, P->stats.p, P->uv.p, jp)) != kHaSuccess)
@@ -1020,6 +1031,8 @@ JacobiParams eig_params(bool only_flagged) {
 	jp.weak = weak_factor();
 	jp.eig = 1;
 	jp.only_flagged = only_flagged ? 1 : 0;
+	jp.keep_v = 0;
+	jp.warm = 0;
 	return jp;
 }
 
@@ -2266,6 +2279,8 @@ extern "C" int ha_b200_local_procrustes_noalloc(const double *d_X, const double 
 	jp.weak = 1000.0;
 	jp.eig = 0;
 	jp.only_flagged = 0;
+	jp.keep_v = 0;
+	jp.warm = 0;
 	int64_t tofs = 0;  // packed output offset of the current searchlight
 	int32_t s = 0;
 	while (s < count) {

@@ -604,6 +604,8 @@ struct JacobiParams {
 	int eig;           // eigenvector mode (A A^T = G): no V; write u_c = b_c / sigma_c (column-major, ld n,
 	                   // zero for numerically zero columns) to the V scratch and sigma_c^2 to uvbuf
 	int only_flagged;  // process only searchlights whose stats carry kFlagIllCond (FP64 re-solve)
+	int keep_v;        // write V (column-major, ld n) to the V scratch for searchlights this solve flags
+	int warm;          // start from the rotations V in the V scratch (A already multiplied by V)
 };
 
 template <typename Real, int RPL>
@@ -655,7 +657,8 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) k_jacobi(const
 		for (int e = threadIdx.x; e < mst * LD; e += blockDim.x) {
 			const int c = e / LD, i = e - c * LD;
 			Bs[e] = (c < ncol && i < n) ? Ag[c * n + i] : Real(0);
-			if (!prm.eig) Vs[e] = (c == i && c < n) ? Real(1) : Real(0);
+			if (!prm.eig)
+				Vs[e] = prm.warm ? ((c < n && i < n) ? Vg[c * n + i] : Real(0)) : ((c == i && c < n) ? Real(1) : Real(0));
 		}
 		__syncthreads();
 		for (sweep = 0; sweep < prm.max_sweeps; sweep++) {
@@ -670,7 +673,7 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) k_jacobi(const
 			}
 		}
 	} else {
-		if (!prm.eig)
+		if (!prm.eig && !prm.warm)
 			for (int e = threadIdx.x; e < ncol * n; e += blockDim.x) {
 				const int c = e / n, i = e - c * n;
 				Vg[e] = (c == i) ? Real(1) : Real(0);
@@ -811,6 +814,12 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) k_jacobi(const
 		}
 		__syncthreads();
 	}
+	// keep V of a searchlight handed to the float64 re-solve (its warm start)
+	if (prm.keep_v && resident && (stats[w.slot].flags & kFlagIllCond))
+		for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+			const int c = e / n, i = e - c * n;
+			Vg[e] = Vs[c * LD + i];
+		}
 	// eigenvector mode: A W = B with orthogonal columns, so G = A A^T = B B^T has the eigenvectors
 	// b_c / sigma_c and the eigenvalues sigma_c^2
 	if (prm.eig) {
@@ -908,6 +917,67 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) k_jacobi(const
 		Real (*qs)[65] = ps + 16;
 		block_gemm(g, ps, qs);
 	}
+}
+
+// Warm start of the float64 re-solve of a searchlight the float32 solve flagged, part 1: the
+// float32 rotations V32 (column-major, ld n, in the V scratch, same bytes as the float64 V) become
+// float64 and get one Newton-Schulz step, V = V32 (3I - V32^T V32) / 2, which takes their
+// orthogonality error (~1e-6) to float64 level.  The A scratch and the float64 T scratch are
+// temporaries (A is computed after this).  Padding columns of V are zero.
+__global__ void __launch_bounds__(256) k_warm_v(const SlWork *__restrict__ work, double *__restrict__ Ascr,
+                                                double *__restrict__ Vscr, double *__restrict__ Tmp,
+                                                const SlStats *__restrict__ stats) {
+	__shared__ double ps[16][65], qs[16][65];
+	const SlWork w = work[blockIdx.x];
+	if (!(stats[w.slot].flags & kFlagIllCond)) return;
+	const int n = w.n, ncol = w.nblk * w.bsz;
+	const int64_t n2 = (int64_t)n * n;
+	const float *V32 = reinterpret_cast<const float *>(Vscr + w.aofs);
+	double *W = Ascr + w.aofs;
+	double *G = Tmp + w.tofs;
+	double *V = Vscr + w.aofs;
+	for (int64_t e = threadIdx.x; e < n2; e += blockDim.x) W[e] = (double)V32[e];
+	__syncthreads();
+	GemmArgs<double, double> g;
+	g.d = nullptr; g.E = nullptr; g.ei = 0; g.ej = 0; g.beta = 0.0;
+	// G = -W^T W / 2, then + 3I/2
+	g.M = n; g.N = n; g.K = n; g.alpha = -0.5;
+	g.P = W; g.pk = 1; g.pi = n;
+	g.Q = W; g.qk = 1; g.qj = n;
+	g.C = G; g.ci = 1; g.cj = n;
+	block_gemm(g, ps, qs);
+	for (int i = threadIdx.x; i < n; i += blockDim.x) G[(int64_t)i * n + i] += 1.5;
+	__syncthreads();
+	// V = W G
+	g.alpha = 1.0;
+	g.P = W; g.pk = n; g.pi = 1;
+	g.Q = G; g.qk = 1; g.qj = n;
+	g.C = V; g.ci = 1; g.cj = n;
+	block_gemm(g, ps, qs);
+	for (int64_t e = n2 + threadIdx.x; e < (int64_t)n * ncol; e += blockDim.x) V[e] = 0.0;
+}
+
+// Part 2, after the float64 cross-covariance: A := A V (through the float64 T scratch), so the
+// rotations continue from the float32 solution and most pairs are already orthogonal.
+__global__ void __launch_bounds__(256) k_warm_av(const SlWork *__restrict__ work, double *__restrict__ Ascr,
+                                                 const double *__restrict__ Vscr, double *__restrict__ Tmp,
+                                                 const SlStats *__restrict__ stats) {
+	__shared__ double ps[16][65], qs[16][65];
+	const SlWork w = work[blockIdx.x];
+	if (!(stats[w.slot].flags & kFlagIllCond)) return;
+	const int n = w.n;
+	const int64_t n2 = (int64_t)n * n;
+	double *A = Ascr + w.aofs;
+	const double *V = Vscr + w.aofs;
+	double *Tm = Tmp + w.tofs;
+	GemmArgs<double, double> g;
+	g.d = nullptr; g.E = nullptr; g.ei = 0; g.ej = 0; g.beta = 0.0; g.alpha = 1.0;
+	g.M = n; g.N = n; g.K = n;
+	g.P = A; g.pk = n; g.pi = 1;
+	g.Q = V; g.qk = 1; g.qj = n;
+	g.C = Tm; g.ci = 1; g.cj = n;
+	block_gemm(g, ps, qs);
+	for (int64_t e = threadIdx.x; e < n2; e += blockDim.x) A[e] = Tm[e];
 }
 
 // Blocked-mode T formation: T = U V^T with U, V in global scratch (one CTA per searchlight).
