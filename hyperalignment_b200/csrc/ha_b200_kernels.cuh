@@ -709,6 +709,16 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) k_jacobi(const
 				if (Vst) Vs[sc * LD + i] = Vg[gc * n + i];
 			}
 		};
+		// pull the next block to be staged (A and V columns) towards L2 while the current pair rotates
+		auto prefetch = [&](int blk) {
+			const int lines = bsz * n * (int)sizeof(Real) / 128;  // every prefetched address inside the block
+			const char *a = reinterpret_cast<const char *>(Ag + blk * bsz * n);
+			const char *v = reinterpret_cast<const char *>(Vg + blk * bsz * n);
+			for (int l = threadIdx.x; l < lines; l += blockDim.x) {
+				asm volatile("prefetch.global.L2 [%0];" ::"l"(a + 128 * l));
+				if (Vst) asm volatile("prefetch.global.L2 [%0];" ::"l"(v + 128 * l));
+			}
+		};
 		// Block pairs in row-cyclic order (0,1), (0,2), .., (0,nb-1), (1,2), ..: block I stays staged
 		// while J streams past, so each pair stages one block.  Each block's internal pairs run when
 		// it first meets block 0 (block 0's own with block 1), so a sweep visits every pair once.
@@ -727,6 +737,10 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) k_jacobi(const
 						unstage(J - 1, 1);
 					}
 					stage(J, 1);
+					if (J + 1 < nb)
+						prefetch(J + 1);
+					else if (I + 2 < nb)
+						prefetch(I + 2);
 					__syncthreads();
 					column_norms<Real, RPL>(Bs, nrm, mst);
 					Real c;
