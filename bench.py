@@ -147,6 +147,21 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def max_over_ranks(value, ws, device=None):
+    """The largest per-rank value over all ranks (the job's time); the value itself on one rank."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(ws, units_per_rank, steps, seconds):
+    """Whole-job rate of N replicas, each processing units_per_rank per step (weak scaling)."""
+    return ws * units_per_rank * steps / seconds
+
+
 def dist_setup(args):
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -299,21 +314,19 @@ def run_b200(args):
             lib.ha_b200_kernel_times(ms.ctypes.data_as(L.c_double_p), cnt.ctypes.data_as(L.c_int64_p))
             kt = (ms, cnt)
         clocks = sampler.stop() if sampler else None
-        dev_ms = float(sum(a.elapsed_time(b) for a, b in evs))
-        t = torch.tensor([dev_ms], dtype=torch.float64, device=dev)
+        dev_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in evs), ws, dev)
         if ws > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
             dist.barrier()
-        return float(t.item()), wall, launches, kt, clocks
+        return dev_ms, wall, launches, kt, clocks
 
     K = args.steps
     total_ms, wall, launches, kt, clocks = timed_loop(L.SOLVER_MIXED, K, sample_clocks=True, trace=True)
-    value = ws * w.sls.count * K / (total_ms / 1e3)
+    value = aggregate_rate(ws, w.sls.count, K, total_ms / 1e3)
     plain_ms, _, _, _, _ = timed_loop(L.SOLVER_FP32, K)
-    plain_value = ws * w.sls.count * K / (plain_ms / 1e3)
+    plain_value = aggregate_rate(ws, w.sls.count, K, plain_ms / 1e3)
     plain_stats = plan.stats()
     fp64_ms, _, _, _, _ = timed_loop(L.SOLVER_FP64, max(1, K // 4))
-    fp64_value = ws * w.sls.count * max(1, K // 4) / (fp64_ms / 1e3)
+    fp64_value = aggregate_rate(ws, w.sls.count, max(1, K // 4), fp64_ms / 1e3)
     fp64_stats = plan.stats()
     step(L.SOLVER_MIXED)
     torch.cuda.synchronize()
@@ -406,10 +419,8 @@ def run_b200(args):
             t0 = time.perf_counter()
             L.check(lib.ha_searchlight_procrustes_dense(*argsv), "dense")
             ts.append(time.perf_counter() - t0)
-        tmax = torch.tensor([sum(ts)], dtype=torch.float64, device=dev)
-        if ws > 1:
-            dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        e2e = {"value": ws * s.count * K / float(tmax.item()), "unit": UNIT,
+        tmax = max_over_ranks(sum(ts), ws, dev)
+        e2e = {"value": aggregate_rate(ws, s.count, K, tmax), "unit": UNIT,
                "h2d_bytes_per_step": int(2 * w.nt * w.nv * 8), "d2h_bytes_per_step": int(plan.nnz * 8),
                "path": "ha_searchlight_procrustes_dense(backend=4) host float64 in, host dense nv x nv out (+=)"}
 
