@@ -669,6 +669,20 @@ double ill_ratio() {
 	return r;
 }
 
+// Early stop of the float32 solves: a sweep whose largest |cos| is at most this is the last
+// (HA_B200_STOP_COS overrides the default 1e-2; 0 turns it off).  Measured in float32 on template
+// searchlights: the sweep after one with |cos| <= 1e-2 only confirms convergence (its largest |cos|
+// is ~1e-6), and stopping without it leaves the per-T error unchanged.
+double fp32_stop_cos() {
+	static double r = -1.0;
+	if (r < 0.0) {
+		const char *e = getenv("HA_B200_STOP_COS");
+		r = e ? atof(e) : 1e-2;
+		if (!(r >= 0.0)) r = 1e-2;
+	}
+	return r;
+}
+
 // Weak-column factor of k_jacobi (HA_B200_WEAK_FACTOR overrides the default).
 double weak_factor() {
 	static double r = -1.0;
@@ -721,6 +735,7 @@ int run_procrustes(HaB200Plan *P, const double *d_X, const double *d_Y, bool ref
 		jp.eig = 0;
 		jp.keep_v = (solver == kHaB200SolverMixed) ? 1 : 0;
 		jp.warm = 0;
+		jp.stop_cos = fp32_stop_cos();
 		if (use32) {
 			float *A = reinterpret_cast<float *>(P->scrA.p);
 			float *V = reinterpret_cast<float *>(P->scrV.p);
@@ -746,6 +761,7 @@ int run_procrustes(HaB200Plan *P, const double *d_X, const double *d_Y, bool ref
 			jp.only_flagged = only;
 			jp.keep_v = 0;
 			jp.warm = only;  // the mixed solver's re-solve starts from the float32 rotations
+			jp.stop_cos = 0.0;
 			if ((rc = g_fan.begin(st)) != kHaSuccess) return rc;
 			for (size_t bi = 0; bi < ch.b64.size(); bi++) {
 				const Bucket &b = ch.b64[bi];
@@ -1033,6 +1049,7 @@ JacobiParams eig_params(bool only_flagged) {
 	jp.only_flagged = only_flagged ? 1 : 0;
 	jp.keep_v = 0;
 	jp.warm = 0;
+	jp.stop_cos = 0.0;
 	return jp;
 }
 
@@ -2281,6 +2298,7 @@ extern "C" int ha_b200_local_procrustes_noalloc(const double *d_X, const double 
 	jp.only_flagged = 0;
 	jp.keep_v = 0;
 	jp.warm = 0;
+	jp.stop_cos = 0.0;
 	int64_t tofs = 0;  // packed output offset of the current searchlight
 	int32_t s = 0;
 	while (s < count) {

@@ -606,6 +606,7 @@ struct JacobiParams {
 	int only_flagged;  // process only searchlights whose stats carry kFlagIllCond (FP64 re-solve)
 	int keep_v;        // write V (column-major, ld n) to the V scratch for searchlights this solve flags
 	int warm;          // start from the rotations V in the V scratch (A already multiplied by V)
+	double stop_cos;   // also stop after a sweep whose largest |cos| is at most this (0: off)
 };
 
 template <typename Real, int RPL>
@@ -649,7 +650,9 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) k_jacobi(const
 	JacobiTol<Real> tol;
 	tol.rot = eps * sqn;
 	tol.zero2 = (Real)(frob2 * (double)(eps * sqn) * (double)(eps * sqn));
-	const Real tol_conv = Real(4) * eps * sqn;
+	// Rotations converge quadratically: a sweep that starts with every |cos| below stop_cos leaves the
+	// columns orthogonal to working precision, so the sweep that would only confirm it is skipped.
+	const Real tol_conv = fmax(Real(4) * eps * sqn, (Real)prm.stop_cos);
 
 	bool converged = false;
 	int sweep = 0;
