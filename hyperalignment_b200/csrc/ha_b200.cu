@@ -683,6 +683,18 @@ double fp32_stop_cos() {
 	return r;
 }
 
+// The same for the float64 solves (HA_B200_STOP_COS64 overrides the default 1e-8): measured in
+// float64, the sweep after one with |cos| <= 1e-6 changes T by less than 1e-14.
+double fp64_stop_cos() {
+	static double r = -1.0;
+	if (r < 0.0) {
+		const char *e = getenv("HA_B200_STOP_COS64");
+		r = e ? atof(e) : 1e-8;
+		if (!(r >= 0.0)) r = 1e-8;
+	}
+	return r;
+}
+
 // Weak-column factor of k_jacobi (HA_B200_WEAK_FACTOR overrides the default).
 double weak_factor() {
 	static double r = -1.0;
@@ -761,7 +773,7 @@ int run_procrustes(HaB200Plan *P, const double *d_X, const double *d_Y, bool ref
 			jp.only_flagged = only;
 			jp.keep_v = 0;
 			jp.warm = only;  // the mixed solver's re-solve starts from the float32 rotations
-			jp.stop_cos = 0.0;
+			jp.stop_cos = fp64_stop_cos();
 			if ((rc = g_fan.begin(st)) != kHaSuccess) return rc;
 			for (size_t bi = 0; bi < ch.b64.size(); bi++) {
 				const Bucket &b = ch.b64[bi];
@@ -1049,7 +1061,7 @@ JacobiParams eig_params(bool only_flagged) {
 	jp.only_flagged = only_flagged ? 1 : 0;
 	jp.keep_v = 0;
 	jp.warm = 0;
-	jp.stop_cos = 0.0;
+	jp.stop_cos = fp64_stop_cos();
 	return jp;
 }
 
