@@ -229,7 +229,7 @@ int launch_jacobi(int rpl, int grid, int threads, size_t smem, cudaStream_t st, 
                   float *T, SlStats *stats, double *uv, JacobiParams jp) {
 	switch (rpl) {
 #define HA_RPL_CASE(R) \
-	case R: k_jacobi<Real, R><<<grid, threads, smem, st>>>(wk, A, V, T, stats, uv, jp); break;
+	case R: k_jacobi<Real, R><<<grid, std::min(threads, JacobiBounds<Real, R>::threads), smem, st>>>(wk, A, V, T, stats, uv, jp); break;
 		HA_RPL_CASE(1) HA_RPL_CASE(2) HA_RPL_CASE(3) HA_RPL_CASE(4) HA_RPL_CASE(5)
 		HA_RPL_CASE(6) HA_RPL_CASE(8) HA_RPL_CASE(10) HA_RPL_CASE(12) HA_RPL_CASE(16)
 #undef HA_RPL_CASE

@@ -222,10 +222,18 @@ __global__ void __launch_bounds__(256) k_xcov(const SlWork *__restrict__ work, c
 // then the cross pairs, later pairs only the cross pairs, so one sweep visits every column pair
 // exactly once.  Blocks have an even width.
 
-// Pairs processed together by one warp (their reductions overlap), by rows per lane.
-template <int RPL>
+// Pairs processed together by one warp (their reductions overlap), by rows per lane.  The float
+// instance with 10 rows per lane runs at most 384 threads (its blocked buckets use 10 warps),
+// which leaves the registers for two pairs per warp without spills.
+template <typename Real, int RPL>
 struct PairsPerWarp {
-	static constexpr int value = RPL <= 4 ? 4 : (RPL <= 8 ? 2 : 1);
+	static constexpr int value = RPL <= 4 ? 4 : ((RPL <= 8 || (sizeof(Real) == 4 && RPL == 10)) ? 2 : 1);
+};
+
+template <typename Real, int RPL>
+struct JacobiBounds {
+	static constexpr int threads = (sizeof(Real) == 4 && RPL == 10) ? 384 : 512;
+	static constexpr int blocks = sizeof(Real) == 4 ? 2 : 1;
 };
 
 // circle method: pair k of round r among m players (m even); no integer division
@@ -339,7 +347,7 @@ __device__ __forceinline__ Real pair_sums(const Real (&g)[JPW], int lane) {
 template <typename Real, int RPL>
 __device__ __forceinline__ Real jacobi_pairs(Real *B, Real *V, Real *nrm, const int *p, const int *q,
                                              const JacobiTol<Real> &tol, int lane, bool &rotated) {
-	constexpr int JPW = PairsPerWarp<RPL>::value;
+	constexpr int JPW = PairsPerWarp<Real, RPL>::value;
 	constexpr int LD = 32 * RPL;
 	constexpr int GRP = 32 / JPW;  // lanes per pair group
 	using LR = LaneRows<Real, RPL>;
@@ -434,7 +442,7 @@ __device__ __forceinline__ void column_norms(const Real *B, Real *nrm, int m) {
 template <typename Real, int RPL>
 __device__ __forceinline__ Real jacobi_full_rr(Real *B, Real *V, Real *nrm, int m, const JacobiTol<Real> &tol,
                                                bool &rotated) {
-	constexpr int JPW = PairsPerWarp<RPL>::value;
+	constexpr int JPW = PairsPerWarp<Real, RPL>::value;
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
 	Real mc = 0;
 	const int npairs = m / 2;
@@ -463,7 +471,7 @@ __device__ __forceinline__ Real jacobi_full_rr(Real *B, Real *V, Real *nrm, int 
 template <typename Real, int RPL>
 __device__ __forceinline__ Real jacobi_cross(Real *B, Real *V, Real *nrm, int h, const JacobiTol<Real> &tol,
                                              bool &rotated) {
-	constexpr int JPW = PairsPerWarp<RPL>::value;
+	constexpr int JPW = PairsPerWarp<Real, RPL>::value;
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
 	Real mc = 0;
 	for (int r = 0; r < h; r++) {
@@ -610,7 +618,7 @@ struct JacobiParams {
 };
 
 template <typename Real, int RPL>
-__global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) k_jacobi(const SlWork *__restrict__ work, Real *__restrict__ Ascr,
+__global__ void __launch_bounds__(JacobiBounds<Real, RPL>::threads, JacobiBounds<Real, RPL>::blocks) k_jacobi(const SlWork *__restrict__ work, Real *__restrict__ Ascr,
                                                    Real *__restrict__ Vscr, float *__restrict__ Tscr,
                                                    SlStats *__restrict__ stats, double *__restrict__ uvbuf,
                                                    JacobiParams prm) {
