@@ -223,8 +223,8 @@ __global__ void __launch_bounds__(256) k_xcov(const SlWork *__restrict__ work, c
 // exactly once.  Blocks have an even width.
 
 // Pairs processed together by one warp (their reductions overlap), by rows per lane.  The float
-// instance with 10 rows per lane runs at most 384 threads (its blocked buckets use 10 warps),
-// which leaves the registers for two pairs per warp without spills.
+// instances with 8 and 10 rows per lane run at most 384 threads (their blocked buckets use 12 and
+// 10 warps), which leaves 80 registers a thread: no spills, and two pairs per warp at 10 rows.
 template <typename Real, int RPL>
 struct PairsPerWarp {
 	static constexpr int value = RPL <= 4 ? 4 : ((RPL <= 8 || (sizeof(Real) == 4 && RPL == 10)) ? 2 : 1);
@@ -232,7 +232,7 @@ struct PairsPerWarp {
 
 template <typename Real, int RPL>
 struct JacobiBounds {
-	static constexpr int threads = (sizeof(Real) == 4 && RPL == 10) ? 384 : 512;
+	static constexpr int threads = (sizeof(Real) == 4 && (RPL == 8 || RPL == 10)) ? 384 : 512;
 	static constexpr int blocks = sizeof(Real) == 4 ? 2 : 1;
 };
 
