@@ -62,6 +62,8 @@ def parse_args():
                    help="template: the headline Procrustes step; grid: the searchlight ridge grid search "
                         "(40962 vertices, every --grid-step-th searchlight); learned: the learned proposal")
     p.add_argument("--grid-step", type=int, default=16)
+    p.add_argument("--ref-seconds", type=float, default=0.0,
+                   help="reference arm: seconds of CPU work per step (default: 150 s over all steps)")
     return p.parse_args()
 
 
@@ -222,7 +224,7 @@ def run_reference(args):
         return
     w = workload(0, args.nv, args.nt)
     threads = os.cpu_count() or 1
-    budget = max(2.0, 150.0 / max(1, args.steps + args.warmup))
+    budget = args.ref_seconds if args.ref_seconds > 0 else max(2.0, 150.0 / max(1, args.steps + args.warmup))
     rates, times, counts = [], [], []
     start = 0
     for i in range(args.warmup + args.steps):
