@@ -266,3 +266,58 @@ def test_mlp_oracle_gradient_vs_finite_differences():
         assert abs(fd - g[k]) <= 1e-7 + 1e-5 * abs(g[k]), (k, fd, g[k])
     assert np.isclose(loss, np.mean(np.log(np.exp(O.mlp_forward(params, C, X)).sum(1))
                                     - O.mlp_forward(params, C, X)[np.arange(9), y]))
+
+
+# ---------------------------------------------------------------------------------------------
+# the restatement against the compiled reference on fresh seeds (skipped when it is not built)
+# ---------------------------------------------------------------------------------------------
+
+def _ref():
+    from oracle import ref_lib as R
+    if not R.available():
+        pytest.skip("compiled reference not built (make -C oracle)")
+    return R
+
+
+@pytest.mark.parametrize("refl,scal,weighted", [(True, False, True), (False, False, True), (True, True, False),
+                                               (False, True, True)])
+def test_dense_procrustes_vs_live_reference(refl, scal, weighted):
+    R = _ref()
+    from hyperalignment_b200 import workloads as W
+    w = W.small_case(seed=41, nv=162, nt=50, lo=6, hi=30)
+    s = w.sls
+    d = s.dists if weighted else None
+    a = O.searchlight_procrustes_dense(w.X, w.Y, s.indices, s.offsets, d, s.radius, refl, scal)
+    b = R.procrustes_dense(w.X, w.Y, s.indices, s.offsets, d, s.radius, refl, scal, 0, threads=1)
+    np.testing.assert_allclose(a, b, atol=1e-10, rtol=0)
+
+
+@pytest.mark.parametrize("alpha", [1e-3, 1.0, 100.0])
+def test_sparse_procrustes_and_ridge_vs_live_reference(alpha):
+    R = _ref()
+    from hyperalignment_b200 import workloads as W
+    w = W.small_case(seed=43, nv=162, nt=40, lo=6, hi=24)
+    s = w.sls
+    indptr, indices = O.sparse_init(s.indices, s.offsets, w.nv)
+    ri, rj = R.sparse_init(s.indices, s.offsets, w.nv)
+    np.testing.assert_array_equal(indptr, ri)
+    np.testing.assert_array_equal(indices, rj)
+    wts = O.searchlight_weights(s.indices, s.offsets, s.dists, s.radius, w.nv)
+    np.testing.assert_array_equal(wts, R.searchlight_weights(s.indices, s.offsets, s.dists, s.radius))
+    a = O.searchlight_ridge_csc(w.X, w.Y, s.indices, s.offsets, indptr, indices, np.zeros(indices.size), alpha, wts)
+    b = R.searchlight_ridge_csc(w.X, w.Y, s.indices, s.offsets, indptr, indices, alpha, wts, threads=1)
+    np.testing.assert_allclose(a, b, atol=1e-10 * max(1.0, np.abs(b).max()), rtol=0)
+    a = O.searchlight_procrustes_csc(w.X, w.Y, s.indices, s.offsets, indptr, indices, np.zeros(indices.size), wts,
+                                     True, False)
+    b = R.searchlight_procrustes_csc(w.X, w.Y, s.indices, s.offsets, indptr, indices, wts, True, False, threads=1)
+    np.testing.assert_allclose(a, b, atol=1e-10, rtol=0)
+
+
+@pytest.mark.parametrize("args", [(300, 3, 4, 8, 0, 11), (97, 2, 3, 5, 2, 0), (64, 1, 2, 16, 4, 123456789)])
+def test_ensemble_indices_vs_live_reference(args):
+    R = _ref()
+    tr, te = O.ensemble_indices(*args)
+    rtr, rte = R.ensemble_indices(*args)
+    assert len(tr) == len(rtr)
+    for a, b in zip(tr + te, rtr + rte):
+        np.testing.assert_array_equal(a, b)
