@@ -143,3 +143,18 @@ def test_ridge_grid_argument_errors(hlib):
             L.dptr(data), L.dptr(al), al.size, L.iptr(pc), pc.size, trl.ptrs, tel.ptrs, L.iptr(trl.sizes),
             L.iptr(tel.sizes), 1, L.iptr(best), None, True)
         assert rc == L.ERROR_ARG
+
+
+def test_mlp_parameter_count_and_argument_errors(hlib):
+    # 65 -> 128 -> 128 -> C with biases; C outside 1..64 is rejected
+    for C in (1, 40, 64):
+        assert hlib.ha_b200_mlp_param_count(C) == 65 * 128 + 128 + 128 * 128 + 128 + 128 * C + C
+    assert hlib.ha_b200_mlp_param_count(0) == -1 and hlib.ha_b200_mlp_param_count(65) == -1
+    # checked before any device work: missing buffers, empty sets, non-positive learning rate
+    buf = ctypes.c_void_p(1)
+    assert hlib.ha_b200_mlp_train(None, 40, buf, buf, 10, 1, 8, 1e-3, 0, None) == L.ERROR_ARG
+    assert hlib.ha_b200_mlp_train(buf, 40, buf, buf, 0, 1, 8, 1e-3, 0, None) == L.ERROR_ARG
+    assert hlib.ha_b200_mlp_train(buf, 40, buf, buf, 10, 1, 8, 0.0, 0, None) == L.ERROR_ARG
+    assert hlib.ha_b200_mlp_grad(buf, 40, buf, buf, 0, buf, None) == L.ERROR_ARG
+    assert hlib.ha_b200_mlp_infer(buf, 40, buf, -1, buf, buf, None) == L.ERROR_ARG
+    assert hlib.ha_b200_mlp_init(None, 40, 0) == L.ERROR_ARG
