@@ -58,9 +58,10 @@ def parse_args():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
-    p.add_argument("--workload", choices=["template", "grid", "learned"], default="template",
+    p.add_argument("--workload", choices=["template", "grid", "learned", "rankdef"], default="template",
                    help="template: the headline Procrustes step; grid: the searchlight ridge grid search "
-                        "(40962 vertices, every --grid-step-th searchlight); learned: the learned proposal")
+                        "(40962 vertices, every --grid-step-th searchlight); learned: the learned proposal; "
+                        "rankdef: the mixed form on the template pair with duplicated columns")
     p.add_argument("--grid-step", type=int, default=16)
     p.add_argument("--ref-seconds", type=float, default=0.0,
                    help="reference arm: seconds of CPU work per step (default: 150 s over all steps)")
@@ -648,6 +649,108 @@ def run_learned(args):
         print(json.dumps(out))
 
 
+# ---------------------------------------------------------------------------------------------
+# rank-deficient template pair: about 10% of searchlights hold a duplicated vertex column
+# ---------------------------------------------------------------------------------------------
+
+def range_part(T, A, rel=1e-9):
+    """T restricted to the row space of A, the part of the polar factor that A determines."""
+    _, sv, Vt = np.linalg.svd(A)
+    Vp = Vt[sv > sv[0] * rel].T
+    return T @ Vp @ Vp.T
+
+
+def rankdef_errors(w, singular, sample, Ts, fp64_flags):
+    """Per-T relative Frobenius error vs the float64 oracle, split into singular searchlights (T
+    judged on the row space of A) and regular ones, and by whether the searchlight went to FP64."""
+    from oracle import ha_oracle as O
+    groups = {"singular": [], "regular": [], "fp64": [], "fp32": []}
+    for j, q in enumerate(sample):
+        sl = w.sls.indices[w.sls.offsets[q]:w.sls.offsets[q + 1]]
+        Xs, Ys = w.X[:, sl], w.Y[:, sl]
+        Tref = O.procrustes(Xs, Ys, True, False)
+        if singular[q]:
+            A = Xs.T @ Ys
+            a, b = range_part(Ts[j], A), range_part(Tref, A)
+        else:
+            a, b = Ts[j], Tref
+        e = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+        groups["singular" if singular[q] else "regular"].append(e)
+        groups["fp64" if fp64_flags[j] else "fp32"].append(e)
+    return {k: ({"T_relfrob_max": float(np.max(v)), "T_relfrob_median": float(np.median(v)), "count": len(v)}
+                if v else {"count": 0}) for k, v in groups.items()}
+
+
+def run_rankdef(args):
+    import torch
+    from hyperalignment_b200 import _lib as L
+    from hyperalignment_b200 import workloads as W
+    from hyperalignment_b200.plan import Plan
+
+    ws, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    lib = L.lib()
+    L.check(lib.ha_b200_init(), "ha_b200_init")
+    w = W.rank_deficient_pair(rank, nv=args.nv, nt=args.nt)
+    singular = w.extra["singular"]
+    plan = Plan.from_workload(w)
+    dev = torch.device("cuda", local)
+    dX = torch.from_numpy(np.asfortranarray(w.X).ravel(order="F")).to(dev)
+    dY = torch.from_numpy(np.asfortranarray(w.Y).ravel(order="F")).to(dev)
+    vals = torch.zeros(plan.nnz, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        plan.procrustes_device(dX.data_ptr(), dY.data_ptr(), vals.data_ptr(), True, True, L.SOLVER_MIXED,
+                               L.OUT_CSR, stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.5)
+    evs = []
+    for _ in range(args.steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        step()
+        b.record(stream)
+        evs.append((a, b))
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    total_ms = float(sum(a.elapsed_time(b) for a, b in evs))
+    stats = plan.stats()
+    rng = np.random.default_rng(7)
+    sing = np.flatnonzero(singular)
+    reg = np.flatnonzero(~singular)
+    sample = np.sort(np.concatenate([rng.choice(sing, size=min(24, sing.size), replace=False),
+                                     rng.choice(reg, size=min(24, reg.size), replace=False)]))
+    sub = w.sls.subset(sample)
+    splan = Plan(w.nt, w.nv, sub.indices, sub.offsets, sub.dists, sub.radius)
+    svals = torch.zeros(splan.nnz, dtype=torch.float64, device=dev)
+    splan.procrustes_device(dX.data_ptr(), dY.data_ptr(), svals.data_ptr(), True, True, L.SOLVER_MIXED,
+                            L.OUT_CSR, stream.cuda_stream)
+    torch.cuda.synchronize()
+    Ts = splan.local_transforms(0, sub.count)
+    fp64 = (splan.searchlight_stats(0, sub.count)["flags"] & 8) != 0
+    errs = rankdef_errors(w, singular, sample, Ts, fp64)
+    if rank == 0:
+        sizes = w.sls.sizes
+        print(json.dumps({
+            "metric": "searchlight solves/sec, mixed form, rank-deficient searchlights",
+            "value": w.sls.count * args.steps / (total_ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "rank_deficient_template_pair", "nv": w.nv, "nt": w.nt,
+                       "searchlights": w.sls.count, "singular_searchlights": int(singular.sum()),
+                       "sl_size_min": int(sizes.min()), "sl_size_max": int(sizes.max()),
+                       "l2": "flushed between steps (256 MiB write)"},
+            "solver_stats": stats, "error_vs_fp64": errs, "clocks": clocks}))
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -656,6 +759,8 @@ def main():
         run_grid(args)
     elif args.workload == "learned":
         run_learned(args)
+    elif args.workload == "rankdef":
+        run_rankdef(args)
     else:
         run_b200(args)
 

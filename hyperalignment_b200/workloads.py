@@ -239,10 +239,11 @@ def ridge_grid_pair(seed: int = 0, nv: int = 40962, nt: int = 500, size_lo: int 
 
 
 def duplicate_columns(X: np.ndarray, sls: Searchlights, frac: float, rng) -> np.ndarray:
-    """Copy a neighbour's column into a searchlight member for about ``frac`` of searchlights.
+    """Copy one member's column onto another in about ``frac * count / 4`` random searchlights.
 
-    Makes the chosen searchlights' cross-covariance exactly rank-deficient.
-    Returns the boolean mask of searchlights that contain a duplicated pair.
+    Every searchlight that holds both vertices of a copied pair becomes exactly rank-deficient;
+    with overlapping searchlights that is usually far more than ``frac`` of them (see
+    duplicate_columns_to_fraction for a set fraction).  Returns the mask of those searchlights.
     """
     nv = X.shape[1]
     dup_of = -np.ones(nv, dtype=np.int64)
@@ -265,12 +266,44 @@ def duplicate_columns(X: np.ndarray, sls: Searchlights, frac: float, rng) -> np.
     return mask
 
 
+def duplicate_columns_to_fraction(X: np.ndarray, sls: Searchlights, frac: float, rng) -> np.ndarray:
+    """Copy columns pair by pair until about ``frac`` of the searchlights are rank-deficient.
+
+    Each step picks a not yet singular searchlight and two of its members that are in no earlier
+    pair, copies one column onto the other, and marks every searchlight holding both.  Returns
+    the exact mask of singular searchlights.
+    """
+    nv = X.shape[1]
+    order = np.argsort(sls.indices, kind="stable")
+    owner = np.repeat(np.arange(sls.count), np.diff(sls.offsets))[order]
+    starts = np.searchsorted(sls.indices[order], np.arange(nv + 1))
+    members = [owner[starts[v]:starts[v + 1]] for v in range(nv)]  # searchlights holding v
+    mask = np.zeros(sls.count, dtype=bool)
+    used = np.zeros(nv, dtype=bool)
+    target = frac * sls.count
+    for _ in range(20 * sls.count):
+        if mask.sum() >= target:
+            break
+        s = int(rng.integers(sls.count))
+        if mask[s]:
+            continue
+        sl = sls.indices[sls.offsets[s]:sls.offsets[s + 1]]
+        a, b = rng.choice(sl.size, size=2, replace=False)
+        v1, v2 = int(sl[a]), int(sl[b])
+        if used[v1] or used[v2]:
+            continue
+        X[:, v2] = X[:, v1]
+        used[v1] = used[v2] = True
+        mask[np.intersect1d(members[v1], members[v2])] = True
+    return mask
+
+
 def rank_deficient_pair(seed: int = 0, nv: int = 10242, nt: int = 400, frac: float = 0.10) -> Workload:
     """Template pair with duplicated vertex columns so about ``frac`` of searchlights are singular."""
     w = template_procrustes_pair(seed, nv=nv, nt=nt)
     rng = np.random.default_rng(seed + 1000)
     X = w.X.copy()
-    mask = duplicate_columns(X, w.sls, frac, rng)
+    mask = duplicate_columns_to_fraction(X, w.sls, frac, rng)
     return Workload("rank_deficient", X, w.Y, w.sls, True, True, {"singular": mask})
 
 
