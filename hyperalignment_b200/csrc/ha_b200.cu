@@ -1384,9 +1384,26 @@ int host_threads() {
 	return std::max(1, t);
 }
 
-// Cached plan for the host entry points (geometry + weights identify it).
+// Cached plan for the host entry points (geometry + weights identify it). The hash only
+// screens; a hit is confirmed against the full key, so a collision rebuilds instead of reusing.
 HaB200Plan *g_cached_plan = nullptr;
 uint64_t g_cached_key = 0;
+int g_cached_mode = 0;
+double g_cached_radius = 0.0;
+std::vector<double> g_cached_aux;  // the dists or weights the cached plan was built from
+
+bool cached_plan_matches(int32_t nt, int32_t nv, const int32_t *idx, const int32_t *off, int32_t count,
+                         double radius, int mode, const double *aux) {
+	const HaB200Plan *P = g_cached_plan;
+	if (P->nt != nt || P->nv != nv || P->count != count || g_cached_mode != mode) return false;
+	if (std::memcmp(&g_cached_radius, &radius, sizeof(radius)) != 0) return false;
+	if (std::memcmp(P->h_off.data(), off, ((size_t)count + 1) * 4) != 0) return false;
+	if (std::memcmp(P->h_idx.data(), idx, (size_t)off[count] * 4) != 0) return false;
+	if (aux && (g_cached_aux.size() != (size_t)off[count] ||
+	            std::memcmp(g_cached_aux.data(), aux, (size_t)off[count] * 8) != 0))
+		return false;
+	return true;
+}
 
 int get_plan(int32_t nt, int32_t nv, const int32_t *idx, const int32_t *off, const double *dists, int32_t count,
              double radius, const double *weights, bool unweighted, HaB200Plan **out) {
@@ -1402,7 +1419,9 @@ int get_plan(int32_t nt, int32_t nv, const int32_t *idx, const int32_t *off, con
 	h = fnv1a(&mode, sizeof(mode), h);
 	if (dists) h = fnv1a(dists, (size_t)off[count] * 8, h);
 	if (weights) h = fnv1a(weights, (size_t)off[count] * 8, h);
-	if (g_cached_plan && g_cached_key == h) {
+	const double *aux = weights ? weights : dists;  // weights override dists in plan_create_impl
+	if (g_cached_plan && g_cached_key == h &&
+	    cached_plan_matches(nt, nv, idx, off, count, radius, mode, aux)) {
 		*out = g_cached_plan;
 		return kHaSuccess;
 	}
@@ -1414,6 +1433,10 @@ int get_plan(int32_t nt, int32_t nv, const int32_t *idx, const int32_t *off, con
 	if (rc != kHaSuccess) return rc;
 	g_cached_plan = *out;
 	g_cached_key = h;
+	g_cached_mode = mode;
+	g_cached_radius = radius;
+	if (aux) g_cached_aux.assign(aux, aux + off[count]);
+	else g_cached_aux.clear();
 	return kHaSuccess;
 }
 
@@ -1680,6 +1703,7 @@ void ha_b200_cleanup(void) {
 		ha_b200_plan_destroy(g_cached_plan);
 		g_cached_plan = nullptr;
 	}
+	std::vector<double>().swap(g_cached_aux);
 	g_bufs.release();
 	g_fan.release();
 	g_mlp.release();
