@@ -58,10 +58,11 @@ def parse_args():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
-    p.add_argument("--workload", choices=["template", "grid", "learned", "rankdef"], default="template",
+    p.add_argument("--workload", choices=["template", "grid", "learned", "rankdef", "shard"], default="template",
                    help="template: the headline Procrustes step; grid: the searchlight ridge grid search "
                         "(40962 vertices, every --grid-step-th searchlight); learned: the learned proposal; "
-                        "rankdef: the mixed form on the template pair with duplicated columns")
+                        "rankdef: the mixed form on the template pair with duplicated columns; shard: one "
+                        "hemisphere split over the N GPUs (strong scaling)")
     p.add_argument("--grid-step", type=int, default=16)
     p.add_argument("--ref-seconds", type=float, default=0.0,
                    help="reference arm: seconds of CPU work per step (default: 150 s over all steps)")
@@ -751,6 +752,136 @@ def run_rankdef(args):
             "solver_stats": stats, "error_vs_fp64": errs, "clocks": clocks}))
 
 
+# ---------------------------------------------------------------------------------------------
+# one hemisphere sharded over the ranks (strong scaling)
+# ---------------------------------------------------------------------------------------------
+
+def run_shard(args):
+    """The template pair's hemisphere (seed 0 on every rank) split over the N ranks: contiguous
+    searchlight ranges balanced by n^3, one all-to-all of partial CSC values per step to the
+    column owners. value = searchlights of the hemisphere x steps / max over ranks of the device
+    time (solve + exchange)."""
+    import torch
+    import torch.distributed as dist
+    from hyperalignment_b200 import _lib as L
+    from hyperalignment_b200.plan import Plan
+    from hyperalignment_b200.shard import ShardedSearchlights
+
+    ws, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    lib = L.lib()
+    L.check(lib.ha_b200_init(), "ha_b200_init")
+    w = workload(0, args.nv, args.nt)
+    s = w.sls
+    dev = torch.device("cuda", local)
+    sh = ShardedSearchlights(w.nt, w.nv, s.indices, s.offsets, s.dists, s.radius)
+    hX = torch.from_numpy(np.asfortranarray(w.X).ravel(order="F")).pin_memory()
+    hY = torch.from_numpy(np.asfortranarray(w.Y).ravel(order="F")).pin_memory()
+    dX, dY = hX.to(dev), hY.to(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        return sh.procrustes(dX, dY, True, True, L.SOLVER_MIXED)
+
+    for _ in range(args.warmup):
+        owned = step()
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.5)
+    n0 = lib.ha_b200_launch_count()
+    torch.cuda.synchronize()
+    evs = []
+    for _ in range(args.steps):
+        flush.zero_()
+        a, m, b = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        a.record(stream)
+        sh.partial.zero_()
+        if sh.plan is not None:
+            sh.plan.procrustes_device(dX.data_ptr(), dY.data_ptr(), sh.partial.data_ptr(), True, True,
+                                      L.SOLVER_MIXED, L.OUT_CSC, stream.cuda_stream)
+        m.record(stream)
+        owned = sh.exchange.combine(sh.partial)
+        b.record(stream)
+        evs.append((a, m, b))
+    torch.cuda.synchronize()
+    launches = lib.ha_b200_launch_count() - n0
+    clocks = sampler.stop()
+    K = args.steps
+    job_ms = max_over_ranks(sum(a.elapsed_time(b) for a, _, b in evs), ws, dev)
+    solve_ms = max_over_ranks(sum(a.elapsed_time(m) for a, m, _ in evs), ws, dev)
+    exch_ms = max_over_ranks(sum(m.elapsed_time(b) for _, m, b in evs), ws, dev)
+    value = s.count * K / (job_ms / 1e3)
+
+    # end to end: every step copies X and Y from pinned host memory and the owned values back
+    hout = torch.empty(owned.numel(), dtype=torch.float64).pin_memory()
+    for _ in range(args.warmup):
+        dX.copy_(hX, non_blocking=True)
+        dY.copy_(hY, non_blocking=True)
+        hout.copy_(step(), non_blocking=True)
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    ee = []
+    for _ in range(K):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        dX.copy_(hX, non_blocking=True)
+        dY.copy_(hY, non_blocking=True)
+        hout.copy_(step(), non_blocking=True)
+        b.record(stream)
+        ee.append((a, b))
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in ee), ws, dev)
+
+    # the sharded result against one plan of the whole hemisphere on rank 0
+    full = sh.exchange.assemble(owned, dst=0)
+    check = None
+    if rank == 0:
+        one = Plan.from_workload(w)
+        ref = torch.zeros(one.nnz, dtype=torch.float64, device=dev)
+        one.procrustes_device(dX.data_ptr(), dY.data_ptr(), ref.data_ptr(), True, True, L.SOLVER_MIXED, L.OUT_CSC,
+                              stream.cuda_stream)
+        torch.cuda.synchronize()
+        indptr, rows = one.pattern()
+        refv = ref.cpu().numpy()
+        same = bool(np.array_equal(full[0], indptr) and np.array_equal(full[1], rows))
+        check = {"pattern_identical": same,
+                 "values_relfrob": float(np.linalg.norm(full[2] - refv) / np.linalg.norm(refv)) if same else None}
+        one.close()
+    if rank == 0:
+        lo, hi = sh.col_range
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": args.warmup,
+            "ms_per_step": job_ms / K, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": config_dict(w, {"workload": "hemisphere_template_pair_sharded",
+                                      "parallelism": f"one hemisphere over {ws} GPU(s): contiguous searchlight "
+                                                     "ranges balanced by n^3, column owners, one all-to-all of "
+                                                     "partial CSC values per step"}),
+            "solve_ms_per_step": solve_ms / K, "exchange_ms_per_step": exch_ms / K,
+            "searchlights_rank0": int(sh.bounds[1] - sh.bounds[0]), "columns_rank0": [int(lo), int(hi)],
+            "vs_one_plan": check,
+            "e2e": {"value": s.count * K / (e2e_ms / 1e3), "unit": UNIT,
+                    "h2d_bytes_per_step": int(2 * w.nt * w.nv * 8), "d2h_bytes_per_step": int(owned.numel() * 8),
+                    "path": "ShardedSearchlights.procrustes with X, Y copied from pinned host memory and the "
+                            "owned CSC values copied back every step (rank 0's bytes)"},
+            "roofline": None, "cpu_baseline": None,
+            "gpu_launches": int(launches), "clocks": clocks,
+        }
+        print(json.dumps(out))
+    sh.close()
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -761,6 +892,8 @@ def main():
         run_learned(args)
     elif args.workload == "rankdef":
         run_rankdef(args)
+    elif args.workload == "shard":
+        run_shard(args)
     else:
         run_b200(args)
 

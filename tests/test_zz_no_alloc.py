@@ -6,8 +6,8 @@ in their loop) pass their own device buffers and the library uses only a static 
 Its output must match the allocating plan API's plain FP32 local transforms on the same inputs,
 within the per-transform tolerance of the parity tests, on two calls in a row (the shared scratch
 keeps the previous call's contents).  The inputs have more samples than any searchlight has
-vertices, so every transform is unique and two correct solvers agree.  The file sorts last so
-that a run stopping at the first failure has run every other test first.
+vertices, so every transform is unique and two correct solvers agree.  The file sorts after the
+parity tests so that a run stopping at the first failure has run them first.
 """
 
 import ctypes
