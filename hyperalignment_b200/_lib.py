@@ -99,10 +99,13 @@ SIGNATURES = {
     "ha_b200_set_kernel_timing": (None, [ctypes.c_bool]),
     "ha_b200_kernel_times": (ctypes.c_int, [c_double_p, c_int64_p]),
     "ha_b200_launch_count": (ctypes.c_int64, []),
+    "ha_b200_aligned_correlation_device": (ctypes.c_int, [
+        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+        ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
 }
 
 KERNEL_KINDS = ["convert", "colvar", "xcov32", "jacobi32", "formT32", "xcov64", "jacobi64", "formT64", "refine",
-                "reflect", "scale", "reduce", "pattern", "ridge", "grid", "mlp"]
+                "reflect", "scale", "reduce", "pattern", "ridge", "grid", "mlp", "eval"]
 
 # Error codes and enum values (include/hyperalignment_b200.h, same as the reference's ha_common.h).
 SUCCESS, ERROR_ALLOC, ERROR_SVD, ERROR_ARG, ERROR_INTERNAL = 0, -1, -2, -3, -4

@@ -1926,6 +1926,29 @@ int ha_b200_plan_ridge_device(HaB200Plan *P, const double *d_X, const double *d_
 	return run_ridge(P, d_X, d_Y, alpha, out_kind, d_values, (cudaStream_t)stream);
 }
 
+int ha_b200_aligned_correlation_device(const double *d_X, const double *d_Y, int32_t nt, int32_t nv,
+                                       const int64_t *d_indptr, const int32_t *d_indices, const double *d_values,
+                                       int64_t nnz, double *d_r, double *d_aligned, void *stream) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	if (!d_X || !d_Y || !d_r || nt < 1 || nv < 1) return kHaErrorArg;
+	if (d_values && (!d_indptr || !d_indices || nnz < 0)) return kHaErrorArg;
+	int rc = check_cuda_ready();
+	if (rc != kHaSuccess) return rc;
+	cudaStream_t st = (cudaStream_t)stream;
+	constexpr int kWarps = 8;  // columns per CTA, one warp each
+	const unsigned blocks = (unsigned)(((int64_t)nv + kWarps - 1) / kWarps);
+	{
+		HA_LAUNCH(kHaB200KEval, st);
+		k_aligned_corr<<<blocks, kWarps * 32, 0, st>>>(d_X, d_Y, nt, nv, d_indptr, d_indices, d_values, nnz, d_r,
+		                                                d_aligned);
+	}
+	if (cudaGetLastError() != cudaSuccess) {
+		fprintf(stderr, "ha_b200_aligned_correlation_device: launch failed\n");
+		return kHaErrorInternal;
+	}
+	return kHaSuccess;
+}
+
 void ha_b200_set_kernel_timing(bool on) {
 	std::lock_guard<std::recursive_mutex> lk(g_mu);
 	g_timing = on;

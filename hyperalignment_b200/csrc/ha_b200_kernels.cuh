@@ -1430,6 +1430,67 @@ __global__ void k_spmm_csc(const double *__restrict__ X, int nt, int nv, const i
 	}
 }
 
+// Vertex-wise correlation of A with Y, the evaluation of benchmark_neuroboros.py:204-211 (mean
+// over time of zscore(A)[:, c] * zscore(Y)[:, c] with population statistics), where A = X @ W for W
+// in CSC form (ptr, row, vals) or A = X when vals is null. One warp per column c, lanes over time,
+// two passes: the means, then the centred sums, r = sum(da dy) / sqrt(sum(da^2) sum(dy^2)). A column
+// with zero variance gives 0 / 0 = NaN, as the z-score does. Pattern entries are checked before use:
+// a column whose range lies outside [0, nnz] or decreases, or holds a row outside [0, nv), gets NaN
+// and reads nothing. aligned (may be null) receives A; pass 2 reads it back instead of recomputing.
+__global__ void k_aligned_corr(const double *__restrict__ X, const double *__restrict__ Y, int nt, int nv,
+                               const int64_t *__restrict__ ptr, const int32_t *__restrict__ row,
+                               const double *__restrict__ vals, int64_t nnz, double *__restrict__ r,
+                               double *__restrict__ aligned) {
+	const int lane = threadIdx.x & 31;
+	const int64_t c = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+	if (c >= nv) return;  // whole warps leave together: c is the same for every lane of a warp
+	const int64_t off = c * (int64_t)nt;
+	int64_t k0 = 0, k1 = 0;
+	if (vals) {
+		k0 = ptr[c];
+		k1 = ptr[c + 1];
+		int ok = (k0 >= 0 && k1 >= k0 && k1 <= nnz) ? 1 : 0;
+		if (ok)
+			for (int64_t k = k0 + lane; k < k1; k += 32) ok &= (row[k] >= 0 && row[k] < nv) ? 1 : 0;
+		if (!__all_sync(0xffffffffu, ok)) {
+			const double nan = __longlong_as_double(0x7ff8000000000000LL);
+			if (lane == 0) r[c] = nan;
+			if (aligned)
+				for (int t = lane; t < nt; t += 32) aligned[off + t] = nan;
+			return;
+		}
+	}
+	auto value = [&](int t) -> double {
+		if (!vals) return X[off + t];
+		double acc = 0.0;
+		for (int64_t k = k0; k < k1; k++) acc = fma(vals[k], X[(int64_t)row[k] * nt + t], acc);
+		return acc;
+	};
+	const double *y = Y + off;
+	double sa = 0.0, sy = 0.0;
+	for (int t = lane; t < nt; t += 32) {
+		const double a = value(t);
+		if (aligned) aligned[off + t] = a;
+		sa += a;
+		sy += y[t];
+	}
+	sa = warp_sum(sa);
+	sy = warp_sum(sy);
+	const double ma = sa / nt, my = sy / nt;
+	double saa = 0.0, syy = 0.0, say = 0.0;
+	for (int t = lane; t < nt; t += 32) {
+		const double da = (aligned ? aligned[off + t] : value(t)) - ma;  // written by this lane in pass 1
+		const double dy = y[t] - my;
+		saa = fma(da, da, saa);
+		syy = fma(dy, dy, syy);
+		say = fma(da, dy, say);
+	}
+	saa = warp_sum(saa);
+	syy = warp_sum(syy);
+	say = warp_sum(say);
+	if (lane == 0) r[c] = say / sqrt(saa * syy);
+}
+
 // One-pass column z-score of csrc/ha_linalg.c:263-291 (population variance from E[x^2] - m^2,
 // var < 1e-30 -> the column becomes 0), float64, one thread per column summing in time order.
 __global__ void k_zscore_cols(double *__restrict__ X, int nt, int nv) {

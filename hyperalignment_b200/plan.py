@@ -87,6 +87,21 @@ class Plan:
             L.iptr(te.sizes), len(tr), out_kind, ctypes.c_void_p(d_values), ctypes.c_void_p(d_choice),
             ctypes.c_void_p(d_prob), ctypes.c_void_p(stream)), "ha_b200_plan_ridge_learned_device")
 
+    def aligned_correlation_device(self, d_X: int, d_Y: int, d_values: int, d_r: int, d_aligned: int = 0,
+                                   nt: int | None = None, stream: int = 0):
+        """Vertex-wise correlation of X @ W with Y (W: this plan's pattern with d_values in CSC order,
+        as a kHaB200OutCSC run leaves them; d_values 0 correlates X itself) into d_r (nv float64).
+        X and Y (nt x nv, column-major) may be other time points than the plan's, e.g. held-out
+        ones: nt defaults to the plan's."""
+        ptr, idx = ctypes.c_void_p(), ctypes.c_void_p()
+        L.check(self.lib.ha_b200_plan_device_pattern(self.handle, ctypes.byref(ptr), ctypes.byref(idx)),
+                "ha_b200_plan_device_pattern")
+        L.check(self.lib.ha_b200_aligned_correlation_device(
+            ctypes.c_void_p(d_X), ctypes.c_void_p(d_Y), int(self.nt if nt is None else nt), self.nv, ptr, idx,
+            ctypes.c_void_p(d_values or None),
+            self.nnz, ctypes.c_void_p(d_r), ctypes.c_void_p(d_aligned or None), ctypes.c_void_p(stream)),
+            "ha_b200_aligned_correlation_device")
+
     def stats(self):
         a, b = ctypes.c_int32(), ctypes.c_int32()
         L.check(self.lib.ha_b200_plan_stats(self.handle, ctypes.byref(a), ctypes.byref(b)), "ha_b200_plan_stats")

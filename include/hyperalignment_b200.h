@@ -385,6 +385,25 @@ int ha_b200_plan_ridge_learned_device(
 	const int32_t *train_sizes, const int32_t *test_sizes, int32_t n_models,
 	int out_kind, double *d_values, int32_t *d_choice, float *d_prob, void *stream);
 
+/* ---- evaluation ---- */
+
+/*
+ * Vertex-wise correlation of aligned data with a target: the evaluation step of the reference's
+ * benchmark (benchmark_neuroboros.py:204-211, the mean over time of zscore(A) * zscore(Y) per
+ * vertex with scipy's population z-score; benchmark_neuroboros.py:229-232 forms A = X @ W).
+ * A = X @ W for W in CSC form (d_indptr: nv + 1 int64, d_indices: nnz int32 rows, d_values: nnz
+ * float64, e.g. a plan's device pattern and the values of a kHaB200OutCSC run), or A = X when
+ * d_values is NULL (the unaligned correlation).  d_X, d_Y: nt x nv float64 column-major DEVICE
+ * memory.  d_r: nv float64 DEVICE memory, overwritten; a column with zero variance gives NaN, as
+ * the z-score does, and so does a column whose pattern entries are out of range (indptr outside
+ * [0, nnz] or decreasing, a row outside [0, nv)).  d_aligned (nt x nv float64 DEVICE, may be NULL)
+ * receives A.  Returns after enqueueing on stream (a cudaStream_t, or NULL).
+ */
+int ha_b200_aligned_correlation_device(
+	const double *d_X, const double *d_Y, int32_t nt, int32_t nv,
+	const int64_t *d_indptr, const int32_t *d_indices, const double *d_values, int64_t nnz,
+	double *d_r, double *d_aligned, void *stream);
+
 /* ---- tracing ---- */
 
 /* Kernel kinds reported by ha_b200_kernel_times. */
@@ -405,7 +424,8 @@ enum {
 	kHaB200KRidge = 13,     /* ridge solves, pivoted Cholesky factors of the grid */
 	kHaB200KGrid = 14,      /* ridge grid: per-model products and grid evaluation */
 	kHaB200KMlp = 15,       /* learned proposal: training and inference */
-	kHaB200NumKernelKinds = 16,
+	kHaB200KEval = 16,      /* vertex-wise correlation of aligned data with a target */
+	kHaB200NumKernelKinds = 17,
 };
 
 /*

@@ -463,6 +463,18 @@ def mlp_loss_grad(params, C, X, y):
 # z-score (csrc/ha_linalg.c:263-291)
 # ---------------------------------------------------------------------------------------------
 
+def aligned_correlation(X, Y, W=None):
+    """Vertex-wise correlation of A = X @ W (A = X when W is None) with Y, the evaluation of
+    benchmark_neuroboros.py:204-211 (np.mean(zscore(A, axis=0) * zscore(Y, axis=0), axis=0), scipy's
+    population z-score; benchmark_neuroboros.py:229-232 forms X @ W). W: dense or scipy sparse."""
+    import warnings
+    from scipy.stats import zscore
+    A = X if W is None else np.asarray(X @ W)
+    with warnings.catch_warnings(), np.errstate(invalid="ignore", divide="ignore"):
+        warnings.simplefilter("ignore", RuntimeWarning)  # a constant column: 0 / 0, NaN as in the reference
+        return np.mean(zscore(A, axis=0) * zscore(Y, axis=0), axis=0)
+
+
 def zscore_columns(X):
     """One-pass population z-score, var < 1e-30 -> 0 (csrc/ha_linalg.c:263-291)."""
     M = X.shape[0]

@@ -158,3 +158,16 @@ def test_mlp_parameter_count_and_argument_errors(hlib):
     assert hlib.ha_b200_mlp_grad(buf, 40, buf, buf, 0, buf, None) == L.ERROR_ARG
     assert hlib.ha_b200_mlp_infer(buf, 40, buf, -1, buf, buf, None) == L.ERROR_ARG
     assert hlib.ha_b200_mlp_init(None, 40, 0) == L.ERROR_ARG
+
+
+def test_aligned_correlation_argument_errors(hlib):
+    # checked on the host before any device work; the non-null pointers here are never read
+    f = hlib.ha_b200_aligned_correlation_device
+    p = 4096
+    assert f(None, p, 10, 4, None, None, None, 0, p, None, None) == L.ERROR_ARG   # no X
+    assert f(p, p, 10, 4, None, None, None, 0, None, None, None) == L.ERROR_ARG   # no output
+    assert f(p, p, 0, 4, None, None, None, 0, p, None, None) == L.ERROR_ARG       # nt < 1
+    assert f(p, p, 10, 0, None, None, None, 0, p, None, None) == L.ERROR_ARG      # nv < 1
+    assert f(p, p, 10, 4, None, p, p, 8, p, None, None) == L.ERROR_ARG            # values without indptr
+    assert f(p, p, 10, 4, p, None, p, 8, p, None, None) == L.ERROR_ARG            # values without rows
+    assert f(p, p, 10, 4, p, p, p, -1, p, None, None) == L.ERROR_ARG              # negative nnz

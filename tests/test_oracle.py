@@ -321,3 +321,22 @@ def test_ensemble_indices_vs_live_reference(args):
     assert len(tr) == len(rtr)
     for a, b in zip(tr + te, rtr + rte):
         np.testing.assert_array_equal(a, b)
+
+
+def test_aligned_correlation_restatement():
+    """The evaluation of benchmark_neuroboros.py:204-211 against per-column Pearson correlation,
+    with X @ W for a sparse W, and NaN for a constant column (scipy's z-score divides 0 by 0)."""
+    import scipy.sparse as sp
+    rng = np.random.default_rng(4)
+    X = rng.standard_normal((50, 12))
+    Y = rng.standard_normal((50, 12))
+    W = sp.random(12, 12, density=0.4, random_state=5, format="csc") + sp.identity(12, format="csc")
+    A = np.asarray(X @ W)
+    r = O.aligned_correlation(X, Y, W)
+    want = np.array([np.corrcoef(A[:, j], Y[:, j])[0, 1] for j in range(12)])
+    np.testing.assert_allclose(r, want, rtol=0, atol=1e-12)
+    np.testing.assert_allclose(O.aligned_correlation(X, Y), [np.corrcoef(X[:, j], Y[:, j])[0, 1] for j in range(12)],
+                               rtol=0, atol=1e-12)
+    Y[:, 3] = 2.5
+    r = O.aligned_correlation(X, Y, W)
+    assert np.isnan(r[3]) and np.isfinite(np.delete(r, 3)).all()
