@@ -475,6 +475,39 @@ def aligned_correlation(X, Y, W=None):
         return np.mean(zscore(A, axis=0) * zscore(Y, axis=0), axis=0)
 
 
+def searchlight_pca_template(dms, idx, off, dists, radius):
+    """Searchlight PCA template, src/hyperalignment/searchlight.py:215-236 with
+    compute_template(kind="pca", max_npc=n, common_topography=True, demean=False)
+    (src/hyperalignment/local_template.py:224-248, :72-78, :11-53).
+
+    Per searchlight: X = [dms_1[:, sl], ..., dms_ns[:, sl]] (nt x ns*n); the local template is
+    U_k S_k / sqrt(ns) for the top k = min(n, nt, ns*n) singular pairs of X; it is rotated by the
+    Procrustes of the stacked template onto the stacked subjects, whose cross product is
+    tmpl^T sum_s dms_s[:, sl] (src/hyperalignment/procrustes.py, reflection allowed, no scaling);
+    the rotated template is added into the columns sl with the searchlight weights.
+
+    The reference takes the top singular pairs from scikit-learn's randomized_svd (Halko,
+    Martinsson and Tropp 2011; random_state=0, 4 or 7 power iterations, 10 oversamples). This
+    restatement takes them from an exact SVD: the two agree where the top-k singular subspace is
+    separated from the rest (pinned on such inputs); without a gap the reference's result depends
+    on its random draws.
+    """
+    ns = len(dms)
+    nt, nv = dms[0].shape
+    w = searchlight_weights(idx, off, dists, radius, nv)
+    tpl = np.zeros((nt, nv))
+    for s in range(len(off) - 1):
+        sl = np.asarray(idx[off[s]:off[s + 1]])
+        X = np.hstack([d[:, sl] for d in dms])
+        k = min(sl.size, nt, X.shape[1])
+        U, sv, _ = np.linalg.svd(X, full_matrices=False)
+        tmpl = U[:, :k] * (sv[:k] / np.sqrt(ns))
+        M = np.sum([d[:, sl] for d in dms], axis=0)
+        Ua, _, Vta = np.linalg.svd(tmpl.T @ M, full_matrices=False)
+        tpl[:, sl] += (tmpl @ (Ua @ Vta)) * w[off[s]:off[s + 1]][np.newaxis]
+    return tpl
+
+
 def zscore_columns(X):
     """One-pass population z-score, var < 1e-30 -> 0 (csrc/ha_linalg.c:263-291)."""
     M = X.shape[0]

@@ -19,6 +19,11 @@ self-contained):
                     outputs on seeded inputs
   python_ref.npz    the Python reference package (src/hyperalignment) on the same small
                     case: procrustes per searchlight and initialize_sparse_matrix
+  pca_template.npz  searchlight_template(tpl_kind="pca") of the Python reference package on
+                    four subjects sharing one latent time series plus 1% noise, so that every
+                    searchlight's top singular subspace is separated from the rest
+
+    python tests/golden/make_golden.py [name ...]   # only the named fixtures (file stems)
 """
 
 from __future__ import annotations
@@ -175,14 +180,29 @@ def make_python_ref():
                         indptr=mat.indptr.astype(np.int32), indices=mat.indices.astype(np.int32))
 
 
+def make_pca_template():
+    sys.path.insert(0, os.path.join(REF_DIR, "src"))
+    from hyperalignment.searchlight import searchlight_template  # noqa: E402
+    rng = np.random.default_rng(1)
+    pts = W.fibonacci_sphere(162)
+    sls = W.searchlights_knn(pts, rng.integers(8, 25, size=162))
+    L = rng.standard_normal((60, 162))
+    dms = np.stack([L + 0.01 * rng.standard_normal((60, 162)) for _ in range(4)])
+    sl_list, d_list = sls.as_lists()
+    tpl = searchlight_template(dms, sl_list, d_list, sls.radius, tpl_kind="pca")
+    np.savez_compressed(os.path.join(HERE, "pca_template.npz"), dms=dms, idx=sls.indices, off=sls.offsets,
+                        dists=sls.dists, radius=np.float64(sls.radius), template=tpl)
+
+
+MAKERS = {"small_dense": make_small_dense, "small_sparse": make_small_sparse, "kat": make_kat, "grid": make_grid,
+          "python_ref": make_python_ref, "pca_template": make_pca_template}
+
 if __name__ == "__main__":
-    if not R.available():
+    names = sys.argv[1:] or list(MAKERS)
+    if any(n in ("small_dense", "small_sparse", "kat", "grid") for n in names) and not R.available():
         raise SystemExit("build the reference first: make -C oracle")
-    make_small_dense()
-    make_small_sparse()
-    make_kat()
-    make_grid()
-    make_python_ref()
+    for n in names:
+        MAKERS[n]()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -340,3 +340,12 @@ def test_aligned_correlation_restatement():
     Y[:, 3] = 2.5
     r = O.aligned_correlation(X, Y, W)
     assert np.isnan(r[3]) and np.isfinite(np.delete(r, 3)).all()
+
+
+def test_pca_template_restatement_vs_python_reference():
+    """searchlight_template(tpl_kind="pca") of the Python reference on subjects whose searchlights
+    have a separated top singular subspace: the exact-SVD restatement agrees with the reference's
+    randomized SVD there (the fixture is made by tests/golden/make_golden.py)."""
+    g = golden("pca_template.npz")
+    tpl = O.searchlight_pca_template(list(g["dms"]), g["idx"], g["off"], g["dists"], float(g["radius"]))
+    assert np.linalg.norm(tpl - g["template"]) <= 1e-12 * np.linalg.norm(g["template"])
