@@ -663,7 +663,7 @@ def range_part(T, A, rel=1e-9):
 
 def rankdef_errors(w, singular, sample, Ts, fp64_flags):
     """Per-T relative Frobenius error vs the float64 oracle, split into singular searchlights (T
-    judged on the row space of A) and regular ones, and by whether the searchlight went to FP64."""
+    compared on the row space of A) and regular ones, and by whether the searchlight went to FP64."""
     from oracle import ha_oracle as O
     groups = {"singular": [], "regular": [], "fp64": [], "fp32": []}
     for j, q in enumerate(sample):
