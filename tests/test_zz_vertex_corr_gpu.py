@@ -36,8 +36,8 @@ def test_vertex_correlation_matches_oracle(gpu):
     nte = Xte.shape[0]
     plan = Plan(n_fit, w.nv, s.indices, s.offsets, s.dists, s.radius)
     vals = torch.zeros(plan.nnz, dtype=torch.float64, device="cuda")
-    plan.procrustes_device(_dev(Xtr).data_ptr(), _dev(Ytr).data_ptr(), vals.data_ptr(), True, True,
-                           L.SOLVER_MIXED, L.OUT_CSC)
+    dXtr, dYtr = _dev(Xtr), _dev(Ytr)  # held: the library reads them after the call returns
+    plan.procrustes_device(dXtr.data_ptr(), dYtr.data_ptr(), vals.data_ptr(), True, True, L.SOLVER_MIXED, L.OUT_CSC)
     torch.cuda.synchronize()
     indptr, rows = plan.pattern()
     Wm = sp.csc_matrix((vals.cpu().numpy(), rows, indptr), shape=(w.nv, w.nv))
@@ -67,11 +67,15 @@ def test_vertex_correlation_matches_oracle(gpu):
     torch.cuda.synchronize()
     assert np.abs(r0.cpu().numpy() - O.aligned_correlation(Xte, Yte)).max() <= ATOL
 
+    # the fit is real: alignment raises the mean correlation on the held-out time points
+    assert float(r.mean()) > float(r0.mean()) + 0.05
+
     # a constant target column: NaN, as scipy's z-score gives
     Yc = Yte.copy()
     Yc[:, 5] = 1.5
     rc = torch.zeros_like(r)
-    plan.aligned_correlation_device(dXte.data_ptr(), _dev(Yc).data_ptr(), vals.data_ptr(), rc.data_ptr(), nt=nte)
+    dYc = _dev(Yc)
+    plan.aligned_correlation_device(dXte.data_ptr(), dYc.data_ptr(), vals.data_ptr(), rc.data_ptr(), nt=nte)
     torch.cuda.synchronize()
     got = rc.cpu().numpy()
     want = O.aligned_correlation(Xte, Yc, Wm)
