@@ -854,6 +854,25 @@ def run_shard(args):
         same = bool(np.array_equal(full[0], indptr) and np.array_equal(full[1], rows))
         check = {"pattern_identical": same,
                  "values_relfrob": float(np.linalg.norm(full[2] - refv) / np.linalg.norm(refv)) if same else None}
+        # the evaluation step on the same data: A = X @ W and its per-vertex correlation with Y
+        r = torch.empty(w.nv, dtype=torch.float64, device=dev)
+        A = torch.empty(w.nt * w.nv, dtype=torch.float64, device=dev)
+        for _ in range(2):
+            one.aligned_correlation_device(dX.data_ptr(), dY.data_ptr(), ref.data_ptr(), r.data_ptr(), A.data_ptr(),
+                                           stream=stream.cuda_stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(K):
+            one.aligned_correlation_device(dX.data_ptr(), dY.data_ptr(), ref.data_ptr(), r.data_ptr(), A.data_ptr(),
+                                           stream=stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ev_ms = e0.elapsed_time(e1) / K
+        evaluation = {"kernel": "k_aligned_corr", "ms": ev_ms, "nnz": int(one.nnz), "mean_r": float(r.mean()),
+                      "gflops": 2.0 * one.nnz * w.nt / (ev_ms / 1e3) / 1e9,
+                      "hbm_gbs_min_bytes": 4.0 * w.nt * w.nv * 8 / (ev_ms / 1e3) / 1e9,
+                      "note": "X in L2 between steps (no flush); min bytes = X, Y once, A written and read"}
+        check["evaluation"] = evaluation
         one.close()
     if rank == 0:
         lo, hi = sh.col_range
