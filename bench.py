@@ -434,9 +434,12 @@ def run_b200(args):
         if R.available():
             threads = os.cpu_count() or 1
             r, m, dt = reference_rate(w, args.cpu_seconds, threads)
+            r1, m1, dt1 = reference_rate(w, min(5.0, args.cpu_seconds / 3.0), 1)
             cpu = {"value": r, "unit": UNIT, "cores": threads, "kind": "reference",
                    "sample": f"{m} contiguous searchlights of {w.sls.count} ({dt:.1f} s), reference cpu64 arm, "
-                             f"OpenMP {threads} threads, OPENBLAS_NUM_THREADS=1"}
+                             f"OpenMP {threads} threads, OPENBLAS_NUM_THREADS=1",
+                   "single_thread": {"value": r1, "unit": UNIT, "cores": 1,
+                                     "sample": f"{m1} contiguous searchlights ({dt1:.1f} s), one OpenMP thread"}}
         else:
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                    "sample": "oracle/_ref/libhyperalignment.so not built"}
