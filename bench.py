@@ -177,8 +177,9 @@ def dist_setup(args):
 # reference CPU arm
 # ---------------------------------------------------------------------------------------------
 
-def reference_rate(w, seconds, threads, start=0):
-    """Reference cpu64 dense entry point on a contiguous sample of searchlights sized to ~seconds."""
+def reference_rate(w, seconds, threads, start=0, backend=0):
+    """Reference dense entry point (backend 0 = cpu64, 1 = cpu32) on a contiguous sample of
+    searchlights sized to ~seconds."""
     from oracle import ref_lib as R
     R.set_threads(threads)
     s = w.sls
@@ -186,14 +187,14 @@ def reference_rate(w, seconds, threads, start=0):
     probe = s.subset(np.arange(start, min(start + 4 * threads, s.count)))
     Xf, Yf = np.asfortranarray(w.X), np.asfortranarray(w.Y)
     t0 = time.perf_counter()
-    _ref_call(R, Xf, Yf, probe)
+    _ref_call(R, Xf, Yf, probe, backend)
     dt = time.perf_counter() - t0
     rate = probe.count / max(dt, 1e-6)
     m = int(min(s.count, max(threads, rate * seconds)))
     idx = (start + np.arange(m)) % s.count
     sample = s.subset(idx)
     t0 = time.perf_counter()
-    _ref_call(R, Xf, Yf, sample)
+    _ref_call(R, Xf, Yf, sample, backend)
     dt = time.perf_counter() - t0
     return sample.count / dt, sample.count, dt
 
@@ -201,7 +202,7 @@ def reference_rate(w, seconds, threads, start=0):
 _REF_T = {}
 
 
-def _ref_call(R, Xf, Yf, sls):
+def _ref_call(R, Xf, Yf, sls, backend=0):
     h = R.lib()
     nt, nv = Xf.shape
     T = _REF_T.get(nv)
@@ -211,7 +212,7 @@ def _ref_call(R, Xf, Yf, sls):
         Xf.ctypes.data_as(R.c_double_p), Yf.ctypes.data_as(R.c_double_p), nt, nv,
         sls.indices.ctypes.data_as(R.c_int32_p), sls.offsets.ctypes.data_as(R.c_int32_p),
         sls.dists.ctypes.data_as(R.c_double_p), sls.count, sls.radius, T.ctypes.data_as(R.c_double_p),
-        True, True, 0, True)
+        True, True, backend, True)
     if rc != 0:
         raise RuntimeError(f"reference rc={rc}")
 
@@ -435,11 +436,15 @@ def run_b200(args):
             threads = os.cpu_count() or 1
             r, m, dt = reference_rate(w, args.cpu_seconds, threads)
             r1, m1, dt1 = reference_rate(w, min(5.0, args.cpu_seconds / 3.0), 1)
+            r32, m32, dt32 = reference_rate(w, min(5.0, args.cpu_seconds / 3.0), threads, backend=1)
             cpu = {"value": r, "unit": UNIT, "cores": threads, "kind": "reference",
                    "sample": f"{m} contiguous searchlights of {w.sls.count} ({dt:.1f} s), reference cpu64 arm, "
                              f"OpenMP {threads} threads, OPENBLAS_NUM_THREADS=1",
                    "single_thread": {"value": r1, "unit": UNIT, "cores": 1,
-                                     "sample": f"{m1} contiguous searchlights ({dt1:.1f} s), one OpenMP thread"}}
+                                     "sample": f"{m1} contiguous searchlights ({dt1:.1f} s), one OpenMP thread"},
+                   "cpu32_arm": {"value": r32, "unit": UNIT, "cores": threads,
+                                 "sample": f"{m32} contiguous searchlights ({dt32:.1f} s), the reference's float32 "
+                                           f"arm, OpenMP {threads} threads"}}
         else:
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                    "sample": "oracle/_ref/libhyperalignment.so not built"}
