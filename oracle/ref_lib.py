@@ -136,6 +136,26 @@ def procrustes_dense(X, Y, idx, off, dists, radius, reflection=True, scaling=Fal
     return T
 
 
+def template_procrustes(dms, reflection=True, scaling=False, zscore_common=True, level2_iter=1):
+    """Reference ha_template_procrustes (csrc/ha_template.c:14-114): the whole-matrix Procrustes
+    template (row-major nt x nv subjects)."""
+    h = lib()
+    mats = [np.ascontiguousarray(d, dtype=np.float64) for d in dms]
+    nt, nv = mats[0].shape
+    tms = [TMat(_dp(m), nt, nv) for m in mats]
+    arr = (ctypes.POINTER(TMat) * len(tms))(*[ctypes.pointer(t) for t in tms])
+    out = np.zeros((nt, nv))
+    tout = TMat(_dp(out), nt, nv)
+    h.ha_template_procrustes.restype = ctypes.c_int
+    h.ha_template_procrustes.argtypes = [ctypes.POINTER(ctypes.POINTER(TMat)), ctypes.c_int32, ctypes.c_bool,
+                                         ctypes.c_bool, ctypes.c_bool, ctypes.c_int32, ctypes.POINTER(TMat)]
+    rc = h.ha_template_procrustes(arr, len(tms), bool(reflection), bool(scaling), bool(zscore_common),
+                                  int(level2_iter), ctypes.byref(tout))
+    if rc != 0:
+        raise RuntimeError(f"reference ha_template_procrustes rc={rc}")
+    return out
+
+
 class _Sls:
     """Keeps the ctypes arrays of a TSearchlights alive."""
 

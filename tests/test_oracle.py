@@ -349,3 +349,25 @@ def test_pca_template_restatement_vs_python_reference():
     g = golden("pca_template.npz")
     tpl = O.searchlight_pca_template(list(g["dms"]), g["idx"], g["off"], g["dists"], float(g["radius"]))
     assert np.linalg.norm(tpl - g["template"]) <= 1e-12 * np.linalg.norm(g["template"])
+
+
+@pytest.mark.parametrize("refl,scal,zs,level2", [(True, False, True, 1), (False, True, False, 2), (True, True, True, 0)])
+def test_template_loop_vs_live_reference(refl, scal, zs, level2):
+    """The template loop restated around searchlight solves reduces, for one searchlight holding
+    every vertex (weight 1), to the reference's whole-matrix ha_template_procrustes
+    (csrc/ha_template.c:14-114): same running average, leave-one-out passes, z-scores and final
+    sum."""
+    from oracle import ref_lib as R
+    if not R.available():
+        pytest.skip("compiled reference not built (make -C oracle)")
+    rng = np.random.default_rng(3)
+    nt, nv, ns = 30, 12, 4
+    L = rng.standard_normal((nt, nv))
+    dms = []
+    for _ in range(ns):
+        Q, r = np.linalg.qr(rng.standard_normal((nv, nv)))
+        dms.append(L @ (Q * np.sign(np.diag(r))) + 0.3 * rng.standard_normal((nt, nv)))
+    ref = R.template_procrustes(dms, refl, scal, zs, level2)
+    ours = O.searchlight_template(dms, np.arange(nv, dtype=np.int32), np.array([0, nv], dtype=np.int32), None, 0.0,
+                                  refl, scal, zs, level2)
+    assert np.linalg.norm(ours - ref) <= 1e-12 * np.linalg.norm(ref)
