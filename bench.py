@@ -58,11 +58,12 @@ def parse_args():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
-    p.add_argument("--workload", choices=["template", "grid", "learned", "rankdef", "shard"], default="template",
+    p.add_argument("--workload", choices=["template", "grid", "learned", "rankdef", "shard", "forrest"], default="template",
                    help="template: the headline Procrustes step; grid: the searchlight ridge grid search "
                         "(40962 vertices, every --grid-step-th searchlight); learned: the learned proposal; "
                         "rankdef: the mixed form on the template pair with duplicated columns; shard: one "
-                        "hemisphere split over the N GPUs (strong scaling)")
+                        "hemisphere split over the N GPUs (strong scaling); forrest: the shapes of the "
+                        "reference's published run (nt 1818, searchlights of 90-170)")
     p.add_argument("--grid-step", type=int, default=16)
     p.add_argument("--ref-seconds", type=float, default=0.0,
                    help="reference arm: seconds of CPU work per step (default: 150 s over all steps)")
@@ -909,6 +910,115 @@ def run_shard(args):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------------------------
+# the shapes of the reference's published run (StudyForrest: nt 1818, ~9,675 searchlights of 90-170)
+# ---------------------------------------------------------------------------------------------
+
+# The reference's published per-hemisphere timings of this run (README.md:223-241), as
+# searchlights/s = 9,675 / seconds per hemisphere, for context: other hardware, the real data set.
+PUBLISHED_FORREST = {"c_cuda_fp32_rtx4090": 459, "c_cpu_fp32_96_threads_tr7995wx": 15100,
+                     "c_cpu_fp64_96_threads_tr7995wx": 8880, "c_cpu_fp32_10_threads_m4pro": 7740}
+
+
+def run_forrest(args):
+    """Dense searchlight Procrustes (reflection allowed, no scaling, distance weights) on synthetic
+    inputs with the shapes of the reference's published run: device-resident steps (value) and the
+    C-ABI dense entry from host buffers into a host nv x nv matrix (e2e, the published runs' form)."""
+    import torch
+    from hyperalignment_b200 import _lib as L
+    from hyperalignment_b200 import workloads as W
+    from hyperalignment_b200.plan import Plan
+    torch.cuda.set_device(0)
+    lib = L.lib()
+    L.check(lib.ha_b200_init(), "ha_b200_init")
+    w = W.forrest_shaped(0)
+    s = w.sls
+    dev = torch.device("cuda", 0)
+    plan = Plan.from_workload(w)
+    dX = torch.from_numpy(np.asfortranarray(w.X).ravel(order="F")).to(dev)
+    dY = torch.from_numpy(np.asfortranarray(w.Y).ravel(order="F")).to(dev)
+    vals = torch.zeros(plan.nnz, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        plan.procrustes_device(dX.data_ptr(), dY.data_ptr(), vals.data_ptr(), True, False, L.SOLVER_MIXED,
+                               L.OUT_CSR, stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(0)
+    sampler.start()
+    n0 = lib.ha_b200_launch_count()
+    evs = []
+    for _ in range(args.steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        step()
+        b.record(stream)
+        evs.append((a, b))
+    torch.cuda.synchronize()
+    launches = lib.ha_b200_launch_count() - n0
+    clocks = sampler.stop()
+    K = args.steps
+    ms = sum(a.elapsed_time(b) for a, b in evs)
+    stats = plan.stats()
+
+    e2e = None
+    if not args.no_e2e:
+        Xf, Yf = np.asfortranarray(w.X), np.asfortranarray(w.Y)
+        T_out = np.zeros((w.nv, w.nv))
+        argsv = (Xf.ctypes.data_as(L.c_double_p), Yf.ctypes.data_as(L.c_double_p), w.nt, w.nv, L.iptr(s.indices),
+                 L.iptr(s.offsets), L.dptr(s.dists), s.count, s.radius, T_out.ctypes.data_as(L.c_double_p), True,
+                 False, L.BACKEND_B200, True)
+        lib.ha_set_num_threads(os.cpu_count() or 1)
+        L.check(lib.ha_searchlight_procrustes_dense(*argsv), "dense")
+        ts = []
+        for _ in range(max(1, K - 1)):
+            t0 = time.perf_counter()
+            L.check(lib.ha_searchlight_procrustes_dense(*argsv), "dense")
+            ts.append(time.perf_counter() - t0)
+        e2e = {"value": s.count * len(ts) / sum(ts), "unit": UNIT, "h2d_bytes_per_step": int(2 * w.nt * w.nv * 8),
+               "d2h_bytes_per_step": int(plan.nnz * 8),
+               "path": "ha_searchlight_procrustes_dense(backend=4), host float64 in, host dense nv x nv out (+=); "
+                       "wall clock per call"}
+
+    from oracle import ha_oracle as O
+    rng = np.random.default_rng(5)
+    sample = np.sort(rng.choice(s.count, size=12, replace=False))
+    sub = s.subset(sample)
+    splan = Plan(w.nt, w.nv, sub.indices, sub.offsets, sub.dists, sub.radius)
+    svals = torch.zeros(splan.nnz, dtype=torch.float64, device=dev)
+    splan.procrustes_device(dX.data_ptr(), dY.data_ptr(), svals.data_ptr(), True, False, L.SOLVER_MIXED, L.OUT_CSR,
+                            stream.cuda_stream)
+    torch.cuda.synchronize()
+    Ts = splan.local_transforms(0, sub.count)
+    err = []
+    for j, q in enumerate(sample):
+        sl = s.indices[s.offsets[q]:s.offsets[q + 1]]
+        Tref = O.procrustes(w.X[:, sl], w.Y[:, sl], True, False)
+        err.append(np.linalg.norm(Ts[j] - Tref) / np.linalg.norm(Tref))
+    splan.close()
+    sizes = s.sizes
+    out = {
+        "metric": METRIC, "value": s.count * K / (ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": K,
+        "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "forrest_shaped", "nv": w.nv, "nt": w.nt, "searchlights": s.count,
+                   "sl_size_min": int(sizes.min()), "sl_size_max": int(sizes.max()),
+                   "sl_size_mean": round(float(sizes.mean()), 2), "reflection": True, "scaling": False,
+                   "weights": "linear distance", "l2": "flushed between steps (256 MiB write)"},
+        "e2e": e2e, "error_vs_fp64": {"T_relfrob_max": float(max(err)), "T_relfrob_median": float(np.median(err)),
+                                      "sample": len(err)},
+        "solver_stats": stats, "gpu_launches": int(launches), "clocks": clocks,
+        "published_reference_searchlights_per_s": PUBLISHED_FORREST,
+    }
+    print(json.dumps(out))
+    plan.close()
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -921,6 +1031,8 @@ def main():
         run_rankdef(args)
     elif args.workload == "shard":
         run_shard(args)
+    elif args.workload == "forrest":
+        run_forrest(args)
     else:
         run_b200(args)
 
