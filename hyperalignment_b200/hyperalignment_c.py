@@ -33,6 +33,38 @@ def _flatten(sls, dists):
     return idx, offsets, d
 
 
+def _check_xy(X, Y):
+    """X and Y as Fortran-order float64 of one shape (the library reads nt x nv of each)."""
+    X = np.asfortranarray(X, dtype=np.float64)
+    Y = np.asfortranarray(Y, dtype=np.float64)
+    if X.ndim != 2 or X.shape != Y.shape:
+        raise ValueError(f"X and Y must be 2-D arrays of one shape, got {X.shape} and {Y.shape}")
+    return X, Y
+
+
+def _check_csc(indptr, indices, data, nv):
+    """The CSC arrays the library reads (indptr, indices) and accumulates into (data, in place)."""
+    indptr = np.ascontiguousarray(indptr, dtype=np.int32)
+    indices = np.ascontiguousarray(indices, dtype=np.int32)
+    if indptr.shape != (nv + 1,) or indptr[0] != 0 or indptr[-1] != indices.size:
+        raise ValueError("indptr must hold nv + 1 entries from 0 to len(indices)")
+    if not isinstance(data, np.ndarray) or data.dtype != np.float64 or not data.flags.c_contiguous \
+            or not data.flags.writeable or data.shape != (indices.size,):
+        raise ValueError("data must be a writable C-contiguous float64 array of len(indices) entries")
+    return indptr, indices
+
+
+def _check_weights(weights, sls):
+    """Per-searchlight weight arrays (or any list of arrays whose concatenation is the flat
+    weights): one float64 weight per searchlight member, in searchlight order."""
+    if weights is None:
+        return None
+    w = np.ascontiguousarray(np.concatenate([np.ravel(a) for a in weights]).astype(np.float64))
+    if w.size != sum(len(sl) for sl in sls):
+        raise ValueError("weights must hold one value per searchlight member")
+    return w
+
+
 def _init():
     lib = L.lib()
     rc = lib.ha_b200_init()
@@ -51,11 +83,10 @@ def searchlight_procrustes(X, Y, sls, dists, radius, backend="b200", reflection=
     """
     if backend not in _BACKENDS:
         raise ValueError(f"Unknown backend '{backend}'. Choose from: {list(_BACKENDS.keys())}")
+    X, Y = _check_xy(X, Y)
     lib = _init()
     if n_jobs > 0:
         lib.ha_set_num_threads(n_jobs)
-    X = np.asfortranarray(X, dtype=np.float64)
-    Y = np.asfortranarray(Y, dtype=np.float64)
     nt, nv = X.shape
     idx, offsets, d = _flatten(sls, dists)
     if T_out is None:
@@ -99,32 +130,30 @@ def sparse_pattern(sls, nv):
 
 def searchlight_procrustes_csc(X, Y, sls, indptr, indices, data, weights=None, reflection=True, scaling=False):
     """Sparse-output searchlight Procrustes: accumulates into ``data`` (CSC, pattern ``indptr``/``indices``)."""
-    lib = _init()
-    X = np.asfortranarray(X, dtype=np.float64)
-    Y = np.asfortranarray(Y, dtype=np.float64)
+    X, Y = _check_xy(X, Y)
     nt, nv = X.shape
+    indptr, indices = _check_csc(indptr, indices, data, nv)
+    w = _check_weights(weights, sls)
+    lib = _init()
     idx, offsets, _ = _flatten(sls, None)
-    w = None if weights is None else np.ascontiguousarray(np.concatenate(weights).astype(np.float64))
     L.check(lib.ha_searchlight_procrustes_csc_b200(
-        L.dptr(X), L.dptr(Y), nt, nv, L.iptr(idx), L.iptr(offsets), len(sls), L.dptr(w),
-        L.iptr(np.ascontiguousarray(indptr, dtype=np.int32)), L.iptr(np.ascontiguousarray(indices, dtype=np.int32)),
-        int(len(indices)), L.dptr(data), bool(reflection), bool(scaling), True),
+        L.dptr(X), L.dptr(Y), nt, nv, L.iptr(idx), L.iptr(offsets), len(sls), L.dptr(w), L.iptr(indptr),
+        L.iptr(indices), int(indices.size), L.dptr(data), bool(reflection), bool(scaling), True),
         "ha_searchlight_procrustes_csc_b200")
     return data
 
 
 def searchlight_ridge_csc(X, Y, sls, indptr, indices, data, alpha, weights=None):
     """Sparse-output searchlight ridge (float64): accumulates into ``data``."""
-    lib = _init()
-    X = np.asfortranarray(X, dtype=np.float64)
-    Y = np.asfortranarray(Y, dtype=np.float64)
+    X, Y = _check_xy(X, Y)
     nt, nv = X.shape
+    indptr, indices = _check_csc(indptr, indices, data, nv)
+    w = _check_weights(weights, sls)
+    lib = _init()
     idx, offsets, _ = _flatten(sls, None)
-    w = None if weights is None else np.ascontiguousarray(np.concatenate(weights).astype(np.float64))
     L.check(lib.ha_searchlight_ridge_csc_b200(
-        L.dptr(X), L.dptr(Y), nt, nv, L.iptr(idx), L.iptr(offsets), len(sls), L.dptr(w),
-        L.iptr(np.ascontiguousarray(indptr, dtype=np.int32)), L.iptr(np.ascontiguousarray(indices, dtype=np.int32)),
-        int(len(indices)), L.dptr(data), float(alpha), True), "ha_searchlight_ridge_csc_b200")
+        L.dptr(X), L.dptr(Y), nt, nv, L.iptr(idx), L.iptr(offsets), len(sls), L.dptr(w), L.iptr(indptr),
+        L.iptr(indices), int(indices.size), L.dptr(data), float(alpha), True), "ha_searchlight_ridge_csc_b200")
     return data
 
 
@@ -133,12 +162,12 @@ def searchlight_ridge_grid(X, Y, sls, indptr, indices, data, alphas, npcs, train
     """Searchlight ridge grid search with CV ensembles (float64): the winner's model-averaged
     betas of every searchlight accumulate into ``data`` (CSC); returns the winning grid index per
     searchlight (g = alpha index * len(npcs) + PC index), and the cost grid when asked."""
-    lib = _init()
-    X = np.asfortranarray(X, dtype=np.float64)
-    Y = np.asfortranarray(Y, dtype=np.float64)
+    X, Y = _check_xy(X, Y)
     nt, nv = X.shape
+    indptr, indices = _check_csc(indptr, indices, data, nv)
+    w = _check_weights(weights, sls)
+    lib = _init()
     idx, offsets, _ = _flatten(sls, None)
-    w = None if weights is None else np.ascontiguousarray(np.concatenate(weights).astype(np.float64))
     al = np.ascontiguousarray(alphas, dtype=np.float64)
     pc = np.ascontiguousarray(npcs, dtype=np.int32)
     tr, te = L.IndexLists(train_li), L.IndexLists(test_li)
@@ -147,9 +176,8 @@ def searchlight_ridge_grid(X, Y, sls, indptr, indices, data, alphas, npcs, train
     best = np.zeros(len(sls), dtype=np.int32)
     costs = np.zeros((len(sls), al.size, pc.size)) if return_costs else None
     L.check(lib.ha_searchlight_ridge_grid_b200(
-        L.dptr(X), L.dptr(Y), nt, nv, L.iptr(idx), L.iptr(offsets), len(sls), L.dptr(w),
-        L.iptr(np.ascontiguousarray(indptr, dtype=np.int32)), L.iptr(np.ascontiguousarray(indices, dtype=np.int32)),
-        int(len(indices)), L.dptr(data), L.dptr(al), al.size, L.iptr(pc), pc.size, tr.ptrs, te.ptrs,
+        L.dptr(X), L.dptr(Y), nt, nv, L.iptr(idx), L.iptr(offsets), len(sls), L.dptr(w), L.iptr(indptr),
+        L.iptr(indices), int(indices.size), L.dptr(data), L.dptr(al), al.size, L.iptr(pc), pc.size, tr.ptrs, te.ptrs,
         L.iptr(tr.sizes), L.iptr(te.sizes), len(tr), L.iptr(best), L.dptr(costs), True),
         "ha_searchlight_ridge_grid_b200")
     return (best, costs) if return_costs else best
