@@ -30,6 +30,8 @@ def _flatten(sls, dists):
     np.cumsum(sizes, out=offsets[1:])
     idx = np.ascontiguousarray(np.concatenate(sls).astype(np.int32))
     d = None if dists is None else np.ascontiguousarray(np.concatenate(dists).astype(np.float64))
+    if d is not None and d.size != idx.size:
+        raise ValueError("dists must hold one distance per searchlight member")
     return idx, offsets, d
 
 

@@ -82,3 +82,7 @@ def test_dense_shape_mismatch_raises(stub_device):
         H.searchlight_procrustes(X, np.zeros((10, 5)), [np.arange(3)], None, 0.0)
     with pytest.raises(ValueError):
         H.searchlight_procrustes(X, X, [np.arange(3)], None, 0.0, backend="cuda")
+    with pytest.raises(ValueError):  # one distance short
+        H.searchlight_procrustes(X, X, [np.arange(3)], [np.ones(2)], 2.0)
+    with pytest.raises(ValueError):
+        H.searchlight_weights([np.arange(3)], [np.ones(2)], 2.0)
