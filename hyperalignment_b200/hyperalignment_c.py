@@ -86,11 +86,11 @@ def searchlight_procrustes(X, Y, sls, dists, radius, backend="b200", reflection=
     if backend not in _BACKENDS:
         raise ValueError(f"Unknown backend '{backend}'. Choose from: {list(_BACKENDS.keys())}")
     X, Y = _check_xy(X, Y)
+    idx, offsets, d = _flatten(sls, dists)
     lib = _init()
     if n_jobs > 0:
         lib.ha_set_num_threads(n_jobs)
     nt, nv = X.shape
-    idx, offsets, d = _flatten(sls, dists)
     if T_out is None:
         T_out = np.zeros((nv, nv), dtype=np.float64)
     elif T_out.dtype != np.float64 or not T_out.flags.c_contiguous or T_out.shape != (nv, nv):
