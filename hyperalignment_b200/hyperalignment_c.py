@@ -211,13 +211,13 @@ def searchlight_template(dms, sls, dists, radius, reflection=True, scaling=False
     The loop of the reference's ``ha_template_procrustes`` (csrc/ha_template.c:14-114) with each
     whole-matrix Procrustes replaced by a searchlight solve; returns the nt x nv template.
     """
-    lib = _init()
     ns = len(dms)
     nt, nv = dms[0].shape
     stack = np.empty((ns, nv, nt), dtype=np.float64)  # each subject column-major
     for s, D in enumerate(dms):
-        stack[s] = np.asarray(D, dtype=np.float64).T
+        stack[s] = np.asarray(D, dtype=np.float64).T  # raises if a subject's shape differs
     idx, offsets, d = _flatten(sls, dists)
+    lib = _init()
     out = np.empty((nv, nt), dtype=np.float64)
     L.check(lib.ha_searchlight_template_b200(
         L.dptr(stack), ns, nt, nv, L.iptr(idx), L.iptr(offsets), L.dptr(d), len(sls), float(radius),
