@@ -914,7 +914,7 @@ def run_shard(args):
 # the shapes of the reference's published run (StudyForrest: nt 1818, ~9,675 searchlights of 90-170)
 # ---------------------------------------------------------------------------------------------
 
-# The reference's published per-hemisphere timings of this run (README.md:223-241), as
+# The reference's published per-hemisphere timings of this run (the reference project's README.md:223-241), as
 # searchlights/s = 9,675 / seconds per hemisphere, for context: other hardware, the real data set.
 PUBLISHED_FORREST = {"c_cuda_fp32_rtx4090": 459, "c_cpu_fp32_96_threads_tr7995wx": 15100,
                      "c_cpu_fp64_96_threads_tr7995wx": 8880, "c_cpu_fp32_10_threads_m4pro": 7740}
