@@ -171,3 +171,26 @@ def test_aligned_correlation_argument_errors(hlib):
     assert f(p, p, 10, 4, None, p, p, 8, p, None, None) == L.ERROR_ARG            # values without indptr
     assert f(p, p, 10, 4, p, None, p, 8, p, None, None) == L.ERROR_ARG            # values without rows
     assert f(p, p, 10, 4, p, p, p, -1, p, None, None) == L.ERROR_ARG              # negative nnz
+
+
+@pytest.mark.parametrize("args,mask_seed", [
+    ((300, 3, 4, 8, 0, 11), None), ((97, 2, 3, 5, 2, 0), None), ((64, 1, 2, 16, 4, 123456789), None),
+    ((500, 1, 5, 10, 10, 5), None), ((500, 4, 5, 10, 10, 2**63 + 7), None), ((41, 2, 7, 1, 0, 3), None),
+    ((200, 2, 4, 6, 3, 17), 1), ((150, 1, 5, 10, 10, 99), 2),
+])
+def test_ensemble_indices_c_abi_vs_live_reference(hlib, args, mask_seed):
+    """The library's host split generator against the compiled reference's ha_ensemble_indices
+    (csrc/ha_ensemble.c:58-249), draw for draw, over fold counts, block and buffer sizes,
+    several permutations, 64-bit seeds and masks."""
+    from oracle import ref_lib as R
+    if not R.available():
+        pytest.skip("compiled reference not built (make -C oracle)")
+    from hyperalignment_b200 import hyperalignment_c as H
+    mask = None
+    if mask_seed is not None:
+        mask = np.random.default_rng(mask_seed).random(args[0]) < 0.8
+    tr, te = H.ensemble_indices(*args, mask=mask)
+    rtr, rte = R.ensemble_indices(*args, mask=mask)
+    assert len(tr) == len(rtr) == len(te) == len(rte)
+    for a, b in zip(tr + te, rtr + rte):
+        np.testing.assert_array_equal(a, b)
