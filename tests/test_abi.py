@@ -194,3 +194,21 @@ def test_ensemble_indices_c_abi_vs_live_reference(hlib, args, mask_seed):
     assert len(tr) == len(rtr) == len(te) == len(rte)
     for a, b in zip(tr + te, rtr + rte):
         np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("seed,uniform", [(0, False), (1, True), (2, False), (3, True)])
+def test_weights_c_abi_vs_live_reference(hlib, seed, uniform):
+    """The library's host weights (the rule of csrc/ha_searchlight.c:970-1001 and :36-92) against
+    the compiled reference's ha_searchlight_weights, bit for bit, on ragged k-NN searchlights with
+    distance weights and uniform ones."""
+    from oracle import ref_lib as R
+    if not R.available():
+        pytest.skip("compiled reference not built (make -C oracle)")
+    from hyperalignment_b200 import hyperalignment_c as H
+    from hyperalignment_b200 import workloads as W
+    s = W.small_case(seed=seed, nv=642, nt=8, lo=5, hi=70).sls
+    sls = [s.indices[s.offsets[q]:s.offsets[q + 1]] for q in range(s.count)]
+    ds = None if uniform else [s.dists[s.offsets[q]:s.offsets[q + 1]] for q in range(s.count)]
+    ours = H.searchlight_weights(sls, ds, None if uniform else s.radius, 642)
+    ref = R.searchlight_weights(s.indices, s.offsets, None if uniform else s.dists, 0.0 if uniform else s.radius)
+    assert np.array_equal(ours, ref)
