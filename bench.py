@@ -357,10 +357,13 @@ def run_b200(args):
             T = Ts[j]
             sl = w.sls.indices[w.sls.offsets[q]:w.sls.offsets[q + 1]]
             Tref = O.procrustes(w.X[:, sl], w.Y[:, sl], True, False)
-            e.append((np.linalg.norm(T - Tref) / np.linalg.norm(Tref), np.abs(T - Tref).max()))
+            XT, XTref = w.X[:, sl] @ T, w.X[:, sl] @ Tref  # the aligned data of the searchlight
+            e.append((np.linalg.norm(T - Tref) / np.linalg.norm(Tref), np.abs(T - Tref).max(),
+                      np.linalg.norm(XT - XTref) / np.linalg.norm(XTref), np.abs(XT - XTref).max()))
         e = np.array(e)
         errs[name] = {"T_relfrob_max": float(e[:, 0].max()), "T_relfrob_median": float(np.median(e[:, 0])),
-                      "T_maxabs_max": float(e[:, 1].max()), "sample": int(sample.size)}
+                      "T_maxabs_max": float(e[:, 1].max()), "XT_relfrob_max": float(e[:, 2].max()),
+                      "XT_maxabs_max": float(e[:, 3].max()), "sample": int(sample.size)}
 
     # roofline of the dominant kernel
     peaks, peak_src = load_peaks()
