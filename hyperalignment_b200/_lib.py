@@ -99,19 +99,21 @@ SIGNATURES = {
     "ha_b200_set_kernel_timing": (None, [ctypes.c_bool]),
     "ha_b200_kernel_times": (ctypes.c_int, [c_double_p, c_int64_p]),
     "ha_b200_launch_count": (ctypes.c_int64, []),
+    "ha_b200_tc_selftest": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, c_float_p, c_float_p,
+                                           c_float_p]),
     "ha_b200_aligned_correlation_device": (ctypes.c_int, [
         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
         ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
 }
 
 KERNEL_KINDS = ["convert", "colvar", "xcov32", "jacobi32", "formT32", "xcov64", "jacobi64", "formT64", "refine",
-                "reflect", "scale", "reduce", "pattern", "ridge", "grid", "mlp", "eval"]
+                "reflect", "scale", "reduce", "pattern", "ridge", "grid", "mlp", "eval", "tc_xcov", "tc_ns"]
 
 # Error codes and enum values (include/hyperalignment_b200.h, same as the reference's ha_common.h).
 SUCCESS, ERROR_ALLOC, ERROR_SVD, ERROR_ARG, ERROR_INTERNAL = 0, -1, -2, -3, -4
 BACKEND_B200 = 4
 OUT_CSR, OUT_CSC = 0, 1
-SOLVER_MIXED, SOLVER_FP32, SOLVER_FP64 = 0, 1, 2
+SOLVER_MIXED, SOLVER_FP32, SOLVER_FP64, SOLVER_TC = 0, 1, 2, 3
 
 _lib = None
 

@@ -10,6 +10,7 @@
 #include "ha_b200_kernels.cuh"
 #include "ha_b200_grid.cuh"
 #include "ha_b200_mlp.cuh"
+#include "ha_b200_tc.cuh"
 
 #include <cuda_runtime.h>
 #include <omp.h>
@@ -269,6 +270,13 @@ struct Chunk {
 	int64_t uv_elems;
 	SlWork *d_w32 = nullptr, *d_w64 = nullptr, *d_weig = nullptr;
 	int64_t *d_tofs = nullptr;
+	// tensor-core solve: one work item per searchlight (slot order), 128-row tiles in two size
+	// classes (np <= 256: two CTAs per SM; np > 256), largest searchlights first
+	std::vector<TcWork> tcw;
+	std::vector<TcTile> tct[2];
+	TcWork *d_tcw = nullptr;
+	TcTile *d_tct[2] = {nullptr, nullptr};
+	int64_t tc_x_elems = 0, tc_a_elems = 0;
 };
 
 }  // namespace
@@ -302,7 +310,13 @@ struct HaB200Plan {
 	// per-run data
 	DevArr<float> X32, Y32;
 	DevArr<double> var;
-	DevArr<int32_t> counters;  // [n_fp64, n_unconverged]
+	DevArr<int32_t> counters;  // [n_fp64, n_unconverged, sweeps sum, sweeps max, tensor-core wait failures]
+	// tensor-core solve, allocated on first use: vertex-major bf16 planes of X and Y, iterate and P
+	// planes, cross-covariance, iteration state (two copies) and residual partials
+	DevArr<__nv_bfloat16> tcXb, tcYb, tcXp, tcPp;
+	DevArr<float> tcA, tcRes;
+	DevArr<TcState> tcSt;
+	bool tc_ready = false;
 	// ridge grid search: scratch and the uploaded grid / CV description, allocated on first use
 	DevArr<double> gridscr, galpha, gwinv;
 	DevArr<int64_t> gbase;
@@ -513,7 +527,7 @@ int build_chunks(HaB200Plan *P) {
 	if ((rc = P->uv.ensure((size_t)maxUV)) != kHaSuccess) return rc;
 	if ((rc = P->scale.ensure((size_t)max_slots)) != kHaSuccess) return rc;
 	if ((rc = P->stats.ensure((size_t)max_slots)) != kHaSuccess) return rc;
-	if ((rc = P->counters.ensure(4)) != kHaSuccess) return rc;
+	if ((rc = P->counters.ensure(5)) != kHaSuccess) return rc;
 	P->max_slots = max_slots;
 	return kHaSuccess;
 }
@@ -706,9 +720,253 @@ double weak_factor() {
 	return r;
 }
 
+// ---- tensor-core Newton-Schulz solver ----
+
+// Dynamic shared memory of the tile-product launches: np <= 256 runs two CTAs per SM (two
+// 110 KB stage rings plus static and reserved shared memory within the SM's 228 KB, 2 x 256
+// tensor-memory columns), np > 256 one CTA per SM.
+constexpr int kTcSmemSmall = 110 * 1024;
+constexpr int kTcSmemLarge = 200 * 1024;
+
+double env_double(const char *name, double dflt, double lo, double hi) {
+	const char *e = getenv(name);
+	if (!e) return dflt;
+	const double v = atof(e);
+	return (v >= lo && v <= hi) ? v : dflt;
+}
+
+// Iteration schedule, shared by every searchlight.  X_0 = A / u has its singular values in
+// [l0, 1] for a condition number up to 1/l0 (u overestimates sigma_max by a few units, which the
+// bound absorbs).  Each step is the scaled cubic step of the lower bound l:
+// a = sqrt(3 / (1 + l + l^2)), capped at `cap` (larger scalings map the largest singular values
+// near zero and lose their precision), l <- a l (3 - a^2 l^2) / 2; once a < 1.02 the steps are the
+// plain ones (a = 1) until the residual criterion ends each searchlight.  HA_B200_NS_L0,
+// HA_B200_NS_CAP and HA_B200_NS_MAXIT override the defaults.
+struct NsStep {
+	float c1, c3;
+	int plain;
+};
+std::vector<NsStep> ns_schedule() {
+	const double l0 = env_double("HA_B200_NS_L0", 1e-5, 1e-12, 0.5);
+	const double cap = env_double("HA_B200_NS_CAP", 1.6, 1.0, 1.7);
+	const int maxit = (int)env_double("HA_B200_NS_MAXIT", 40, 4, 200);
+	std::vector<NsStep> out;
+	double l = l0;
+	bool plain = false;
+	for (int k = 0; k < maxit; k++) {
+		double a = 1.0;
+		if (!plain) {
+			a = std::min(std::sqrt(3.0 / (1.0 + l + l * l)), cap);
+			if (a < 1.02) {
+				plain = true;
+				a = 1.0;
+			}
+		}
+		out.push_back({(float)(1.5 * a), (float)(-0.5 * a * a * a), plain ? 1 : 0});
+		l = std::min(1.0, 0.5 * a * l * (3.0 - a * a * l * l));
+	}
+	return out;
+}
+
+// Residual ||G - I||_F / sqrt(n) below which a plain step is the last (HA_B200_NS_TOL).  The
+// largest |1 - sigma^2| is then below 1e-4 sqrt(n); the final step squares it.
+double ns_tol() { return env_double("HA_B200_NS_TOL", 1e-4, 1e-7, 1e-1); }
+
+int set_tc_attrs() {
+	static bool done = false;
+	if (done) return kHaSuccess;
+	HA_CUDA(cudaFuncSetAttribute(k_tc_gemm<kTcPhaseXcov>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemLarge));
+	HA_CUDA(cudaFuncSetAttribute(k_tc_gemm<kTcPhaseGram>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemLarge));
+	HA_CUDA(cudaFuncSetAttribute(k_tc_gemm<kTcPhaseUpdate>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemLarge));
+	done = true;
+	return kHaSuccess;
+}
+
+// Work lists and buffers of the tensor-core solve (once per plan).
+int build_tc(HaB200Plan *P) {
+	if (P->tc_ready) return kHaSuccess;
+	int rc;
+	if ((rc = set_tc_attrs()) != kHaSuccess) return rc;
+	int64_t maxX = 1, maxA = 1;
+	for (auto &ch : P->chunks) {
+		const int nsl = ch.s1 - ch.s0;
+		ch.tcw.clear();
+		int64_t xacc = 0, aacc = 0;
+		for (int q = 0; q < nsl; q++) {
+			const int s = ch.s0 + q;
+			const int n = P->h_off[s + 1] - P->h_off[s];
+			const int np = (n + 15) & ~15;
+			if (np > kTcMaxNp) return kHaErrorArg;
+			TcWork w = {};
+			w.s = s;
+			w.slot = q;
+			w.n = n;
+			w.np = np;
+			w.sofs = P->h_off[s];
+			w.xofs = xacc;
+			w.pofs = xacc;
+			w.aofs = aacc;
+			w.tofs = ch.tofs[q];
+			xacc += 3 * (int64_t)np * np;
+			aacc += (int64_t)np * np;
+			ch.tcw.push_back(w);
+		}
+		ch.tc_x_elems = xacc;
+		ch.tc_a_elems = aacc;
+		maxX = std::max(maxX, xacc);
+		maxA = std::max(maxA, aacc);
+		std::vector<int> order((size_t)nsl);
+		for (int q = 0; q < nsl; q++) order[q] = q;
+		std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return ch.tcw[x].n > ch.tcw[y].n; });
+		for (int c = 0; c < 2; c++) ch.tct[c].clear();
+		for (int q : order) {
+			const int np = ch.tcw[q].np;
+			const int c = np > 256 ? 1 : 0;
+			for (int t = 0; t * 128 < np; t++) ch.tct[c].push_back({q, t});
+		}
+		if (cudaMalloc(&ch.d_tcw, (size_t)nsl * sizeof(TcWork)) != cudaSuccess) return kHaErrorAlloc;
+		HA_CUDA(cudaMemcpy(ch.d_tcw, ch.tcw.data(), (size_t)nsl * sizeof(TcWork), cudaMemcpyHostToDevice));
+		for (int c = 0; c < 2; c++) {
+			const size_t cnt = std::max<size_t>(ch.tct[c].size(), 1);
+			if (cudaMalloc(&ch.d_tct[c], cnt * sizeof(TcTile)) != cudaSuccess) return kHaErrorAlloc;
+			if (!ch.tct[c].empty())
+				HA_CUDA(cudaMemcpy(ch.d_tct[c], ch.tct[c].data(), ch.tct[c].size() * sizeof(TcTile), cudaMemcpyHostToDevice));
+		}
+	}
+	if ((rc = P->tcXp.ensure((size_t)maxX)) != kHaSuccess) return rc;
+	if ((rc = P->tcPp.ensure((size_t)maxX)) != kHaSuccess) return rc;
+	if ((rc = P->tcA.ensure((size_t)maxA)) != kHaSuccess) return rc;
+	if ((rc = P->tcRes.ensure((size_t)P->max_slots * kTcResSlots)) != kHaSuccess) return rc;
+	if ((rc = P->tcSt.ensure((size_t)P->max_slots * 2)) != kHaSuccess) return rc;
+	P->tc_ready = true;
+	return kHaSuccess;
+}
+
+// Launch one phase of the tile product over both size classes of a chunk.
+template <int PHASE>
+int launch_tc(const Chunk &ch, TcArgs a, cudaStream_t st, int kind) {
+	for (int c = 0; c < 2; c++) {
+		const int ntiles = (int)ch.tct[c].size();
+		if (!ntiles) continue;
+		a.tiles = ch.d_tct[c];
+		a.smem_bytes = c ? kTcSmemLarge : kTcSmemSmall;
+		HA_LAUNCH(kind, st);
+		k_tc_gemm<PHASE><<<ntiles, kTcThreads, a.smem_bytes, st>>>(a);
+	}
+	HA_CUDA(cudaGetLastError());
+	return kHaSuccess;
+}
+
+// Enqueue one tensor-core solve + reduction over all chunks: split-BF16 cross-covariance,
+// Newton-Schulz polar, float64 Jacobi re-solve of the searchlights whose iteration did not
+// converge (exactly singular A), scaling, reduction.  Reflection is allowed (isReflection).
+int run_procrustes_tc(HaB200Plan *P, const double *d_X, const double *d_Y, bool scal, int out_kind, double *d_vals,
+                      cudaStream_t st) {
+	const int nt = P->nt, nv = P->nv;
+	const int ntp = (nt + 15) & ~15;
+	const int rowmajor = out_kind == kHaB200OutCSR ? 1 : 0;
+	int rc;
+	if (P->chunks.empty() && (rc = build_chunks(P)) != kHaSuccess) return rc;
+	if ((rc = build_tc(P)) != kHaSuccess) return rc;
+	const int64_t vplane = (int64_t)nv * ntp;
+	if ((rc = P->tcXb.ensure((size_t)(3 * vplane))) != kHaSuccess) return rc;
+	if ((rc = P->tcYb.ensure((size_t)(3 * vplane))) != kHaSuccess) return rc;
+	{ HA_LAUNCH(kHaB200KConvert, st); k_split3_vertex_major<<<148 * 8, kBlock, 0, st>>>(d_X, nt, nv, ntp, P->tcXb.p); }
+	{ HA_LAUNCH(kHaB200KConvert, st); k_split3_vertex_major<<<148 * 8, kBlock, 0, st>>>(d_Y, nt, nv, ntp, P->tcYb.p); }
+	if (scal) {
+		if ((rc = P->var.ensure((size_t)nv)) != kHaSuccess) return rc;
+		{ HA_LAUNCH(kHaB200KColVar, st); k_col_var_over_nt<<<(nv + 127) / 128, 128, 0, st>>>(d_X, nt, nv, P->var.p); }
+	}
+	HA_CUDA(cudaMemsetAsync(P->counters.p, 0, 5 * sizeof(int32_t), st));
+	static const std::vector<NsStep> sched = ns_schedule();
+	const int maxit = (int)sched.size();
+	float *T = P->scrT.p;
+	const int smem_cap = std::min(P->max_row, 16384);
+	const size_t red_smem = (size_t)smem_cap * 12;
+	for (size_t c = 0; c < P->chunks.size(); c++) {
+		Chunk &ch = P->chunks[c];
+		const int nsl = ch.s1 - ch.s0;
+		HA_CUDA(cudaMemsetAsync(P->stats.p, 0, (size_t)nsl * sizeof(SlStats), st));
+		TcArgs a = {};
+		a.work = ch.d_tcw;
+		a.Xb = P->tcXb.p;
+		a.Yb = P->tcYb.p;
+		a.vplane = vplane;
+		a.ntp = ntp;
+		a.sl_idx = P->idx.p;
+		a.Xp = P->tcXp.p;
+		a.Pp = P->tcPp.p;
+		a.A32 = P->tcA.p;
+		a.T = T;
+		a.t_rowmajor = rowmajor;
+		a.res_part = P->tcRes.p;
+		a.tol_stop = (float)ns_tol();
+		a.err = P->counters.p + 4;
+		if ((rc = launch_tc<kTcPhaseXcov>(ch, a, st, kHaB200KTcXcov)) != kHaSuccess) return rc;
+		{ HA_LAUNCH(kHaB200KTcNs, st); k_tc_ns_init<<<nsl, 256, 0, st>>>(ch.d_tcw, P->tcA.p, P->tcXp.p, P->tcSt.p, P->tcRes.p); }
+		for (int k = 0; k < maxit; k++) {
+			a.st_in = P->tcSt.p + (size_t)(k & 1) * P->max_slots;
+			a.st_out = P->tcSt.p + (size_t)((k + 1) & 1) * P->max_slots;
+			a.c1 = sched[k].c1;
+			a.c3 = sched[k].c3;
+			a.plain = sched[k].plain;
+			a.last = (k == maxit - 1) ? 1 : 0;
+			if ((rc = launch_tc<kTcPhaseGram>(ch, a, st, kHaB200KTcNs)) != kHaSuccess) return rc;
+			if ((rc = launch_tc<kTcPhaseUpdate>(ch, a, st, kHaB200KTcNs)) != kHaSuccess) return rc;
+		}
+		{ HA_LAUNCH(kHaB200KTcNs, st); k_tc_ns_finish<<<nsl, 256, 0, st>>>(ch.d_tcw, P->tcA.p, T, P->tcSt.p + (size_t)(maxit & 1) * P->max_slots,
+		                                                              P->stats.p, rowmajor); }
+		// float64 Jacobi re-solve of the flagged searchlights (cold start)
+		{
+			JacobiParams jp;
+			jp.max_sweeps = 40;
+			jp.t_rowmajor = rowmajor;
+			jp.ill_ratio = 0.0;
+			jp.weak = weak_factor();
+			jp.eig = 0;
+			jp.keep_v = 0;
+			jp.warm = 0;
+			jp.only_flagged = 1;
+			jp.stop_cos = fp64_stop_cos();
+			double *A = P->scrA.p, *V = P->scrV.p;
+			if ((rc = g_fan.begin(st)) != kHaSuccess) return rc;
+			for (size_t bi = 0; bi < ch.b64.size(); bi++) {
+				const Bucket &b = ch.b64[bi];
+				const cudaStream_t bs = g_fan.at((int)bi);
+				const SlWork *wk = ch.d_w64 + b.first;
+				{ HA_LAUNCH(kHaB200KXcov64, bs); k_xcov<double, 16><<<b.count, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_Y, nt, nt, A, P->stats.p, 1); }
+				{
+					HA_LAUNCH(kHaB200KJacobi64, bs);
+					if ((rc = launch_jacobi<double>(b.rpl, b.count, b.threads, b.smem, bs, wk, A, V, T, P->stats.p, P->uv.p, jp)) != kHaSuccess)
+						return rc;
+				}
+				if (b.blocked) { HA_LAUNCH(kHaB200KFormT64, bs); k_form_t_global<double><<<b.count, kBlock, 0, bs>>>(wk, A, V, T, P->stats.p, rowmajor, 1); }
+			}
+			if ((rc = g_fan.end(st)) != kHaSuccess) return rc;
+		}
+		{ HA_LAUNCH(kHaB200KScale, st); k_scale<<<(nsl + 127) / 128, 128, 0, st>>>(ch.d_w64, nsl, P->idx.p, P->var.p, P->stats.p, nt, scal ? 1 : 0,
+		                                          P->scale.p); }
+		{ HA_LAUNCH(kHaB200KScale, st); k_count_flags<<<(nsl + 127) / 128, 128, 0, st>>>(P->stats.p, nsl, P->counters.p); }
+		{ HA_LAUNCH(kHaB200KReduce, st); k_reduce<float><<<nv, kBlock, red_smem, st>>>(P->vlptr.p, P->vlent.p, P->off.p, P->idx.p,
+		                                       P->has_weights ? P->w.p : nullptr, P->patptr.p, P->patcol.p, T,
+		                                       ch.d_tofs, P->scale.p, ch.s0, ch.s1, out_kind == kHaB200OutCSC ? 1 : 0,
+		                                       smem_cap, d_vals); }
+		HA_CUDA(cudaGetLastError());
+	}
+	P->last_chunk = (int)P->chunks.size() - 1;
+	P->last_rowmajor = rowmajor;
+	return kHaSuccess;
+}
+
 // Enqueue one solve + reduction over all chunks.
 int run_procrustes(HaB200Plan *P, const double *d_X, const double *d_Y, bool refl, bool scal, int solver,
                    int out_kind, double *d_vals, cudaStream_t st) {
+	if (solver == kHaB200SolverTC) {
+		// The reflection fix needs the smallest singular pair, which the polar iteration does not
+		// produce: without reflection the mixed Jacobi solver runs instead.
+		if (refl) return run_procrustes_tc(P, d_X, d_Y, scal, out_kind, d_vals, st);
+		solver = kHaB200SolverMixed;
+	}
 	const int nt = P->nt, nv = P->nv;
 	const int ntp = (nt + 31) & ~31;
 	const bool use32 = solver != kHaB200SolverFP64;
@@ -731,7 +989,7 @@ int run_procrustes(HaB200Plan *P, const double *d_X, const double *d_Y, bool ref
 		if ((rc = P->var.ensure((size_t)nv)) != kHaSuccess) return rc;
 		{ HA_LAUNCH(kHaB200KColVar, st); k_col_var_over_nt<<<(nv + 127) / 128, 128, 0, st>>>(d_X, nt, nv, P->var.p); }
 	}
-	HA_CUDA(cudaMemsetAsync(P->counters.p, 0, 4 * sizeof(int32_t), st));
+	HA_CUDA(cudaMemsetAsync(P->counters.p, 0, 5 * sizeof(int32_t), st));
 	float *T = P->scrT.p;
 	int smem_cap = std::min(P->max_row, 16384);
 	size_t red_smem = (size_t)smem_cap * 12;
@@ -820,7 +1078,7 @@ int run_ridge(HaB200Plan *P, const double *d_X, const double *d_Y, double alpha,
 	int64_t maxT = 1;
 	for (auto &ch : P->chunks) maxT = std::max(maxT, ch.t_elems);
 	if ((rc = P->scrT64.ensure((size_t)maxT)) != kHaSuccess) return rc;
-	HA_CUDA(cudaMemsetAsync(P->counters.p, 0, 4 * sizeof(int32_t), st));
+	HA_CUDA(cudaMemsetAsync(P->counters.p, 0, 5 * sizeof(int32_t), st));
 	const int smem_cap = std::min(P->max_row, 16384);
 	const size_t red_smem = (size_t)smem_cap * 12;
 	for (size_t c = 0; c < P->chunks.size(); c++) {
@@ -1150,7 +1408,7 @@ int run_ridge_grid(HaB200Plan *P, const double *d_X, const double *d_Y, const Gr
 	if ((rc = grid_prepare(P)) != kHaSuccess) return rc;
 	GridParams gp;
 	if ((rc = grid_upload(P, gs, st, gp)) != kHaSuccess) return rc;
-	HA_CUDA(cudaMemsetAsync(P->counters.p, 0, 4 * sizeof(int32_t), st));
+	HA_CUDA(cudaMemsetAsync(P->counters.p, 0, 5 * sizeof(int32_t), st));
 	for (size_t c = 0; c < P->chunks.size(); c++) {
 		Chunk &ch = P->chunks[c];
 		HA_CUDA(cudaMemsetAsync(P->stats.p, 0, (size_t)(ch.s1 - ch.s0) * sizeof(SlStats), st));
@@ -1232,7 +1490,7 @@ int run_ridge_learned(HaB200Plan *P, const double *d_X, const double *d_Y, const
 	GridParams gp;
 	if ((rc = grid_upload(P, gs, st, gp)) != kHaSuccess) return rc;
 	if ((rc = P->gfeat.ensure((size_t)P->count * (kFeatSv + 1))) != kHaSuccess) return rc;
-	HA_CUDA(cudaMemsetAsync(P->counters.p, 0, 4 * sizeof(int32_t), st));
+	HA_CUDA(cudaMemsetAsync(P->counters.p, 0, 5 * sizeof(int32_t), st));
 	std::vector<float> hprob;
 	for (size_t c = 0; c < P->chunks.size(); c++) {
 		Chunk &ch = P->chunks[c];
@@ -1841,6 +2099,9 @@ void ha_b200_plan_destroy(HaB200Plan *P) {
 		if (ch.d_w64) cudaFree(ch.d_w64);
 		if (ch.d_weig) cudaFree(ch.d_weig);
 		if (ch.d_tofs) cudaFree(ch.d_tofs);
+		if (ch.d_tcw) cudaFree(ch.d_tcw);
+		for (int c = 0; c < 2; c++)
+			if (ch.d_tct[c]) cudaFree(ch.d_tct[c]);
 	}
 	P->idx.release(); P->off.release(); P->lo.release(); P->hi.release(); P->w.release();
 	P->vlptr.release(); P->vlent.release(); P->patptr.release(); P->patcol.release();
@@ -1849,6 +2110,8 @@ void ha_b200_plan_destroy(HaB200Plan *P) {
 	P->gridscr.release(); P->galpha.release(); P->gwinv.release(); P->gbase.release(); P->gnpcs.release();
 	P->grows.release(); P->gtpos.release(); P->gurows.release(); P->guntested.release(); P->gmdl.release();
 	P->gfit.release(); P->gfeat.release(); P->gwork.release();
+	P->tcXb.release(); P->tcYb.release(); P->tcXp.release(); P->tcPp.release(); P->tcA.release(); P->tcRes.release();
+	P->tcSt.release();
 	delete P;
 }
 
@@ -1911,7 +2174,7 @@ int ha_b200_plan_procrustes_device(HaB200Plan *P, const double *d_X, const doubl
                                    bool isScaling, int solver, int out_kind, double *d_values, void *stream) {
 	std::lock_guard<std::recursive_mutex> lk(g_mu);
 	if (!P || !d_X || !d_Y || !d_values) return kHaErrorArg;
-	if (solver < 0 || solver > 2 || out_kind < 0 || out_kind > 1) return kHaErrorArg;
+	if (solver < 0 || solver > 3 || out_kind < 0 || out_kind > 1) return kHaErrorArg;
 	return run_procrustes(P, d_X, d_Y, isReflection, isScaling, solver, out_kind, d_values, (cudaStream_t)stream);
 }
 
@@ -2159,6 +2422,140 @@ int ha_b200_kernel_times(double *ms, int64_t *launches) {
 }
 
 int64_t ha_b200_launch_count(void) { return g_launches; }
+
+int ha_b200_tc_selftest(int32_t which, int32_t n, int32_t nt, const float *h_a, const float *h_b, float *h_out) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	if (!h_a || !h_out || n <= 0 || n > kTcMaxNp || which < 0 || which > 2) return kHaErrorArg;
+	if (which != 0 && !h_b) return kHaErrorArg;
+	if (which == 2 && nt <= 0) return kHaErrorArg;
+	int rc = check_cuda_ready();
+	if (rc != kHaSuccess) return rc;
+	if ((rc = set_tc_attrs()) != kHaSuccess) return rc;
+	const int np = (n + 15) & ~15;
+	const int ntp = (nt + 15) & ~15;
+	const int64_t pe3 = 3 * (int64_t)np * np;
+	DevArr<__nv_bfloat16> Xp, Pp, Xb, Yb;
+	DevArr<float> A32, T, R, in0, in1;
+	DevArr<double> d0, d1;
+	DevArr<TcWork> dw;
+	DevArr<TcTile> dt;
+	DevArr<TcState> dst;
+	DevArr<int32_t> sl, err;
+	auto release_all = [&]() {
+		Xp.release(); Pp.release(); Xb.release(); Yb.release(); A32.release(); T.release(); R.release();
+		in0.release(); in1.release(); d0.release(); d1.release(); dw.release(); dt.release(); dst.release();
+		sl.release(); err.release();
+	};
+	if (Xp.ensure(pe3) || Pp.ensure(pe3) || A32.ensure((size_t)np * np) || T.ensure((size_t)n * n) ||
+	    R.ensure(kTcResSlots) || dw.ensure(1) || dt.ensure(kTcMaxNp / 128) || dst.ensure(2) || sl.ensure(n) ||
+	    err.ensure(1)) {
+		release_all();
+		return kHaErrorAlloc;
+	}
+	TcWork w = {};
+	w.n = n;
+	w.np = np;
+	std::vector<TcTile> tiles;
+	for (int t = 0; t * 128 < np; t++) tiles.push_back({0, t});
+	std::vector<int32_t> hs((size_t)n);
+	for (int i = 0; i < n; i++) hs[i] = i;
+	cudaStream_t st = 0;
+	rc = kHaSuccess;
+	do {
+		if (cudaMemcpy(dw.p, &w, sizeof(w), cudaMemcpyHostToDevice) != cudaSuccess ||
+		    cudaMemcpy(dt.p, tiles.data(), tiles.size() * sizeof(TcTile), cudaMemcpyHostToDevice) != cudaSuccess ||
+		    cudaMemcpy(sl.p, hs.data(), (size_t)n * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+		    cudaMemset(dst.p, 0, 2 * sizeof(TcState)) != cudaSuccess ||
+		    cudaMemset(R.p, 0, kTcResSlots * sizeof(float)) != cudaSuccess ||
+		    cudaMemset(err.p, 0, sizeof(int32_t)) != cudaSuccess) {
+			rc = kHaErrorInternal;
+			break;
+		}
+		TcArgs a = {};
+		a.work = dw.p;
+		a.tiles = dt.p;
+		a.Xp = Xp.p;
+		a.Pp = Pp.p;
+		a.A32 = A32.p;
+		a.T = T.p;
+		a.t_rowmajor = 1;
+		a.st_in = dst.p;
+		a.st_out = dst.p + 1;
+		a.res_part = R.p;
+		a.smem_bytes = np > 256 ? kTcSmemLarge : kTcSmemSmall;
+		a.err = err.p;
+		const int grid = (int)tiles.size();
+		if (which == 2) {
+			const int64_t vplane = (int64_t)n * ntp;
+			if (Xb.ensure(3 * vplane) || Yb.ensure(3 * vplane) || d0.ensure((size_t)n * nt) || d1.ensure((size_t)n * nt)) {
+				rc = kHaErrorAlloc;
+				break;
+			}
+			std::vector<double> hx((size_t)n * nt), hy((size_t)n * nt);
+			for (size_t i = 0; i < hx.size(); i++) { hx[i] = h_a[i]; hy[i] = h_b[i]; }
+			if (cudaMemcpy(d0.p, hx.data(), hx.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+			    cudaMemcpy(d1.p, hy.data(), hy.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess) {
+				rc = kHaErrorInternal;
+				break;
+			}
+			k_split3_vertex_major<<<64, kBlock, 0, st>>>(d0.p, nt, n, ntp, Xb.p);
+			k_split3_vertex_major<<<64, kBlock, 0, st>>>(d1.p, nt, n, ntp, Yb.p);
+			a.Xb = Xb.p; a.Yb = Yb.p; a.vplane = vplane; a.ntp = ntp; a.sl_idx = sl.p;
+			{ HA_LAUNCH(kHaB200KTcXcov, st); k_tc_gemm<kTcPhaseXcov><<<grid, kTcThreads, a.smem_bytes, st>>>(a); }
+			std::vector<float> full((size_t)np * np);
+			if (cudaGetLastError() != cudaSuccess ||
+			    cudaMemcpy(full.data(), A32.p, full.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess) {
+				rc = kHaErrorInternal;
+				break;
+			}
+			for (int r = 0; r < n; r++)
+				for (int c = 0; c < n; c++) h_out[(size_t)r * n + c] = full[(size_t)r * np + c];
+		} else {
+			if (in0.ensure((size_t)n * n) || in1.ensure((size_t)n * n)) {
+				rc = kHaErrorAlloc;
+				break;
+			}
+			if (cudaMemcpy(in0.p, h_a, (size_t)n * n * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+				rc = kHaErrorInternal;
+				break;
+			}
+			k_tc_pack<<<64, kBlock, 0, st>>>(in0.p, n, np, Xp.p);
+			if (which == 0) {
+				a.c1 = 0.f;
+				a.c3 = 1.f;  // P = X^T X
+				{ HA_LAUNCH(kHaB200KTcNs, st); k_tc_gemm<kTcPhaseGram><<<grid, kTcThreads, a.smem_bytes, st>>>(a); }
+				k_tc_unpack<<<64, kBlock, 0, st>>>(Pp.p, n, np, T.p);
+			} else {
+				if (cudaMemcpy(in1.p, h_b, (size_t)n * n * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+					rc = kHaErrorInternal;
+					break;
+				}
+				k_tc_pack<<<64, kBlock, 0, st>>>(in1.p, n, np, Pp.p);
+				a.plain = 1;
+				a.tol_stop = 1e30f;  // residual 0 < tol: the update is final and writes T = X P
+				{ HA_LAUNCH(kHaB200KTcNs, st); k_tc_gemm<kTcPhaseUpdate><<<grid, kTcThreads, a.smem_bytes, st>>>(a); }
+			}
+			if (cudaGetLastError() != cudaSuccess ||
+			    cudaMemcpy(h_out, T.p, (size_t)n * n * 4, cudaMemcpyDeviceToHost) != cudaSuccess) {
+				rc = kHaErrorInternal;
+				break;
+			}
+		}
+		int32_t e = 0;
+		if (cudaMemcpy(&e, err.p, 4, cudaMemcpyDeviceToHost) != cudaSuccess) {
+			rc = kHaErrorInternal;
+			break;
+		}
+		if (e) {
+			fprintf(stderr, "ha_b200: tensor-core self-test: a pipeline wait timed out\n");
+			rc = kHaErrorInternal;
+		}
+	} while (false);
+	if (rc == kHaErrorInternal) fprintf(stderr, "ha_b200: tensor-core self-test failed: %s\n", cudaGetErrorString(cudaGetLastError()));
+	release_all();
+	return rc;
+}
+
 
 int ha_b200_plan_local_transforms(const HaB200Plan *P, int32_t first, int32_t n, float *out) {
 	std::lock_guard<std::recursive_mutex> lk(g_mu);

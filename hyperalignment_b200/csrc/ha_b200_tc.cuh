@@ -1,0 +1,654 @@
+// ha_b200_tc.cuh -- tensor-core (tcgen05) kernels: split-BF16 cross-covariance and the
+// Newton-Schulz polar iteration of the searchlight Procrustes solve.
+//
+// The reference forms A = X_sl^T Y_sl with cblas_dgemm and T = U V^T from dgesdd
+// (csrc/ha_searchlight.c:581-609).  Here T is the polar factor of A, computed by the scaled
+// Newton-Schulz iteration
+//     X_0 = A / u,   G_k = X_k^T X_k,   X_{k+1} = X_k (c1_k I + c3_k G_k),
+// (u >= sigma_max(A); c1 = 3a/2, c3 = -a^3/2 with a from a capped scaling schedule, a = 1 in the
+// final phase) on the 5th-generation tensor cores.  Every product runs in BF16 with FP32
+// accumulation in tensor memory, with each FP32 operand split exactly into three BF16 parts
+// (x = hi + mid + lo) and the six products hi*hi + hi*mid + mid*hi + mid*mid + hi*lo + lo*hi
+// accumulated: the result carries FP32 accuracy (the dropped terms are below 2^-32 relative).
+//
+// One CTA computes one 128-row tile of one searchlight's product: 128 threads stage K-slices of
+// 16 with cp.async into a ring of shared-memory stages (canonical no-swizzle core-matrix
+// layout: 8 rows x 16 bytes per core matrix), thread 0 issues tcgen05.mma (M = 128, N = the
+// searchlight's padded size, K = 16) into tensor memory and commits each stage to an mbarrier,
+// and the four warps read the accumulator back with tcgen05.ld for the epilogue.
+//
+// Storage of a searchlight's iterate X and of P = c1 I + c3 G in HBM: three bf16 planes of
+// np x np (np = n rounded up to 16), each in 8 x 8 core matrices, core (r, c) = rows 8r..8r+7,
+// columns 8c..8c+7 at element offset (r * np/8 + c) * 64, row-major inside (16 bytes a row).
+// The same bytes serve as a K-major operand (X in X P) and as an MN-major operand (X in X^T X,
+// P in X P), so no transposed copy exists.  Padding rows and columns are zero and stay zero.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "ha_b200_kernels.cuh"
+
+namespace hab200 {
+
+constexpr int kTcThreads = 128;
+constexpr int kTcMaxStages = 4;
+constexpr int kTcMaxNp = 512;                  // largest padded searchlight size (four 128-row tiles)
+constexpr int kTcResSlots = 16;                // residual partials per searchlight: tiles x warps
+constexpr uint64_t kTcWaitNs = 2000000000ull;  // a pipeline wait longer than 2 s is declared failed
+
+enum : int { kTcPhaseXcov = 0, kTcPhaseGram = 1, kTcPhaseUpdate = 2 };
+
+// One searchlight of the tensor-core solve.
+struct TcWork {
+	int32_t s;     // searchlight index
+	int32_t slot;  // index within the chunk (stats, state, residual slots)
+	int32_t n;     // size
+	int32_t np;    // n rounded up to 16
+	int32_t sofs;  // flat offset of the searchlight in sl_indices
+	int32_t pad_;
+	int64_t xofs;  // bf16 element offset of the iterate's three planes (3 np^2)
+	int64_t pofs;  // bf16 element offset of P's three planes
+	int64_t aofs;  // float element offset of A (np x np, row-major, leading dimension np)
+	int64_t tofs;  // float element offset of T in the T scratch (n x n)
+};
+
+struct TcTile {
+	int32_t w;  // work index
+	int32_t t;  // 128-row tile
+};
+
+// Per-searchlight iteration state; one copy is read and the other written by each update launch.
+struct TcState {
+	int32_t plain;  // the last update used the plain coefficients (a = 1)
+	int32_t done;   // T written; no further work
+	int32_t iters;  // iterations taken
+	int32_t conv;   // residual fell below the stop threshold
+	float res;      // ||G - I||_F / sqrt(n) of the last Gram product
+	float u;        // the upper bound of sigma_max(A) that X_0 was scaled by
+	float pad_[2];
+};
+
+struct TcArgs {
+	const TcWork *work;
+	const TcTile *tiles;
+	// cross-covariance: vertex-major bf16 planes [plane][nv][ntp], ntp = nt rounded up to 16
+	const __nv_bfloat16 *Xb;
+	const __nv_bfloat16 *Yb;
+	int64_t vplane;  // elements per vertex-major plane (nv * ntp)
+	int ntp;
+	const int32_t *sl_idx;
+	// Newton-Schulz
+	__nv_bfloat16 *Xp;  // iterate planes (offsets from TcWork::xofs)
+	__nv_bfloat16 *Pp;  // P planes (TcWork::pofs)
+	float *A32;         // cross-covariance (TcWork::aofs)
+	float *T;           // T scratch (TcWork::tofs)
+	int t_rowmajor;
+	const TcState *st_in;
+	TcState *st_out;
+	float *res_part;  // [slot][kTcResSlots]
+	float c1, c3;     // schedule coefficients of this iteration
+	int plain;        // c1 = 3/2, c3 = -1/2 exactly (convergence is only accepted on such an iteration)
+	int last;         // the iteration limit: this update is final for every searchlight
+	float tol_stop;   // stop once ||G - I||_F / sqrt(n) is below this (after one more update)
+	int smem_bytes;   // dynamic shared memory of the launch
+	int *err;         // set when a wait times out
+};
+
+// ---------------------------------------------------------------------------------------------
+// PTX wrappers
+// ---------------------------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+	return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+	asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+	uint32_t ok;
+	asm volatile(
+	    "{\n\t.reg .pred p;\n\t"
+	    "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+	    "selp.u32 %0, 1, 0, p;\n\t}"
+	    : "=r"(ok)
+	    : "r"(smem_u32(bar)), "r"(parity)
+	    : "memory");
+	return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+	uint64_t t;
+	asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+	return t;
+}
+
+// Bounded wait for phase `parity` of an mbarrier: false once kTcWaitNs have passed.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+	if (mbar_try_wait(bar, parity)) return true;
+	const uint64_t t0 = global_ns();
+	while (!mbar_try_wait(bar, parity))
+		if (global_ns() - t0 > kTcWaitNs) return false;
+	return true;
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, uint32_t src_bytes) {
+	asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_keep(int keep) {
+	// wait until at most `keep` groups are pending (immediate operand, so one branch per value)
+	if (keep <= 1)
+		asm volatile("cp.async.wait_group 1;" ::: "memory");
+	else if (keep == 2)
+		asm volatile("cp.async.wait_group 2;" ::: "memory");
+	else
+		asm volatile("cp.async.wait_group 3;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+	asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// Warp-wide: allocate `ncols` (power of two >= 32) tensor-memory columns; the base address is
+// written to shared memory at `dst`.
+__device__ __forceinline__ void tmem_alloc(uint32_t *dst, uint32_t ncols) {
+	asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst)), "r"(ncols)
+	             : "memory");
+	asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t base, uint32_t ncols) {
+	asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(base), "r"(ncols) : "memory");
+}
+
+// Shared-memory matrix descriptor, no swizzle: start address, leading byte offset (between
+// core matrices adjacent in K), stride byte offset (between core matrices adjacent in M/N),
+// descriptor version 1 (sm_100).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+	uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+	d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+	d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+	d |= (uint64_t)1 << 46;
+	return d;
+}
+
+// Instruction descriptor of kind::f16 with BF16 A and B and an FP32 accumulator.
+__host__ __device__ __forceinline__ uint32_t mma_idesc(int M, int N, int a_mn, int b_mn) {
+	return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)a_mn << 15) | ((uint32_t)b_mn << 16) |
+	       ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
+	asm volatile(
+	    "{\n\t.reg .pred p;\n\t"
+	    "setp.ne.b32 p, %4, 0;\n\t"
+	    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+	    "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+	    : "memory");
+}
+
+// Arrive on `bar` once every tcgen05.mma issued so far by this thread has completed.
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+	asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+	             : "memory");
+}
+
+// Warp-wide: 16 consecutive FP32 columns of this warp's 32 tensor-memory lanes (lane i of the
+// warp gets row 32 * (warp % 4) + i).
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+	uint32_t r[16];
+	asm volatile(
+	    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+	    "%15}, [%16];"
+	    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+	      "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+	    : "r"(taddr));
+	asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+	for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+// Exact three-way split of an FP32 value into BF16 parts: v = hi + mid + lo.
+__device__ __forceinline__ void split3(float v, __nv_bfloat16 &hi, __nv_bfloat16 &mid, __nv_bfloat16 &lo) {
+	hi = __float2bfloat16_rn(v);
+	const float r1 = v - __bfloat162float(hi);
+	mid = __float2bfloat16_rn(r1);
+	lo = __float2bfloat16_rn(r1 - __bfloat162float(mid));
+}
+
+// Eight consecutive FP32 values of one core-matrix row -> 16 bytes in each of the three planes.
+__device__ __forceinline__ void store_split8(const float *v, __nv_bfloat16 *p0, __nv_bfloat16 *p1,
+                                             __nv_bfloat16 *p2) {
+	__align__(16) __nv_bfloat16 h[8], m[8], l[8];
+#pragma unroll
+	for (int i = 0; i < 8; i++) split3(v[i], h[i], m[i], l[i]);
+	*reinterpret_cast<uint4 *>(p0) = *reinterpret_cast<const uint4 *>(h);
+	*reinterpret_cast<uint4 *>(p1) = *reinterpret_cast<const uint4 *>(m);
+	*reinterpret_cast<uint4 *>(p2) = *reinterpret_cast<const uint4 *>(l);
+}
+
+// Bytes of one pipeline stage for an N-column product: A (128 x 16) and B (N x 16), three planes each.
+__host__ __device__ __forceinline__ int tc_stage_bytes(int N) { return 3 * (128 * 16 * 2) + 3 * (N * 16 * 2); }
+
+// tensor-memory columns for an N-column FP32 accumulator
+__device__ __forceinline__ uint32_t tc_tmem_cols(int N) {
+	uint32_t c = 32;
+	while ((int)c < N) c <<= 1;
+	return c;
+}
+
+// ---------------------------------------------------------------------------------------------
+// stage loads
+// ---------------------------------------------------------------------------------------------
+// Stage layout (bytes): A plane p at p * 4096, B plane p at 12288 + p * 32 N.  Inside a plane,
+// core matrix (g, k) (g: 8-row group along M or N, k: which 8-element half of the K-slice) sits at
+// (g * 2 + k) * 128, so LBO = 128 and SBO = 256 for both operand majors.
+
+// Cross-covariance, K-slice ks: A core (mg, k) row r = Xb[sl[128 t + 8 mg + r]][16 ks + 8 k ..],
+// B core (ng, k) row r = Yb[sl[8 ng + r]][16 ks + 8 k ..]; rows past n are zero.
+__device__ __forceinline__ void tc_load_xcov(const TcArgs &a, const int32_t *s_sl, int n, int N, int t, int ks,
+                                             uint32_t stage) {
+	const int per_plane = 256 + 2 * N;
+	const int total = 3 * per_plane;
+	for (int c = threadIdx.x; c < total; c += kTcThreads) {
+		const int plane = c / per_plane;
+		int rem = c - plane * per_plane;
+		const bool isA = rem < 256;
+		if (!isA) rem -= 256;
+		const int core = rem >> 3, r = rem & 7;
+		const int g = core >> 1, k = core & 1;
+		const int row = isA ? (128 * t + 8 * g + r) : (8 * g + r);
+		const uint32_t dst = stage + (isA ? plane * 4096 : 12288 + plane * 32 * N) + core * 128 + r * 16;
+		const __nv_bfloat16 *base = (isA ? a.Xb : a.Yb) + (int64_t)plane * a.vplane;
+		const bool ok = row < n;
+		const __nv_bfloat16 *src = ok ? base + (int64_t)s_sl[row] * a.ntp + 16 * ks + 8 * k : base;
+		cp_async16(dst, src, ok ? 16u : 0u);
+	}
+}
+
+// Newton-Schulz products, K-slice ks of a searchlight with padded size np (npg = np / 8 core groups):
+//   Gram   (D = X^T X, rows p of tile t):  A core (mg, k) <- X core (2 ks + k, 16 t + mg)  [MN-major]
+//                                          B core (ng, k) <- X core (2 ks + k, ng)        [MN-major]
+//   update (D = X P,   rows i of tile t):  A core (mg, k) <- X core (16 t + mg, 2 ks + k) [K-major]
+//                                          B core (ng, k) <- P core (2 ks + k, ng)        [MN-major]
+template <int PHASE>
+__device__ __forceinline__ void tc_load_ns(const __nv_bfloat16 *Xs, const __nv_bfloat16 *Bs, int np, int t, int ks,
+                                           uint32_t stage) {
+	const int N = np, npg = np >> 3;
+	const int64_t plane_elems = (int64_t)np * np;
+	const int per_plane = 256 + 2 * N;
+	const int total = 3 * per_plane;
+	for (int c = threadIdx.x; c < total; c += kTcThreads) {
+		const int plane = c / per_plane;
+		int rem = c - plane * per_plane;
+		const bool isA = rem < 256;
+		if (!isA) rem -= 256;
+		const int core = rem >> 3, r = rem & 7;
+		const int g = core >> 1, k = core & 1;
+		int cr, cc;  // source core (row group, column group)
+		bool ok = true;
+		if (isA) {
+			if (PHASE == kTcPhaseGram) { cr = 2 * ks + k; cc = 16 * t + g; ok = cc < npg; }
+			else { cr = 16 * t + g; cc = 2 * ks + k; ok = cr < npg; }
+		} else {
+			cr = 2 * ks + k;
+			cc = g;
+		}
+		const __nv_bfloat16 *src = (isA ? Xs : Bs) + plane * plane_elems;
+		if (ok) src += ((int64_t)cr * npg + cc) * 64 + r * 8;
+		const uint32_t dst = stage + (isA ? plane * 4096 : 12288 + plane * 32 * N) + core * 128 + r * 16;
+		cp_async16(dst, src, ok ? 16u : 0u);
+	}
+}
+
+// ---------------------------------------------------------------------------------------------
+// the tile-product kernel
+// ---------------------------------------------------------------------------------------------
+// PHASE kTcPhaseXcov:   A32 = X_sl^T Y_sl                       (K = time, padded to 16)
+// PHASE kTcPhaseGram:   P = c1 I + c3 X^T X, residual partials   (skips searchlights already done)
+// PHASE kTcPhaseUpdate: X <- X P, or T = X P for the final update (decided from the residual)
+template <int PHASE>
+__global__ void __launch_bounds__(kTcThreads) k_tc_gemm(const TcArgs a) {
+	extern __shared__ __align__(128) unsigned char tc_smem[];
+	__shared__ uint64_t s_bar[kTcMaxStages];
+	__shared__ uint64_t s_acc;
+	__shared__ uint32_t s_tmem;
+	__shared__ int s_fail;
+	__shared__ int32_t s_sl[PHASE == kTcPhaseXcov ? kTcMaxNp : 1];
+
+	const TcTile tl = a.tiles[blockIdx.x];
+	const TcWork w = a.work[tl.w];
+	const int n = w.n, np = w.np, t = tl.t;
+	const int N = np;
+	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+	const float c1 = a.c1, c3 = a.c3;
+	bool final_update = false;
+	if (PHASE != kTcPhaseXcov) {
+		const TcState st = a.st_in[w.slot];
+		if (st.done) {
+			if (PHASE == kTcPhaseUpdate && t == 0 && tid == 0) a.st_out[w.slot] = st;
+			return;
+		}
+		if (PHASE == kTcPhaseUpdate) {
+			// residual of this iteration's Gram product: fixed-order sum, identical in every tile CTA
+			double ss = 0.0;
+			for (int i = 0; i < kTcResSlots; i++) ss += (double)a.res_part[(int64_t)w.slot * kTcResSlots + i];
+			const float res = (float)sqrt(ss / (double)n);
+			const bool conv = a.plain && res < a.tol_stop;
+			final_update = conv || a.last;
+			if (t == 0 && tid == 0) {
+				TcState o = st;
+				o.iters = st.iters + 1;
+				o.res = res;
+				o.conv = conv ? 1 : 0;
+				o.done = final_update ? 1 : 0;
+				o.plain = a.plain;
+				a.st_out[w.slot] = o;
+			}
+		}
+	}
+
+	const int stage_bytes = tc_stage_bytes(N);
+	int S = a.smem_bytes / stage_bytes;
+	if (S > kTcMaxStages) S = kTcMaxStages;
+	const int nk = (PHASE == kTcPhaseXcov) ? (a.ntp >> 4) : (np >> 4);
+	const uint32_t ncols = tc_tmem_cols(N);
+	const uint32_t smem0 = smem_u32(tc_smem);
+
+	if (tid == 0) {
+		for (int i = 0; i < kTcMaxStages; i++) mbar_init(&s_bar[i], 1);
+		mbar_init(&s_acc, 1);
+		s_fail = (S < 2) ? 1 : 0;
+		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+	}
+	if (PHASE == kTcPhaseXcov)
+		for (int i = tid; i < n; i += kTcThreads) s_sl[i] = a.sl_idx[w.sofs + i];
+	if (warp == 0) tmem_alloc(&s_tmem, ncols);
+	tc_fence_before();
+	__syncthreads();
+	tc_fence_after();
+	const uint32_t tmem = s_tmem;
+	bool failed = s_fail != 0;
+
+	const __nv_bfloat16 *Xs = a.Xp + w.xofs;
+	const __nv_bfloat16 *Bs = (PHASE == kTcPhaseGram) ? Xs : (const __nv_bfloat16 *)(a.Pp + w.pofs);
+	auto load = [&](int ks, int s) {
+		const uint32_t stage = smem0 + s * stage_bytes;
+		if (PHASE == kTcPhaseXcov) tc_load_xcov(a, s_sl, n, N, t, ks, stage);
+		else tc_load_ns<PHASE>(Xs, Bs, np, t, ks, stage);
+	};
+
+	// operand majors: cross-covariance K/K, Gram MN/MN, update K/MN
+	const int a_mn = (PHASE == kTcPhaseGram) ? 1 : 0;
+	const int b_mn = (PHASE == kTcPhaseXcov) ? 0 : 1;
+	const int N0 = N > 256 ? 256 : N;
+	const uint32_t id0 = mma_idesc(128, N0, a_mn, b_mn);
+	const uint32_t id1 = N > 256 ? mma_idesc(128, N - 256, a_mn, b_mn) : 0u;
+
+	if (!failed) {
+		for (int j = 0; j < S - 1; j++) {
+			if (j < nk) load(j, j);
+			cp_async_commit();
+		}
+		for (int ks = 0; ks < nk; ks++) {
+			const int s = ks % S;
+			const int kn = ks + S - 1;
+			if (kn < nk) {
+				// stage kn % S was last read by the products of K-slice ks - 1
+				if (ks >= 1 && !mbar_wait(&s_bar[(ks - 1) % S], (uint32_t)(((ks - 1) / S) & 1))) s_fail = 1;
+				load(kn, kn % S);
+			}
+			cp_async_commit();
+			cp_async_wait_keep(S - 1);
+			fence_proxy_async_smem();
+			__syncthreads();
+			if (s_fail) { failed = true; break; }
+			if (tid == 0) {
+				tc_fence_after();
+				const uint32_t st = smem0 + s * stage_bytes;
+				// products in increasing size: lo*hi, hi*lo, mid*mid, mid*hi, hi*mid, hi*hi
+#pragma unroll
+				for (int q = 0; q < 6; q++) {
+					const int pa = (q == 0) ? 2 : (q == 2 || q == 3) ? 1 : 0;
+					const int pb = (q == 1) ? 2 : (q == 2 || q == 4) ? 1 : 0;
+					const uint32_t aaddr = st + pa * 4096;
+					const uint32_t baddr = st + 12288 + pb * 32 * N;
+					const uint32_t acc = (ks > 0 || q > 0) ? 1u : 0u;
+					const uint64_t ad = smem_desc(aaddr, 128, 256);
+					mma_bf16(tmem, ad, smem_desc(baddr, 128, 256), id0, acc);
+					if (N > 256) mma_bf16(tmem + 256, ad, smem_desc(baddr + 32 * 256, 128, 256), id1, acc);
+				}
+				mma_commit(&s_bar[s]);
+			}
+		}
+	}
+	cp_async_wait_all();
+	if (!failed) {
+		if (tid == 0) mma_commit(&s_acc);
+		if (!mbar_wait(&s_acc, 0)) s_fail = 1;
+	}
+	__syncthreads();
+	failed = failed || s_fail;
+	tc_fence_after();
+
+	if (!failed) {
+		// epilogue: row m of the tile = tensor-memory lane m; warp w owns lanes 32w..32w+31
+		const int m = 32 * warp + lane;
+		const int row = 128 * t + m;
+		const uint32_t trow = tmem + ((uint32_t)(32 * warp) << 16);
+		const int npg = np >> 3;
+		float res = 0.f;
+		for (int c0 = 0; c0 < N; c0 += 16) {
+			float v[16];
+			tmem_ld16(trow + (uint32_t)c0, v);
+			if (row >= np) continue;
+			if (PHASE == kTcPhaseXcov) {
+				if (row < n) {
+					float4 *dst = reinterpret_cast<float4 *>(a.A32 + w.aofs + (int64_t)row * np + c0);
+#pragma unroll
+					for (int q = 0; q < 4; q++) dst[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+				}
+			} else if (PHASE == kTcPhaseGram) {
+#pragma unroll
+				for (int q = 0; q < 16; q++) {
+					const int col = c0 + q;
+					const float g = v[q];
+					if (row < n && col < n) {
+						const float d = g - (col == row ? 1.f : 0.f);
+						res += d * d;
+					}
+					v[q] = c3 * g + (col == row ? c1 : 0.f);
+				}
+				__nv_bfloat16 *P0 = a.Pp + w.pofs;
+				const int64_t pe = (int64_t)np * np;
+#pragma unroll
+				for (int h = 0; h < 2; h++) {
+					const int64_t o = ((int64_t)(row >> 3) * npg + (c0 >> 3) + h) * 64 + (row & 7) * 8;
+					store_split8(v + 8 * h, P0 + o, P0 + pe + o, P0 + 2 * pe + o);
+				}
+			} else {
+				if (final_update) {
+					if (row < n) {
+						float *T = a.T + w.tofs;
+						for (int q = 0; q < 16; q++) {
+							const int col = c0 + q;
+							if (col < n) T[a.t_rowmajor ? (int64_t)row * n + col : (int64_t)col * n + row] = v[q];
+						}
+					}
+				} else {
+					__nv_bfloat16 *X0 = a.Xp + w.xofs;
+					const int64_t pe = (int64_t)np * np;
+#pragma unroll
+					for (int h = 0; h < 2; h++) {
+						const int64_t o = ((int64_t)(row >> 3) * npg + (c0 >> 3) + h) * 64 + (row & 7) * 8;
+						store_split8(v + 8 * h, X0 + o, X0 + pe + o, X0 + 2 * pe + o);
+					}
+				}
+			}
+		}
+		if (PHASE == kTcPhaseGram) {
+			res = warp_sum(res);
+			if (lane == 0) a.res_part[(int64_t)w.slot * kTcResSlots + t * 4 + warp] = res;
+		}
+	} else if (tid == 0) {
+		atomicOr(a.err, 1);
+	}
+	tc_fence_before();
+	__syncthreads();
+	if (warp == 0) tmem_dealloc(tmem, ncols);
+}
+
+// ---------------------------------------------------------------------------------------------
+// SIMT helpers of the tensor-core solve
+// ---------------------------------------------------------------------------------------------
+
+// float64 column-major [v][nt] -> three bf16 planes [plane][v][ntp] (exact split of the value rounded
+// to FP32; samples past nt are zero).
+__global__ void k_split3_vertex_major(const double *__restrict__ X, int nt, int nv, int ntp,
+                                      __nv_bfloat16 *__restrict__ out) {
+	const int64_t total = (int64_t)nv * ntp;
+	for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+		const int64_t v = e / ntp;
+		const int t = (int)(e - v * ntp);
+		const float x = (t < nt) ? (float)X[v * nt + t] : 0.f;
+		__nv_bfloat16 h, m, l;
+		split3(x, h, m, l);
+		out[e] = h;
+		out[total + e] = m;
+		out[2 * total + e] = l;
+	}
+}
+
+// X_0 = A / u with u = min(||A||_F, sqrt(||A||_1 ||A||_inf)) >= sigma_max(A), written as the three
+// core-tiled planes (np x np, padding zero); iteration state and residual slots cleared.
+__global__ void __launch_bounds__(256) k_tc_ns_init(const TcWork *__restrict__ work, const float *__restrict__ A32,
+                                                    __nv_bfloat16 *__restrict__ Xp, TcState *__restrict__ st,
+                                                    float *__restrict__ res_part) {
+	const TcWork w = work[blockIdx.x];
+	const int n = w.n, np = w.np, npg = np >> 3;
+	const float *A = A32 + w.aofs;
+	__shared__ double s_red[2][8];
+	__shared__ float s_colsum[kTcMaxNp];
+	__shared__ float s_u;
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	double fro = 0.0, rowmax = 0.0;
+	for (int r = warp; r < n; r += 8) {
+		double rs = 0.0;
+		for (int c = lane; c < n; c += 32) {
+			const double x = A[(int64_t)r * np + c];
+			fro += x * x;
+			rs += fabs(x);
+		}
+		rs = warp_sum(rs);
+		rowmax = fmax(rowmax, rs);
+	}
+	for (int c = threadIdx.x; c < n; c += blockDim.x) {
+		float cs = 0.f;
+		for (int r = 0; r < n; r++) cs += fabsf(A[(int64_t)r * np + c]);
+		s_colsum[c] = cs;
+	}
+	fro = warp_sum(fro);
+	if (lane == 0) { s_red[0][warp] = fro; s_red[1][warp] = rowmax; }
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		double f = 0.0, rm = 0.0, cm = 0.0;
+		for (int i = 0; i < 8; i++) { f += s_red[0][i]; rm = fmax(rm, s_red[1][i]); }
+		for (int c = 0; c < n; c++) cm = fmax(cm, (double)s_colsum[c]);
+		double u = fmin(sqrt(f), sqrt(rm * cm));
+		if (!(u > 0.0)) u = 1.0;  // zero matrix: the iterate stays zero and the solve is flagged
+		s_u = (float)(u * (1.0 + 1e-6));
+		TcState z = {};
+		z.u = s_u;
+		st[w.slot] = z;
+	}
+	for (int i = threadIdx.x; i < kTcResSlots; i += blockDim.x) res_part[(int64_t)w.slot * kTcResSlots + i] = 0.f;
+	__syncthreads();
+	const float inv = 1.f / s_u;
+	const int64_t pe = (int64_t)np * np;
+	__nv_bfloat16 *X0 = Xp + w.xofs;
+	// one thread per core-matrix row (8 elements)
+	const int64_t chunks = (int64_t)np * npg;
+	for (int64_t e = threadIdx.x; e < chunks; e += blockDim.x) {
+		const int row = (int)(e / npg), cg = (int)(e - (int64_t)row * npg);
+		float v[8];
+#pragma unroll
+		for (int q = 0; q < 8; q++) {
+			const int col = 8 * cg + q;
+			v[q] = (row < n && col < n) ? A[(int64_t)row * np + col] * inv : 0.f;
+		}
+		const int64_t o = ((int64_t)(row >> 3) * npg + cg) * 64 + (row & 7) * 8;
+		store_split8(v, X0 + o, X0 + pe + o, X0 + 2 * pe + o);
+	}
+}
+
+// After the iteration: sum of singular values = trace(T^T A) (the scaling numerator,
+// csrc/ha_searchlight.c:635-656), iteration count, and the flag that hands unconverged
+// searchlights (exactly singular ones keep a zero singular value that the iteration cannot
+// complete) to the float64 Jacobi re-solve.
+__global__ void __launch_bounds__(256) k_tc_ns_finish(const TcWork *__restrict__ work, const float *__restrict__ A32,
+                                                      const float *__restrict__ Tscr, const TcState *__restrict__ st,
+                                                      SlStats *__restrict__ stats, int t_rowmajor) {
+	const TcWork w = work[blockIdx.x];
+	const int n = w.n, np = w.np;
+	const float *A = A32 + w.aofs;
+	const float *T = Tscr + w.tofs;
+	double s = 0.0;
+	for (int64_t e = threadIdx.x; e < (int64_t)n * n; e += blockDim.x) {
+		const int r = (int)(e / n), c = (int)(e - (int64_t)r * n);
+		const float tv = t_rowmajor ? T[(int64_t)r * n + c] : T[(int64_t)c * n + r];
+		s += (double)tv * (double)A[(int64_t)r * np + c];
+	}
+	s = warp_sum(s);
+	__shared__ double red[8];
+	if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		double tot = 0.0;
+		for (int i = 0; i < (int)(blockDim.x >> 5); i++) tot += red[i];
+		const TcState z = st[w.slot];
+		SlStats o = {};
+		o.s_sum = tot;
+		o.s_max = (double)z.u;
+		o.s_min = 0.0;
+		o.k_min = 0;
+		o.sweeps = z.iters;
+		o.flags = z.conv ? 0 : kFlagIllCond;
+		stats[w.slot] = o;
+	}
+}
+
+// Row-major FP32 n x n (leading dimension n) -> three core-tiled bf16 planes of np x np; unpack
+// reverses it (hi + mid + lo).  Used by the product self-test.
+__global__ void k_tc_pack(const float *__restrict__ M, int n, int np, __nv_bfloat16 *__restrict__ planes) {
+	const int npg = np >> 3;
+	const int64_t pe = (int64_t)np * np;
+	for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < (int64_t)np * npg; e += (int64_t)gridDim.x * blockDim.x) {
+		const int row = (int)(e / npg), cg = (int)(e - (int64_t)row * npg);
+		float v[8];
+		for (int q = 0; q < 8; q++) {
+			const int col = 8 * cg + q;
+			v[q] = (row < n && col < n) ? M[(int64_t)row * n + col] : 0.f;
+		}
+		const int64_t o = ((int64_t)(row >> 3) * npg + cg) * 64 + (row & 7) * 8;
+		store_split8(v, planes + o, planes + pe + o, planes + 2 * pe + o);
+	}
+}
+__global__ void k_tc_unpack(const __nv_bfloat16 *__restrict__ planes, int n, int np, float *__restrict__ M) {
+	const int npg = np >> 3;
+	const int64_t pe = (int64_t)np * np;
+	for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < (int64_t)n * n; e += (int64_t)gridDim.x * blockDim.x) {
+		const int row = (int)(e / n), col = (int)(e - (int64_t)row * n);
+		const int64_t o = ((int64_t)(row >> 3) * npg + (col >> 3)) * 64 + (row & 7) * 8 + (col & 7);
+		M[e] = __bfloat162float(planes[o]) + __bfloat162float(planes[pe + o]) + __bfloat162float(planes[2 * pe + o]);
+	}
+}
+
+}  // namespace hab200

@@ -245,6 +245,10 @@ enum {
 	                           with sigma_min / sigma_max < 5e-5 (environment HA_B200_ILL_RATIO overrides) */
 	kHaB200SolverFP32  = 1, /* plain FP32 form: FP32 Jacobi only, no refinement, no FP64 re-solve */
 	kHaB200SolverFP64  = 2, /* every searchlight in FP64 */
+	kHaB200SolverTC    = 3, /* tensor cores: split-BF16 (three parts, six products, FP32 accuracy)
+	                           cross-covariance and Newton-Schulz polar iteration; searchlights whose
+	                           iteration does not converge (exactly singular A) are re-solved by FP64
+	                           Jacobi.  Needs isReflection; without it the mixed solver runs. */
 };
 
 /*
@@ -425,7 +429,9 @@ enum {
 	kHaB200KGrid = 14,      /* ridge grid: per-model products and grid evaluation */
 	kHaB200KMlp = 15,       /* learned proposal: training and inference */
 	kHaB200KEval = 16,      /* vertex-wise correlation of aligned data with a target */
-	kHaB200NumKernelKinds = 17,
+	kHaB200KTcXcov = 17,    /* cross-covariance on the tensor cores (split BF16) */
+	kHaB200KTcNs = 18,      /* Newton-Schulz polar iteration on the tensor cores */
+	kHaB200NumKernelKinds = 19,
 };
 
 /*
@@ -439,6 +445,15 @@ void ha_b200_set_kernel_timing(bool on);
 int ha_b200_kernel_times(double *ms, int64_t *launches);
 /* Kernels launched by this library since it was loaded. */
 int64_t ha_b200_launch_count(void);
+
+/*
+ * Diagnostic: one tensor-core product of the Newton-Schulz solver's kernels on host data, FP32
+ * row-major n x n output (n <= 512).  which 0: h_a^T h_a (h_a row-major n x n); which 1:
+ * h_a h_b (both row-major n x n); which 2: the cross-covariance h_a h_b^T of two n x nt
+ * vertex-major matrices (h_a[j * nt + t], vertex j's series contiguous).  Checks the operand
+ * layouts of every product type.
+ */
+int ha_b200_tc_selftest(int32_t which, int32_t n, int32_t nt, const float *h_a, const float *h_b, float *h_out);
 
 #ifdef __cplusplus
 }

@@ -42,7 +42,15 @@ from hyperalignment_b200 import workloads as W  # noqa: E402
 from oracle import ha_oracle as O  # noqa: E402
 from oracle import ref_lib as R  # noqa: E402
 
-REF_DIR = os.environ.get("HA_REFERENCE_DIR", "/root/reference")
+def _reference_dir():
+    """HA_REFERENCE_DIR, else a checkout named "reference" beside this repository."""
+    for cand in (os.environ.get("HA_REFERENCE_DIR"), os.path.join(os.path.dirname(ROOT), "reference")):
+        if cand and os.path.isdir(os.path.join(cand, "src", "hyperalignment")):
+            return os.path.abspath(cand)
+    raise SystemExit("make_golden.py: set HA_REFERENCE_DIR to the neurolabusc/hyperalignment checkout")
+
+
+REF_DIR = _reference_dir()
 
 
 def small_inputs(seed=0):

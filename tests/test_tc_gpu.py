@@ -1,0 +1,140 @@
+"""GPU parity of the tensor-core solver (kHaB200SolverTC) through the C ABI.
+
+Tolerances (written per test):
+  * one tensor-core product (split BF16, six products, FP32 accumulation) vs float64:
+    relative Frobenius <= 2e-6
+  * per-searchlight transform T_s vs the float64 oracle: relative Frobenius <= 1e-5
+    (the metric's bound is 1e-4; the three-part split carries FP32 accuracy)
+  * dense results vs the reference float64 / float32 CPU backends: relative Frobenius and
+    max-abs <= 1e-5
+  * repeated runs: bitwise identical
+"""
+
+import numpy as np
+import pytest
+
+from conftest import golden
+from hyperalignment_b200 import _lib as L
+from hyperalignment_b200 import workloads as W
+from hyperalignment_b200.plan import Plan
+from oracle import ha_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+PROD_REL = 2e-6
+T_REL_TC = 1e-5
+GLOBAL_REL = 1e-5
+
+
+def relf(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def selftest(hlib, which, n, a, b=None, nt=0):
+    out = np.zeros((n, n), dtype=np.float32)
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    b = None if b is None else np.ascontiguousarray(b, dtype=np.float32)
+    fp = L.c_float_p
+    rc = hlib.ha_b200_tc_selftest(which, n, nt, a.ctypes.data_as(fp),
+                                  None if b is None else b.ctypes.data_as(fp), out.ctypes.data_as(fp))
+    assert rc == 0
+    return out.astype(np.float64)
+
+
+@pytest.mark.parametrize("n", [16, 40, 100, 128, 144, 200, 256, 272, 304, 400, 512])
+def test_tc_products(gpu, hlib, n):
+    """Each product type of the solver on one matrix: X^T X (MN-major A and B), X M (K-major A,
+    MN-major B), and the gathered cross-covariance (K-major A and B, K = time)."""
+    rng = np.random.default_rng(n)
+    X = rng.standard_normal((n, n)).astype(np.float32)
+    M = rng.standard_normal((n, n)).astype(np.float32)
+    x64, m64 = X.astype(np.float64), M.astype(np.float64)
+    assert relf(selftest(hlib, 0, n, X), x64.T @ x64) <= PROD_REL
+    assert relf(selftest(hlib, 1, n, X, M), x64 @ m64) <= PROD_REL
+    nt = 200 + (n % 3) * 7  # time length not a multiple of 16
+    A = rng.standard_normal((n, nt)).astype(np.float32)  # vertex-major: row j = vertex j's series
+    B = rng.standard_normal((n, nt)).astype(np.float32)
+    got = selftest(hlib, 2, n, A, B, nt=nt)
+    assert relf(got, A.astype(np.float64) @ B.astype(np.float64).T) <= PROD_REL
+
+
+def _device_run(w, solver, refl=True, scal=False, out_kind=L.OUT_CSR):
+    import torch
+    plan = Plan.from_workload(w)
+    dX = torch.from_numpy(np.asfortranarray(w.X).ravel(order="F")).cuda()
+    dY = torch.from_numpy(np.asfortranarray(w.Y).ravel(order="F")).cuda()
+    vals = torch.zeros(plan.nnz, dtype=torch.float64, device="cuda")
+    plan.procrustes_device(dX.data_ptr(), dY.data_ptr(), vals.data_ptr(), refl, scal, solver, out_kind)
+    torch.cuda.synchronize()
+    return plan, vals.cpu().numpy()
+
+
+@pytest.mark.parametrize("lo,hi", [(1, 12), (60, 90), (150, 240), (250, 300), (300, 420), (481, 512)])
+def test_tc_local_transforms_vs_fp64(gpu, lo, hi):
+    """Per-searchlight T_s of the tensor-core solver against the float64 oracle, across one to four
+    128-row tiles and both size classes."""
+    nv = 642 if hi <= 240 else 1442
+    w = W.small_case(seed=11, nv=nv, nt=max(2 * hi, 40), lo=lo, hi=hi)
+    count = min(w.sls.count, 24)
+    w.sls = w.sls.subset(np.arange(count))
+    plan, _ = _device_run(w, L.SOLVER_TC)
+    Ts = plan.local_transforms(0, count)
+    worst = 0.0
+    for q in range(count):
+        sl = w.sls.indices[w.sls.offsets[q]:w.sls.offsets[q + 1]]
+        worst = max(worst, relf(Ts[q], O.procrustes(w.X[:, sl], w.Y[:, sl])))
+    assert worst <= T_REL_TC, worst
+    assert plan.stats()["n_fp64"] == 0
+
+
+@pytest.mark.parametrize("key,weighted", [("T_cpu64", True), ("T_cpu64_uniform", False)])
+def test_tc_dense_matches_reference_golden(gpu, key, weighted):
+    g = golden("small_dense.npz")
+    w = W.Workload("golden", g["X"], g["Y"],
+                   W.Searchlights(g["idx"], g["off"], g["dists"] if weighted else None, float(g["radius"]),
+                                  g["X"].shape[1]), True, False)
+    plan, csr = _device_run(w, L.SOLVER_TC)
+    indptr, indices = plan.pattern()
+    ref = O.dense_to_csr_values(g[key], indptr, indices)
+    assert relf(csr, ref) <= GLOBAL_REL
+    assert np.abs(csr - ref).max() <= GLOBAL_REL
+    if key == "T_cpu64":
+        assert relf(csr, O.dense_to_csr_values(g["T_cpu32"], indptr, indices)) <= GLOBAL_REL
+
+
+def test_tc_scaling_vs_oracle(gpu):
+    w = W.small_case(seed=21, nv=642, nt=120, lo=30, hi=80, scaling=True)
+    s = w.sls
+    plan, csr = _device_run(w, L.SOLVER_TC, scal=True)
+    indptr, indices = plan.pattern()
+    Tref = O.searchlight_procrustes_dense(w.X, w.Y, s.indices, s.offsets, s.dists, s.radius, True, True)
+    assert relf(csr, O.dense_to_csr_values(Tref, indptr, indices)) <= GLOBAL_REL
+
+
+def test_tc_is_deterministic(gpu):
+    w = W.small_case(seed=3, nv=642, nt=60, lo=20, hi=60)
+    _, a = _device_run(w, L.SOLVER_TC)
+    _, b = _device_run(w, L.SOLVER_TC)
+    assert a.tobytes() == b.tobytes()
+
+
+def test_tc_rank_deficient_searchlights(gpu):
+    """Exactly singular A keeps a zero singular value the iteration cannot complete: those
+    searchlights go to the float64 re-solve; X @ T and T on the row space of A are unique."""
+    w = W.small_case(seed=9, nv=642, nt=100, lo=30, hi=60)
+    mask = W.duplicate_columns(w.X, w.sls, 0.5, np.random.default_rng(1))
+    assert mask.sum() > 0
+    plan, _ = _device_run(w, L.SOLVER_TC)
+    Ts = plan.local_transforms(0, w.sls.count)
+    worst = 0.0
+    for q in np.flatnonzero(mask)[:40]:
+        sl = w.sls.indices[w.sls.offsets[q]:w.sls.offsets[q + 1]]
+        Xs = w.X[:, sl]
+        Tref = O.procrustes(Xs, w.Y[:, sl])
+        worst = max(worst, relf(Xs @ Ts[q], Xs @ Tref))
+        _, sv, Vt = np.linalg.svd(Xs.T @ w.Y[:, sl])
+        Vp = Vt[sv > sv[0] * 1e-9].T
+        worst = max(worst, relf(Ts[q] @ Vp @ Vp.T, Tref @ Vp @ Vp.T))
+        assert np.abs(Ts[q].T @ Ts[q] - np.eye(sl.size)).max() < 1e-4
+    assert worst <= 1e-4, worst
+    assert plan.stats()["n_fp64"] >= 1
