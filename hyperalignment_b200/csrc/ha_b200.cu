@@ -916,7 +916,8 @@ int run_procrustes_tc(HaB200Plan *P, const double *d_X, const double *d_Y, bool 
 		}
 		{ HA_LAUNCH(kHaB200KTcNs, st); k_tc_ns_finish<<<nsl, 256, 0, st>>>(ch.d_tcw, P->tcA.p, T, P->tcSt.p + (size_t)(maxit & 1) * P->max_slots,
 		                                                              P->stats.p, rowmajor); }
-		// float64 Jacobi re-solve of the flagged searchlights (cold start)
+		{ HA_LAUNCH(kHaB200KTcNs, st); k_tc_complete<<<nsl, 256, 0, st>>>(ch.d_tcw, T, P->tcXp.p, P->tcPp.p, P->stats.p, rowmajor); }
+		// float64 Jacobi re-solve of the searchlights still flagged (cold start)
 		{
 			JacobiParams jp;
 			jp.max_sweeps = 40;
@@ -1735,7 +1736,7 @@ int dense_impl(const double *X, const double *Y, int32_t nt, int32_t nv, const i
 	if ((rc = upload_inputs(X, Y, nt, nv, col_major, &dX, &dY, st)) != kHaSuccess) return rc;
 	if ((rc = g_bufs.vals.ensure((size_t)P->nnz)) != kHaSuccess) return rc;
 	HA_CUDA(cudaMemsetAsync(g_bufs.vals.p, 0, (size_t)P->nnz * 8, st));
-	if ((rc = run_procrustes(P, dX, dY, refl, scal, kHaB200SolverMixed, kHaB200OutCSR, g_bufs.vals.p, st)) != kHaSuccess)
+	if ((rc = run_procrustes(P, dX, dY, refl, scal, kHaB200SolverTC, kHaB200OutCSR, g_bufs.vals.p, st)) != kHaSuccess)
 		return rc;
 	g_bufs.h_vals.resize((size_t)P->nnz);
 	HA_CUDA(cudaMemcpyAsync(g_bufs.h_vals.data(), g_bufs.vals.p, (size_t)P->nnz * 8, cudaMemcpyDeviceToHost, st));
@@ -1798,7 +1799,7 @@ int csc_impl(const double *X, const double *Y, int32_t nt, int32_t nv, const int
 	if (ridge)
 		rc = ha_b200_plan_ridge_device(P, dX, dY, alpha, kHaB200OutCSC, g_bufs.vals.p, st);
 	else
-		rc = run_procrustes(P, dX, dY, refl, scal, kHaB200SolverMixed, kHaB200OutCSC, g_bufs.vals.p, st);
+		rc = run_procrustes(P, dX, dY, refl, scal, kHaB200SolverTC, kHaB200OutCSC, g_bufs.vals.p, st);
 	if (rc != kHaSuccess) return rc;
 	g_bufs.h_vals.resize((size_t)P->nnz);
 	HA_CUDA(cudaMemcpyAsync(g_bufs.h_vals.data(), g_bufs.vals.p, (size_t)P->nnz * 8, cudaMemcpyDeviceToHost, st));
@@ -1886,7 +1887,7 @@ int template_impl(const double *dms, int ns, int nt, int nv, const int32_t *idx,
 	// aligned_s = X_s @ SL(X_s -> target)
 	auto align = [&](int s, const double *target) -> int {
 		if (cudaMemsetAsync(vals.p, 0, (size_t)P->nnz * 8, st) != cudaSuccess) return kHaErrorInternal;
-		int r = run_procrustes(P, D.p + m * s, target, refl, scal, kHaB200SolverMixed, kHaB200OutCSC, vals.p, st);
+		int r = run_procrustes(P, D.p + m * s, target, refl, scal, kHaB200SolverTC, kHaB200OutCSC, vals.p, st);
 		if (r != kHaSuccess) return r;
 		k_spmm_csc<<<nv, 128, 0, st>>>(D.p + m * s, nt, nv, P->patptr.p, P->patcol.p, vals.p, A.p + m * s);
 		return cudaGetLastError() == cudaSuccess ? kHaSuccess : kHaErrorInternal;

@@ -69,7 +69,7 @@ struct SlStats {
 	int32_t ncols;    // eigenvector mode: the nonzero columns of A lead and number ncols (0: all)
 };
 
-enum : int32_t { kFlagUnconverged = 1, kFlagIllCond = 2, kFlagReflected = 4, kFlagFP64 = 8 };
+enum : int32_t { kFlagUnconverged = 1, kFlagIllCond = 2, kFlagReflected = 4, kFlagFP64 = 8, kFlagCompleted = 16 };
 
 // ---------------------------------------------------------------------------------------------
 // layout conversion

@@ -65,9 +65,10 @@ struct TcState {
 	int32_t done;   // T written; no further work
 	int32_t iters;  // iterations taken
 	int32_t conv;   // residual fell below the stop threshold
-	float res;      // ||G - I||_F / sqrt(n) of the last Gram product
-	float u;        // the upper bound of sigma_max(A) that X_0 was scaled by
-	float pad_[2];
+	float res;        // ||G - I||_F / sqrt(n) of the last Gram product
+	float u;          // the upper bound of sigma_max(A) that X_0 was scaled by
+	int32_t stalled;  // plain steps stopped changing the residual: some singular values stay zero
+	float pad_;
 };
 
 struct TcArgs {
@@ -341,14 +342,22 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_gemm(const TcArgs a) {
 			// residual of this iteration's Gram product: fixed-order sum, identical in every tile CTA
 			double ss = 0.0;
 			for (int i = 0; i < kTcResSlots; i++) ss += (double)a.res_part[(int64_t)w.slot * kTcResSlots + i];
-			const float res = (float)sqrt(ss / (double)n);
+			const double resd = sqrt(ss / (double)n);
+			const float res = (float)resd;
 			const bool conv = a.plain && res < a.tol_stop;
-			final_update = conv || a.last;
+			// A plain step multiplies every singular value sigma < 1 by about 3/2, which changes the
+			// residual by about 2.5 sigma^2 / (n res^2) relative; a residual that a plain step leaves
+			// unchanged to 5e-7 relative belongs to singular values below ~1e-3 after the schedule's
+			// growth, i.e. below the FP32 resolution of A (exact zeros for duplicated or zero vertex
+			// columns): stop here and let the completion kernel fill them.
+			const bool stalled = !conv && a.plain && st.plain && fabs(resd - (double)st.res) <= 5e-7 * resd;
+			final_update = conv || stalled || a.last;
 			if (t == 0 && tid == 0) {
 				TcState o = st;
 				o.iters = st.iters + 1;
 				o.res = res;
 				o.conv = conv ? 1 : 0;
+				o.stalled = stalled ? 1 : 0;
 				o.done = final_update ? 1 : 0;
 				o.plain = a.plain;
 				a.st_out[w.slot] = o;
@@ -622,6 +631,166 @@ __global__ void __launch_bounds__(256) k_tc_ns_finish(const TcWork *__restrict__
 		o.sweeps = z.iters;
 		o.flags = z.conv ? 0 : kFlagIllCond;
 		stats[w.slot] = o;
+	}
+}
+
+// ---------------------------------------------------------------------------------------------
+// completion of exactly singular searchlights
+// ---------------------------------------------------------------------------------------------
+// A searchlight whose iteration stalled ends with T = U_r V_r^T (its converged directions) and
+// d singular values that stay exactly zero (A singular: duplicated or zero vertex columns).  The
+// reference's SVD completes such a T with an arbitrary orthonormal pairing of the null spaces
+// (only T on the row space of A, and X T, are unique); here: E = I - T^T T and F = I - T T^T are
+// the projectors onto the right and left null spaces, pivoted Cholesky (stopping at pivots below
+// 1e-4, the level of the converged directions' residue) gives their bases L_E, L_F, which must be
+// orthonormal already (L^T L = I to 1e-3: the extracted directions are fully null, not partly
+// converged), Gram-Schmidt cleans them, and T <- (I - U_0 U_0^T) T + U_0 V_0^T.  Searchlights that
+// fail a check keep kFlagIllCond and go to the float64 re-solve.  E and F use the searchlight's
+// P and iterate planes (free after the iteration) as FP32 scratch.
+constexpr int kTcNullMax = 8;
+
+__device__ __forceinline__ float block_sum256(float v, float *red) {
+	v = warp_sum(v);
+	__syncthreads();
+	if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+	__syncthreads();
+	float t = 0.f;
+	for (int i = 0; i < 8; i++) t += red[i];
+	return t;
+}
+
+__global__ void __launch_bounds__(256) k_tc_complete(const TcWork *__restrict__ work, float *__restrict__ Tscr,
+                                                     __nv_bfloat16 *__restrict__ Xp, __nv_bfloat16 *__restrict__ Pp,
+                                                     SlStats *__restrict__ stats, int t_rowmajor) {
+	const TcWork w = work[blockIdx.x];
+	if (!(stats[w.slot].flags & kFlagIllCond)) return;
+	const int n = w.n;
+	float *T = Tscr + w.tofs;
+	float *E = reinterpret_cast<float *>(Pp + w.pofs);
+	float *F = reinterpret_cast<float *>(Xp + w.xofs);
+	const int64_t ti = t_rowmajor ? n : 1, tj = t_rowmajor ? 1 : n;  // T(i, j) = T[i ti + j tj]
+	__shared__ float ps[16][65], qs[16][65];
+	__shared__ float Lv[2][kTcNullMax][kTcMaxNp];
+	__shared__ float red[8];
+	__shared__ float s_best;
+	__shared__ int s_piv, s_d[2], s_bad;
+	GemmArgs<float> g;
+	g.M = n; g.N = n; g.K = n;
+	g.d = nullptr; g.alpha = -1.f;
+	g.E = nullptr; g.ei = 0; g.ej = 0; g.beta = 0.f;
+	g.ci = n; g.cj = 1;
+	// E(i, j) = delta - sum_k T(k, i) T(k, j);  F(i, j) = delta - sum_k T(i, k) T(j, k)
+	g.P = T; g.pk = ti; g.pi = tj; g.Q = T; g.qk = ti; g.qj = tj; g.C = E;
+	block_gemm(g, ps, qs);
+	g.P = T; g.pk = tj; g.pi = ti; g.Q = T; g.qk = tj; g.qj = ti; g.C = F;
+	block_gemm(g, ps, qs);
+	for (int i = threadIdx.x; i < n; i += blockDim.x) {
+		E[(int64_t)i * n + i] += 1.f;
+		F[(int64_t)i * n + i] += 1.f;
+	}
+	if (threadIdx.x == 0) s_bad = 0;
+	__syncthreads();
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	for (int m = 0; m < 2; m++) {
+		float *M = m ? F : E;
+		int d = 0;
+		for (;;) {
+			// largest remaining diagonal entry (first index on ties)
+			float best = -1.f;
+			int bi = 0;
+			for (int i = threadIdx.x; i < n; i += blockDim.x) {
+				const float v = M[(int64_t)i * n + i];
+				if (v > best) { best = v; bi = i; }
+			}
+			for (int o = 16; o > 0; o >>= 1) {
+				const float ob = __shfl_xor_sync(0xffffffffu, best, o);
+				const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+				if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+			}
+			__syncthreads();
+			if (lane == 0) { red[warp] = best; reinterpret_cast<volatile int *>(qs)[warp] = bi; }
+			__syncthreads();
+			if (threadIdx.x == 0) {
+				float b = -1.f;
+				int p = 0;
+				for (int q = 0; q < 8; q++) {
+					const int pq = reinterpret_cast<volatile int *>(qs)[q];
+					if (red[q] > b || (red[q] == b && pq < p)) { b = red[q]; p = pq; }
+				}
+				s_best = b;
+				s_piv = p;
+			}
+			__syncthreads();
+			if (s_best < 1e-4f) break;
+			if (d == kTcNullMax) {
+				if (threadIdx.x == 0) s_bad = 1;
+				break;
+			}
+			const int p = s_piv;
+			const float inv = rsqrtf(s_best);
+			for (int i = threadIdx.x; i < n; i += blockDim.x) Lv[m][d][i] = M[(int64_t)i * n + p] * inv;
+			__syncthreads();
+			for (int64_t e = threadIdx.x; e < (int64_t)n * n; e += blockDim.x) {
+				const int i = (int)(e / n), j = (int)(e - (int64_t)i * n);
+				M[e] -= Lv[m][d][i] * Lv[m][d][j];
+			}
+			__syncthreads();
+			d++;
+		}
+		if (threadIdx.x == 0) s_d[m] = d;
+		__syncthreads();
+	}
+	if (s_bad || s_d[0] != s_d[1] || s_d[0] == 0) return;
+	const int d = s_d[0];
+	// the bases must be orthonormal already; then two Gram-Schmidt passes make them so to rounding
+	for (int m = 0; m < 2; m++) {
+		for (int a = 0; a < d; a++)
+			for (int b = 0; b <= a; b++) {
+				float v = 0.f;
+				for (int i = threadIdx.x; i < n; i += blockDim.x) v += Lv[m][a][i] * Lv[m][b][i];
+				v = block_sum256(v, red);
+				if (fabsf(v - (a == b ? 1.f : 0.f)) > 1e-3f) {
+					if (threadIdx.x == 0) s_bad = 1;
+				}
+			}
+		__syncthreads();
+		if (s_bad) return;
+		for (int a = 0; a < d; a++) {
+			for (int pass = 0; pass < 2; pass++)
+				for (int b = 0; b < a; b++) {
+					float v = 0.f;
+					for (int i = threadIdx.x; i < n; i += blockDim.x) v += Lv[m][a][i] * Lv[m][b][i];
+					v = block_sum256(v, red);
+					for (int i = threadIdx.x; i < n; i += blockDim.x) Lv[m][a][i] -= v * Lv[m][b][i];
+					__syncthreads();
+				}
+			float v = 0.f;
+			for (int i = threadIdx.x; i < n; i += blockDim.x) v += Lv[m][a][i] * Lv[m][a][i];
+			v = rsqrtf(block_sum256(v, red));
+			for (int i = threadIdx.x; i < n; i += blockDim.x) Lv[m][a][i] *= v;
+			__syncthreads();
+		}
+	}
+	// T <- (I - U_0 U_0^T) T + U_0 V_0^T  (U_0 = the left null basis from F, V_0 from E); the
+	// projection is applied column by column of T through the shared coefficients c = U_0^T T(:, j)
+	for (int j = 0; j < n; j++) {
+		float c[kTcNullMax];
+		for (int a = 0; a < d; a++) {
+			float v = 0.f;
+			for (int i = threadIdx.x; i < n; i += blockDim.x) v += Lv[1][a][i] * T[i * ti + j * tj];
+			c[a] = block_sum256(v, red);
+		}
+		for (int i = threadIdx.x; i < n; i += blockDim.x) {
+			float v = T[i * ti + j * tj];
+			for (int a = 0; a < d; a++) v += Lv[1][a][i] * (Lv[0][a][j] - c[a]);
+			T[i * ti + j * tj] = v;
+		}
+		__syncthreads();
+	}
+	if (threadIdx.x == 0) {
+		SlStats st = stats[w.slot];
+		st.flags = (st.flags & ~kFlagIllCond) | kFlagCompleted;
+		stats[w.slot] = st;
 	}
 }
 

@@ -246,9 +246,10 @@ enum {
 	kHaB200SolverFP32  = 1, /* plain FP32 form: FP32 Jacobi only, no refinement, no FP64 re-solve */
 	kHaB200SolverFP64  = 2, /* every searchlight in FP64 */
 	kHaB200SolverTC    = 3, /* tensor cores: split-BF16 (three parts, six products, FP32 accuracy)
-	                           cross-covariance and Newton-Schulz polar iteration; searchlights whose
-	                           iteration does not converge (exactly singular A) are re-solved by FP64
-	                           Jacobi.  Needs isReflection; without it the mixed solver runs. */
+	                           cross-covariance and Newton-Schulz polar iteration; exactly singular A
+	                           get their null spaces completed, and searchlights that still do not
+	                           converge are re-solved by FP64 Jacobi.  Needs isReflection; without it
+	                           the mixed solver runs. */
 };
 
 /*
@@ -275,7 +276,10 @@ int ha_b200_plan_sweep_stats(const HaB200Plan *plan, int64_t *sweeps_sum, int32_
 /*
  * Per-searchlight solve record of the last run, searchlights [first, first + n) of its last
  * chunk: smallest and largest singular value, flags (1 unconverged, 2 ill-conditioned,
- * 4 reflection removed, 8 solved in FP64) and Jacobi sweeps.  Any output may be NULL.
+ * 4 reflection removed, 8 solved in FP64, 16 zero singular values completed after the tensor-core
+ * iteration) and Jacobi sweeps (tensor-core solver: Newton-Schulz iterations; its sigma_max is
+ * the upper bound the iterate was scaled by and sigma_min is not computed, 0).  Any output may
+ * be NULL.
  */
 int ha_b200_plan_searchlight_stats(const HaB200Plan *plan, int32_t first, int32_t n, double *s_min,
                                    double *s_max, int32_t *flags, int32_t *sweeps);
