@@ -1,18 +1,23 @@
 #!/usr/bin/env python
-"""Searchlight solves/sec on the hemisphere template workload.
+"""Searchlight solves/sec on the hemisphere template workload with singular searchlights.
 
 One step = one searchlight Procrustes pass (with scaling) over a hemisphere:
 10242 Fibonacci-sphere vertices, nt = 400, one searchlight of 100-300 vertices
-per vertex, subject 1 aligned onto subject 0 of the template workload, output
-the weighted transforms combined into the symmetric CSC/CSR matrix.
+per vertex, subject 1 aligned onto subject 0 of the template workload, with
+vertex columns duplicated until ~10% of the searchlights are exactly singular;
+output the weighted transforms combined into the symmetric CSC/CSR matrix.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
-value     device-resident inputs (float64 X, Y already in HBM), CUDA events around each
-          step on the launching stream, L2 flushed (256 MiB write) between steps
+value     the tensor-core solver (split-BF16 products, Newton-Schulz polar) on device-resident
+          inputs (float64 X, Y already in HBM), CUDA events around each step on the launching
+          stream, L2 flushed (256 MiB write) between steps
+plain_fp32  the same step and inputs in the plain FP32 form (FP32 Jacobi, no refinement, no FP64):
+          the metric's denominator; mixed_form, fp64_form the other solvers
+config2_template_pair  the same pair without duplicated columns (tensor-core and plain FP32)
 e2e       the C ABI dense entry point (ha_searchlight_procrustes_dense, backend 4) from
-          host float64 buffers into a host nv x nv float64 matrix, wall clock per call
-plain_fp32  the same step with the plain FP32 form (FP32 Jacobi, no refinement, no FP64)
+          host float64 buffers into a host nv x nv float64 matrix, wall clock per call; a
+          cold first call after ha_b200_cleanup beside it
 roofline  dominant kernel (per-kind CUDA event times recorded by the library)
 cpu_baseline  the reference C library (oracle/_ref, cpu64 arm, all host threads) on a
           bounded sample of the same searchlights
@@ -42,7 +47,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "searchlight solves/sec vs plain FP32 GPU form at stated FP64-oracle error"
 UNIT = "searchlights/s"
-WORKLOAD = "hemisphere_template_pair"
+WORKLOAD = "hemisphere_template_pair_10pct_singular"
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
 FP32_SIMT_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 
@@ -58,10 +63,11 @@ def parse_args():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
-    p.add_argument("--workload", choices=["template", "grid", "learned", "rankdef", "shard", "forrest"], default="template",
-                   help="template: the headline Procrustes step; grid: the searchlight ridge grid search "
-                        "(40962 vertices, every --grid-step-th searchlight); learned: the learned proposal; "
-                        "rankdef: the mixed form on the template pair with duplicated columns; shard: one "
+    p.add_argument("--workload", choices=["template", "rankdef", "grid", "learned", "shard", "forrest"], default="rankdef",
+                   help="rankdef (default; 'template' is the same run): the headline Procrustes step on the "
+                        "template pair with 10%% singular searchlights, the plain pair as a sub-field; grid: the "
+                        "searchlight ridge grid search (40962 vertices, every --grid-step-th searchlight); "
+                        "learned: the learned proposal; shard: one "
                         "hemisphere split over the N GPUs (strong scaling); forrest: the shapes of the "
                         "reference's published run (nt 1818, searchlights of 90-170)")
     p.add_argument("--grid-step", type=int, default=16)
@@ -226,7 +232,8 @@ def run_reference(args):
     if not R.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libhyperalignment.so not built"}))
         return
-    w = workload(0, args.nv, args.nt)
+    from hyperalignment_b200 import workloads as W
+    w = W.rank_deficient_pair(0, nv=args.nv, nt=args.nt)
     threads = os.cpu_count() or 1
     budget = args.ref_seconds if args.ref_seconds > 0 else max(2.0, 150.0 / max(1, args.steps + args.warmup))
     rates, times, counts = [], [], []
@@ -257,10 +264,55 @@ def run_reference(args):
 # B200 arm
 # ---------------------------------------------------------------------------------------------
 
+def tc_algorithmic_flops(sizes, iters):
+    """BF16 tensor-core work of the Newton-Schulz polar iteration as the algorithm defines it (no
+    padding): per searchlight and iteration two n x n x n products (X^T X and X P), each executed as
+    six BF16 products of the three-part split: 24 n^3 flops."""
+    n = sizes.astype(np.float64)
+    return float((24.0 * iters.astype(np.float64) * n ** 3).sum())
+
+
+def tc_executed_flops(sizes, iters):
+    """BF16 MMA work the kernels issue, padding included: rows in 128-row tiles, N and K padded to 16."""
+    n = sizes.astype(np.int64)
+    npad = (n + 15) // 16 * 16
+    mpad = (npad + 127) // 128 * 128
+    return float((2 * 6 * 2 * iters.astype(np.float64) * mpad * npad.astype(np.float64) ** 2).sum())
+
+
+def sample_errors(w, singular, sample, Ts):
+    """Per-T and aligned-data (X_sl T) errors vs the float64 oracle; singular searchlights are compared
+    on the row space of A (the part of T that A determines) and on X_sl T (unique)."""
+    from oracle import ha_oracle as O
+    rows = {"singular": [], "regular": []}
+    for j, q in enumerate(sample):
+        sl = w.sls.indices[w.sls.offsets[q]:w.sls.offsets[q + 1]]
+        Xs, Ys = w.X[:, sl], w.Y[:, sl]
+        Tref = O.procrustes(Xs, Ys, True, False)
+        T = Ts[j]
+        XT, XTref = Xs @ T, Xs @ Tref
+        if singular is not None and singular[q]:
+            A = Xs.T @ Ys
+            T, Tref = range_part(T, A), range_part(Tref, A)
+        rows["singular" if singular is not None and singular[q] else "regular"].append(
+            (np.linalg.norm(T - Tref) / np.linalg.norm(Tref), np.abs(T - Tref).max(),
+             np.linalg.norm(XT - XTref) / np.linalg.norm(XTref), np.abs(XT - XTref).max()))
+    out = {}
+    for k, v in rows.items():
+        if not v:
+            continue
+        e = np.array(v)
+        out[k] = {"T_relfrob_max": float(e[:, 0].max()), "T_relfrob_median": float(np.median(e[:, 0])),
+                  "T_maxabs_max": float(e[:, 1].max()), "XT_relfrob_max": float(e[:, 2].max()),
+                  "XT_maxabs_max": float(e[:, 3].max()), "count": int(e.shape[0])}
+    return out
+
+
 def run_b200(args):
     import torch
     import torch.distributed as dist
     from hyperalignment_b200 import _lib as L
+    from hyperalignment_b200 import workloads as W
     from hyperalignment_b200.plan import Plan
 
     ws, rank, local = dist_setup(args)
@@ -271,22 +323,28 @@ def run_b200(args):
     lib = L.lib()
     L.check(lib.ha_b200_init(), "ha_b200_init")
 
-    w = workload(rank, args.nv, args.nt)
-    plan = Plan.from_workload(w)
+    # config 3 (headline): the template pair with ~10% of the searchlights made exactly singular;
+    # config 2 (sub-field): the same pair without the duplicated columns
+    w3 = W.rank_deficient_pair(rank, nv=args.nv, nt=args.nt)
+    singular = w3.extra["singular"]
+    w2 = workload(rank, args.nv, args.nt)
+    assert np.array_equal(w2.Y, w3.Y) and np.array_equal(w2.sls.indices, w3.sls.indices)
+    plan = Plan.from_workload(w3)
     dev = torch.device("cuda", local)
-    dX = torch.from_numpy(np.asfortranarray(w.X).ravel(order="F")).to(dev)
-    dY = torch.from_numpy(np.asfortranarray(w.Y).ravel(order="F")).to(dev)
+    dX3 = torch.from_numpy(np.asfortranarray(w3.X).ravel(order="F")).to(dev)
+    dX2 = torch.from_numpy(np.asfortranarray(w2.X).ravel(order="F")).to(dev)
+    dY = torch.from_numpy(np.asfortranarray(w3.Y).ravel(order="F")).to(dev)
     vals = torch.zeros(plan.nnz, dtype=torch.float64, device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
 
-    def step(solver):
+    def step(solver, dX):
         plan.procrustes_device(dX.data_ptr(), dY.data_ptr(), vals.data_ptr(), True, True, solver, L.OUT_CSR,
                                stream.cuda_stream)
 
-    def timed_loop(solver, k, sample_clocks=False, trace=False):
+    def timed_loop(solver, dX, k, sample_clocks=False, trace=False):
         for _ in range(args.warmup):
-            step(solver)
+            step(solver, dX)
         torch.cuda.synchronize()
         if ws > 1:
             dist.barrier()
@@ -306,7 +364,7 @@ def run_b200(args):
             a = torch.cuda.Event(enable_timing=True)
             b = torch.cuda.Event(enable_timing=True)
             a.record(stream)
-            step(solver)
+            step(solver, dX)
             b.record(stream)
             evs.append((a, b))
         torch.cuda.synchronize()
@@ -326,76 +384,77 @@ def run_b200(args):
         return dev_ms, wall, launches, kt, clocks
 
     K = args.steps
-    total_ms, wall, launches, kt, clocks = timed_loop(L.SOLVER_MIXED, K, sample_clocks=True, trace=True)
-    value = aggregate_rate(ws, w.sls.count, K, total_ms / 1e3)
-    plain_ms, _, _, _, _ = timed_loop(L.SOLVER_FP32, K)
-    plain_value = aggregate_rate(ws, w.sls.count, K, plain_ms / 1e3)
-    plain_stats = plan.stats()
-    fp64_ms, _, _, _, _ = timed_loop(L.SOLVER_FP64, max(1, K // 4))
-    fp64_value = aggregate_rate(ws, w.sls.count, max(1, K // 4), fp64_ms / 1e3)
-    fp64_stats = plan.stats()
-    step(L.SOLVER_MIXED)
+    count = w3.sls.count
+    # untimed iteration counts of the tensor-core solve (for the roofline's work per launch)
+    step(L.SOLVER_TC, dX3)
     torch.cuda.synchronize()
-    stats = {"mixed": plan.stats(), "plain_fp32": plain_stats, "fp64": fp64_stats}
+    tc_iters = plan.searchlight_stats(0, count)["sweeps"].astype(np.int64)
+    tc_flags = plan.searchlight_stats(0, count)["flags"]
+    total_ms, wall, launches, kt, clocks = timed_loop(L.SOLVER_TC, dX3, K, sample_clocks=True, trace=True)
+    value = aggregate_rate(ws, count, K, total_ms / 1e3)
+    tc_stats = plan.stats()
+    plain_ms, _, _, _, _ = timed_loop(L.SOLVER_FP32, dX3, K)
+    plain_value = aggregate_rate(ws, count, K, plain_ms / 1e3)
+    plain_stats = plan.stats()
+    km = max(1, K // 2)
+    mixed_ms, _, _, _, _ = timed_loop(L.SOLVER_MIXED, dX3, km)
+    mixed_value = aggregate_rate(ws, count, km, mixed_ms / 1e3)
+    mixed_stats = plan.stats()
+    fp64_ms, _, _, _, _ = timed_loop(L.SOLVER_FP64, dX3, 1)
+    fp64_value = aggregate_rate(ws, count, 1, fp64_ms / 1e3)
+    # config 2: the same step without the duplicated columns
+    c2_ms, _, _, _, _ = timed_loop(L.SOLVER_TC, dX2, K)
+    c2_value = aggregate_rate(ws, count, K, c2_ms / 1e3)
+    c2_stats = plan.stats()
+    c2_plain_ms, _, _, _, _ = timed_loop(L.SOLVER_FP32, dX2, K)
+    c2_plain = aggregate_rate(ws, count, K, c2_plain_ms / 1e3)
 
-    # accuracy vs the float64 oracle on a fixed sample of searchlights (both forms), solved by a
-    # plan over the sampled searchlights only (same kernels, one chunk)
-    from oracle import ha_oracle as O
-    rng = np.random.default_rng(123)
-    sample = np.sort(rng.choice(w.sls.count, size=16, replace=False))
-    sub = w.sls.subset(sample)
-    splan = Plan(w.nt, w.nv, sub.indices, sub.offsets, sub.dists, sub.radius)
-    svals = torch.zeros(splan.nnz, dtype=torch.float64, device=dev)
-    errs = {}
-    for name, solver in (("mixed", L.SOLVER_MIXED), ("plain_fp32", L.SOLVER_FP32)):
-        splan.procrustes_device(dX.data_ptr(), dY.data_ptr(), svals.data_ptr(), True, True, solver, L.OUT_CSR,
-                                stream.cuda_stream)
-        torch.cuda.synchronize()
-        Ts = splan.local_transforms(0, sub.count)
-        e = []
-        for j, q in enumerate(sample):
-            T = Ts[j]
-            sl = w.sls.indices[w.sls.offsets[q]:w.sls.offsets[q + 1]]
-            Tref = O.procrustes(w.X[:, sl], w.Y[:, sl], True, False)
-            XT, XTref = w.X[:, sl] @ T, w.X[:, sl] @ Tref  # the aligned data of the searchlight
-            e.append((np.linalg.norm(T - Tref) / np.linalg.norm(Tref), np.abs(T - Tref).max(),
-                      np.linalg.norm(XT - XTref) / np.linalg.norm(XTref), np.abs(XT - XTref).max()))
-        e = np.array(e)
-        errs[name] = {"T_relfrob_max": float(e[:, 0].max()), "T_relfrob_median": float(np.median(e[:, 0])),
-                      "T_maxabs_max": float(e[:, 1].max()), "XT_relfrob_max": float(e[:, 2].max()),
-                      "XT_maxabs_max": float(e[:, 3].max()), "sample": int(sample.size)}
+    # accuracy vs the float64 oracle on fixed samples (24 singular + 24 regular searchlights of
+    # config 3, 24 of config 2), solved by a plan over the sampled searchlights only (same kernels)
+    rng = np.random.default_rng(7)
+    sing, reg = np.flatnonzero(singular), np.flatnonzero(~singular)
+    sample3 = np.sort(np.concatenate([rng.choice(sing, size=min(24, sing.size), replace=False),
+                                      rng.choice(reg, size=min(24, reg.size), replace=False)]))
+    sample2 = np.sort(np.random.default_rng(123).choice(count, size=24, replace=False))
+    errs, errs2 = {}, {}
+    for smp, wk, dX, sg, out in ((sample3, w3, dX3, singular, errs), (sample2, w2, dX2, None, errs2)):
+        sub = wk.sls.subset(smp)
+        splan = Plan(wk.nt, wk.nv, sub.indices, sub.offsets, sub.dists, sub.radius)
+        svals = torch.zeros(splan.nnz, dtype=torch.float64, device=dev)
+        for name, solver in (("tensor_core", L.SOLVER_TC), ("plain_fp32", L.SOLVER_FP32), ("mixed", L.SOLVER_MIXED)):
+            splan.procrustes_device(dX.data_ptr(), dY.data_ptr(), svals.data_ptr(), True, True, solver, L.OUT_CSR,
+                                    stream.cuda_stream)
+            torch.cuda.synchronize()
+            out[name] = sample_errors(wk, sg, smp, splan.local_transforms(0, sub.count))
+        splan.close()
 
-    # roofline of the dominant kernel
+    # roofline of the dominant kernel (the Newton-Schulz products on the tensor cores)
     peaks, peak_src = load_peaks()
     ms, cnt = kt
     dom = int(np.argmax(ms))
     dom_name = L.KERNEL_KINDS[dom]
-    sizes = w.sls.sizes.astype(np.float64)
-    alg = {
-        "jacobi32": ("flop", 21.0 * (sizes ** 3).sum()),
-        "xcov32": ("flop", 2.0 * w.nt * (sizes ** 2).sum()),
-        "refine": ("flop", 4.0 * (sizes ** 3).sum()),
-        "formT32": ("flop", 2.0 * (sizes[sizes > 164] ** 3).sum()),
-        "reduce": ("byte", (sizes ** 2).sum() * 4 + plan.nnz * 16.0),
-    }
+    sizes = w3.sls.sizes
     roof = None
-    if dom_name in alg and ms[dom] > 0:
-        kind, per_step = alg[dom_name]
+    if dom_name == "tc_ns" and ms[dom] > 0:
+        per_step = tc_algorithmic_flops(sizes, tc_iters)
         per_launch = per_step * K / max(1, cnt[dom])
         avg_ms = ms[dom] / max(1, cnt[dom])
         achieved = per_launch / (avg_ms / 1e3)
-        if kind == "flop":
-            peak = float(peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops")))
-            roof = {"bound": "tensor", "kernel": dom_name, "achieved": achieved / 1e12, "peak": peak,
-                    "unit": "TFLOP/s", "frac": achieved / 1e12 / peak, "traffic": None,
-                    "peak_source": f"{peak_src} bf16 sustained",
-                    "fp32_simt": {"peak_nominal": FP32_SIMT_NOMINAL_TFLOPS,
-                                  "frac": achieved / 1e12 / FP32_SIMT_NOMINAL_TFLOPS},
-                    "algorithmic": "21 n^3 flops per searchlight (square SVD, Golub-Van Loan count)"}
-        else:
-            peak = float(peaks["hbm_gbs"])
-            roof = {"bound": "hbm", "kernel": dom_name, "achieved": achieved / 1e9, "peak": peak, "unit": "GB/s",
-                    "frac": achieved / 1e9 / peak, "traffic": None, "peak_source": f"{peak_src} hbm copy"}
+        peak = float(peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops")))
+        executed = tc_executed_flops(sizes, tc_iters) * K / max(1, cnt[dom]) / (avg_ms / 1e3)
+        useful = 23.0 * float((sizes.astype(np.float64) ** 3).sum()) * K / max(1, cnt[dom]) / (avg_ms / 1e3)
+        roof = {"bound": "tensor", "kernel": "tc_ns (k_tc_gemm Gram + update, k_tc_ns_init)", "achieved": achieved / 1e12,
+                "peak": peak, "unit": "TFLOP/s", "frac": achieved / 1e12 / peak, "traffic": None,
+                "peak_source": f"{peak_src} bf16 sustained",
+                "algorithmic": "24 n^3 BF16 flops per searchlight and iteration (two n^3 products, six BF16 "
+                               "products each); iterations as run (mean %.2f)" % float(tc_iters.mean()),
+                "executed_with_padding_tflops": executed / 1e12,
+                "svd_equivalent_tflops": useful / 1e12,
+                "svd_equivalent": "23 n^3 per searchlight (square SVD 21 n^3 + U V^T 2 n^3, the reference's work)",
+                "avg_launch_ms": float(avg_ms), "launches_per_step": float(cnt[dom] / K)}
+    elif ms[dom] > 0:
+        roof = {"bound": "unknown", "kernel": dom_name, "achieved": None, "peak": None, "unit": None, "frac": None,
+                "traffic": None}
     traffic_file = os.path.join(ROOT, "profiles", "traffic.json")
     if roof is not None and os.path.exists(traffic_file):
         with open(traffic_file) as f:
@@ -404,18 +463,20 @@ def run_b200(args):
             per_sl = tr[dom_name].get("bytes_per_searchlight")
             if per_sl:
                 # ncu capture of a smaller case scaled to a full launch by the searchlights it solves
-                roof["traffic"] = per_sl * w.sls.count * K / max(1, cnt[dom])
+                roof["traffic"] = per_sl * count * K / max(1, cnt[dom])
                 roof["traffic_source"] = tr[dom_name].get("source")
     kernel_share = {L.KERNEL_KINDS[i]: {"ms_per_step": float(ms[i] / K), "launches_per_step": float(cnt[i] / K)}
                     for i in range(len(ms)) if cnt[i] > 0}
 
-    # end to end through the C ABI dense entry point (host buffers)
+    # end to end through the C ABI dense entry point (host buffers): warm calls, then one cold call
+    # after ha_b200_cleanup (plan, pattern and buffers rebuilt, as a caller that cleans up after
+    # every call pays)
     e2e = None
     if not args.no_e2e:
-        Xf, Yf = np.asfortranarray(w.X), np.asfortranarray(w.Y)
-        T_out = np.zeros((w.nv, w.nv))
-        s = w.sls
-        argsv = (Xf.ctypes.data_as(L.c_double_p), Yf.ctypes.data_as(L.c_double_p), w.nt, w.nv,
+        Xf, Yf = np.asfortranarray(w3.X), np.asfortranarray(w3.Y)
+        T_out = np.zeros((w3.nv, w3.nv))
+        s = w3.sls
+        argsv = (Xf.ctypes.data_as(L.c_double_p), Yf.ctypes.data_as(L.c_double_p), w3.nt, w3.nv,
                  L.iptr(s.indices), L.iptr(s.offsets), L.dptr(s.dists), s.count, s.radius,
                  T_out.ctypes.data_as(L.c_double_p), True, True, L.BACKEND_B200, True)
         lib.ha_set_num_threads(os.cpu_count() or 1)
@@ -429,20 +490,28 @@ def run_b200(args):
             L.check(lib.ha_searchlight_procrustes_dense(*argsv), "dense")
             ts.append(time.perf_counter() - t0)
         tmax = max_over_ranks(sum(ts), ws, dev)
+        lib.ha_b200_cleanup()
+        t0 = time.perf_counter()
+        L.check(lib.ha_searchlight_procrustes_dense(*argsv), "dense")
+        cold = max_over_ranks(time.perf_counter() - t0, ws, dev)
         e2e = {"value": aggregate_rate(ws, s.count, K, tmax), "unit": UNIT,
-               "h2d_bytes_per_step": int(2 * w.nt * w.nv * 8), "d2h_bytes_per_step": int(plan.nnz * 8),
-               "path": "ha_searchlight_procrustes_dense(backend=4) host float64 in, host dense nv x nv out (+=)"}
+               "h2d_bytes_per_step": int(2 * w3.nt * w3.nv * 8), "d2h_bytes_per_step": int(plan.nnz * 8),
+               "path": "ha_searchlight_procrustes_dense(backend=4) host float64 in, host dense nv x nv out (+=); "
+                       "tensor-core solver",
+               "cold_first_call": {"value": aggregate_rate(ws, s.count, 1, cold), "unit": UNIT, "seconds": cold,
+                                   "what": "first call after ha_b200_cleanup: plan, pattern, work lists and "
+                                           "buffers built inside the call"}}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         from oracle import ref_lib as R
         if R.available():
             threads = os.cpu_count() or 1
-            r, m, dt = reference_rate(w, args.cpu_seconds, threads)
-            r1, m1, dt1 = reference_rate(w, min(5.0, args.cpu_seconds / 3.0), 1)
-            r32, m32, dt32 = reference_rate(w, min(5.0, args.cpu_seconds / 3.0), threads, backend=1)
+            r, m, dt = reference_rate(w3, args.cpu_seconds, threads)
+            r1, m1, dt1 = reference_rate(w3, min(5.0, args.cpu_seconds / 3.0), 1)
+            r32, m32, dt32 = reference_rate(w3, min(5.0, args.cpu_seconds / 3.0), threads, backend=1)
             cpu = {"value": r, "unit": UNIT, "cores": threads, "kind": "reference",
-                   "sample": f"{m} contiguous searchlights of {w.sls.count} ({dt:.1f} s), reference cpu64 arm, "
+                   "sample": f"{m} contiguous searchlights of {count} ({dt:.1f} s), reference cpu64 arm, "
                              f"OpenMP {threads} threads, OPENBLAS_NUM_THREADS=1",
                    "single_thread": {"value": r1, "unit": UNIT, "cores": 1,
                                      "sample": f"{m1} contiguous searchlights ({dt1:.1f} s), one OpenMP thread"},
@@ -457,16 +526,27 @@ def run_b200(args):
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": args.warmup,
             "ms_per_step": total_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic",
-            "config": config_dict(w, {"parallelism": f"replicas x{ws} (one subject pair per GPU)" if ws > 1 else "single GPU",
-                                      "solver": "FP32 Jacobi + FP32 Newton-Schulz refinement, FP64 re-solve below sigma ratio 5e-5"}),
+            "dtype": "bf16x6 (FP32-accurate split) tensor-core products, f32/f64 host data", "data": "synthetic",
+            "config": config_dict(w3, {"workload": WORKLOAD, "singular_searchlights": int(singular.sum()),
+                                       "parallelism": f"replicas x{ws} (one subject pair per GPU)" if ws > 1 else "single GPU",
+                                       "solver": "tensor cores: split-BF16 cross-covariance + Newton-Schulz polar, "
+                                                 "null-space completion of exactly singular searchlights"}),
             "plain_fp32": {"value": plain_value, "unit": UNIT, "ms_per_step": plain_ms / K,
-                           "speedup_of_value": value / plain_value},
+                           "speedup_of_value": value / plain_value, "what": "FP32 Jacobi SVD, no refinement, no FP64"},
+            "mixed_form": {"value": mixed_value, "unit": UNIT, "ms_per_step": mixed_ms / km,
+                           "what": "FP32 Jacobi + Newton-Schulz refinement + FP64 re-solve below sigma ratio 5e-5"},
             "fp64_form": {"value": fp64_value, "unit": UNIT},
+            "config2_template_pair": {"value": c2_value, "unit": UNIT, "ms_per_step": c2_ms / K,
+                                      "plain_fp32": c2_plain, "speedup_of_value": c2_value / c2_plain,
+                                      "solver_stats": c2_stats, "error_vs_fp64": errs2},
             "error_vs_fp64": errs,
-            "solver_stats": stats,
+            "solver_stats": {"tensor_core": tc_stats, "plain_fp32": plain_stats, "mixed": mixed_stats,
+                             "completed_null_spaces": int(((tc_flags & 16) != 0).sum()),
+                             "iterations_mean": float(tc_iters.mean()), "iterations_max": int(tc_iters.max())},
             "roofline": roof,
             "kernels": kernel_share,
+            "kernels_note": "per-kind CUDA-event intervals of the tensor-core step; its kernels run in order on one "
+                            "stream (the float64 re-solve's side streams run only for searchlights left flagged)",
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": int(launches),
@@ -692,76 +772,6 @@ def rankdef_errors(w, singular, sample, Ts, fp64_flags):
         groups["fp64" if fp64_flags[j] else "fp32"].append(e)
     return {k: ({"T_relfrob_max": float(np.max(v)), "T_relfrob_median": float(np.median(v)), "count": len(v)}
                 if v else {"count": 0}) for k, v in groups.items()}
-
-
-def run_rankdef(args):
-    import torch
-    from hyperalignment_b200 import _lib as L
-    from hyperalignment_b200 import workloads as W
-    from hyperalignment_b200.plan import Plan
-
-    ws, rank, local = dist_setup(args)
-    torch.cuda.set_device(local)
-    lib = L.lib()
-    L.check(lib.ha_b200_init(), "ha_b200_init")
-    w = W.rank_deficient_pair(rank, nv=args.nv, nt=args.nt)
-    singular = w.extra["singular"]
-    plan = Plan.from_workload(w)
-    dev = torch.device("cuda", local)
-    dX = torch.from_numpy(np.asfortranarray(w.X).ravel(order="F")).to(dev)
-    dY = torch.from_numpy(np.asfortranarray(w.Y).ravel(order="F")).to(dev)
-    vals = torch.zeros(plan.nnz, dtype=torch.float64, device=dev)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    stream = torch.cuda.current_stream(dev)
-
-    def step():
-        plan.procrustes_device(dX.data_ptr(), dY.data_ptr(), vals.data_ptr(), True, True, L.SOLVER_MIXED,
-                               L.OUT_CSR, stream.cuda_stream)
-
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    sampler = ClockSampler(local)
-    sampler.start()
-    time.sleep(0.5)
-    evs = []
-    for _ in range(args.steps):
-        flush.zero_()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        step()
-        b.record(stream)
-        evs.append((a, b))
-    torch.cuda.synchronize()
-    clocks = sampler.stop()
-    total_ms = float(sum(a.elapsed_time(b) for a, b in evs))
-    stats = plan.stats()
-    rng = np.random.default_rng(7)
-    sing = np.flatnonzero(singular)
-    reg = np.flatnonzero(~singular)
-    sample = np.sort(np.concatenate([rng.choice(sing, size=min(24, sing.size), replace=False),
-                                     rng.choice(reg, size=min(24, reg.size), replace=False)]))
-    sub = w.sls.subset(sample)
-    splan = Plan(w.nt, w.nv, sub.indices, sub.offsets, sub.dists, sub.radius)
-    svals = torch.zeros(splan.nnz, dtype=torch.float64, device=dev)
-    splan.procrustes_device(dX.data_ptr(), dY.data_ptr(), svals.data_ptr(), True, True, L.SOLVER_MIXED,
-                            L.OUT_CSR, stream.cuda_stream)
-    torch.cuda.synchronize()
-    Ts = splan.local_transforms(0, sub.count)
-    fp64 = (splan.searchlight_stats(0, sub.count)["flags"] & 8) != 0
-    errs = rankdef_errors(w, singular, sample, Ts, fp64)
-    if rank == 0:
-        sizes = w.sls.sizes
-        print(json.dumps({
-            "metric": "searchlight solves/sec, mixed form, rank-deficient searchlights",
-            "value": w.sls.count * args.steps / (total_ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "rank_deficient_template_pair", "nv": w.nv, "nt": w.nt,
-                       "searchlights": w.sls.count, "singular_searchlights": int(singular.sum()),
-                       "sl_size_min": int(sizes.min()), "sl_size_max": int(sizes.max()),
-                       "l2": "flushed between steps (256 MiB write)"},
-            "solver_stats": stats, "error_vs_fp64": errs, "clocks": clocks}))
 
 
 # ---------------------------------------------------------------------------------------------
@@ -1030,8 +1040,6 @@ def main():
         run_grid(args)
     elif args.workload == "learned":
         run_learned(args)
-    elif args.workload == "rankdef":
-        run_rankdef(args)
     elif args.workload == "shard":
         run_shard(args)
     elif args.workload == "forrest":
