@@ -276,6 +276,8 @@ struct Chunk {
 	std::vector<TcTile> tct[2];
 	TcWork *d_tcw = nullptr;
 	TcTile *d_tct[2] = {nullptr, nullptr};
+	std::vector<int32_t> tco[2];  // persistent solve: work indices per size class, largest first
+	int32_t *d_tco[2] = {nullptr, nullptr};
 	int64_t tc_x_elems = 0, tc_a_elems = 0;
 };
 
@@ -316,6 +318,9 @@ struct HaB200Plan {
 	DevArr<__nv_bfloat16> tcXb, tcYb, tcXp, tcPp;
 	DevArr<float> tcA, tcRes;
 	DevArr<TcState> tcSt;
+	DevArr<float> tcSched;      // c1[maxit], c3[maxit] of the iteration schedule
+	DevArr<int32_t> tcPlain;    // plain[maxit]
+	DevArr<int32_t> tcQueue;    // work queue positions of the persistent solve (two size classes)
 	bool tc_ready = false;
 	// ridge grid search: scratch and the uploaded grid / CV description, allocated on first use
 	DevArr<double> gridscr, galpha, gwinv;
@@ -772,12 +777,38 @@ std::vector<NsStep> ns_schedule() {
 // largest |1 - sigma^2| is then below 1e-4 sqrt(n); the final step squares it.
 double ns_tol() { return env_double("HA_B200_NS_TOL", 1e-4, 1e-7, 1e-1); }
 
+// One launch per phase and iteration (default), or the persistent solve (HA_B200_TC_PERSIST=1: one
+// CTA runs whole searchlights, their planes stay in L2; measured 3% slower on the template pair).
+bool tc_persistent() {
+	static int v = -1;
+	if (v < 0) {
+		const char *e = getenv("HA_B200_TC_PERSIST");
+		v = (e && e[0] == '1') ? 1 : 0;
+	}
+	return v == 1;
+}
+
+int g_num_sms = 148;
+
+// CTAs per SM of the persistent solve for searchlights of np <= 256: two (110 KB of stages each)
+// or one (200 KB, so deeper pipelines, and half the planes live in L2 at a time).
+// HA_B200_TC_CTAS overrides the default.
+int tc_small_ctas_per_sm() {
+	static int v = 0;
+	if (!v) {
+		const char *e = getenv("HA_B200_TC_CTAS");
+		v = (e && e[0] == '1') ? 1 : 2;
+	}
+	return v;
+}
+
 int set_tc_attrs() {
 	static bool done = false;
 	if (done) return kHaSuccess;
 	HA_CUDA(cudaFuncSetAttribute(k_tc_gemm<kTcPhaseXcov>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemLarge));
 	HA_CUDA(cudaFuncSetAttribute(k_tc_gemm<kTcPhaseGram>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemLarge));
 	HA_CUDA(cudaFuncSetAttribute(k_tc_gemm<kTcPhaseUpdate>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemLarge));
+	HA_CUDA(cudaFuncSetAttribute(k_tc_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemLarge));
 	done = true;
 	return kHaSuccess;
 }
@@ -818,11 +849,15 @@ int build_tc(HaB200Plan *P) {
 		std::vector<int> order((size_t)nsl);
 		for (int q = 0; q < nsl; q++) order[q] = q;
 		std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return ch.tcw[x].n > ch.tcw[y].n; });
-		for (int c = 0; c < 2; c++) ch.tct[c].clear();
+		for (int c = 0; c < 2; c++) {
+			ch.tct[c].clear();
+			ch.tco[c].clear();
+		}
 		for (int q : order) {
 			const int np = ch.tcw[q].np;
 			const int c = np > 256 ? 1 : 0;
 			for (int t = 0; t * 128 < np; t++) ch.tct[c].push_back({q, t});
+			ch.tco[c].push_back(q);
 		}
 		if (cudaMalloc(&ch.d_tcw, (size_t)nsl * sizeof(TcWork)) != cudaSuccess) return kHaErrorAlloc;
 		HA_CUDA(cudaMemcpy(ch.d_tcw, ch.tcw.data(), (size_t)nsl * sizeof(TcWork), cudaMemcpyHostToDevice));
@@ -831,6 +866,10 @@ int build_tc(HaB200Plan *P) {
 			if (cudaMalloc(&ch.d_tct[c], cnt * sizeof(TcTile)) != cudaSuccess) return kHaErrorAlloc;
 			if (!ch.tct[c].empty())
 				HA_CUDA(cudaMemcpy(ch.d_tct[c], ch.tct[c].data(), ch.tct[c].size() * sizeof(TcTile), cudaMemcpyHostToDevice));
+			const size_t co = std::max<size_t>(ch.tco[c].size(), 1);
+			if (cudaMalloc(&ch.d_tco[c], co * sizeof(int32_t)) != cudaSuccess) return kHaErrorAlloc;
+			if (!ch.tco[c].empty())
+				HA_CUDA(cudaMemcpy(ch.d_tco[c], ch.tco[c].data(), ch.tco[c].size() * sizeof(int32_t), cudaMemcpyHostToDevice));
 		}
 	}
 	if ((rc = P->tcXp.ensure((size_t)maxX)) != kHaSuccess) return rc;
@@ -838,6 +877,22 @@ int build_tc(HaB200Plan *P) {
 	if ((rc = P->tcA.ensure((size_t)maxA)) != kHaSuccess) return rc;
 	if ((rc = P->tcRes.ensure((size_t)P->max_slots * kTcResSlots)) != kHaSuccess) return rc;
 	if ((rc = P->tcSt.ensure((size_t)P->max_slots * 2)) != kHaSuccess) return rc;
+	{
+		const std::vector<NsStep> sched = ns_schedule();
+		const size_t m = sched.size();
+		std::vector<float> hc((size_t)2 * m);
+		std::vector<int32_t> hp(m);
+		for (size_t k = 0; k < m; k++) {
+			hc[k] = sched[k].c1;
+			hc[m + k] = sched[k].c3;
+			hp[k] = sched[k].plain;
+		}
+		if ((rc = P->tcSched.ensure(2 * m)) != kHaSuccess) return rc;
+		if ((rc = P->tcPlain.ensure(m)) != kHaSuccess) return rc;
+		if ((rc = P->tcQueue.ensure(2)) != kHaSuccess) return rc;
+		HA_CUDA(cudaMemcpy(P->tcSched.p, hc.data(), hc.size() * sizeof(float), cudaMemcpyHostToDevice));
+		HA_CUDA(cudaMemcpy(P->tcPlain.p, hp.data(), hp.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+	}
 	P->tc_ready = true;
 	return kHaSuccess;
 }
@@ -902,6 +957,29 @@ int run_procrustes_tc(HaB200Plan *P, const double *d_X, const double *d_Y, bool 
 		a.res_part = P->tcRes.p;
 		a.tol_stop = (float)ns_tol();
 		a.err = P->counters.p + 4;
+		if (tc_persistent()) {
+			// one launch per size class; the larger searchlights first
+			HA_CUDA(cudaMemsetAsync(P->tcQueue.p, 0, 2 * sizeof(int32_t), st));
+			TcSolveArgs sa = {};
+			sa.work = ch.d_tcw;
+			sa.Xb = P->tcXb.p; sa.Yb = P->tcYb.p; sa.vplane = vplane; sa.ntp = ntp; sa.sl_idx = P->idx.p;
+			sa.Xp = P->tcXp.p; sa.Pp = P->tcPp.p; sa.A32 = P->tcA.p; sa.T = T; sa.t_rowmajor = rowmajor;
+			sa.c1 = P->tcSched.p; sa.c3 = P->tcSched.p + maxit; sa.plain = P->tcPlain.p; sa.maxit = maxit;
+			sa.tol_stop = (float)ns_tol(); sa.stats = P->stats.p; sa.err = P->counters.p + 4;
+			for (int c = 1; c >= 0; c--) {
+				const int cnt = (int)ch.tco[c].size();
+				if (!cnt) continue;
+				sa.order = ch.d_tco[c];
+				sa.count = cnt;
+				sa.queue = P->tcQueue.p + c;
+				const int per_sm = c ? 1 : tc_small_ctas_per_sm();
+				sa.smem_bytes = per_sm == 2 ? kTcSmemSmall : kTcSmemLarge;
+				const int grid = std::min(cnt, g_num_sms * per_sm);
+				HA_LAUNCH(kHaB200KTcNs, st);
+				k_tc_solve<<<grid, kTcThreads, sa.smem_bytes, st>>>(sa);
+			}
+			HA_CUDA(cudaGetLastError());
+		} else {
 		if ((rc = launch_tc<kTcPhaseXcov>(ch, a, st, kHaB200KTcXcov)) != kHaSuccess) return rc;
 		{ HA_LAUNCH(kHaB200KTcNs, st); k_tc_ns_init<<<nsl, 256, 0, st>>>(ch.d_tcw, P->tcA.p, P->tcXp.p, P->tcSt.p, P->tcRes.p); }
 		for (int k = 0; k < maxit; k++) {
@@ -916,6 +994,7 @@ int run_procrustes_tc(HaB200Plan *P, const double *d_X, const double *d_Y, bool 
 		}
 		{ HA_LAUNCH(kHaB200KTcNs, st); k_tc_ns_finish<<<nsl, 256, 0, st>>>(ch.d_tcw, P->tcA.p, T, P->tcSt.p + (size_t)(maxit & 1) * P->max_slots,
 		                                                              P->stats.p, rowmajor); }
+		}
 		{ HA_LAUNCH(kHaB200KTcNs, st); k_tc_complete<<<nsl, 256, 0, st>>>(ch.d_tcw, T, P->tcXp.p, P->tcPp.p, P->stats.p, rowmajor); }
 		// float64 Jacobi re-solve of the searchlights still flagged (cold start)
 		{
@@ -1952,6 +2031,7 @@ int ha_b200_init(void) {
 		return kHaErrorInternal;
 	}
 	if (cudaFree(0) != cudaSuccess) return kHaErrorInternal;
+	g_num_sms = prop.multiProcessorCount;
 	g_inited = true;
 	return kHaSuccess;
 }
@@ -2101,8 +2181,10 @@ void ha_b200_plan_destroy(HaB200Plan *P) {
 		if (ch.d_weig) cudaFree(ch.d_weig);
 		if (ch.d_tofs) cudaFree(ch.d_tofs);
 		if (ch.d_tcw) cudaFree(ch.d_tcw);
-		for (int c = 0; c < 2; c++)
+		for (int c = 0; c < 2; c++) {
 			if (ch.d_tct[c]) cudaFree(ch.d_tct[c]);
+			if (ch.d_tco[c]) cudaFree(ch.d_tco[c]);
+		}
 	}
 	P->idx.release(); P->off.release(); P->lo.release(); P->hi.release(); P->w.release();
 	P->vlptr.release(); P->vlent.release(); P->patptr.release(); P->patcol.release();
@@ -2112,7 +2194,7 @@ void ha_b200_plan_destroy(HaB200Plan *P) {
 	P->grows.release(); P->gtpos.release(); P->gurows.release(); P->guntested.release(); P->gmdl.release();
 	P->gfit.release(); P->gfeat.release(); P->gwork.release();
 	P->tcXb.release(); P->tcYb.release(); P->tcXp.release(); P->tcPp.release(); P->tcA.release(); P->tcRes.release();
-	P->tcSt.release();
+	P->tcSt.release(); P->tcSched.release(); P->tcPlain.release(); P->tcQueue.release();
 	delete P;
 }
 

@@ -33,7 +33,7 @@
 namespace hab200 {
 
 constexpr int kTcThreads = 128;
-constexpr int kTcMaxStages = 4;
+constexpr int kTcMaxStages = 8;
 constexpr int kTcMaxNp = 512;                  // largest padded searchlight size (four 128-row tiles)
 constexpr int kTcResSlots = 16;                // residual partials per searchlight: tiles x warps
 constexpr uint64_t kTcWaitNs = 2000000000ull;  // a pipeline wait longer than 2 s is declared failed
@@ -143,12 +143,20 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_keep(int keep) {
 	// wait until at most `keep` groups are pending (immediate operand, so one branch per value)
-	if (keep <= 1)
+	if (keep <= 0)
+		asm volatile("cp.async.wait_group 0;" ::: "memory");
+	else if (keep == 1)
 		asm volatile("cp.async.wait_group 1;" ::: "memory");
 	else if (keep == 2)
 		asm volatile("cp.async.wait_group 2;" ::: "memory");
-	else
+	else if (keep == 3)
 		asm volatile("cp.async.wait_group 3;" ::: "memory");
+	else if (keep == 4)
+		asm volatile("cp.async.wait_group 4;" ::: "memory");
+	else if (keep == 5)
+		asm volatile("cp.async.wait_group 5;" ::: "memory");
+	else
+		asm volatile("cp.async.wait_group 6;" ::: "memory");
 }
 __device__ __forceinline__ void fence_proxy_async_smem() {
 	asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -224,12 +232,19 @@ __device__ __forceinline__ void split3(float v, __nv_bfloat16 &hi, __nv_bfloat16
 	lo = __float2bfloat16_rn(r1 - __bfloat162float(mid));
 }
 
-// Eight consecutive FP32 values of one core-matrix row -> 16 bytes in each of the three planes.
+// Eight consecutive FP32 values of one core-matrix row -> 16 bytes in each of the three planes
+// (the same exact split as split3, two values per packed conversion).
 __device__ __forceinline__ void store_split8(const float *v, __nv_bfloat16 *p0, __nv_bfloat16 *p1,
                                              __nv_bfloat16 *p2) {
-	__align__(16) __nv_bfloat16 h[8], m[8], l[8];
+	__nv_bfloat162 h[4], m[4], l[4];
 #pragma unroll
-	for (int i = 0; i < 8; i++) split3(v[i], h[i], m[i], l[i]);
+	for (int i = 0; i < 4; i++) {
+		const float a = v[2 * i], b = v[2 * i + 1];
+		h[i] = __floats2bfloat162_rn(a, b);
+		const float ra = a - __low2float(h[i]), rb = b - __high2float(h[i]);
+		m[i] = __floats2bfloat162_rn(ra, rb);
+		l[i] = __floats2bfloat162_rn(ra - __low2float(m[i]), rb - __high2float(m[i]));
+	}
 	*reinterpret_cast<uint4 *>(p0) = *reinterpret_cast<const uint4 *>(h);
 	*reinterpret_cast<uint4 *>(p1) = *reinterpret_cast<const uint4 *>(m);
 	*reinterpret_cast<uint4 *>(p2) = *reinterpret_cast<const uint4 *>(l);
@@ -252,60 +267,72 @@ __device__ __forceinline__ uint32_t tc_tmem_cols(int N) {
 // core matrix (g, k) (g: 8-row group along M or N, k: which 8-element half of the K-slice) sits at
 // (g * 2 + k) * 128, so LBO = 128 and SBO = 256 for both operand majors.
 
-// Cross-covariance, K-slice ks: A core (mg, k) row r = Xb[sl[128 t + 8 mg + r]][16 ks + 8 k ..],
-// B core (ng, k) row r = Yb[sl[8 ng + r]][16 ks + 8 k ..]; rows past n are zero.
-__device__ __forceinline__ void tc_load_xcov(const TcArgs &a, const int32_t *s_sl, int n, int N, int t, int ks,
-                                             uint32_t stage) {
-	const int per_plane = 256 + 2 * N;
-	const int total = 3 * per_plane;
-	for (int c = threadIdx.x; c < total; c += kTcThreads) {
-		const int plane = c / per_plane;
-		int rem = c - plane * per_plane;
-		const bool isA = rem < 256;
-		if (!isA) rem -= 256;
-		const int core = rem >> 3, r = rem & 7;
-		const int g = core >> 1, k = core & 1;
-		const int row = isA ? (128 * t + 8 * g + r) : (8 * g + r);
-		const uint32_t dst = stage + (isA ? plane * 4096 : 12288 + plane * 32 * N) + core * 128 + r * 16;
-		const __nv_bfloat16 *base = (isA ? a.Xb : a.Yb) + (int64_t)plane * a.vplane;
-		const bool ok = row < n;
-		const __nv_bfloat16 *src = ok ? base + (int64_t)s_sl[row] * a.ntp + 16 * ks + 8 * k : base;
-		cp_async16(dst, src, ok ? 16u : 0u);
+// Per-thread load plan of one tile: the thread's chunks (16 bytes each) of one plane's A and B
+// stages, with their shared-memory offsets and their source element offsets at K-slice 0.  Every
+// source offset grows linearly with the K-slice (by strideA / strideB elements), so a K-slice's
+// loads are one add and one cp.async per chunk and plane.  Chunk c of A (256 per plane) is row
+// r = c & 7 of core matrix c >> 3 = (g, k) = (8-row group, K half); B has 2N chunks per plane.
+constexpr int kTcMaxBChunks = 8;  // 2N / 128 for N <= 512
+struct TcLoadPlan {
+	uint32_t dA[2], dB[kTcMaxBChunks];
+	int32_t sA[2], sB[kTcMaxBChunks];  // -1: zero fill
+	int nB;
+	int32_t strideA, strideB;
+};
+
+// PHASE kTcPhaseXcov: sources are vertex rows of the vertex-major planes (s_sl: the searchlight's
+// vertices); Gram / update: core-tiled planes of the searchlight (npg = np / 8 core groups).
+template <int PHASE>
+__device__ __forceinline__ void tc_plan_tile(TcLoadPlan &lp, const int32_t *s_sl, int n, int np, int ntp, int t) {
+	const int N = np, npg = np >> 3, tid = threadIdx.x;
+#pragma unroll
+	for (int i = 0; i < 2; i++) {
+		const int c = tid + 128 * i, core = c >> 3, r = c & 7, g = core >> 1, k = core & 1;
+		lp.dA[i] = (uint32_t)(core * 128 + r * 16);
+		if (PHASE == kTcPhaseXcov) {
+			const int row = 128 * t + 8 * g + r;
+			lp.sA[i] = row < n ? s_sl[row] * ntp + 8 * k : -1;
+		} else if (PHASE == kTcPhaseGram) {
+			lp.sA[i] = (16 * t + g < npg) ? (k * npg + 16 * t + g) * 64 + 8 * r : -1;
+		} else {
+			lp.sA[i] = (16 * t + g < npg) ? ((16 * t + g) * npg + k) * 64 + 8 * r : -1;
+		}
 	}
+	lp.nB = (2 * N + 127) >> 7;
+#pragma unroll
+	for (int j = 0; j < kTcMaxBChunks; j++) {
+		const int c = tid + 128 * j, core = c >> 3, r = c & 7, g = core >> 1, k = core & 1;
+		lp.dB[j] = (uint32_t)(core * 128 + r * 16);
+		if (c >= 2 * N) lp.sB[j] = -2;  // not a chunk of this tile
+		else if (PHASE == kTcPhaseXcov) lp.sB[j] = (8 * g + r) < n ? s_sl[8 * g + r] * ntp + 8 * k : -1;
+		else lp.sB[j] = (k * npg + g) * 64 + 8 * r;
+	}
+	lp.strideA = (PHASE == kTcPhaseXcov) ? 16 : (PHASE == kTcPhaseGram) ? 128 * npg : 128;
+	lp.strideB = (PHASE == kTcPhaseXcov) ? 16 : 128 * npg;
 }
 
-// Newton-Schulz products, K-slice ks of a searchlight with padded size np (npg = np / 8 core groups):
-//   Gram   (D = X^T X, rows p of tile t):  A core (mg, k) <- X core (2 ks + k, 16 t + mg)  [MN-major]
-//                                          B core (ng, k) <- X core (2 ks + k, ng)        [MN-major]
-//   update (D = X P,   rows i of tile t):  A core (mg, k) <- X core (16 t + mg, 2 ks + k) [K-major]
-//                                          B core (ng, k) <- P core (2 ks + k, ng)        [MN-major]
-template <int PHASE>
-__device__ __forceinline__ void tc_load_ns(const __nv_bfloat16 *Xs, const __nv_bfloat16 *Bs, int np, int t, int ks,
-                                           uint32_t stage) {
-	const int N = np, npg = np >> 3;
-	const int64_t plane_elems = (int64_t)np * np;
-	const int per_plane = 256 + 2 * N;
-	const int total = 3 * per_plane;
-	for (int c = threadIdx.x; c < total; c += kTcThreads) {
-		const int plane = c / per_plane;
-		int rem = c - plane * per_plane;
-		const bool isA = rem < 256;
-		if (!isA) rem -= 256;
-		const int core = rem >> 3, r = rem & 7;
-		const int g = core >> 1, k = core & 1;
-		int cr, cc;  // source core (row group, column group)
-		bool ok = true;
-		if (isA) {
-			if (PHASE == kTcPhaseGram) { cr = 2 * ks + k; cc = 16 * t + g; ok = cc < npg; }
-			else { cr = 16 * t + g; cc = 2 * ks + k; ok = cr < npg; }
-		} else {
-			cr = 2 * ks + k;
-			cc = g;
+// Issue the cp.async copies of K-slice ks into the stage at shared address `stage`.  A planes at
+// A + p * pstrideA, B planes at B + p * pstrideB (elements).
+__device__ __forceinline__ void tc_load_slice(const TcLoadPlan &lp, const __nv_bfloat16 *A, int64_t pstrideA,
+                                              const __nv_bfloat16 *B, int64_t pstrideB, int N, int ks,
+                                              uint32_t stage) {
+	const int32_t oa = ks * lp.strideA, ob = ks * lp.strideB;
+#pragma unroll
+	for (int p = 0; p < 3; p++) {
+		const __nv_bfloat16 *Ap = A + p * pstrideA;
+		const __nv_bfloat16 *Bp = B + p * pstrideB;
+		const uint32_t sa = stage + p * 4096, sb = stage + 12288 + p * 32 * N;
+#pragma unroll
+		for (int i = 0; i < 2; i++) {
+			const bool ok = lp.sA[i] >= 0;
+			cp_async16(sa + lp.dA[i], ok ? Ap + lp.sA[i] + oa : Ap, ok ? 16u : 0u);
 		}
-		const __nv_bfloat16 *src = (isA ? Xs : Bs) + plane * plane_elems;
-		if (ok) src += ((int64_t)cr * npg + cc) * 64 + r * 8;
-		const uint32_t dst = stage + (isA ? plane * 4096 : 12288 + plane * 32 * N) + core * 128 + r * 16;
-		cp_async16(dst, src, ok ? 16u : 0u);
+#pragma unroll
+		for (int j = 0; j < kTcMaxBChunks; j++) {
+			if (j >= lp.nB || lp.sB[j] == -2) break;
+			const bool ok = lp.sB[j] >= 0;
+			cp_async16(sb + lp.dB[j], ok ? Bp + lp.sB[j] + ob : Bp, ok ? 16u : 0u);
+		}
 	}
 }
 
@@ -389,11 +416,12 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_gemm(const TcArgs a) {
 
 	const __nv_bfloat16 *Xs = a.Xp + w.xofs;
 	const __nv_bfloat16 *Bs = (PHASE == kTcPhaseGram) ? Xs : (const __nv_bfloat16 *)(a.Pp + w.pofs);
-	auto load = [&](int ks, int s) {
-		const uint32_t stage = smem0 + s * stage_bytes;
-		if (PHASE == kTcPhaseXcov) tc_load_xcov(a, s_sl, n, N, t, ks, stage);
-		else tc_load_ns<PHASE>(Xs, Bs, np, t, ks, stage);
-	};
+	TcLoadPlan lp;
+	tc_plan_tile<PHASE>(lp, s_sl, n, np, a.ntp, t);
+	const __nv_bfloat16 *srcA = (PHASE == kTcPhaseXcov) ? a.Xb : Xs;
+	const __nv_bfloat16 *srcB = (PHASE == kTcPhaseXcov) ? a.Yb : Bs;
+	const int64_t pstride = (PHASE == kTcPhaseXcov) ? a.vplane : (int64_t)np * np;
+	auto load = [&](int ks, int s) { tc_load_slice(lp, srcA, pstride, srcB, pstride, N, ks, smem0 + s * stage_bytes); };
 
 	// operand majors: cross-covariance K/K, Gram MN/MN, update K/MN
 	const int a_mn = (PHASE == kTcPhaseGram) ? 1 : 0;
@@ -407,16 +435,11 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_gemm(const TcArgs a) {
 			if (j < nk) load(j, j);
 			cp_async_commit();
 		}
+		// K-slice ks: wait for its stage, issue its products, then refill the stage the products of
+		// slice ks - 1 read (so slice ks stays queued on the tensor pipe while the refill waits)
 		for (int ks = 0; ks < nk; ks++) {
 			const int s = ks % S;
-			const int kn = ks + S - 1;
-			if (kn < nk) {
-				// stage kn % S was last read by the products of K-slice ks - 1
-				if (ks >= 1 && !mbar_wait(&s_bar[(ks - 1) % S], (uint32_t)(((ks - 1) / S) & 1))) s_fail = 1;
-				load(kn, kn % S);
-			}
-			cp_async_commit();
-			cp_async_wait_keep(S - 1);
+			cp_async_wait_keep(S - 2);
 			fence_proxy_async_smem();
 			__syncthreads();
 			if (s_fail) { failed = true; break; }
@@ -437,6 +460,13 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_gemm(const TcArgs a) {
 				}
 				mma_commit(&s_bar[s]);
 			}
+			const int kn = ks + S - 1;
+			if (kn < nk) {
+				// stage kn % S was last read by the products of K-slice ks - 1
+				if (ks >= 1 && !mbar_wait(&s_bar[(ks - 1) % S], (uint32_t)(((ks - 1) / S) & 1))) s_fail = 1;
+				load(kn, kn % S);
+			}
+			cp_async_commit();
 		}
 	}
 	cp_async_wait_all();
@@ -510,6 +540,347 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_gemm(const TcArgs a) {
 	} else if (tid == 0) {
 		atomicOr(a.err, 1);
 	}
+	tc_fence_before();
+	__syncthreads();
+	if (warp == 0) tmem_dealloc(tmem, ncols);
+}
+
+// ---------------------------------------------------------------------------------------------
+// persistent solve: one CTA runs whole searchlights
+// ---------------------------------------------------------------------------------------------
+// Each CTA takes searchlights from a queue (largest first) and runs the whole solve of one
+// searchlight before the next: the cross-covariance tiles, X_0 = A / u, every Gram and update
+// phase (the residual is summed in shared memory), the trace for the scaling.  The searchlight's
+// planes (~12 np^2 bytes) stay in L2 across its iterations instead of streaming through DRAM
+// once per phase, and the whole step is one launch per size class.  The products are the same
+// as k_tc_gemm's; mbarrier phases are tracked per stage across tiles and searchlights.
+
+struct TcSolveArgs {
+	const TcWork *work;
+	const int32_t *order;  // work indices of this launch's size class, largest first
+	int count;
+	int32_t *queue;        // next position in `order` (zero before the launch)
+	const __nv_bfloat16 *Xb;
+	const __nv_bfloat16 *Yb;
+	int64_t vplane;
+	int ntp;
+	const int32_t *sl_idx;
+	__nv_bfloat16 *Xp;
+	__nv_bfloat16 *Pp;
+	float *A32;
+	float *T;
+	int t_rowmajor;
+	const float *c1;  // schedule, maxit entries
+	const float *c3;
+	const int32_t *plain;
+	int maxit;
+	float tol_stop;
+	SlStats *stats;
+	int smem_bytes;
+	int *err;
+};
+
+struct TcPipe {
+	uint32_t uses[kTcMaxStages];  // completed commits per stage barrier (identical in every thread)
+	uint32_t acc;                 // completed commits of the accumulator barrier
+};
+
+__device__ __forceinline__ float block_sum128(float v, float *red) {
+	v = warp_sum(v);
+	__syncthreads();
+	if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+	__syncthreads();
+	return red[0] + red[1] + red[2] + red[3];
+}
+
+// One 128-row tile of one phase, inside the persistent CTA.  Returns false (in every thread) when
+// a wait timed out.  On return all products are complete and the epilogue's stores are issued.
+template <int PHASE>
+__device__ bool tc_tile(const TcSolveArgs &a, const TcWork &w, int t, const int32_t *s_sl, float c1, float c3,
+                        bool final_update, TcPipe &pp, uint64_t *s_bar, uint64_t *s_acc, uint32_t tmem,
+                        uint32_t smem0, int S, int stage_bytes, int *s_fail, float *s_res) {
+	const int n = w.n, np = w.np, N = np;
+	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+	const int nk = (PHASE == kTcPhaseXcov) ? (a.ntp >> 4) : (np >> 4);
+	const __nv_bfloat16 *Xs = a.Xp + w.xofs;
+	const __nv_bfloat16 *Bs = (PHASE == kTcPhaseGram) ? Xs : (const __nv_bfloat16 *)(a.Pp + w.pofs);
+	TcLoadPlan lp;
+	tc_plan_tile<PHASE>(lp, s_sl, n, np, a.ntp, t);
+	const __nv_bfloat16 *srcA = (PHASE == kTcPhaseXcov) ? a.Xb : Xs;
+	const __nv_bfloat16 *srcB = (PHASE == kTcPhaseXcov) ? a.Yb : Bs;
+	const int64_t pstride = (PHASE == kTcPhaseXcov) ? a.vplane : (int64_t)np * np;
+	auto load = [&](int ks, int s) { tc_load_slice(lp, srcA, pstride, srcB, pstride, N, ks, smem0 + s * stage_bytes); };
+	const int a_mn = (PHASE == kTcPhaseGram) ? 1 : 0;
+	const int b_mn = (PHASE == kTcPhaseXcov) ? 0 : 1;
+	const int N0 = N > 256 ? 256 : N;
+	const uint32_t id0 = mma_idesc(128, N0, a_mn, b_mn);
+	const uint32_t id1 = N > 256 ? mma_idesc(128, N - 256, a_mn, b_mn) : 0u;
+
+	// every stage is free here: the previous tile's products all completed
+	for (int j = 0; j < S - 1; j++) {
+		if (j < nk) load(j, j);
+		cp_async_commit();
+	}
+	bool failed = false;
+	for (int ks = 0; ks < nk; ks++) {
+		const int s = ks % S;
+		cp_async_wait_keep(S - 2);
+		fence_proxy_async_smem();
+		__syncthreads();
+		if (*s_fail) { failed = true; break; }
+		if (tid == 0) {
+			tc_fence_after();
+			const uint32_t st = smem0 + s * stage_bytes;
+#pragma unroll
+			for (int q = 0; q < 6; q++) {
+				const int pa = (q == 0) ? 2 : (q == 2 || q == 3) ? 1 : 0;
+				const int pb = (q == 1) ? 2 : (q == 2 || q == 4) ? 1 : 0;
+				const uint32_t acc = (ks > 0 || q > 0) ? 1u : 0u;
+				const uint64_t ad = smem_desc(st + pa * 4096, 128, 256);
+				const uint32_t baddr = st + 12288 + pb * 32 * N;
+				mma_bf16(tmem, ad, smem_desc(baddr, 128, 256), id0, acc);
+				if (N > 256) mma_bf16(tmem + 256, ad, smem_desc(baddr + 32 * 256, 128, 256), id1, acc);
+			}
+			mma_commit(&s_bar[s]);
+		}
+		pp.uses[s]++;
+		// refill the stage the products of K-slice ks - 1 read, while slice ks stays queued
+		const int kn = ks + S - 1;
+		if (kn < nk) {
+			const int sp = kn % S;
+			if (ks >= 1 && !mbar_wait(&s_bar[sp], (pp.uses[sp] - 1u) & 1u)) *s_fail = 1;
+			load(kn, sp);
+		}
+		cp_async_commit();
+	}
+	cp_async_wait_all();
+	if (!failed) {
+		if (tid == 0) mma_commit(s_acc);
+		pp.acc++;
+		if (!mbar_wait(s_acc, (pp.acc - 1u) & 1u)) *s_fail = 1;
+	}
+	__syncthreads();
+	if (*s_fail) return false;
+	tc_fence_after();
+
+	const int m = 32 * warp + lane;
+	const int row = 128 * t + m;
+	const uint32_t trow = tmem + ((uint32_t)(32 * warp) << 16);
+	const int npg = np >> 3;
+	float res = 0.f;
+	for (int c0 = 0; c0 < N; c0 += 16) {
+		float v[16];
+		tmem_ld16(trow + (uint32_t)c0, v);
+		if (row >= np) continue;
+		if (PHASE == kTcPhaseXcov) {
+			if (row < n) {
+				float4 *dst = reinterpret_cast<float4 *>(a.A32 + w.aofs + (int64_t)row * np + c0);
+#pragma unroll
+				for (int q = 0; q < 4; q++) dst[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+			}
+		} else if (PHASE == kTcPhaseGram) {
+#pragma unroll
+			for (int q = 0; q < 16; q++) {
+				const int col = c0 + q;
+				const float g = v[q];
+				if (row < n && col < n) {
+					const float d = g - (col == row ? 1.f : 0.f);
+					res += d * d;
+				}
+				v[q] = c3 * g + (col == row ? c1 : 0.f);
+			}
+			__nv_bfloat16 *P0 = a.Pp + w.pofs;
+			const int64_t pe = (int64_t)np * np;
+#pragma unroll
+			for (int h = 0; h < 2; h++) {
+				const int64_t o = ((int64_t)(row >> 3) * npg + (c0 >> 3) + h) * 64 + (row & 7) * 8;
+				store_split8(v + 8 * h, P0 + o, P0 + pe + o, P0 + 2 * pe + o);
+			}
+		} else if (final_update) {
+			if (row < n) {
+				float *T = a.T + w.tofs;
+				for (int q = 0; q < 16; q++) {
+					const int col = c0 + q;
+					if (col < n) T[a.t_rowmajor ? (int64_t)row * n + col : (int64_t)col * n + row] = v[q];
+				}
+			}
+		} else {
+			__nv_bfloat16 *X0 = a.Xp + w.xofs;
+			const int64_t pe = (int64_t)np * np;
+#pragma unroll
+			for (int h = 0; h < 2; h++) {
+				const int64_t o = ((int64_t)(row >> 3) * npg + (c0 >> 3) + h) * 64 + (row & 7) * 8;
+				store_split8(v + 8 * h, X0 + o, X0 + pe + o, X0 + 2 * pe + o);
+			}
+		}
+	}
+	if (PHASE == kTcPhaseGram) {
+		res = warp_sum(res);
+		if (lane == 0) s_res[t * 4 + warp] = res;
+	}
+	// the next tile's products overwrite tensor memory: order this tile's reads before them, and
+	// make the global stores visible to the next phase's cp.async reads (through L2)
+	tc_fence_before();
+	__threadfence();
+	__syncthreads();
+	return true;
+}
+
+__global__ void __launch_bounds__(kTcThreads) k_tc_solve(const TcSolveArgs a) {
+	extern __shared__ __align__(128) unsigned char tc_smem[];
+	__shared__ uint64_t s_bar[kTcMaxStages];
+	__shared__ uint64_t s_acc;
+	__shared__ uint32_t s_tmem;
+	__shared__ int s_fail, s_item;
+	__shared__ int32_t s_sl[kTcMaxNp];
+	__shared__ float s_res[kTcResSlots];
+	__shared__ float s_red[4];
+	__shared__ float s_u;
+	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+	const uint32_t smem0 = smem_u32(tc_smem);
+	// tensor memory for the largest accumulator this launch can meet
+	const uint32_t ncols = a.smem_bytes > 120 * 1024 ? 512u : 256u;
+	if (tid == 0) {
+		for (int i = 0; i < kTcMaxStages; i++) mbar_init(&s_bar[i], 1);
+		mbar_init(&s_acc, 1);
+		s_fail = 0;
+		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+	}
+	if (warp == 0) tmem_alloc(&s_tmem, ncols);
+	tc_fence_before();
+	__syncthreads();
+	tc_fence_after();
+	const uint32_t tmem = s_tmem;
+	TcPipe pp = {};
+	bool failed = false;
+	for (;;) {
+		if (tid == 0) s_item = atomicAdd(a.queue, 1);
+		__syncthreads();
+		const int item = s_item;
+		if (item >= a.count) break;
+		const TcWork w = a.work[a.order[item]];
+		const int n = w.n, np = w.np, ntiles = (np + 127) >> 7;
+		const int stage_bytes = tc_stage_bytes(np);
+		int S = a.smem_bytes / stage_bytes;
+		if (S > kTcMaxStages) S = kTcMaxStages;
+		if (S < 2 || (uint32_t)np > ncols) { s_fail = 1; failed = true; break; }
+		for (int i = tid; i < n; i += kTcThreads) s_sl[i] = a.sl_idx[w.sofs + i];
+		__syncthreads();
+		// cross-covariance A = X_sl^T Y_sl
+		for (int t = 0; t < ntiles && !failed; t++)
+			failed = !tc_tile<kTcPhaseXcov>(a, w, t, s_sl, 0.f, 0.f, false, pp, s_bar, &s_acc, tmem, smem0, S,
+			                                 stage_bytes, &s_fail, s_res);
+		if (failed) break;
+		// X_0 = A / u, u = min(||A||_F, sqrt(||A||_1 ||A||_inf)) >= sigma_max
+		const float *A = a.A32 + w.aofs;
+		{
+			float *colsum = reinterpret_cast<float *>(tc_smem);  // the stages are free here
+			float fro = 0.f, rowmax = 0.f;
+			for (int r = warp; r < n; r += 4) {
+				float rs = 0.f;
+				for (int c = lane; c < n; c += 32) {
+					const float x = A[(int64_t)r * np + c];
+					fro += x * x;
+					rs += fabsf(x);
+				}
+				rowmax = fmaxf(rowmax, warp_sum(rs));
+			}
+			for (int c = tid; c < n; c += kTcThreads) {
+				float cs = 0.f;
+				for (int r = 0; r < n; r++) cs += fabsf(A[(int64_t)r * np + c]);
+				colsum[c] = cs;
+			}
+			const float f = block_sum128(fro, s_red);
+			float cm = 0.f;
+			for (int c = tid; c < n; c += kTcThreads) cm = fmaxf(cm, colsum[c]);
+			for (int o = 16; o > 0; o >>= 1) {
+				cm = fmaxf(cm, __shfl_xor_sync(0xffffffffu, cm, o));
+				rowmax = fmaxf(rowmax, __shfl_xor_sync(0xffffffffu, rowmax, o));
+			}
+			__syncthreads();
+			if (lane == 0) { s_red[warp] = cm; colsum[kTcMaxNp + warp] = rowmax; }
+			__syncthreads();
+			if (tid == 0) {
+				float cmax = 0.f, rmax = 0.f;
+				for (int i = 0; i < 4; i++) { cmax = fmaxf(cmax, s_red[i]); rmax = fmaxf(rmax, colsum[kTcMaxNp + i]); }
+				double u = fmin(sqrt((double)f), sqrt((double)rmax * (double)cmax));
+				if (!(u > 0.0)) u = 1.0;
+				s_u = (float)(u * (1.0 + 1e-6));
+			}
+			__syncthreads();
+			const float inv = 1.f / s_u;
+			const int npg = np >> 3;
+			const int64_t pe = (int64_t)np * np;
+			__nv_bfloat16 *X0 = a.Xp + w.xofs;
+			for (int64_t e = tid; e < (int64_t)np * npg; e += kTcThreads) {
+				const int row = (int)(e / npg), cg = (int)(e - (int64_t)row * npg);
+				float v[8];
+#pragma unroll
+				for (int q = 0; q < 8; q++) {
+					const int col = 8 * cg + q;
+					v[q] = (row < n && col < n) ? A[(int64_t)row * np + col] * inv : 0.f;
+				}
+				const int64_t o = ((int64_t)(row >> 3) * npg + cg) * 64 + (row & 7) * 8;
+				store_split8(v, X0 + o, X0 + pe + o, X0 + 2 * pe + o);
+			}
+			__threadfence();
+			__syncthreads();
+		}
+		// the iteration
+		bool conv = false, stalled = false, prev_plain = false;
+		double prev_res = 0.0;
+		int k = 0;
+		for (; k < a.maxit; k++) {
+			if (tid < kTcResSlots) s_res[tid] = 0.f;
+			__syncthreads();
+			const float c1 = a.c1[k], c3 = a.c3[k];
+			const bool plain = a.plain[k] != 0;
+			for (int t = 0; t < ntiles && !failed; t++)
+				failed = !tc_tile<kTcPhaseGram>(a, w, t, s_sl, c1, c3, false, pp, s_bar, &s_acc, tmem, smem0, S,
+				                                 stage_bytes, &s_fail, s_res);
+			if (failed) break;
+			double ss = 0.0;
+			for (int i = 0; i < kTcResSlots; i++) ss += (double)s_res[i];
+			const double resd = sqrt(ss / (double)n);
+			conv = plain && (float)resd < a.tol_stop;
+			stalled = !conv && plain && prev_plain && fabs(resd - prev_res) <= 5e-7 * resd;
+			const bool final_update = conv || stalled || k == a.maxit - 1;
+			for (int t = 0; t < ntiles && !failed; t++)
+				failed = !tc_tile<kTcPhaseUpdate>(a, w, t, s_sl, 0.f, 0.f, final_update, pp, s_bar, &s_acc, tmem,
+				                                   smem0, S, stage_bytes, &s_fail, s_res);
+			if (failed) break;
+			prev_plain = plain;
+			prev_res = (double)(float)resd;
+			if (final_update) { k++; break; }
+		}
+		if (failed) break;
+		// sum of singular values = trace(T^T A) (the scaling numerator), flags
+		{
+			const float *T = a.T + w.tofs;
+			double s = 0.0;
+			for (int64_t e = tid; e < (int64_t)n * n; e += kTcThreads) {
+				const int r = (int)(e / n), c = (int)(e - (int64_t)r * n);
+				const float tv = a.t_rowmajor ? T[(int64_t)r * n + c] : T[(int64_t)c * n + r];
+				s += (double)tv * (double)A[(int64_t)r * np + c];
+			}
+			s = warp_sum(s);
+			__syncthreads();
+			double *red = reinterpret_cast<double *>(tc_smem);
+			if (lane == 0) red[warp] = s;
+			__syncthreads();
+			if (tid == 0) {
+				SlStats o = {};
+				o.s_sum = red[0] + red[1] + red[2] + red[3];
+				o.s_max = (double)s_u;
+				o.sweeps = k;
+				o.flags = conv ? 0 : kFlagIllCond;
+				a.stats[w.slot] = o;
+			}
+			__syncthreads();
+		}
+	}
+	if (failed && tid == 0) atomicOr(a.err, 1);
+	cp_async_wait_all();
 	tc_fence_before();
 	__syncthreads();
 	if (warp == 0) tmem_dealloc(tmem, ncols);
