@@ -20,6 +20,7 @@
 // Storage of a searchlight's iterate X and of P = c1 I + c3 G in HBM: three bf16 planes of
 // np x np (np = n rounded up to 16), each in 8 x 8 core matrices, core (r, c) = rows 8r..8r+7,
 // columns 8c..8c+7 at element offset (r * np/8 + c) * 64, row-major inside (16 bytes a row).
+// The iterate alternates between two buffers (the update reads one and writes the other).
 // The same bytes serve as a K-major operand (X in X P) and as an MN-major operand (X in X^T X,
 // P in X P), so no transposed copy exists.  Padding rows and columns are zero and stay zero.
 #pragma once
@@ -35,7 +36,7 @@ namespace hab200 {
 constexpr int kTcThreads = 128;
 constexpr int kTcMaxStages = 8;
 constexpr int kTcMaxNp = 512;                  // largest padded searchlight size (four 128-row tiles)
-constexpr int kTcResSlots = 16;                // residual partials per searchlight: tiles x warps
+constexpr int kTcResSlots = 32;                // residual partials per searchlight: row tiles x column halves x warps
 constexpr uint64_t kTcWaitNs = 2000000000ull;  // a pipeline wait longer than 2 s is declared failed
 
 enum : int { kTcPhaseXcov = 0, kTcPhaseGram = 1, kTcPhaseUpdate = 2 };
@@ -54,9 +55,13 @@ struct TcWork {
 	int64_t tofs;  // float element offset of T in the T scratch (n x n)
 };
 
+// One CTA's output tile: 128 rows x nn columns starting at column n0 (nn <= 256; searchlights with
+// np > 256 have two column halves, so every tile fits two CTAs per SM).
 struct TcTile {
-	int32_t w;  // work index
-	int32_t t;  // 128-row tile
+	int32_t w;   // work index
+	int32_t t;   // 128-row tile
+	int32_t n0;  // first column
+	int32_t nn;  // columns (a multiple of 16)
 };
 
 // Per-searchlight iteration state; one copy is read and the other written by each update launch.
@@ -81,7 +86,9 @@ struct TcArgs {
 	int ntp;
 	const int32_t *sl_idx;
 	// Newton-Schulz
-	__nv_bfloat16 *Xp;  // iterate planes (offsets from TcWork::xofs)
+	__nv_bfloat16 *Xp;  // iterate planes (offsets from TcWork::xofs), read
+	__nv_bfloat16 *Xw;  // where the update writes the next iterate: the other of two buffers, since the
+	                    // two column halves of a row tile both read the whole row tile of X
 	__nv_bfloat16 *Pp;  // P planes (TcWork::pofs)
 	float *A32;         // cross-covariance (TcWork::aofs)
 	float *T;           // T scratch (TcWork::tofs)
@@ -283,8 +290,9 @@ struct TcLoadPlan {
 // PHASE kTcPhaseXcov: sources are vertex rows of the vertex-major planes (s_sl: the searchlight's
 // vertices); Gram / update: core-tiled planes of the searchlight (npg = np / 8 core groups).
 template <int PHASE>
-__device__ __forceinline__ void tc_plan_tile(TcLoadPlan &lp, const int32_t *s_sl, int n, int np, int ntp, int t) {
-	const int N = np, npg = np >> 3, tid = threadIdx.x;
+__device__ __forceinline__ void tc_plan_tile(TcLoadPlan &lp, const int32_t *s_sl, int n, int np, int ntp, int t,
+                                             int n0, int N) {
+	const int npg = np >> 3, g0 = n0 >> 3, tid = threadIdx.x;
 #pragma unroll
 	for (int i = 0; i < 2; i++) {
 		const int c = tid + 128 * i, core = c >> 3, r = c & 7, g = core >> 1, k = core & 1;
@@ -304,8 +312,8 @@ __device__ __forceinline__ void tc_plan_tile(TcLoadPlan &lp, const int32_t *s_sl
 		const int c = tid + 128 * j, core = c >> 3, r = c & 7, g = core >> 1, k = core & 1;
 		lp.dB[j] = (uint32_t)(core * 128 + r * 16);
 		if (c >= 2 * N) lp.sB[j] = -2;  // not a chunk of this tile
-		else if (PHASE == kTcPhaseXcov) lp.sB[j] = (8 * g + r) < n ? s_sl[8 * g + r] * ntp + 8 * k : -1;
-		else lp.sB[j] = (k * npg + g) * 64 + 8 * r;
+		else if (PHASE == kTcPhaseXcov) lp.sB[j] = (n0 + 8 * g + r) < n ? s_sl[n0 + 8 * g + r] * ntp + 8 * k : -1;
+		else lp.sB[j] = (k * npg + g0 + g) * 64 + 8 * r;
 	}
 	lp.strideA = (PHASE == kTcPhaseXcov) ? 16 : (PHASE == kTcPhaseGram) ? 128 * npg : 128;
 	lp.strideB = (PHASE == kTcPhaseXcov) ? 16 : 128 * npg;
@@ -354,7 +362,11 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_gemm(const TcArgs a) {
 	const TcTile tl = a.tiles[blockIdx.x];
 	const TcWork w = a.work[tl.w];
 	const int n = w.n, np = w.np, t = tl.t;
-	const int N = np;
+	const int n0 = tl.n0, N = tl.nn;
+	if (PHASE == kTcPhaseUpdate && a.Xw == nullptr) {  // no target for the next iterate: refuse
+		if (threadIdx.x == 0) atomicOr(a.err, 1);
+		return;
+	}
 	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
 	const float c1 = a.c1, c3 = a.c3;
@@ -417,7 +429,7 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_gemm(const TcArgs a) {
 	const __nv_bfloat16 *Xs = a.Xp + w.xofs;
 	const __nv_bfloat16 *Bs = (PHASE == kTcPhaseGram) ? Xs : (const __nv_bfloat16 *)(a.Pp + w.pofs);
 	TcLoadPlan lp;
-	tc_plan_tile<PHASE>(lp, s_sl, n, np, a.ntp, t);
+	tc_plan_tile<PHASE>(lp, s_sl, n, np, a.ntp, t, n0, N);
 	const __nv_bfloat16 *srcA = (PHASE == kTcPhaseXcov) ? a.Xb : Xs;
 	const __nv_bfloat16 *srcB = (PHASE == kTcPhaseXcov) ? a.Yb : Bs;
 	const int64_t pstride = (PHASE == kTcPhaseXcov) ? a.vplane : (int64_t)np * np;
@@ -491,14 +503,14 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_gemm(const TcArgs a) {
 			if (row >= np) continue;
 			if (PHASE == kTcPhaseXcov) {
 				if (row < n) {
-					float4 *dst = reinterpret_cast<float4 *>(a.A32 + w.aofs + (int64_t)row * np + c0);
+					float4 *dst = reinterpret_cast<float4 *>(a.A32 + w.aofs + (int64_t)row * np + n0 + c0);
 #pragma unroll
 					for (int q = 0; q < 4; q++) dst[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
 				}
 			} else if (PHASE == kTcPhaseGram) {
 #pragma unroll
 				for (int q = 0; q < 16; q++) {
-					const int col = c0 + q;
+					const int col = n0 + c0 + q;
 					const float g = v[q];
 					if (row < n && col < n) {
 						const float d = g - (col == row ? 1.f : 0.f);
@@ -510,7 +522,7 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_gemm(const TcArgs a) {
 				const int64_t pe = (int64_t)np * np;
 #pragma unroll
 				for (int h = 0; h < 2; h++) {
-					const int64_t o = ((int64_t)(row >> 3) * npg + (c0 >> 3) + h) * 64 + (row & 7) * 8;
+					const int64_t o = ((int64_t)(row >> 3) * npg + ((n0 + c0) >> 3) + h) * 64 + (row & 7) * 8;
 					store_split8(v + 8 * h, P0 + o, P0 + pe + o, P0 + 2 * pe + o);
 				}
 			} else {
@@ -518,16 +530,16 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_gemm(const TcArgs a) {
 					if (row < n) {
 						float *T = a.T + w.tofs;
 						for (int q = 0; q < 16; q++) {
-							const int col = c0 + q;
+							const int col = n0 + c0 + q;
 							if (col < n) T[a.t_rowmajor ? (int64_t)row * n + col : (int64_t)col * n + row] = v[q];
 						}
 					}
 				} else {
-					__nv_bfloat16 *X0 = a.Xp + w.xofs;
+					__nv_bfloat16 *X0 = a.Xw + w.xofs;
 					const int64_t pe = (int64_t)np * np;
 #pragma unroll
 					for (int h = 0; h < 2; h++) {
-						const int64_t o = ((int64_t)(row >> 3) * npg + (c0 >> 3) + h) * 64 + (row & 7) * 8;
+						const int64_t o = ((int64_t)(row >> 3) * npg + ((n0 + c0) >> 3) + h) * 64 + (row & 7) * 8;
 						store_split8(v + 8 * h, X0 + o, X0 + pe + o, X0 + 2 * pe + o);
 					}
 				}
@@ -535,7 +547,7 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_gemm(const TcArgs a) {
 		}
 		if (PHASE == kTcPhaseGram) {
 			res = warp_sum(res);
-			if (lane == 0) a.res_part[(int64_t)w.slot * kTcResSlots + t * 4 + warp] = res;
+			if (lane == 0) a.res_part[(int64_t)w.slot * kTcResSlots + (2 * t + (n0 > 0 ? 1 : 0)) * 4 + warp] = res;
 		}
 	} else if (tid == 0) {
 		atomicOr(a.err, 1);
@@ -605,7 +617,7 @@ __device__ bool tc_tile(const TcSolveArgs &a, const TcWork &w, int t, const int3
 	const __nv_bfloat16 *Xs = a.Xp + w.xofs;
 	const __nv_bfloat16 *Bs = (PHASE == kTcPhaseGram) ? Xs : (const __nv_bfloat16 *)(a.Pp + w.pofs);
 	TcLoadPlan lp;
-	tc_plan_tile<PHASE>(lp, s_sl, n, np, a.ntp, t);
+	tc_plan_tile<PHASE>(lp, s_sl, n, np, a.ntp, t, 0, N);
 	const __nv_bfloat16 *srcA = (PHASE == kTcPhaseXcov) ? a.Xb : Xs;
 	const __nv_bfloat16 *srcB = (PHASE == kTcPhaseXcov) ? a.Yb : Bs;
 	const int64_t pstride = (PHASE == kTcPhaseXcov) ? a.vplane : (int64_t)np * np;
@@ -716,7 +728,7 @@ __device__ bool tc_tile(const TcSolveArgs &a, const TcWork &w, int t, const int3
 	}
 	if (PHASE == kTcPhaseGram) {
 		res = warp_sum(res);
-		if (lane == 0) s_res[t * 4 + warp] = res;
+		if (lane == 0) s_res[2 * t * 4 + warp] = res;
 	}
 	// the next tile's products overwrite tensor memory: order this tile's reads before them, and
 	// make the global stores visible to the next phase's cp.async reads (through L2)
