@@ -63,13 +63,15 @@ def parse_args():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
-    p.add_argument("--workload", choices=["template", "rankdef", "grid", "learned", "shard", "forrest"], default="rankdef",
+    p.add_argument("--workload", choices=["template", "rankdef", "grid", "learned", "shard", "forrest", "refgpu"],
+                   default="rankdef",
                    help="rankdef (default; 'template' is the same run): the headline Procrustes step on the "
                         "template pair with 10%% singular searchlights, the plain pair as a sub-field; grid: the "
                         "searchlight ridge grid search (40962 vertices, every --grid-step-th searchlight); "
                         "learned: the learned proposal; shard: one "
                         "hemisphere split over the N GPUs (strong scaling); forrest: the shapes of the "
-                        "reference's published run (nt 1818, searchlights of 90-170)")
+                        "reference's published run (nt 1818, searchlights of 90-170); refgpu: the reference's "
+                        "own CUDA arm (oracle/_ref_cuda) against this library on config 1 and the Forrest shape")
     p.add_argument("--grid-step", type=int, default=16)
     p.add_argument("--ref-seconds", type=float, default=0.0,
                    help="reference arm: seconds of CPU work per step (default: 150 s over all steps)")
@@ -560,6 +562,114 @@ def run_b200(args):
 
 
 # ---------------------------------------------------------------------------------------------
+# the reference's own GPU arm on the same B200 (its cuBLAS + cuSOLVER path, rebuilt for sm_100a)
+# ---------------------------------------------------------------------------------------------
+
+def run_refgpu(args):
+    """Config 1 (2562 vertices, nt 200, geodesic-disc searchlights of 71-78, reflection allowed, no
+    scaling) and the Forrest shape (9675 vertices, nt 1818, searchlights of 90-170): the reference's
+    CUDA arm (dense entry, backend 3) against this library's tensor-core solver and its plain FP32
+    form, all from host buffers into a host dense nv x nv matrix, wall clock per call; errors of the
+    dense result against the reference's float64 CPU arm."""
+    import torch
+    from hyperalignment_b200 import _lib as L
+    from hyperalignment_b200 import workloads as W
+    from hyperalignment_b200.plan import Plan
+    from oracle import ref_lib as R
+
+    ws, rank, local = dist_setup(args)
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    lib = L.lib()
+    L.check(lib.ha_b200_init(), "ha_b200_init")
+    if not R.cuda_available():
+        print(json.dumps({"workload": "refgpu", "unavailable": "oracle/_ref_cuda not built (make -C oracle cuda)"}))
+        return
+    rc_lib = R.cuda_lib()
+    if rc_lib.ha_cuda_init() != 0 or not rc_lib.ha_cuda_available():
+        print(json.dumps({"workload": "refgpu", "unavailable": "the reference's ha_cuda_init failed on this GPU"}))
+        return
+    rc_lib.ha_set_num_threads(os.cpu_count() or 1)
+    R.set_threads(os.cpu_count() or 1)
+    out = {"workload": "reference_gpu_comparison", "unit": UNIT, "higher_is_better": True, "data": "synthetic",
+           "path": "host float64 in, host dense nv x nv float64 out, wall clock per call", "configs": {}}
+    for name, w in (("config1_plain_procrustes", W.plain_procrustes(0)), ("forrest_shaped", W.forrest_shaped(0))):
+        s = w.sls
+        Xf, Yf = np.asfortranarray(w.X), np.asfortranarray(w.Y)
+        nt, nv = w.nt, w.nv
+        ref64 = R.procrustes_dense(w.X, w.Y, s.indices, s.offsets, s.dists, s.radius, True, False, 0)
+        nref = np.linalg.norm(ref64)
+
+        def err(T):
+            return {"relfrob": float(np.linalg.norm(T - ref64) / nref), "maxabs": float(np.abs(T - ref64).max())}
+
+        def time_calls(call, k):
+            call()
+            ts = []
+            for _ in range(k):
+                t0 = time.perf_counter()
+                call()
+                ts.append(time.perf_counter() - t0)
+            return s.count * k / sum(ts), float(np.mean(ts))
+
+        T_ref = np.zeros((nv, nv))
+
+        def ref_call():
+            T_ref[:] = 0.0
+            rc = rc_lib.ha_searchlight_procrustes_dense(
+                Xf.ctypes.data_as(R.c_double_p), Yf.ctypes.data_as(R.c_double_p), nt, nv,
+                s.indices.ctypes.data_as(R.c_int32_p), s.offsets.ctypes.data_as(R.c_int32_p),
+                s.dists.ctypes.data_as(R.c_double_p), s.count, s.radius, T_ref.ctypes.data_as(R.c_double_p),
+                True, False, 3, True)
+            if rc != 0:
+                raise RuntimeError(f"reference CUDA rc={rc}")
+
+        k_ref = max(1, min(args.steps, 3))
+        r_val, r_s = time_calls(ref_call, k_ref)
+        T_tc = np.zeros((nv, nv))
+        argsv = (Xf.ctypes.data_as(L.c_double_p), Yf.ctypes.data_as(L.c_double_p), nt, nv, L.iptr(s.indices),
+                 L.iptr(s.offsets), L.dptr(s.dists), s.count, s.radius, T_tc.ctypes.data_as(L.c_double_p),
+                 True, False, L.BACKEND_B200, True)
+
+        def tc_call():
+            T_tc[:] = 0.0
+            L.check(lib.ha_searchlight_procrustes_dense(*argsv), "dense")
+
+        t_val, t_s = time_calls(tc_call, max(1, min(args.steps, 5)))
+        # plain FP32 form of this library on device-resident inputs (the metric's denominator)
+        plan = Plan.from_workload(w)
+        dX = torch.from_numpy(np.asfortranarray(w.X).ravel(order="F")).cuda()
+        dY = torch.from_numpy(np.asfortranarray(w.Y).ravel(order="F")).cuda()
+        vals = torch.zeros(plan.nnz, dtype=torch.float64, device="cuda")
+        evs = []
+        for i in range(4):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            plan.procrustes_device(dX.data_ptr(), dY.data_ptr(), vals.data_ptr(), True, False, L.SOLVER_FP32,
+                                   L.OUT_CSR)
+            b.record()
+            evs.append((a, b))
+        torch.cuda.synchronize()
+        p_ms = min(a.elapsed_time(b) for a, b in evs[1:])
+        plan.close()
+        sizes = s.sizes
+        out["configs"][name] = {
+            "nv": nv, "nt": nt, "searchlights": s.count, "sl_size_min": int(sizes.min()),
+            "sl_size_max": int(sizes.max()), "reflection": True, "scaling": False,
+            "reference_cuda": {"value": r_val, "seconds_per_call": r_s, "calls": k_ref, "error_vs_cpu64": err(T_ref),
+                               "what": "reference csrc/ha_cuda.cu (cuBLAS SGEMM batched + cuSOLVER "
+                                       "gesvdaStridedBatched, batches of 256 padded to max_sz), -arch sm_100a"},
+            "tensor_core": {"value": t_val, "seconds_per_call": t_s, "error_vs_cpu64": err(T_tc),
+                            "what": "ha_searchlight_procrustes_dense(backend=4), tensor-core solver"},
+            "speedup_vs_reference_cuda": t_val / r_val,
+            "plain_fp32_device": {"value": s.count / (p_ms / 1e3), "ms": p_ms},
+        }
+    rc_lib.ha_cuda_cleanup()
+    print(json.dumps(out))
+
+
+# ---------------------------------------------------------------------------------------------
 # ridge grid search (40962 vertices, sizes 50-500, nt 500, 10 alphas x 4 PC counts, 5 CV folds)
 # and the learned proposal on top of it
 # ---------------------------------------------------------------------------------------------
@@ -1044,6 +1154,8 @@ def main():
         run_shard(args)
     elif args.workload == "forrest":
         run_forrest(args)
+    elif args.workload == "refgpu":
+        run_refgpu(args)
     else:
         run_b200(args)
 

@@ -35,10 +35,41 @@ class TSearchlights(ctypes.Structure):  # csrc/ha_common.h:62-68
 
 
 _lib = None
+REF_CUDA_LIB = os.path.join(HERE, "_ref_cuda", "libhyperalignment_cuda.so")
+_cuda_lib = None
 
 
 def available() -> bool:
     return os.path.exists(REF_LIB)
+
+
+def cuda_available() -> bool:
+    """The reference built with its CUDA arm (make -C oracle cuda) is present."""
+    return os.path.exists(REF_CUDA_LIB)
+
+
+def cuda_lib():
+    """The reference library with its own GPU arm (csrc/ha_cuda.cu, cuBLAS + cuSOLVER) compiled for
+    sm_100a: the dense entry point with backend 3, and ha_cuda_init / cleanup / available
+    (csrc/ha_cuda.h:32-42)."""
+    global _cuda_lib
+    if _cuda_lib is None:
+        os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+        h = ctypes.CDLL(REF_CUDA_LIB)
+        h.ha_searchlight_procrustes_dense.restype = ctypes.c_int
+        h.ha_searchlight_procrustes_dense.argtypes = [
+            c_double_p, c_double_p, ctypes.c_int32, ctypes.c_int32, c_int32_p, c_int32_p, c_double_p,
+            ctypes.c_int32, ctypes.c_double, c_double_p, ctypes.c_bool, ctypes.c_bool, ctypes.c_int, ctypes.c_bool]
+        h.ha_cuda_init.restype = ctypes.c_int
+        h.ha_cuda_init.argtypes = []
+        h.ha_cuda_cleanup.restype = None
+        h.ha_cuda_cleanup.argtypes = []
+        h.ha_cuda_available.restype = ctypes.c_bool
+        h.ha_cuda_available.argtypes = []
+        h.ha_set_num_threads.restype = None
+        h.ha_set_num_threads.argtypes = [ctypes.c_int]
+        _cuda_lib = h
+    return _cuda_lib
 
 
 def lib():
