@@ -602,7 +602,13 @@ def run_refgpu(args):
         nref = np.linalg.norm(ref64)
 
         def err(T):
-            return {"relfrob": float(np.linalg.norm(T - ref64) / nref), "maxabs": float(np.abs(T - ref64).max())}
+            """Relative Frobenius and max-abs error over the finite entries, and how many are not finite
+            (the reference's CUDA arm does not check cuSOLVER's per-matrix status)."""
+            ok = np.isfinite(T)
+            d = np.where(ok, T - ref64, 0.0)
+            bad = np.flatnonzero(~ok.all(axis=1))
+            return {"relfrob": float(np.linalg.norm(d) / nref), "maxabs": float(np.abs(d).max()),
+                    "nonfinite_entries": int((~ok).sum()), "rows_with_nonfinite": int(bad.size)}
 
         def time_calls(call, k):
             call()
