@@ -1736,6 +1736,7 @@ int host_threads() {
 // Cached plan for the host entry points (geometry + weights identify it). The hash only
 // screens; a hit is confirmed against the full key, so a collision rebuilds instead of reusing.
 HaB200Plan *g_cached_plan = nullptr;
+int g_cached_dev = -1;  // device the cached plan and the host-call buffers live on
 uint64_t g_cached_key = 0;
 int g_cached_mode = 0;
 double g_cached_radius = 0.0;
@@ -1769,6 +1770,18 @@ int get_plan(int32_t nt, int32_t nv, const int32_t *idx, const int32_t *off, con
 	if (dists) h = fnv1a(dists, (size_t)off[count] * 8, h);
 	if (weights) h = fnv1a(weights, (size_t)off[count] * 8, h);
 	const double *aux = weights ? weights : dists;  // weights override dists in plan_create_impl
+	int dev = 0;
+	if (cudaGetDevice(&dev) != cudaSuccess) return kHaErrorInternal;
+	if (g_cached_plan && g_cached_dev != dev) {
+		// the caller switched devices: free the old device's plan and buffers on that device
+		if (cudaSetDevice(g_cached_dev) == cudaSuccess) {
+			ha_b200_plan_destroy(g_cached_plan);
+			g_bufs.release();
+			g_fan.release();  // the side streams belong to the old device too
+		}
+		g_cached_plan = nullptr;
+		if (cudaSetDevice(dev) != cudaSuccess) return kHaErrorInternal;
+	}
 	if (g_cached_plan && g_cached_key == h &&
 	    cached_plan_matches(nt, nv, idx, off, count, radius, mode, aux)) {
 		*out = g_cached_plan;
@@ -1781,6 +1794,7 @@ int get_plan(int32_t nt, int32_t nv, const int32_t *idx, const int32_t *off, con
 	int rc = plan_create_impl(nt, nv, idx, off, dists, count, radius, weights, unweighted, out);
 	if (rc != kHaSuccess) return rc;
 	g_cached_plan = *out;
+	g_cached_dev = dev;
 	g_cached_key = h;
 	g_cached_mode = mode;
 	g_cached_radius = radius;
@@ -2856,6 +2870,14 @@ extern "C" int ha_b200_local_procrustes_noalloc(const double *d_X, const double 
 	jp.stop_cos = 0.0;
 	int64_t tofs = 0;  // packed output offset of the current searchlight
 	int32_t s = 0;
+	// an error after work was queued: wait for that work before returning, so no later call finds
+	// the shared array still in use
+	auto fail_after_enqueue = [&](int code, const char *what) {
+		fprintf(stderr, "ha_b200_local_procrustes_noalloc: %s failed: %s\n", what, cudaGetErrorString(cudaGetLastError()));
+		cudaStreamSynchronize(st);
+		cudaGetLastError();
+		return code;
+	};
 	while (s < count) {
 		// one batch: as many searchlights as fit the work-item and A areas
 		int nb = 0;
@@ -2882,11 +2904,12 @@ extern "C" int ha_b200_local_procrustes_noalloc(const double *d_X, const double 
 			tofs += (int64_t)n * n;
 			nb++;
 		}
-		HA_CUDA(cudaMemcpyAsync(d_work, g_noalloc_items, (size_t)nb * sizeof(SlWork), cudaMemcpyHostToDevice, st));
-		HA_CUDA(cudaMemsetAsync(d_stats, 0, (size_t)nb * sizeof(SlStats), st));
+		if (cudaMemcpyAsync(d_work, g_noalloc_items, (size_t)nb * sizeof(SlWork), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+		    cudaMemsetAsync(d_stats, 0, (size_t)nb * sizeof(SlStats), st) != cudaSuccess)
+			return fail_after_enqueue(kHaErrorInternal, "staging a batch");
 		// one launch per rows-per-lane group (items of a batch are in searchlight order)
 		k_xcov_f64in<32><<<nb, kBlock, 0, st>>>(d_work, d_sl_indices, d_X, d_Y, nt, nv, d_A, d_status);
-		HA_CUDA(cudaGetLastError());
+		if (cudaGetLastError() != cudaSuccess) return fail_after_enqueue(kHaErrorInternal, "the cross-covariance launch");
 		int q = 0;
 		while (q < nb) {
 			const int rpl = rpl_for(g_noalloc_items[q].n);
@@ -2902,12 +2925,12 @@ extern "C" int ha_b200_local_procrustes_noalloc(const double *d_X, const double 
 			}
 			if ((rc = launch_jacobi<float>(rpl, e - q, jacobi_threads(maxb, false), smem, st, d_work + q, d_A, d_A,
 			                               d_T_out, d_stats, d_uv, jp)) != kHaSuccess)
-				return rc;
-			HA_CUDA(cudaGetLastError());
+				return fail_after_enqueue(rc, "the Jacobi launch");
+			if (cudaGetLastError() != cudaSuccess) return fail_after_enqueue(kHaErrorInternal, "the Jacobi launch");
 			q = e;
 		}
 		// the next batch reuses the scratch: finish this one before its items are overwritten
-		HA_CUDA(cudaStreamSynchronize(st));
+		if (cudaStreamSynchronize(st) != cudaSuccess) return fail_after_enqueue(kHaErrorInternal, "a batch");
 		s += nb;
 	}
 	HA_CUDA(cudaMemcpyAsync(&g_noalloc_status_host, d_status, sizeof(int32_t), cudaMemcpyDeviceToHost, st));

@@ -5,9 +5,10 @@ program forbids new allocations, or cudaMalloc's device-wide synchronisation is 
 in their loop) pass their own device buffers and the library uses only a static scratch array.
 Its output must match the allocating plan API's plain FP32 local transforms on the same inputs,
 within the per-transform tolerance of the parity tests, on two calls in a row (the shared scratch
-keeps the previous call's contents).  The inputs have more samples than any searchlight has
-vertices, so every transform is unique and two correct solvers agree.  The file sorts after the
-parity tests so that a run stopping at the first failure has run them first.
+keeps the previous call's contents), and the float64 oracle directly.  The inputs have more
+samples than any searchlight has vertices, so every transform is unique and two correct solvers
+agree.  The file sorts after the parity tests so that a run stopping at the first failure has
+run them first.
 """
 
 import ctypes
@@ -18,6 +19,7 @@ import pytest
 from hyperalignment_b200 import _lib as L
 from hyperalignment_b200 import workloads as W
 from hyperalignment_b200.plan import Plan
+from oracle import ha_oracle as O
 
 pytestmark = pytest.mark.gpu
 
@@ -37,30 +39,75 @@ def _plan_transforms(w, X, Y):
     return Ts
 
 
-def test_noalloc_matches_plan_on_two_calls(gpu):
+def _noalloc(lib, w, X, Y, indices=None):
+    """One call; returns (return code, the packed transforms as a list of n x n arrays)."""
     import torch
-    w = W.small_case(seed=31, nv=642, nt=400, lo=1, hi=160)
     s = w.sls
-    d_idx = torch.from_numpy(s.indices).cuda()
+    idx = s.indices if indices is None else indices
+    d_idx = torch.from_numpy(np.ascontiguousarray(idx, dtype=np.int32)).cuda()
     total = int((s.sizes.astype(np.int64) ** 2).sum())
+    dX = torch.from_numpy(np.asfortranarray(X).ravel(order="F")).cuda()
+    dY = torch.from_numpy(np.asfortranarray(Y).ravel(order="F")).cuda()
+    out = torch.full((total,), float("nan"), dtype=torch.float32, device="cuda")
+    rc = lib.ha_b200_local_procrustes_noalloc(ctypes.c_void_p(dX.data_ptr()), ctypes.c_void_p(dY.data_ptr()),
+                                              w.nt, w.nv, ctypes.c_void_p(d_idx.data_ptr()), L.iptr(s.offsets),
+                                              s.count, ctypes.c_void_p(out.data_ptr()), None)
+    got = out.cpu().numpy().astype(np.float64)
+    Ts, o = [], 0
+    for q in range(s.count):
+        n = int(s.sizes[q])
+        Ts.append(got[o:o + n * n].reshape(n, n))
+        o += n * n
+    return rc, Ts
+
+
+def _worst(Ts, refs):
+    return max(float(np.linalg.norm(T - R) / np.linalg.norm(R)) for T, R in zip(Ts, refs))
+
+
+def test_noalloc_matches_plan_on_two_calls(gpu):
+    w = W.small_case(seed=31, nv=642, nt=400, lo=1, hi=160)
     for X, Y in ((w.X, w.Y), (w.Y, w.X)):
-        ref = _plan_transforms(w, X, Y)
-        dX = torch.from_numpy(np.asfortranarray(X).ravel(order="F")).cuda()
-        dY = torch.from_numpy(np.asfortranarray(Y).ravel(order="F")).cuda()
-        out = torch.full((total,), float("nan"), dtype=torch.float32, device="cuda")
-        rc = gpu.ha_b200_local_procrustes_noalloc(ctypes.c_void_p(dX.data_ptr()), ctypes.c_void_p(dY.data_ptr()),
-                                                  w.nt, w.nv, ctypes.c_void_p(d_idx.data_ptr()), L.iptr(s.offsets),
-                                                  s.count, ctypes.c_void_p(out.data_ptr()), None)
+        rc, Ts = _noalloc(gpu, w, X, Y)
         assert rc == 0
-        got = out.cpu().numpy().astype(np.float64)
-        o = 0
-        worst = 0.0
-        for q in range(s.count):
-            n = int(s.sizes[q])
-            T = got[o:o + n * n].reshape(n, n)
-            o += n * n
-            worst = max(worst, float(np.linalg.norm(T - ref[q]) / np.linalg.norm(ref[q])))
-        assert worst <= TOL, worst
+        assert _worst(Ts, _plan_transforms(w, X, Y)) <= TOL
+
+
+def test_noalloc_matches_oracle(gpu):
+    """Against the float64 restatement of the reference's local Procrustes directly."""
+    w = W.small_case(seed=33, nv=642, nt=300, lo=5, hi=160)
+    rc, Ts = _noalloc(gpu, w, w.X, w.Y)
+    assert rc == 0
+    s = w.sls
+    pick = np.arange(0, s.count, 7)
+    refs = [O.procrustes(w.X[:, s.indices[s.offsets[q]:s.offsets[q + 1]]],
+                         w.Y[:, s.indices[s.offsets[q]:s.offsets[q + 1]]]) for q in pick]
+    assert _worst([Ts[q] for q in pick], refs) <= TOL
+
+
+@pytest.mark.parametrize("nv,lo,hi", [(2562, 1, 12),      # 2562 items: more than one 2048-item batch
+                                      (1442, 150, 160)])  # large matrices: the scratch area splits batches
+def test_noalloc_several_batches(gpu, nv, lo, hi):
+    """Work split over several batches (output offsets carried between them), twice in a row."""
+    w = W.small_case(seed=35, nv=nv, nt=max(2 * hi, 40), lo=lo, hi=hi)
+    ref = _plan_transforms(w, w.X, w.Y)
+    for _ in range(2):
+        rc, Ts = _noalloc(gpu, w, w.X, w.Y)
+        assert rc == 0
+        assert _worst(Ts, ref) <= TOL
+
+
+def test_noalloc_rejects_out_of_range_index(gpu):
+    """A vertex index equal to nv is caught by the kernel's own check (read as a zero column, never
+    dereferenced) and reported as an argument error; the next call succeeds."""
+    w = W.small_case(seed=37, nv=162, nt=40, lo=8, hi=24)
+    bad = w.sls.indices.copy()
+    bad[len(bad) // 2] = w.nv
+    rc, _ = _noalloc(gpu, w, w.X, w.Y, indices=bad)
+    assert rc == L.ERROR_ARG
+    rc, Ts = _noalloc(gpu, w, w.X, w.Y)
+    assert rc == 0
+    assert _worst(Ts, _plan_transforms(w, w.X, w.Y)) <= TOL
 
 
 def test_noalloc_rejects_oversized_searchlights(gpu):
