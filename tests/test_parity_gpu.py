@@ -131,7 +131,7 @@ def _device_run(w, solver, refl=True, scal=False, out_kind=L.OUT_CSR):
 
 
 @pytest.mark.parametrize("solver", [L.SOLVER_MIXED, L.SOLVER_FP32, L.SOLVER_FP64])
-@pytest.mark.parametrize("lo,hi", [(1, 12), (60, 90), (150, 240), (300, 420)])
+@pytest.mark.parametrize("lo,hi", [(1, 12), (60, 90), (150, 240), (300, 420), (481, 512)])
 def test_local_transforms_vs_fp64(gpu, solver, lo, hi):
     """Per-searchlight T_s against the float64 oracle, covering resident and blocked Jacobi sizes."""
     nv = 642 if hi <= 240 else 1442
@@ -300,6 +300,17 @@ def test_template_vs_oracle(gpu, zscore, level2, scal):
     tpl = H.searchlight_template(subj, sls_lists(s.indices, s.offsets), sls_lists(s.dists, s.offsets), s.radius,
                                  True, scal, zscore, level2)
     ref = O.searchlight_template(subj, s.indices, s.offsets, s.dists, s.radius, True, scal, zscore, level2)
+    assert relf(tpl, ref) <= TEMPLATE_REL
+
+
+def test_template_ten_subjects_vs_oracle(gpu):
+    """Config 2's loop shape: 10 subjects, 9 sequential solves and 10 leave-one-out solves (19
+    chained), z-scored common space, scaling, one level-2 pass, against the float64 oracle."""
+    _, sls, subj = W.hemisphere_subjects(seed=5, nv=642, nt=120, n_subj=10, size_lo=20, size_hi=50)
+    s = sls
+    tpl = H.searchlight_template(subj, sls_lists(s.indices, s.offsets), sls_lists(s.dists, s.offsets), s.radius,
+                                 True, True, True, 1)
+    ref = O.searchlight_template(subj, s.indices, s.offsets, s.dists, s.radius, True, True, True, 1)
     assert relf(tpl, ref) <= TEMPLATE_REL
 
 

@@ -149,3 +149,21 @@ def test_tc_rank_deficient_searchlights(gpu):
     completed = (plan.searchlight_stats(0, w.sls.count)["flags"] & 16) != 0
     assert not (completed & ~singular).any()
     assert completed.sum() >= singular.sum() // 2
+
+
+def test_tc_accuracy_at_full_size(gpu):
+    """Template workload (10242 searchlights of 100-300): the 150 searchlights that needed the most
+    iterations (the worst conditioned: condition numbers up to ~4e5) and 50 others, each within the
+    metric's 1e-4 of float64, with no float64 re-solve."""
+    w = W.template_procrustes_pair(seed=0)
+    plan, _ = _device_run(w, L.SOLVER_TC, scal=True)
+    iters = plan.searchlight_stats(0, w.sls.count)["sweeps"]
+    rng = np.random.default_rng(7)
+    pick = np.unique(np.concatenate([np.argsort(-iters, kind="stable")[:150], rng.choice(w.sls.count, 50, replace=False)]))
+    worst = 0.0
+    for q in pick:
+        T = plan.local_transforms(int(q), 1)[0]
+        sl = w.sls.indices[w.sls.offsets[q]:w.sls.offsets[q + 1]]
+        worst = max(worst, relf(T, O.procrustes(w.X[:, sl], w.Y[:, sl])))
+    assert worst <= 1e-4, worst
+    assert plan.stats()["n_fp64"] == 0
