@@ -395,6 +395,7 @@ def run_b200(args):
     total_ms, wall, launches, kt, clocks = timed_loop(L.SOLVER_TC, dX3, K, sample_clocks=True, trace=True)
     value = aggregate_rate(ws, count, K, total_ms / 1e3)
     tc_stats = plan.stats()
+    tc_layout = plan.tc_layout()
     plain_ms, _, _, _, _ = timed_loop(L.SOLVER_FP32, dX3, K)
     plain_value = aggregate_rate(ws, count, K, plain_ms / 1e3)
     plain_stats = plan.stats()
@@ -544,6 +545,7 @@ def run_b200(args):
             "error_vs_fp64": errs,
             "solver_stats": {"tensor_core": tc_stats, "plain_fp32": plain_stats, "mixed": mixed_stats,
                              "completed_null_spaces": int(((tc_flags & 16) != 0).sum()),
+                             "tc_layout": tc_layout,
                              "iterations_mean": float(tc_iters.mean()), "iterations_max": int(tc_iters.max())},
             "roofline": roof,
             "kernels": kernel_share,

@@ -322,6 +322,12 @@ struct HaB200Plan {
 	DevArr<int32_t> tcPlain;    // plain[maxit]
 	DevArr<int32_t> tcQueue;    // work queue positions of the persistent solve (two size classes)
 	bool tc_ready = false;
+	// tile layout of the per-phase launches per size class (tiles of <= 128 columns, of 129-256):
+	// dynamic shared memory per CTA, which sets the CTAs per SM and the pipeline depth; chosen by
+	// timing the candidates on the plan's first tensor-core run (autotune_tc), or pinned
+	int tc_smem[2] = {110 * 1024, 110 * 1024};
+	bool tc_tuned = false;
+	double tc_tune_ms[2][3] = {{0}};  // measured Gram-launch times of the candidates
 	// ridge grid search: scratch and the uploaded grid / CV description, allocated on first use
 	DevArr<double> gridscr, galpha, gwinv;
 	DevArr<int64_t> gbase;
@@ -858,11 +864,12 @@ int build_tc(HaB200Plan *P) {
 		for (int q : order) {
 			const int np = ch.tcw[q].np;
 			const int c = np > 256 ? 1 : 0;
-			// per-phase launches: tiles of at most 256 columns (two halves when np > 256), one class
+			// per-phase launches: tiles of at most 256 columns (two halves when np > 256), in two
+			// classes by column count (<= 128: 128 tensor-memory columns a CTA; 129-256)
 			const int h0 = np > 256 ? ((np / 2 + 15) & ~15) : np;
 			for (int t = 0; t * 128 < np; t++) {
-				ch.tct[0].push_back({q, t, 0, h0});
-				if (h0 < np) ch.tct[0].push_back({q, t, h0, np - h0});
+				ch.tct[h0 <= 128 ? 0 : 1].push_back({q, t, 0, h0});
+				if (h0 < np) ch.tct[np - h0 <= 128 ? 0 : 1].push_back({q, t, h0, np - h0});
 			}
 			ch.tco[c].push_back(q);
 		}
@@ -905,18 +912,70 @@ int build_tc(HaB200Plan *P) {
 	return kHaSuccess;
 }
 
-// Launch one phase of the tile product over both size classes of a chunk.
+// Launch one phase of the tile product over the size classes of a chunk (only class `only` when
+// it is 0 or 1), each with its layout's shared memory.
 template <int PHASE>
-int launch_tc(const Chunk &ch, TcArgs a, cudaStream_t st, int kind) {
+int launch_tc(const Chunk &ch, TcArgs a, cudaStream_t st, int kind, const int *smem, int only = -1) {
 	for (int c = 0; c < 2; c++) {
 		const int ntiles = (int)ch.tct[c].size();
-		if (!ntiles) continue;
+		if (!ntiles || (only >= 0 && c != only)) continue;
 		a.tiles = ch.d_tct[c];
-		a.smem_bytes = c ? kTcSmemLarge : kTcSmemSmall;
+		a.smem_bytes = smem[c];
 		HA_LAUNCH(kind, st);
 		k_tc_gemm<PHASE><<<ntiles, kTcThreads, a.smem_bytes, st>>>(a);
 	}
 	HA_CUDA(cudaGetLastError());
+	return kHaSuccess;
+}
+
+// Layout candidates per size class (dynamic shared memory per CTA): tiles of <= 128 columns hold
+// 128 tensor-memory columns, so two, three or four CTAs fit an SM (4, 3 or 2 pipeline stages);
+// tiles of 129-256 columns run two CTAs per SM (110 KB, 3-4 stages) or one (200 KB, 5-7 stages).
+const int kTcCand[2][3] = {{110 * 1024, 72 * 1024, 53 * 1024}, {110 * 1024, 200 * 1024, 0}};
+
+bool autotune_enabled() {
+	static int v = -1;
+	if (v < 0) {
+		const char *e = getenv("HA_B200_AUTOTUNE");
+		v = (e && e[0] == '0') ? 0 : 1;
+	}
+	return v == 1;
+}
+
+// Time one Gram launch of every candidate layout per size class on the chunk's current iterate
+// (the launches only write P and the residual partials, which the iteration then recomputes) and
+// keep the fastest.  Synchronises the stream once.
+int autotune_tc(HaB200Plan *P, const Chunk &ch, TcArgs a, cudaStream_t st) {
+	cudaEvent_t e0, e1;
+	HA_CUDA(cudaEventCreate(&e0));
+	HA_CUDA(cudaEventCreate(&e1));
+	for (int c = 0; c < 2; c++) {
+		if (ch.tct[c].empty()) continue;
+		double best = 1e300;
+		for (int i = 0; i < 3 && kTcCand[c][i]; i++) {
+			int smem[2] = {P->tc_smem[0], P->tc_smem[1]};
+			smem[c] = kTcCand[c][i];
+			double tmin = 1e300;
+			for (int rep = 0; rep < 2; rep++) {
+				HA_CUDA(cudaEventRecord(e0, st));
+				int rc = launch_tc<kTcPhaseGram>(ch, a, st, kHaB200KTcNs, smem, c);
+				HA_CUDA(cudaEventRecord(e1, st));
+				if (rc != kHaSuccess) return rc;
+				HA_CUDA(cudaEventSynchronize(e1));
+				float ms = 0.f;
+				HA_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+				tmin = std::min(tmin, (double)ms);
+			}
+			P->tc_tune_ms[c][i] = tmin;
+			if (tmin < best) {
+				best = tmin;
+				P->tc_smem[c] = kTcCand[c][i];
+			}
+		}
+	}
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	P->tc_tuned = true;
 	return kHaSuccess;
 }
 
@@ -989,8 +1048,14 @@ int run_procrustes_tc(HaB200Plan *P, const double *d_X, const double *d_Y, bool 
 			}
 			HA_CUDA(cudaGetLastError());
 		} else {
-		if ((rc = launch_tc<kTcPhaseXcov>(ch, a, st, kHaB200KTcXcov)) != kHaSuccess) return rc;
+		if ((rc = launch_tc<kTcPhaseXcov>(ch, a, st, kHaB200KTcXcov, P->tc_smem)) != kHaSuccess) return rc;
 		{ HA_LAUNCH(kHaB200KTcNs, st); k_tc_ns_init<<<nsl, 256, 0, st>>>(ch.d_tcw, P->tcA.p, P->tcXp.p, P->tcSt.p, P->tcRes.p); }
+		if (!P->tc_tuned && autotune_enabled()) {
+			a.st_in = P->tcSt.p;
+			a.c1 = sched[0].c1;
+			a.c3 = sched[0].c3;
+			if ((rc = autotune_tc(P, ch, a, st)) != kHaSuccess) return rc;
+		}
 		for (int k = 0; k < maxit; k++) {
 			a.st_in = P->tcSt.p + (size_t)(k & 1) * P->max_slots;
 			a.st_out = P->tcSt.p + (size_t)((k + 1) & 1) * P->max_slots;
@@ -1000,8 +1065,8 @@ int run_procrustes_tc(HaB200Plan *P, const double *d_X, const double *d_Y, bool 
 			a.c3 = sched[k].c3;
 			a.plain = sched[k].plain;
 			a.last = (k == maxit - 1) ? 1 : 0;
-			if ((rc = launch_tc<kTcPhaseGram>(ch, a, st, kHaB200KTcNs)) != kHaSuccess) return rc;
-			if ((rc = launch_tc<kTcPhaseUpdate>(ch, a, st, kHaB200KTcNs)) != kHaSuccess) return rc;
+			if ((rc = launch_tc<kTcPhaseGram>(ch, a, st, kHaB200KTcNs, P->tc_smem)) != kHaSuccess) return rc;
+			if ((rc = launch_tc<kTcPhaseUpdate>(ch, a, st, kHaB200KTcNs, P->tc_smem)) != kHaSuccess) return rc;
 		}
 		{ HA_LAUNCH(kHaB200KTcNs, st); k_tc_ns_finish<<<nsl, 256, 0, st>>>(ch.d_tcw, P->tcA.p, T, P->tcSt.p + (size_t)(maxit & 1) * P->max_slots,
 		                                                              P->stats.p, rowmajor); }
@@ -2530,6 +2595,34 @@ int ha_b200_kernel_times(double *ms, int64_t *launches) {
 }
 
 int64_t ha_b200_launch_count(void) { return g_launches; }
+
+int ha_b200_plan_tc_layout(const HaB200Plan *P, int32_t *smem_kb, int32_t *tuned, double *cand_ms) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	if (!P) return kHaErrorArg;
+	for (int c = 0; c < 2; c++) {
+		if (smem_kb) smem_kb[c] = P->tc_smem[c] / 1024;
+		if (cand_ms)
+			for (int i = 0; i < 3; i++) cand_ms[3 * c + i] = P->tc_tune_ms[c][i];
+	}
+	if (tuned) *tuned = P->tc_tuned ? 1 : 0;
+	return kHaSuccess;
+}
+
+int ha_b200_plan_set_tc_layout(HaB200Plan *P, const int32_t *smem_kb) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	if (!P || !smem_kb) return kHaErrorArg;
+	for (int c = 0; c < 2; c++) {
+		bool ok = false;
+		for (int i = 0; i < 3; i++) ok = ok || (kTcCand[c][i] && smem_kb[c] * 1024 == kTcCand[c][i]);
+		if (!ok) {
+			fprintf(stderr, "ha_b200_plan_set_tc_layout: %d KB is not a layout of size class %d\n", smem_kb[c], c);
+			return kHaErrorArg;
+		}
+	}
+	for (int c = 0; c < 2; c++) P->tc_smem[c] = smem_kb[c] * 1024;
+	P->tc_tuned = true;
+	return kHaSuccess;
+}
 
 int ha_b200_tc_selftest(int32_t which, int32_t n, int32_t nt, const float *h_a, const float *h_b, float *h_out) {
 	std::lock_guard<std::recursive_mutex> lk(g_mu);

@@ -133,6 +133,22 @@ class Plan:
             o += k * k
         return out
 
+    def tc_layout(self):
+        """Tensor-core tile layout per size class: shared memory per CTA (KB), whether it was tuned or
+        pinned, and the candidates' measured Gram-launch times (ms; 0 = not timed)."""
+        kb = np.zeros(2, dtype=np.int32)
+        tuned = ctypes.c_int32()
+        ms = np.zeros(6)
+        L.check(self.lib.ha_b200_plan_tc_layout(self.handle, L.iptr(kb), ctypes.byref(tuned), L.dptr(ms)),
+                "ha_b200_plan_tc_layout")
+        return {"smem_kb": [int(x) for x in kb], "tuned": bool(tuned.value),
+                "candidates_ms": {"le128_cols": {"110": ms[0], "72": ms[1], "53": ms[2]},
+                                  "129_256_cols": {"110": ms[3], "200": ms[4]}}}
+
+    def set_tc_layout(self, smem_kb):
+        kb = np.ascontiguousarray(smem_kb, dtype=np.int32)
+        L.check(self.lib.ha_b200_plan_set_tc_layout(self.handle, L.iptr(kb)), "ha_b200_plan_set_tc_layout")
+
     def close(self):
         if self.handle:
             self.lib.ha_b200_plan_destroy(self.handle)

@@ -451,6 +451,18 @@ int ha_b200_kernel_times(double *ms, int64_t *launches);
 int64_t ha_b200_launch_count(void);
 
 /*
+ * Tile layout of the tensor-core solver's per-phase launches, per size class (tiles of at most 128
+ * columns; of 129-256): shared memory per CTA in KB, which sets the CTAs per SM and the pipeline
+ * depth.  Class 0 candidates: 110, 72, 53 KB (2, 3, 4 CTAs per SM); class 1: 110, 200 KB (2, 1).
+ * The plan's first tensor-core run times one Gram launch per candidate with CUDA events and keeps
+ * the fastest (environment HA_B200_AUTOTUNE=0 keeps 110 / 110 instead); every layout gives the same
+ * results bit for bit.  cand_ms (6 doubles, may be NULL) receives the measured times (0 = not
+ * timed); tuned is 1 once a layout was chosen or pinned.  set_tc_layout pins one.
+ */
+int ha_b200_plan_tc_layout(const HaB200Plan *plan, int32_t *smem_kb, int32_t *tuned, double *cand_ms);
+int ha_b200_plan_set_tc_layout(HaB200Plan *plan, const int32_t *smem_kb);
+
+/*
  * Diagnostic: one tensor-core product of the Newton-Schulz solver's kernels on host data, FP32
  * row-major n x n output (n <= 512).  which 0: h_a^T h_a (h_a row-major n x n); which 1:
  * h_a h_b (both row-major n x n); which 2: the cross-covariance h_a h_b^T of two n x nt

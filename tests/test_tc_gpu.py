@@ -167,3 +167,32 @@ def test_tc_accuracy_at_full_size(gpu):
         worst = max(worst, relf(T, O.procrustes(w.X[:, sl], w.Y[:, sl])))
     assert worst <= 1e-4, worst
     assert plan.stats()["n_fp64"] == 0
+
+
+def test_tc_layouts_give_identical_results(gpu):
+    """The autotuner's layouts (shared memory per CTA, so CTAs per SM and pipeline depth) change
+    the schedule, not the arithmetic: the tuned run and every pinned layout agree bit for bit."""
+    import torch
+    w = W.small_case(seed=13, nv=642, nt=300, lo=60, hi=200)
+    plan = Plan.from_workload(w)
+    dX = torch.from_numpy(np.asfortranarray(w.X).ravel(order="F")).cuda()
+    dY = torch.from_numpy(np.asfortranarray(w.Y).ravel(order="F")).cuda()
+    outs = []
+    for layout in (None, (110, 110), (53, 200), (72, 110)):
+        if layout is not None:
+            plan.set_tc_layout(layout)
+        vals = torch.zeros(plan.nnz, dtype=torch.float64, device="cuda")
+        plan.procrustes_device(dX.data_ptr(), dY.data_ptr(), vals.data_ptr(), True, True, L.SOLVER_TC, L.OUT_CSR)
+        torch.cuda.synchronize()
+        outs.append(vals.cpu().numpy())
+        lay = plan.tc_layout()
+        assert lay["tuned"]
+        if layout is None:  # the first run tuned both classes (this case has tiles of both)
+            assert all(v > 0 for v in lay["candidates_ms"]["le128_cols"].values())
+            assert lay["candidates_ms"]["129_256_cols"]["110"] > 0
+        else:
+            assert tuple(lay["smem_kb"]) == layout
+    for o in outs[1:]:
+        assert o.tobytes() == outs[0].tobytes()
+    with pytest.raises(RuntimeError):
+        plan.set_tc_layout((64, 110))
