@@ -278,6 +278,11 @@ struct Chunk {
 	TcTile *d_tct[2] = {nullptr, nullptr};
 	std::vector<int32_t> tco[2];  // persistent solve: work indices per size class, largest first
 	int32_t *d_tco[2] = {nullptr, nullptr};
+	// the tensor-core iteration loop of this chunk captured as a CUDA graph, and what it was
+	// captured for (output order, layouts); replayed while those are unchanged
+	cudaGraphExec_t tc_graph = nullptr;
+	int tc_graph_key[3] = {-1, -1, -1};
+	int tc_graph_kernels = 0;
 	int64_t tc_x_elems = 0, tc_a_elems = 0;
 };
 
@@ -933,6 +938,27 @@ int launch_tc(const Chunk &ch, TcArgs a, cudaStream_t st, int kind, const int *s
 // tiles of 129-256 columns run two CTAs per SM (110 KB, 3-4 stages) or one (200 KB, 5-7 stages).
 const int kTcCand[2][3] = {{110 * 1024, 72 * 1024, 53 * 1024}, {110 * 1024, 200 * 1024, 0}};
 
+// CUDA-graph replay of captured launch sequences (ha_b200_set_graphs; on by default,
+// HA_B200_GRAPHS=0 turns it off).
+int g_graphs = -1;
+bool graphs_enabled() {
+	if (g_graphs < 0) {
+		const char *e = getenv("HA_B200_GRAPHS");
+		g_graphs = (e && e[0] == '0') ? 0 : 1;
+	}
+	return g_graphs == 1;
+}
+
+// A private non-blocking stream for captures (the legacy default stream cannot be captured).
+cudaStream_t capture_stream() {
+	static cudaStream_t s = nullptr;
+	if (!s && cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+		cudaGetLastError();
+		s = nullptr;
+	}
+	return s;
+}
+
 bool autotune_enabled() {
 	static int v = -1;
 	if (v < 0) {
@@ -1056,17 +1082,60 @@ int run_procrustes_tc(HaB200Plan *P, const double *d_X, const double *d_Y, bool 
 			a.c3 = sched[0].c3;
 			if ((rc = autotune_tc(P, ch, a, st)) != kHaSuccess) return rc;
 		}
-		for (int k = 0; k < maxit; k++) {
-			a.st_in = P->tcSt.p + (size_t)(k & 1) * P->max_slots;
-			a.st_out = P->tcSt.p + (size_t)((k + 1) & 1) * P->max_slots;
-			a.Xp = (k & 1) ? P->tcXq.p : P->tcXp.p;
-			a.Xw = (k & 1) ? P->tcXp.p : P->tcXq.p;
-			a.c1 = sched[k].c1;
-			a.c3 = sched[k].c3;
-			a.plain = sched[k].plain;
-			a.last = (k == maxit - 1) ? 1 : 0;
-			if ((rc = launch_tc<kTcPhaseGram>(ch, a, st, kHaB200KTcNs, P->tc_smem)) != kHaSuccess) return rc;
-			if ((rc = launch_tc<kTcPhaseUpdate>(ch, a, st, kHaB200KTcNs, P->tc_smem)) != kHaSuccess) return rc;
+		// the iteration: 2 x maxit launches per size class, the same every call on this plan, so
+		// captured once into a CUDA graph (on a private stream) and replayed on the caller's stream
+		auto enqueue_loop = [&](cudaStream_t ls) -> int {
+			for (int k = 0; k < maxit; k++) {
+				a.st_in = P->tcSt.p + (size_t)(k & 1) * P->max_slots;
+				a.st_out = P->tcSt.p + (size_t)((k + 1) & 1) * P->max_slots;
+				a.Xp = (k & 1) ? P->tcXq.p : P->tcXp.p;
+				a.Xw = (k & 1) ? P->tcXp.p : P->tcXq.p;
+				a.c1 = sched[k].c1;
+				a.c3 = sched[k].c3;
+				a.plain = sched[k].plain;
+				a.last = (k == maxit - 1) ? 1 : 0;
+				int r = launch_tc<kTcPhaseGram>(ch, a, ls, kHaB200KTcNs, P->tc_smem);
+				if (r != kHaSuccess) return r;
+				if ((r = launch_tc<kTcPhaseUpdate>(ch, a, ls, kHaB200KTcNs, P->tc_smem)) != kHaSuccess) return r;
+			}
+			return kHaSuccess;
+		};
+		if (!graphs_enabled() || g_timing) {
+			if ((rc = enqueue_loop(st)) != kHaSuccess) return rc;
+		} else {
+			const int key[3] = {rowmajor, P->tc_smem[0], P->tc_smem[1]};
+			if (!ch.tc_graph || memcmp(key, ch.tc_graph_key, sizeof(key)) != 0) {
+				if (ch.tc_graph) cudaGraphExecDestroy(ch.tc_graph);
+				ch.tc_graph = nullptr;
+				cudaStream_t cs = capture_stream();
+				if (!cs) return kHaErrorInternal;
+				const int64_t l0 = g_launches, n0 = g_kernel_n[kHaB200KTcNs];
+				HA_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+				rc = enqueue_loop(cs);
+				cudaGraph_t gr = nullptr;
+				const cudaError_t ce = cudaStreamEndCapture(cs, &gr);
+				g_launches = l0;  // counted when the graph runs
+				g_kernel_n[kHaB200KTcNs] = n0;
+				if (rc != kHaSuccess || ce != cudaSuccess) {
+					if (gr) cudaGraphDestroy(gr);
+					fprintf(stderr, "ha_b200: capture of the tensor-core iteration failed: %s\n", cudaGetErrorString(ce));
+					return rc != kHaSuccess ? rc : kHaErrorInternal;
+				}
+				const cudaError_t ie = cudaGraphInstantiate(&ch.tc_graph, gr, 0);
+				size_t nodes = 0;
+				cudaGraphGetNodes(gr, nullptr, &nodes);
+				cudaGraphDestroy(gr);
+				if (ie != cudaSuccess) {
+					ch.tc_graph = nullptr;
+					fprintf(stderr, "ha_b200: instantiating the tensor-core iteration graph failed: %s\n", cudaGetErrorString(ie));
+					return kHaErrorInternal;
+				}
+				ch.tc_graph_kernels = (int)nodes;
+				memcpy(ch.tc_graph_key, key, sizeof(key));
+			}
+			HA_CUDA(cudaGraphLaunch(ch.tc_graph, st));
+			g_launches += ch.tc_graph_kernels;
+			g_kernel_n[kHaB200KTcNs] += ch.tc_graph_kernels;
 		}
 		{ HA_LAUNCH(kHaB200KTcNs, st); k_tc_ns_finish<<<nsl, 256, 0, st>>>(ch.d_tcw, P->tcA.p, T, P->tcSt.p + (size_t)(maxit & 1) * P->max_slots,
 		                                                              P->stats.p, rowmajor); }
@@ -2271,6 +2340,7 @@ void ha_b200_plan_destroy(HaB200Plan *P) {
 		if (ch.d_weig) cudaFree(ch.d_weig);
 		if (ch.d_tofs) cudaFree(ch.d_tofs);
 		if (ch.d_tcw) cudaFree(ch.d_tcw);
+		if (ch.tc_graph) cudaGraphExecDestroy(ch.tc_graph);
 		for (int c = 0; c < 2; c++) {
 			if (ch.d_tct[c]) cudaFree(ch.d_tct[c]);
 			if (ch.d_tco[c]) cudaFree(ch.d_tco[c]);
@@ -2595,6 +2665,11 @@ int ha_b200_kernel_times(double *ms, int64_t *launches) {
 }
 
 int64_t ha_b200_launch_count(void) { return g_launches; }
+
+void ha_b200_set_graphs(bool on) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	g_graphs = on ? 1 : 0;
+}
 
 int ha_b200_plan_tc_layout(const HaB200Plan *P, int32_t *smem_kb, int32_t *tuned, double *cand_ms) {
 	std::lock_guard<std::recursive_mutex> lk(g_mu);

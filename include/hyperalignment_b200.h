@@ -460,6 +460,13 @@ int64_t ha_b200_launch_count(void);
  * timed); tuned is 1 once a layout was chosen or pinned.  set_tc_layout pins one.
  */
 int ha_b200_plan_tc_layout(const HaB200Plan *plan, int32_t *smem_kb, int32_t *tuned, double *cand_ms);
+
+/*
+ * Repeated launch sequences (the tensor-core iteration of a plan chunk, the ridge grid search of a
+ * plan) are captured once into CUDA graphs and replayed; off, they are launched one by one.  On by
+ * default (environment HA_B200_GRAPHS=0 turns it off); the results are the same bit for bit.
+ */
+void ha_b200_set_graphs(bool on);
 int ha_b200_plan_set_tc_layout(HaB200Plan *plan, const int32_t *smem_kb);
 
 /*

@@ -196,3 +196,31 @@ def test_tc_layouts_give_identical_results(gpu):
         assert o.tobytes() == outs[0].tobytes()
     with pytest.raises(RuntimeError):
         plan.set_tc_layout((64, 110))
+
+
+def test_tc_graph_replay_matches_direct_launches(gpu, hlib):
+    """The iteration loop captured as a CUDA graph (the default) and replayed gives the same bits as
+    launching it kernel by kernel, on the first (capturing) call and on replays."""
+    import torch
+    w = W.small_case(seed=17, nv=642, nt=200, lo=40, hi=150)
+    plan = Plan.from_workload(w)
+    dX = torch.from_numpy(np.asfortranarray(w.X).ravel(order="F")).cuda()
+    dY = torch.from_numpy(np.asfortranarray(w.Y).ravel(order="F")).cuda()
+
+    def run():
+        vals = torch.zeros(plan.nnz, dtype=torch.float64, device="cuda")
+        plan.procrustes_device(dX.data_ptr(), dY.data_ptr(), vals.data_ptr(), True, True, L.SOLVER_TC, L.OUT_CSC)
+        torch.cuda.synchronize()
+        return vals.cpu().numpy().tobytes()
+
+    try:
+        hlib.ha_b200_set_graphs(False)
+        direct = run()
+        hlib.ha_b200_set_graphs(True)
+        n0 = hlib.ha_b200_launch_count()
+        captured = run()
+        replayed = run()
+        assert hlib.ha_b200_launch_count() > n0
+    finally:
+        hlib.ha_b200_set_graphs(True)
+    assert captured == direct and replayed == direct
