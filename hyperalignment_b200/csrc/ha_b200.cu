@@ -332,6 +332,10 @@ struct HaB200Plan {
 	// timing the candidates on the plan's first tensor-core run (autotune_tc), or pinned
 	int tc_smem[2] = {110 * 1024, 110 * 1024};
 	bool tc_tuned = false;
+	// the ridge grid search captured as a CUDA graph, and the key it was captured for
+	cudaGraphExec_t grid_graph = nullptr;
+	std::vector<uint64_t> grid_key;
+	int64_t grid_graph_launches = 0;
 	double tc_tune_ms[2][3] = {{0}};  // measured Gram-launch times of the candidates
 	// ridge grid search: scratch and the uploaded grid / CV description, allocated on first use
 	DevArr<double> gridscr, galpha, gwinv;
@@ -1568,31 +1572,50 @@ int reduce_chunk64(HaB200Plan *P, Chunk &ch, int out_kind, double *d_vals, cudaS
 // factor and its float64 Jacobi eigen decomposition, and the per-model products; then the grid
 // evaluation, the winners (d_best) and their betas in the float64 T scratch.  The chunk's work list
 // may be a subset of the plan chunk's (the learned form's fallback searchlights).
-int grid_chunk(HaB200Plan *P, Chunk &ch, const double *d_X, const double *d_Y, const GridSpec &gs,
-               const GridParams &gp, int rowmajor, int32_t *d_best, double *d_cost, cudaStream_t st) {
-	const int nt = P->nt;
+// Sub-batches of a chunk's grid search: searchlights [i0, i1) of the eigenvector-mode work list,
+// as many as fit the grid scratch budget, and each one's per-slot scratch base offsets.
+struct GridBatch {
+	int i0, i1;
+	int64_t total;  // float64 elements of grid scratch
+};
+
+void grid_plan_chunk(const Chunk &ch, const GridParams &gp, std::vector<GridBatch> &bt, std::vector<int64_t> &gbase_all) {
 	const int nsl = ch.s1 - ch.s0;
 	const int grid = gp.n_alphas * gp.n_npcs;
 	const size_t budget = grid_budget_bytes();
-	const JacobiParams jp = eig_params(false);
-	std::vector<int64_t> gbase;
-	int rc;
 	const int nitems = (int)ch.weig.size();
+	bt.clear();
 	int i0 = 0;
 	while (i0 < nitems) {
-		gbase.assign((size_t)nsl, 0);
+		const size_t g0 = gbase_all.size();
+		gbase_all.resize(g0 + (size_t)nsl, 0);
 		int64_t total = 0;
 		int i1 = i0;
 		while (i1 < nitems) {
 			const SlWork &wi = ch.weig[i1];
-			const GridLayout L = GridLayout::make(wi.n, gp.models, gp.mte, gp.ntu, gp.n_alphas, grid);
-			if (i1 > i0 && (size_t)(total + L.total) * 8 > budget) break;
-			gbase[wi.slot] = total;
-			total += L.total;
+			const GridLayout Lg = GridLayout::make(wi.n, gp.models, gp.mte, gp.ntu, gp.n_alphas, grid);
+			if (i1 > i0 && (size_t)(total + Lg.total) * 8 > budget) break;
+			gbase_all[g0 + wi.slot] = total;
+			total += Lg.total;
 			i1++;
 		}
-		if ((rc = P->gridscr.ensure((size_t)total)) != kHaSuccess) return rc;
-		HA_CUDA(cudaMemcpyAsync(P->gbase.p, gbase.data(), (size_t)nsl * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+		bt.push_back({i0, i1, total});
+		i0 = i1;
+	}
+}
+
+// The launches of one chunk's grid search (no host copies or allocations: capturable); the
+// sub-batches' base offsets are at d_gbase (nsl per sub-batch).
+int grid_chunk_launch(HaB200Plan *P, Chunk &ch, const double *d_X, const double *d_Y, const GridSpec &gs,
+                      GridParams gp, const std::vector<GridBatch> &bt, const int64_t *d_gbase, int rowmajor,
+                      int32_t *d_best, double *d_cost, cudaStream_t st) {
+	const int nt = P->nt;
+	const int nsl = ch.s1 - ch.s0;
+	const JacobiParams jp = eig_params(false);
+	int rc;
+	for (size_t bi_ = 0; bi_ < bt.size(); bi_++) {
+		const int i0 = bt[bi_].i0, i1 = bt[bi_].i1;
+		gp.gbase = d_gbase + bi_ * (size_t)nsl;
 		double *A = P->scrA.p, *V = P->scrV.p;
 		for (int mo = 0; mo < gp.models; mo++) {
 			const GridModel &md = gs.mdl[mo];
@@ -1620,12 +1643,26 @@ int grid_chunk(HaB200Plan *P, Chunk &ch, const double *d_X, const double *d_Y, c
 		{ HA_LAUNCH(kHaB200KGrid, st); k_grid_eval<<<dim3(i1 - i0, gp.n_alphas), kBlock, 0, st>>>(ch.d_weig + i0, P->gridscr.p, gp); }
 		{ HA_LAUNCH(kHaB200KGrid, st); k_grid_final<<<i1 - i0, kBlock, 0, st>>>(ch.d_weig + i0, P->idx.p, d_Y, P->gridscr.p, gp, P->scrT64.p, rowmajor, d_best, d_cost); }
 		HA_CUDA(cudaGetLastError());
-		i0 = i1;
 	}
 	return kHaSuccess;
 }
 
-// Enqueue the searchlight ridge grid search + reduction of the winners' betas over all chunks.
+// One chunk's grid search enqueued directly (sub-batch plan, scratch and offsets, launches).
+int grid_chunk(HaB200Plan *P, Chunk &ch, const double *d_X, const double *d_Y, const GridSpec &gs,
+               const GridParams &gp, int rowmajor, int32_t *d_best, double *d_cost, cudaStream_t st) {
+	std::vector<GridBatch> bt;
+	std::vector<int64_t> gbase;
+	grid_plan_chunk(ch, gp, bt, gbase);
+	int64_t mx = 1;
+	for (const auto &b : bt) mx = std::max(mx, b.total);
+	int rc;
+	if ((rc = P->gridscr.ensure((size_t)mx)) != kHaSuccess) return rc;
+	if ((rc = P->gbase.ensure(std::max<size_t>(gbase.size(), 1))) != kHaSuccess) return rc;
+	HA_CUDA(cudaMemcpyAsync(P->gbase.p, gbase.data(), gbase.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+	HA_CUDA(cudaStreamSynchronize(st));  // the host vector goes out of scope
+	return grid_chunk_launch(P, ch, d_X, d_Y, gs, gp, bt, P->gbase.p, rowmajor, d_best, d_cost, st);
+}
+
 int run_ridge_grid(HaB200Plan *P, const double *d_X, const double *d_Y, const GridSpec &gs, int out_kind,
                    double *d_vals, int32_t *d_best, double *d_cost, cudaStream_t st) {
 	const int rowmajor = out_kind == kHaB200OutCSR ? 1 : 0;
@@ -1633,12 +1670,78 @@ int run_ridge_grid(HaB200Plan *P, const double *d_X, const double *d_Y, const Gr
 	if ((rc = grid_prepare(P)) != kHaSuccess) return rc;
 	GridParams gp;
 	if ((rc = grid_upload(P, gs, st, gp)) != kHaSuccess) return rc;
-	HA_CUDA(cudaMemsetAsync(P->counters.p, 0, 5 * sizeof(int32_t), st));
+	// sub-batches of every chunk, their scratch offsets uploaded once, the scratch sized once: what
+	// follows is launches only, captured into a CUDA graph (fold x alpha x PC grid of every
+	// searchlight) and replayed while the inputs, outputs, grid shape and buffers are the same
+	std::vector<std::vector<GridBatch>> bts(P->chunks.size());
+	std::vector<size_t> gofs(P->chunks.size());
+	std::vector<int64_t> gbase;
+	int64_t mx = 1;
 	for (size_t c = 0; c < P->chunks.size(); c++) {
-		Chunk &ch = P->chunks[c];
-		HA_CUDA(cudaMemsetAsync(P->stats.p, 0, (size_t)(ch.s1 - ch.s0) * sizeof(SlStats), st));
-		if ((rc = grid_chunk(P, ch, d_X, d_Y, gs, gp, rowmajor, d_best, d_cost, st)) != kHaSuccess) return rc;
-		if ((rc = reduce_chunk64(P, ch, out_kind, d_vals, st)) != kHaSuccess) return rc;
+		gofs[c] = gbase.size();
+		grid_plan_chunk(P->chunks[c], gp, bts[c], gbase);
+		for (const auto &b : bts[c]) mx = std::max(mx, b.total);
+	}
+	if ((rc = P->gridscr.ensure((size_t)mx)) != kHaSuccess) return rc;
+	if ((rc = P->gbase.ensure(std::max<size_t>(gbase.size(), 1))) != kHaSuccess) return rc;
+	HA_CUDA(cudaMemcpyAsync(P->gbase.p, gbase.data(), gbase.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+	HA_CUDA(cudaStreamSynchronize(st));
+	auto enqueue = [&](cudaStream_t ls) -> int {
+		HA_CUDA(cudaMemsetAsync(P->counters.p, 0, 5 * sizeof(int32_t), ls));
+		for (size_t c = 0; c < P->chunks.size(); c++) {
+			Chunk &ch = P->chunks[c];
+			HA_CUDA(cudaMemsetAsync(P->stats.p, 0, (size_t)(ch.s1 - ch.s0) * sizeof(SlStats), ls));
+			int r = grid_chunk_launch(P, ch, d_X, d_Y, gs, gp, bts[c], P->gbase.p + gofs[c], rowmajor, d_best, d_cost, ls);
+			if (r != kHaSuccess) return r;
+			if ((r = reduce_chunk64(P, ch, out_kind, d_vals, ls)) != kHaSuccess) return r;
+		}
+		return kHaSuccess;
+	};
+	if (!graphs_enabled() || g_timing) {
+		if ((rc = enqueue(st)) != kHaSuccess) return rc;
+	} else {
+		const uint64_t key[] = {(uint64_t)(uintptr_t)d_X, (uint64_t)(uintptr_t)d_Y, (uint64_t)(uintptr_t)d_vals,
+		                        (uint64_t)(uintptr_t)d_best, (uint64_t)(uintptr_t)d_cost, (uint64_t)out_kind,
+		                        (uint64_t)gp.models, (uint64_t)gp.mte, (uint64_t)gp.ntu, (uint64_t)gp.n_alphas,
+		                        (uint64_t)gp.n_npcs, (uint64_t)gp.n_untested, (uint64_t)(uintptr_t)gp.alphas,
+		                        (uint64_t)(uintptr_t)gp.npcs, (uint64_t)(uintptr_t)gp.mdl, (uint64_t)(uintptr_t)gp.rows,
+		                        (uint64_t)(uintptr_t)gp.tpos, (uint64_t)(uintptr_t)gp.winv, (uint64_t)(uintptr_t)gp.urows,
+		                        (uint64_t)(uintptr_t)gp.untested, (uint64_t)(uintptr_t)P->gridscr.p,
+		                        (uint64_t)(uintptr_t)P->gbase.p, fnv1a(gbase.data(), gbase.size() * 8, 1469598103934665603ULL)};
+		std::vector<uint64_t> kv(key, key + sizeof(key) / sizeof(key[0]));
+		for (const auto &m : gs.mdl) kv.push_back(((uint64_t)m.tr_ofs << 32) ^ (uint64_t)m.tr_n);
+		if (!P->grid_graph || kv != P->grid_key) {
+			if (P->grid_graph) cudaGraphExecDestroy(P->grid_graph);
+			P->grid_graph = nullptr;
+			if ((rc = g_fan.init()) != kHaSuccess) return rc;  // no stream creation inside the capture
+			cudaStream_t cs = capture_stream();
+			if (!cs) return kHaErrorInternal;
+			int64_t n0[kHaB200NumKernelKinds];
+			memcpy(n0, g_kernel_n, sizeof(n0));
+			const int64_t l0 = g_launches;
+			HA_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+			rc = enqueue(cs);
+			cudaGraph_t gr = nullptr;
+			const cudaError_t ce = cudaStreamEndCapture(cs, &gr);
+			P->grid_graph_launches = g_launches - l0;
+			g_launches = l0;
+			memcpy(g_kernel_n, n0, sizeof(n0));
+			if (rc != kHaSuccess || ce != cudaSuccess) {
+				if (gr) cudaGraphDestroy(gr);
+				fprintf(stderr, "ha_b200: capture of the grid search failed: %s\n", cudaGetErrorString(ce));
+				return rc != kHaSuccess ? rc : kHaErrorInternal;
+			}
+			const cudaError_t ie = cudaGraphInstantiate(&P->grid_graph, gr, 0);
+			cudaGraphDestroy(gr);
+			if (ie != cudaSuccess) {
+				P->grid_graph = nullptr;
+				fprintf(stderr, "ha_b200: instantiating the grid-search graph failed: %s\n", cudaGetErrorString(ie));
+				return kHaErrorInternal;
+			}
+			P->grid_key = kv;
+		}
+		HA_CUDA(cudaGraphLaunch(P->grid_graph, st));
+		g_launches += P->grid_graph_launches;
 	}
 	P->last_chunk = (int)P->chunks.size() - 1;
 	P->last_rowmajor = rowmajor;
@@ -2355,6 +2458,7 @@ void ha_b200_plan_destroy(HaB200Plan *P) {
 	P->gfit.release(); P->gfeat.release(); P->gwork.release();
 	P->tcXb.release(); P->tcYb.release(); P->tcXp.release(); P->tcXq.release(); P->tcPp.release(); P->tcA.release(); P->tcRes.release();
 	P->tcSt.release(); P->tcSched.release(); P->tcPlain.release(); P->tcQueue.release();
+	if (P->grid_graph) cudaGraphExecDestroy(P->grid_graph);
 	delete P;
 }
 

@@ -412,6 +412,40 @@ def test_ridge_grid_few_rows_odd_pcs_untested_rows(gpu):
     _check_grid(w, Y, np.array([1e-2, 1.0, 30.0]), [8, 4, 12, 0, 100], tr, te)
 
 
+def test_ridge_grid_graph_matches_direct_launches(gpu, hlib):
+    """The grid search (every searchlight's fold x alpha x PC grid, all chunks, the reduction)
+    captured as one CUDA graph and replayed gives the same bits as launching it kernel by kernel."""
+    import torch
+    w, Y = _grid_case(8, 642, 120, 10, 60)
+    tr, te = H.ensemble_indices(120, 1, 5, 6, 3, 4)
+    alphas, npcs = np.logspace(-3, 3, 4), [5, 10, 40]
+    plan = Plan(w.nt, w.nv, w.sls.indices, w.sls.offsets, w.sls.dists, w.sls.radius)
+    dX = torch.from_numpy(np.asfortranarray(w.X).ravel(order="F")).cuda()
+    dY = torch.from_numpy(np.asfortranarray(Y).ravel(order="F")).cuda()
+    vals = torch.zeros(plan.nnz, dtype=torch.float64, device="cuda")
+    best = torch.zeros(w.sls.count, dtype=torch.int32, device="cuda")
+    cost = torch.zeros(w.sls.count * len(alphas) * len(npcs), dtype=torch.float64, device="cuda")
+
+    def run():
+        vals.zero_()
+        best.fill_(-1)
+        cost.zero_()
+        plan.ridge_grid_device(dX.data_ptr(), dY.data_ptr(), vals.data_ptr(), best.data_ptr(), alphas, npcs, tr, te,
+                               d_cost=cost.data_ptr())
+        torch.cuda.synchronize()
+        return vals.cpu().numpy().tobytes(), best.cpu().numpy().tobytes(), cost.cpu().numpy().tobytes()
+
+    try:
+        hlib.ha_b200_set_graphs(False)
+        direct = run()
+        hlib.ha_b200_set_graphs(True)
+        captured = run()
+        replayed = run()
+    finally:
+        hlib.ha_b200_set_graphs(True)
+    assert captured == direct and replayed == direct
+
+
 def test_ridge_grid_device_deterministic(gpu):
     import torch
     w, Y = _grid_case(8, 642, 120, 10, 40)
