@@ -54,6 +54,9 @@ SIGNATURES = {
     "ha_searchlight_template_b200": (ctypes.c_int, [
         c_double_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, c_int32_p, c_int32_p, c_double_p, ctypes.c_int32,
         ctypes.c_double, ctypes.c_bool, ctypes.c_bool, ctypes.c_bool, ctypes.c_int32, c_double_p]),
+    "ha_searchlight_pca_template_b200": (ctypes.c_int, [
+        c_double_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, c_int32_p, c_int32_p, c_double_p, ctypes.c_int32,
+        ctypes.c_double, c_double_p]),
     "ha_b200_plan_create": (ctypes.c_int, [
         ctypes.c_int32, ctypes.c_int32, c_int32_p, c_int32_p, c_double_p, ctypes.c_int32, ctypes.c_double,
         c_double_p, ctypes.POINTER(ctypes.c_void_p)]),
@@ -110,7 +113,8 @@ SIGNATURES = {
 }
 
 KERNEL_KINDS = ["convert", "colvar", "xcov32", "jacobi32", "formT32", "xcov64", "jacobi64", "formT64", "refine",
-                "reflect", "scale", "reduce", "pattern", "ridge", "grid", "mlp", "eval", "tc_xcov", "tc_ns"]
+                "reflect", "scale", "reduce", "pattern", "ridge", "grid", "mlp", "eval", "tc_xcov", "tc_ns",
+                "pca"]
 
 # Error codes and enum values (include/hyperalignment_b200.h, same as the reference's ha_common.h).
 SUCCESS, ERROR_ALLOC, ERROR_SVD, ERROR_ARG, ERROR_INTERNAL = 0, -1, -2, -3, -4

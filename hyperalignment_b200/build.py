@@ -18,7 +18,7 @@ ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libha_b200.so")
 SOURCES = [os.path.join(HERE, "csrc", "ha_b200.cu")]
 DEPS = SOURCES + [os.path.join(HERE, "csrc", "ha_b200_kernels.cuh"), os.path.join(HERE, "csrc", "ha_b200_grid.cuh"), os.path.join(HERE, "csrc", "ha_b200_mlp.cuh"),
-                  os.path.join(HERE, "csrc", "ha_b200_tc.cuh"),
+                  os.path.join(HERE, "csrc", "ha_b200_tc.cuh"), os.path.join(HERE, "csrc", "ha_b200_pca.cuh"),
                   os.path.join(ROOT, "include", "hyperalignment_b200.h")]
 
 NVCC_FLAGS = [

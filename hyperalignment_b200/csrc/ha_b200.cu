@@ -11,6 +11,7 @@
 #include "ha_b200_grid.cuh"
 #include "ha_b200_mlp.cuh"
 #include "ha_b200_tc.cuh"
+#include "ha_b200_pca.cuh"
 
 #include <cuda_runtime.h>
 #include <omp.h>
@@ -423,6 +424,40 @@ size_t scratch_budget_bytes() {
 	return (size_t)(gb * 1073741824.0);
 }
 
+// Sort work items by Jacobi class (resident or blocked, rows per lane), largest first inside a
+// class, and cut them into buckets of one Jacobi kernel instance each.  prec: 0 float32 polar,
+// 1 float64 polar, 2 float64 eigenvector mode.
+std::vector<Bucket> bucketize(std::vector<SlWork> &items, int prec) {
+	auto key = [](const SlWork &w) { return (w.nblk == 2 ? 0 : 32) + rpl_for(w.n); };
+	std::stable_sort(items.begin(), items.end(), [&](const SlWork &a, const SlWork &b) {
+		int ka = key(a), kb = key(b);
+		if (ka != kb) return ka < kb;
+		return a.n > b.n;
+	});
+	std::vector<Bucket> buckets;
+	for (int i = 0; i < (int)items.size();) {
+		int j = i;
+		size_t smem = 0;
+		while (j < (int)items.size() && key(items[j]) == key(items[i])) {
+			int bb, kk;
+			size_t mm;
+			jacobi_layout(items[j].n, prec >= 1, bb, kk, mm, prec >= 1 ? kSmemMax : fp32_jacobi_budget(), prec != 2);
+			smem = std::max(smem, mm);
+			j++;
+		}
+		Bucket b;
+		b.first = i;
+		b.count = j - i;
+		b.smem = smem;
+		b.blocked = items[i].nblk != 2;
+		b.threads = jacobi_threads(items[i].bsz, prec >= 1);
+		b.rpl = rpl_for(items[i].n);
+		buckets.push_back(b);
+		i = j;
+	}
+	return buckets;
+}
+
 int build_chunks(HaB200Plan *P) {
 	const size_t budget = scratch_budget_bytes();
 	P->chunks.clear();
@@ -487,33 +522,7 @@ int build_chunks(HaB200Plan *P) {
 				uvo += 2 * (int64_t)n;
 				items.push_back(w);
 			}
-			auto key = [](const SlWork &w) { return (w.nblk == 2 ? 0 : 32) + rpl_for(w.n); };
-			std::stable_sort(items.begin(), items.end(), [&](const SlWork &a, const SlWork &b) {
-				int ka = key(a), kb = key(b);
-				if (ka != kb) return ka < kb;
-				return a.n > b.n;
-			});
-			std::vector<Bucket> buckets;
-			for (int i = 0; i < (int)items.size();) {
-				int j = i;
-				size_t smem = 0;
-				while (j < (int)items.size() && key(items[j]) == key(items[i])) {
-					int bb, kk;
-					size_t mm;
-					jacobi_layout(items[j].n, prec >= 1, bb, kk, mm, prec >= 1 ? kSmemMax : fp32_jacobi_budget(), prec != 2);
-					smem = std::max(smem, mm);
-					j++;
-				}
-				Bucket b;
-				b.first = i;
-				b.count = j - i;
-				b.smem = smem;
-				b.blocked = items[i].nblk != 2;
-				b.threads = jacobi_threads(items[i].bsz, prec >= 1);
-				b.rpl = rpl_for(items[i].n);
-				buckets.push_back(b);
-				i = j;
-			}
+			std::vector<Bucket> buckets = bucketize(items, prec);
 			if (prec == 0) { ch.w32 = items; ch.b32 = buckets; }
 			else if (prec == 1) { ch.w64 = items; ch.b64 = buckets; }
 			else { ch.weig = items; ch.beig = buckets; }
@@ -2267,6 +2276,195 @@ int template_impl(const double *dms, int ns, int nt, int nv, const int32_t *idx,
 	return done(kHaSuccess);
 }
 
+// Searchlight PCA template (src/hyperalignment/searchlight.py:215-236, tpl_kind="pca"), float64
+// throughout.  Consecutive searchlights form batches sized to the scratch budget; per batch: the
+// Gram of the smaller side (k_pca_gram), its pivoted Cholesky factor and eigenvector-mode Jacobi,
+// the template and B = tmpl^T M (k_pca_tmpl), the float64 Jacobi polar of B, C = tmpl R
+// (k_pca_contrib) and the weighted per-vertex reduction into the template (k_pca_reduce).
+int pca_template_impl(const double *dms, int ns, int nt, int nv, const int32_t *idx, const int32_t *off,
+                      const double *dists, int count, double radius, double *tpl_out) {
+	if (!dms || !tpl_out || ns < 1 || nt <= 0 || nv <= 0 || count <= 0) return kHaErrorArg;
+	int rc = check_cuda_ready();
+	if (rc != kHaSuccess) return rc;
+	HaB200Plan *P = nullptr;
+	if ((rc = get_plan(nt, nv, idx, off, dists, count, radius, nullptr, false, &P)) != kHaSuccess) return rc;
+	// per searchlight: Gram order, scratch region of the eigen / polar solves, template scratch
+	std::vector<int> mg(count), nn(count);
+	std::vector<int64_t> region(count), ptot(count);
+	std::vector<size_t> bytes(count);
+	for (int s = 0; s < count; s++) {
+		const int n = P->h_off[s + 1] - P->h_off[s];
+		const int64_t vn = (int64_t)ns * n;
+		const int m = vn < nt ? (int)vn : nt;
+		if (n > nt || m > kPcaMaxM) {
+			fprintf(stderr,
+			        "ha_searchlight_pca_template_b200: searchlight %d has %d vertices; the GPU template needs n <= nt (%d) "
+			        "and min(nt, n_subj * n) <= %d\n", s, n, nt, kPcaMaxM);
+			return kHaErrorArg;
+		}
+		nn[s] = n;
+		mg[s] = n > 0 ? m : nt;
+		if (n == 0) { region[s] = ptot[s] = 0; bytes[s] = 0; continue; }
+		int be, ke, bp, kp;
+		size_t me, mp;
+		jacobi_layout(m, true, be, ke, me, kSmemMax, false);
+		jacobi_layout(n, true, bp, kp, mp);
+		int64_t r = std::max<int64_t>((int64_t)m * std::max(m, be * ke), (int64_t)n * kp * bp);
+		region[s] = (r + 31) & ~(int64_t)31;
+		ptot[s] = PcaLayout::make(nt, n, m, m != nt).total;
+		bytes[s] = (size_t)(2 * region[s] + ptot[s] + m + 2 * n) * 8 + (size_t)n * n * 4 + 2 * sizeof(SlStats);
+	}
+	// batches of consecutive searchlights
+	const size_t budget = scratch_budget_bytes();
+	std::vector<int> bstart{0};
+	{
+		size_t acc = 0;
+		for (int s = 0; s < count; s++) {
+			if (s > bstart.back() && acc + bytes[s] > budget) {
+				bstart.push_back(s);
+				acc = 0;
+			}
+			acc += bytes[s];
+		}
+		bstart.push_back(count);
+	}
+	int64_t maxR = 1, maxP = 1, maxT = 1, maxUV = 1;
+	int maxS = 1;
+	for (size_t b = 0; b + 1 < bstart.size(); b++) {
+		int64_t R = 0, Pt = 0, Tt = 0, U = 0;
+		for (int s = bstart[b]; s < bstart[b + 1]; s++) {
+			R += region[s];
+			Pt += ptot[s];
+			Tt += (int64_t)nn[s] * nn[s];
+			U += nn[s] > 0 ? mg[s] + 2 * nn[s] : 0;
+		}
+		maxR = std::max(maxR, R);
+		maxP = std::max(maxP, Pt);
+		maxT = std::max(maxT, Tt);
+		maxUV = std::max(maxUV, U);
+		maxS = std::max(maxS, bstart[b + 1] - bstart[b]);
+	}
+	const size_t m1 = (size_t)nt * nv;
+	DevArr<double> D, eA, eV, Pw, uvb, tpl;
+	DevArr<float> T;
+	DevArr<SlStats> stE, stP;
+	DevArr<SlWork> dwe, dwp, dwes, dwps;
+	DevArr<int64_t> dpofs;
+	DevArr<int32_t> dmg;
+	auto done = [&](int code) {
+		D.release(); eA.release(); eV.release(); Pw.release(); uvb.release(); tpl.release(); T.release();
+		stE.release(); stP.release(); dwe.release(); dwp.release(); dwes.release(); dwps.release();
+		dpofs.release(); dmg.release();
+		return code;
+	};
+	if ((rc = D.ensure(m1 * ns)) != kHaSuccess || (rc = tpl.ensure(m1)) != kHaSuccess ||
+	    (rc = eA.ensure((size_t)maxR)) != kHaSuccess || (rc = eV.ensure((size_t)maxR)) != kHaSuccess ||
+	    (rc = Pw.ensure((size_t)maxP)) != kHaSuccess || (rc = uvb.ensure((size_t)maxUV)) != kHaSuccess ||
+	    (rc = T.ensure((size_t)maxT)) != kHaSuccess || (rc = stE.ensure((size_t)maxS)) != kHaSuccess ||
+	    (rc = stP.ensure((size_t)maxS)) != kHaSuccess || (rc = dwe.ensure((size_t)maxS)) != kHaSuccess ||
+	    (rc = dwp.ensure((size_t)maxS)) != kHaSuccess || (rc = dwes.ensure((size_t)maxS)) != kHaSuccess ||
+	    (rc = dwps.ensure((size_t)maxS)) != kHaSuccess || (rc = dpofs.ensure((size_t)maxS)) != kHaSuccess ||
+	    (rc = dmg.ensure((size_t)maxS)) != kHaSuccess)
+		return done(rc);
+	cudaStream_t st = 0;
+	if (cudaMemcpyAsync(D.p, dms, m1 * ns * 8, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+	    cudaMemsetAsync(tpl.p, 0, m1 * 8, st) != cudaSuccess)
+		return done(kHaErrorInternal);
+	const JacobiParams jpe = eig_params(false);
+	JacobiParams jpp;
+	jpp.max_sweeps = 40;
+	jpp.t_rowmajor = 0;
+	jpp.ill_ratio = 0.0;
+	jpp.weak = weak_factor();
+	jpp.eig = 0;
+	jpp.only_flagged = 0;
+	jpp.keep_v = 0;
+	jpp.warm = 0;
+	jpp.stop_cos = fp64_stop_cos();
+	for (size_t b = 0; b + 1 < bstart.size(); b++) {
+		const int s_lo = bstart[b], s_hi = bstart[b + 1];
+		std::vector<SlWork> we, wp;
+		std::vector<int64_t> pofs(s_hi - s_lo, 0);
+		std::vector<int32_t> mgb(s_hi - s_lo);
+		int64_t ro = 0, po = 0, to = 0, uo = 0;
+		for (int s = s_lo; s < s_hi; s++) {
+			const int q = s - s_lo, n = nn[s], m = mg[s];
+			mgb[q] = m;
+			if (n == 0) continue;
+			SlWork e, p;
+			e.s = p.s = s;
+			e.slot = p.slot = q;
+			e.sofs = p.sofs = P->h_off[s];
+			e.aofs = p.aofs = ro;
+			e.tofs = p.tofs = to;
+			e.n = m;
+			p.n = n;
+			{
+				int bb, kk;
+				size_t mm;
+				jacobi_layout(m, true, bb, kk, mm, kSmemMax, false);
+				e.bsz = bb; e.nblk = kk;
+				jacobi_layout(n, true, bb, kk, mm);
+				p.bsz = bb; p.nblk = kk;
+			}
+			e.uvofs = uo;
+			p.uvofs = uo + m;
+			we.push_back(e);
+			wp.push_back(p);
+			pofs[q] = po;
+			ro += region[s];
+			po += ptot[s];
+			to += (int64_t)n * n;
+			uo += m + 2 * n;
+		}
+		const int nb = (int)we.size();
+		if (nb == 0) continue;
+		std::vector<SlWork> wes = we, wps = wp;
+		const std::vector<Bucket> be = bucketize(wes, 2), bp = bucketize(wps, 1);
+		if (cudaMemcpyAsync(dwe.p, we.data(), nb * sizeof(SlWork), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+		    cudaMemcpyAsync(dwp.p, wp.data(), nb * sizeof(SlWork), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+		    cudaMemcpyAsync(dwes.p, wes.data(), nb * sizeof(SlWork), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+		    cudaMemcpyAsync(dwps.p, wps.data(), nb * sizeof(SlWork), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+		    cudaMemcpyAsync(dpofs.p, pofs.data(), pofs.size() * 8, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+		    cudaMemcpyAsync(dmg.p, mgb.data(), mgb.size() * 4, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+		    cudaMemsetAsync(stE.p, 0, (size_t)(s_hi - s_lo) * sizeof(SlStats), st) != cudaSuccess ||
+		    cudaMemsetAsync(stP.p, 0, (size_t)(s_hi - s_lo) * sizeof(SlStats), st) != cudaSuccess)
+			return done(kHaErrorInternal);
+		{ HA_LAUNCH(kHaB200KPca, st); k_pca_gram<16><<<nb, kBlock, 0, st>>>(dwe.p, P->idx.p, P->off.p, D.p, ns, nt, nv, eV.p); }
+		for (const Bucket &k : be) {
+			const SlWork *wk = dwes.p + k.first;
+			{ HA_LAUNCH(kHaB200KPca, st); k_pchol<<<k.count, kBlock, pchol_smem(k.rpl), st>>>(wk, eV.p, eA.p, stE.p); }
+			HA_LAUNCH(kHaB200KPca, st);
+			if ((rc = launch_jacobi<double>(k.rpl, k.count, k.threads, k.smem, st, wk, eA.p, eV.p, T.p, stE.p, uvb.p, jpe)) != kHaSuccess)
+				return done(rc);
+		}
+		{ HA_LAUNCH(kHaB200KPca, st); k_pca_tmpl<<<nb, kBlock, 0, st>>>(dwe.p, dwp.p, P->idx.p, D.p, ns, nt, nv, eV.p, uvb.p, dpofs.p, Pw.p, eA.p); }
+		for (const Bucket &k : bp) {
+			const SlWork *wk = dwps.p + k.first;
+			{
+				HA_LAUNCH(kHaB200KPca, st);
+				if ((rc = launch_jacobi<double>(k.rpl, k.count, k.threads, k.smem, st, wk, eA.p, eV.p, T.p, stP.p, uvb.p, jpp)) != kHaSuccess)
+					return done(rc);
+			}
+			if (k.blocked) { HA_LAUNCH(kHaB200KPca, st); k_form_t_global<double><<<k.count, kBlock, 0, st>>>(wk, eA.p, eV.p, T.p, stP.p, 0, 0); }
+		}
+		{ HA_LAUNCH(kHaB200KPca, st); k_pca_contrib<<<nb, kBlock, 0, st>>>(dwe.p, dwp.p, T.p, nt, dpofs.p, Pw.p); }
+		{ HA_LAUNCH(kHaB200KPca, st); k_pca_reduce<<<nv, kBlock, 0, st>>>(P->vlptr.p, P->vlent.p, P->off.p, P->has_weights ? P->w.p : nullptr,
+		                                                              dpofs.p, dmg.p, Pw.p, nt, s_lo, s_hi, tpl.p); }
+		// the host work lists are rebuilt for the next batch
+		if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess) {
+			fprintf(stderr, "ha_searchlight_pca_template_b200: CUDA failure: %s\n", cudaGetErrorString(cudaGetLastError()));
+			return done(kHaErrorInternal);
+		}
+	}
+	if (cudaMemcpyAsync(tpl_out, tpl.p, m1 * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+	    cudaStreamSynchronize(st) != cudaSuccess) {
+		fprintf(stderr, "ha_searchlight_pca_template_b200: CUDA failure: %s\n", cudaGetErrorString(cudaGetLastError()));
+		return done(kHaErrorInternal);
+	}
+	return done(kHaSuccess);
+}
+
 // =============================================================================================
 // C ABI
 // =============================================================================================
@@ -2348,6 +2546,13 @@ int ha_searchlight_template_b200(const double *dms, int32_t n_subj, int32_t nt, 
 	std::lock_guard<std::recursive_mutex> lk(g_mu);
 	return template_impl(dms, n_subj, nt, nv, sl_indices, sl_offsets, sl_dists, count, radius, isReflection,
 	                     isScaling, isZscoreCommon, level2_iter, tpl_out);
+}
+
+int ha_searchlight_pca_template_b200(const double *dms, int32_t n_subj, int32_t nt, int32_t nv,
+                                     const int32_t *sl_indices, const int32_t *sl_offsets, const double *sl_dists,
+                                     int32_t count, double radius, double *tpl_out) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	return pca_template_impl(dms, n_subj, nt, nv, sl_indices, sl_offsets, sl_dists, count, radius, tpl_out);
 }
 
 int ha_sparse_pattern_b200(const int32_t *sl_indices, const int32_t *sl_offsets, int32_t count, int32_t nv,

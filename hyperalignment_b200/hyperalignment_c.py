@@ -224,3 +224,27 @@ def searchlight_template(dms, sls, dists, radius, reflection=True, scaling=False
         bool(reflection), bool(scaling), bool(zscore_common), int(level2_iter), L.dptr(out)),
         "ha_searchlight_template_b200")
     return np.ascontiguousarray(out.T)
+
+
+def searchlight_pca_template(dms, sls, dists, radius, n_jobs=1, tpl_kind="pca"):
+    """Searchlight PCA template of subjects ``dms`` (list of nt x nv arrays), on the GPU.
+
+    Same arguments and result as the Python package's ``searchlight_template(dms, sls, dists,
+    radius, n_jobs=1, tpl_kind="pca")`` (src/hyperalignment/searchlight.py:215-236); ``n_jobs``
+    is accepted and ignored (every searchlight runs on the GPU).  Needs len(sl) <= nt and
+    min(nt, len(dms) * len(sl)) <= 512 for every searchlight.
+    """
+    if tpl_kind != "pca":
+        raise ValueError(f"tpl_kind {tpl_kind!r}: only 'pca' runs here (the Procrustes loop is searchlight_template)")
+    ns = len(dms)
+    nt, nv = np.shape(dms[0])
+    stack = np.empty((ns, nv, nt), dtype=np.float64)  # each subject column-major
+    for s, D in enumerate(dms):
+        stack[s] = np.asarray(D, dtype=np.float64).T
+    idx, offsets, d = _flatten(sls, dists)
+    lib = _init()
+    out = np.empty((nv, nt), dtype=np.float64)
+    L.check(lib.ha_searchlight_pca_template_b200(
+        L.dptr(stack), ns, nt, nv, L.iptr(idx), L.iptr(offsets), L.dptr(d), len(sls), float(radius), L.dptr(out)),
+        "ha_searchlight_pca_template_b200")
+    return np.ascontiguousarray(out.T)

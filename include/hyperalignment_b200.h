@@ -229,6 +229,25 @@ int ha_searchlight_template_b200(
 	bool isReflection, bool isScaling, bool isZscoreCommon, int32_t level2_iter,
 	double *tpl_out);
 
+/*
+ * Searchlight PCA template: replaces searchlight_template(..., tpl_kind="pca") of the Python
+ * package (src/hyperalignment/searchlight.py:215-236 with compute_template(kind="pca",
+ * max_npc=n, common_topography=True, demean=False), src/hyperalignment/local_template.py:224-248,
+ * :72-78, :11-53).  Per searchlight (n vertices sl): X = [dms_1[:, sl] .. dms_ns[:, sl]];
+ * tmpl = U_n S_n / sqrt(n_subj) from the top n singular pairs of X; R = polar(tmpl^T sum_s
+ * dms_s[:, sl]) (reflection allowed, no scaling); tpl_out[:, sl] += (tmpl R) diag(w) with the
+ * searchlight weights of sl_dists and radius (ha_compute_weights).  The singular pairs are exact
+ * (float64 Gram of the smaller side, eigen decomposition by Jacobi rotations): they agree with the
+ * reference's randomized SVD where the top-n singular subspace is separated from the rest.
+ * dms: n_subj consecutive nt x nv float64 column-major matrices (host); tpl_out: nt x nv float64
+ * column-major (host, overwritten).  kHaErrorArg when a searchlight holds more than nt vertices
+ * or min(nt, n_subj * n) exceeds 512.
+ */
+int ha_searchlight_pca_template_b200(
+	const double *dms, int32_t n_subj, int32_t nt, int32_t nv,
+	const int32_t *sl_indices, const int32_t *sl_offsets, const double *sl_dists,
+	int32_t count, double radius, double *tpl_out);
+
 /* ---- device-resident plan (repeated calls on one searchlight geometry) ---- */
 
 typedef struct HaB200Plan HaB200Plan;
@@ -435,7 +454,8 @@ enum {
 	kHaB200KEval = 16,      /* vertex-wise correlation of aligned data with a target */
 	kHaB200KTcXcov = 17,    /* cross-covariance on the tensor cores (split BF16) */
 	kHaB200KTcNs = 18,      /* Newton-Schulz polar iteration on the tensor cores */
-	kHaB200NumKernelKinds = 19,
+	kHaB200KPca = 19,       /* searchlight PCA template: Gram, eigen, template, polar, reduction */
+	kHaB200NumKernelKinds = 20,
 };
 
 /*

@@ -314,6 +314,60 @@ def test_template_ten_subjects_vs_oracle(gpu):
     assert relf(tpl, ref) <= TEMPLATE_REL
 
 
+PCA_REL = 1e-6  # searchlight PCA template vs the golden fixture and the float64 oracle
+
+
+def pca_case(seed, nv, nt, ns, size_lo, size_hi, noise=0.01):
+    """Subjects sharing one nt x nv signal plus small independent noise: every searchlight's top
+    len(sl) singular subspace of X is separated from the rest by the noise ratio."""
+    rng = np.random.default_rng(seed)
+    sls = W.searchlights_knn(W.fibonacci_sphere(nv), rng.integers(size_lo, size_hi + 1, size=nv))
+    base = rng.standard_normal((nt, nv))
+    dms = [base + noise * rng.standard_normal((nt, nv)) for _ in range(ns)]
+    return sls, dms
+
+
+def pca_b200(dms, sls):
+    return H.searchlight_pca_template(dms, sls_lists(sls.indices, sls.offsets), sls_lists(sls.dists, sls.offsets),
+                                      sls.radius)
+
+
+def test_pca_template_vs_python_reference_golden(gpu):
+    """searchlight_template(tpl_kind="pca") of the Python reference (src/hyperalignment/searchlight.py:215-236)
+    on 162 searchlights of 8-24 vertices, 4 subjects, 60 time points: searchlights of at most 14
+    vertices take the vertex-side Gram (4 n < 60), the others the time-side one."""
+    g = golden("pca_template.npz")
+    off = g["off"]
+    tpl = H.searchlight_pca_template(list(g["dms"]), sls_lists(g["idx"], off), sls_lists(g["dists"], off),
+                                     float(g["radius"]))
+    assert relf(tpl, g["template"]) <= PCA_REL
+    assert np.abs(tpl - g["template"]).max() <= PCA_REL * np.abs(g["template"]).max()
+
+
+@pytest.mark.parametrize("seed,nv,nt,ns,lo,hi", [
+    (11, 162, 200, 3, 20, 60),     # vertex side, m = 60-180 (eigen solve blocked above 160)
+    (12, 162, 90, 5, 10, 30),      # both sides (m = 50-90)
+    (13, 162, 300, 2, 100, 150),   # vertex side m = 200-300 (blocked eigen), polar blocked from n = 100
+    (14, 162, 512, 4, 40, 128),    # vertex side m = 160-508 and the time side at the 512 limit
+])
+def test_pca_template_vs_oracle(gpu, seed, nv, nt, ns, lo, hi):
+    sls, dms = pca_case(seed, nv, nt, ns, lo, hi)
+    tpl = pca_b200(dms, sls)
+    ref = O.searchlight_pca_template(dms, sls.indices, sls.offsets, sls.dists, sls.radius)
+    assert relf(tpl, ref) <= PCA_REL
+
+
+def test_pca_template_deterministic_and_rejects_oversized(gpu):
+    sls, dms = pca_case(15, 162, 80, 3, 10, 40)
+    a = pca_b200(dms, sls)
+    b = pca_b200(dms, sls)
+    np.testing.assert_array_equal(a, b)
+    # a searchlight larger than nt: the reference's template is then nt x nt (k = nt); not supported here
+    sls2, dms2 = pca_case(16, 162, 30, 3, 20, 40)
+    with pytest.raises(RuntimeError):
+        pca_b200(dms2, sls2)
+
+
 def test_template_identical_subjects(gpu):
     # searchlight form of csrc/ha_test.c:503-537: identical subjects, no z-scoring -> the input back
     _, sls, subj = W.hemisphere_subjects(seed=4, nv=162, nt=60, n_subj=3, size_lo=8, size_hi=20)
