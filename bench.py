@@ -63,7 +63,8 @@ def parse_args():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
-    p.add_argument("--workload", choices=["template", "rankdef", "grid", "learned", "shard", "forrest", "refgpu"],
+    p.add_argument("--workload", choices=["template", "rankdef", "grid", "learned", "shard", "forrest", "refgpu",
+                                           "pca"],
                    default="rankdef",
                    help="rankdef (default; 'template' is the same run): the headline Procrustes step on the "
                         "template pair with 10%% singular searchlights, the plain pair as a sub-field; grid: the "
@@ -71,7 +72,8 @@ def parse_args():
                         "learned: the learned proposal; shard: one "
                         "hemisphere split over the N GPUs (strong scaling); forrest: the shapes of the "
                         "reference's published run (nt 1818, searchlights of 90-170); refgpu: the reference's "
-                        "own CUDA arm (oracle/_ref_cuda) against this library on config 1 and the Forrest shape")
+                        "own CUDA arm (oracle/_ref_cuda) against this library on config 1 and the Forrest shape; pca: the "
+                        "searchlight PCA template on the template workload's hemisphere (10 subjects)")
     p.add_argument("--grid-step", type=int, default=16)
     p.add_argument("--ref-seconds", type=float, default=0.0,
                    help="reference arm: seconds of CPU work per step (default: 150 s over all steps)")
@@ -1157,6 +1159,108 @@ def run_forrest(args):
     plan.close()
 
 
+def run_pca(args):
+    """Searchlight PCA template (the Python package's searchlight_template(tpl_kind="pca"),
+    src/hyperalignment/searchlight.py:215-236) on the hemisphere of the template workload: 10242
+    searchlights of 100-300 vertices, 10 subjects, nt 400, through the C entry from host buffers
+    (every step uploads the subjects and downloads the template).  The float64 CPU oracle (exact SVD
+    per searchlight) is timed on a sample of searchlights, and the GPU template of the same sample
+    is checked against it."""
+    import torch
+    from threadpoolctl import threadpool_info
+    from hyperalignment_b200 import _lib as L
+    from hyperalignment_b200 import hyperalignment_c as H
+    from hyperalignment_b200 import workloads as W
+    from oracle import ha_oracle as O
+    torch.cuda.set_device(0)
+    lib = L.lib()
+    L.check(lib.ha_b200_init(), "ha_b200_init")
+    _, sls, subj = W.hemisphere_subjects(seed=0, nv=args.nv, nt=args.nt, n_subj=10, size_lo=100, size_hi=300)
+    ns, nt, nv = len(subj), args.nt, args.nv
+    stack = np.empty((ns, nv, nt))
+    for j, D in enumerate(subj):
+        stack[j] = D.T
+    out = np.empty((nv, nt))
+    argv = (L.dptr(stack), ns, nt, nv, L.iptr(sls.indices), L.iptr(sls.offsets), L.dptr(sls.dists), sls.count,
+            float(sls.radius), L.dptr(out))
+
+    def step():
+        L.check(lib.ha_searchlight_pca_template_b200(*argv), "ha_searchlight_pca_template_b200")
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    sampler = ClockSampler(0)
+    sampler.start()
+    time.sleep(0.5)
+    n0 = lib.ha_b200_launch_count()
+    evs, walls = [], []
+    for _ in range(args.steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        a.record(stream)
+        step()
+        b.record(stream)
+        torch.cuda.synchronize()
+        walls.append(time.perf_counter() - t0)
+        evs.append((a, b))
+    launches = lib.ha_b200_launch_count() - n0
+    clocks = sampler.stop()
+    K = args.steps
+    ms = sum(a.elapsed_time(b) for a, b in evs)
+    # kernel time of one traced step (CUDA events around every launch)
+    lib.ha_b200_kernel_times(None, None)
+    lib.ha_b200_set_kernel_timing(True)
+    step()
+    lib.ha_b200_set_kernel_timing(False)
+    kms = np.zeros(len(L.KERNEL_KINDS))
+    kcnt = np.zeros(len(L.KERNEL_KINDS), dtype=np.int64)
+    lib.ha_b200_kernel_times(kms.ctypes.data_as(L.c_double_p), kcnt.ctypes.data_as(L.c_int64_p))
+    pca_k = L.KERNEL_KINDS.index("pca")
+    # CPU oracle on a growing sample of searchlights, and the GPU template of the same sample
+    rng = np.random.default_rng(3)
+    order = rng.permutation(sls.count)
+    take, cpu_s = 4, 0.0
+    while True:
+        sample = np.sort(order[:take])
+        sub = sls.subset(sample)
+        t0 = time.perf_counter()
+        ref = O.searchlight_pca_template(subj, sub.indices, sub.offsets, sub.dists, sub.radius)
+        cpu_s = time.perf_counter() - t0
+        if cpu_s >= args.cpu_seconds or take >= sls.count:
+            break
+        take = min(sls.count, max(take * 2, int(take * args.cpu_seconds / max(cpu_s, 1e-3) * 1.1)))
+    got = H.searchlight_pca_template(subj, [sub.indices[sub.offsets[q]:sub.offsets[q + 1]] for q in range(sub.count)],
+                                     [sub.dists[sub.offsets[q]:sub.offsets[q + 1]] for q in range(sub.count)],
+                                     sub.radius)
+    err = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+    blas = max((i.get("num_threads", 1) for i in threadpool_info()), default=1)
+    sizes = sls.sizes
+    value = sls.count * K / (ms / 1e3)
+    res = {
+        "metric": "searchlight PCA template: searchlights/s", "value": value, "unit": "searchlights/s", "n_gpus": 1,
+        "steps": K, "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "hemisphere_pca_template", "nv": nv, "nt": nt, "subjects": ns,
+                   "searchlights": sls.count, "sl_size_min": int(sizes.min()), "sl_size_max": int(sizes.max()),
+                   "sl_size_mean": round(float(sizes.mean()), 2), "gram_order": int(min(nt, ns * sizes.min())),
+                   "weights": "linear distance",
+                   "l2": "inputs (328 MB of subjects) larger than L2, uploaded every step"},
+        "timing": "CUDA events on the default stream around the C entry (host float64 in, host template out)",
+        "e2e": {"value": sls.count * K / sum(walls), "unit": "searchlights/s",
+                "h2d_bytes_per_step": int(stack.nbytes), "d2h_bytes_per_step": int(out.nbytes),
+                "path": "ha_searchlight_pca_template_b200, wall clock per call"},
+        "pca_kernels_ms_per_step": float(kms[pca_k]), "pca_launches_per_step": int(kcnt[pca_k]),
+        "error_vs_oracle": {"template_relfrob": err, "sample": int(sub.count)},
+        "cpu_baseline": {"value": sub.count / cpu_s, "unit": "searchlights/s", "cores": int(blas), "kind": "port",
+                         "sample": f"{sub.count} random searchlights, oracle exact-SVD template (numpy LAPACK, "
+                                   f"{blas} BLAS threads), {cpu_s:.1f} s"},
+        "gpu_launches": int(launches), "clocks": clocks,
+    }
+    print(json.dumps(res))
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -1171,6 +1275,8 @@ def main():
         run_forrest(args)
     elif args.workload == "refgpu":
         run_refgpu(args)
+    elif args.workload == "pca":
+        run_pca(args)
     else:
         run_b200(args)
 
