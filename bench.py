@@ -312,6 +312,260 @@ def sample_errors(w, singular, sample, Ts):
     return out
 
 
+class StepClock:
+    """Device timer of the sharded steps: CUDA events on the current stream (GPU ranks) or
+    perf_counter (CPU ranks of the gloo tests)."""
+
+    def __init__(self, device):
+        import torch
+        self.cuda = torch.device(device).type == "cuda"
+        self.device = device
+
+    def mark(self):
+        import torch
+        if self.cuda:
+            e = torch.cuda.Event(enable_timing=True)
+            e.record(torch.cuda.current_stream(self.device))
+            return e
+        return time.perf_counter()
+
+    def ms(self, a, b):
+        return a.elapsed_time(b) if self.cuda else (b - a) * 1e3
+
+    def sync(self):
+        import torch
+        if self.cuda:
+            torch.cuda.synchronize(self.device)
+
+
+def sharded_rank(ws, rank, offsets, nv, make_range, steps, warmup, device, flush=None, group=None):
+    """The rank code of one hemisphere over ws ranks (strong scaling; hyperalignment_b200/shard.py):
+    this rank's contiguous searchlight range (balanced by n^3), its pattern and the column exchange
+    are built once; every step zeroes the partial CSC values, solves the range into them and sends
+    them to the column owners in one all-to-all.  make_range(lo, hi) -> (indptr, rows, solve) with
+    solve(partial) writing the range's weighted local transforms into its CSC pattern.  Times are
+    the max over ranks of the per-rank sums over the timed steps."""
+    import torch
+    import torch.distributed as dist
+    from hyperalignment_b200 import shard as S
+    b = S.split_searchlights(offsets, ws)
+    lo, hi = int(b[rank]), int(b[rank + 1])
+    solve = None
+    if hi > lo:
+        indptr, rows, solve = make_range(lo, hi)
+    else:
+        indptr, rows = np.zeros(nv + 1, dtype=np.int64), np.zeros(0, dtype=np.int32)
+    ex = S.ColumnExchange(indptr, rows, nv, group=group, device=device)
+    partial = torch.zeros(int(np.asarray(indptr)[-1]), dtype=torch.float64, device=device)
+    clock = StepClock(device)
+
+    def solve_part():
+        partial.zero_()
+        if solve is not None:
+            solve(partial)
+
+    for _ in range(warmup):
+        solve_part()
+        owned = ex.combine(partial)
+    clock.sync()
+    if ws > 1:
+        dist.barrier(group=group)
+    marks = []
+    for _ in range(steps):
+        if flush is not None:
+            flush.zero_()
+        a = clock.mark()
+        solve_part()
+        m = clock.mark()
+        owned = ex.combine(partial)
+        e = clock.mark()
+        marks.append((a, m, e))
+    clock.sync()
+    job = max_over_ranks(sum(clock.ms(a, e) for a, _, e in marks), ws, device)
+    solve_ms = max_over_ranks(sum(clock.ms(a, m) for a, m, _ in marks), ws, device)
+    exch_ms = max_over_ranks(sum(clock.ms(m, e) for _, m, e in marks), ws, device)
+    return {"job_ms": job, "solve_ms": solve_ms, "exchange_ms": exch_ms, "owned": owned, "bounds": b,
+            "range": (lo, hi), "exchange": ex, "partial": partial, "solve_part": solve_part}
+
+
+def sharded_same_split(offsets, nv, ws, partial_of):
+    """The ws-way split run in one process (no collective): every range's partial from
+    partial_of(lo, hi) -> (indptr, rows, values torch), combined in rank order by the owners as
+    hyperalignment_b200.shard.exchange_in_process does.  The sharded run must equal it bit for bit."""
+    from hyperalignment_b200 import shard as S
+    import torch
+    b = S.split_searchlights(offsets, ws)
+    ptrs, rows, parts = [], [], []
+    for q in range(ws):
+        lo, hi = int(b[q]), int(b[q + 1])
+        if hi > lo:
+            p, r, v = partial_of(lo, hi)
+        else:
+            p, r, v = np.zeros(nv + 1, dtype=np.int64), np.zeros(0, dtype=np.int32), torch.zeros(0, dtype=torch.float64)
+        ptrs.append(np.asarray(p, dtype=np.int64))
+        rows.append(np.asarray(r, dtype=np.int32))
+        parts.append(v)
+    return S.exchange_in_process(ptrs, rows, parts, nv)
+
+
+def bitwise_equal(a, b):
+    return all(np.array_equal(np.asarray(x), np.asarray(y)) for x, y in zip(a, b))
+
+
+def run_sharded_b200(args, ws, rank, local, lib):
+    """bench.py --gpus N (N > 1): config 3's hemisphere (seed 0 on every rank) over the N GPUs with
+    the tensor-core solver, one NCCL all-to-all of partial CSC values per step; value = searchlights
+    of the hemisphere x steps / max over ranks of the device time (strong scaling).  Independent
+    replicas (one hemisphere per GPU, no exchange) are a sub-field."""
+    import torch
+    import torch.distributed as dist
+    from hyperalignment_b200 import _lib as L
+    from hyperalignment_b200 import shard as S
+    from hyperalignment_b200 import workloads as W
+    from hyperalignment_b200.plan import Plan
+    dev = torch.device("cuda", local)
+    w3 = W.rank_deficient_pair(0, nv=args.nv, nt=args.nt)
+    s = w3.sls
+    K = args.steps
+    hX = torch.from_numpy(np.asfortranarray(w3.X).ravel(order="F")).pin_memory()
+    hY = torch.from_numpy(np.asfortranarray(w3.Y).ravel(order="F")).pin_memory()
+    dX, dY = hX.to(dev), hY.to(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    wts = S.hemisphere_weights(s.indices, s.offsets, s.dists, s.radius, w3.nv)
+    plans = []
+
+    def make_range(lo, hi):
+        idx, off, sw = S.sub_geometry(s.indices, s.offsets, wts, lo, hi)
+        plan = Plan(w3.nt, w3.nv, idx, off, weights=sw)
+        plans.append(plan)
+        indptr, rows = plan.pattern()
+
+        def solve(partial):
+            plan.procrustes_device(dX.data_ptr(), dY.data_ptr(), partial.data_ptr(), True, True, L.SOLVER_TC,
+                                   L.OUT_CSC, torch.cuda.current_stream(dev).cuda_stream)
+        return indptr, rows, solve
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    n0 = lib.ha_b200_launch_count()
+    res = sharded_rank(ws, rank, s.offsets, w3.nv, make_range, K, args.warmup, dev, flush=flush)
+    launches = lib.ha_b200_launch_count() - n0
+    clocks = sampler.stop()
+    value = s.count * K / (res["job_ms"] / 1e3)
+    ex = res["exchange"]
+
+    # end to end: X and Y copied from pinned host memory, the owned values copied back, every step
+    hout = torch.empty(res["owned"].numel(), dtype=torch.float64).pin_memory()
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(args.warmup):
+        dX.copy_(hX, non_blocking=True)
+        dY.copy_(hY, non_blocking=True)
+        res["solve_part"]()
+        hout.copy_(ex.combine(res["partial"]), non_blocking=True)
+    torch.cuda.synchronize()
+    dist.barrier()
+    ee = []
+    for _ in range(K):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        dX.copy_(hX, non_blocking=True)
+        dY.copy_(hY, non_blocking=True)
+        res["solve_part"]()
+        hout.copy_(ex.combine(res["partial"]), non_blocking=True)
+        b.record(stream)
+        ee.append((a, b))
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in ee), ws, dev)
+    owned = ex.combine(res["partial"])
+    full = ex.assemble(owned, dst=0)
+    for p in plans:
+        p.close()
+
+    # replicas: every rank solves a whole hemisphere of its own (seed = rank), no exchange
+    wr = W.rank_deficient_pair(rank, nv=args.nv, nt=args.nt)
+    rplan = Plan.from_workload(wr)
+    rX = torch.from_numpy(np.asfortranarray(wr.X).ravel(order="F")).to(dev)
+    rY = torch.from_numpy(np.asfortranarray(wr.Y).ravel(order="F")).to(dev)
+    rvals = torch.zeros(rplan.nnz, dtype=torch.float64, device=dev)
+
+    def rstep():
+        rplan.procrustes_device(rX.data_ptr(), rY.data_ptr(), rvals.data_ptr(), True, True, L.SOLVER_TC, L.OUT_CSR,
+                                stream.cuda_stream)
+    for _ in range(args.warmup):
+        rstep()
+    torch.cuda.synchronize()
+    dist.barrier()
+    evs = []
+    for _ in range(K):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        rstep()
+        b.record(stream)
+        evs.append((a, b))
+    torch.cuda.synchronize()
+    rep_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in evs), ws, dev)
+    rplan.close()
+    del rX, rY, rvals
+
+    check = None
+    if rank == 0:
+        def partial_of(lo, hi):
+            idx, off, sw = S.sub_geometry(s.indices, s.offsets, wts, lo, hi)
+            plan = Plan(w3.nt, w3.nv, idx, off, weights=sw)
+            v = torch.zeros(plan.nnz, dtype=torch.float64, device=dev)
+            plan.procrustes_device(dX.data_ptr(), dY.data_ptr(), v.data_ptr(), True, True, L.SOLVER_TC, L.OUT_CSC,
+                                   stream.cuda_stream)
+            torch.cuda.synchronize()
+            p, r = plan.pattern()
+            plan.close()
+            return p, r, v
+        same = sharded_same_split(s.offsets, w3.nv, ws, partial_of)
+        one = Plan.from_workload(w3)
+        ref = torch.zeros(one.nnz, dtype=torch.float64, device=dev)
+        one.procrustes_device(dX.data_ptr(), dY.data_ptr(), ref.data_ptr(), True, True, L.SOLVER_TC, L.OUT_CSC,
+                              stream.cuda_stream)
+        torch.cuda.synchronize()
+        indptr, rows = one.pattern()
+        refv = ref.cpu().numpy()
+        one.close()
+        pat = bool(np.array_equal(full[0], indptr) and np.array_equal(full[1], rows))
+        check = {"bitwise_vs_same_split_on_rank0": bitwise_equal(full, same),
+                 "pattern_identical_to_one_plan": pat,
+                 "values_relfrob_vs_one_plan": float(np.linalg.norm(full[2] - refv) / np.linalg.norm(refv))
+                 if pat else None,
+                 "what": "the assembled CSC matrix against (a) the same N-way split solved on rank 0 and combined "
+                         "in one process (must be bit-identical) and (b) one plan of the whole hemisphere (float64 "
+                         "sums associated differently)"}
+    dist.barrier()
+    if rank == 0:
+        lo, hi = res["range"]
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": args.warmup,
+            "ms_per_step": res["job_ms"] / K, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "bf16x6 (FP32-accurate split) tensor-core products, f32/f64 host data", "data": "synthetic",
+            "config": config_dict(w3, {"workload": WORKLOAD, "singular_searchlights": int(w3.extra["singular"].sum()),
+                                       "parallelism": f"one hemisphere over {ws} GPUs: contiguous searchlight ranges "
+                                                      "balanced by n^3, column owners, one NCCL all-to-all of partial "
+                                                      "CSC values per step",
+                                       "solver": "tensor cores: split-BF16 cross-covariance + Newton-Schulz polar"}),
+            "solve_ms_per_step": res["solve_ms"] / K, "exchange_ms_per_step": res["exchange_ms"] / K,
+            "searchlights_rank0": int(hi - lo), "columns_rank0": [int(c) for c in ex.col_range],
+            "vs_one_plan": check,
+            "replicas": {"value": aggregate_rate(ws, s.count, K, rep_ms / 1e3), "unit": UNIT, "ms_per_step": rep_ms / K,
+                         "scaling": "weak", "what": "one hemisphere per GPU (seed = rank), no exchange"},
+            "e2e": {"value": s.count * K / (e2e_ms / 1e3), "unit": UNIT,
+                    "h2d_bytes_per_step": int(2 * w3.nt * w3.nv * 8), "d2h_bytes_per_step": int(hout.numel() * 8),
+                    "path": "sharded step with X, Y copied from pinned host memory and the owned CSC values copied "
+                            "back every step (rank 0's bytes)"},
+            "roofline": None, "roofline_note": "reported by the one-GPU line",
+            "cpu_baseline": None, "gpu_launches": int(launches), "clocks": clocks,
+        }
+        print(json.dumps(out))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
 def run_b200(args):
     import torch
     import torch.distributed as dist
@@ -326,6 +580,8 @@ def run_b200(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     lib = L.lib()
     L.check(lib.ha_b200_init(), "ha_b200_init")
+    if ws > 1:
+        return run_sharded_b200(args, ws, rank, local, lib)
 
     # config 3 (headline): the template pair with ~10% of the searchlights made exactly singular;
     # config 2 (sub-field): the same pair without the duplicated columns
@@ -536,10 +792,10 @@ def run_b200(args):
     if rank == 0:
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": args.warmup,
-            "ms_per_step": total_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "ms_per_step": total_ms / K, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
             "dtype": "bf16x6 (FP32-accurate split) tensor-core products, f32/f64 host data", "data": "synthetic",
             "config": config_dict(w3, {"workload": WORKLOAD, "singular_searchlights": int(singular.sum()),
-                                       "parallelism": f"replicas x{ws} (one subject pair per GPU)" if ws > 1 else "single GPU",
+                                       "parallelism": "single GPU (bench.py --gpus N shards this hemisphere over N)",
                                        "solver": "tensor cores: split-BF16 cross-covariance + Newton-Schulz polar, "
                                                  "null-space completion of exactly singular searchlights"}),
             "plain_fp32": {"value": plain_value, "unit": UNIT, "ms_per_step": plain_ms / K,
@@ -1217,7 +1473,6 @@ def run_pca(args):
     kms = np.zeros(len(L.KERNEL_KINDS))
     kcnt = np.zeros(len(L.KERNEL_KINDS), dtype=np.int64)
     lib.ha_b200_kernel_times(kms.ctypes.data_as(L.c_double_p), kcnt.ctypes.data_as(L.c_int64_p))
-    pca_k = L.KERNEL_KINDS.index("pca")
     # CPU oracle on a growing sample of searchlights, and the GPU template of the same sample
     rng = np.random.default_rng(3)
     order = rng.permutation(sls.count)
@@ -1251,7 +1506,11 @@ def run_pca(args):
         "e2e": {"value": sls.count * K / sum(walls), "unit": "searchlights/s",
                 "h2d_bytes_per_step": int(stack.nbytes), "d2h_bytes_per_step": int(out.nbytes),
                 "path": "ha_searchlight_pca_template_b200, wall clock per call"},
-        "pca_kernels_ms_per_step": float(kms[pca_k]), "pca_launches_per_step": int(kcnt[pca_k]),
+        "kernel_ms_per_step": {L.KERNEL_KINDS[i]: round(float(kms[i]), 3) for i in range(len(L.KERNEL_KINDS))
+                               if kcnt[i] > 0},
+        "kernel_kinds": "pca: k_pca_gram, k_pca_tmpl, k_pca_contrib, k_pca_reduce; ridge: k_pchol; jacobi64: "
+                        "k_jacobi<double> (eigenvector mode on the Gram factors, then the polar); formT64: "
+                        "k_form_t_global<double>",
         "error_vs_oracle": {"template_relfrob": err, "sample": int(sub.count)},
         "cpu_baseline": {"value": sub.count / cpu_s, "unit": "searchlights/s", "cores": int(blas), "kind": "port",
                          "sample": f"{sub.count} random searchlights, oracle exact-SVD template (numpy LAPACK, "

@@ -2433,8 +2433,8 @@ int pca_template_impl(const double *dms, int ns, int nt, int nv, const int32_t *
 		{ HA_LAUNCH(kHaB200KPca, st); k_pca_gram<16><<<nb, kBlock, 0, st>>>(dwe.p, P->idx.p, P->off.p, D.p, ns, nt, nv, eV.p); }
 		for (const Bucket &k : be) {
 			const SlWork *wk = dwes.p + k.first;
-			{ HA_LAUNCH(kHaB200KPca, st); k_pchol<<<k.count, kBlock, pchol_smem(k.rpl), st>>>(wk, eV.p, eA.p, stE.p); }
-			HA_LAUNCH(kHaB200KPca, st);
+			{ HA_LAUNCH(kHaB200KRidge, st); k_pchol<<<k.count, kBlock, pchol_smem(k.rpl), st>>>(wk, eV.p, eA.p, stE.p); }
+			HA_LAUNCH(kHaB200KJacobi64, st);
 			if ((rc = launch_jacobi<double>(k.rpl, k.count, k.threads, k.smem, st, wk, eA.p, eV.p, T.p, stE.p, uvb.p, jpe)) != kHaSuccess)
 				return done(rc);
 		}
@@ -2442,11 +2442,11 @@ int pca_template_impl(const double *dms, int ns, int nt, int nv, const int32_t *
 		for (const Bucket &k : bp) {
 			const SlWork *wk = dwps.p + k.first;
 			{
-				HA_LAUNCH(kHaB200KPca, st);
+				HA_LAUNCH(kHaB200KJacobi64, st);
 				if ((rc = launch_jacobi<double>(k.rpl, k.count, k.threads, k.smem, st, wk, eA.p, eV.p, T.p, stP.p, uvb.p, jpp)) != kHaSuccess)
 					return done(rc);
 			}
-			if (k.blocked) { HA_LAUNCH(kHaB200KPca, st); k_form_t_global<double><<<k.count, kBlock, 0, st>>>(wk, eA.p, eV.p, T.p, stP.p, 0, 0); }
+			if (k.blocked) { HA_LAUNCH(kHaB200KFormT64, st); k_form_t_global<double><<<k.count, kBlock, 0, st>>>(wk, eA.p, eV.p, T.p, stP.p, 0, 0); }
 		}
 		{ HA_LAUNCH(kHaB200KPca, st); k_pca_contrib<<<nb, kBlock, 0, st>>>(dwe.p, dwp.p, T.p, nt, dpofs.p, Pw.p); }
 		{ HA_LAUNCH(kHaB200KPca, st); k_pca_reduce<<<nv, kBlock, 0, st>>>(P->vlptr.p, P->vlent.p, P->off.p, P->has_weights ? P->w.p : nullptr,

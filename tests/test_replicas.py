@@ -1,9 +1,11 @@
-"""The N-GPU bench path on the CPU: two gloo ranks (world size 2) through bench.py's own helpers.
+"""The N-GPU bench path on the CPU: two gloo ranks (world size 2) through bench.py's own code.
 
-bench.py --gpus N runs N independent replicas (one subject pair per rank, no data-path exchange).
-What the ranks share is the timing: the job time is the max over ranks and the value is the
-whole-job aggregate.  This checks those helpers across real processes, and that the replicas
-solve different inputs.
+bench.py --gpus N shards one hemisphere over the N ranks (bench.sharded_rank: contiguous
+searchlight ranges, column owners, one all-to-all of partial CSC values per step) and keeps N
+independent replicas as a sub-field.  Here the ranks run that rank code with partial values from
+the oracle: the assembled result must equal the same split combined in one process bit for bit
+and the whole hemisphere up to the association of the float64 sums; the job time is the max over
+ranks and the replica value the whole-job aggregate.
 """
 
 import os
@@ -51,3 +53,56 @@ def test_two_rank_timing_and_replicas(tmp_path):
     assert r0[2] == r1[2] == 150.0                      # job time = max over ranks
     assert r0[3] == pytest.approx(2 * 1000 * 3 / 0.150)  # whole-job aggregate
     assert r0[4] != r1[4]                               # each replica solves its own subject pair
+
+
+def _sharded_main(rank, ws, port, out, case):
+    sys.path.insert(0, ROOT)
+    import datetime
+    import torch
+    import torch.distributed as dist
+    import bench
+    from hyperalignment_b200 import shard as S
+    from oracle import ha_oracle as O
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=ws,
+                            timeout=datetime.timedelta(seconds=60))
+    w, wts, T = case
+
+    def partial_np(lo, hi):
+        idx, off, sw = S.sub_geometry(w.sls.indices, w.sls.offsets, wts, lo, hi)
+        indptr, rows = O.sparse_init(idx, off, w.nv)
+        data = np.zeros(rows.size)
+        O.searchlight_procrustes_csc(w.X, w.Y, idx, off, indptr, rows, data, weights=sw, transforms=T[lo:hi])
+        return indptr.astype(np.int64), rows, data
+
+    def make_range(lo, hi):
+        indptr, rows, data = partial_np(lo, hi)
+        src = torch.from_numpy(data)
+        return indptr, rows, lambda partial: partial.copy_(src)
+
+    res = bench.sharded_rank(ws, rank, w.sls.offsets, w.nv, make_range, 3, 1, "cpu")
+    full = res["exchange"].assemble(res["owned"], dst=0)
+    if rank == 0:
+        same = bench.sharded_same_split(w.sls.offsets, w.nv, ws,
+                                        lambda lo, hi: (lambda p: (p[0], p[1], torch.from_numpy(p[2])))(partial_np(lo, hi)))
+        np.savez(os.path.join(out, "sharded.npz"), indptr=full[0], rows=full[1], vals=full[2],
+                 bitwise=bench.bitwise_equal(full, same), job=res["job_ms"], solve=res["solve_ms"],
+                 exch=res["exchange_ms"], bounds=res["bounds"])
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_rank_sharded_hemisphere(tmp_path):
+    """bench.py --gpus 2's rank code (bench.sharded_rank) over two gloo ranks."""
+    import torch.multiprocessing as mp
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from test_shard import _case, _full
+    w, wts, T = _case(seed=9)
+    mp.spawn(_sharded_main, args=(2, _free_port(), str(tmp_path), (w, wts, T)), nprocs=2, join=True)
+    r = np.load(tmp_path / "sharded.npz")
+    indptr, rows, data = _full(w, wts, T)
+    assert bool(r["bitwise"])                                   # same split in one process: identical bits
+    assert np.array_equal(r["indptr"], indptr) and np.array_equal(r["rows"], rows)
+    assert np.linalg.norm(r["vals"] - data) <= 1e-13 * np.linalg.norm(data)
+    assert 0 < r["bounds"][1] < w.sls.count                     # both ranks hold searchlights
+    assert r["job"] >= r["solve"] and r["job"] >= r["exch"] >= 0.0
+

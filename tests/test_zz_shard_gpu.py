@@ -58,3 +58,33 @@ def test_sharded_plans_equal_one_plan(gpu, solver):
         np.testing.assert_array_equal(got[1], rows)
         rel = np.linalg.norm(got[2] - ref) / np.linalg.norm(ref)
         assert rel <= REL[solver], (world, rel)
+
+
+def test_bench_sharded_path_one_rank_nccl(gpu, capsys):
+    """bench.py --gpus N's sharded rank code (bench.run_sharded_b200) on a one-rank NCCL group: the
+    same collectives (all-reduce, all-to-all, point-to-point assembly) on this GPU alone, and the
+    line's own checks: bit-identical to the same split solved on rank 0, the one plan's pattern."""
+    import argparse
+    import json
+    import os
+    import socket
+    import sys
+    import datetime
+    import torch.distributed as dist
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=120))
+    args = argparse.Namespace(nv=2562, nt=200, steps=2, warmup=1)
+    bench.run_sharded_b200(args, 1, 0, 0, L.lib())
+    assert not dist.is_initialized()
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert line["n_gpus"] == 1 and line["scaling"] == "strong" and line["value"] > 0
+    assert line["exchange_ms_per_step"] >= 0.0 and line["solve_ms_per_step"] > 0.0
+    chk = line["vs_one_plan"]
+    assert chk["bitwise_vs_same_split_on_rank0"] and chk["pattern_identical_to_one_plan"]
+    assert chk["values_relfrob_vs_one_plan"] <= 1e-12
+    assert line["replicas"]["value"] > 0 and line["e2e"]["value"] > 0
