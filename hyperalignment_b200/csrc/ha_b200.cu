@@ -864,7 +864,7 @@ int build_tc(HaB200Plan *P) {
 			w.pofs = xacc;
 			w.aofs = aacc;
 			w.tofs = ch.tofs[q];
-			xacc += 3 * (int64_t)np * np;
+			xacc += 2 * (int64_t)np * np;  // the iteration's two FP16 planes
 			aacc += (int64_t)np * np;
 			ch.tcw.push_back(w);
 		}

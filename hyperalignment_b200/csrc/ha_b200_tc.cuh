@@ -6,10 +6,16 @@
 // Newton-Schulz iteration
 //     X_0 = A / u,   G_k = X_k^T X_k,   X_{k+1} = X_k (c1_k I + c3_k G_k),
 // (u >= sigma_max(A); c1 = 3a/2, c3 = -a^3/2 with a from a capped scaling schedule, a = 1 in the
-// final phase) on the 5th-generation tensor cores.  Every product runs in BF16 with FP32
-// accumulation in tensor memory, with each FP32 operand split exactly into three BF16 parts
-// (x = hi + mid + lo) and the six products hi*hi + hi*mid + mid*hi + mid*mid + hi*lo + lo*hi
-// accumulated: the result carries FP32 accuracy (the dropped terms are below 2^-32 relative).
+// final phase) on the 5th-generation tensor cores, with FP32 accumulation in tensor memory and
+// every FP32 operand split exactly into 16-bit parts:
+//   * the cross-covariance (inputs of any range): three BF16 parts x = hi + mid + lo and the six
+//     products hi*hi + hi*mid + mid*hi + mid*mid + hi*lo + lo*hi (the dropped terms are below
+//     2^-32 relative);
+//   * the iteration, whose operands are bounded (the iterate's singular values stay <= 1, so
+//     |X| <= 1, and |P| = |c1 I + c3 X^T X| <= |c1| + |c3| < 5): two FP16 parts of x * 2^12,
+//     hi = fp16(x 2^12), mid = fp16(x 2^12 - hi), 22 significant bits (values below 2^-15 keep an
+//     absolute error under 2^-37), and the three products hi*hi + hi*mid + mid*hi (the dropped
+//     mid*mid is 2^-22 relative); the accumulator holds 2^24 times the product.
 //
 // One CTA computes one 128-row tile of one searchlight's product: 128 threads stage K-slices of
 // 16 with cp.async into a ring of shared-memory stages (canonical no-swizzle core-matrix
@@ -17,7 +23,7 @@
 // searchlight's padded size, K = 16) into tensor memory and commits each stage to an mbarrier,
 // and the four warps read the accumulator back with tcgen05.ld for the epilogue.
 //
-// Storage of a searchlight's iterate X and of P = c1 I + c3 G in HBM: three bf16 planes of
+// Storage of a searchlight's iterate X and of P = c1 I + c3 G in HBM: two FP16 planes of
 // np x np (np = n rounded up to 16), each in 8 x 8 core matrices, core (r, c) = rows 8r..8r+7,
 // columns 8c..8c+7 at element offset (r * np/8 + c) * 64, row-major inside (16 bytes a row).
 // The iterate alternates between two buffers (the update reads one and writes the other).
@@ -26,6 +32,7 @@
 #pragma once
 
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -41,6 +48,16 @@ constexpr uint64_t kTcWaitNs = 2000000000ull;  // a pipeline wait longer than 2 
 
 enum : int { kTcPhaseXcov = 0, kTcPhaseGram = 1, kTcPhaseUpdate = 2 };
 
+constexpr float kTcOpScale = 4096.f;                 // iteration operands are stored as x * 2^12
+constexpr float kTcAccUnscale = 1.f / 16777216.f;    // 2^-24: the iteration's accumulator -> product
+
+// 16-bit planes per operand: three BF16 parts for the cross-covariance, two FP16 parts for the
+// iteration's Gram and update products.
+template <int PHASE>
+struct TcFmt {
+	static constexpr int planes = PHASE == kTcPhaseXcov ? 3 : 2;
+};
+
 // One searchlight of the tensor-core solve.
 struct TcWork {
 	int32_t s;     // searchlight index
@@ -49,8 +66,8 @@ struct TcWork {
 	int32_t np;    // n rounded up to 16
 	int32_t sofs;  // flat offset of the searchlight in sl_indices
 	int32_t pad_;
-	int64_t xofs;  // bf16 element offset of the iterate's three planes (3 np^2)
-	int64_t pofs;  // bf16 element offset of P's three planes
+	int64_t xofs;  // 16-bit element offset of the iterate's two planes (2 np^2)
+	int64_t pofs;  // 16-bit element offset of P's two planes
 	int64_t aofs;  // float element offset of A (np x np, row-major, leading dimension np)
 	int64_t tofs;  // float element offset of T in the T scratch (n x n)
 };
@@ -195,8 +212,10 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint
 }
 
 // Instruction descriptor of kind::f16 with BF16 A and B and an FP32 accumulator.
-__host__ __device__ __forceinline__ uint32_t mma_idesc(int M, int N, int a_mn, int b_mn) {
-	return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)a_mn << 15) | ((uint32_t)b_mn << 16) |
+// f16: A and B are FP16 (type field 0) instead of BF16 (type field 1); both operands always share
+// one type.
+__host__ __device__ __forceinline__ uint32_t mma_idesc(int M, int N, int a_mn, int b_mn, bool f16 = false) {
+	return (1u << 4) | (f16 ? 0u : ((1u << 7) | (1u << 10))) | ((uint32_t)a_mn << 15) | ((uint32_t)b_mn << 16) |
 	       ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
@@ -239,26 +258,25 @@ __device__ __forceinline__ void split3(float v, __nv_bfloat16 &hi, __nv_bfloat16
 	lo = __float2bfloat16_rn(r1 - __bfloat162float(mid));
 }
 
-// Eight consecutive FP32 values of one core-matrix row -> 16 bytes in each of the three planes
-// (the same exact split as split3, two values per packed conversion).
-__device__ __forceinline__ void store_split8(const float *v, __nv_bfloat16 *p0, __nv_bfloat16 *p1,
-                                             __nv_bfloat16 *p2) {
-	__nv_bfloat162 h[4], m[4], l[4];
+// Eight consecutive FP32 values of one core-matrix row of an iteration operand -> 16 bytes in each
+// of the two FP16 planes: hi = fp16(x 2^12), mid = fp16(x 2^12 - hi) (the difference is exact in
+// FP32).
+__device__ __forceinline__ void store_split8h(const float *v, __nv_bfloat16 *p0, __nv_bfloat16 *p1) {
+	__half2 h[4], m[4];
 #pragma unroll
 	for (int i = 0; i < 4; i++) {
-		const float a = v[2 * i], b = v[2 * i + 1];
-		h[i] = __floats2bfloat162_rn(a, b);
-		const float ra = a - __low2float(h[i]), rb = b - __high2float(h[i]);
-		m[i] = __floats2bfloat162_rn(ra, rb);
-		l[i] = __floats2bfloat162_rn(ra - __low2float(m[i]), rb - __high2float(m[i]));
+		const float a = v[2 * i] * kTcOpScale, b = v[2 * i + 1] * kTcOpScale;
+		h[i] = __floats2half2_rn(a, b);
+		m[i] = __floats2half2_rn(a - __low2float(h[i]), b - __high2float(h[i]));
 	}
 	*reinterpret_cast<uint4 *>(p0) = *reinterpret_cast<const uint4 *>(h);
 	*reinterpret_cast<uint4 *>(p1) = *reinterpret_cast<const uint4 *>(m);
-	*reinterpret_cast<uint4 *>(p2) = *reinterpret_cast<const uint4 *>(l);
 }
 
-// Bytes of one pipeline stage for an N-column product: A (128 x 16) and B (N x 16), three planes each.
-__host__ __device__ __forceinline__ int tc_stage_bytes(int N) { return 3 * (128 * 16 * 2) + 3 * (N * 16 * 2); }
+// Bytes of one pipeline stage for an N-column product: A (128 x 16) and B (N x 16), `planes` each.
+__host__ __device__ __forceinline__ int tc_stage_bytes(int N, int planes) {
+	return planes * (128 * 16 * 2) + planes * (N * 16 * 2);
+}
 
 // tensor-memory columns for an N-column FP32 accumulator
 __device__ __forceinline__ uint32_t tc_tmem_cols(int N) {
@@ -270,7 +288,8 @@ __device__ __forceinline__ uint32_t tc_tmem_cols(int N) {
 // ---------------------------------------------------------------------------------------------
 // stage loads
 // ---------------------------------------------------------------------------------------------
-// Stage layout (bytes): A plane p at p * 4096, B plane p at 12288 + p * 32 N.  Inside a plane,
+// Stage layout (bytes), NPL planes per operand: A plane p at p * 4096, B plane p at NPL * 4096 +
+// p * 32 N.  Inside a plane,
 // core matrix (g, k) (g: 8-row group along M or N, k: which 8-element half of the K-slice) sits at
 // (g * 2 + k) * 128, so LBO = 128 and SBO = 256 for both operand majors.
 
@@ -321,15 +340,16 @@ __device__ __forceinline__ void tc_plan_tile(TcLoadPlan &lp, const int32_t *s_sl
 
 // Issue the cp.async copies of K-slice ks into the stage at shared address `stage`.  A planes at
 // A + p * pstrideA, B planes at B + p * pstrideB (elements).
+template <int NPL>
 __device__ __forceinline__ void tc_load_slice(const TcLoadPlan &lp, const __nv_bfloat16 *A, int64_t pstrideA,
                                               const __nv_bfloat16 *B, int64_t pstrideB, int N, int ks,
                                               uint32_t stage) {
 	const int32_t oa = ks * lp.strideA, ob = ks * lp.strideB;
 #pragma unroll
-	for (int p = 0; p < 3; p++) {
+	for (int p = 0; p < NPL; p++) {
 		const __nv_bfloat16 *Ap = A + p * pstrideA;
 		const __nv_bfloat16 *Bp = B + p * pstrideB;
-		const uint32_t sa = stage + p * 4096, sb = stage + 12288 + p * 32 * N;
+		const uint32_t sa = stage + p * 4096, sb = stage + NPL * 4096 + p * 32 * N;
 #pragma unroll
 		for (int i = 0; i < 2; i++) {
 			const bool ok = lp.sA[i] >= 0;
@@ -341,6 +361,26 @@ __device__ __forceinline__ void tc_load_slice(const TcLoadPlan &lp, const __nv_b
 			const bool ok = lp.sB[j] >= 0;
 			cp_async16(sb + lp.dB[j], ok ? Bp + lp.sB[j] + ob : Bp, ok ? 16u : 0u);
 		}
+	}
+}
+
+// The products of one K-slice staged at shared address `st` into the accumulator at `tmem`
+// (columns 0..255 and, for N > 256, 256..N-1), smallest first.  Issued by one thread.
+template <int PHASE>
+__device__ __forceinline__ void tc_issue_products(uint32_t tmem, uint32_t st, int N, uint32_t id0, uint32_t id1,
+                                                  bool first) {
+	constexpr int NPL = TcFmt<PHASE>::planes;
+	constexpr int NQ = NPL == 3 ? 6 : 3;
+#pragma unroll
+	for (int q = 0; q < NQ; q++) {
+		// three planes: lo*hi, hi*lo, mid*mid, mid*hi, hi*mid, hi*hi; two: mid*hi, hi*mid, hi*hi
+		const int pa = NPL == 3 ? ((q == 0) ? 2 : (q == 2 || q == 3) ? 1 : 0) : (q == 0 ? 1 : 0);
+		const int pb = NPL == 3 ? ((q == 1) ? 2 : (q == 2 || q == 4) ? 1 : 0) : (q == 1 ? 1 : 0);
+		const uint32_t acc = (!first || q > 0) ? 1u : 0u;
+		const uint64_t ad = smem_desc(st + pa * 4096, 128, 256);
+		const uint32_t baddr = st + NPL * 4096 + pb * 32 * N;
+		mma_bf16(tmem, ad, smem_desc(baddr, 128, 256), id0, acc);
+		if (N > 256) mma_bf16(tmem + 256, ad, smem_desc(baddr + 32 * 256, 128, 256), id1, acc);
 	}
 }
 
@@ -404,7 +444,8 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_gemm(const TcArgs a) {
 		}
 	}
 
-	const int stage_bytes = tc_stage_bytes(N);
+	constexpr int NPL = TcFmt<PHASE>::planes;
+	const int stage_bytes = tc_stage_bytes(N, NPL);
 	int S = a.smem_bytes / stage_bytes;
 	if (S > kTcMaxStages) S = kTcMaxStages;
 	const int nk = (PHASE == kTcPhaseXcov) ? (a.ntp >> 4) : (np >> 4);
@@ -433,14 +474,17 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_gemm(const TcArgs a) {
 	const __nv_bfloat16 *srcA = (PHASE == kTcPhaseXcov) ? a.Xb : Xs;
 	const __nv_bfloat16 *srcB = (PHASE == kTcPhaseXcov) ? a.Yb : Bs;
 	const int64_t pstride = (PHASE == kTcPhaseXcov) ? a.vplane : (int64_t)np * np;
-	auto load = [&](int ks, int s) { tc_load_slice(lp, srcA, pstride, srcB, pstride, N, ks, smem0 + s * stage_bytes); };
+	auto load = [&](int ks, int s) {
+		tc_load_slice<NPL>(lp, srcA, pstride, srcB, pstride, N, ks, smem0 + s * stage_bytes);
+	};
 
 	// operand majors: cross-covariance K/K, Gram MN/MN, update K/MN
 	const int a_mn = (PHASE == kTcPhaseGram) ? 1 : 0;
 	const int b_mn = (PHASE == kTcPhaseXcov) ? 0 : 1;
 	const int N0 = N > 256 ? 256 : N;
-	const uint32_t id0 = mma_idesc(128, N0, a_mn, b_mn);
-	const uint32_t id1 = N > 256 ? mma_idesc(128, N - 256, a_mn, b_mn) : 0u;
+	const bool f16 = PHASE != kTcPhaseXcov;
+	const uint32_t id0 = mma_idesc(128, N0, a_mn, b_mn, f16);
+	const uint32_t id1 = N > 256 ? mma_idesc(128, N - 256, a_mn, b_mn, f16) : 0u;
 
 	if (!failed) {
 		for (int j = 0; j < S - 1; j++) {
@@ -457,19 +501,7 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_gemm(const TcArgs a) {
 			if (s_fail) { failed = true; break; }
 			if (tid == 0) {
 				tc_fence_after();
-				const uint32_t st = smem0 + s * stage_bytes;
-				// products in increasing size: lo*hi, hi*lo, mid*mid, mid*hi, hi*mid, hi*hi
-#pragma unroll
-				for (int q = 0; q < 6; q++) {
-					const int pa = (q == 0) ? 2 : (q == 2 || q == 3) ? 1 : 0;
-					const int pb = (q == 1) ? 2 : (q == 2 || q == 4) ? 1 : 0;
-					const uint32_t aaddr = st + pa * 4096;
-					const uint32_t baddr = st + 12288 + pb * 32 * N;
-					const uint32_t acc = (ks > 0 || q > 0) ? 1u : 0u;
-					const uint64_t ad = smem_desc(aaddr, 128, 256);
-					mma_bf16(tmem, ad, smem_desc(baddr, 128, 256), id0, acc);
-					if (N > 256) mma_bf16(tmem + 256, ad, smem_desc(baddr + 32 * 256, 128, 256), id1, acc);
-				}
+				tc_issue_products<PHASE>(tmem, smem0 + s * stage_bytes, N, id0, id1, ks == 0);
 				mma_commit(&s_bar[s]);
 			}
 			const int kn = ks + S - 1;
@@ -501,6 +533,10 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_gemm(const TcArgs a) {
 			float v[16];
 			tmem_ld16(trow + (uint32_t)c0, v);
 			if (row >= np) continue;
+			if (PHASE != kTcPhaseXcov) {
+#pragma unroll
+				for (int q = 0; q < 16; q++) v[q] *= kTcAccUnscale;
+			}
 			if (PHASE == kTcPhaseXcov) {
 				if (row < n) {
 					float4 *dst = reinterpret_cast<float4 *>(a.A32 + w.aofs + (int64_t)row * np + n0 + c0);
@@ -523,7 +559,7 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_gemm(const TcArgs a) {
 #pragma unroll
 				for (int h = 0; h < 2; h++) {
 					const int64_t o = ((int64_t)(row >> 3) * npg + ((n0 + c0) >> 3) + h) * 64 + (row & 7) * 8;
-					store_split8(v + 8 * h, P0 + o, P0 + pe + o, P0 + 2 * pe + o);
+					store_split8h(v + 8 * h, P0 + o, P0 + pe + o);
 				}
 			} else {
 				if (final_update) {
@@ -540,7 +576,7 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_gemm(const TcArgs a) {
 #pragma unroll
 					for (int h = 0; h < 2; h++) {
 						const int64_t o = ((int64_t)(row >> 3) * npg + ((n0 + c0) >> 3) + h) * 64 + (row & 7) * 8;
-						store_split8(v + 8 * h, X0 + o, X0 + pe + o, X0 + 2 * pe + o);
+						store_split8h(v + 8 * h, X0 + o, X0 + pe + o);
 					}
 				}
 			}
@@ -621,12 +657,16 @@ __device__ bool tc_tile(const TcSolveArgs &a, const TcWork &w, int t, const int3
 	const __nv_bfloat16 *srcA = (PHASE == kTcPhaseXcov) ? a.Xb : Xs;
 	const __nv_bfloat16 *srcB = (PHASE == kTcPhaseXcov) ? a.Yb : Bs;
 	const int64_t pstride = (PHASE == kTcPhaseXcov) ? a.vplane : (int64_t)np * np;
-	auto load = [&](int ks, int s) { tc_load_slice(lp, srcA, pstride, srcB, pstride, N, ks, smem0 + s * stage_bytes); };
+	constexpr int NPL = TcFmt<PHASE>::planes;
+	auto load = [&](int ks, int s) {
+		tc_load_slice<NPL>(lp, srcA, pstride, srcB, pstride, N, ks, smem0 + s * stage_bytes);
+	};
 	const int a_mn = (PHASE == kTcPhaseGram) ? 1 : 0;
 	const int b_mn = (PHASE == kTcPhaseXcov) ? 0 : 1;
 	const int N0 = N > 256 ? 256 : N;
-	const uint32_t id0 = mma_idesc(128, N0, a_mn, b_mn);
-	const uint32_t id1 = N > 256 ? mma_idesc(128, N - 256, a_mn, b_mn) : 0u;
+	const bool f16 = PHASE != kTcPhaseXcov;
+	const uint32_t id0 = mma_idesc(128, N0, a_mn, b_mn, f16);
+	const uint32_t id1 = N > 256 ? mma_idesc(128, N - 256, a_mn, b_mn, f16) : 0u;
 
 	// every stage is free here: the previous tile's products all completed
 	for (int j = 0; j < S - 1; j++) {
@@ -642,17 +682,7 @@ __device__ bool tc_tile(const TcSolveArgs &a, const TcWork &w, int t, const int3
 		if (*s_fail) { failed = true; break; }
 		if (tid == 0) {
 			tc_fence_after();
-			const uint32_t st = smem0 + s * stage_bytes;
-#pragma unroll
-			for (int q = 0; q < 6; q++) {
-				const int pa = (q == 0) ? 2 : (q == 2 || q == 3) ? 1 : 0;
-				const int pb = (q == 1) ? 2 : (q == 2 || q == 4) ? 1 : 0;
-				const uint32_t acc = (ks > 0 || q > 0) ? 1u : 0u;
-				const uint64_t ad = smem_desc(st + pa * 4096, 128, 256);
-				const uint32_t baddr = st + 12288 + pb * 32 * N;
-				mma_bf16(tmem, ad, smem_desc(baddr, 128, 256), id0, acc);
-				if (N > 256) mma_bf16(tmem + 256, ad, smem_desc(baddr + 32 * 256, 128, 256), id1, acc);
-			}
+			tc_issue_products<PHASE>(tmem, smem0 + s * stage_bytes, N, id0, id1, ks == 0);
 			mma_commit(&s_bar[s]);
 		}
 		pp.uses[s]++;
@@ -684,6 +714,10 @@ __device__ bool tc_tile(const TcSolveArgs &a, const TcWork &w, int t, const int3
 		float v[16];
 		tmem_ld16(trow + (uint32_t)c0, v);
 		if (row >= np) continue;
+		if (PHASE != kTcPhaseXcov) {
+#pragma unroll
+			for (int q = 0; q < 16; q++) v[q] *= kTcAccUnscale;
+		}
 		if (PHASE == kTcPhaseXcov) {
 			if (row < n) {
 				float4 *dst = reinterpret_cast<float4 *>(a.A32 + w.aofs + (int64_t)row * np + c0);
@@ -706,7 +740,7 @@ __device__ bool tc_tile(const TcSolveArgs &a, const TcWork &w, int t, const int3
 #pragma unroll
 			for (int h = 0; h < 2; h++) {
 				const int64_t o = ((int64_t)(row >> 3) * npg + (c0 >> 3) + h) * 64 + (row & 7) * 8;
-				store_split8(v + 8 * h, P0 + o, P0 + pe + o, P0 + 2 * pe + o);
+				store_split8h(v + 8 * h, P0 + o, P0 + pe + o);
 			}
 		} else if (final_update) {
 			if (row < n) {
@@ -722,7 +756,7 @@ __device__ bool tc_tile(const TcSolveArgs &a, const TcWork &w, int t, const int3
 #pragma unroll
 			for (int h = 0; h < 2; h++) {
 				const int64_t o = ((int64_t)(row >> 3) * npg + (c0 >> 3) + h) * 64 + (row & 7) * 8;
-				store_split8(v + 8 * h, X0 + o, X0 + pe + o, X0 + 2 * pe + o);
+				store_split8h(v + 8 * h, X0 + o, X0 + pe + o);
 			}
 		}
 	}
@@ -772,7 +806,7 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_solve(const TcSolveArgs a) {
 		if (item >= a.count) break;
 		const TcWork w = a.work[a.order[item]];
 		const int n = w.n, np = w.np, ntiles = (np + 127) >> 7;
-		const int stage_bytes = tc_stage_bytes(np);
+		const int stage_bytes = tc_stage_bytes(np, 3);  // the largest format; the iteration's fit too
 		int S = a.smem_bytes / stage_bytes;
 		if (S > kTcMaxStages) S = kTcMaxStages;
 		if (S < 2 || (uint32_t)np > ncols) { s_fail = 1; failed = true; break; }
@@ -833,7 +867,7 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_solve(const TcSolveArgs a) {
 					v[q] = (row < n && col < n) ? A[(int64_t)row * np + col] * inv : 0.f;
 				}
 				const int64_t o = ((int64_t)(row >> 3) * npg + cg) * 64 + (row & 7) * 8;
-				store_split8(v, X0 + o, X0 + pe + o, X0 + 2 * pe + o);
+				store_split8h(v, X0 + o, X0 + pe + o);
 			}
 			__threadfence();
 			__syncthreads();
@@ -919,8 +953,9 @@ __global__ void k_split3_vertex_major(const double *__restrict__ X, int nt, int 
 	}
 }
 
-// X_0 = A / u with u = min(||A||_F, sqrt(||A||_1 ||A||_inf)) >= sigma_max(A), written as the three
-// core-tiled planes (np x np, padding zero); iteration state and residual slots cleared.
+// X_0 = A / u with u = min(||A||_F, sqrt(||A||_1 ||A||_inf)) >= sigma_max(A), written as the two
+// core-tiled FP16 planes of the iteration (np x np, padding zero); iteration state and residual
+// slots cleared.
 __global__ void __launch_bounds__(256) k_tc_ns_init(const TcWork *__restrict__ work, const float *__restrict__ A32,
                                                     __nv_bfloat16 *__restrict__ Xp, TcState *__restrict__ st,
                                                     float *__restrict__ res_part) {
@@ -977,7 +1012,7 @@ __global__ void __launch_bounds__(256) k_tc_ns_init(const TcWork *__restrict__ w
 			v[q] = (row < n && col < n) ? A[(int64_t)row * np + col] * inv : 0.f;
 		}
 		const int64_t o = ((int64_t)(row >> 3) * npg + cg) * 64 + (row & 7) * 8;
-		store_split8(v, X0 + o, X0 + pe + o, X0 + 2 * pe + o);
+		store_split8h(v, X0 + o, X0 + pe + o);
 	}
 }
 
@@ -1177,8 +1212,8 @@ __global__ void __launch_bounds__(256) k_tc_complete(const TcWork *__restrict__ 
 	}
 }
 
-// Row-major FP32 n x n (leading dimension n) -> three core-tiled bf16 planes of np x np; unpack
-// reverses it (hi + mid + lo).  Used by the product self-test.
+// Row-major FP32 n x n (leading dimension n) -> the iteration's two core-tiled FP16 planes of np x
+// np; unpack reverses it ((hi + mid) / 2^12).  Used by the product self-test.
 __global__ void k_tc_pack(const float *__restrict__ M, int n, int np, __nv_bfloat16 *__restrict__ planes) {
 	const int npg = np >> 3;
 	const int64_t pe = (int64_t)np * np;
@@ -1190,7 +1225,7 @@ __global__ void k_tc_pack(const float *__restrict__ M, int n, int np, __nv_bfloa
 			v[q] = (row < n && col < n) ? M[(int64_t)row * n + col] : 0.f;
 		}
 		const int64_t o = ((int64_t)(row >> 3) * npg + cg) * 64 + (row & 7) * 8;
-		store_split8(v, planes + o, planes + pe + o, planes + 2 * pe + o);
+		store_split8h(v, planes + o, planes + pe + o);
 	}
 }
 __global__ void k_tc_unpack(const __nv_bfloat16 *__restrict__ planes, int n, int np, float *__restrict__ M) {
@@ -1199,7 +1234,8 @@ __global__ void k_tc_unpack(const __nv_bfloat16 *__restrict__ planes, int n, int
 	for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < (int64_t)n * n; e += (int64_t)gridDim.x * blockDim.x) {
 		const int row = (int)(e / n), col = (int)(e - (int64_t)row * n);
 		const int64_t o = ((int64_t)(row >> 3) * npg + (col >> 3)) * 64 + (row & 7) * 8 + (col & 7);
-		M[e] = __bfloat162float(planes[o]) + __bfloat162float(planes[pe + o]) + __bfloat162float(planes[2 * pe + o]);
+		const __half *hp = reinterpret_cast<const __half *>(planes);
+		M[e] = (__half2float(hp[o]) + __half2float(hp[pe + o])) * (1.f / kTcOpScale);
 	}
 }
 

@@ -1,8 +1,9 @@
 """GPU parity of the tensor-core solver (kHaB200SolverTC) through the C ABI.
 
 Tolerances (written per test):
-  * one tensor-core product (split BF16, six products, FP32 accumulation over K up to 512)
-    vs float64: relative Frobenius <= 5e-6
+  * one tensor-core product vs float64: relative Frobenius <= 5e-6 (the cross-covariance: three
+    BF16 parts, six products; the iteration's Gram and update: two FP16 parts of x 2^12, three
+    products; FP32 accumulation over K up to 512)
   * per-searchlight transform T_s vs the float64 oracle: relative Frobenius <= 2e-5 (the
     metric's bound is 1e-4; the three-part split carries FP32 accuracy, measured 1.0e-5 at
     n = 512)
@@ -45,10 +46,12 @@ def selftest(hlib, which, n, a, b=None, nt=0):
 @pytest.mark.parametrize("n", [16, 40, 100, 128, 144, 200, 256, 272, 304, 400, 512])
 def test_tc_products(gpu, hlib, n):
     """Each product type of the solver on one matrix: X^T X (MN-major A and B), X M (K-major A,
-    MN-major B), and the gathered cross-covariance (K-major A and B, K = time)."""
+    MN-major B), and the gathered cross-covariance (K-major A and B, K = time).  The iteration's
+    operands are in its range (entries of a matrix with singular values about 1, so X^T X and
+    X M stay below the FP16 planes' limit); the cross-covariance's inputs have any scale."""
     rng = np.random.default_rng(n)
-    X = rng.standard_normal((n, n)).astype(np.float32)
-    M = rng.standard_normal((n, n)).astype(np.float32)
+    X = (rng.standard_normal((n, n)) / np.sqrt(n)).astype(np.float32)
+    M = (rng.standard_normal((n, n)) / np.sqrt(n)).astype(np.float32)
     x64, m64 = X.astype(np.float64), M.astype(np.float64)
     assert relf(selftest(hlib, 0, n, X), x64.T @ x64) <= PROD_REL
     assert relf(selftest(hlib, 1, n, X, M), x64 @ m64) <= PROD_REL
