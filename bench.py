@@ -269,19 +269,20 @@ def run_reference(args):
 # ---------------------------------------------------------------------------------------------
 
 def tc_algorithmic_flops(sizes, iters):
-    """BF16 tensor-core work of the Newton-Schulz polar iteration as the algorithm defines it (no
+    """Tensor-core work of the Newton-Schulz polar iteration as the algorithm defines it (no
     padding): per searchlight and iteration two n x n x n products (X^T X and X P), each executed as
-    six BF16 products of the three-part split: 24 n^3 flops."""
+    three FP16 products of the two-part split: 12 n^3 flops."""
     n = sizes.astype(np.float64)
-    return float((24.0 * iters.astype(np.float64) * n ** 3).sum())
+    return float((12.0 * iters.astype(np.float64) * n ** 3).sum())
 
 
 def tc_executed_flops(sizes, iters):
-    """BF16 MMA work the kernels issue, padding included: rows in 128-row tiles, N and K padded to 16."""
+    """MMA work the iteration's kernels issue, padding included: rows in 128-row tiles, N and K padded
+    to 16, three products per n^3 product, two n^3 products per iteration."""
     n = sizes.astype(np.int64)
     npad = (n + 15) // 16 * 16
     mpad = (npad + 127) // 128 * 128
-    return float((2 * 6 * 2 * iters.astype(np.float64) * mpad * npad.astype(np.float64) ** 2).sum())
+    return float((2 * 3 * 2 * iters.astype(np.float64) * mpad * npad.astype(np.float64) ** 2).sum())
 
 
 def sample_errors(w, singular, sample, Ts):
@@ -711,7 +712,7 @@ def run_b200(args):
         roof = {"bound": "tensor", "kernel": "tc_ns (k_tc_gemm Gram + update, k_tc_ns_init)", "achieved": achieved / 1e12,
                 "peak": peak, "unit": "TFLOP/s", "frac": achieved / 1e12 / peak, "traffic": None,
                 "peak_source": f"{peak_src} bf16 sustained",
-                "algorithmic": "24 n^3 BF16 flops per searchlight and iteration (two n^3 products, six BF16 "
+                "algorithmic": "12 n^3 tensor flops per searchlight and iteration (two n^3 products, three FP16 "
                                "products each); iterations as run (mean %.2f)" % float(tc_iters.mean()),
                 "executed_with_padding_tflops": executed / 1e12,
                 "svd_equivalent_tflops": useful / 1e12,
