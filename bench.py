@@ -544,12 +544,12 @@ def run_sharded_b200(args, ws, rank, local, lib):
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": args.warmup,
             "ms_per_step": res["job_ms"] / K, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
-            "dtype": "bf16x6 (FP32-accurate split) tensor-core products, f32/f64 host data", "data": "synthetic",
+            "dtype": "tensor-core products, FP32-accurate splits: bf16x6 cross-covariance, fp16x3 iteration; f32/f64 host data", "data": "synthetic",
             "config": config_dict(w3, {"workload": WORKLOAD, "singular_searchlights": int(w3.extra["singular"].sum()),
                                        "parallelism": f"one hemisphere over {ws} GPUs: contiguous searchlight ranges "
                                                       "balanced by n^3, column owners, one NCCL all-to-all of partial "
                                                       "CSC values per step",
-                                       "solver": "tensor cores: split-BF16 cross-covariance + Newton-Schulz polar"}),
+                                       "solver": "tensor cores: split-BF16 cross-covariance + split-FP16 Newton-Schulz polar"}),
             "solve_ms_per_step": res["solve_ms"] / K, "exchange_ms_per_step": res["exchange_ms"] / K,
             "searchlights_rank0": int(hi - lo), "columns_rank0": [int(c) for c in ex.col_range],
             "vs_one_plan": check,
@@ -794,10 +794,10 @@ def run_b200(args):
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": args.warmup,
             "ms_per_step": total_ms / K, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
-            "dtype": "bf16x6 (FP32-accurate split) tensor-core products, f32/f64 host data", "data": "synthetic",
+            "dtype": "tensor-core products, FP32-accurate splits: bf16x6 cross-covariance, fp16x3 iteration; f32/f64 host data", "data": "synthetic",
             "config": config_dict(w3, {"workload": WORKLOAD, "singular_searchlights": int(singular.sum()),
                                        "parallelism": "single GPU (bench.py --gpus N shards this hemisphere over N)",
-                                       "solver": "tensor cores: split-BF16 cross-covariance + Newton-Schulz polar, "
+                                       "solver": "tensor cores: split-BF16 cross-covariance + split-FP16 Newton-Schulz polar, "
                                                  "null-space completion of exactly singular searchlights"}),
             "plain_fp32": {"value": plain_value, "unit": UNIT, "ms_per_step": plain_ms / K,
                            "speedup_of_value": value / plain_value, "what": "FP32 Jacobi SVD, no refinement, no FP64"},
