@@ -834,6 +834,8 @@ int set_tc_attrs() {
 	HA_CUDA(cudaFuncSetAttribute(k_tc_gemm<kTcPhaseXcov>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemLarge));
 	HA_CUDA(cudaFuncSetAttribute(k_tc_gemm<kTcPhaseGram>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemLarge));
 	HA_CUDA(cudaFuncSetAttribute(k_tc_gemm<kTcPhaseUpdate>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemLarge));
+	HA_CUDA(cudaFuncSetAttribute(k_tc_gemm<kTcPhaseGram, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemLarge));
+	HA_CUDA(cudaFuncSetAttribute(k_tc_gemm<kTcPhaseUpdate, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemLarge));
 	HA_CUDA(cudaFuncSetAttribute(k_tc_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemLarge));
 	done = true;
 	return kHaSuccess;
@@ -930,6 +932,26 @@ int build_tc(HaB200Plan *P) {
 	return kHaSuccess;
 }
 
+// The iteration's Gram and update products fill their stages with bulk copies from a producer
+// thread (default), or with the per-thread loads of the cross-covariance (HA_B200_TC_BULK=0).
+bool tc_bulk() {
+	static int v = -1;
+	if (v < 0) {
+		const char *e = getenv("HA_B200_TC_BULK");
+		v = (e && e[0] == '0') ? 0 : 1;
+	}
+	return v == 1;
+}
+
+// One launch of the tile product of PHASE over `ntiles` tiles.
+template <int PHASE>
+void launch_tc_tiles(int ntiles, const TcArgs &a, cudaStream_t st) {
+	if (PHASE != kTcPhaseXcov && tc_bulk())
+		k_tc_gemm<PHASE, PHASE != kTcPhaseXcov><<<ntiles, kTcThreads, a.smem_bytes, st>>>(a);
+	else
+		k_tc_gemm<PHASE><<<ntiles, kTcThreads, a.smem_bytes, st>>>(a);
+}
+
 // Launch one phase of the tile product over the size classes of a chunk (only class `only` when
 // it is 0 or 1), each with its layout's shared memory.
 template <int PHASE>
@@ -940,7 +962,7 @@ int launch_tc(const Chunk &ch, TcArgs a, cudaStream_t st, int kind, const int *s
 		a.tiles = ch.d_tct[c];
 		a.smem_bytes = smem[c];
 		HA_LAUNCH(kind, st);
-		k_tc_gemm<PHASE><<<ntiles, kTcThreads, a.smem_bytes, st>>>(a);
+		launch_tc_tiles<PHASE>(ntiles, a, st);
 	}
 	HA_CUDA(cudaGetLastError());
 	return kHaSuccess;
@@ -3113,7 +3135,7 @@ int ha_b200_tc_selftest(int32_t which, int32_t n, int32_t nt, const float *h_a, 
 			if (which == 0) {
 				a.c1 = 0.f;
 				a.c3 = 1.f;  // P = X^T X
-				{ HA_LAUNCH(kHaB200KTcNs, st); k_tc_gemm<kTcPhaseGram><<<grid, kTcThreads, a.smem_bytes, st>>>(a); }
+				{ HA_LAUNCH(kHaB200KTcNs, st); launch_tc_tiles<kTcPhaseGram>(grid, a, st); }
 				k_tc_unpack<<<64, kBlock, 0, st>>>(Pp.p, n, np, T.p);
 			} else {
 				if (cudaMemcpy(in1.p, h_b, (size_t)n * n * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
@@ -3123,7 +3145,7 @@ int ha_b200_tc_selftest(int32_t which, int32_t n, int32_t nt, const float *h_a, 
 				k_tc_pack<<<64, kBlock, 0, st>>>(in1.p, n, np, Pp.p);
 				a.plain = 1;
 				a.tol_stop = 1e30f;  // residual 0 < tol: the update is final and writes T = X P
-				{ HA_LAUNCH(kHaB200KTcNs, st); k_tc_gemm<kTcPhaseUpdate><<<grid, kTcThreads, a.smem_bytes, st>>>(a); }
+				{ HA_LAUNCH(kHaB200KTcNs, st); launch_tc_tiles<kTcPhaseUpdate>(grid, a, st); }
 			}
 			if (cudaGetLastError() != cudaSuccess ||
 			    cudaMemcpy(h_out, T.p, (size_t)n * n * 4, cudaMemcpyDeviceToHost) != cudaSuccess) {

@@ -160,6 +160,21 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
 	return true;
 }
 
+// One arrival on `bar` that also expects `bytes` of bulk copies to land before its phase ends.
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+	             : "memory");
+}
+
+// Bulk copy of `bytes` (a multiple of 16; both addresses 16-byte aligned) from global memory into
+// this CTA's shared memory; its completion counts against the transaction bytes of `bar`.  A plain
+// copy into the CTA's own shared memory: no multicast.
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint64_t *bar) {
+	asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+	             "l"(src), "r"(bytes), "r"(smem_u32(bar))
+	             : "memory");
+}
+
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, uint32_t src_bytes) {
 	asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
 }
@@ -366,21 +381,31 @@ __device__ __forceinline__ void tc_load_slice(const TcLoadPlan &lp, const __nv_b
 
 // The products of one K-slice staged at shared address `st` into the accumulator at `tmem`
 // (columns 0..255 and, for N > 256, 256..N-1), smallest first.  Issued by one thread.
-template <int PHASE>
+// Stage layouts: the per-thread loads put core matrix (g, k) (g along M or N, k the K half) at
+// (2 g + k) * 128 in every operand (LBO 128 between the K halves, SBO 256 between 8-row groups).
+// The bulk-copy pipeline (BULK) keeps that layout for the update's K-major A, whose K halves are
+// adjacent in memory, and puts the MN-major operands (the Gram's A, every B) K half by K half:
+// core (g, k) at (k G + g) * 128 with G the operand's 8-row groups (16 for A, N / 8 for B), so each
+// K half of a plane is one contiguous copy (LBO G * 128, SBO 128).
+template <int PHASE, bool BULK = false>
 __device__ __forceinline__ void tc_issue_products(uint32_t tmem, uint32_t st, int N, uint32_t id0, uint32_t id1,
                                                   bool first) {
 	constexpr int NPL = TcFmt<PHASE>::planes;
 	constexpr int NQ = NPL == 3 ? 6 : 3;
+	const uint32_t a_lbo = (BULK && PHASE == kTcPhaseGram) ? 2048u : 128u;
+	const uint32_t a_sbo = (BULK && PHASE == kTcPhaseGram) ? 128u : 256u;
+	const uint32_t b_lbo = BULK ? 16u * N : 128u, b_sbo = BULK ? 128u : 256u;
+	const uint32_t b_half = BULK ? 32u * 128u : 32u * 256u;  // 32 8-row groups: the second MMA's B
 #pragma unroll
 	for (int q = 0; q < NQ; q++) {
 		// three planes: lo*hi, hi*lo, mid*mid, mid*hi, hi*mid, hi*hi; two: mid*hi, hi*mid, hi*hi
 		const int pa = NPL == 3 ? ((q == 0) ? 2 : (q == 2 || q == 3) ? 1 : 0) : (q == 0 ? 1 : 0);
 		const int pb = NPL == 3 ? ((q == 1) ? 2 : (q == 2 || q == 4) ? 1 : 0) : (q == 1 ? 1 : 0);
 		const uint32_t acc = (!first || q > 0) ? 1u : 0u;
-		const uint64_t ad = smem_desc(st + pa * 4096, 128, 256);
+		const uint64_t ad = smem_desc(st + pa * 4096, a_lbo, a_sbo);
 		const uint32_t baddr = st + NPL * 4096 + pb * 32 * N;
-		mma_bf16(tmem, ad, smem_desc(baddr, 128, 256), id0, acc);
-		if (N > 256) mma_bf16(tmem + 256, ad, smem_desc(baddr + 32 * 256, 128, 256), id1, acc);
+		mma_bf16(tmem, ad, smem_desc(baddr, b_lbo, b_sbo), id0, acc);
+		if (N > 256) mma_bf16(tmem + 256, ad, smem_desc(baddr + b_half, b_lbo, b_sbo), id1, acc);
 	}
 }
 
@@ -390,10 +415,14 @@ __device__ __forceinline__ void tc_issue_products(uint32_t tmem, uint32_t st, in
 // PHASE kTcPhaseXcov:   A32 = X_sl^T Y_sl                       (K = time, padded to 16)
 // PHASE kTcPhaseGram:   P = c1 I + c3 X^T X, residual partials   (skips searchlights already done)
 // PHASE kTcPhaseUpdate: X <- X P, or T = X P for the final update (decided from the residual)
-template <int PHASE>
+// BULK (Gram and update only): warp-specialised stages filled by bulk copies instead of the
+// per-thread loads (see the main loop).
+template <int PHASE, bool BULK = false>
 __global__ void __launch_bounds__(kTcThreads) k_tc_gemm(const TcArgs a) {
+	static_assert(!(BULK && PHASE == kTcPhaseXcov), "the gathered cross-covariance has no bulk form");
 	extern __shared__ __align__(128) unsigned char tc_smem[];
-	__shared__ uint64_t s_bar[kTcMaxStages];
+	__shared__ uint64_t s_bar[kTcMaxStages];   // stage consumed: the stage's products completed
+	__shared__ uint64_t s_full[kTcMaxStages];  // stage filled (bulk form): its copies landed
 	__shared__ uint64_t s_acc;
 	__shared__ uint32_t s_tmem;
 	__shared__ int s_fail;
@@ -452,14 +481,26 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_gemm(const TcArgs a) {
 	const uint32_t ncols = tc_tmem_cols(N);
 	const uint32_t smem0 = smem_u32(tc_smem);
 
+	// bulk form: 8-row groups of the A tile inside the searchlight (the rest of A stays zero)
+	const int gA = min(16, (np >> 3) - 16 * t);
 	if (tid == 0) {
-		for (int i = 0; i < kTcMaxStages; i++) mbar_init(&s_bar[i], 1);
+		for (int i = 0; i < kTcMaxStages; i++) {
+			mbar_init(&s_bar[i], 1);
+			mbar_init(&s_full[i], 1);
+		}
 		mbar_init(&s_acc, 1);
 		s_fail = (S < 2) ? 1 : 0;
 		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 	}
 	if (PHASE == kTcPhaseXcov)
 		for (int i = tid; i < n; i += kTcThreads) s_sl[i] = a.sl_idx[w.sofs + i];
+	if (BULK && gA < 16 && S <= kTcMaxStages) {
+		// the copies fill only the A rows inside the searchlight: zero every stage's A planes once
+		for (int st = 0; st < S; st++)
+			for (int e = tid; e < NPL * 4096 / 16; e += kTcThreads)
+				reinterpret_cast<uint4 *>(tc_smem + st * stage_bytes)[e] = make_uint4(0u, 0u, 0u, 0u);
+		fence_proxy_async_smem();
+	}
 	if (warp == 0) tmem_alloc(&s_tmem, ncols);
 	tc_fence_before();
 	__syncthreads();
@@ -486,7 +527,61 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_gemm(const TcArgs a) {
 	const uint32_t id0 = mma_idesc(128, N0, a_mn, b_mn, f16);
 	const uint32_t id1 = N > 256 ? mma_idesc(128, N - 256, a_mn, b_mn, f16) : 0u;
 
-	if (!failed) {
+	if (BULK && !failed) {
+		// Thread 0 fills stage ks % S with bulk copies (their bytes complete the stage's full barrier)
+		// once the products of slice ks - S have released it; thread 32 issues each slice's products
+		// as soon as its stage is full and commits them to the stage's consumed barrier.  Per slice
+		// and plane: the Gram's A as two K halves of gA cores (contiguous along M), the update's A as
+		// gA pairs of K-adjacent cores, B as two K halves of N / 8 cores.
+		volatile int *vfail = &s_fail;
+		const int64_t pe = (int64_t)np * np;
+		const int npg = np >> 3, g0 = n0 >> 3;
+		const uint32_t tx = 2u * (256u * (uint32_t)gA + 32u * (uint32_t)N);
+		if (tid == 0) {
+			int issued = 0;
+			for (int ks = 0; ks < nk && !*vfail; ks++) {
+				const int s = ks % S;
+				if (ks >= S && !mbar_wait(&s_bar[s], (uint32_t)((ks / S - 1) & 1))) {
+					*vfail = 1;
+					break;
+				}
+				const uint32_t st = smem0 + s * stage_bytes;
+				mbar_expect_tx(&s_full[s], tx);
+#pragma unroll
+				for (int p = 0; p < 2; p++) {
+					const __nv_bfloat16 *Ap = srcA + p * pe;
+					const __nv_bfloat16 *Bp = srcB + p * pe;
+					const uint32_t sa = st + p * 4096, sb = st + 2 * 4096 + p * 32 * N;
+					if (PHASE == kTcPhaseGram) {
+						for (int k = 0; k < 2; k++)
+							bulk_g2s(sa + k * 2048, Ap + ((int64_t)(2 * ks + k) * npg + 16 * t) * 64, 128u * gA, &s_full[s]);
+					} else {
+						for (int g = 0; g < gA; g++)
+							bulk_g2s(sa + g * 256, Ap + ((int64_t)(16 * t + g) * npg + 2 * ks) * 64, 256u, &s_full[s]);
+					}
+					for (int k = 0; k < 2; k++)
+						bulk_g2s(sb + k * 16 * N, Bp + ((int64_t)(2 * ks + k) * npg + g0) * 64, 16u * N, &s_full[s]);
+				}
+				issued = ks + 1;
+			}
+			// the copies still in flight must land before the CTA may leave
+			for (int ks = issued > S ? issued - S : 0; ks < issued; ks++)
+				if (!mbar_wait(&s_full[ks % S], (uint32_t)((ks / S) & 1))) *vfail = 1;
+		} else if (tid == 32) {
+			for (int ks = 0; ks < nk; ks++) {
+				const int s = ks % S;
+				if (!mbar_wait(&s_full[s], (uint32_t)((ks / S) & 1))) {
+					*vfail = 1;
+					break;
+				}
+				tc_fence_after();
+				tc_issue_products<PHASE, true>(tmem, smem0 + s * stage_bytes, N, id0, id1, ks == 0);
+				mma_commit(&s_bar[s]);
+			}
+			mma_commit(&s_acc);  // tracks every product issued, also after a failed wait
+		}
+	}
+	if (!BULK && !failed) {
 		for (int j = 0; j < S - 1; j++) {
 			if (j < nk) load(j, j);
 			cp_async_commit();
@@ -515,7 +610,7 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_gemm(const TcArgs a) {
 	}
 	cp_async_wait_all();
 	if (!failed) {
-		if (tid == 0) mma_commit(&s_acc);
+		if (!BULK && tid == 0) mma_commit(&s_acc);
 		if (!mbar_wait(&s_acc, 0)) s_fail = 1;
 	}
 	__syncthreads();
