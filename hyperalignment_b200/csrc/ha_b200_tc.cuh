@@ -528,7 +528,7 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_gemm(const TcArgs a) {
 	const uint32_t id1 = N > 256 ? mma_idesc(128, N - 256, a_mn, b_mn, f16) : 0u;
 
 	if (BULK && !failed) {
-		// Thread 0 fills stage ks % S with bulk copies (their bytes complete the stage's full barrier)
+		// Warp 0 fills stage ks % S with bulk copies (their bytes complete the stage's full barrier)
 		// once the products of slice ks - S have released it; thread 32 issues each slice's products
 		// as soon as its stage is full and commits them to the stage's consumed barrier.  Per slice
 		// and plane: the Gram's A as two K halves of gA cores (contiguous along M), the update's A as
@@ -537,36 +537,44 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_gemm(const TcArgs a) {
 		const int64_t pe = (int64_t)np * np;
 		const int npg = np >> 3, g0 = n0 >> 3;
 		const uint32_t tx = 2u * (256u * (uint32_t)gA + 32u * (uint32_t)N);
-		if (tid == 0) {
+		if (warp == 0) {
+			// the producer warp: lane 0 waits for the stage and sets the expected bytes, then every
+			// lane issues its share of the copies (one A part each; lanes 0-3 also the B parts)
 			int issued = 0;
-			for (int ks = 0; ks < nk && !*vfail; ks++) {
+			for (int ks = 0; ks < nk; ks++) {
 				const int s = ks % S;
-				if (ks >= S && !mbar_wait(&s_bar[s], (uint32_t)((ks / S - 1) & 1))) {
-					*vfail = 1;
-					break;
-				}
-				const uint32_t st = smem0 + s * stage_bytes;
-				mbar_expect_tx(&s_full[s], tx);
-#pragma unroll
-				for (int p = 0; p < 2; p++) {
-					const __nv_bfloat16 *Ap = srcA + p * pe;
-					const __nv_bfloat16 *Bp = srcB + p * pe;
-					const uint32_t sa = st + p * 4096, sb = st + 2 * 4096 + p * 32 * N;
-					if (PHASE == kTcPhaseGram) {
-						for (int k = 0; k < 2; k++)
-							bulk_g2s(sa + k * 2048, Ap + ((int64_t)(2 * ks + k) * npg + 16 * t) * 64, 128u * gA, &s_full[s]);
-					} else {
-						for (int g = 0; g < gA; g++)
-							bulk_g2s(sa + g * 256, Ap + ((int64_t)(16 * t + g) * npg + 2 * ks) * 64, 256u, &s_full[s]);
+				int ok = 1;
+				if (lane == 0) {
+					ok = !*vfail;
+					if (ok && ks >= S && !mbar_wait(&s_bar[s], (uint32_t)((ks / S - 1) & 1))) {
+						*vfail = 1;
+						ok = 0;
 					}
-					for (int k = 0; k < 2; k++)
-						bulk_g2s(sb + k * 16 * N, Bp + ((int64_t)(2 * ks + k) * npg + g0) * 64, 16u * N, &s_full[s]);
+					if (ok) mbar_expect_tx(&s_full[s], tx);
+				}
+				if (!__shfl_sync(0xffffffffu, ok, 0)) break;
+				const uint32_t st = smem0 + s * stage_bytes;
+				const int p = lane >> 4, q = lane & 15;  // A part: plane p, core group q (update) or K half q (Gram)
+				const __nv_bfloat16 *Ap = srcA + p * pe;
+				const uint32_t sa = st + p * 4096;
+				if (PHASE == kTcPhaseGram) {
+					if (q < 2)
+						bulk_g2s(sa + q * 2048, Ap + ((int64_t)(2 * ks + q) * npg + 16 * t) * 64, 128u * gA, &s_full[s]);
+				} else if (q < gA) {
+					bulk_g2s(sa + q * 256, Ap + ((int64_t)(16 * t + q) * npg + 2 * ks) * 64, 256u, &s_full[s]);
+				}
+				if (lane < 4) {  // B part: plane lane >> 1, K half lane & 1
+					const int pb = lane >> 1, k = lane & 1;
+					bulk_g2s(st + 2 * 4096 + pb * 32 * N + k * 16 * N,
+					         srcB + pb * pe + ((int64_t)(2 * ks + k) * npg + g0) * 64, 16u * N, &s_full[s]);
 				}
 				issued = ks + 1;
 			}
 			// the copies still in flight must land before the CTA may leave
-			for (int ks = issued > S ? issued - S : 0; ks < issued; ks++)
-				if (!mbar_wait(&s_full[ks % S], (uint32_t)((ks / S) & 1))) *vfail = 1;
+			if (lane == 0)
+				for (int ks = issued > S ? issued - S : 0; ks < issued; ks++)
+					if (!mbar_wait(&s_full[ks % S], (uint32_t)((ks / S) & 1))) *vfail = 1;
+			__syncwarp();
 		} else if (tid == 32) {
 			for (int ks = 0; ks < nk; ks++) {
 				const int s = ks % S;
