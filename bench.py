@@ -62,6 +62,8 @@ def parse_args():
     p.add_argument("--nt", type=int, default=400)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-extras", action="store_true",
+                   help="skip the config-4 (full-size grid search) and config-5 (learned proposal) sub-fields")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--workload", choices=["template", "rankdef", "grid", "learned", "shard", "forrest", "refgpu",
                                            "pca"],
@@ -790,6 +792,18 @@ def run_b200(args):
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                    "sample": "oracle/_ref/libhyperalignment.so not built"}
 
+    # configs 4 and 5 (the grid search at full size, the learned proposal), after the headline's
+    # timed steps; a failure there is reported in its field and does not lose the line
+    extras = {}
+    if not args.no_extras:
+        plan.close()
+        for key, fn in (("config4_ridge_grid_full", lambda: config4_grid_full(args, dev)),
+                        ("config5_learned", lambda: config5_learned(args))):
+            try:
+                extras[key] = fn()
+            except Exception as ex:  # noqa: BLE001
+                extras[key] = {"error": repr(ex)}
+
     if rank == 0:
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": args.warmup,
@@ -822,6 +836,7 @@ def run_b200(args):
             "gpu_launches": int(launches),
             "clocks": clocks,
             "wall_s_timed": wall,
+            **extras,
         }
         print(json.dumps(out))
     if ws > 1:
@@ -979,6 +994,94 @@ def grid_cpu_rate(w, sls, tr, te, seconds):
         pool.map(_oracle_grid_worker, jobs, chunksize=1)
         dt = time.perf_counter() - t0
     return m / dt, m, dt, cores
+
+
+def config4_grid_full(args, dev):
+    """Config 4 at full size, a sub-field of the default line: the ridge grid search (10 alphas x
+    4 PC counts, 5-fold blocked CV with 10-TR buffers) over all 40962 searchlights of 50-500
+    vertices, nt 500, AR(1) noise; one warm-up and one timed step (CUDA events, L2 flushed).  The
+    winners and cost grids of a sample of searchlights are checked against the oracle's
+    composition of ha_ensemble_ridge."""
+    import torch
+    from hyperalignment_b200 import hyperalignment_c as H
+    from hyperalignment_b200 import workloads as W
+    from hyperalignment_b200.plan import Plan
+    from oracle import ha_oracle as O
+    w = W.ridge_grid_pair(0, nv=40962, nt=500)
+    sls = w.sls
+    tr, te = H.ensemble_indices(w.nt, 1, 5, 10, 10, 0)
+    plan = Plan(w.nt, w.nv, sls.indices, sls.offsets, sls.dists, sls.radius)
+    dX = torch.from_numpy(np.asfortranarray(w.X).ravel(order="F")).to(dev)
+    dY = torch.from_numpy(np.asfortranarray(w.Y).ravel(order="F")).to(dev)
+    vals = torch.zeros(plan.nnz, dtype=torch.float64, device=dev)
+    best = torch.zeros(sls.count, dtype=torch.int32, device=dev)
+    grid = len(W.GRID_ALPHAS) * len(W.GRID_NPCS)
+    cost = torch.zeros(sls.count * grid, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        vals.zero_()
+        plan.ridge_grid_device(dX.data_ptr(), dY.data_ptr(), vals.data_ptr(), best.data_ptr(), W.GRID_ALPHAS,
+                               W.GRID_NPCS, tr, te, d_cost=cost.data_ptr(), stream=stream.cuda_stream)
+
+    t0 = time.perf_counter()
+    step()  # warm-up: plan work lists, graph capture
+    torch.cuda.synchronize()
+    first_s = time.perf_counter() - t0
+    flush.zero_()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    step()
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b)
+    hb, hc = best.cpu().numpy(), cost.cpu().numpy().reshape(sls.count, grid)
+    rng = np.random.default_rng(4)
+    sample = np.sort(rng.choice(sls.count, 6, replace=False))
+    rel, same = [], 0
+    for q in sample:
+        sl = sls.indices[sls.offsets[q]:sls.offsets[q + 1]]
+        r = O.ensemble_ridge(w.X[:, sl], w.Y[:, sl], W.GRID_ALPHAS, W.GRID_NPCS, tr, te)
+        rc = np.asarray(r[6]).ravel()
+        rel.append(float(np.max(np.abs(hc[q] - rc) / np.abs(rc))))
+        same += int(hb[q] == int(np.argmin(rc)))
+    st = plan.stats()
+    plan.close()
+    sizes = sls.sizes
+    return {"value": sls.count / (ms / 1e3), "unit": UNIT, "ms_per_step": ms, "steps": 1, "warmup": 1,
+            "first_call_s": first_s,
+            "config": {"workload": "ridge_grid_full", "nv": w.nv, "nt": w.nt, "searchlights": sls.count,
+                       "sl_size_min": int(sizes.min()), "sl_size_max": int(sizes.max()),
+                       "alphas": "10 log-spaced in [1e-3, 1e3]", "npcs": [10, 20, 50, "all"],
+                       "cv": "ha_ensemble_indices(500, 1, 5, 10, 10, 0)", "noise": "AR(1) rho 0.5",
+                       "dtype": "f64", "l2": "flushed before the timed step"},
+            "error_vs_oracle": {"cost_grid_max_rel": max(rel), "winners_identical": f"{same} of {len(sample)}",
+                                "sample": [int(q) for q in sample]},
+            "winners_distinct": int(np.unique(hb).size), "solver_stats": st}
+
+
+def config5_learned(args):
+    """Config 5, a sub-field of the default line: the learned (alpha, PC count) proposal on the
+    40962-vertex grid workload.  The perceptron is trained on the GPU on the full grid's winners for
+    four training subjects (every 16th searchlight each), then the held-out subject (every 4th
+    searchlight, 10240) runs through the full grid and through the learned form (proposal where its
+    probability is at least 0.6, the full grid elsewhere); warm runs are timed.  The generator's noise
+    amplitude varies from 0.2 to 6 over the sphere so that the best grid point varies between
+    searchlights (with homogeneous noise one grid point wins almost everywhere)."""
+    from hyperalignment_b200 import learned as LR
+    res = LR.study(nv=40962, step=4, train_step=16, size_lo=50, size_hi=500, epochs=60, log=lambda *a: None)
+    g, l = res["grid"], res["learned"]
+    return {"value": l["searchlights_per_s"], "unit": UNIT, "ms_per_step": l["ms"],
+            "full_grid": {"value": g["searchlights_per_s"], "ms_per_step": g["ms"], "heldout_corr": g["heldout_corr"]},
+            "speedup_over_full_grid": l["searchlights_per_s"] / g["searchlights_per_s"],
+            "heldout_corr": l["heldout_corr"], "heldout_corr_minus_grid": l["heldout_corr"] - g["heldout_corr"],
+            "fallback_searchlights": l["fallback"], "proposal_matches_grid": l["proposal_matches_grid"],
+            "fixed_point": res["fixed_point"], "train": res["train"],
+            "config": {"workload": "ridge_grid_learned", "nv": 40962, "nt": 500, "fit_rows": 400, "eval_rows": 100,
+                       "heldout_searchlights": res["searchlights"], "train_subset": "every 16th, seeds 1-4",
+                       "heldout_subset": "every 4th, seed 5", "sizes": "50-500",
+                       "noise": "AR(1) rho 0.5, amplitude 0.2 to 6 over the sphere", "min_prob": 0.6}}
 
 
 def run_grid(args):

@@ -137,15 +137,17 @@ def heldout_correlation(sub, vals):
 
 
 def study(train_seeds=(1, 2, 3, 4), test_seed=5, nv=10242, step=4, size_lo=50, size_hi=500, epochs=40,
-          min_prob=0.6, log=print):
-    """The learned-proposal study: labels from the full grid on the training subjects, training on
-    the GPU, then the held-out subject through both the full grid and the learned form."""
+          min_prob=0.6, log=print, train_step=None):
+    """The learned-proposal study: labels from the full grid on the training subjects (every
+    train_step-th searchlight, default step), training on the GPU, then the held-out subject (every
+    step-th searchlight) through both the full grid and the learned form."""
+    train_step = step if train_step is None else train_step
     import torch
     C = len(W.GRID_ALPHAS) * len(W.GRID_NPCS)
     feats, labels = [], []
     t0 = time.time()
     for sd in train_seeds:
-        sub = make_subject(sd, nv, step=step, size_lo=size_lo, size_hi=size_hi)
+        sub = make_subject(sd, nv, step=train_step, size_lo=size_lo, size_hi=size_hi)
         _, best, ms = grid_labels(sub)
         feats.append(features(sub))
         labels.append(best)
