@@ -932,21 +932,24 @@ int build_tc(HaB200Plan *P) {
 	return kHaSuccess;
 }
 
-// The iteration's Gram and update products fill their stages with bulk copies from a producer
-// thread (default), or with the per-thread loads of the cross-covariance (HA_B200_TC_BULK=0).
-bool tc_bulk() {
+// Which of the iteration's products fill their stages with bulk copies from a producer warp
+// rather than with per-thread loads: bit 0 the Gram, bit 1 the update (HA_B200_TC_BULK, default
+// 1).  On the full template hemisphere the bulk Gram takes 1.32 ms a launch against 1.37, while the
+// bulk update takes 1.80 against 1.37: its K-major A tile arrives as 16 strided 256-byte pieces
+// per plane, which the copy engine streams from DRAM more slowly than 128 threads' loads.
+int tc_bulk_mask() {
 	static int v = -1;
 	if (v < 0) {
 		const char *e = getenv("HA_B200_TC_BULK");
-		v = (e && e[0] == '0') ? 0 : 1;
+		v = e ? (atoi(e) & 3) : 1;
 	}
-	return v == 1;
+	return v;
 }
 
 // One launch of the tile product of PHASE over `ntiles` tiles.
 template <int PHASE>
 void launch_tc_tiles(int ntiles, const TcArgs &a, cudaStream_t st) {
-	if (PHASE != kTcPhaseXcov && tc_bulk())
+	if (PHASE != kTcPhaseXcov && (tc_bulk_mask() >> (PHASE - 1) & 1))
 		k_tc_gemm<PHASE, PHASE != kTcPhaseXcov><<<ntiles, kTcThreads, a.smem_bytes, st>>>(a);
 	else
 		k_tc_gemm<PHASE><<<ntiles, kTcThreads, a.smem_bytes, st>>>(a);
