@@ -227,3 +227,44 @@ def test_tc_graph_replay_matches_direct_launches(gpu, hlib):
     finally:
         hlib.ha_b200_set_graphs(True)
     assert captured == direct and replayed == direct
+
+
+_PIPELINE_SCRIPT = r"""
+import sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+from hyperalignment_b200 import _lib as L
+lib = L.lib()
+assert lib.ha_b200_init() == 0
+out = {}
+for n in (16, 100, 200, 272, 512):
+    rng = np.random.default_rng(n)
+    X = (rng.standard_normal((n, n)) / np.sqrt(n)).astype(np.float32)
+    M = (rng.standard_normal((n, n)) / np.sqrt(n)).astype(np.float32)
+    for which, b in ((0, None), (1, M)):
+        o = np.zeros((n, n), dtype=np.float32)
+        fp = L.c_float_p
+        rc = lib.ha_b200_tc_selftest(which, n, 0, X.ctypes.data_as(fp), None if b is None else b.ctypes.data_as(fp),
+                                     o.ctypes.data_as(fp))
+        assert rc == 0
+        out[f"{which}_{n}"] = o
+np.savez(sys.argv[2], **out)
+"""
+
+
+def test_bulk_and_thread_pipelines_bitwise_equal(gpu, tmp_path):
+    """The iteration's products staged by bulk copies (HA_B200_TC_BULK bits) and by per-thread loads
+    feed the same MMAs with the same bytes, so every setting gives identical bits."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    res = {}
+    for mask in ("0", "1", "3"):
+        path = tmp_path / f"m{mask}.npz"
+        env = dict(os.environ, HA_B200_TC_BULK=mask)
+        subprocess.run([sys.executable, "-c", _PIPELINE_SCRIPT, root, str(path)], env=env, check=True, timeout=300)
+        res[mask] = np.load(path)
+    for k in res["0"].files:
+        assert res["1"][k].tobytes() == res["0"][k].tobytes(), k
+        assert res["3"][k].tobytes() == res["0"][k].tobytes(), k
