@@ -175,6 +175,18 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t
 	             : "memory");
 }
 
+// The same bounded wait for threads with nothing else to do meanwhile: a short sleep between
+// polls leaves the issue slots to the warps that produce and consume the stages.
+__device__ __forceinline__ bool mbar_wait_idle(uint64_t *bar, uint32_t parity) {
+	if (mbar_try_wait(bar, parity)) return true;
+	const uint64_t t0 = global_ns();
+	while (!mbar_try_wait(bar, parity)) {
+		__nanosleep(64);
+		if (global_ns() - t0 > kTcWaitNs) return false;
+	}
+	return true;
+}
+
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, uint32_t src_bytes) {
 	asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
 }
@@ -575,18 +587,25 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_gemm(const TcArgs a) {
 				for (int ks = issued > S ? issued - S : 0; ks < issued; ks++)
 					if (!mbar_wait(&s_full[ks % S], (uint32_t)((ks / S) & 1))) *vfail = 1;
 			__syncwarp();
-		} else if (tid == 32) {
+		} else if (warp == 1) {
+			// lane 0 issues; the other lanes wait at the warp barrier instead of polling beside it
 			for (int ks = 0; ks < nk; ks++) {
-				const int s = ks % S;
-				if (!mbar_wait(&s_full[s], (uint32_t)((ks / S) & 1))) {
-					*vfail = 1;
-					break;
+				int ok = 1;
+				if (lane == 0) {
+					const int s = ks % S;
+					if (mbar_wait(&s_full[s], (uint32_t)((ks / S) & 1))) {
+						tc_fence_after();
+						tc_issue_products<PHASE, true>(tmem, smem0 + s * stage_bytes, N, id0, id1, ks == 0);
+						mma_commit(&s_bar[s]);
+					} else {
+						*vfail = 1;
+						ok = 0;
+					}
 				}
-				tc_fence_after();
-				tc_issue_products<PHASE, true>(tmem, smem0 + s * stage_bytes, N, id0, id1, ks == 0);
-				mma_commit(&s_bar[s]);
+				if (!__shfl_sync(0xffffffffu, ok, 0)) break;
 			}
-			mma_commit(&s_acc);  // tracks every product issued, also after a failed wait
+			if (lane == 0) mma_commit(&s_acc);  // tracks every product issued, also after a failed wait
+			__syncwarp();
 		}
 	}
 	if (!BULK && !failed) {
@@ -619,7 +638,7 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_gemm(const TcArgs a) {
 	cp_async_wait_all();
 	if (!failed) {
 		if (!BULK && tid == 0) mma_commit(&s_acc);
-		if (!mbar_wait(&s_acc, 0)) s_fail = 1;
+		if (!(BULK ? mbar_wait_idle(&s_acc, 0) : mbar_wait(&s_acc, 0))) s_fail = 1;
 	}
 	__syncthreads();
 	failed = failed || s_fail;
