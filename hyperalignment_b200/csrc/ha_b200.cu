@@ -835,6 +835,8 @@ int set_tc_attrs() {
 	HA_CUDA(cudaFuncSetAttribute(k_tc_gemm<kTcPhaseGram>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemLarge));
 	HA_CUDA(cudaFuncSetAttribute(k_tc_gemm<kTcPhaseUpdate>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemLarge));
 	HA_CUDA(cudaFuncSetAttribute(k_tc_gemm<kTcPhaseGram, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemLarge));
+	HA_CUDA(cudaFuncSetAttribute(k_tc_iter<kTcPhaseGram>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemLarge));
+	HA_CUDA(cudaFuncSetAttribute(k_tc_iter<kTcPhaseUpdate>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemLarge));
 	HA_CUDA(cudaFuncSetAttribute(k_tc_gemm<kTcPhaseUpdate, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemLarge));
 	HA_CUDA(cudaFuncSetAttribute(k_tc_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemLarge));
 	done = true;
@@ -946,9 +948,28 @@ int tc_bulk_mask() {
 	return v;
 }
 
-// One launch of the tile product of PHASE over `ntiles` tiles.
+// The iteration's products by the persistent kernel (one CTA per SM walking the tiles, loads,
+// products and epilogues overlapped across tiles: HA_B200_TC_ITER=1) or by one CTA per tile.
+bool tc_iter_persist() {
+	static int v = -1;
+	if (v < 0) {
+		const char *e = getenv("HA_B200_TC_ITER");
+		v = (e && e[0] == '1') ? 1 : 0;
+	}
+	return v == 1;
+}
+
+// One launch of the tile product of PHASE over `ntiles` tiles of at most `nmax` columns.
 template <int PHASE>
-void launch_tc_tiles(int ntiles, const TcArgs &a, cudaStream_t st) {
+void launch_tc_tiles(int ntiles, TcArgs a, cudaStream_t st, int nmax) {
+	if constexpr (PHASE != kTcPhaseXcov) {
+		if (tc_iter_persist()) {
+			const int stage = 2 * 4096 + 64 * nmax;
+			a.smem_bytes = std::min(kTcMaxStages, kTcSmemLarge / stage) * stage;
+			k_tc_iter<PHASE><<<std::min(ntiles, g_num_sms), kTcIterThreads, a.smem_bytes, st>>>(a, ntiles, nmax);
+			return;
+		}
+	}
 	if (PHASE != kTcPhaseXcov && (tc_bulk_mask() >> (PHASE - 1) & 1))
 		k_tc_gemm<PHASE, PHASE != kTcPhaseXcov><<<ntiles, kTcThreads, a.smem_bytes, st>>>(a);
 	else
@@ -965,7 +986,7 @@ int launch_tc(const Chunk &ch, TcArgs a, cudaStream_t st, int kind, const int *s
 		a.tiles = ch.d_tct[c];
 		a.smem_bytes = smem[c];
 		HA_LAUNCH(kind, st);
-		launch_tc_tiles<PHASE>(ntiles, a, st);
+		launch_tc_tiles<PHASE>(ntiles, a, st, c ? 256 : 128);
 	}
 	HA_CUDA(cudaGetLastError());
 	return kHaSuccess;
@@ -3138,7 +3159,7 @@ int ha_b200_tc_selftest(int32_t which, int32_t n, int32_t nt, const float *h_a, 
 			if (which == 0) {
 				a.c1 = 0.f;
 				a.c3 = 1.f;  // P = X^T X
-				{ HA_LAUNCH(kHaB200KTcNs, st); launch_tc_tiles<kTcPhaseGram>(grid, a, st); }
+				{ HA_LAUNCH(kHaB200KTcNs, st); launch_tc_tiles<kTcPhaseGram>(grid, a, st, 256); }
 				k_tc_unpack<<<64, kBlock, 0, st>>>(Pp.p, n, np, T.p);
 			} else {
 				if (cudaMemcpy(in1.p, h_b, (size_t)n * n * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
@@ -3148,7 +3169,7 @@ int ha_b200_tc_selftest(int32_t which, int32_t n, int32_t nt, const float *h_a, 
 				k_tc_pack<<<64, kBlock, 0, st>>>(in1.p, n, np, Pp.p);
 				a.plain = 1;
 				a.tol_stop = 1e30f;  // residual 0 < tol: the update is final and writes T = X P
-				{ HA_LAUNCH(kHaB200KTcNs, st); launch_tc_tiles<kTcPhaseUpdate>(grid, a, st); }
+				{ HA_LAUNCH(kHaB200KTcNs, st); launch_tc_tiles<kTcPhaseUpdate>(grid, a, st, 256); }
 			}
 			if (cudaGetLastError() != cudaSuccess ||
 			    cudaMemcpy(h_out, T.p, (size_t)n * n * 4, cudaMemcpyDeviceToHost) != cudaSuccess) {

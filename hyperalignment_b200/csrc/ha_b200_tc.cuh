@@ -166,6 +166,16 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
 	             : "memory");
 }
 
+// `bytes` more bulk-copy bytes for the current phase of `bar`, without an arrival.
+__device__ __forceinline__ void mbar_add_tx(uint64_t *bar, uint32_t bytes) {
+	asm volatile("mbarrier.expect_tx.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+// One plain arrival on `bar`.
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+	asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 // Bulk copy of `bytes` (a multiple of 16; both addresses 16-byte aligned) from global memory into
 // this CTA's shared memory; its completion counts against the transaction bytes of `bar`.  A plain
 // copy into the CTA's own shared memory: no multicast.
@@ -399,15 +409,17 @@ __device__ __forceinline__ void tc_load_slice(const TcLoadPlan &lp, const __nv_b
 // adjacent in memory, and puts the MN-major operands (the Gram's A, every B) K half by K half:
 // core (g, k) at (k G + g) * 128 with G the operand's 8-row groups (16 for A, N / 8 for B), so each
 // K half of a plane is one contiguous copy (LBO G * 128, SBO 128).
-template <int PHASE, bool BULK = false>
+// A_KH / B_KH: the operand is staged K half by K half (else interleaved); by default the bulk form's
+// choice.  The persistent iteration kernel stages A interleaved (per-lane copies) and B by K halves.
+template <int PHASE, bool BULK = false, bool A_KH = BULK && PHASE == kTcPhaseGram, bool B_KH = BULK>
 __device__ __forceinline__ void tc_issue_products(uint32_t tmem, uint32_t st, int N, uint32_t id0, uint32_t id1,
                                                   bool first) {
 	constexpr int NPL = TcFmt<PHASE>::planes;
 	constexpr int NQ = NPL == 3 ? 6 : 3;
-	const uint32_t a_lbo = (BULK && PHASE == kTcPhaseGram) ? 2048u : 128u;
-	const uint32_t a_sbo = (BULK && PHASE == kTcPhaseGram) ? 128u : 256u;
-	const uint32_t b_lbo = BULK ? 16u * N : 128u, b_sbo = BULK ? 128u : 256u;
-	const uint32_t b_half = BULK ? 32u * 128u : 32u * 256u;  // 32 8-row groups: the second MMA's B
+	const uint32_t a_lbo = A_KH ? 2048u : 128u;
+	const uint32_t a_sbo = A_KH ? 128u : 256u;
+	const uint32_t b_lbo = B_KH ? 16u * N : 128u, b_sbo = B_KH ? 128u : 256u;
+	const uint32_t b_half = B_KH ? 32u * 128u : 32u * 256u;  // 32 8-row groups: the second MMA's B
 #pragma unroll
 	for (int q = 0; q < NQ; q++) {
 		// three planes: lo*hi, hi*lo, mid*mid, mid*hi, hi*mid, hi*hi; two: mid*hi, hi*mid, hi*hi
@@ -713,6 +725,286 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_gemm(const TcArgs a) {
 	tc_fence_before();
 	__syncthreads();
 	if (warp == 0) tmem_dealloc(tmem, ncols);
+}
+
+// ---------------------------------------------------------------------------------------------
+// persistent iteration kernel: one CTA per SM walks the tiles of a phase
+// ---------------------------------------------------------------------------------------------
+// Epilogue of one iteration tile read from the accumulator at tensor-memory column `col0`: warp
+// quarter q (warp % 4) owns rows 32 q .. 32 q + 31 of the tile.  Gram: P = c1 I + c3 G into the P
+// planes and the tile's residual partials; update: the next iterate into the other iterate buffer,
+// or T for the final update.  The accumulator holds 2^24 times the product.
+template <int PHASE>
+__device__ __forceinline__ void tc_iter_epilogue(const TcArgs &a, const TcWork &w, int t, int n0, int N,
+                                                 uint32_t tmem, uint32_t col0, int q, int lane, bool final_update,
+                                                 float c1, float c3) {
+	const int n = w.n, np = w.np, npg = np >> 3;
+	const int row = 128 * t + 32 * q + lane;
+	const uint32_t trow = tmem + ((uint32_t)(32 * q) << 16) + col0;
+	const int64_t pe = (int64_t)np * np;
+	float res = 0.f;
+	for (int c0 = 0; c0 < N; c0 += 16) {
+		float v[16];
+		tmem_ld16(trow + (uint32_t)c0, v);
+		if (row >= np) continue;
+#pragma unroll
+		for (int k = 0; k < 16; k++) v[k] *= kTcAccUnscale;
+		if (PHASE == kTcPhaseGram) {
+#pragma unroll
+			for (int k = 0; k < 16; k++) {
+				const int col = n0 + c0 + k;
+				const float g = v[k];
+				if (row < n && col < n) {
+					const float d = g - (col == row ? 1.f : 0.f);
+					res += d * d;
+				}
+				v[k] = c3 * g + (col == row ? c1 : 0.f);
+			}
+			__nv_bfloat16 *P0 = a.Pp + w.pofs;
+#pragma unroll
+			for (int h = 0; h < 2; h++) {
+				const int64_t o = ((int64_t)(row >> 3) * npg + ((n0 + c0) >> 3) + h) * 64 + (row & 7) * 8;
+				store_split8h(v + 8 * h, P0 + o, P0 + pe + o);
+			}
+		} else if (final_update) {
+			if (row < n) {
+				float *T = a.T + w.tofs;
+				for (int k = 0; k < 16; k++) {
+					const int col = n0 + c0 + k;
+					if (col < n) T[a.t_rowmajor ? (int64_t)row * n + col : (int64_t)col * n + row] = v[k];
+				}
+			}
+		} else {
+			__nv_bfloat16 *X0 = a.Xw + w.xofs;
+#pragma unroll
+			for (int h = 0; h < 2; h++) {
+				const int64_t o = ((int64_t)(row >> 3) * npg + ((n0 + c0) >> 3) + h) * 64 + (row & 7) * 8;
+				store_split8h(v + 8 * h, X0 + o, X0 + pe + o);
+			}
+		}
+	}
+	if (PHASE == kTcPhaseGram) {
+		res = warp_sum(res);
+		if (lane == 0) a.res_part[(int64_t)w.slot * kTcResSlots + (2 * t + (n0 > 0 ? 1 : 0)) * 4 + q] = res;
+	}
+}
+
+// The update's decision for one searchlight from the residual partials of this iteration's Gram
+// (fixed-order sum, the same in every thread) and the state it read: final update or not; the
+// state for the next iteration goes to *out.
+__device__ __forceinline__ bool tc_update_decision(const TcArgs &a, const TcWork &w, const TcState &st, TcState *out) {
+	double ss = 0.0;
+	for (int i = 0; i < kTcResSlots; i++) ss += (double)a.res_part[(int64_t)w.slot * kTcResSlots + i];
+	const double resd = sqrt(ss / (double)w.n);
+	const float res = (float)resd;
+	const bool conv = a.plain && res < a.tol_stop;
+	// a residual that a plain step leaves unchanged to 5e-7 relative: singular values below the FP32
+	// resolution of A (see k_tc_gemm)
+	const bool stalled = !conv && a.plain && st.plain && fabs(resd - (double)st.res) <= 5e-7 * resd;
+	const bool fin = conv || stalled || a.last;
+	TcState o = st;
+	o.iters = st.iters + 1;
+	o.res = res;
+	o.conv = conv ? 1 : 0;
+	o.stalled = stalled ? 1 : 0;
+	o.done = fin ? 1 : 0;
+	o.plain = a.plain;
+	*out = o;
+	return fin;
+}
+
+constexpr int kTcIterThreads = 192;    // warp 0 producer, warp 1 MMA, warps 2-5 epilogue
+constexpr uint32_t kTcIterCols = 512;  // two accumulators of up to 256 columns
+
+// The Gram (PHASE 1) or update (PHASE 2) products of every tile of a launch, one CTA per SM walking
+// tiles blockIdx.x, blockIdx.x + gridDim.x, ...  Stages are filled continuously across tile
+// boundaries: warp 0 copies the A tile with per-lane cp.async (each lane signals a stage's full
+// barrier once its copies of that stage have landed, S - 1 stages behind its issue, after a proxy
+// fence) and the B operand with bulk copies (K half by K half, their bytes counted by the same
+// barrier); lane 0 of warp 1 issues each stage's three products into one of two tensor-memory
+// accumulators (tiles alternate) and commits the stage to its consumed barrier and the finished
+// tile to the accumulator's full barrier; warps 2-5 read the finished accumulator, write the
+// epilogue and release it, while the next tile's products run in the other accumulator.
+// Searchlights already done are skipped by every role alike.  nmax: the widest tile of the launch
+// (128 or 256), which sizes the B planes of a stage.  Every wait is bounded; a timeout sets the
+// error flag and every role ends.
+template <int PHASE>
+__global__ void __launch_bounds__(kTcIterThreads, 1) k_tc_iter(const TcArgs a, int ntiles, int nmax) {
+	static_assert(PHASE != kTcPhaseXcov, "the cross-covariance keeps the per-tile kernel");
+	extern __shared__ __align__(128) unsigned char tc_smem[];
+	__shared__ uint64_t s_full[kTcMaxStages], s_empty[kTcMaxStages], s_accf[2], s_acce[2], s_fin;
+	__shared__ uint32_t s_tmem;
+	__shared__ int s_fail;
+	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+	if (PHASE == kTcPhaseUpdate && a.Xw == nullptr) {
+		if (tid == 0) atomicOr(a.err, 1);
+		return;
+	}
+	const int stage_bytes = 2 * 4096 + 2 * 32 * nmax;
+	int S = a.smem_bytes / stage_bytes;
+	if (S > kTcMaxStages) S = kTcMaxStages;
+	const int L = S - 1;  // how far the per-lane A copies' arrivals trail their issue
+	const uint32_t smem0 = smem_u32(tc_smem);
+	if (tid == 0) {
+		for (int i = 0; i < kTcMaxStages; i++) {
+			mbar_init(&s_full[i], 32);
+			mbar_init(&s_empty[i], 1);
+		}
+		for (int b = 0; b < 2; b++) {
+			mbar_init(&s_accf[b], 1);
+			mbar_init(&s_acce[b], 4);
+		}
+		mbar_init(&s_fin, 1);
+		s_fail = (S < 2 || nmax > 256) ? 1 : 0;
+		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+	}
+	if (warp == 0) tmem_alloc(&s_tmem, kTcIterCols);
+	tc_fence_before();
+	__syncthreads();
+	tc_fence_after();
+	const uint32_t tmem = s_tmem;
+	volatile int *vfail = &s_fail;
+	const bool failed0 = *vfail != 0;
+
+	if (warp == 0 && !failed0) {
+		uint32_t g = 0;  // slices issued by this CTA
+		bool ok = true;
+		for (int i = blockIdx.x; i < ntiles && ok; i += gridDim.x) {
+			const TcTile tl = a.tiles[i];
+			const TcWork w = a.work[tl.w];
+			if (a.st_in[w.slot].done) continue;
+			const int np = w.np, npg = np >> 3, t = tl.t, N = tl.nn, g0 = tl.n0 >> 3, nk = np >> 4;
+			const int64_t pe = (int64_t)np * np;
+			const __nv_bfloat16 *As = a.Xp + w.xofs;
+			const __nv_bfloat16 *Bs = (PHASE == kTcPhaseGram) ? As : (const __nv_bfloat16 *)(a.Pp + w.pofs);
+			for (int ks = 0; ks < nk; ks++, g++) {
+				const int s = (int)(g % (uint32_t)S);
+				int go = 1;
+				if (lane == 0) {
+					if (g >= (uint32_t)S && !mbar_wait(&s_empty[s], (g / S - 1) & 1u)) {
+						*vfail = 1;
+						go = 0;
+					}
+					if (go) mbar_add_tx(&s_full[s], 64u * (uint32_t)N);  // B: two planes x two K halves x 16 N
+				}
+				if (!__shfl_sync(0xffffffffu, go, 0)) {
+					ok = false;
+					break;
+				}
+				const uint32_t st = smem0 + s * stage_bytes;
+				if (lane < 4) {  // B: plane lane >> 1, K half lane & 1
+					const int pb = lane >> 1, k = lane & 1;
+					bulk_g2s(st + 8192 + pb * 32 * nmax + k * 16 * N, Bs + pb * pe + ((int64_t)(2 * ks + k) * npg + g0) * 64,
+					         16u * N, &s_full[s]);
+				}
+				// A: 256 chunks of 16 bytes per plane, chunk c = lane + 32 j: core (g, k) = (c >> 4, (c >> 3) & 1)
+#pragma unroll
+				for (int p = 0; p < 2; p++)
+#pragma unroll
+					for (int j = 0; j < 8; j++) {
+						const int c = lane + 32 * j, core = c >> 3, r = c & 7, gg = core >> 1, k = core & 1;
+						const bool valid = 16 * t + gg < npg;
+						const int64_t src = (PHASE == kTcPhaseGram) ? ((int64_t)(2 * ks + k) * npg + 16 * t + gg) * 64 + 8 * r
+						                                            : ((int64_t)(16 * t + gg) * npg + 2 * ks + k) * 64 + 8 * r;
+						cp_async16(st + p * 4096 + core * 128 + r * 16, valid ? As + p * pe + src : As, valid ? 16u : 0u);
+					}
+				cp_async_commit();
+				if (g >= (uint32_t)L) {  // this lane's copies of slice g - L have landed
+					cp_async_wait_keep(L);
+					fence_proxy_async_smem();
+					mbar_arrive(&s_full[(g - L) % S]);
+				}
+			}
+		}
+		// the arrivals still owed: slices max(0, g - L) .. g - 1
+		cp_async_wait_all();
+		fence_proxy_async_smem();
+		for (uint32_t h = g > (uint32_t)L ? g - L : 0u; h < g; h++) mbar_arrive(&s_full[h % S]);
+		// every bulk copy issued has landed before the CTA may leave
+		if (lane == 0)
+			for (uint32_t h = g > (uint32_t)S ? g - S : 0u; h < g; h++)
+				if (!mbar_wait(&s_full[h % S], (h / S) & 1u)) *vfail = 1;
+		__syncwarp();
+	}
+	if (warp == 1 && !failed0) {
+		// lane 0 issues; the other lanes wait at the warp barrier
+		uint32_t g = 0, j = 0;  // slices consumed, tiles computed
+		const int a_mn = (PHASE == kTcPhaseGram) ? 1 : 0;
+		for (int i = blockIdx.x; i < ntiles; i += gridDim.x) {
+			const TcTile tl = a.tiles[i];
+			const TcWork w = a.work[tl.w];
+			if (a.st_in[w.slot].done) continue;
+			const int nk = w.np >> 4, N = tl.nn, b = (int)(j & 1u);
+			int ok = 1;
+			if (lane == 0) {
+				// the accumulator's previous tile (j - 2) must have been read out
+				if (j >= 2 && !mbar_wait(&s_acce[b], ((j >> 1) - 1) & 1u)) ok = 0;
+				const uint32_t id = mma_idesc(128, N, a_mn, 1, true);
+				const uint32_t acc_t = tmem + (uint32_t)(256 * b);
+				tc_fence_after();
+				for (int ks = 0; ks < nk && ok; ks++, g++) {
+					const int s = (int)(g % (uint32_t)S);
+					if (!mbar_wait(&s_full[s], (g / S) & 1u)) {
+						ok = 0;
+						break;
+					}
+					tc_fence_after();
+					const uint32_t st = smem0 + s * stage_bytes;
+#pragma unroll
+					for (int q = 0; q < 3; q++) {  // mid*hi, hi*mid, hi*hi
+						const int pa = q == 0 ? 1 : 0, pb = q == 1 ? 1 : 0;
+						mma_bf16(acc_t, smem_desc(st + pa * 4096, 128, 256),
+						         smem_desc(st + 8192 + pb * 32 * nmax, 16u * N, 128), id, (ks > 0 || q > 0) ? 1u : 0u);
+					}
+					mma_commit(&s_empty[s]);
+				}
+				if (ok) mma_commit(&s_accf[b]);
+				else *vfail = 1;
+			}
+			if (!__shfl_sync(0xffffffffu, ok, 0)) break;
+			j++;
+		}
+		if (lane == 0) mma_commit(&s_fin);  // completes once every product issued has
+		__syncwarp();
+	}
+	if (warp >= 2 && !failed0) {
+		uint32_t j = 0;
+		for (int i = blockIdx.x; i < ntiles; i += gridDim.x) {
+			const TcTile tl = a.tiles[i];
+			const TcWork w = a.work[tl.w];
+			const TcState st = a.st_in[w.slot];
+			if (st.done) {
+				if (PHASE == kTcPhaseUpdate && tl.t == 0 && tl.n0 == 0 && tid == 64) a.st_out[w.slot] = st;
+				continue;
+			}
+			bool fin = false;
+			if (PHASE == kTcPhaseUpdate) {
+				TcState o;
+				fin = tc_update_decision(a, w, st, &o);
+				if (tl.t == 0 && tl.n0 == 0 && tid == 64) a.st_out[w.slot] = o;
+			}
+			const int b = (int)(j & 1u);
+			if (!mbar_wait_idle(&s_accf[b], (j >> 1) & 1u)) {
+				*vfail = 1;
+				break;
+			}
+			tc_fence_after();
+			tc_iter_epilogue<PHASE>(a, w, tl.t, tl.n0, tl.nn, tmem, (uint32_t)(256 * b), warp & 3, lane, fin, a.c1, a.c3);
+			tc_fence_before();
+			__syncwarp();
+			if (lane == 0) mbar_arrive(&s_acce[b]);
+			j++;
+		}
+	}
+	__syncthreads();
+	if (tid == 0) {
+		if (!failed0 && !mbar_wait(&s_fin, 0)) *vfail = 1;
+		if (*vfail) atomicOr(a.err, 1);
+	}
+	tc_fence_before();
+	__syncthreads();
+	tc_fence_after();
+	if (warp == 0) tmem_dealloc(tmem, kTcIterCols);
 }
 
 // ---------------------------------------------------------------------------------------------

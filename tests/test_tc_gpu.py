@@ -253,18 +253,20 @@ np.savez(sys.argv[2], **out)
 
 
 def test_bulk_and_thread_pipelines_bitwise_equal(gpu, tmp_path):
-    """The iteration's products staged by bulk copies (HA_B200_TC_BULK bits) and by per-thread loads
-    feed the same MMAs with the same bytes, so every setting gives identical bits."""
+    """The iteration's products staged by bulk copies (HA_B200_TC_BULK bits), by per-thread loads, or
+    by the persistent tile kernel (HA_B200_TC_ITER=1) feed the same MMAs with the same bytes, so
+    every setting gives identical bits."""
     import os
     import subprocess
     import sys
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     res = {}
-    for mask in ("0", "1", "3"):
+    for mask in ("0", "1", "3", "iter"):
         path = tmp_path / f"m{mask}.npz"
-        env = dict(os.environ, HA_B200_TC_BULK=mask)
+        env = dict(os.environ, HA_B200_TC_ITER="1") if mask == "iter" else dict(os.environ, HA_B200_TC_BULK=mask)
         subprocess.run([sys.executable, "-c", _PIPELINE_SCRIPT, root, str(path)], env=env, check=True, timeout=300)
         res[mask] = np.load(path)
     for k in res["0"].files:
         assert res["1"][k].tobytes() == res["0"][k].tobytes(), k
         assert res["3"][k].tobytes() == res["0"][k].tobytes(), k
+        assert res["iter"][k].tobytes() == res["0"][k].tobytes(), k
