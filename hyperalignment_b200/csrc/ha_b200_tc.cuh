@@ -287,6 +287,27 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 	for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
+// Warp-wide: 64 consecutive FP32 columns of this warp's 32 tensor-memory lanes, one load and one
+// wait (the wait is inside the same statement, so no use of the registers can precede it).
+__device__ __forceinline__ void tmem_ld64(uint32_t taddr, float (&v)[64]) {
+	uint32_t r[64];
+	asm volatile(
+	    "tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, %48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63}, [%64];\n\t"
+	    "tcgen05.wait::ld.sync.aligned;"
+	    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+	      "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+	      "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+	      "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]),
+	      "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]),
+	      "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]),
+	      "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]),
+	      "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+	    : "r"(taddr)
+	    : "memory");
+#pragma unroll
+	for (int i = 0; i < 64; i++) v[i] = __uint_as_float(r[i]);
+}
+
 // Exact three-way split of an FP32 value into BF16 parts: v = hi + mid + lo.
 __device__ __forceinline__ void split3(float v, __nv_bfloat16 &hi, __nv_bfloat16 &mid, __nv_bfloat16 &lo) {
 	hi = __float2bfloat16_rn(v);
@@ -743,43 +764,51 @@ __device__ __forceinline__ void tc_iter_epilogue(const TcArgs &a, const TcWork &
 	const uint32_t trow = tmem + ((uint32_t)(32 * q) << 16) + col0;
 	const int64_t pe = (int64_t)np * np;
 	float res = 0.f;
-	for (int c0 = 0; c0 < N; c0 += 16) {
-		float v[16];
-		tmem_ld16(trow + (uint32_t)c0, v);
+	for (int cb = 0; cb < N; cb += 64) {
+		// 64 columns per tensor-memory load (inside the 256-column accumulator; columns past N unused)
+		float vv[64];
+		tmem_ld64(trow + (uint32_t)cb, vv);
 		if (row >= np) continue;
 #pragma unroll
-		for (int k = 0; k < 16; k++) v[k] *= kTcAccUnscale;
-		if (PHASE == kTcPhaseGram) {
+		for (int sb = 0; sb < 4; sb++) {
+			const int c0 = cb + 16 * sb;
+			if (c0 >= N) break;
+			float *v = vv + 16 * sb;
 #pragma unroll
-			for (int k = 0; k < 16; k++) {
-				const int col = n0 + c0 + k;
-				const float g = v[k];
-				if (row < n && col < n) {
-					const float d = g - (col == row ? 1.f : 0.f);
-					res += d * d;
-				}
-				v[k] = c3 * g + (col == row ? c1 : 0.f);
-			}
-			__nv_bfloat16 *P0 = a.Pp + w.pofs;
+			for (int k = 0; k < 16; k++) v[k] *= kTcAccUnscale;
+			if (PHASE == kTcPhaseGram) {
 #pragma unroll
-			for (int h = 0; h < 2; h++) {
-				const int64_t o = ((int64_t)(row >> 3) * npg + ((n0 + c0) >> 3) + h) * 64 + (row & 7) * 8;
-				store_split8h(v + 8 * h, P0 + o, P0 + pe + o);
-			}
-		} else if (final_update) {
-			if (row < n) {
-				float *T = a.T + w.tofs;
 				for (int k = 0; k < 16; k++) {
 					const int col = n0 + c0 + k;
-					if (col < n) T[a.t_rowmajor ? (int64_t)row * n + col : (int64_t)col * n + row] = v[k];
+					const float g = v[k];
+					if (row < n && col < n) {
+						const float d = g - (col == row ? 1.f : 0.f);
+						res += d * d;
+					}
+					v[k] = c3 * g + (col == row ? c1 : 0.f);
 				}
-			}
-		} else {
-			__nv_bfloat16 *X0 = a.Xw + w.xofs;
+				__nv_bfloat16 *P0 = a.Pp + w.pofs;
 #pragma unroll
-			for (int h = 0; h < 2; h++) {
-				const int64_t o = ((int64_t)(row >> 3) * npg + ((n0 + c0) >> 3) + h) * 64 + (row & 7) * 8;
-				store_split8h(v + 8 * h, X0 + o, X0 + pe + o);
+				for (int h = 0; h < 2; h++) {
+					const int64_t o = ((int64_t)(row >> 3) * npg + ((n0 + c0) >> 3) + h) * 64 + (row & 7) * 8;
+					store_split8h(v + 8 * h, P0 + o, P0 + pe + o);
+				}
+			} else if (final_update) {
+				if (row < n) {
+					float *T = a.T + w.tofs;
+#pragma unroll
+					for (int k = 0; k < 16; k++) {
+						const int col = n0 + c0 + k;
+						if (col < n) T[a.t_rowmajor ? (int64_t)row * n + col : (int64_t)col * n + row] = v[k];
+					}
+				}
+			} else {
+				__nv_bfloat16 *X0 = a.Xw + w.xofs;
+#pragma unroll
+				for (int h = 0; h < 2; h++) {
+					const int64_t o = ((int64_t)(row >> 3) * npg + ((n0 + c0) >> 3) + h) * 64 + (row & 7) * 8;
+					store_split8h(v + 8 * h, X0 + o, X0 + pe + o);
+				}
 			}
 		}
 	}
