@@ -171,6 +171,12 @@ __device__ __forceinline__ void mbar_add_tx(uint64_t *bar, uint32_t bytes) {
 	asm volatile("mbarrier.expect_tx.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
 
+// An arrival on `bar` once every cp.async this thread has issued so far has completed (the
+// barrier's expected count includes it).
+__device__ __forceinline__ void cp_async_arrive_noinc(uint64_t *bar) {
+	asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 // One plain arrival on `bar`.
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 	asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
@@ -847,9 +853,9 @@ constexpr uint32_t kTcIterCols = 512;  // two accumulators of up to 256 columns
 
 // The Gram (PHASE 1) or update (PHASE 2) products of every tile of a launch, one CTA per SM walking
 // tiles blockIdx.x, blockIdx.x + gridDim.x, ...  Stages are filled continuously across tile
-// boundaries: warp 0 copies the A tile with per-lane cp.async (each lane signals a stage's full
-// barrier once its copies of that stage have landed, S - 1 stages behind its issue, after a proxy
-// fence) and the B operand with bulk copies (K half by K half, their bytes counted by the same
+// boundaries: warp 0 copies the A tile with per-lane cp.async (the hardware arrives on the stage's
+// full barrier for each lane once that lane's copies have landed; the MMA thread fences the proxy
+// after its wait) and the B operand with bulk copies (K half by K half, their bytes counted by the same
 // barrier); lane 0 of warp 1 issues each stage's three products into one of two tensor-memory
 // accumulators (tiles alternate) and commits the stage to its consumed barrier and the finished
 // tile to the accumulator's full barrier; warps 2-5 read the finished accumulator, write the
@@ -872,7 +878,6 @@ __global__ void __launch_bounds__(kTcIterThreads, 1) k_tc_iter(const TcArgs a, i
 	const int stage_bytes = 2 * 4096 + 2 * 32 * nmax;
 	int S = a.smem_bytes / stage_bytes;
 	if (S > kTcMaxStages) S = kTcMaxStages;
-	const int L = S - 1;  // how far the per-lane A copies' arrivals trail their issue
 	const uint32_t smem0 = smem_u32(tc_smem);
 	if (tid == 0) {
 		for (int i = 0; i < kTcMaxStages; i++) {
@@ -937,19 +942,11 @@ __global__ void __launch_bounds__(kTcIterThreads, 1) k_tc_iter(const TcArgs a, i
 						                                            : ((int64_t)(16 * t + gg) * npg + 2 * ks + k) * 64 + 8 * r;
 						cp_async16(st + p * 4096 + core * 128 + r * 16, valid ? As + p * pe + src : As, valid ? 16u : 0u);
 					}
-				cp_async_commit();
-				if (g >= (uint32_t)L) {  // this lane's copies of slice g - L have landed
-					cp_async_wait_keep(L);
-					fence_proxy_async_smem();
-					mbar_arrive(&s_full[(g - L) % S]);
-				}
+				cp_async_arrive_noinc(&s_full[s]);  // when this lane's copies of the stage have landed
 			}
 		}
-		// the arrivals still owed: slices max(0, g - L) .. g - 1
 		cp_async_wait_all();
-		fence_proxy_async_smem();
-		for (uint32_t h = g > (uint32_t)L ? g - L : 0u; h < g; h++) mbar_arrive(&s_full[h % S]);
-		// every bulk copy issued has landed before the CTA may leave
+		// every copy issued has landed before the CTA may leave
 		if (lane == 0)
 			for (uint32_t h = g > (uint32_t)S ? g - S : 0u; h < g; h++)
 				if (!mbar_wait(&s_full[h % S], (h / S) & 1u)) *vfail = 1;
@@ -977,6 +974,7 @@ __global__ void __launch_bounds__(kTcIterThreads, 1) k_tc_iter(const TcArgs a, i
 						ok = 0;
 						break;
 					}
+					fence_proxy_async_smem();  // the lanes' cp.async writes, seen through the barrier, to the MMA
 					tc_fence_after();
 					const uint32_t st = smem0 + s * stage_bytes;
 #pragma unroll
