@@ -835,8 +835,8 @@ int set_tc_attrs() {
 	HA_CUDA(cudaFuncSetAttribute(k_tc_gemm<kTcPhaseGram>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemLarge));
 	HA_CUDA(cudaFuncSetAttribute(k_tc_gemm<kTcPhaseUpdate>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemLarge));
 	HA_CUDA(cudaFuncSetAttribute(k_tc_gemm<kTcPhaseGram, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemLarge));
-	HA_CUDA(cudaFuncSetAttribute(k_tc_iter<kTcPhaseGram>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemLarge));
-	HA_CUDA(cudaFuncSetAttribute(k_tc_iter<kTcPhaseUpdate>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemLarge));
+	HA_CUDA(cudaFuncSetAttribute(k_tc_iter<kTcPhaseGram>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax));
+	HA_CUDA(cudaFuncSetAttribute(k_tc_iter<kTcPhaseUpdate>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax));
 	HA_CUDA(cudaFuncSetAttribute(k_tc_gemm<kTcPhaseUpdate, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemLarge));
 	HA_CUDA(cudaFuncSetAttribute(k_tc_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemLarge));
 	done = true;
@@ -964,9 +964,13 @@ template <int PHASE>
 void launch_tc_tiles(int ntiles, TcArgs a, cudaStream_t st, int nmax) {
 	if constexpr (PHASE != kTcPhaseXcov) {
 		if (tc_iter_persist()) {
+			// stages for the tiles' widest B, then the CTA's tile list; enough CTAs that none holds
+			// more than kTcIterMaxTiles tiles (beyond one per SM they run in later waves)
 			const int stage = 2 * 4096 + 64 * nmax;
-			a.smem_bytes = std::min(kTcMaxStages, kTcSmemLarge / stage) * stage;
-			k_tc_iter<PHASE><<<std::min(ntiles, g_num_sms), kTcIterThreads, a.smem_bytes, st>>>(a, ntiles, nmax);
+			const int list = kTcIterMaxTiles * (int)sizeof(TcIterTile);
+			a.smem_bytes = std::min(kTcMaxStages, (int)(kSmemMax - list) / stage) * stage + list;
+			const int grid = std::min(ntiles, std::max(g_num_sms, (ntiles + kTcIterMaxTiles - 1) / kTcIterMaxTiles));
+			k_tc_iter<PHASE><<<grid, kTcIterThreads, a.smem_bytes, st>>>(a, ntiles, nmax);
 			return;
 		}
 	}

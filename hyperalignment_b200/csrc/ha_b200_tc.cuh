@@ -850,6 +850,15 @@ __device__ __forceinline__ bool tc_update_decision(const TcArgs &a, const TcWork
 
 constexpr int kTcIterThreads = 192;    // warp 0 producer, warp 1 MMA, warps 2-5 epilogue
 constexpr uint32_t kTcIterCols = 512;  // two accumulators of up to 256 columns
+constexpr int kTcIterMaxTiles = 256;   // tiles per CTA (the grid grows to keep within it)
+
+// One tile of a persistent launch as the roles need it, gathered once at the kernel's start.
+struct TcIterTile {
+	int32_t slot, n, np, t, n0, nn;
+	int32_t skip;  // the searchlight is done
+	int32_t fin;   // update: this update is the searchlight's last (it writes T)
+	int64_t xofs, pofs, tofs;
+};
 
 // The Gram (PHASE 1) or update (PHASE 2) products of every tile of a launch, one CTA per SM walking
 // tiles blockIdx.x, blockIdx.x + gridDim.x, ...  Stages are filled continuously across tile
@@ -876,8 +885,11 @@ __global__ void __launch_bounds__(kTcIterThreads, 1) k_tc_iter(const TcArgs a, i
 		return;
 	}
 	const int stage_bytes = 2 * 4096 + 2 * 32 * nmax;
-	int S = a.smem_bytes / stage_bytes;
+	// the tile list sits after the stages
+	const int mine = ntiles > (int)blockIdx.x ? (ntiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x : 0;
+	int S = (a.smem_bytes - kTcIterMaxTiles * (int)sizeof(TcIterTile)) / stage_bytes;
 	if (S > kTcMaxStages) S = kTcMaxStages;
+	TcIterTile *tlist = reinterpret_cast<TcIterTile *>(tc_smem + S * stage_bytes);
 	const uint32_t smem0 = smem_u32(tc_smem);
 	if (tid == 0) {
 		for (int i = 0; i < kTcMaxStages; i++) {
@@ -889,10 +901,29 @@ __global__ void __launch_bounds__(kTcIterThreads, 1) k_tc_iter(const TcArgs a, i
 			mbar_init(&s_acce[b], 4);
 		}
 		mbar_init(&s_fin, 1);
-		s_fail = (S < 2 || nmax > 256) ? 1 : 0;
+		s_fail = (S < 2 || nmax > 256 || mine > kTcIterMaxTiles) ? 1 : 0;
 		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 	}
 	if (warp == 0) tmem_alloc(&s_tmem, kTcIterCols);
+	// every thread gathers some of this CTA's tiles: one round of independent loads instead of a
+	// chain of dependent ones per tile in every role; the update's decisions and next states too
+	if (mine <= kTcIterMaxTiles)
+		for (int e = tid; e < mine; e += kTcIterThreads) {
+			const TcTile tl = a.tiles[blockIdx.x + e * gridDim.x];
+			const TcWork w = a.work[tl.w];
+			const TcState st = a.st_in[w.slot];
+			TcIterTile d;
+			d.slot = w.slot; d.n = w.n; d.np = w.np; d.t = tl.t; d.n0 = tl.n0; d.nn = tl.nn;
+			d.skip = st.done ? 1 : 0;
+			d.fin = 0;
+			d.xofs = w.xofs; d.pofs = w.pofs; d.tofs = w.tofs;
+			if (PHASE == kTcPhaseUpdate) {
+				TcState o = st;
+				if (!st.done) d.fin = tc_update_decision(a, w, st, &o) ? 1 : 0;
+				if (tl.t == 0 && tl.n0 == 0) a.st_out[w.slot] = o;
+			}
+			tlist[e] = d;
+		}
 	tc_fence_before();
 	__syncthreads();
 	tc_fence_after();
@@ -903,14 +934,13 @@ __global__ void __launch_bounds__(kTcIterThreads, 1) k_tc_iter(const TcArgs a, i
 	if (warp == 0 && !failed0) {
 		uint32_t g = 0;  // slices issued by this CTA
 		bool ok = true;
-		for (int i = blockIdx.x; i < ntiles && ok; i += gridDim.x) {
-			const TcTile tl = a.tiles[i];
-			const TcWork w = a.work[tl.w];
-			if (a.st_in[w.slot].done) continue;
-			const int np = w.np, npg = np >> 3, t = tl.t, N = tl.nn, g0 = tl.n0 >> 3, nk = np >> 4;
+		for (int e = 0; e < mine && ok; e++) {
+			const TcIterTile d = tlist[e];
+			if (d.skip) continue;
+			const int np = d.np, npg = np >> 3, t = d.t, N = d.nn, g0 = d.n0 >> 3, nk = np >> 4;
 			const int64_t pe = (int64_t)np * np;
-			const __nv_bfloat16 *As = a.Xp + w.xofs;
-			const __nv_bfloat16 *Bs = (PHASE == kTcPhaseGram) ? As : (const __nv_bfloat16 *)(a.Pp + w.pofs);
+			const __nv_bfloat16 *As = a.Xp + d.xofs;
+			const __nv_bfloat16 *Bs = (PHASE == kTcPhaseGram) ? As : (const __nv_bfloat16 *)(a.Pp + d.pofs);
 			for (int ks = 0; ks < nk; ks++, g++) {
 				const int s = (int)(g % (uint32_t)S);
 				int go = 1;
@@ -956,11 +986,10 @@ __global__ void __launch_bounds__(kTcIterThreads, 1) k_tc_iter(const TcArgs a, i
 		// lane 0 issues; the other lanes wait at the warp barrier
 		uint32_t g = 0, j = 0;  // slices consumed, tiles computed
 		const int a_mn = (PHASE == kTcPhaseGram) ? 1 : 0;
-		for (int i = blockIdx.x; i < ntiles; i += gridDim.x) {
-			const TcTile tl = a.tiles[i];
-			const TcWork w = a.work[tl.w];
-			if (a.st_in[w.slot].done) continue;
-			const int nk = w.np >> 4, N = tl.nn, b = (int)(j & 1u);
+		for (int e = 0; e < mine; e++) {
+			const TcIterTile d = tlist[e];
+			if (d.skip) continue;
+			const int nk = d.np >> 4, N = d.nn, b = (int)(j & 1u);
 			int ok = 1;
 			if (lane == 0) {
 				// the accumulator's previous tile (j - 2) must have been read out
@@ -996,27 +1025,19 @@ __global__ void __launch_bounds__(kTcIterThreads, 1) k_tc_iter(const TcArgs a, i
 	}
 	if (warp >= 2 && !failed0) {
 		uint32_t j = 0;
-		for (int i = blockIdx.x; i < ntiles; i += gridDim.x) {
-			const TcTile tl = a.tiles[i];
-			const TcWork w = a.work[tl.w];
-			const TcState st = a.st_in[w.slot];
-			if (st.done) {
-				if (PHASE == kTcPhaseUpdate && tl.t == 0 && tl.n0 == 0 && tid == 64) a.st_out[w.slot] = st;
-				continue;
-			}
-			bool fin = false;
-			if (PHASE == kTcPhaseUpdate) {
-				TcState o;
-				fin = tc_update_decision(a, w, st, &o);
-				if (tl.t == 0 && tl.n0 == 0 && tid == 64) a.st_out[w.slot] = o;
-			}
+		for (int e = 0; e < mine; e++) {
+			const TcIterTile d = tlist[e];
+			if (d.skip) continue;
+			TcWork w = {};
+			w.slot = d.slot; w.n = d.n; w.np = d.np; w.xofs = d.xofs; w.pofs = d.pofs; w.tofs = d.tofs;
+			const bool fin = d.fin != 0;
 			const int b = (int)(j & 1u);
 			if (!mbar_wait_idle(&s_accf[b], (j >> 1) & 1u)) {
 				*vfail = 1;
 				break;
 			}
 			tc_fence_after();
-			tc_iter_epilogue<PHASE>(a, w, tl.t, tl.n0, tl.nn, tmem, (uint32_t)(256 * b), warp & 3, lane, fin, a.c1, a.c3);
+			tc_iter_epilogue<PHASE>(a, w, d.t, d.n0, d.nn, tmem, (uint32_t)(256 * b), warp & 3, lane, fin, a.c1, a.c3);
 			tc_fence_before();
 			__syncwarp();
 			if (lane == 0) mbar_arrive(&s_acce[b]);
