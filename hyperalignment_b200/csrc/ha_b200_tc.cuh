@@ -886,7 +886,12 @@ __global__ void __launch_bounds__(kTcIterThreads, 1) k_tc_iter(const TcArgs a, i
 	}
 	const int stage_bytes = 2 * 4096 + 2 * 32 * nmax;
 	// the tile list sits after the stages
-	const int mine = ntiles > (int)blockIdx.x ? (ntiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x : 0;
+	// tiles dealt in snake order (round e: CTA b takes e G + b, or e G + G - 1 - b in odd rounds), which
+	// balances a largest-first tile list better than plain round-robin
+	const int G = (int)gridDim.x, B = (int)blockIdx.x;
+	auto tile_of = [&](int e) { return e * G + ((e & 1) ? G - 1 - B : B); };
+	int mine = ntiles / G;
+	if (mine * G < ntiles && tile_of(mine) < ntiles) mine++;
 	int S = (a.smem_bytes - kTcIterMaxTiles * (int)sizeof(TcIterTile)) / stage_bytes;
 	if (S > kTcMaxStages) S = kTcMaxStages;
 	TcIterTile *tlist = reinterpret_cast<TcIterTile *>(tc_smem + S * stage_bytes);
@@ -909,7 +914,7 @@ __global__ void __launch_bounds__(kTcIterThreads, 1) k_tc_iter(const TcArgs a, i
 	// chain of dependent ones per tile in every role; the update's decisions and next states too
 	if (mine <= kTcIterMaxTiles)
 		for (int e = tid; e < mine; e += kTcIterThreads) {
-			const TcTile tl = a.tiles[blockIdx.x + e * gridDim.x];
+			const TcTile tl = a.tiles[tile_of(e)];
 			const TcWork w = a.work[tl.w];
 			const TcState st = a.st_in[w.slot];
 			TcIterTile d;
