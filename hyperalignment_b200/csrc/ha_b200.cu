@@ -948,22 +948,28 @@ int tc_bulk_mask() {
 	return v;
 }
 
-// The iteration's products by the persistent kernel (one CTA per SM walking the tiles, loads,
-// products and epilogues overlapped across tiles: HA_B200_TC_ITER=1) or by one CTA per tile.
-bool tc_iter_persist() {
+// The first iteration whose products run in the persistent kernel (one CTA per SM walking the
+// tiles; loads, products and epilogues overlapped across tiles); earlier iterations launch one CTA
+// per tile.  While every searchlight is active the per-tile launches are faster (their tails
+// overlap the next launch); once most have converged, a per-tile launch still starts every tile's
+// CTA (about 0.25 ms for the template hemisphere's 24,054 tiles) where the persistent launch reads
+// a short tile list (8-18 us).  Both compute identical bits.  HA_B200_TC_ITER_FROM overrides the
+// default 16 (0: always persistent, also in the product self-test; 1000: never).
+int tc_iter_from() {
 	static int v = -1;
 	if (v < 0) {
-		const char *e = getenv("HA_B200_TC_ITER");
-		v = (e && e[0] == '1') ? 1 : 0;
+		const char *e = getenv("HA_B200_TC_ITER_FROM");
+		v = e ? std::max(0, atoi(e)) : 16;
 	}
-	return v == 1;
+	return v;
 }
 
-// One launch of the tile product of PHASE over `ntiles` tiles of at most `nmax` columns.
+// One launch of the tile product of PHASE over `ntiles` tiles of at most `nmax` columns, by the
+// persistent kernel when `persist`.
 template <int PHASE>
-void launch_tc_tiles(int ntiles, TcArgs a, cudaStream_t st, int nmax) {
+void launch_tc_tiles(int ntiles, TcArgs a, cudaStream_t st, int nmax, bool persist) {
 	if constexpr (PHASE != kTcPhaseXcov) {
-		if (tc_iter_persist()) {
+		if (persist) {
 			// stages for the tiles' widest B, then the CTA's tile list; enough CTAs that none holds
 			// more than kTcIterMaxTiles tiles (beyond one per SM they run in later waves)
 			const int stage = 2 * 4096 + 64 * nmax;
@@ -983,14 +989,15 @@ void launch_tc_tiles(int ntiles, TcArgs a, cudaStream_t st, int nmax) {
 // Launch one phase of the tile product over the size classes of a chunk (only class `only` when
 // it is 0 or 1), each with its layout's shared memory.
 template <int PHASE>
-int launch_tc(const Chunk &ch, TcArgs a, cudaStream_t st, int kind, const int *smem, int only = -1) {
+int launch_tc(const Chunk &ch, TcArgs a, cudaStream_t st, int kind, const int *smem, int only = -1,
+              bool persist = false) {
 	for (int c = 0; c < 2; c++) {
 		const int ntiles = (int)ch.tct[c].size();
 		if (!ntiles || (only >= 0 && c != only)) continue;
 		a.tiles = ch.d_tct[c];
 		a.smem_bytes = smem[c];
 		HA_LAUNCH(kind, st);
-		launch_tc_tiles<PHASE>(ntiles, a, st, c ? 256 : 128);
+		launch_tc_tiles<PHASE>(ntiles, a, st, c ? 256 : 128, persist);
 	}
 	HA_CUDA(cudaGetLastError());
 	return kHaSuccess;
@@ -1157,9 +1164,11 @@ int run_procrustes_tc(HaB200Plan *P, const double *d_X, const double *d_Y, bool 
 				a.c3 = sched[k].c3;
 				a.plain = sched[k].plain;
 				a.last = (k == maxit - 1) ? 1 : 0;
-				int r = launch_tc<kTcPhaseGram>(ch, a, ls, kHaB200KTcNs, P->tc_smem);
+				const bool persist = k >= tc_iter_from();
+				int r = launch_tc<kTcPhaseGram>(ch, a, ls, kHaB200KTcNs, P->tc_smem, -1, persist);
 				if (r != kHaSuccess) return r;
-				if ((r = launch_tc<kTcPhaseUpdate>(ch, a, ls, kHaB200KTcNs, P->tc_smem)) != kHaSuccess) return r;
+				if ((r = launch_tc<kTcPhaseUpdate>(ch, a, ls, kHaB200KTcNs, P->tc_smem, -1, persist)) != kHaSuccess)
+					return r;
 			}
 			return kHaSuccess;
 		};
@@ -3163,7 +3172,7 @@ int ha_b200_tc_selftest(int32_t which, int32_t n, int32_t nt, const float *h_a, 
 			if (which == 0) {
 				a.c1 = 0.f;
 				a.c3 = 1.f;  // P = X^T X
-				{ HA_LAUNCH(kHaB200KTcNs, st); launch_tc_tiles<kTcPhaseGram>(grid, a, st, 256); }
+				{ HA_LAUNCH(kHaB200KTcNs, st); launch_tc_tiles<kTcPhaseGram>(grid, a, st, 256, tc_iter_from() == 0); }
 				k_tc_unpack<<<64, kBlock, 0, st>>>(Pp.p, n, np, T.p);
 			} else {
 				if (cudaMemcpy(in1.p, h_b, (size_t)n * n * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
@@ -3173,7 +3182,7 @@ int ha_b200_tc_selftest(int32_t which, int32_t n, int32_t nt, const float *h_a, 
 				k_tc_pack<<<64, kBlock, 0, st>>>(in1.p, n, np, Pp.p);
 				a.plain = 1;
 				a.tol_stop = 1e30f;  // residual 0 < tol: the update is final and writes T = X P
-				{ HA_LAUNCH(kHaB200KTcNs, st); launch_tc_tiles<kTcPhaseUpdate>(grid, a, st, 256); }
+				{ HA_LAUNCH(kHaB200KTcNs, st); launch_tc_tiles<kTcPhaseUpdate>(grid, a, st, 256, tc_iter_from() == 0); }
 			}
 			if (cudaGetLastError() != cudaSuccess ||
 			    cudaMemcpy(h_out, T.p, (size_t)n * n * 4, cudaMemcpyDeviceToHost) != cudaSuccess) {

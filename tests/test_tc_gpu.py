@@ -254,7 +254,7 @@ np.savez(sys.argv[2], **out)
 
 def test_bulk_and_thread_pipelines_bitwise_equal(gpu, tmp_path):
     """The iteration's products staged by bulk copies (HA_B200_TC_BULK bits), by per-thread loads, or
-    by the persistent tile kernel (HA_B200_TC_ITER=1) feed the same MMAs with the same bytes, so
+    by the persistent tile kernel (HA_B200_TC_ITER_FROM=0) feed the same MMAs with the same bytes, so
     every setting gives identical bits."""
     import os
     import subprocess
@@ -263,7 +263,7 @@ def test_bulk_and_thread_pipelines_bitwise_equal(gpu, tmp_path):
     res = {}
     for mask in ("0", "1", "3", "iter"):
         path = tmp_path / f"m{mask}.npz"
-        env = dict(os.environ, HA_B200_TC_ITER="1") if mask == "iter" else dict(os.environ, HA_B200_TC_BULK=mask)
+        env = dict(os.environ, HA_B200_TC_ITER_FROM="0") if mask == "iter" else dict(os.environ, HA_B200_TC_BULK=mask)
         subprocess.run([sys.executable, "-c", _PIPELINE_SCRIPT, root, str(path)], env=env, check=True, timeout=300)
         res[mask] = np.load(path)
     for k in res["0"].files:
