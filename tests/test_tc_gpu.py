@@ -270,3 +270,42 @@ def test_bulk_and_thread_pipelines_bitwise_equal(gpu, tmp_path):
         assert res["1"][k].tobytes() == res["0"][k].tobytes(), k
         assert res["3"][k].tobytes() == res["0"][k].tobytes(), k
         assert res["iter"][k].tobytes() == res["0"][k].tobytes(), k
+
+
+_SOLVE_SCRIPT = r"""
+import sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+import torch
+from hyperalignment_b200 import _lib as L
+from hyperalignment_b200 import workloads as W
+from hyperalignment_b200.plan import Plan
+assert L.lib().ha_b200_init() == 0
+w = W.rank_deficient_pair(3, nv=642, nt=200)
+plan = Plan.from_workload(w)
+dX = torch.from_numpy(np.asfortranarray(w.X).ravel(order="F")).cuda()
+dY = torch.from_numpy(np.asfortranarray(w.Y).ravel(order="F")).cuda()
+vals = torch.zeros(plan.nnz, dtype=torch.float64, device="cuda")
+for _ in range(2):
+    vals.zero_()
+    plan.procrustes_device(dX.data_ptr(), dY.data_ptr(), vals.data_ptr(), True, True, L.SOLVER_TC, L.OUT_CSR)
+torch.cuda.synchronize()
+np.save(sys.argv[2], vals.cpu().numpy())
+"""
+
+
+def test_iteration_kernels_switch_point_bitwise(gpu, tmp_path):
+    """The whole tensor-core solve gives identical bits whichever iteration the persistent kernel
+    takes over from (HA_B200_TC_ITER_FROM: always, from iteration 5, never)."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = {}
+    for v in ("0", "5", "1000"):
+        path = tmp_path / f"f{v}.npy"
+        env = dict(os.environ, HA_B200_TC_ITER_FROM=v)
+        subprocess.run([sys.executable, "-c", _SOLVE_SCRIPT, root, str(path)], env=env, check=True, timeout=600)
+        out[v] = np.load(path)
+    assert out["0"].tobytes() == out["1000"].tobytes()
+    assert out["5"].tobytes() == out["1000"].tobytes()
