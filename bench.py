@@ -1046,10 +1046,37 @@ def config4_grid_full(args, dev):
         rc = np.asarray(r[6]).ravel()
         rel.append(float(np.max(np.abs(hc[q] - rc) / np.abs(rc))))
         same += int(hb[q] == int(np.argmin(rc)))
+    # the plain FP32 form of the same grid search: one warm-up, one timed step, costs and winners
+    # against the float64 search's (all searchlights)
+    plan.set_grid_precision(32)
+    best32 = torch.zeros_like(best)
+    cost32 = torch.zeros_like(cost)
+
+    def step32():
+        vals.zero_()
+        plan.ridge_grid_device(dX.data_ptr(), dY.data_ptr(), vals.data_ptr(), best32.data_ptr(), W.GRID_ALPHAS,
+                               W.GRID_NPCS, tr, te, d_cost=cost32.data_ptr(), stream=stream.cuda_stream)
+
+    step32()
+    torch.cuda.synchronize()
+    flush.zero_()
+    a.record(stream)
+    step32()
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms32 = a.elapsed_time(b)
+    plan.set_grid_precision(64)
+    hb32, hc32 = best32.cpu().numpy(), cost32.cpu().numpy().reshape(sls.count, grid)
+    rows = np.arange(sls.count)
+    plain = {"value": sls.count / (ms32 / 1e3), "ms_per_step": ms32, "steps": 1, "warmup": 1, "dtype": "f32",
+             "cost_grid_max_rel_vs_f64": float(np.max(np.abs(hc32 - hc) / np.abs(hc))),
+             "winners_equal_f64": float(np.mean(hb32 == hb)),
+             "winner_cost_regret_max": float(np.max(hc[rows, hb32] / hc.min(axis=1) - 1.0))}
     st = plan.stats()
     plan.close()
     sizes = sls.sizes
     return {"value": sls.count / (ms / 1e3), "unit": UNIT, "ms_per_step": ms, "steps": 1, "warmup": 1,
+            "plain_fp32": plain, "speedup_over_plain_fp32": ms32 / ms,
             "first_call_s": first_s,
             "config": {"workload": "ridge_grid_full", "nv": w.nv, "nt": w.nt, "searchlights": sls.count,
                        "sl_size_min": int(sizes.min()), "sl_size_max": int(sizes.max()),
@@ -1071,10 +1098,13 @@ def config5_learned(args):
     searchlights (with homogeneous noise one grid point wins almost everywhere)."""
     from hyperalignment_b200 import learned as LR
     res = LR.study(nv=40962, step=4, train_step=16, size_lo=50, size_hi=500, epochs=60, log=lambda *a: None)
-    g, l = res["grid"], res["learned"]
+    g, l, g32 = res["grid"], res["learned"], res["grid_fp32"]
     return {"value": l["searchlights_per_s"], "unit": UNIT, "ms_per_step": l["ms"],
             "full_grid": {"value": g["searchlights_per_s"], "ms_per_step": g["ms"], "heldout_corr": g["heldout_corr"]},
             "speedup_over_full_grid": l["searchlights_per_s"] / g["searchlights_per_s"],
+            "plain_fp32_grid": {"value": g32["searchlights_per_s"], "ms_per_step": g32["ms"],
+                                "heldout_corr": g32["heldout_corr"], "winners_equal_fp64": g32["winners_equal_fp64"]},
+            "speedup_over_plain_fp32_grid": l["searchlights_per_s"] / g32["searchlights_per_s"],
             "heldout_corr": l["heldout_corr"], "heldout_corr_minus_grid": l["heldout_corr"] - g["heldout_corr"],
             "fallback_searchlights": l["fallback"], "proposal_matches_grid": l["proposal_matches_grid"],
             "fixed_point": res["fixed_point"], "train": res["train"],

@@ -107,6 +107,7 @@ SIGNATURES = {
     "ha_b200_plan_tc_layout": (ctypes.c_int, [ctypes.c_void_p, c_int32_p, c_int32_p, c_double_p]),
     "ha_b200_set_graphs": (None, [ctypes.c_bool]),
     "ha_b200_plan_set_tc_layout": (ctypes.c_int, [ctypes.c_void_p, c_int32_p]),
+    "ha_b200_plan_set_grid_precision": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
     "ha_b200_aligned_correlation_device": (ctypes.c_int, [
         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
         ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),

@@ -265,11 +265,13 @@ struct Chunk {
 	int s0, s1;
 	std::vector<SlWork> w32, w64, weig;  // float32 polar, float64 polar, float64 eigenvector mode
 	std::vector<Bucket> b32, b64, beig;
+	std::vector<SlWork> weig32;  // float32 eigenvector mode (the plain FP32 grid search)
+	std::vector<Bucket> beig32;
 	std::vector<int64_t> tofs;  // per slot
 	int64_t scratch_elems8;     // scratch size in 8-byte units (A and V each)
 	int64_t t_elems;            // T scratch floats
 	int64_t uv_elems;
-	SlWork *d_w32 = nullptr, *d_w64 = nullptr, *d_weig = nullptr;
+	SlWork *d_w32 = nullptr, *d_w64 = nullptr, *d_weig = nullptr, *d_weig32 = nullptr;
 	int64_t *d_tofs = nullptr;
 	// tensor-core solve: one work item per searchlight (slot order), 128-row tiles in two size
 	// classes (np <= 256: two CTAs per SM; np > 256), largest searchlights first
@@ -336,6 +338,7 @@ struct HaB200Plan {
 	// the ridge grid search captured as a CUDA graph, and the key it was captured for
 	cudaGraphExec_t grid_graph = nullptr;
 	std::vector<uint64_t> grid_key;
+	int grid_bits = 64;  // arithmetic of ha_b200_plan_ridge_grid_device: 64 (float64) or 32 (plain FP32)
 	int64_t grid_graph_launches = 0;
 	double tc_tune_ms[2][3] = {{0}};  // measured Gram-launch times of the candidates
 	// ridge grid search: scratch and the uploaded grid / CV description, allocated on first use
@@ -426,7 +429,7 @@ size_t scratch_budget_bytes() {
 
 // Sort work items by Jacobi class (resident or blocked, rows per lane), largest first inside a
 // class, and cut them into buckets of one Jacobi kernel instance each.  prec: 0 float32 polar,
-// 1 float64 polar, 2 float64 eigenvector mode.
+// 1 float64 polar, 2 float64 eigenvector mode, 3 float32 eigenvector mode.
 std::vector<Bucket> bucketize(std::vector<SlWork> &items, int prec) {
 	auto key = [](const SlWork &w) { return (w.nblk == 2 ? 0 : 32) + rpl_for(w.n); };
 	std::stable_sort(items.begin(), items.end(), [&](const SlWork &a, const SlWork &b) {
@@ -441,7 +444,8 @@ std::vector<Bucket> bucketize(std::vector<SlWork> &items, int prec) {
 		while (j < (int)items.size() && key(items[j]) == key(items[i])) {
 			int bb, kk;
 			size_t mm;
-			jacobi_layout(items[j].n, prec >= 1, bb, kk, mm, prec >= 1 ? kSmemMax : fp32_jacobi_budget(), prec != 2);
+			const bool f64 = prec == 1 || prec == 2;
+			jacobi_layout(items[j].n, f64, bb, kk, mm, f64 ? kSmemMax : fp32_jacobi_budget(), prec < 2);
 			smem = std::max(smem, mm);
 			j++;
 		}
@@ -450,7 +454,7 @@ std::vector<Bucket> bucketize(std::vector<SlWork> &items, int prec) {
 		b.count = j - i;
 		b.smem = smem;
 		b.blocked = items[i].nblk != 2;
-		b.threads = jacobi_threads(items[i].bsz, prec >= 1);
+		b.threads = jacobi_threads(items[i].bsz, prec == 1 || prec == 2);
 		b.rpl = rpl_for(items[i].n);
 		buckets.push_back(b);
 		i = j;
@@ -468,7 +472,7 @@ int build_chunks(HaB200Plan *P) {
 		int64_t acc8 = 0, tacc = 0, uvacc = 0;
 		std::vector<int64_t> tofs;
 		std::vector<int64_t> aofs8;
-		std::vector<int> bs32, nb32, bs64, nb64, bse, nbe;
+		std::vector<int> bs32, nb32, bs64, nb64, bse, nbe, bse32, nbe32;
 		std::vector<size_t> sm32, sm64;
 		while (s < P->count) {
 			int n = P->h_off[s + 1] - P->h_off[s];
@@ -479,10 +483,13 @@ int build_chunks(HaB200Plan *P) {
 			int be, ke;
 			size_t me;
 			jacobi_layout(n, true, be, ke, me, kSmemMax, false);
+			int be32, ke32;
+			jacobi_layout(n, false, be32, ke32, me, fp32_jacobi_budget(), false);
 			int64_t e32 = ((int64_t)n * k32 * b32 * 4 + 7) / 8;
 			int64_t e64 = (int64_t)n * k64 * b64;
 			int64_t eeig = (int64_t)n * ke * be;
-			int64_t region = std::max<int64_t>(std::max(std::max(e32, e64), eeig), (int64_t)n * n);
+			int64_t eeig32 = ((int64_t)n * ke32 * be32 * 4 + 7) / 8;
+			int64_t region = std::max<int64_t>(std::max(std::max(e32, e64), std::max(eeig, eeig32)), (int64_t)n * n);
 			region = (region + 31) & ~(int64_t)31;
 			size_t bytes_if = (size_t)(acc8 + region) * 8 * 2 + (size_t)(tacc + (int64_t)n * n) * 4;
 			if (!tofs.empty() && bytes_if > budget) break;
@@ -493,6 +500,7 @@ int build_chunks(HaB200Plan *P) {
 			bs32.push_back(b32); nb32.push_back(k32); sm32.push_back(m32);
 			bs64.push_back(b64); nb64.push_back(k64); sm64.push_back(m64);
 			bse.push_back(be); nbe.push_back(ke);
+			bse32.push_back(be32); nbe32.push_back(ke32);
 			uvacc += 2 * (int64_t)n;
 			s++;
 		}
@@ -503,7 +511,7 @@ int build_chunks(HaB200Plan *P) {
 		ch.tofs = tofs;
 		const int nsl = ch.s1 - ch.s0;
 		// work items, bucketed by (mode, n range), largest first inside a bucket
-		for (int prec = 0; prec < 3; prec++) {  // float32, float64, float64 eigenvector mode
+		for (int prec = 0; prec < 4; prec++) {  // float32, float64, float64 / float32 eigenvector mode
 			std::vector<SlWork> items;
 			int64_t uvo = 0;
 			for (int q = 0; q < nsl; q++) {
@@ -512,9 +520,9 @@ int build_chunks(HaB200Plan *P) {
 				SlWork w;
 				w.s = sidx;
 				w.n = n;
-				w.bsz = prec == 2 ? bse[q] : (prec ? bs64[q] : bs32[q]);
-				w.nblk = prec == 2 ? nbe[q] : (prec ? nb64[q] : nb32[q]);
-				w.aofs = prec ? aofs8[q] : aofs8[q] * 2;
+				w.bsz = prec == 3 ? bse32[q] : prec == 2 ? bse[q] : (prec ? bs64[q] : bs32[q]);
+				w.nblk = prec == 3 ? nbe32[q] : prec == 2 ? nbe[q] : (prec ? nb64[q] : nb32[q]);
+				w.aofs = (prec == 1 || prec == 2) ? aofs8[q] : aofs8[q] * 2;
 				w.tofs = tofs[q];
 				w.sofs = P->h_off[sidx];
 				w.slot = q;
@@ -525,7 +533,8 @@ int build_chunks(HaB200Plan *P) {
 			std::vector<Bucket> buckets = bucketize(items, prec);
 			if (prec == 0) { ch.w32 = items; ch.b32 = buckets; }
 			else if (prec == 1) { ch.w64 = items; ch.b64 = buckets; }
-			else { ch.weig = items; ch.beig = buckets; }
+			else if (prec == 2) { ch.weig = items; ch.beig = buckets; }
+			else { ch.weig32 = items; ch.beig32 = buckets; }
 		}
 		P->chunks.push_back(std::move(ch));
 	}
@@ -536,6 +545,8 @@ int build_chunks(HaB200Plan *P) {
 		if (cudaMalloc(&ch.d_w64, n64 * sizeof(SlWork)) != cudaSuccess) return kHaErrorAlloc;
 		if (cudaMalloc(&ch.d_weig, ne * sizeof(SlWork)) != cudaSuccess) return kHaErrorAlloc;
 		HA_CUDA(cudaMemcpy(ch.d_weig, ch.weig.data(), ne * sizeof(SlWork), cudaMemcpyHostToDevice));
+		if (cudaMalloc(&ch.d_weig32, ch.weig32.size() * sizeof(SlWork)) != cudaSuccess) return kHaErrorAlloc;
+		HA_CUDA(cudaMemcpy(ch.d_weig32, ch.weig32.data(), ch.weig32.size() * sizeof(SlWork), cudaMemcpyHostToDevice));
 		if (cudaMalloc(&ch.d_tofs, ch.tofs.size() * sizeof(int64_t)) != cudaSuccess) return kHaErrorAlloc;
 		HA_CUDA(cudaMemcpy(ch.d_w32, ch.w32.data(), n32 * sizeof(SlWork), cudaMemcpyHostToDevice));
 		HA_CUDA(cudaMemcpy(ch.d_w64, ch.w64.data(), n64 * sizeof(SlWork), cudaMemcpyHostToDevice));
@@ -581,7 +592,8 @@ int set_smem_attrs() {
 	HA_CUDA(cudaFuncSetAttribute(k_reduce<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax));
 	HA_CUDA(cudaFuncSetAttribute(k_reduce<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax));
 	HA_CUDA(cudaFuncSetAttribute(k_pattern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax));
-	HA_CUDA(cudaFuncSetAttribute(k_pchol, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(kPcholNb * kGridMaxN * 8)));
+	HA_CUDA(cudaFuncSetAttribute(k_pchol<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(kPcholNb * kGridMaxN * 8)));
+	HA_CUDA(cudaFuncSetAttribute(k_pchol<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(kPcholNb * kGridMaxN * 4)));
 	done = true;
 	return kHaSuccess;
 }
@@ -980,7 +992,7 @@ void launch_tc_tiles(int ntiles, TcArgs a, cudaStream_t st, int nmax, bool persi
 			return;
 		}
 	}
-	if (PHASE != kTcPhaseXcov && (tc_bulk_mask() >> (PHASE - 1) & 1))
+	if (PHASE != kTcPhaseXcov && (tc_bulk_mask() >> (PHASE > 0 ? PHASE - 1 : 0) & 1))
 		k_tc_gemm<PHASE, PHASE != kTcPhaseXcov><<<ntiles, kTcThreads, a.smem_bytes, st>>>(a);
 	else
 		k_tc_gemm<PHASE><<<ntiles, kTcThreads, a.smem_bytes, st>>>(a);
@@ -1604,7 +1616,7 @@ int grid_prepare(HaB200Plan *P) {
 	return P->scrT64.ensure((size_t)maxT);
 }
 
-size_t pchol_smem(int rpl) { return (size_t)kPcholNb * 32 * rpl * sizeof(double); }
+size_t pchol_smem(int rpl, size_t esz = sizeof(double)) { return (size_t)kPcholNb * 32 * rpl * esz; }
 
 JacobiParams eig_params(bool only_flagged) {
 	JacobiParams jp;
@@ -1647,11 +1659,14 @@ struct GridBatch {
 	int64_t total;  // float64 elements of grid scratch
 };
 
-void grid_plan_chunk(const Chunk &ch, const GridParams &gp, std::vector<GridBatch> &bt, std::vector<int64_t> &gbase_all) {
+void grid_plan_chunk(const Chunk &ch, const GridParams &gp, bool fp32, std::vector<GridBatch> &bt,
+                     std::vector<int64_t> &gbase_all) {
 	const int nsl = ch.s1 - ch.s0;
 	const int grid = gp.n_alphas * gp.n_npcs;
 	const size_t budget = grid_budget_bytes();
-	const int nitems = (int)ch.weig.size();
+	const std::vector<SlWork> &items = fp32 ? ch.weig32 : ch.weig;
+	const size_t esz = fp32 ? 4 : 8;
+	const int nitems = (int)items.size();
 	bt.clear();
 	int i0 = 0;
 	while (i0 < nitems) {
@@ -1660,9 +1675,9 @@ void grid_plan_chunk(const Chunk &ch, const GridParams &gp, std::vector<GridBatc
 		int64_t total = 0;
 		int i1 = i0;
 		while (i1 < nitems) {
-			const SlWork &wi = ch.weig[i1];
+			const SlWork &wi = items[i1];
 			const GridLayout Lg = GridLayout::make(wi.n, gp.models, gp.mte, gp.ntu, gp.n_alphas, grid);
-			if (i1 > i0 && (size_t)(total + Lg.total) * 8 > budget) break;
+			if (i1 > i0 && (size_t)(total + Lg.total) * esz > budget) break;
 			gbase_all[g0 + wi.slot] = total;
 			total += Lg.total;
 			i1++;
@@ -1673,46 +1688,61 @@ void grid_plan_chunk(const Chunk &ch, const GridParams &gp, std::vector<GridBatc
 }
 
 // The launches of one chunk's grid search (no host copies or allocations: capturable); the
-// sub-batches' base offsets are at d_gbase (nsl per sub-batch).
-int grid_chunk_launch(HaB200Plan *P, Chunk &ch, const double *d_X, const double *d_Y, const GridSpec &gs,
-                      GridParams gp, const std::vector<GridBatch> &bt, const int64_t *d_gbase, int rowmajor,
-                      int32_t *d_best, double *d_cost, cudaStream_t st) {
+// sub-batches' base offsets are at d_gbase (nsl per sub-batch).  Real is the arithmetic type:
+// double for the float64 grid search, float for the plain FP32 one (the float32 eigenvector-mode
+// work list, the A / V / grid scratch read as float; the winners' betas still go to the float64
+// T scratch for the reduction).
+template <typename Real>
+int grid_chunk_launch_t(HaB200Plan *P, Chunk &ch, const double *d_X, const double *d_Y, const GridSpec &gs,
+                        GridParams gp, const std::vector<GridBatch> &bt, const int64_t *d_gbase, int rowmajor,
+                        int32_t *d_best, double *d_cost, cudaStream_t st) {
+	constexpr bool f32 = sizeof(Real) == 4;
 	const int nt = P->nt;
 	const int nsl = ch.s1 - ch.s0;
 	const JacobiParams jp = eig_params(false);
+	const std::vector<Bucket> &beig = f32 ? ch.beig32 : ch.beig;
+	SlWork *d_work = f32 ? ch.d_weig32 : ch.d_weig;
+	Real *A = reinterpret_cast<Real *>(P->scrA.p), *V = reinterpret_cast<Real *>(P->scrV.p);
+	Real *G = reinterpret_cast<Real *>(P->gridscr.p);
 	int rc;
 	for (size_t bi_ = 0; bi_ < bt.size(); bi_++) {
 		const int i0 = bt[bi_].i0, i1 = bt[bi_].i1;
 		gp.gbase = d_gbase + bi_ * (size_t)nsl;
-		double *A = P->scrA.p, *V = P->scrV.p;
 		for (int mo = 0; mo < gp.models; mo++) {
 			const GridModel &md = gs.mdl[mo];
 			const int32_t *tr = P->grows.p + md.tr_ofs;
 			if ((rc = g_fan.begin(st)) != kHaSuccess) return rc;
-			for (size_t bi = 0; bi < ch.beig.size(); bi++) {
-				const Bucket &b = ch.beig[bi];
+			for (size_t bi = 0; bi < beig.size(); bi++) {
+				const Bucket &b = beig[bi];
 				const int x0 = std::max(i0, b.first), x1 = std::min(i1, b.first + b.count);
 				if (x1 <= x0) continue;
 				const cudaStream_t bs = g_fan.at((int)bi);
-				const SlWork *wk = ch.d_weig + x0;
+				const SlWork *wk = d_work + x0;
 				// Gram into the V scratch, its pivoted Cholesky factor into the A scratch
-				{ HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16><<<x1 - x0, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_X, nt, tr, md.tr_n, V, P->gridscr.p, gp, 0); }
-				{ HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16><<<x1 - x0, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_Y, nt, tr, md.tr_n, A, P->gridscr.p, gp, 1); }
-				{ HA_LAUNCH(kHaB200KRidge, bs); k_pchol<<<x1 - x0, kBlock, pchol_smem(b.rpl), bs>>>(wk, V, A, P->stats.p); }
+				{ HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16, Real><<<x1 - x0, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_X, nt, tr, md.tr_n, V, G, gp, 0); }
+				{ HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16, Real><<<x1 - x0, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_Y, nt, tr, md.tr_n, A, G, gp, 1); }
+				{ HA_LAUNCH(kHaB200KRidge, bs); k_pchol<Real><<<x1 - x0, kBlock, pchol_smem(b.rpl, sizeof(Real)), bs>>>(wk, V, A, P->stats.p); }
 				{
-					HA_LAUNCH(kHaB200KJacobi64, bs);
-					if ((rc = launch_jacobi<double>(b.rpl, x1 - x0, b.threads, b.smem, bs, wk, A, V, P->scrT.p, P->stats.p, P->uv.p, jp)) != kHaSuccess)
+					HA_LAUNCH(f32 ? kHaB200KJacobi32 : kHaB200KJacobi64, bs);
+					if ((rc = launch_jacobi<Real>(b.rpl, x1 - x0, b.threads, b.smem, bs, wk, A, V, P->scrT.p, P->stats.p, P->uv.p, jp)) != kHaSuccess)
 						return rc;
 				}
 			}
 			if ((rc = g_fan.end(st)) != kHaSuccess) return rc;
-			{ HA_LAUNCH(kHaB200KGrid, st); k_grid_model<<<i1 - i0, kBlock, 0, st>>>(ch.d_weig + i0, P->idx.p, d_X, d_Y, V, P->uv.p, mo, P->gridscr.p, gp); }
+			{ HA_LAUNCH(kHaB200KGrid, st); k_grid_model<Real><<<i1 - i0, kBlock, 0, st>>>(d_work + i0, P->idx.p, d_X, d_Y, V, P->uv.p, mo, G, gp); }
 		}
-		{ HA_LAUNCH(kHaB200KGrid, st); k_grid_eval<<<dim3(i1 - i0, gp.n_alphas), kBlock, 0, st>>>(ch.d_weig + i0, P->gridscr.p, gp); }
-		{ HA_LAUNCH(kHaB200KGrid, st); k_grid_final<<<i1 - i0, kBlock, 0, st>>>(ch.d_weig + i0, P->idx.p, d_Y, P->gridscr.p, gp, P->scrT64.p, rowmajor, d_best, d_cost); }
+		{ HA_LAUNCH(kHaB200KGrid, st); k_grid_eval<Real><<<dim3(i1 - i0, gp.n_alphas), kBlock, 0, st>>>(d_work + i0, G, gp); }
+		{ HA_LAUNCH(kHaB200KGrid, st); k_grid_final<Real><<<i1 - i0, kBlock, 0, st>>>(d_work + i0, P->idx.p, d_Y, G, gp, P->scrT64.p, rowmajor, d_best, d_cost); }
 		HA_CUDA(cudaGetLastError());
 	}
 	return kHaSuccess;
+}
+
+int grid_chunk_launch(HaB200Plan *P, Chunk &ch, const double *d_X, const double *d_Y, const GridSpec &gs,
+                      GridParams gp, bool fp32, const std::vector<GridBatch> &bt, const int64_t *d_gbase,
+                      int rowmajor, int32_t *d_best, double *d_cost, cudaStream_t st) {
+	return fp32 ? grid_chunk_launch_t<float>(P, ch, d_X, d_Y, gs, gp, bt, d_gbase, rowmajor, d_best, d_cost, st)
+	            : grid_chunk_launch_t<double>(P, ch, d_X, d_Y, gs, gp, bt, d_gbase, rowmajor, d_best, d_cost, st);
 }
 
 // One chunk's grid search enqueued directly (sub-batch plan, scratch and offsets, launches).
@@ -1720,7 +1750,7 @@ int grid_chunk(HaB200Plan *P, Chunk &ch, const double *d_X, const double *d_Y, c
                const GridParams &gp, int rowmajor, int32_t *d_best, double *d_cost, cudaStream_t st) {
 	std::vector<GridBatch> bt;
 	std::vector<int64_t> gbase;
-	grid_plan_chunk(ch, gp, bt, gbase);
+	grid_plan_chunk(ch, gp, false, bt, gbase);
 	int64_t mx = 1;
 	for (const auto &b : bt) mx = std::max(mx, b.total);
 	int rc;
@@ -1728,12 +1758,13 @@ int grid_chunk(HaB200Plan *P, Chunk &ch, const double *d_X, const double *d_Y, c
 	if ((rc = P->gbase.ensure(std::max<size_t>(gbase.size(), 1))) != kHaSuccess) return rc;
 	HA_CUDA(cudaMemcpyAsync(P->gbase.p, gbase.data(), gbase.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st));
 	HA_CUDA(cudaStreamSynchronize(st));  // the host vector goes out of scope
-	return grid_chunk_launch(P, ch, d_X, d_Y, gs, gp, bt, P->gbase.p, rowmajor, d_best, d_cost, st);
+	return grid_chunk_launch(P, ch, d_X, d_Y, gs, gp, false, bt, P->gbase.p, rowmajor, d_best, d_cost, st);
 }
 
 int run_ridge_grid(HaB200Plan *P, const double *d_X, const double *d_Y, const GridSpec &gs, int out_kind,
                    double *d_vals, int32_t *d_best, double *d_cost, cudaStream_t st) {
 	const int rowmajor = out_kind == kHaB200OutCSR ? 1 : 0;
+	const bool fp32 = P->grid_bits == 32;
 	int rc;
 	if ((rc = grid_prepare(P)) != kHaSuccess) return rc;
 	GridParams gp;
@@ -1747,7 +1778,7 @@ int run_ridge_grid(HaB200Plan *P, const double *d_X, const double *d_Y, const Gr
 	int64_t mx = 1;
 	for (size_t c = 0; c < P->chunks.size(); c++) {
 		gofs[c] = gbase.size();
-		grid_plan_chunk(P->chunks[c], gp, bts[c], gbase);
+		grid_plan_chunk(P->chunks[c], gp, fp32, bts[c], gbase);
 		for (const auto &b : bts[c]) mx = std::max(mx, b.total);
 	}
 	if ((rc = P->gridscr.ensure((size_t)mx)) != kHaSuccess) return rc;
@@ -1759,7 +1790,7 @@ int run_ridge_grid(HaB200Plan *P, const double *d_X, const double *d_Y, const Gr
 		for (size_t c = 0; c < P->chunks.size(); c++) {
 			Chunk &ch = P->chunks[c];
 			HA_CUDA(cudaMemsetAsync(P->stats.p, 0, (size_t)(ch.s1 - ch.s0) * sizeof(SlStats), ls));
-			int r = grid_chunk_launch(P, ch, d_X, d_Y, gs, gp, bts[c], P->gbase.p + gofs[c], rowmajor, d_best, d_cost, ls);
+			int r = grid_chunk_launch(P, ch, d_X, d_Y, gs, gp, fp32, bts[c], P->gbase.p + gofs[c], rowmajor, d_best, d_cost, ls);
 			if (r != kHaSuccess) return r;
 			if ((r = reduce_chunk64(P, ch, out_kind, d_vals, ls)) != kHaSuccess) return r;
 		}
@@ -1775,7 +1806,8 @@ int run_ridge_grid(HaB200Plan *P, const double *d_X, const double *d_Y, const Gr
 		                        (uint64_t)(uintptr_t)gp.npcs, (uint64_t)(uintptr_t)gp.mdl, (uint64_t)(uintptr_t)gp.rows,
 		                        (uint64_t)(uintptr_t)gp.tpos, (uint64_t)(uintptr_t)gp.winv, (uint64_t)(uintptr_t)gp.urows,
 		                        (uint64_t)(uintptr_t)gp.untested, (uint64_t)(uintptr_t)P->gridscr.p,
-		                        (uint64_t)(uintptr_t)P->gbase.p, fnv1a(gbase.data(), gbase.size() * 8, 1469598103934665603ULL)};
+		                        (uint64_t)(uintptr_t)P->gbase.p, fnv1a(gbase.data(), gbase.size() * 8, 1469598103934665603ULL),
+		                        (uint64_t)P->grid_bits};
 		std::vector<uint64_t> kv(key, key + sizeof(key) / sizeof(key[0]));
 		for (const auto &m : gs.mdl) kv.push_back(((uint64_t)m.tr_ofs << 32) ^ (uint64_t)m.tr_n);
 		if (!P->grid_graph || kv != P->grid_key) {
@@ -1831,9 +1863,9 @@ int eigen_chunk(HaB200Plan *P, Chunk &ch, const double *d_X, const double *d_Y, 
 		const Bucket &b = ch.beig[bi];
 		const cudaStream_t bs = g_fan.at((int)bi);
 		const SlWork *wk = ch.d_weig + b.first;
-		{ HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16><<<b.count, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_X, P->nt, d_rows, n_rows, V, nullptr, gp, 0); }
-		if (d_Y) { HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16><<<b.count, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_Y, P->nt, d_rows, n_rows, P->scrT64.p, nullptr, gp, 2); }
-		{ HA_LAUNCH(kHaB200KRidge, bs); k_pchol<<<b.count, kBlock, pchol_smem(b.rpl), bs>>>(wk, V, A, P->stats.p); }
+		{ HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16, double><<<b.count, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_X, P->nt, d_rows, n_rows, V, nullptr, gp, 0); }
+		if (d_Y) { HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16, double><<<b.count, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_Y, P->nt, d_rows, n_rows, P->scrT64.p, nullptr, gp, 2); }
+		{ HA_LAUNCH(kHaB200KRidge, bs); k_pchol<double><<<b.count, kBlock, pchol_smem(b.rpl), bs>>>(wk, V, A, P->stats.p); }
 		{
 			HA_LAUNCH(kHaB200KJacobi64, bs);
 			if ((rc = launch_jacobi<double>(b.rpl, b.count, b.threads, b.smem, bs, wk, A, V, P->scrT.p, P->stats.p, P->uv.p, jp)) != kHaSuccess)
@@ -2492,7 +2524,7 @@ int pca_template_impl(const double *dms, int ns, int nt, int nv, const int32_t *
 		{ HA_LAUNCH(kHaB200KPca, st); k_pca_gram<16><<<nb, kBlock, 0, st>>>(dwe.p, P->idx.p, P->off.p, D.p, ns, nt, nv, eV.p); }
 		for (const Bucket &k : be) {
 			const SlWork *wk = dwes.p + k.first;
-			{ HA_LAUNCH(kHaB200KRidge, st); k_pchol<<<k.count, kBlock, pchol_smem(k.rpl), st>>>(wk, eV.p, eA.p, stE.p); }
+			{ HA_LAUNCH(kHaB200KRidge, st); k_pchol<double><<<k.count, kBlock, pchol_smem(k.rpl), st>>>(wk, eV.p, eA.p, stE.p); }
 			HA_LAUNCH(kHaB200KJacobi64, st);
 			if ((rc = launch_jacobi<double>(k.rpl, k.count, k.threads, k.smem, st, wk, eA.p, eV.p, T.p, stE.p, uvb.p, jpe)) != kHaSuccess)
 				return done(rc);
@@ -2705,6 +2737,7 @@ void ha_b200_plan_destroy(HaB200Plan *P) {
 		if (ch.d_w32) cudaFree(ch.d_w32);
 		if (ch.d_w64) cudaFree(ch.d_w64);
 		if (ch.d_weig) cudaFree(ch.d_weig);
+		if (ch.d_weig32) cudaFree(ch.d_weig32);
 		if (ch.d_tofs) cudaFree(ch.d_tofs);
 		if (ch.d_tcw) cudaFree(ch.d_tcw);
 		if (ch.tc_graph) cudaGraphExecDestroy(ch.tc_graph);
@@ -3037,6 +3070,13 @@ int64_t ha_b200_launch_count(void) { return g_launches; }
 void ha_b200_set_graphs(bool on) {
 	std::lock_guard<std::recursive_mutex> lk(g_mu);
 	g_graphs = on ? 1 : 0;
+}
+
+int ha_b200_plan_set_grid_precision(HaB200Plan *P, int32_t bits) {
+	std::lock_guard<std::recursive_mutex> lk(g_mu);
+	if (!P || (bits != 32 && bits != 64)) return kHaErrorArg;
+	P->grid_bits = bits;
+	return kHaSuccess;
 }
 
 int ha_b200_plan_tc_layout(const HaB200Plan *P, int32_t *smem_kb, int32_t *tuned, double *cand_ms) {

@@ -1,4 +1,6 @@
-// ha_b200_grid.cuh -- per-searchlight ridge grid search with cross-validated ensembles (float64).
+// ha_b200_grid.cuh -- per-searchlight ridge grid search with cross-validated ensembles.  The grid
+// kernels are templated on the arithmetic type Real: double for the float64 search, float for the
+// plain FP32 form (inputs, alphas and the output betas stay float64).
 //
 // Composition of the reference's ha_ridge_grid (csrc/ha_ridge.c:97-227) and ha_ensemble_ridge
 // (csrc/ha_ridge.c:229-345) applied to every searchlight: X = X[:, sl] and the searchlight's n
@@ -41,7 +43,7 @@ struct GridParams {
 	const int64_t *gbase;      // per work slot: base offset of the searchlight's grid scratch
 };
 
-// Per-searchlight layout of the grid scratch (float64 elements from the searchlight's base).
+// Per-searchlight layout of the grid scratch (Real elements from the searchlight's base).
 // Per model: V and Q with components in decreasing-lambda order (V column r = r-th component,
 // Q row r), lambda in that order and E = X_te V (mte x n, column-major, ld mte).  Per alpha (the
 // grid evaluation runs one CTA per searchlight and alpha): the models' cumulative test predictions
@@ -80,21 +82,21 @@ __device__ __forceinline__ GridLayout grid_layout(const GridParams &gp, int n) {
 }
 
 // A_s = X[rows, sl]^T Z[rows, sl] (Z = X for the Gram, Y for the cross-covariance) over one row
-// list with duplicates, float64, the k_xcov tiling with gathered rows.  Output column-major:
+// list with duplicates, in Real, the k_xcov tiling with gathered rows.  Output column-major:
 // mode 0 at Ascr + w.aofs with ncol columns (padding columns zero), mode 1 into the searchlight's
 // grid C block, mode 2 at Ascr + w.tofs (n x n).
-template <int KT>
+template <int KT, typename Real>
 __global__ void __launch_bounds__(256) k_xcov_rows(const SlWork *__restrict__ work, const int32_t *__restrict__ sl_idx,
                                                    const double *__restrict__ X, const double *__restrict__ Z, int nt,
-                                                   const int32_t *__restrict__ rows, int nrows, double *__restrict__ Ascr,
-                                                   double *__restrict__ Gscr, GridParams gp, int mode) {
+                                                   const int32_t *__restrict__ rows, int nrows, Real *__restrict__ Ascr,
+                                                   Real *__restrict__ Gscr, GridParams gp, int mode) {
 	const SlWork w = work[blockIdx.x];
 	const int n = w.n;
 	const int ncol = w.nblk * w.bsz;
 	const int32_t *sl = sl_idx + w.sofs;
-	double *A = mode == 1 ? Gscr + gp.gbase[w.slot] + grid_layout(gp, n).C : Ascr + (mode == 2 ? w.tofs : w.aofs);
-	__shared__ double xs[KT][64 + 1];
-	__shared__ double zs[KT][64 + 1];
+	Real *A = mode == 1 ? Gscr + gp.gbase[w.slot] + grid_layout(gp, n).C : Ascr + (mode == 2 ? w.tofs : w.aofs);
+	__shared__ Real xs[KT][64 + 1];
+	__shared__ Real zs[KT][64 + 1];
 	__shared__ int32_t vi[64], vj[64];
 	__shared__ int32_t rt[KT];
 	const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
@@ -108,11 +110,11 @@ __global__ void __launch_bounds__(256) k_xcov_rows(const SlWork *__restrict__ wo
 				const int j = j0 + threadIdx.x - 64;
 				vj[threadIdx.x - 64] = (j < n) ? sl[j] : -1;
 			}
-			double acc[4][4];
+			Real acc[4][4];
 #pragma unroll
 			for (int a = 0; a < 4; a++)
 #pragma unroll
-				for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
+				for (int b = 0; b < 4; b++) acc[a][b] = Real(0);
 			for (int t0 = 0; t0 < nrows; t0 += KT) {
 				__syncthreads();
 				if (threadIdx.x < KT) rt[threadIdx.x] = (t0 + threadIdx.x < nrows) ? rows[t0 + threadIdx.x] : -1;
@@ -121,13 +123,13 @@ __global__ void __launch_bounds__(256) k_xcov_rows(const SlWork *__restrict__ wo
 					const int r = e / KT, t = e - r * KT;
 					const int tt = rt[t];
 					const int v = vi[r], u = vj[r];
-					xs[t][r] = (v >= 0 && tt >= 0) ? X[(int64_t)v * nt + tt] : 0.0;
-					zs[t][r] = (u >= 0 && tt >= 0) ? Z[(int64_t)u * nt + tt] : 0.0;
+					xs[t][r] = (v >= 0 && tt >= 0) ? (Real)X[(int64_t)v * nt + tt] : Real(0);
+					zs[t][r] = (u >= 0 && tt >= 0) ? (Real)Z[(int64_t)u * nt + tt] : Real(0);
 				}
 				__syncthreads();
 #pragma unroll 4
 				for (int t = 0; t < KT; t++) {
-					double a[4], b[4];
+					Real a[4], b[4];
 #pragma unroll
 					for (int q = 0; q < 4; q++) {
 						a[q] = xs[t][ty + 16 * q];
@@ -152,7 +154,7 @@ __global__ void __launch_bounds__(256) k_xcov_rows(const SlWork *__restrict__ wo
 		}
 	}
 	if (mode == 0)
-		for (int64_t e = (int64_t)n * n + threadIdx.x; e < (int64_t)n * ncol; e += 256) A[e] = 0.0;
+		for (int64_t e = (int64_t)n * n + threadIdx.x; e < (int64_t)n * ncol; e += 256) A[e] = Real(0);
 }
 
 // Pivoted Cholesky G = sum_k r_k r_k^T (pivot = largest remaining diagonal, ties to the smaller
@@ -164,39 +166,41 @@ __global__ void __launch_bounds__(256) k_xcov_rows(const SlWork *__restrict__ wo
 // the rest zero), so G = Rt Rt^T; the number of columns (the numerical rank) goes to the stats.
 // The one-sided Jacobi rotations then run on Rt: its columns come in decreasing, graded norms and
 // only rank(G) of them are nonzero, which takes fewer sweeps than rotating G itself and needs no
-// accumulated rotations.  Dynamic shared memory: kPcholNb * 32 * RPL doubles (>= kPcholNb * n).
+// accumulated rotations.  Dynamic shared memory: kPcholNb * 32 * RPL elements (>= kPcholNb * n).
 constexpr int kPcholNb = 16;
 
-__global__ void __launch_bounds__(256) k_pchol(const SlWork *__restrict__ work, double *__restrict__ Gscr,
-                                               double *__restrict__ Rscr, SlStats *__restrict__ stats) {
-	extern __shared__ __align__(16) double pan[];  // [kPcholNb][n], indexed by vertex
+template <typename Real>
+__global__ void __launch_bounds__(256) k_pchol(const SlWork *__restrict__ work, Real *__restrict__ Gscr,
+                                               Real *__restrict__ Rscr, SlStats *__restrict__ stats) {
+	extern __shared__ __align__(16) unsigned char pan_raw[];
+	Real *pan = reinterpret_cast<Real *>(pan_raw);  // [kPcholNb][n], indexed by vertex
 	__shared__ int rem[kGridMaxN];                  // vertices not yet pivoted (positions 0 .. m-1)
-	__shared__ double dg[kGridMaxN];                // current Schur diagonal, by vertex
-	__shared__ double rv[32];
+	__shared__ Real dg[kGridMaxN];                // current Schur diagonal, by vertex
+	__shared__ Real rv[32];
 	__shared__ int ri[32], rpos[32];
-	__shared__ double s_tol, s_piv;
+	__shared__ Real s_tol, s_piv;
 	__shared__ int s_pos;
 	const SlWork w = work[blockIdx.x];
 	const int n = w.n, ncol = w.nblk * w.bsz;
-	double *S = Gscr + w.aofs;
-	double *Rt = Rscr + w.aofs;
+	Real *S = Gscr + w.aofs;
+	Real *Rt = Rscr + w.aofs;
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
 	for (int i = threadIdx.x; i < n; i += blockDim.x) {
 		rem[i] = i;
 		dg[i] = S[(int64_t)i * n + i];
 	}
-	for (int64_t e = threadIdx.x; e < (int64_t)n * ncol; e += blockDim.x) Rt[e] = 0.0;
+	for (int64_t e = threadIdx.x; e < (int64_t)n * ncol; e += blockDim.x) Rt[e] = Real(0);
 	__syncthreads();
 	{
-		double mx = 0.0;
+		Real mx = Real(0);
 		for (int i = threadIdx.x; i < n; i += blockDim.x) mx = fmax(mx, dg[i]);
 		for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
 		if (lane == 0) rv[warp] = mx;
 		__syncthreads();
 		if (threadIdx.x == 0) {
-			double t = 0.0;
+			Real t = Real(0);
 			for (int q = 0; q < nwarp; q++) t = fmax(t, rv[q]);
-			s_tol = (double)n * 2.220446049250313e-16 * t;
+			s_tol = (Real)n * Eps<Real>::v() * t;
 		}
 		__syncthreads();
 	}
@@ -206,15 +210,15 @@ __global__ void __launch_bounds__(256) k_pchol(const SlWork *__restrict__ work, 
 		int nbk = 0;  // columns of the current panel
 		for (; nbk < kPcholNb && k < n; nbk++, k++) {
 			// pivot: largest remaining diagonal (ties: smaller vertex index)
-			double bv = -1.0;
+			Real bv = Real(-1);
 			int bi = 0x7fffffff, bpos = 0;
 			for (int a = threadIdx.x; a < m; a += blockDim.x) {
 				const int v = rem[a];
-				const double d = dg[v];
+				const Real d = dg[v];
 				if (d > bv || (d == bv && v < bi)) { bv = d; bi = v; bpos = a; }
 			}
 			for (int o = 16; o > 0; o >>= 1) {
-				const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+				const Real ov = __shfl_xor_sync(0xffffffffu, bv, o);
 				const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
 				const int op = __shfl_xor_sync(0xffffffffu, bpos, o);
 				if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; bpos = op; }
@@ -222,7 +226,7 @@ __global__ void __launch_bounds__(256) k_pchol(const SlWork *__restrict__ work, 
 			if (lane == 0) { rv[warp] = bv; ri[warp] = bi; rpos[warp] = bpos; }
 			__syncthreads();
 			if (threadIdx.x == 0) {
-				double v = rv[0];
+				Real v = rv[0];
 				int vi = ri[0], pos = rpos[0];
 				for (int q = 1; q < nwarp; q++)
 					if (rv[q] > v || (rv[q] == v && ri[q] < vi)) { v = rv[q]; vi = ri[q]; pos = rpos[q]; }
@@ -235,13 +239,13 @@ __global__ void __launch_bounds__(256) k_pchol(const SlWork *__restrict__ work, 
 				break;
 			}
 			const int a = s_pos, p = rem[a];
-			const double rp = sqrt(s_piv);
-			double *rk = pan + (int64_t)nbk * n;
+			const Real rp = sqrt(s_piv);
+			Real *rk = pan + (int64_t)nbk * n;
 			for (int b = threadIdx.x; b < m; b += blockDim.x) {
 				const int v = rem[b];
-				double r = rp;
+				Real r = rp;
 				if (b != a) {
-					double x = S[(int64_t)p * n + v];
+					Real x = S[(int64_t)p * n + v];
 					for (int j = 0; j < nbk; j++) x -= pan[(int64_t)j * n + p] * pan[(int64_t)j * n + v];
 					r = x / rp;
 					dg[v] -= r * r;
@@ -258,10 +262,10 @@ __global__ void __launch_bounds__(256) k_pchol(const SlWork *__restrict__ work, 
 		// Schur complement on the remaining vertices with the panel's nbk columns
 		for (int c = warp; c < m; c += nwarp) {
 			const int u = rem[c];
-			double *Su = S + (int64_t)u * n;
+			Real *Su = S + (int64_t)u * n;
 			for (int b = lane; b < m; b += 32) {
 				const int v = rem[b];
-				double acc = 0.0;
+				Real acc = Real(0);
 				for (int j = 0; j < nbk; j++) acc += pan[(int64_t)j * n + v] * pan[(int64_t)j * n + u];
 				Su[v] -= acc;
 			}
@@ -285,36 +289,37 @@ __device__ __forceinline__ void rank_desc(const double *lam, int n, int *order) 
 }
 
 // One CV model of every searchlight: the eigenvectors (column-major, ld n) in the V scratch and
-// lambda in the u/v buffer come from the float64 Jacobi kernel in eigenvector mode run on the
+// lambda in the u/v buffer come from the Jacobi kernel (in Real) in eigenvector mode run on the
 // pivoted Cholesky factor of the Gram; C is in the grid scratch.
 // Stores V, lambda in decreasing-lambda order, Q = V^T C and E = X_te V for the model.
+template <typename Real>
 __global__ void __launch_bounds__(256) k_grid_model(const SlWork *__restrict__ work, const int32_t *__restrict__ sl_idx,
                                                     const double *__restrict__ X, const double *__restrict__ Y,
-                                                    const double *__restrict__ Vscr, const double *__restrict__ uvbuf,
-                                                    int model, double *__restrict__ Gscr, GridParams gp) {
-	__shared__ double ps[16][65], qs[16][65];
+                                                    const Real *__restrict__ Vscr, const double *__restrict__ uvbuf,
+                                                    int model, Real *__restrict__ Gscr, GridParams gp) {
+	__shared__ Real ps[16][65], qs[16][65];
 	__shared__ int order[kGridMaxN];
 	const SlWork w = work[blockIdx.x];
 	const int n = w.n;
 	const GridLayout L = grid_layout(gp, n);
-	double *base = Gscr + gp.gbase[w.slot];
-	const double *V = Vscr + w.aofs;
+	Real *base = Gscr + gp.gbase[w.slot];
+	const Real *V = Vscr + w.aofs;
 	const double *lam = uvbuf + w.uvofs;
 	const int32_t *sl = sl_idx + w.sofs;
 	const GridModel md = gp.mdl[model];
 	const int m = md.te_n;
 	const int64_t n2 = (int64_t)n * n, mn = (int64_t)gp.mte * n;
-	double *Vst = base + L.Vst + model * n2;
-	double *Qst = base + L.Qst + model * n2;
-	double *Lst = base + L.Lst + (int64_t)model * n;
-	double *Est = base + L.Est + model * mn;
-	double *Xte = base + L.Xte;
-	const double *C = base + L.C;
+	Real *Vst = base + L.Vst + model * n2;
+	Real *Qst = base + L.Qst + model * n2;
+	Real *Lst = base + L.Lst + (int64_t)model * n;
+	Real *Est = base + L.Est + model * mn;
+	Real *Xte = base + L.Xte;
+	const Real *C = base + L.C;
 	const int32_t *te = gp.rows + md.te_ofs;
 	if (model == 0)  // the targets on the tested rows, for the grid evaluation
 		for (int64_t e = threadIdx.x; e < (int64_t)gp.ntu * n; e += blockDim.x) {
 			const int j = (int)(e / gp.ntu), u = (int)(e - (int64_t)j * gp.ntu);
-			base[L.Yu + e] = Y[(int64_t)sl[j] * gp.nt + gp.urows[u]];
+			base[L.Yu + e] = (Real)Y[(int64_t)sl[j] * gp.nt + gp.urows[u]];
 		}
 	rank_desc(lam, n, order);
 	__syncthreads();
@@ -322,15 +327,15 @@ __global__ void __launch_bounds__(256) k_grid_model(const SlWork *__restrict__ w
 		const int r = (int)(e / n), i = (int)(e - (int64_t)r * n);
 		Vst[e] = V[(int64_t)order[r] * n + i];
 	}
-	for (int r = threadIdx.x; r < n; r += blockDim.x) Lst[r] = lam[order[r]];
+	for (int r = threadIdx.x; r < n; r += blockDim.x) Lst[r] = (Real)lam[order[r]];
 	// test rows of X, column-major by vertex: Xte[v * m + t]
 	for (int64_t e = threadIdx.x; e < (int64_t)m * n; e += blockDim.x) {
 		const int v = (int)(e / m), t = (int)(e - (int64_t)v * m);
-		Xte[e] = X[(int64_t)sl[v] * gp.nt + te[t]];
+		Xte[e] = (Real)X[(int64_t)sl[v] * gp.nt + te[t]];
 	}
 	__syncthreads();
-	GemmArgs<double, double> g;
-	g.d = nullptr; g.alpha = 1.0; g.E = nullptr; g.ei = 0; g.ej = 0; g.beta = 0.0;
+	GemmArgs<Real, Real> g;
+	g.d = nullptr; g.alpha = Real(1); g.E = nullptr; g.ei = 0; g.ej = 0; g.beta = Real(0);
 	// Q(r, j) = sum_k Vst(k, r) C(k, j), column-major ld n
 	g.M = n; g.N = n; g.K = n;
 	g.P = Vst; g.pk = 1; g.pi = n;
@@ -358,12 +363,13 @@ __device__ __forceinline__ void pc_chunk(const int32_t *npcs, int p, int K, int 
 }
 
 // Block-wide sum of one value per thread (256 threads), result in every thread.
-__device__ __forceinline__ double block_sum256(double v, double *red) {
+template <typename Real>
+__device__ __forceinline__ Real grid_block_sum(Real v, Real *red) {
 	v = warp_sum(v);
 	__syncthreads();
 	if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
 	__syncthreads();
-	double tot = 0.0;
+	Real tot = Real(0);
 	for (int q = 0; q < (int)(blockDim.x >> 5); q++) tot += red[q];
 	return tot;
 }
@@ -372,27 +378,28 @@ __device__ __forceinline__ double block_sum256(double v, double *red) {
 // cumulative test predictions over the PC chunks, their average per tested row and the squared
 // error over the tested rows and the targets, cost[alpha * n_npcs + p] (without the untested
 // rows, which k_grid_final adds).
-__global__ void __launch_bounds__(256) k_grid_eval(const SlWork *__restrict__ work, double *__restrict__ Gscr,
+template <typename Real>
+__global__ void __launch_bounds__(256) k_grid_eval(const SlWork *__restrict__ work, Real *__restrict__ Gscr,
                                                    GridParams gp) {
-	__shared__ double ps[16][65], qs[16][65];
-	__shared__ double cval[kGridMaxN];
-	__shared__ double red[32];
+	__shared__ Real ps[16][65], qs[16][65];
+	__shared__ Real cval[kGridMaxN];
+	__shared__ Real red[32];
 	const SlWork w = work[blockIdx.x];
 	const int a = blockIdx.y;
 	const int n = w.n;
 	const GridLayout L = grid_layout(gp, n);
-	double *base = Gscr + gp.gbase[w.slot];
+	Real *base = Gscr + gp.gbase[w.slot];
 	const int64_t n2 = (int64_t)n * n, mn = (int64_t)gp.mte * n;
 	const int ntu = gp.ntu;
-	double *Pma = base + L.Pm(a);
-	double *P = base + L.P(a, gp.models, gp.mte, n);
-	const double *Yu = base + L.Yu;
-	double *cost = base + L.cost;
-	const double al = gp.alphas[a];
-	GemmArgs<double, double> g;
-	g.alpha = 1.0;
-	g.beta = 1.0;
-	for (int64_t e = threadIdx.x; e < gp.models * mn; e += blockDim.x) Pma[e] = 0.0;
+	Real *Pma = base + L.Pm(a);
+	Real *P = base + L.P(a, gp.models, gp.mte, n);
+	const Real *Yu = base + L.Yu;
+	Real *cost = base + L.cost;
+	const Real al = (Real)gp.alphas[a];
+	GemmArgs<Real, Real> g;
+	g.alpha = Real(1);
+	g.beta = Real(1);
+	for (int64_t e = threadIdx.x; e < gp.models * mn; e += blockDim.x) Pma[e] = Real(0);
 	__syncthreads();
 	for (int p = 0; p < gp.n_npcs; p++) {
 		// Pm += E[:, r0:r1] diag(1 / (alpha + lambda)) Q[r0:r1, :] for every model
@@ -402,13 +409,13 @@ __global__ void __launch_bounds__(256) k_grid_eval(const SlWork *__restrict__ wo
 			int r0, r1;
 			pc_chunk(gp.npcs, p, min(md.tr_n, n), r0, r1);
 			if (r1 <= r0 || m == 0) continue;
-			const double *lam = base + L.Lst + (int64_t)mo * n;
+			const Real *lam = base + L.Lst + (int64_t)mo * n;
 			__syncthreads();
-			for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x) cval[r] = 1.0 / (al + lam[r]);
+			for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x) cval[r] = Real(1) / (al + lam[r]);
 			__syncthreads();
-			const double *E = base + L.Est + mo * mn;
-			const double *Q = base + L.Qst + mo * n2;
-			double *Pm = Pma + mo * mn;
+			const Real *E = base + L.Est + mo * mn;
+			const Real *Q = base + L.Qst + mo * n2;
+			Real *Pm = Pma + mo * mn;
 			g.M = m; g.N = n; g.K = r1 - r0;
 			g.P = E + (int64_t)r0 * m; g.pk = m; g.pi = 1;
 			g.Q = Q + r0; g.qk = 1; g.qj = n;
@@ -419,26 +426,26 @@ __global__ void __launch_bounds__(256) k_grid_eval(const SlWork *__restrict__ wo
 		}
 		// average over the models that test each row, then the squared error
 		__syncthreads();
-		for (int64_t e = threadIdx.x; e < (int64_t)ntu * n; e += blockDim.x) P[e] = 0.0;
+		for (int64_t e = threadIdx.x; e < (int64_t)ntu * n; e += blockDim.x) P[e] = Real(0);
 		for (int mo = 0; mo < gp.models; mo++) {
 			const GridModel md = gp.mdl[mo];
 			const int m = md.te_n;
-			const double *Pm = Pma + mo * mn;
+			const Real *Pm = Pma + mo * mn;
 			const int32_t *tp = gp.tpos + md.te_ofs;
 			__syncthreads();
 			for (int64_t e = threadIdx.x; e < (int64_t)m * n; e += blockDim.x) {
 				const int j = (int)(e / m), i = (int)(e - (int64_t)j * m);
 				const int u = tp[i];
-				P[(int64_t)j * ntu + u] += gp.winv[u] * Pm[e];
+				P[(int64_t)j * ntu + u] += (Real)gp.winv[u] * Pm[e];
 			}
 		}
 		__syncthreads();
-		double s = 0.0;
+		Real s = Real(0);
 		for (int64_t e = threadIdx.x; e < (int64_t)ntu * n; e += blockDim.x) {
-			const double d = Yu[e] - P[e];
+			const Real d = Yu[e] - P[e];
 			s += d * d;
 		}
-		s = block_sum256(s, red);
+		s = grid_block_sum(s, red);
 		if (threadIdx.x == 0) cost[a * gp.n_npcs + p] = s;
 	}
 }
@@ -447,29 +454,30 @@ __global__ void __launch_bounds__(256) k_grid_eval(const SlWork *__restrict__ wo
 // model-averaged beta, written float64 in the T layout (row-major for CSR output, column-major for
 // CSC), plus the cost row (cost_out may be null) with the untested rows' squared targets added
 // (their prediction is zero, csrc/ha_ridge.c:297-319).
+template <typename Real>
 __global__ void __launch_bounds__(256) k_grid_final(const SlWork *__restrict__ work, const int32_t *__restrict__ sl_idx,
-                                                    const double *__restrict__ Y, double *__restrict__ Gscr,
+                                                    const double *__restrict__ Y, Real *__restrict__ Gscr,
                                                     GridParams gp, double *__restrict__ Bout, int t_rowmajor,
                                                     int32_t *__restrict__ best_out, double *__restrict__ cost_out) {
-	__shared__ double ps[16][65], qs[16][65];
-	__shared__ double cval[kGridMaxN];
-	__shared__ double red[32];
+	__shared__ Real ps[16][65], qs[16][65];
+	__shared__ Real cval[kGridMaxN];
+	__shared__ Real red[32];
 	__shared__ int best;
 	const SlWork w = work[blockIdx.x];
 	const int n = w.n;
 	const int grid = gp.n_alphas * gp.n_npcs;
 	const GridLayout L = grid_layout(gp, n);
-	double *base = Gscr + gp.gbase[w.slot];
+	Real *base = Gscr + gp.gbase[w.slot];
 	const int32_t *sl = sl_idx + w.sofs;
 	const int64_t n2 = (int64_t)n * n;
-	const double *cost = base + L.cost;
-	double yc = 0.0;
+	const Real *cost = base + L.cost;
+	Real yc = Real(0);
 	for (int64_t e = threadIdx.x; e < (int64_t)gp.n_untested * n; e += blockDim.x) {
 		const int j = (int)(e / gp.n_untested), t = (int)(e - (int64_t)j * gp.n_untested);
-		const double y = Y[(int64_t)sl[j] * gp.nt + gp.untested[t]];
+		const Real y = (Real)Y[(int64_t)sl[j] * gp.nt + gp.untested[t]];
 		yc += y * y;
 	}
-	const double yconst = block_sum256(yc, red);
+	const Real yconst = grid_block_sum(yc, red);
 	if (threadIdx.x == 0) {
 		int b = 0;
 		for (int gi = 1; gi < grid; gi++)
@@ -479,26 +487,26 @@ __global__ void __launch_bounds__(256) k_grid_final(const SlWork *__restrict__ w
 	}
 	__syncthreads();
 	if (cost_out)
-		for (int gi = threadIdx.x; gi < grid; gi += blockDim.x) cost_out[(int64_t)w.s * grid + gi] = cost[gi] + yconst;
+		for (int gi = threadIdx.x; gi < grid; gi += blockDim.x) cost_out[(int64_t)w.s * grid + gi] = (double)(cost[gi] + yconst);
 	// beta of the winner: the cumulative PC chunks up to p of every model, averaged
 	const int ba = best / gp.n_npcs, bp = best % gp.n_npcs;
-	const double al = gp.alphas[ba];
-	double *acc = base + L.P(0, gp.models, gp.mte, n);  // n x n accumulator (column-major)
-	for (int64_t e = threadIdx.x; e < n2; e += blockDim.x) acc[e] = 0.0;
-	GemmArgs<double, double> g;
-	g.alpha = 1.0;
-	g.beta = 1.0;
+	const Real al = (Real)gp.alphas[ba];
+	Real *acc = base + L.P(0, gp.models, gp.mte, n);  // n x n accumulator (column-major)
+	for (int64_t e = threadIdx.x; e < n2; e += blockDim.x) acc[e] = Real(0);
+	GemmArgs<Real, Real> g;
+	g.alpha = Real(1);
+	g.beta = Real(1);
 	for (int mo = 0; mo < gp.models; mo++) {
 		const GridModel md = gp.mdl[mo];
-		const double *V = base + L.Vst + mo * n2;
-		const double *Q = base + L.Qst + mo * n2;
-		const double *lam = base + L.Lst + (int64_t)mo * n;
+		const Real *V = base + L.Vst + mo * n2;
+		const Real *Q = base + L.Qst + mo * n2;
+		const Real *lam = base + L.Lst + (int64_t)mo * n;
 		for (int p = 0; p <= bp; p++) {
 			int r0, r1;
 			pc_chunk(gp.npcs, p, min(md.tr_n, n), r0, r1);
 			if (r1 <= r0) continue;
 			__syncthreads();
-			for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x) cval[r] = 1.0 / (al + lam[r]);
+			for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x) cval[r] = Real(1) / (al + lam[r]);
 			__syncthreads();
 			// acc(i, j) += sum_r V(i, r) c_r Q(r, j)
 			g.M = n; g.N = n; g.K = r1 - r0;
@@ -515,7 +523,7 @@ __global__ void __launch_bounds__(256) k_grid_final(const SlWork *__restrict__ w
 	const int64_t ti = t_rowmajor ? n : 1, tj = t_rowmajor ? 1 : n;
 	for (int64_t e = threadIdx.x; e < n2; e += blockDim.x) {
 		const int j = (int)(e / n), i = (int)(e - (int64_t)j * n);
-		Bo[i * ti + j * tj] = acc[e] / gp.models;
+		Bo[i * ti + j * tj] = (double)(acc[e] / (Real)gp.models);
 	}
 }
 

@@ -161,6 +161,11 @@ def study(train_seeds=(1, 2, 3, 4), test_seed=5, nv=10242, step=4, size_lo=50, s
     sub = make_subject(test_seed, nv, step=step, size_lo=size_lo, size_hi=size_hi)
     gvals, gbest, gms = grid_labels(sub)
     gvals2, gbest2, gms2 = grid_labels(sub)  # second run: warm
+    # the plain FP32 form of the same full grid search (warm run timed)
+    sub.plan.set_grid_precision(32)
+    grid_labels(sub)
+    fvals32, fbest32, fms32 = grid_labels(sub)
+    sub.plan.set_grid_precision(64)
     lvals, choice, prob, lms = learned(sub, prm, min_prob)
     lvals, choice, prob, lms = learned(sub, prm, min_prob)
     p = prob.cpu().numpy()
@@ -171,6 +176,9 @@ def study(train_seeds=(1, 2, 3, 4), test_seed=5, nv=10242, step=4, size_lo=50, s
         "searchlights": int(sub.sls.count),
         "grid": {"ms": gms2, "searchlights_per_s": sub.sls.count / gms2 * 1e3,
                  "heldout_corr": heldout_correlation(sub, gvals2)},
+        "grid_fp32": {"ms": fms32, "searchlights_per_s": sub.sls.count / fms32 * 1e3,
+                      "heldout_corr": heldout_correlation(sub, fvals32),
+                      "winners_equal_fp64": float((fbest32.cpu().numpy() == gb).mean())},
         "learned": {"ms": lms, "searchlights_per_s": sub.sls.count / lms * 1e3,
                     "heldout_corr": heldout_correlation(sub, lvals), "fallback": int((~conf).sum()),
                     "proposal_matches_grid": float((ch[conf] == gb[conf]).mean()) if conf.any() else None},

@@ -149,6 +149,10 @@ class Plan:
         kb = np.ascontiguousarray(smem_kb, dtype=np.int32)
         L.check(self.lib.ha_b200_plan_set_tc_layout(self.handle, L.iptr(kb)), "ha_b200_plan_set_tc_layout")
 
+    def set_grid_precision(self, bits: int):
+        """Arithmetic of ridge_grid_device: 64 (float64, the default) or 32 (the plain FP32 form)."""
+        L.check(self.lib.ha_b200_plan_set_grid_precision(self.handle, int(bits)), "ha_b200_plan_set_grid_precision")
+
     def close(self):
         if self.handle:
             self.lib.ha_b200_plan_destroy(self.handle)

@@ -500,6 +500,61 @@ def test_ridge_grid_graph_matches_direct_launches(gpu, hlib):
     assert captured == direct and replayed == direct
 
 
+# Plain FP32 grid search (float32 Gram, factor, eigen solve and costs) vs float64: the cost of each
+# searchlight's winning grid point to GRID32_COST_REL.  Away from the winner, at the smallest alphas of
+# searchlights with more vertices than distinct training rows, the float32 rounding of V^T C on the
+# near-null components (about eps32 |C|) is amplified by 1 / alpha: those costs can be off by tens of
+# percent, which moves no winner.
+GRID32_COST_REL = 2e-4
+
+
+# resident and blocked float32 eigen solves, up to the 512-vertex limit (32 rows per lane x 16)
+@pytest.mark.parametrize("lo,hi", [(5, 30), (60, 140), (385, 512)])
+def test_ridge_grid_fp32_vs_fp64(gpu, lo, hi):
+    """The plain FP32 form of the grid search (ha_b200_plan_set_grid_precision(plan, 32)) against the
+    float64 search, which the tests above pin to the oracle at 1e-8: costs to float32 accuracy, and
+    every FP32 winner optimal to that accuracy; switching back gives the float64 bits again."""
+    import torch
+    w, Y = _grid_case(21, 642, 120, lo, hi)
+    tr, te = H.ensemble_indices(120, 1, 4, 6, 3, 17)
+    alphas, npcs = np.logspace(-3, 3, 5), [5, 20, 10000]
+    plan = Plan(w.nt, w.nv, w.sls.indices, w.sls.offsets, w.sls.dists, w.sls.radius)
+    dX = torch.from_numpy(np.asfortranarray(w.X).ravel(order="F")).cuda()
+    dY = torch.from_numpy(np.asfortranarray(Y).ravel(order="F")).cuda()
+    S, G = w.sls.count, len(alphas) * len(npcs)
+
+    def run(bits):
+        plan.set_grid_precision(bits)
+        vals = torch.zeros(plan.nnz, dtype=torch.float64, device="cuda")
+        best = torch.full((S,), -1, dtype=torch.int32, device="cuda")
+        cost = torch.zeros(S * G, dtype=torch.float64, device="cuda")
+        plan.ridge_grid_device(dX.data_ptr(), dY.data_ptr(), vals.data_ptr(), best.data_ptr(), alphas, npcs, tr, te,
+                               d_cost=cost.data_ptr())
+        torch.cuda.synchronize()
+        return vals.cpu().numpy(), best.cpu().numpy(), cost.cpu().numpy().reshape(S, G)
+
+    v64, b64, c64 = run(64)
+    v32, b32, c32 = run(32)
+    v64b, b64b, c64b = run(64)
+    plan.close()
+    assert np.array_equal(v64, v64b) and np.array_equal(b64, b64b) and np.array_equal(c64, c64b)
+    rows = np.arange(S)
+    cerr = float(np.max(np.abs(c32 - c64) / c64))
+    werr = float(np.max(np.abs(c32[rows, b64] - c64[rows, b64]) / c64[rows, b64]))
+    regret = float(np.max(c64[rows, b32] / c64.min(axis=1) - 1.0))
+    agree = float(np.mean(b32 == b64))
+    same = b32 == b64
+    print(f"fp32 grid: cost rel err at the winner max {werr:.2e} (all grid points {cerr:.2e}), "
+          f"winner regret max {regret:.2e}, winners equal {agree:.3f}")
+    assert np.all(np.isfinite(c32)) and werr <= GRID32_COST_REL
+    assert regret <= 2 * GRID32_COST_REL
+    assert agree >= 0.9 and b32.min() >= 0
+    if same.all():
+        berr = relf(v32, v64)
+        print(f"fp32 grid: betas rel-Frobenius {berr:.2e}")
+        assert berr <= 1e-2
+
+
 def test_ridge_grid_device_deterministic(gpu):
     import torch
     w, Y = _grid_case(8, 642, 120, 10, 40)
