@@ -1093,20 +1093,29 @@ def config5_learned(args):
     40962-vertex grid workload.  The perceptron is trained on the GPU on the full grid's winners for
     four training subjects (every 16th searchlight each), then the held-out subject (every 4th
     searchlight, 10240) runs through the full grid and through the learned form (proposal where its
-    probability is at least 0.6, the full grid elsewhere); warm runs are timed.  The generator's noise
+    probability is at least 0.6, the full grid elsewhere); warm runs are timed.  The value is the
+    mixed-precision learned form (float32 eigen solve, proposal fit and fallback grid, bf16
+    inference), set against the plain FP32 full grid on the same searchlights; the float64 full grid
+    and the float64 learned form are sub-fields.  The generator's noise
     amplitude varies from 0.2 to 6 over the sphere so that the best grid point varies between
     searchlights (with homogeneous noise one grid point wins almost everywhere)."""
     from hyperalignment_b200 import learned as LR
     res = LR.study(nv=40962, step=4, train_step=16, size_lo=50, size_hi=500, epochs=60, log=lambda *a: None)
-    g, l, g32 = res["grid"], res["learned"], res["grid_fp32"]
-    return {"value": l["searchlights_per_s"], "unit": UNIT, "ms_per_step": l["ms"],
-            "full_grid": {"value": g["searchlights_per_s"], "ms_per_step": g["ms"], "heldout_corr": g["heldout_corr"]},
-            "speedup_over_full_grid": l["searchlights_per_s"] / g["searchlights_per_s"],
+    g, l, g32, m = res["grid"], res["learned"], res["grid_fp32"], res["learned_fp32"]
+    return {"value": m["searchlights_per_s"], "unit": UNIT, "ms_per_step": m["ms"],
+            "form": "mixed-precision learned form: float32 eigen solve, features, proposal fit and fallback grid; "
+                    "bf16 inference; float64 inputs, betas and reduction",
             "plain_fp32_grid": {"value": g32["searchlights_per_s"], "ms_per_step": g32["ms"],
                                 "heldout_corr": g32["heldout_corr"], "winners_equal_fp64": g32["winners_equal_fp64"]},
-            "speedup_over_plain_fp32_grid": l["searchlights_per_s"] / g32["searchlights_per_s"],
-            "heldout_corr": l["heldout_corr"], "heldout_corr_minus_grid": l["heldout_corr"] - g["heldout_corr"],
-            "fallback_searchlights": l["fallback"], "proposal_matches_grid": l["proposal_matches_grid"],
+            "speedup_over_plain_fp32_grid": m["searchlights_per_s"] / g32["searchlights_per_s"],
+            "heldout_corr": m["heldout_corr"], "heldout_corr_minus_plain_fp32_grid": m["heldout_corr"] - g32["heldout_corr"],
+            "fallback_searchlights": m["fallback"], "choices_equal_fp64_learned": m["choices_equal_fp64_learned"],
+            "full_grid": {"value": g["searchlights_per_s"], "ms_per_step": g["ms"], "heldout_corr": g["heldout_corr"]},
+            "learned_fp64": {"value": l["searchlights_per_s"], "ms_per_step": l["ms"], "heldout_corr": l["heldout_corr"],
+                             "fallback_searchlights": l["fallback"],
+                             "speedup_over_full_grid": l["searchlights_per_s"] / g["searchlights_per_s"]},
+            "heldout_corr_minus_grid": m["heldout_corr"] - g["heldout_corr"],
+            "proposal_matches_grid": l["proposal_matches_grid"],
             "fixed_point": res["fixed_point"], "train": res["train"],
             "config": {"workload": "ridge_grid_learned", "nv": 40962, "nt": 500, "fit_rows": 400, "eval_rows": 100,
                        "heldout_searchlights": res["searchlights"], "train_subset": "every 16th, seeds 1-4",

@@ -1747,10 +1747,10 @@ int grid_chunk_launch(HaB200Plan *P, Chunk &ch, const double *d_X, const double 
 
 // One chunk's grid search enqueued directly (sub-batch plan, scratch and offsets, launches).
 int grid_chunk(HaB200Plan *P, Chunk &ch, const double *d_X, const double *d_Y, const GridSpec &gs,
-               const GridParams &gp, int rowmajor, int32_t *d_best, double *d_cost, cudaStream_t st) {
+               const GridParams &gp, bool fp32, int rowmajor, int32_t *d_best, double *d_cost, cudaStream_t st) {
 	std::vector<GridBatch> bt;
 	std::vector<int64_t> gbase;
-	grid_plan_chunk(ch, gp, false, bt, gbase);
+	grid_plan_chunk(ch, gp, fp32, bt, gbase);
 	int64_t mx = 1;
 	for (const auto &b : bt) mx = std::max(mx, b.total);
 	int rc;
@@ -1758,7 +1758,7 @@ int grid_chunk(HaB200Plan *P, Chunk &ch, const double *d_X, const double *d_Y, c
 	if ((rc = P->gbase.ensure(std::max<size_t>(gbase.size(), 1))) != kHaSuccess) return rc;
 	HA_CUDA(cudaMemcpyAsync(P->gbase.p, gbase.data(), gbase.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st));
 	HA_CUDA(cudaStreamSynchronize(st));  // the host vector goes out of scope
-	return grid_chunk_launch(P, ch, d_X, d_Y, gs, gp, false, bt, P->gbase.p, rowmajor, d_best, d_cost, st);
+	return grid_chunk_launch(P, ch, d_X, d_Y, gs, gp, fp32, bt, P->gbase.p, rowmajor, d_best, d_cost, st);
 }
 
 int run_ridge_grid(HaB200Plan *P, const double *d_X, const double *d_Y, const GridSpec &gs, int out_kind,
@@ -1850,32 +1850,45 @@ int run_ridge_grid(HaB200Plan *P, const double *d_X, const double *d_Y, const Gr
 
 // Eigen decomposition of every searchlight's Gram over the given rows (device list, n_rows
 // entries): the pivoted Cholesky factor and the eigenvector-mode Jacobi leave the eigenvectors in
-// the V scratch and the eigenvalues in the u/v buffer; with d_C, C = X^T Y over the same rows goes
-// to the float64 T scratch.  Then the features of the chunk's searchlights.
+// the V scratch and the eigenvalues in the u/v buffer; with d_Y, C = X^T Y over the same rows goes
+// to the T scratch of the arithmetic type (float64 T scratch for double, float32 T scratch for
+// float).  Then the features of the chunk's searchlights.
+template <typename Real>
 int eigen_chunk(HaB200Plan *P, Chunk &ch, const double *d_X, const double *d_Y, const int32_t *d_rows, int n_rows,
                 float *d_feat, cudaStream_t st) {
+	constexpr bool f32 = sizeof(Real) == 4;
 	GridParams gp = {};
 	const JacobiParams jp = eig_params(false);
-	double *A = P->scrA.p, *V = P->scrV.p;
+	Real *A = reinterpret_cast<Real *>(P->scrA.p), *V = reinterpret_cast<Real *>(P->scrV.p);
+	Real *Cout = f32 ? reinterpret_cast<Real *>(P->scrT.p) : reinterpret_cast<Real *>(P->scrT64.p);
+	const std::vector<Bucket> &beig = f32 ? ch.beig32 : ch.beig;
+	const std::vector<SlWork> &items = f32 ? ch.weig32 : ch.weig;
+	SlWork *d_work = f32 ? ch.d_weig32 : ch.d_weig;
 	int rc;
 	if ((rc = g_fan.begin(st)) != kHaSuccess) return rc;
-	for (size_t bi = 0; bi < ch.beig.size(); bi++) {
-		const Bucket &b = ch.beig[bi];
+	for (size_t bi = 0; bi < beig.size(); bi++) {
+		const Bucket &b = beig[bi];
 		const cudaStream_t bs = g_fan.at((int)bi);
-		const SlWork *wk = ch.d_weig + b.first;
-		{ HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16, double><<<b.count, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_X, P->nt, d_rows, n_rows, V, nullptr, gp, 0); }
-		if (d_Y) { HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16, double><<<b.count, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_Y, P->nt, d_rows, n_rows, P->scrT64.p, nullptr, gp, 2); }
-		{ HA_LAUNCH(kHaB200KRidge, bs); k_pchol<double><<<b.count, kBlock, pchol_smem(b.rpl), bs>>>(wk, V, A, P->stats.p); }
+		const SlWork *wk = d_work + b.first;
+		{ HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16, Real><<<b.count, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_X, P->nt, d_rows, n_rows, V, nullptr, gp, 0); }
+		if (d_Y) { HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16, Real><<<b.count, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_Y, P->nt, d_rows, n_rows, Cout, nullptr, gp, 2); }
+		{ HA_LAUNCH(kHaB200KRidge, bs); k_pchol<Real><<<b.count, kBlock, pchol_smem(b.rpl, sizeof(Real)), bs>>>(wk, V, A, P->stats.p); }
 		{
-			HA_LAUNCH(kHaB200KJacobi64, bs);
-			if ((rc = launch_jacobi<double>(b.rpl, b.count, b.threads, b.smem, bs, wk, A, V, P->scrT.p, P->stats.p, P->uv.p, jp)) != kHaSuccess)
+			HA_LAUNCH(f32 ? kHaB200KJacobi32 : kHaB200KJacobi64, bs);
+			if ((rc = launch_jacobi<Real>(b.rpl, b.count, b.threads, b.smem, bs, wk, A, V, P->scrT.p, P->stats.p, P->uv.p, jp)) != kHaSuccess)
 				return rc;
 		}
 	}
 	if ((rc = g_fan.end(st)) != kHaSuccess) return rc;
-	{ HA_LAUNCH(kHaB200KGrid, st); k_features<<<(int)ch.weig.size(), kBlock, 0, st>>>(ch.d_weig, P->uv.p, d_feat); }
+	{ HA_LAUNCH(kHaB200KGrid, st); k_features<<<(int)items.size(), kBlock, 0, st>>>(d_work, P->uv.p, d_feat); }
 	HA_CUDA(cudaGetLastError());
 	return kHaSuccess;
+}
+
+int eigen_chunk_any(HaB200Plan *P, Chunk &ch, const double *d_X, const double *d_Y, const int32_t *d_rows, int n_rows,
+                    float *d_feat, cudaStream_t st) {
+	return P->grid_bits == 32 ? eigen_chunk<float>(P, ch, d_X, d_Y, d_rows, n_rows, d_feat, st)
+	                          : eigen_chunk<double>(P, ch, d_X, d_Y, d_rows, n_rows, d_feat, st);
 }
 
 int upload_rows(HaB200Plan *P, const int32_t *rows, int n_rows, cudaStream_t st) {
@@ -1898,7 +1911,7 @@ int run_ridge_features(HaB200Plan *P, const double *d_X, const int32_t *rows, in
 	for (size_t c = 0; c < P->chunks.size(); c++) {
 		Chunk &ch = P->chunks[c];
 		HA_CUDA(cudaMemsetAsync(P->stats.p, 0, (size_t)(ch.s1 - ch.s0) * sizeof(SlStats), st));
-		if ((rc = eigen_chunk(P, ch, d_X, nullptr, P->gfit.p, n_rows, d_feat, st)) != kHaSuccess) return rc;
+		if ((rc = eigen_chunk_any(P, ch, d_X, nullptr, P->gfit.p, n_rows, d_feat, st)) != kHaSuccess) return rc;
 	}
 	return kHaSuccess;
 }
@@ -1910,6 +1923,7 @@ int run_ridge_learned(HaB200Plan *P, const double *d_X, const double *d_Y, const
                       const GridSpec &gs, const float *d_params, float min_prob, int out_kind, double *d_vals,
                       int32_t *d_choice, float *d_prob, cudaStream_t st) {
 	const int rowmajor = out_kind == kHaB200OutCSR ? 1 : 0;
+	const bool fp32 = P->grid_bits == 32;
 	const int C = (int)(gs.alphas.size() * gs.npcs.size());
 	int rc;
 	if ((rc = mlp_check(C)) != kHaSuccess) return rc;
@@ -1924,11 +1938,17 @@ int run_ridge_learned(HaB200Plan *P, const double *d_X, const double *d_Y, const
 		Chunk &ch = P->chunks[c];
 		const int nsl = ch.s1 - ch.s0;
 		HA_CUDA(cudaMemsetAsync(P->stats.p, 0, (size_t)nsl * sizeof(SlStats), st));
-		if ((rc = eigen_chunk(P, ch, d_X, d_Y, P->gfit.p, n_rows, P->gfeat.p, st)) != kHaSuccess) return rc;
+		if ((rc = eigen_chunk_any(P, ch, d_X, d_Y, P->gfit.p, n_rows, P->gfeat.p, st)) != kHaSuccess) return rc;
 		if ((rc = ha_b200_mlp_infer(d_params, C, P->gfeat.p + (size_t)ch.s0 * (kFeatSv + 1), nsl, d_choice + ch.s0,
 		                            d_prob + ch.s0, st)) != kHaSuccess)
 			return rc;
-		{ HA_LAUNCH(kHaB200KGrid, st); k_proposed_fit<<<(int)ch.weig.size(), kBlock, 0, st>>>(ch.d_weig, P->scrV.p, P->uv.p, P->scrA.p, P->scrT64.p, d_choice, d_prob, min_prob, gp.alphas, gp.npcs, gp.n_npcs, n_rows, rowmajor); }
+		if (fp32) {
+			HA_LAUNCH(kHaB200KGrid, st);
+			k_proposed_fit<float><<<(int)ch.weig32.size(), kBlock, 0, st>>>(ch.d_weig32, reinterpret_cast<const float *>(P->scrV.p), P->uv.p, reinterpret_cast<float *>(P->scrA.p), P->scrT.p, P->scrT64.p, d_choice, d_prob, min_prob, gp.alphas, gp.npcs, gp.n_npcs, n_rows, rowmajor);
+		} else {
+			HA_LAUNCH(kHaB200KGrid, st);
+			k_proposed_fit<double><<<(int)ch.weig.size(), kBlock, 0, st>>>(ch.d_weig, P->scrV.p, P->uv.p, P->scrA.p, P->scrT64.p, P->scrT64.p, d_choice, d_prob, min_prob, gp.alphas, gp.npcs, gp.n_npcs, n_rows, rowmajor);
+		}
 		HA_CUDA(cudaGetLastError());
 		// searchlights below the threshold: the full grid search
 		hprob.resize((size_t)nsl);
@@ -1938,19 +1958,23 @@ int run_ridge_learned(HaB200Plan *P, const double *d_X, const double *d_Y, const
 		Chunk fb;
 		fb.s0 = ch.s0;
 		fb.s1 = ch.s1;
-		for (const Bucket &b : ch.beig) {
+		const std::vector<Bucket> &cb = fp32 ? ch.beig32 : ch.beig;
+		const std::vector<SlWork> &cw = fp32 ? ch.weig32 : ch.weig;
+		std::vector<SlWork> &fw = fp32 ? fb.weig32 : fb.weig;
+		std::vector<Bucket> &fbk = fp32 ? fb.beig32 : fb.beig;
+		for (const Bucket &b : cb) {
 			Bucket nb = b;
-			nb.first = (int)fb.weig.size();
+			nb.first = (int)fw.size();
 			for (int i = b.first; i < b.first + b.count; i++)
-				if (hprob[(size_t)(ch.weig[i].s - ch.s0)] < min_prob) fb.weig.push_back(ch.weig[i]);
-			nb.count = (int)fb.weig.size() - nb.first;
-			if (nb.count > 0) fb.beig.push_back(nb);
+				if (hprob[(size_t)(cw[i].s - ch.s0)] < min_prob) fw.push_back(cw[i]);
+			nb.count = (int)fw.size() - nb.first;
+			if (nb.count > 0) fbk.push_back(nb);
 		}
-		if (!fb.weig.empty()) {
-			if ((rc = P->gwork.ensure(fb.weig.size())) != kHaSuccess) return rc;
-			HA_CUDA(cudaMemcpyAsync(P->gwork.p, fb.weig.data(), fb.weig.size() * sizeof(SlWork), cudaMemcpyHostToDevice, st));
-			fb.d_weig = P->gwork.p;
-			if ((rc = grid_chunk(P, fb, d_X, d_Y, gs, gp, rowmajor, d_choice, nullptr, st)) != kHaSuccess) return rc;
+		if (!fw.empty()) {
+			if ((rc = P->gwork.ensure(fw.size())) != kHaSuccess) return rc;
+			HA_CUDA(cudaMemcpyAsync(P->gwork.p, fw.data(), fw.size() * sizeof(SlWork), cudaMemcpyHostToDevice, st));
+			(fp32 ? fb.d_weig32 : fb.d_weig) = P->gwork.p;
+			if ((rc = grid_chunk(P, fb, d_X, d_Y, gs, gp, fp32, rowmajor, d_choice, nullptr, st)) != kHaSuccess) return rc;
 		}
 		if ((rc = reduce_chunk64(P, ch, out_kind, d_vals, st)) != kHaSuccess) return rc;
 	}

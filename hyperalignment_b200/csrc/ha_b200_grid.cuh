@@ -555,26 +555,29 @@ __global__ void __launch_bounds__(256) k_features(const SlWork *__restrict__ wor
 // (csrc/ha_ridge.c:97-227) restricted to one (alpha, PC count), with mult_k the number of PC
 // chunks up to p that contain component k's rank (clipped at K = min(rows, n)).  V (eigenvectors,
 // column-major ld n) and lambda come from the eigenvector-mode Jacobi, C = X_fit^T Y_fit is at
-// Bout + w.tofs and is replaced by beta (T layout); Q = V^T C goes to the A scratch.
-__global__ void __launch_bounds__(256) k_proposed_fit(const SlWork *__restrict__ work, const double *__restrict__ Vscr,
-                                                      const double *__restrict__ uvbuf, double *__restrict__ Ascr,
-                                                      double *__restrict__ Bout, const int32_t *__restrict__ cls,
+// Cin + w.tofs; beta goes to Bout + w.tofs (float64, T layout; Cin may be Bout: C is read first);
+// Q = V^T C goes to the A scratch.  Real is the arithmetic type of the products.
+template <typename Real>
+__global__ void __launch_bounds__(256) k_proposed_fit(const SlWork *__restrict__ work, const Real *__restrict__ Vscr,
+                                                      const double *__restrict__ uvbuf, Real *__restrict__ Ascr,
+                                                      const Real *Cin, double *Bout, const int32_t *__restrict__ cls,
                                                       const float *__restrict__ prob, float min_prob,
                                                       const double *__restrict__ alphas, const int32_t *__restrict__ npcs,
                                                       int n_npcs, int rows, int t_rowmajor) {
-	__shared__ double ps[16][65], qs[16][65];
+	__shared__ Real ps[16][65], qs[16][65];
 	__shared__ int order[kGridMaxN];
-	__shared__ double cval[kGridMaxN];
+	__shared__ Real cval[kGridMaxN];
 	const SlWork w = work[blockIdx.x];
 	if (prob[w.s] < min_prob) return;
 	const int n = w.n;
-	const double *V = Vscr + w.aofs;
+	const Real *V = Vscr + w.aofs;
 	const double *lam = uvbuf + w.uvofs;
-	double *Q = Ascr + w.aofs;
+	Real *Q = Ascr + w.aofs;
+	const Real *Cs = Cin + w.tofs;
 	double *B = Bout + w.tofs;
 	const int g = cls[w.s];
 	const int a = g / n_npcs, p = g - a * n_npcs;
-	const double al = alphas[a];
+	const Real al = (Real)alphas[a];
 	const int K = min(rows, n);
 	rank_desc(lam, n, order);
 	__syncthreads();
@@ -586,22 +589,26 @@ __global__ void __launch_bounds__(256) k_proposed_fit(const SlWork *__restrict__
 			mult += (r >= r0 && r < r1);
 		}
 		const int k = order[r];
-		cval[k] = mult ? mult / (al + lam[k]) : 0.0;
+		cval[k] = mult ? (Real)mult / (al + (Real)lam[k]) : Real(0);
 	}
-	GemmArgs<double, double> gm;
-	gm.d = nullptr; gm.alpha = 1.0; gm.E = nullptr; gm.ei = 0; gm.ej = 0; gm.beta = 0.0;
+	GemmArgs<Real, Real> gm;
+	gm.d = nullptr; gm.alpha = Real(1); gm.E = nullptr; gm.ei = 0; gm.ej = 0; gm.beta = Real(0);
 	// Q(k, j) = sum_i V(i, k) C(i, j)
 	gm.M = n; gm.N = n; gm.K = n;
 	gm.P = V; gm.pk = 1; gm.pi = n;
-	gm.Q = B; gm.qk = 1; gm.qj = n;
+	gm.Q = Cs; gm.qk = 1; gm.qj = n;
 	gm.C = Q; gm.ci = 1; gm.cj = n;
 	block_gemm(gm, ps, qs);
+	__syncthreads();  // every read of C (which may share memory with beta) is done
 	// beta(i, j) = sum_k V(i, k) c_k Q(k, j), in the T layout
 	gm.P = V; gm.pk = n; gm.pi = 1;
 	gm.Q = Q; gm.qk = 1; gm.qj = n;
 	gm.d = cval;
-	gm.C = B; gm.ci = t_rowmajor ? n : 1; gm.cj = t_rowmajor ? 1 : n;
-	block_gemm(gm, ps, qs);
+	GemmArgs<Real, double> gb;
+	gb.M = gm.M; gb.N = gm.N; gb.K = gm.K; gb.P = gm.P; gb.pk = gm.pk; gb.pi = gm.pi; gb.Q = gm.Q; gb.qk = gm.qk;
+	gb.qj = gm.qj; gb.d = gm.d; gb.alpha = Real(1); gb.E = nullptr; gb.ei = 0; gb.ej = 0; gb.beta = Real(0);
+	gb.C = B; gb.ci = t_rowmajor ? n : 1; gb.cj = t_rowmajor ? 1 : n;
+	block_gemm(gb, ps, qs);
 }
 
 }  // namespace hab200

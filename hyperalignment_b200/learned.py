@@ -168,6 +168,13 @@ def study(train_seeds=(1, 2, 3, 4), test_seed=5, nv=10242, step=4, size_lo=50, s
     sub.plan.set_grid_precision(64)
     lvals, choice, prob, lms = learned(sub, prm, min_prob)
     lvals, choice, prob, lms = learned(sub, prm, min_prob)
+    # the mixed-precision learned form: float32 eigen solve, features, proposal fit and fallback
+    # grid, bf16 inference (warm run timed)
+    sub.plan.set_grid_precision(32)
+    learned(sub, prm, min_prob)
+    mvals, mchoice, mprob, mms = learned(sub, prm, min_prob)
+    sub.plan.set_grid_precision(64)
+    mp = mprob.cpu().numpy()
     p = prob.cpu().numpy()
     ch = choice.cpu().numpy()
     gb = gbest2.cpu().numpy()
@@ -182,6 +189,9 @@ def study(train_seeds=(1, 2, 3, 4), test_seed=5, nv=10242, step=4, size_lo=50, s
         "learned": {"ms": lms, "searchlights_per_s": sub.sls.count / lms * 1e3,
                     "heldout_corr": heldout_correlation(sub, lvals), "fallback": int((~conf).sum()),
                     "proposal_matches_grid": float((ch[conf] == gb[conf]).mean()) if conf.any() else None},
+        "learned_fp32": {"ms": mms, "searchlights_per_s": sub.sls.count / mms * 1e3,
+                         "heldout_corr": heldout_correlation(sub, mvals), "fallback": int((mp < min_prob).sum()),
+                         "choices_equal_fp64_learned": float((mchoice.cpu().numpy() == ch).mean())},
         "train": {"examples": int(F.shape[0]), "final_loss": loss, "epochs": epochs},
     }
     # the method without the network: one fixed grid point (the training winners' mode)

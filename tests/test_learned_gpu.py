@@ -6,6 +6,8 @@ Checks, against the CPU oracle on small cases:
     rows (csrc/ha_ridge.c:97-227): relative 1e-8
   * below the probability threshold the full CV grid search runs: identical to the grid entry
   * a mix of both goes through the fallback mask correctly
+  * the same with the plan's grid precision at 32 (float32 eigen solve, fit and fallback grid):
+    features 1e-4, the proposal's fit 1e-4, the fallback identical to the float32 grid entry
 """
 
 import ctypes
@@ -118,3 +120,34 @@ def test_mixed_proposals_and_fallbacks(sub):
                                                 np.zeros(indices.size), ALPHAS, NPCS, sub.train_li, sub.test_li, wsub)
     if np.array_equal(rbest, gb[~conf]):
         assert relf(vals, ref + d2) <= 1e-8
+
+
+# ---- the mixed-precision learned form: float32 eigen solve, proposal fit and fallback grid ----
+
+@pytest.fixture
+def fp32(sub):
+    sub.plan.set_grid_precision(32)
+    yield sub
+    sub.plan.set_grid_precision(64)
+
+
+def test_fp32_features_match_oracle(fp32):
+    # the network's input: singular values over the largest from the float32 eigen solve
+    f = LR.features(fp32).cpu().numpy().astype(np.float64)
+    ref = O.ridge_features(fp32.w.X, fp32.sls.indices, fp32.sls.offsets, fp32.fit_rows)
+    assert relf(f, ref) <= 1e-4
+
+
+def test_fp32_confident_proposal_is_the_grid_point_fit(fp32):
+    g = 7
+    vals, choice, prob = _run_learned(fp32, _forced(g), 0.5)
+    assert (choice == g).all() and (prob > 0.99).all()
+    ref = _oracle_at(fp32, choice, np.ones(fp32.sls.count, dtype=bool))
+    assert relf(vals, ref) <= 1e-4
+
+
+def test_fp32_fallback_is_the_fp32_full_grid(fp32):
+    gvals, gbest, _ = LR.grid_labels(fp32, ALPHAS, NPCS)
+    vals, choice, prob = _run_learned(fp32, _forced(2), 2.0)
+    assert np.array_equal(vals, gvals.cpu().numpy())
+    assert np.array_equal(choice, gbest.cpu().numpy())
