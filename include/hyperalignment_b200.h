@@ -333,15 +333,19 @@ int ha_b200_plan_ridge_grid_device(
 	int out_kind, double *d_values, int32_t *d_best, double *d_cost, void *stream);
 
 /*
- * Arithmetic of this plan's ha_b200_plan_ridge_grid_device: bits 64 (the default) computes every
- * Gram, factor, eigen decomposition, prediction and cost in float64; bits 32 is the plain FP32
- * form of the same grid search (float32 Gram and cross-covariance over the training rows, pivoted
- * Cholesky, eigenvector-mode Jacobi, per-model products, predictions and costs; the inputs, the
- * winners' betas and the reduction stay float64).  The same composition of ha_ridge_grid and
- * ha_ensemble_ridge (csrc/ha_ridge.c:97-345); its costs carry float32 rounding, so grid points
- * whose costs differ by less than about 1e-5 relative can pick another winner.  Other entry points
- * (the host ha_searchlight_ridge_grid_b200, the learned form and its fallback) stay float64.
- * Returns kHaErrorArg for other values of bits.
+ * Arithmetic of this plan's ridge grid search and learned form.  bits 64 (the default) computes
+ * every Gram, factor, eigen decomposition, prediction and cost in float64.  bits 32 is the plain
+ * FP32 form: float32 Gram and cross-covariance over the rows, pivoted Cholesky, eigenvector-mode
+ * Jacobi, per-model products, predictions and costs in ha_b200_plan_ridge_grid_device, and the
+ * float32 eigen solve, features, proposal fit and fallback grid in
+ * ha_b200_plan_ridge_learned_device and ha_b200_plan_ridge_features_device.  The inputs, the
+ * winners' betas and the reduction stay float64.  It is the same composition of ha_ridge_grid and
+ * ha_ensemble_ridge (csrc/ha_ridge.c:97-345).  Its costs carry float32 rounding: grid points whose
+ * costs differ by less than about 1e-5 relative can pick another winner, and at the smallest
+ * alphas of searchlights with more vertices than distinct training rows the cost of a losing grid
+ * point can be far off (the rounding of V^T C on near-null components, amplified by 1 / alpha).
+ * The host entry ha_searchlight_ridge_grid_b200 stays float64.  Returns kHaErrorArg for other
+ * values of bits.
  */
 int ha_b200_plan_set_grid_precision(HaB200Plan *plan, int32_t bits);
 
