@@ -77,6 +77,8 @@ def parse_args():
                         "own CUDA arm (oracle/_ref_cuda) against this library on config 1 and the Forrest shape; pca: the "
                         "searchlight PCA template on the template workload's hemisphere (10 subjects)")
     p.add_argument("--grid-step", type=int, default=16)
+    p.add_argument("--grid-bits", type=int, choices=[32, 64], default=64,
+                   help="grid workload: float64 search (64) or its plain FP32 form (32)")
     p.add_argument("--ref-seconds", type=float, default=0.0,
                    help="reference arm: seconds of CPU work per step (default: 150 s over all steps)")
     return p.parse_args()
@@ -1139,6 +1141,7 @@ def run_grid(args):
     sls = w.sls.subset(np.arange(0, w.sls.count, args.grid_step))
     tr, te = H.ensemble_indices(w.nt, 1, 5, 10, 10, rank)
     plan = Plan(w.nt, w.nv, sls.indices, sls.offsets, sls.dists, sls.radius)
+    plan.set_grid_precision(args.grid_bits)
     dev = torch.device("cuda", local)
     dX = torch.from_numpy(np.asfortranarray(w.X).ravel(order="F")).to(dev)
     dY = torch.from_numpy(np.asfortranarray(w.Y).ravel(order="F")).to(dev)
@@ -1188,10 +1191,10 @@ def run_grid(args):
     dom = int(np.argmax(ms))
     n3 = float((sls.sizes.astype(np.float64) ** 3).sum())
     roof = None
-    if L.KERNEL_KINDS[dom] == "jacobi64" and ms[dom] > 0:
+    if L.KERNEL_KINDS[dom] in ("jacobi64", "jacobi32") and ms[dom] > 0:
         achieved = 9.0 * n3 * len(tr) * K / (ms[dom] / 1e3) / 1e12
         peak = float(peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops")))
-        roof = {"bound": "tensor", "kernel": "jacobi64 (eigenvector mode)", "achieved": achieved, "peak": peak,
+        roof = {"bound": "tensor", "kernel": f"{L.KERNEL_KINDS[dom]} (eigenvector mode)", "achieved": achieved, "peak": peak,
                 "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
                 "peak_source": f"{peak_src} bf16 sustained",
                 "fp64_simt": {"peak_nominal": FP64_NOMINAL_TFLOPS, "frac": achieved / FP64_NOMINAL_TFLOPS},
@@ -1217,7 +1220,8 @@ def run_grid(args):
             ts.append(time.perf_counter() - t1)
         e2e = {"value": sls.count * K / sum(ts), "unit": UNIT, "h2d_bytes_per_step": int(2 * w.nt * w.nv * 8),
                "d2h_bytes_per_step": int(plan.nnz * 8 + sls.count * 4),
-               "path": "ha_searchlight_ridge_grid_b200 host float64 in, host CSC values out (+=)"}
+               "path": "ha_searchlight_ridge_grid_b200 host float64 in, host CSC values out (+=)"
+                       + ("; the host entry is float64 whatever --grid-bits" if args.grid_bits == 32 else "")}
 
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -1229,7 +1233,8 @@ def run_grid(args):
         sizes = sls.sizes
         out = {"metric": "searchlight ridge grid searches/sec", "value": value, "unit": UNIT, "n_gpus": 1,
                "steps": K, "warmup": args.warmup, "ms_per_step": total_ms / K, "higher_is_better": True,
-               "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+               "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.grid_bits == 64 else "f32",
+               "data": "synthetic",
                "config": {"workload": "ridge_grid", "nv": w.nv, "nt": w.nt, "searchlights": sls.count,
                           "searchlight_subset": f"every {args.grid_step}th of {w.sls.count}",
                           "sl_size_min": int(sizes.min()), "sl_size_max": int(sizes.max()),
