@@ -1530,8 +1530,11 @@ __global__ void __launch_bounds__(256) k_tc_ns_finish(const TcWork *__restrict__
 // 1e-4, the level of the converged directions' residue) gives their bases L_E, L_F, which must be
 // orthonormal already (L^T L = I to 1e-3: the extracted directions are fully null, not partly
 // converged), Gram-Schmidt cleans them, and T <- (I - U_0 U_0^T) T + U_0 V_0^T.  Searchlights that
-// fail a check keep kFlagIllCond and go to the float64 re-solve.  E and F use the searchlight's
-// P and iterate planes (free after the iteration) as FP32 scratch.
+// fail a check keep kFlagIllCond and go to the float64 re-solve.  E and F are never formed: the
+// factorisation is left-looking and reads only the diagonal (1 - the squared column norms of T or
+// T^T) and the at most kTcNullMax + 1 pivot columns (e_p - S^T S(:, p)), O(d n^2) work instead of
+// 2 n^3.  The projection coefficients U_0^T T go to the searchlight's P planes (free after the
+// iteration) as FP32 scratch.
 constexpr int kTcNullMax = 8;
 
 __device__ __forceinline__ float block_sum256(float v, float *red) {
@@ -1544,47 +1547,67 @@ __device__ __forceinline__ float block_sum256(float v, float *red) {
 	return t;
 }
 
+// r[i] = sum_k S(k, i) u(k) for i < n, S(k, i) = S0[k sk + i si], u = the shared vector v, or S(:, i)
+// itself when v is null.  One thread per i when i runs contiguously in memory (si == 1), else one
+// warp per i with k across the lanes (sk == 1): both read memory in order across a warp.
+__device__ __forceinline__ void tc_cols_dot(const float *__restrict__ S0, int64_t sk, int64_t si, int n,
+                                            const float *v, float *r) {
+	if (si == 1) {
+		for (int i = threadIdx.x; i < n; i += blockDim.x) {
+			float acc = 0.f;
+			for (int k = 0; k < n; k++) {
+				const float x = S0[k * sk + i];
+				acc = fmaf(x, v ? v[k] : x, acc);
+			}
+			r[i] = acc;
+		}
+	} else {
+		const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+		for (int i = threadIdx.x >> 5; i < n; i += nw) {
+			float acc = 0.f;
+			for (int k = lane; k < n; k += 32) {
+				const float x = S0[k * sk + i * si];
+				acc = fmaf(x, v ? v[k] : x, acc);
+			}
+			acc = warp_sum(acc);
+			if (lane == 0) r[i] = acc;
+		}
+	}
+}
+
 __global__ void __launch_bounds__(256) k_tc_complete(const TcWork *__restrict__ work, float *__restrict__ Tscr,
                                                      __nv_bfloat16 *__restrict__ Xp, __nv_bfloat16 *__restrict__ Pp,
                                                      SlStats *__restrict__ stats, int t_rowmajor) {
+	(void)Xp;
 	const TcWork w = work[blockIdx.x];
 	if (!(stats[w.slot].flags & kFlagIllCond)) return;
 	const int n = w.n;
 	float *T = Tscr + w.tofs;
-	float *E = reinterpret_cast<float *>(Pp + w.pofs);
-	float *F = reinterpret_cast<float *>(Xp + w.xofs);
+	float *Cs = reinterpret_cast<float *>(Pp + w.pofs);  // d x n projection coefficients
 	const int64_t ti = t_rowmajor ? n : 1, tj = t_rowmajor ? 1 : n;  // T(i, j) = T[i ti + j tj]
-	__shared__ float ps[16][65], qs[16][65];
 	__shared__ float Lv[2][kTcNullMax][kTcMaxNp];
+	__shared__ float dg[kTcMaxNp], vp[kTcMaxNp], col[kTcMaxNp];
 	__shared__ float red[8];
+	__shared__ int redi[8];
 	__shared__ float s_best;
 	__shared__ int s_piv, s_d[2], s_bad;
-	GemmArgs<float> g;
-	g.M = n; g.N = n; g.K = n;
-	g.d = nullptr; g.alpha = -1.f;
-	g.E = nullptr; g.ei = 0; g.ej = 0; g.beta = 0.f;
-	g.ci = n; g.cj = 1;
-	// E(i, j) = delta - sum_k T(k, i) T(k, j);  F(i, j) = delta - sum_k T(i, k) T(j, k)
-	g.P = T; g.pk = ti; g.pi = tj; g.Q = T; g.qk = ti; g.qj = tj; g.C = E;
-	block_gemm(g, ps, qs);
-	g.P = T; g.pk = tj; g.pi = ti; g.Q = T; g.qk = tj; g.qj = ti; g.C = F;
-	block_gemm(g, ps, qs);
-	for (int i = threadIdx.x; i < n; i += blockDim.x) {
-		E[(int64_t)i * n + i] += 1.f;
-		F[(int64_t)i * n + i] += 1.f;
-	}
 	if (threadIdx.x == 0) s_bad = 0;
-	__syncthreads();
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 	for (int m = 0; m < 2; m++) {
-		float *M = m ? F : E;
+		// M = I - S^T S with S(k, i) = T(k, i) (m = 0: E, the right null space) or T(i, k) (m = 1: F,
+		// the left null space)
+		const int64_t sk = m ? tj : ti, si = m ? ti : tj;
+		tc_cols_dot(T, sk, si, n, nullptr, col);
+		__syncthreads();
+		for (int i = threadIdx.x; i < n; i += blockDim.x) dg[i] = 1.f - col[i];
 		int d = 0;
 		for (;;) {
+			__syncthreads();
 			// largest remaining diagonal entry (first index on ties)
 			float best = -1.f;
 			int bi = 0;
 			for (int i = threadIdx.x; i < n; i += blockDim.x) {
-				const float v = M[(int64_t)i * n + i];
+				const float v = dg[i];
 				if (v > best) { best = v; bi = i; }
 			}
 			for (int o = 16; o > 0; o >>= 1) {
@@ -1592,16 +1615,13 @@ __global__ void __launch_bounds__(256) k_tc_complete(const TcWork *__restrict__ 
 				const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
 				if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
 			}
-			__syncthreads();
-			if (lane == 0) { red[warp] = best; reinterpret_cast<volatile int *>(qs)[warp] = bi; }
+			if (lane == 0) { red[warp] = best; redi[warp] = bi; }
 			__syncthreads();
 			if (threadIdx.x == 0) {
 				float b = -1.f;
 				int p = 0;
-				for (int q = 0; q < 8; q++) {
-					const int pq = reinterpret_cast<volatile int *>(qs)[q];
-					if (red[q] > b || (red[q] == b && pq < p)) { b = red[q]; p = pq; }
-				}
+				for (int q = 0; q < 8; q++)
+					if (red[q] > b || (red[q] == b && redi[q] < p)) { b = red[q]; p = redi[q]; }
 				s_best = b;
 				s_piv = p;
 			}
@@ -1613,13 +1633,18 @@ __global__ void __launch_bounds__(256) k_tc_complete(const TcWork *__restrict__ 
 			}
 			const int p = s_piv;
 			const float inv = rsqrtf(s_best);
-			for (int i = threadIdx.x; i < n; i += blockDim.x) Lv[m][d][i] = M[(int64_t)i * n + p] * inv;
+			// column p of M minus the earlier factor columns: L_d = (e_p - S^T S(:, p) - sum_j L_j L_j(p)) / sqrt(M_pp)
+			for (int k = threadIdx.x; k < n; k += blockDim.x) vp[k] = T[k * sk + p * si];
 			__syncthreads();
-			for (int64_t e = threadIdx.x; e < (int64_t)n * n; e += blockDim.x) {
-				const int i = (int)(e / n), j = (int)(e - (int64_t)i * n);
-				M[e] -= Lv[m][d][i] * Lv[m][d][j];
+			tc_cols_dot(T, sk, si, n, vp, col);
+			__syncthreads();
+			for (int i = threadIdx.x; i < n; i += blockDim.x) {
+				float v = (i == p ? 1.f : 0.f) - col[i];
+				for (int j = 0; j < d; j++) v -= Lv[m][j][i] * Lv[m][j][p];
+				v *= inv;
+				Lv[m][d][i] = v;
+				dg[i] -= v * v;
 			}
-			__syncthreads();
 			d++;
 		}
 		if (threadIdx.x == 0) s_d[m] = d;
@@ -1656,21 +1681,50 @@ __global__ void __launch_bounds__(256) k_tc_complete(const TcWork *__restrict__ 
 			__syncthreads();
 		}
 	}
-	// T <- (I - U_0 U_0^T) T + U_0 V_0^T  (U_0 = the left null basis from F, V_0 from E); the
-	// projection is applied column by column of T through the shared coefficients c = U_0^T T(:, j)
-	for (int j = 0; j < n; j++) {
-		float c[kTcNullMax];
-		for (int a = 0; a < d; a++) {
-			float v = 0.f;
-			for (int i = threadIdx.x; i < n; i += blockDim.x) v += Lv[1][a][i] * T[i * ti + j * tj];
-			c[a] = block_sum256(v, red);
+	// T <- (I - U_0 U_0^T) T + U_0 V_0^T  (U_0 = the left null basis from F, V_0 from E): first the
+	// coefficients c(a, j) = U_0(:, a)^T T(:, j) of every column (one thread per column for row-major
+	// T, one warp per column for column-major T), then every entry independently
+	if (tj == 1) {
+		for (int j = threadIdx.x; j < n; j += blockDim.x) {
+			float c[kTcNullMax];
+#pragma unroll
+			for (int a = 0; a < kTcNullMax; a++) c[a] = 0.f;
+			for (int i = 0; i < n; i++) {
+				const float t = T[i * ti + j];
+#pragma unroll
+				for (int a = 0; a < kTcNullMax; a++)
+					if (a < d) c[a] = fmaf(Lv[1][a][i], t, c[a]);
+			}
+#pragma unroll
+			for (int a = 0; a < kTcNullMax; a++)
+				if (a < d) Cs[a * n + j] = c[a];
 		}
-		for (int i = threadIdx.x; i < n; i += blockDim.x) {
-			float v = T[i * ti + j * tj];
-			for (int a = 0; a < d; a++) v += Lv[1][a][i] * (Lv[0][a][j] - c[a]);
-			T[i * ti + j * tj] = v;
+	} else {
+		for (int j = warp; j < n; j += blockDim.x >> 5) {
+			float c[kTcNullMax];
+#pragma unroll
+			for (int a = 0; a < kTcNullMax; a++) c[a] = 0.f;
+			for (int i = lane; i < n; i += 32) {
+				const float t = T[i + j * tj];
+#pragma unroll
+				for (int a = 0; a < kTcNullMax; a++)
+					if (a < d) c[a] = fmaf(Lv[1][a][i], t, c[a]);
+			}
+#pragma unroll
+			for (int a = 0; a < kTcNullMax; a++)
+				if (a < d) {
+					const float sum = warp_sum(c[a]);
+					if (lane == 0) Cs[a * n + j] = sum;
+				}
 		}
-		__syncthreads();
+	}
+	__syncthreads();
+	for (int64_t e = threadIdx.x; e < (int64_t)n * n; e += blockDim.x) {
+		const int r = (int)(e / n), q = (int)(e - (int64_t)r * n);
+		const int i = t_rowmajor ? r : q, j = t_rowmajor ? q : r;
+		float v = T[e];
+		for (int a = 0; a < d; a++) v += Lv[1][a][i] * (Lv[0][a][j] - Cs[a * n + j]);
+		T[e] = v;
 	}
 	if (threadIdx.x == 0) {
 		SlStats st = stats[w.slot];
