@@ -212,3 +212,9 @@ def test_weights_c_abi_vs_live_reference(hlib, seed, uniform):
     ours = H.searchlight_weights(sls, ds, None if uniform else s.radius, 642)
     ref = R.searchlight_weights(s.indices, s.offsets, None if uniform else s.dists, 0.0 if uniform else s.radius)
     assert np.array_equal(ours, ref)
+
+
+def test_grid_precision_argument_errors(hlib):
+    # a plan is needed, and only 32 or 64 bits are accepted (checked before any device work)
+    for bits in (32, 64, 16, 0):
+        assert hlib.ha_b200_plan_set_grid_precision(None, bits) == L.ERROR_ARG
