@@ -1656,7 +1656,7 @@ int reduce_chunk64(HaB200Plan *P, Chunk &ch, int out_kind, double *d_vals, cudaS
 // as many as fit the grid scratch budget, and each one's per-slot scratch base offsets.
 struct GridBatch {
 	int i0, i1;
-	int64_t total;  // float64 elements of grid scratch
+	int64_t total;  // elements of grid scratch (float64 or float32, by the search's arithmetic)
 };
 
 void grid_plan_chunk(const Chunk &ch, const GridParams &gp, bool fp32, std::vector<GridBatch> &bt,
@@ -1719,8 +1719,8 @@ int grid_chunk_launch_t(HaB200Plan *P, Chunk &ch, const double *d_X, const doubl
 				const cudaStream_t bs = g_fan.at((int)bi);
 				const SlWork *wk = d_work + x0;
 				// Gram into the V scratch, its pivoted Cholesky factor into the A scratch
-				{ HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16, Real><<<x1 - x0, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_X, nt, tr, md.tr_n, V, G, gp, 0); }
-				{ HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16, Real><<<x1 - x0, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_Y, nt, tr, md.tr_n, A, G, gp, 1); }
+				{ HA_LAUNCH(f32 ? kHaB200KXcov32 : kHaB200KXcov64, bs); k_xcov_rows<16, Real><<<x1 - x0, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_X, nt, tr, md.tr_n, V, G, gp, 0); }
+				{ HA_LAUNCH(f32 ? kHaB200KXcov32 : kHaB200KXcov64, bs); k_xcov_rows<16, Real><<<x1 - x0, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_Y, nt, tr, md.tr_n, A, G, gp, 1); }
 				{ HA_LAUNCH(kHaB200KRidge, bs); k_pchol<Real><<<x1 - x0, kBlock, pchol_smem(b.rpl, sizeof(Real)), bs>>>(wk, V, A, P->stats.p); }
 				{
 					HA_LAUNCH(f32 ? kHaB200KJacobi32 : kHaB200KJacobi64, bs);
@@ -1870,8 +1870,8 @@ int eigen_chunk(HaB200Plan *P, Chunk &ch, const double *d_X, const double *d_Y, 
 		const Bucket &b = beig[bi];
 		const cudaStream_t bs = g_fan.at((int)bi);
 		const SlWork *wk = d_work + b.first;
-		{ HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16, Real><<<b.count, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_X, P->nt, d_rows, n_rows, V, nullptr, gp, 0); }
-		if (d_Y) { HA_LAUNCH(kHaB200KXcov64, bs); k_xcov_rows<16, Real><<<b.count, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_Y, P->nt, d_rows, n_rows, Cout, nullptr, gp, 2); }
+		{ HA_LAUNCH(f32 ? kHaB200KXcov32 : kHaB200KXcov64, bs); k_xcov_rows<16, Real><<<b.count, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_X, P->nt, d_rows, n_rows, V, nullptr, gp, 0); }
+		if (d_Y) { HA_LAUNCH(f32 ? kHaB200KXcov32 : kHaB200KXcov64, bs); k_xcov_rows<16, Real><<<b.count, kBlock, 0, bs>>>(wk, P->idx.p, d_X, d_Y, P->nt, d_rows, n_rows, Cout, nullptr, gp, 2); }
 		{ HA_LAUNCH(kHaB200KRidge, bs); k_pchol<Real><<<b.count, kBlock, pchol_smem(b.rpl, sizeof(Real)), bs>>>(wk, V, A, P->stats.p); }
 		{
 			HA_LAUNCH(f32 ? kHaB200KJacobi32 : kHaB200KJacobi64, bs);
