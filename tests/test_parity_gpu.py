@@ -552,7 +552,7 @@ def test_ridge_grid_fp32_vs_fp64(gpu, lo, hi):
     if same.all():
         berr = relf(v32, v64)
         print(f"fp32 grid: betas rel-Frobenius {berr:.2e}")
-        assert berr <= 1e-2
+        assert berr <= 1e-4  # 4e-7 to 6e-6 measured on a B200 for the three cases
 
 
 def test_ridge_grid_device_deterministic(gpu):
