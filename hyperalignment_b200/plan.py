@@ -121,7 +121,8 @@ class Plan:
         return {"s_min": smin, "s_max": smax, "flags": flags, "sweeps": sweeps}
 
     def local_transforms(self, first: int, n: int):
-        """Unweighted, unscaled T_s of searchlights [first, first+n) from the last run (row-major if CSR)."""
+        """Unweighted, unscaled T_s of searchlights [first, first+n) from the last run: T_s after a CSR
+        run, T_s transposed after a CSC run (the T scratch is column-major then)."""
         sizes = np.diff(self.offsets[first:first + n + 1])
         buf = np.empty(int((sizes.astype(np.int64) ** 2).sum()), dtype=np.float32)
         L.check(self.lib.ha_b200_plan_local_transforms(self.handle, first, n,

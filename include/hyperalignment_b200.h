@@ -351,8 +351,9 @@ int ha_b200_plan_set_grid_precision(HaB200Plan *plan, int32_t bits);
 
 /*
  * Per-searchlight local transforms of the last device run, for testing:
- * copies T_s (n_s x n_s, row-major, float32, unweighted and unscaled) of
- * searchlights [first, first + n) into host out (sum of n_s^2 floats).
+ * copies T_s (n_s x n_s, float32, unweighted and unscaled; row-major after a
+ * CSR-ordered run, column-major after a CSC-ordered one) of searchlights
+ * [first, first + n) into host out (sum of n_s^2 floats).
  */
 int ha_b200_plan_local_transforms(const HaB200Plan *plan, int32_t first, int32_t n, float *out);
 

@@ -122,15 +122,18 @@ def test_tc_is_deterministic(gpu):
     assert a.tobytes() == b.tobytes()
 
 
-def test_tc_rank_deficient_searchlights(gpu):
+@pytest.mark.parametrize("out_kind", [L.OUT_CSR, L.OUT_CSC])  # T row-major / column-major in the completion
+def test_tc_rank_deficient_searchlights(gpu, out_kind):
     """Exactly singular A keeps zero singular values the iteration cannot grow: the iteration
     stalls and the null spaces are completed (flag 16), keeping T orthogonal; X @ T and T on the
     row space of A are unique and match the oracle."""
     w = W.small_case(seed=9, nv=642, nt=100, lo=30, hi=60)
     mask = W.duplicate_columns(w.X, w.sls, 0.5, np.random.default_rng(1))
     assert mask.sum() > 0
-    plan, _ = _device_run(w, L.SOLVER_TC)
+    plan, _ = _device_run(w, L.SOLVER_TC, out_kind=out_kind)
     Ts = plan.local_transforms(0, w.sls.count)
+    if out_kind == L.OUT_CSC:  # the T scratch is column-major after a CSC run
+        Ts = [t.T for t in Ts]
     worst = 0.0
     for q in np.flatnonzero(mask)[:40]:
         sl = w.sls.indices[w.sls.offsets[q]:w.sls.offsets[q + 1]]
