@@ -21,6 +21,12 @@ e2e       the C ABI dense entry point (ha_searchlight_procrustes_dense, backend 
 roofline  dominant kernel (per-kind CUDA event times recorded by the library)
 cpu_baseline  the reference C library (oracle/_ref, cpu64 arm, all host threads) on a
           bounded sample of the same searchlights
+config4_ridge_grid_full  the ridge grid search over all 40962 searchlights of 50-500 vertices
+          (float64, cost grids checked against the oracle on a sample), with its plain FP32
+          form on the same inputs as plain_fp32 (winners and costs against float64)
+config5_learned  the mixed-precision learned proposal on the held-out subject against the plain
+          FP32 full grid on the same searchlights (the float64 grid and learned form beside them)
+--no-extras  skips the two config fields (N > 1 runs never have them)
 --impl reference  times only the reference CPU implementation (rank 0 of any N)
 """
 
